@@ -1,0 +1,247 @@
+"""hunyuansc25_b200 — B200-native multilevel k-way graph partitioner.
+
+Python mirror of the reference's partition entry point
+(``hunyuangraph_PartitionGraph``, hunyuangraph_partitiongraph.h:284-347) over the
+C ABI in ``include/hp_partition.h``.  Everything runs in the CUDA library
+``lib/libhp_b200.so`` (sm_100a); there is no CPU fallback: if the library or a
+CUDA device is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from ._abi import (ERROR_NAMES, HP_OK, HP_TRACE_ADJNCY, HP_TRACE_ADJWGT, HP_TRACE_CMAP,
+                   HP_TRACE_MATCH, HP_TRACE_VWGT, HP_TRACE_WHERE_FINAL, HP_TRACE_WHERE_START,
+                   HP_TRACE_XADJ, PROTOTYPES, HpOptions, HpStats, default_options)
+
+__all__ = [
+    "HpError", "Context", "partition_graph", "PartitionGraph", "default_options", "HpOptions",
+    "HpStats", "library_path", "load_library",
+]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def library_path() -> str:
+    return os.path.join(_HERE, "lib", "libhp_b200.so")
+
+
+class HpError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        self.code = code
+        name = ERROR_NAMES.get(code, str(code))
+        msg = f"{what}: {name}" if what else name
+        lib = _LIB
+        if lib is not None:
+            try:
+                msg += f" ({lib.hp_strerror(code).decode()})"
+            except Exception:  # pragma: no cover
+                pass
+        super().__init__(msg)
+
+
+def load_library():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        path = library_path()
+        if not os.path.exists(path):
+            raise FileNotFoundError(
+                f"{path} is missing: build it with `python -m hunyuansc25_b200.build`")
+        lib = C.CDLL(path)
+        for name, (res, args) in PROTOTYPES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = lib
+    return _LIB
+
+
+def _check(rc, what):
+    if rc != HP_OK:
+        raise HpError(rc, what)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _p32(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+class Context:
+    """One device arena + per-call state (reentrant replacement of the
+    reference's file-scope globals, hunyuangraph_GPU_memory.h:18-32)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = C.c_void_p()
+        _check(self.lib.hp_context_create(device, C.byref(h)), "hp_context_create")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.hp_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- partition ----------------------------------------------------------------
+    def partition(self, xadj, adjncy, nparts, vwgt=None, adjwgt=None, ubfactor=1.03,
+                  tpwgts=None, options: HpOptions | None = None):
+        """Host arrays in, (part, edgecut) out."""
+        xadj = _i32(xadj)
+        adjncy = _i32(adjncy)
+        vwgt = None if vwgt is None else _i32(vwgt)
+        adjwgt = None if adjwgt is None else _i32(adjwgt)
+        n = xadj.shape[0] - 1
+        part = np.empty(max(n, 1), dtype=np.int32)
+        cut = C.c_int64()
+        tp = None if tpwgts is None else np.ascontiguousarray(tpwgts, dtype=np.float32)
+        opt = options if options is not None else default_options()
+        rc = self.lib.hp_partition(self.h, n, _p32(xadj), _p32(adjncy), _p32(vwgt), _p32(adjwgt),
+                                   nparts, None if tp is None else tp.ctypes.data_as(C.POINTER(C.c_float)),
+                                   C.c_float(ubfactor), C.byref(opt), _p32(part), C.byref(cut))
+        _check(rc, "hp_partition")
+        return part[:n], cut.value
+
+    def partition_graph(self, g, nparts, ubfactor=1.03, tpwgts=None, options=None):
+        return self.partition(g.xadj, g.adjncy, nparts, g.vwgt, g.adjwgt, ubfactor, tpwgts, options)
+
+    def partition_device(self, xadj, adjncy, nparts, vwgt=None, adjwgt=None, ubfactor=1.03,
+                         tpwgts=None, options: HpOptions | None = None, stream=None, part=None):
+        """torch CUDA int32 tensors in (device-resident), (part tensor, cut) out."""
+        import torch
+        n = xadj.numel() - 1
+        if part is None:
+            part = torch.empty(max(n, 1), dtype=torch.int32, device=xadj.device)
+        cut = C.c_int64()
+        tp = None if tpwgts is None else np.ascontiguousarray(tpwgts, dtype=np.float32)
+        opt = options if options is not None else default_options()
+        s = stream if stream is not None else torch.cuda.current_stream(xadj.device)
+        rc = self.lib.hp_partition_device(
+            self.h, n, adjncy.numel(), C.c_void_p(xadj.data_ptr()), C.c_void_p(adjncy.data_ptr()),
+            C.c_void_p(vwgt.data_ptr()) if vwgt is not None else None,
+            C.c_void_p(adjwgt.data_ptr()) if adjwgt is not None else None, nparts,
+            None if tp is None else tp.ctypes.data_as(C.POINTER(C.c_float)), C.c_float(ubfactor),
+            C.byref(opt), C.c_void_p(s.cuda_stream), C.c_void_p(part.data_ptr()), C.byref(cut))
+        _check(rc, "hp_partition_device")
+        return part[:n], cut.value
+
+    def partition_batch(self, graphs, nparts, ubfactor=1.03, options=None):
+        """Partition many independent graphs; returns (list of part arrays, cuts)."""
+        G = len(graphs)
+        nparts = np.ascontiguousarray(np.broadcast_to(np.asarray(nparts, np.int32), (G,)))
+        ub = np.ascontiguousarray(np.broadcast_to(np.asarray(ubfactor, np.float32), (G,)))
+        vtx = np.zeros(G + 1, np.int64)
+        edg = np.zeros(G + 1, np.int64)
+        for i, g in enumerate(graphs):
+            vtx[i + 1] = vtx[i] + g.nvtxs
+            edg[i + 1] = edg[i] + g.nedges
+        xadj = np.concatenate([g.xadj for g in graphs]).astype(np.int32)
+        adj = np.concatenate([g.adjncy for g in graphs]).astype(np.int32)
+        vw = np.concatenate([g.vwgt for g in graphs]).astype(np.int32)
+        ew = np.concatenate([g.adjwgt for g in graphs]).astype(np.int32)
+        part = np.empty(max(int(vtx[-1]), 1), np.int32)
+        cuts = np.zeros(G, np.int64)
+        opt = options if options is not None else default_options()
+        I64 = C.POINTER(C.c_int64)
+        rc = self.lib.hp_partition_batch(self.h, G, vtx.ctypes.data_as(I64), edg.ctypes.data_as(I64),
+                                         _p32(xadj), _p32(adj), _p32(vw), _p32(ew), _p32(nparts),
+                                         ub.ctypes.data_as(C.POINTER(C.c_float)), C.byref(opt),
+                                         _p32(part), cuts.ctypes.data_as(I64))
+        _check(rc, "hp_partition_batch")
+        return [part[vtx[i]:vtx[i + 1]] for i in range(G)], cuts
+
+    def stats(self) -> HpStats:
+        st = HpStats()
+        _check(self.lib.hp_last_stats(self.h, C.byref(st)), "hp_last_stats")
+        return st
+
+    # ---- trace ----------------------------------------------------------------------
+    @property
+    def trace_nlevels(self) -> int:
+        return int(self.lib.hp_trace_nlevels(self.h))
+
+    def trace_level(self, level):
+        n = C.c_int32()
+        m = C.c_int64()
+        cs = C.c_int64()
+        cf = C.c_int64()
+        _check(self.lib.hp_trace_level(self.h, level, C.byref(n), C.byref(m), C.byref(cs),
+                                       C.byref(cf)), "hp_trace_level")
+        return n.value, m.value, cs.value, cf.value
+
+    def trace_array(self, level, what):
+        n, m, _, _ = self.trace_level(level)
+        size = {HP_TRACE_XADJ: n + 1, HP_TRACE_ADJNCY: m, HP_TRACE_ADJWGT: m}.get(what, n)
+        out = np.empty(max(size, 1), dtype=np.int32)
+        rc = self.lib.hp_trace_copy(self.h, level, what, _p32(out), out.shape[0])
+        if rc != HP_OK:
+            return None
+        return out[:size]
+
+    # ---- primitives -------------------------------------------------------------------
+    def scan_exclusive(self, d_in, d_out=None, stream=None):
+        """Exclusive int32 scan of a CUDA tensor; returns a tensor of n+1 entries."""
+        import torch
+        n = d_in.numel()
+        if d_out is None:
+            d_out = torch.empty(n + 1, dtype=torch.int32, device=d_in.device)
+        s = stream if stream is not None else torch.cuda.current_stream(d_in.device)
+        _check(self.lib.hp_scan_exclusive_i32(self.h, C.c_void_p(d_in.data_ptr()),
+                                              C.c_void_p(d_out.data_ptr()), n,
+                                              C.c_void_p(s.cuda_stream)), "hp_scan_exclusive_i32")
+        return d_out
+
+    def edgecut_device(self, xadj, adjncy, adjwgt, where, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(xadj.device)
+        cut = C.c_int64()
+        _check(self.lib.hp_edgecut_device(self.h, xadj.numel() - 1, C.c_void_p(xadj.data_ptr()),
+                                          C.c_void_p(adjncy.data_ptr()),
+                                          C.c_void_p(adjwgt.data_ptr()) if adjwgt is not None else None,
+                                          C.c_void_p(where.data_ptr()), C.c_void_p(s.cuda_stream),
+                                          C.byref(cut)), "hp_edgecut_device")
+        return cut.value
+
+
+_DEFAULT_CTX = None
+
+
+def _default_ctx() -> Context:
+    global _DEFAULT_CTX
+    if _DEFAULT_CTX is None:
+        _DEFAULT_CTX = Context(0)
+    return _DEFAULT_CTX
+
+
+def partition_graph(xadj, adjncy, nparts, vwgt=None, adjwgt=None, ubfactor=1.03, tpwgts=None,
+                    options=None):
+    """Functional form of ``hunyuangraph_PartitionGraph``: returns (part, edgecut)."""
+    return _default_ctx().partition(xadj, adjncy, nparts, vwgt, adjwgt, ubfactor, tpwgts, options)
+
+
+def PartitionGraph(nvtxs, xadj, adjncy, vwgt, adjwgt, nparts, tpwgts, ubvec, part):
+    """Argument-for-argument mirror of the reference's
+    ``hunyuangraph_PartitionGraph(nvtxs, xadj, adjncy, vwgt, adjwgt, nparts, tpwgts,
+    ubvec, part)`` (hunyuangraph_partitiongraph.h:284): writes into ``part``."""
+    ub = float(ubvec[0]) if ubvec is not None else 1.03
+    p, _ = partition_graph(np.asarray(xadj)[: nvtxs + 1], adjncy, nparts, vwgt, adjwgt, ub, tpwgts)
+    part[:nvtxs] = p

@@ -1,0 +1,123 @@
+"""ctypes mirror of include/hp_partition.h (structs, constants, prototypes)."""
+from __future__ import annotations
+
+import ctypes as C
+
+HP_OK = 0
+HP_ERR_INVALID_ARG = -1
+HP_ERR_INVALID_GRAPH = -2
+HP_ERR_NOMEM = -3
+HP_ERR_CUDA = -4
+HP_ERR_TIMEOUT = -5
+HP_ERR_NO_DEVICE = -6
+HP_ERR_UNSUPPORTED = -7
+HP_ERR_INTERNAL = -8
+HP_MAX_PARTS = 16384
+HP_OPTIONS_VERSION = 1
+
+HP_TRACE_XADJ = 0
+HP_TRACE_ADJNCY = 1
+HP_TRACE_ADJWGT = 2
+HP_TRACE_VWGT = 3
+HP_TRACE_MATCH = 4
+HP_TRACE_CMAP = 5
+HP_TRACE_WHERE_START = 6
+HP_TRACE_WHERE_FINAL = 7
+
+ERROR_NAMES = {
+    HP_OK: "HP_OK",
+    HP_ERR_INVALID_ARG: "HP_ERR_INVALID_ARG",
+    HP_ERR_INVALID_GRAPH: "HP_ERR_INVALID_GRAPH",
+    HP_ERR_NOMEM: "HP_ERR_NOMEM",
+    HP_ERR_CUDA: "HP_ERR_CUDA",
+    HP_ERR_TIMEOUT: "HP_ERR_TIMEOUT",
+    HP_ERR_NO_DEVICE: "HP_ERR_NO_DEVICE",
+    HP_ERR_UNSUPPORTED: "HP_ERR_UNSUPPORTED",
+    HP_ERR_INTERNAL: "HP_ERR_INTERNAL",
+}
+
+
+class HpOptions(C.Structure):
+    _fields_ = [
+        ("version", C.c_int32),
+        ("coarsen_to", C.c_int32),
+        ("match_rounds", C.c_int32),
+        ("refine_patience", C.c_int32),
+        ("init_starts", C.c_int32),
+        ("fm_passes", C.c_int32),
+        ("max_levels", C.c_int32),
+        ("learned", C.c_int32),
+        ("validate", C.c_int32),
+        ("trace", C.c_int32),
+        ("seed", C.c_uint64),
+    ]
+
+
+def default_options(**overrides) -> HpOptions:
+    """Same defaults as hp_options_default() (checked by a test)."""
+    o = HpOptions()
+    o.version = HP_OPTIONS_VERSION
+    o.coarsen_to = 0
+    o.match_rounds = 6
+    o.refine_patience = 5
+    o.init_starts = 256
+    o.fm_passes = 10
+    o.max_levels = 64
+    o.learned = 0
+    o.validate = 1
+    o.trace = 0
+    o.seed = 1
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    return o
+
+
+class HpStats(C.Structure):
+    _fields_ = [
+        ("edgecut", C.c_int64),
+        ("max_excess", C.c_int64),
+        ("tvwgt", C.c_int64),
+        ("nlevels", C.c_int32),
+        ("coarsest_nvtxs", C.c_int32),
+        ("coarsest_nedges", C.c_int64),
+        ("refine_passes", C.c_int32),
+        ("kernel_launches", C.c_int32),
+        ("ms_total", C.c_float),
+        ("ms_coarsen", C.c_float),
+        ("ms_init", C.c_float),
+        ("ms_uncoarsen", C.c_float),
+        ("ms_h2d", C.c_float),
+        ("ms_d2h", C.c_float),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+I32P = C.POINTER(C.c_int32)
+I64P = C.POINTER(C.c_int64)
+F32P = C.POINTER(C.c_float)
+
+# name -> (restype, argtypes); every symbol include/hp_partition.h declares.
+PROTOTYPES = {
+    "hp_options_default": (None, [C.POINTER(HpOptions)]),
+    "hp_strerror": (C.c_char_p, [C.c_int]),
+    "hp_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "hp_context_destroy": (None, [C.c_void_p]),
+    "hp_partition": (C.c_int, [C.c_void_p, C.c_int32, I32P, I32P, I32P, I32P, C.c_int32, F32P,
+                               C.c_float, C.POINTER(HpOptions), I32P, I64P]),
+    "hp_partition_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_int32, F32P, C.c_float,
+                                      C.POINTER(HpOptions), C.c_void_p, C.c_void_p, I64P]),
+    "hp_last_stats": (C.c_int, [C.c_void_p, C.POINTER(HpStats)]),
+    "hp_trace_nlevels": (C.c_int, [C.c_void_p]),
+    "hp_trace_level": (C.c_int, [C.c_void_p, C.c_int, I32P, I64P, I64P, I64P]),
+    "hp_trace_copy": (C.c_int, [C.c_void_p, C.c_int, C.c_int, I32P, C.c_int64]),
+    "hp_partition_batch": (C.c_int, [C.c_void_p, C.c_int32, I64P, I64P, I32P, I32P, I32P, I32P,
+                                     I32P, F32P, C.POINTER(HpOptions), I32P, I64P]),
+    "hp_scan_exclusive_i32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                                        C.c_void_p]),
+    "hp_edgecut_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, I64P]),
+    "hunyuangraph_PartitionGraph": (None, [I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P]),
+}

@@ -1,0 +1,587 @@
+// hp_api.cu — C ABI (include/hp_partition.h): contexts, the V-cycle driver,
+// statistics, the level trace and the legacy hunyuangraph_PartitionGraph shim.
+//
+// Reference entry point: hunyuangraph_PartitionGraph
+// (hunyuangraph_partitiongraph.h:284-347) and the V-cycle
+// hunyuangraph_kway_partition (:13-149).  The reference allocates 80 % of the
+// free device memory at every call (hunyuangraph_GPU_memory.h:42-76), forces
+// unit weights and exits on error; here a context keeps one arena sized from
+// (n, m) and grown on demand, the caller's weights are used, and every failure
+// is an error code.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "hp_internal.cuh"
+
+#define HP_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+__global__ void validate_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
+                                const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt,
+                                const int32_t *__restrict__ vwgt, unsigned *status)
+{
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    bool bad = false;
+    for (int64_t v = tid; v < n; v += stride) {
+        int32_t b = xadj[v], e = xadj[v + 1];
+        if (b > e || b < 0 || e > m) { bad = true; continue; }
+        if (vwgt && vwgt[v] < 0) bad = true;
+        for (int32_t j = b; j < e; j++) {
+            int32_t u = adjncy[j];
+            if (u < 0 || u >= n || u == v) bad = true;
+            if (adjwgt && adjwgt[j] <= 0) bad = true;
+        }
+    }
+    if (tid == 0 && (xadj[0] != 0 || xadj[n] != m)) bad = true;
+    if (bad) atomicOr(status, HP_STATUS_BAD_GRAPH);
+}
+
+__global__ void sum_kernel(int64_t n, const int32_t *__restrict__ a, unsigned long long *out)
+{
+    long long acc = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += a[i];
+    hp::block_add_to<256>(acc, out);
+}
+
+__global__ void final_pw_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__restrict__ vwgt,
+                                unsigned long long *pw, int32_t k, unsigned *status)
+{
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        int32_t p = where[v];
+        if (p < 0 || p >= k) { atomicOr(status, HP_STATUS_OVERFLOW); continue; }
+        atomicAdd(&pw[p], (unsigned long long)vwgt[v]);
+    }
+}
+
+__global__ void fill_ones_kernel(int64_t n, int32_t *p)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = 1;
+}
+
+inline unsigned gsz(hp_context *c, int64_t n)
+{
+    int64_t g = (n + 255) / 256;
+    int64_t cap = (int64_t)c->sm_count * 16;
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(g, cap));
+}
+
+int ensure_arena(hp_context *c, size_t bytes)
+{
+    if (c->arena && c->arena_cap >= bytes) return HP_OK;
+    if (c->arena) {
+        cudaFree(c->arena);
+        c->arena = nullptr;
+        c->arena_cap = 0;
+    }
+    void *p = nullptr;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return HP_ERR_NOMEM;
+    }
+    c->arena = (char *)p;
+    c->arena_cap = bytes;
+    return HP_OK;
+}
+
+void reset_arena(hp_context *c)
+{
+    c->lo = 0;
+    c->hi = c->arena_cap;
+    c->oom = false;
+    c->levels.clear();
+    c->trace_valid = false;
+}
+
+size_t estimate_arena(int64_t n, int64_t m)
+{
+    return (size_t)(160 * n + 40 * m) + ((size_t)256 << 20);
+}
+
+int32_t default_coarsen_to(int32_t nparts)
+{
+    int32_t thr = nparts * 8;   // hunyuangraph_partitiongraph.h:298-302
+    if (thr > 1024) thr = std::max(1024, nparts * 2);
+    return thr;
+}
+
+// The V-cycle on the level-0 graph already placed in c->levels[0].
+int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, int64_t *edgecut)
+{
+    HpLevel &g0 = c->levels[0];
+    const int32_t n = g0.n;
+    hp_stats &st = c->stats;
+    unsigned long long *sc = c->d_scal;
+
+    if (c->opt.validate) {
+        HP_LAUNCH(c, validate_kernel, gsz(c, n), 256, 0, n, g0.m, g0.xadj, g0.adjncy, g0.adjwgt,
+                  g0.vwgt, c->d_status);
+    }
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 2, c->stream));
+    HP_LAUNCH(c, sum_kernel, gsz(c, n), 256, 0, (int64_t)n, g0.vwgt, &sc[0]);
+    long long tv = 0;
+    HP_TRY(hp_read_scalars(c, &sc[0], sizeof(long long), &tv));
+    HP_TRY(hp_check_status(c));
+    if (tv >= INT32_MAX) return HP_ERR_UNSUPPORTED;
+    st.tvwgt = tv;
+
+    const int32_t thr = c->opt.coarsen_to > 0 ? c->opt.coarsen_to : default_coarsen_to(nparts);
+    const int64_t maxvwgt = (3 * (int64_t)tv) / (2 * (int64_t)thr);
+
+    HP_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    HP_TRY(hp_coarsen(c, thr, maxvwgt));
+    HP_CUDA(cudaEventRecord(c->ev[2], c->stream));
+
+    for (auto &l : c->levels) {
+        l.where = lalloc_t<int32_t>(c, l.n);
+        HP_CHECK_OOM(c);
+    }
+    std::vector<int64_t> opt(nparts), maxp(nparts);
+    hp_part_targets(tv, nparts, tpwgts, ubfactor, opt.data(), maxp.data());
+    const int64_t ub2 = hp_bisect_ub_fx(ubfactor, nparts);
+    HpLevel &cg = c->levels.back();
+    HP_TRY(hp_fill_i32(c, cg.where, cg.n, 0));   // every vertex gets a part below; never garbage
+    HP_TRY(hp_initial_partition(c, cg, nparts, opt.data(), ub2, cg.where));
+    HP_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    HP_TRY(hp_uncoarsen(c, nparts, opt.data(), maxp.data()));
+    HP_CUDA(cudaEventRecord(c->ev[4], c->stream));
+
+    // exact report of the final partition (also checks the tracked cut)
+    const size_t mark = c->hi;
+    unsigned long long *pw = ralloc_t<unsigned long long>(c, nparts);
+    HP_CHECK_OOM(c);
+    HP_CUDA(cudaMemsetAsync(pw, 0, sizeof(unsigned long long) * nparts, c->stream));
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 2, c->stream));
+    HpLevel &f = c->levels[0];
+    HP_TRY(hp_edgecut_launch(c, n, f.xadj, f.adjncy, f.adjwgt, f.where, &sc[0]));
+    HP_LAUNCH(c, final_pw_kernel, gsz(c, n), 256, 0, n, f.where, f.vwgt, pw, nparts, c->d_status);
+    std::vector<unsigned long long> hpw(nparts);
+    HP_CUDA(cudaMemcpyAsync(hpw.data(), pw, sizeof(unsigned long long) * nparts, cudaMemcpyDeviceToHost, c->stream));
+    long long cut2 = 0;
+    HP_TRY(hp_read_scalars(c, &sc[0], sizeof(long long), &cut2));
+    HP_TRY(hp_check_status(c));
+    c->hi = mark;
+    const int64_t cut = cut2 / 2;
+    if (cut != f.cut_final) {
+        fprintf(stderr, "hp: internal error: tracked cut %lld != recomputed cut %lld\n",
+                (long long)f.cut_final, (long long)cut);
+        return HP_ERR_INTERNAL;
+    }
+    int64_t ex = INT64_MIN;
+    for (int32_t p = 0; p < nparts; p++) ex = std::max<int64_t>(ex, (int64_t)hpw[p] - maxp[p]);
+    st.edgecut = cut;
+    st.max_excess = ex;
+    st.nlevels = (int32_t)c->levels.size();
+    st.coarsest_nvtxs = cg.n;
+    st.coarsest_nedges = cg.m;
+    if (edgecut) *edgecut = cut;
+    return HP_OK;
+}
+
+int begin_call(hp_context *c, const hp_options *opt, void *stream)
+{
+    if (!c) return HP_ERR_INVALID_ARG;
+    if (opt) {
+        if (opt->version != HP_OPTIONS_VERSION) return HP_ERR_INVALID_ARG;
+        c->opt = *opt;
+    } else {
+        hp_options_default(&c->opt);
+    }
+    HP_CUDA(cudaSetDevice(c->device));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    c->launches = 0;
+    memset(&c->stats, 0, sizeof(c->stats));
+    unsigned zero = 0;
+    HP_CUDA(cudaMemcpyAsync(c->d_status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
+    return HP_OK;
+}
+
+void finish_stats(hp_context *c)
+{
+    cudaStreamSynchronize(c->stream);
+    float ms = 0;
+    hp_stats &st = c->stats;
+    if (cudaEventElapsedTime(&ms, c->ev[0], c->ev[5]) == cudaSuccess) st.ms_total = ms;
+    if (cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]) == cudaSuccess) st.ms_coarsen = ms;
+    if (cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]) == cudaSuccess) st.ms_init = ms;
+    if (cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]) == cudaSuccess) st.ms_uncoarsen = ms;
+    st.kernel_launches = c->launches;
+    c->trace_valid = c->opt.trace != 0;
+}
+
+}  // namespace
+
+// ---- shared helpers -------------------------------------------------------------
+int hp_read_scalars(hp_context *c, const void *d_src, size_t nbytes, void *dst)
+{
+    if (nbytes > sizeof(long long) * HP_NSCAL) return HP_ERR_INVALID_ARG;
+    HP_CUDA(cudaMemcpyAsync(c->h_pin, d_src, nbytes, cudaMemcpyDeviceToHost, c->stream));
+    HP_CUDA(cudaStreamSynchronize(c->stream));
+    memcpy(dst, c->h_pin, nbytes);
+    return HP_OK;
+}
+
+int hp_check_status(hp_context *c)
+{
+    unsigned s = 0;
+    HP_TRY(hp_read_scalars(c, c->d_status, sizeof(unsigned), &s));
+    if (s & HP_STATUS_SPIN_TIMEOUT) return HP_ERR_TIMEOUT;
+    if (s & HP_STATUS_BAD_GRAPH) return HP_ERR_INVALID_GRAPH;
+    if (s & HP_STATUS_OVERFLOW) return HP_ERR_INTERNAL;
+    return HP_OK;
+}
+
+void hp_part_targets(int64_t tvwgt, int32_t nparts, const float *tpwgts, float ubfactor,
+                     int64_t *opt, int64_t *maxp)
+{
+    double sum = 0.0;
+    if (tpwgts)
+        for (int32_t p = 0; p < nparts; p++) sum += (double)tpwgts[p];
+    for (int32_t p = 0; p < nparts; p++) {
+        double frac = tpwgts ? (double)tpwgts[p] / sum : 1.0 / (double)nparts;
+        double t = (double)tvwgt * frac;
+        double u = (double)ubfactor * t;
+        opt[p] = (int64_t)floor(t);
+        maxp[p] = (int64_t)floor(u);
+        if (maxp[p] < opt[p]) maxp[p] = opt[p];
+    }
+}
+
+int64_t hp_bisect_ub_fx(float ubfactor, int32_t nparts)
+{
+    double ub2 = nparts > 1 ? pow((double)ubfactor, 1.0 / log((double)nparts)) : (double)ubfactor;
+    return (int64_t)floor(ub2 * 65536.0 + 0.5);
+}
+
+// ---- C ABI ------------------------------------------------------------------------
+HP_API void hp_options_default(hp_options *o)
+{
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->version = HP_OPTIONS_VERSION;
+    o->coarsen_to = 0;
+    o->match_rounds = 6;
+    o->refine_patience = 5;
+    o->init_starts = 256;
+    o->fm_passes = 10;
+    o->max_levels = 64;
+    o->learned = 0;
+    o->validate = 1;
+    o->trace = 0;
+    o->seed = 1;
+}
+
+HP_API const char *hp_strerror(int code)
+{
+    switch (code) {
+    case HP_OK: return "ok";
+    case HP_ERR_INVALID_ARG: return "invalid argument";
+    case HP_ERR_INVALID_GRAPH: return "invalid graph (CSR validation failed)";
+    case HP_ERR_NOMEM: return "device memory exhausted";
+    case HP_ERR_CUDA: return "CUDA runtime error";
+    case HP_ERR_TIMEOUT: return "bounded device wait expired";
+    case HP_ERR_NO_DEVICE: return "no CUDA device";
+    case HP_ERR_UNSUPPORTED: return "unsupported request";
+    case HP_ERR_INTERNAL: return "internal consistency check failed";
+    default: return "unknown error";
+    }
+}
+
+HP_API int hp_context_create(int device, hp_context **out)
+{
+    if (!out) return HP_ERR_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return HP_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return HP_ERR_INVALID_ARG;
+    hp_context *c = new hp_context();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return HP_ERR_NO_DEVICE; }
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    bool ok = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) == cudaSuccess;
+    void *blk = nullptr;
+    ok = ok && cudaMalloc(&blk, 256 + sizeof(unsigned long long) * HP_NSCAL) == cudaSuccess;
+    if (ok) {
+        c->d_status = (unsigned *)blk;
+        c->d_scal = (unsigned long long *)((char *)blk + 256);
+    }
+    ok = ok && cudaMallocHost((void **)&c->h_pin, sizeof(long long) * HP_NSCAL) == cudaSuccess;
+    for (int i = 0; ok && i < 8; i++) ok = cudaEventCreate(&c->ev[i]) == cudaSuccess;
+    ok = ok && hp_refine_init() == HP_OK;
+    if (!ok) {
+        cudaGetLastError();
+        hp_context_destroy(c);
+        return HP_ERR_CUDA;
+    }
+    *out = c;
+    return HP_OK;
+}
+
+HP_API void hp_context_destroy(hp_context *c)
+{
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+    if (c->arena) cudaFree(c->arena);
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->h_pin) cudaFreeHost(c->h_pin);
+    for (int i = 0; i < 8; i++)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+static int check_args(int32_t nvtxs, const void *xadj, const void *adjncy, int32_t nparts,
+                      float ubfactor, const void *part)
+{
+    if (nvtxs < 0 || !xadj || !part) return HP_ERR_INVALID_ARG;
+    if (nvtxs > 0 && !adjncy) return HP_ERR_INVALID_ARG;
+    if (nparts < 1) return HP_ERR_INVALID_ARG;
+    if (nparts > HP_MAX_PARTS) return HP_ERR_UNSUPPORTED;
+    if (!(ubfactor >= 1.0f) || !std::isfinite(ubfactor)) return HP_ERR_INVALID_ARG;
+    return HP_OK;
+}
+
+// Places the level-0 graph (copying host or device inputs into the arena).
+static int place_level0(hp_context *c, int32_t n, int64_t m, const int32_t *xadj, const int32_t *adjncy,
+                        const int32_t *vwgt, const int32_t *adjwgt, cudaMemcpyKind kind)
+{
+    c->levels.emplace_back();
+    HpLevel &g = c->levels[0];
+    g.n = n;
+    g.m = m;
+    g.xadj = lalloc_t<int32_t>(c, (int64_t)n + 1);
+    g.adjncy = lalloc_t<int32_t>(c, m);
+    g.adjwgt = lalloc_t<int32_t>(c, m);
+    g.vwgt = lalloc_t<int32_t>(c, n);
+    HP_CHECK_OOM(c);
+    HP_CUDA(cudaMemcpyAsync(g.xadj, xadj, sizeof(int32_t) * ((size_t)n + 1), kind, c->stream));
+    if (m > 0) HP_CUDA(cudaMemcpyAsync(g.adjncy, adjncy, sizeof(int32_t) * (size_t)m, kind, c->stream));
+    if (adjwgt) {
+        if (m > 0) HP_CUDA(cudaMemcpyAsync(g.adjwgt, adjwgt, sizeof(int32_t) * (size_t)m, kind, c->stream));
+    } else if (m > 0) {
+        HP_LAUNCH(c, fill_ones_kernel, gsz(c, m), 256, 0, m, g.adjwgt);
+    }
+    if (vwgt) {
+        if (n > 0) HP_CUDA(cudaMemcpyAsync(g.vwgt, vwgt, sizeof(int32_t) * (size_t)n, kind, c->stream));
+    } else if (n > 0) {
+        HP_LAUNCH(c, fill_ones_kernel, gsz(c, n), 256, 0, (int64_t)n, g.vwgt);
+    }
+    return HP_OK;
+}
+
+static int partition_common(hp_context *c, int32_t n, int64_t m, const int32_t *xadj,
+                            const int32_t *adjncy, const int32_t *vwgt, const int32_t *adjwgt,
+                            int32_t nparts, const float *tpwgts, float ubfactor, bool host,
+                            int32_t *part, int64_t *edgecut)
+{
+    size_t want = estimate_arena(n, m);
+    int rc = HP_ERR_NOMEM;
+    for (int attempt = 0; attempt < 4 && rc == HP_ERR_NOMEM; attempt++) {
+        HP_TRY(ensure_arena(c, want));
+        reset_arena(c);
+        unsigned zero = 0;
+        HP_CUDA(cudaMemcpyAsync(c->d_status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
+        HP_CUDA(cudaEventRecord(c->ev[0], c->stream));
+        rc = place_level0(c, n, m, xadj, adjncy, vwgt, adjwgt,
+                          host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice);
+        if (rc == HP_OK) HP_CUDA(cudaEventRecord(c->ev[6], c->stream));
+        if (rc == HP_OK) {
+            if (n == 0) {
+                if (edgecut) *edgecut = 0;
+                HP_CUDA(cudaEventRecord(c->ev[1], c->stream));
+                HP_CUDA(cudaEventRecord(c->ev[2], c->stream));
+                HP_CUDA(cudaEventRecord(c->ev[3], c->stream));
+                HP_CUDA(cudaEventRecord(c->ev[4], c->stream));
+            } else {
+                rc = vcycle(c, nparts, tpwgts, ubfactor, edgecut);
+            }
+        }
+        if (rc == HP_ERR_NOMEM) want *= 2;
+    }
+    if (rc != HP_OK) return rc;
+    if (n > 0) {
+        HpLevel &f = c->levels[0];
+        HP_CUDA(cudaEventRecord(c->ev[7], c->stream));
+        HP_CUDA(cudaMemcpyAsync(part, f.where, sizeof(int32_t) * (size_t)n,
+                                host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, c->stream));
+    }
+    HP_CUDA(cudaEventRecord(c->ev[5], c->stream));
+    finish_stats(c);
+    float ms = 0;
+    if (host && cudaEventElapsedTime(&ms, c->ev[0], c->ev[6]) == cudaSuccess) c->stats.ms_h2d = ms;
+    if (host && n > 0 && cudaEventElapsedTime(&ms, c->ev[7], c->ev[5]) == cudaSuccess) c->stats.ms_d2h = ms;
+    return HP_OK;
+}
+
+HP_API int hp_partition(hp_context *ctx, int32_t nvtxs, const int32_t *xadj, const int32_t *adjncy,
+                        const int32_t *vwgt, const int32_t *adjwgt, int32_t nparts, const float *tpwgts,
+                        float ubfactor, const hp_options *opt, int32_t *part, int64_t *edgecut)
+{
+    HP_TRY(check_args(nvtxs, xadj, adjncy, nparts, ubfactor, part));
+    const int64_t m = xadj[nvtxs];
+    if (xadj[0] != 0 || m < 0 || m > INT32_MAX) return HP_ERR_INVALID_GRAPH;
+    HP_TRY(begin_call(ctx, opt, nullptr));
+    return partition_common(ctx, nvtxs, m, xadj, adjncy, vwgt, adjwgt, nparts, tpwgts, ubfactor,
+                            true, part, edgecut);
+}
+
+HP_API int hp_partition_device(hp_context *ctx, int32_t nvtxs, int64_t nedges, const int32_t *d_xadj,
+                               const int32_t *d_adjncy, const int32_t *d_vwgt, const int32_t *d_adjwgt,
+                               int32_t nparts, const float *tpwgts, float ubfactor, const hp_options *opt,
+                               void *stream, int32_t *d_part, int64_t *edgecut)
+{
+    HP_TRY(check_args(nvtxs, d_xadj, d_adjncy, nparts, ubfactor, d_part));
+    if (nedges < 0 || nedges > INT32_MAX) return HP_ERR_INVALID_GRAPH;
+    HP_TRY(begin_call(ctx, opt, stream));
+    return partition_common(ctx, nvtxs, nedges, d_xadj, d_adjncy, d_vwgt, d_adjwgt, nparts, tpwgts,
+                            ubfactor, false, d_part, edgecut);
+}
+
+HP_API int hp_last_stats(const hp_context *ctx, hp_stats *out)
+{
+    if (!ctx || !out) return HP_ERR_INVALID_ARG;
+    *out = ctx->stats;
+    return HP_OK;
+}
+
+HP_API int hp_trace_nlevels(const hp_context *ctx)
+{
+    if (!ctx || !ctx->trace_valid) return 0;
+    return (int)ctx->levels.size();
+}
+
+HP_API int hp_trace_level(const hp_context *ctx, int level, int32_t *nvtxs, int64_t *nedges,
+                          int64_t *cut_start, int64_t *cut_final)
+{
+    if (!ctx || !ctx->trace_valid || level < 0 || level >= (int)ctx->levels.size()) return HP_ERR_INVALID_ARG;
+    const HpLevel &l = ctx->levels[level];
+    if (nvtxs) *nvtxs = l.n;
+    if (nedges) *nedges = l.m;
+    if (cut_start) *cut_start = l.cut_start;
+    if (cut_final) *cut_final = l.cut_final;
+    return HP_OK;
+}
+
+HP_API int hp_trace_copy(const hp_context *ctx, int level, int what, int32_t *dst, int64_t count)
+{
+    if (!ctx || !ctx->trace_valid || level < 0 || level >= (int)ctx->levels.size() || !dst)
+        return HP_ERR_INVALID_ARG;
+    const HpLevel &l = ctx->levels[level];
+    const int32_t *src = nullptr;
+    int64_t len = 0;
+    switch (what) {
+    case HP_TRACE_XADJ: src = l.xadj; len = (int64_t)l.n + 1; break;
+    case HP_TRACE_ADJNCY: src = l.adjncy; len = l.m; break;
+    case HP_TRACE_ADJWGT: src = l.adjwgt; len = l.m; break;
+    case HP_TRACE_VWGT: src = l.vwgt; len = l.n; break;
+    case HP_TRACE_MATCH: src = l.match; len = l.n; break;
+    case HP_TRACE_CMAP: src = l.cmap; len = l.n; break;
+    case HP_TRACE_WHERE_START: src = l.where_start; len = l.n; break;
+    case HP_TRACE_WHERE_FINAL: src = l.where_final; len = l.n; break;
+    default: return HP_ERR_INVALID_ARG;
+    }
+    if (!src || count < len) return HP_ERR_INVALID_ARG;
+    if (len == 0) return HP_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return HP_ERR_CUDA;
+    if (cudaMemcpy(dst, src, sizeof(int32_t) * (size_t)len, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return HP_ERR_CUDA;
+    return HP_OK;
+}
+
+HP_API int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *vtxdist,
+                              const int64_t *edgedist, const int32_t *xadj, const int32_t *adjncy,
+                              const int32_t *vwgt, const int32_t *adjwgt, const int32_t *nparts,
+                              const float *ubfactor, const hp_options *opt, int32_t *part,
+                              int64_t *edgecut)
+{
+    if (!ctx || ngraphs < 0 || !vtxdist || !edgedist || !xadj || !nparts || !ubfactor || !part)
+        return HP_ERR_INVALID_ARG;
+    for (int32_t gi = 0; gi < ngraphs; gi++) {
+        const int64_t v0 = vtxdist[gi], n = vtxdist[gi + 1] - v0, e0 = edgedist[gi];
+        int64_t cut = 0;
+        int rc = hp_partition(ctx, (int32_t)n, xadj + v0 + gi, adjncy + e0, vwgt ? vwgt + v0 : nullptr,
+                              adjwgt ? adjwgt + e0 : nullptr, nparts[gi], nullptr, ubfactor[gi], opt,
+                              part + v0, &cut);
+        if (rc != HP_OK) return rc;
+        if (edgecut) edgecut[gi] = cut;
+    }
+    return HP_OK;
+}
+
+HP_API int hp_scan_exclusive_i32(hp_context *ctx, const int32_t *d_in, int32_t *d_out, int64_t n,
+                                 void *stream)
+{
+    if (!ctx || n < 0 || (!d_in && n > 0) || !d_out) return HP_ERR_INVALID_ARG;
+    if (n >= INT32_MAX) return HP_ERR_UNSUPPORTED;
+    HP_CUDA(cudaSetDevice(ctx->device));
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    size_t need = (size_t)((n + 4096) / 4096 + 2) * 8 + ((size_t)1 << 20);
+    if (!ctx->arena || ctx->arena_cap < need) HP_TRY(ensure_arena(ctx, std::max(need, (size_t)64 << 20)));
+    reset_arena(ctx);
+    unsigned zero = 0;
+    HP_CUDA(cudaMemcpyAsync(ctx->d_status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    HP_TRY(hp_scan_excl(ctx, d_in, d_out, n));
+    return hp_check_status(ctx);
+}
+
+HP_API int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xadj, const int32_t *d_adjncy,
+                             const int32_t *d_adjwgt, const int32_t *d_where, void *stream, int64_t *cut)
+{
+    if (!ctx || nvtxs < 0 || !d_xadj || !d_where || !cut) return HP_ERR_INVALID_ARG;
+    HP_CUDA(cudaSetDevice(ctx->device));
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    HP_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(unsigned long long), ctx->stream));
+    if (d_adjwgt) {
+        HP_TRY(hp_edgecut_launch(ctx, nvtxs, d_xadj, d_adjncy, d_adjwgt, d_where, ctx->d_scal));
+    } else {
+        // unit weights: count cut entries through a ones array in the arena
+        int64_t m = 0;
+        int32_t last = 0;
+        HP_CUDA(cudaMemcpy(&last, d_xadj + nvtxs, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        m = last;
+        size_t need = sizeof(int32_t) * (size_t)(m + 1) + 4096;
+        if (!ctx->arena || ctx->arena_cap < need) HP_TRY(ensure_arena(ctx, std::max(need, (size_t)64 << 20)));
+        reset_arena(ctx);
+        int32_t *ones = ralloc_t<int32_t>(ctx, m);
+        HP_CHECK_OOM(ctx);
+        HP_LAUNCH(ctx, fill_ones_kernel, gsz(ctx, m), 256, 0, m, ones);
+        HP_TRY(hp_edgecut_launch(ctx, nvtxs, d_xadj, d_adjncy, ones, d_where, ctx->d_scal));
+    }
+    long long c2 = 0;
+    HP_TRY(hp_read_scalars(ctx, ctx->d_scal, sizeof(long long), &c2));
+    *cut = c2 / 2;
+    return HP_OK;
+}
+
+// ---- legacy drop-in ------------------------------------------------------------------
+static std::mutex g_legacy_mu;
+static hp_context *g_legacy = nullptr;
+
+HP_API void hunyuangraph_PartitionGraph(int *nvtxs, int *xadj, int *adjncy, int *vwgt, int *adjwgt,
+                                        int *nparts, float *tpwgts, float *ubvec, int *part)
+{
+    std::lock_guard<std::mutex> lk(g_legacy_mu);
+    if (!nvtxs || !nparts || !part) {
+        fprintf(stderr, "hunyuangraph_PartitionGraph: NULL argument\n");
+        return;
+    }
+    int rc = HP_OK;
+    if (!g_legacy) rc = hp_context_create(0, &g_legacy);
+    if (rc == HP_OK) {
+        int64_t cut = 0;
+        rc = hp_partition(g_legacy, *nvtxs, xadj, adjncy, vwgt, adjwgt, *nparts, tpwgts,
+                          ubvec ? ubvec[0] : 1.03f, nullptr, part, &cut);
+    }
+    if (rc != HP_OK) {
+        fprintf(stderr, "hunyuangraph_PartitionGraph: %s (%d)\n", hp_strerror(rc), rc);
+        for (int i = 0; i < *nvtxs; i++) part[i] = -1;
+    }
+}

@@ -1,0 +1,153 @@
+// hp_common.cuh — device helpers shared by every kernel file of the partitioner.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <climits>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "hp_partition.h"
+
+#define HP_FULL_MASK 0xffffffffu
+#define HP_INT_MAX 0x7fffffff
+
+// Device status word bits (ctx->d_status): set by kernels, read by the host.
+#define HP_STATUS_SPIN_TIMEOUT 1u   // a bounded look-back / flag wait gave up
+#define HP_STATUS_BAD_GRAPH    2u   // structural validation failed
+#define HP_STATUS_OVERFLOW     4u   // a capacity bound was exceeded (never expected)
+
+// Spin limit of every device-side wait (iterations with __nanosleep back-off).
+#define HP_SPIN_LIMIT (1u << 22)
+
+namespace hp {
+
+// splitmix64 finaliser (Vigna): the matching tie-break hash.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+}
+
+__host__ __device__ __forceinline__ uint64_t level_key(uint64_t seed, int32_t level)
+{
+    return mix64(seed ^ (0x6d61746368ULL + (uint64_t)level * 0x100000001b3ULL));
+}
+
+__host__ __device__ __forceinline__ uint32_t edge_tie(uint64_t lkey, int32_t a, int32_t b)
+{
+    uint32_t lo = (uint32_t)(a < b ? a : b), hi = (uint32_t)(a < b ? b : a);
+    return (uint32_t)(mix64(lkey ^ (((uint64_t)lo << 32) | hi)) >> 32);
+}
+
+// Matching candidate order: heavier edge, then lower tie key, then lower id.
+__host__ __device__ __forceinline__ bool better(int32_t w1, uint32_t h1, int32_t u1,
+                                                int32_t w2, uint32_t h2, int32_t u2)
+{
+    if (w1 != w2) return w1 > w2;
+    if (h1 != h2) return h1 < h2;
+    return u1 < u2;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__device__ __forceinline__ int warp_sum(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(HP_FULL_MASK, v, o);
+    return v;
+}
+
+__device__ __forceinline__ long long warp_sum64(long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(HP_FULL_MASK, v, o);
+    return v;
+}
+
+__device__ __forceinline__ long long warp_max64(long long v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        long long t = __shfl_xor_sync(HP_FULL_MASK, v, o);
+        v = t > v ? t : v;
+    }
+    return v;
+}
+
+// Inclusive warp scan.
+__device__ __forceinline__ int warp_incl_scan(int v)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(HP_FULL_MASK, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Block-wide sum into *out (atomic add of one value per block).
+template <int BLOCK>
+__device__ __forceinline__ void block_add_to(long long v, unsigned long long *out)
+{
+    __shared__ long long s_part[BLOCK / 32];
+    v = warp_sum64(v);
+    if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        long long t = threadIdx.x < BLOCK / 32 ? s_part[threadIdx.x] : 0;
+        t = warp_sum64(t);
+        if (threadIdx.x == 0 && t != 0) atomicAdd(out, (unsigned long long)t);
+    }
+}
+
+__host__ __device__ __forceinline__ int64_t iabs64(int64_t x) { return x < 0 ? -x : x; }
+
+// Weak-rebalance gain bucket with the float semantics of the reference's
+// gain_bucket (hunyuangraph_GPU_krefine.h:2477-2513); explicit _rn intrinsics
+// keep the device arithmetic identical to a host IEEE evaluation.  Upper clamp
+// 49 (the reference can reach 50, which aliases the next part's buckets).
+__device__ __forceinline__ int32_t gain_bucket(int32_t gain, int32_t vwgt)
+{
+    float g = __fdiv_rn((float)gain, (float)(vwgt > 0 ? vwgt : 1));
+    if (g > 0.0f) return 0;
+    if (g == 0.0f) return 1;
+    int32_t t = 25;
+    g = fabsf(g);
+    if (g < 1.0f) {
+        while (g < 1.0f) { g = __fmul_rn(g, 1.5f); t--; }
+        if (t < 2) t = 2;
+    } else {
+        while (g > 1.0f) { g = __fdiv_rn(g, 1.5f); t++; }
+        if (t > 49) t = 49;
+    }
+    return t;
+}
+
+inline unsigned div_up(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+
+}  // namespace hp
+
+// ---- host error handling ------------------------------------------------------
+#define HP_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            fprintf(stderr, "hp: CUDA error %s at %s:%d\n", cudaGetErrorString(e_),    \
+                    __FILE__, __LINE__);                                               \
+            return HP_ERR_CUDA;                                                        \
+        }                                                                              \
+    } while (0)
+
+#define HP_TRY(call)                  \
+    do {                              \
+        int rc_ = (call);             \
+        if (rc_ != HP_OK) return rc_; \
+    } while (0)

@@ -1,0 +1,128 @@
+// hp_internal.cuh — context, device arena and the interfaces between the kernel files.
+#pragma once
+
+#include <algorithm>
+#include <vector>
+
+#include "hp_common.cuh"
+
+// One coarsening level resident in the arena.
+struct HpLevel {
+    int32_t n = 0;
+    int64_t m = 0;
+    int32_t *xadj = nullptr, *adjncy = nullptr, *adjwgt = nullptr, *vwgt = nullptr;
+    int32_t *match = nullptr, *cmap = nullptr;        // set when a coarser level exists
+    int32_t *where = nullptr;                          // working partition
+    int32_t *where_start = nullptr, *where_final = nullptr;  // trace copies
+    int64_t cut_start = 0, cut_final = 0;
+};
+
+struct hp_context {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;   // stream of the current call
+    cudaStream_t own_stream = nullptr;
+
+    // Device arena: one allocation, used as a two-ended stack.  The low end
+    // holds the level chain and per-call state (lalloc), the high end holds
+    // temporaries released in LIFO order (ralloc).
+    char *arena = nullptr;
+    size_t arena_cap = 0, lo = 0, hi = 0;
+    bool oom = false;
+
+    // Small fixed device block: status word + scalar slots, and a pinned
+    // host mirror for blocking scalar reads.
+    unsigned *d_status = nullptr;
+    unsigned long long *d_scal = nullptr;   // HP_NSCAL slots
+    long long *h_pin = nullptr;             // HP_NSCAL slots, pinned
+
+    cudaEvent_t ev[8] = {};
+    int launches = 0;
+
+    hp_stats stats = {};
+    std::vector<HpLevel> levels;
+    bool trace_valid = false;
+    hp_options opt = {};
+};
+
+#define HP_NSCAL 64
+#define HP_ALIGN 256
+
+// ---- arena -------------------------------------------------------------------
+inline void *hp_lalloc(hp_context *c, size_t bytes)
+{
+    size_t b = (bytes + HP_ALIGN - 1) / HP_ALIGN * HP_ALIGN;
+    if (b == 0) b = HP_ALIGN;
+    if (c->lo + b > c->hi) { c->oom = true; return nullptr; }
+    void *p = c->arena + c->lo;
+    c->lo += b;
+    return p;
+}
+
+inline void *hp_ralloc(hp_context *c, size_t bytes)
+{
+    size_t b = (bytes + HP_ALIGN - 1) / HP_ALIGN * HP_ALIGN;
+    if (b == 0) b = HP_ALIGN;
+    if (c->hi < c->lo + b) { c->oom = true; return nullptr; }
+    c->hi -= b;
+    return c->arena + c->hi;
+}
+
+template <class T> inline T *lalloc_t(hp_context *c, int64_t n) { return (T *)hp_lalloc(c, sizeof(T) * (size_t)(n > 0 ? n : 1)); }
+template <class T> inline T *ralloc_t(hp_context *c, int64_t n) { return (T *)hp_ralloc(c, sizeof(T) * (size_t)(n > 0 ? n : 1)); }
+
+#define HP_CHECK_OOM(c) do { if ((c)->oom) return HP_ERR_NOMEM; } while (0)
+
+// Count and check every kernel launch.
+#define HP_LAUNCH(ctx, kernel, grid, block, smem, ...)                                      \
+    do {                                                                                    \
+        if ((grid) > 0) {                                                                   \
+            kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);                \
+            (ctx)->launches++;                                                              \
+            cudaError_t e__ = cudaGetLastError();                                           \
+            if (e__ != cudaSuccess) {                                                       \
+                fprintf(stderr, "hp: launch %s failed: %s\n", #kernel, cudaGetErrorString(e__)); \
+                return HP_ERR_CUDA;                                                         \
+            }                                                                               \
+        }                                                                                   \
+    } while (0)
+
+// Blocking read of nbytes from device into the pinned mirror, then dst.
+int hp_read_scalars(hp_context *c, const void *d_src, size_t nbytes, void *dst);
+// Status word check after a phase (spin timeouts, bad graph).
+int hp_check_status(hp_context *c);
+
+// ---- primitives (hp_scan.cu) --------------------------------------------------
+// Exclusive scan, n+1 outputs (out[n] = total). in == out allowed.
+int hp_scan_excl(hp_context *c, const int32_t *in, int32_t *out, int64_t n);
+// out[i] = base + i for i < n (iota)
+int hp_fill_i32(hp_context *c, int32_t *p, int64_t n, int32_t value);
+int hp_iota_i32(hp_context *c, int32_t *p, int64_t n);
+// Stable compaction of indices i < n with flag[i] != 0 into out; count -> *d_count.
+int hp_compact_flags(hp_context *c, const int32_t *flags, int64_t n, int32_t *out, int32_t *d_count);
+// Stable LSD radix sort of `bound` slots (count on device) by the low key_bits
+// bits of keys; ping-pongs with tkeys/tvals.  *in_tmp tells which pair holds
+// the result.
+int hp_sort_pairs(hp_context *c, int32_t *keys, int32_t *vals, int32_t *tkeys, int32_t *tvals,
+                  int64_t bound, const int32_t *d_count, int key_bits, bool *in_tmp);
+// Exact edge cut (int64) into *d_cut (device, accumulated; caller zeroes).
+int hp_edgecut_launch(hp_context *c, int32_t n, const int32_t *xadj, const int32_t *adjncy,
+                      const int32_t *adjwgt, const int32_t *where, unsigned long long *d_cut);
+
+// ---- coarsening (hp_coarsen.cu) -----------------------------------------------
+// Builds levels[1..] from levels[0]; returns HP_OK and fills c->levels.
+int hp_coarsen(hp_context *c, int32_t coarsen_to, int64_t maxvwgt);
+
+// ---- initial partition (hp_initpart.cu) ------------------------------------------
+int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_t *h_tw,
+                         int64_t ub2_fx, int32_t *d_where);
+
+// ---- refinement (hp_refine.cu) --------------------------------------------------
+int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int64_t *h_maxp);
+// One-time kernel attributes (dynamic shared memory above 48 KB).
+int hp_refine_init();
+
+// ---- targets shared with the host driver -----------------------------------------
+void hp_part_targets(int64_t tvwgt, int32_t nparts, const float *tpwgts, float ubfactor,
+                     int64_t *opt, int64_t *maxp);
+int64_t hp_bisect_ub_fx(float ubfactor, int32_t nparts);

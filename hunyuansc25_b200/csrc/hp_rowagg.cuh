@@ -1,0 +1,172 @@
+// hp_rowagg.cuh — "aggregate a row": gather (key, weight) entries, merge equal
+// keys by summing weights, drop an excluded key, and write the unique keys in
+// ascending order.  Used by contraction (key = coarse neighbour id, the self
+// key dropped) and by the gain table (key = neighbour's part).
+//
+// Size classes (chosen per row by its entry count):
+//   S   <= 32     one warp, register bitonic sort over the 32 lanes (shuffles)
+//   B   <= CAP    one CTA, shared-memory bitonic sort (CAP = 512 or 4096)
+//   D   larger    one CTA, dense accumulator + presence bitmap over the key
+//                 space, scanned in key order (global scratch per CTA for
+//                 contraction, shared memory for part keys)
+// Every class produces the same canonical row, so the class boundaries are a
+// performance choice only.
+#pragma once
+
+#include "hp_common.cuh"
+
+namespace hp {
+
+constexpr int32_t KEY_NONE = 0x7fffffff;
+
+// Warp-wide aggregation of up to 32 entries already held one per lane.
+// Writes unique keys/sums to out_k/out_w (if non-null) and returns the count
+// (same value in all lanes).
+__device__ __forceinline__ int warp_aggregate32(int32_t key, int32_t w, int32_t *out_k,
+                                                int32_t *out_w)
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            int32_t pk = __shfl_xor_sync(HP_FULL_MASK, key, j);
+            int32_t pw = __shfl_xor_sync(HP_FULL_MASK, w, j);
+            bool up = (lane & k) == 0;
+            bool lower = (lane & j) == 0;
+            bool take = lower ? (up ? pk < key : pk > key) : (up ? pk > key : pk < key);
+            if (take) { key = pk; w = pw; }
+        }
+    }
+    // suffix sums inside runs of equal keys
+    int32_t s = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int32_t t = __shfl_down_sync(HP_FULL_MASK, s, o);
+        int32_t kk = __shfl_down_sync(HP_FULL_MASK, key, o);
+        if (lane + o < 32 && kk == key) s += t;
+    }
+    int32_t prev = __shfl_up_sync(HP_FULL_MASK, key, 1);
+    bool head = key != KEY_NONE && (lane == 0 || prev != key);
+    unsigned hm = __ballot_sync(HP_FULL_MASK, head);
+    if (head && out_k) {
+        int r = __popc(hm & lanemask_lt());
+        out_k[r] = key;
+        out_w[r] = s;
+    }
+    return __popc(hm);
+}
+
+// CTA-wide shared-memory aggregation of len <= CAP entries staged in sk/sw
+// (entries beyond len must already be KEY_NONE up to the pow2 size P).
+template <int NT, int CAP>
+__device__ __forceinline__ int block_aggregate_smem(int32_t *sk, int32_t *sw, int P,
+                                                    int32_t *out_k, int32_t *out_w,
+                                                    int32_t *s_scan /* NT/32 + 2 */)
+{
+    const int tid = threadIdx.x;
+    // bitonic sort of P elements
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < P; i += NT) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    int32_t a = sk[i], b = sk[ixj];
+                    bool up = (i & k) == 0;
+                    if (up ? (a > b) : (a < b)) {
+                        sk[i] = b; sk[ixj] = a;
+                        int32_t t = sw[i]; sw[i] = sw[ixj]; sw[ixj] = t;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // heads and their positions: thread t owns elements [t*per, (t+1)*per)
+    const int per = (P + NT - 1) / NT;
+    const int lo = tid * per, hiE = min(lo + per, P);
+    int cnt = 0;
+    for (int i = lo; i < hiE; i++)
+        cnt += (sk[i] != KEY_NONE && (i == 0 || sk[i - 1] != sk[i]));
+    const int lane = tid & 31, wid = tid >> 5;
+    int incl = warp_incl_scan(cnt);
+    if (lane == 31) s_scan[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int t = lane < NT / 32 ? s_scan[lane] : 0;
+        int ti = warp_incl_scan(t);
+        if (lane < NT / 32) s_scan[lane] = ti - t;
+        if (lane == NT / 32 - 1) s_scan[NT / 32] = ti;
+    }
+    __syncthreads();
+    int pos = s_scan[wid] + incl - cnt;
+    const int total = s_scan[NT / 32];
+    for (int i = lo; i < hiE; i++) {
+        int32_t key = sk[i];
+        if (key == KEY_NONE || (i > 0 && sk[i - 1] == key)) continue;
+        int32_t sum = 0;
+        for (int j = i; j < P && sk[j] == key; j++) sum += sw[j];
+        out_k[pos] = key;
+        out_w[pos] = sum;
+        pos++;
+    }
+    __syncthreads();
+    return total;
+}
+
+// CTA-wide exclusive scan of one int per thread; returns exclusive value and
+// writes the block total to *total.
+template <int NT>
+__device__ __forceinline__ int block_excl_scan(int v, int *total, int32_t *s_scan)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int incl = warp_incl_scan(v);
+    if (lane == 31) s_scan[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int t = lane < NT / 32 ? s_scan[lane] : 0;
+        int ti = warp_incl_scan(t);
+        if (lane < NT / 32) s_scan[lane] = ti - t;
+        if (lane == NT / 32 - 1) s_scan[NT / 32] = ti;
+    }
+    __syncthreads();
+    int r = s_scan[wid] + incl - v;
+    *total = s_scan[NT / 32];
+    __syncthreads();
+    return r;
+}
+
+// Dense aggregation over key space [0, nkeys): dw[nkeys] (zero on entry and on
+// exit), bm[(nkeys+31)/32] presence bits (zero on entry and exit).  Entries
+// must have been accumulated into dw/bm by the caller (atomics) before the
+// barrier that precedes this call.  Writes keys in ascending order.
+template <int NT>
+__device__ __forceinline__ int dense_extract(int32_t *dw, unsigned *bm, int32_t nkeys,
+                                             int32_t *out_k, int32_t *out_w, int32_t *s_scan)
+{
+    const int nwords = (nkeys + 31) >> 5;
+    int running = 0;
+    for (int wb = 0; wb < nwords; wb += NT) {
+        int wi = wb + threadIdx.x;
+        unsigned word = wi < nwords ? bm[wi] : 0u;
+        int tot;
+        int p = running + block_excl_scan<NT>(__popc(word), &tot, s_scan);
+        if (word) {
+            bm[wi] = 0u;
+            while (word) {
+                int b = __ffs(word) - 1;
+                word &= word - 1;
+                int32_t k = (wi << 5) + b;
+                out_k[p] = k;
+                out_w[p] = dw[k];
+                dw[k] = 0;
+                p++;
+            }
+        }
+        running += tot;
+    }
+    __syncthreads();
+    return running;
+}
+
+}  // namespace hp

@@ -1,0 +1,308 @@
+// hp_scan.cu — single-pass decoupled look-back scan and small device primitives.
+//
+// Replaces the reference's recursive reduce-then-propagate prefix sum
+// (hunyuangraph_GPU_prefixsum.h:53-188), which launches three kernels per
+// recursion level and ends each level with cudaDeviceSynchronize().  Here one
+// launch scans the whole array: each CTA takes a dynamic tile index, publishes
+// its aggregate, and the first warp looks back over predecessor tiles (32 at a
+// time) until it meets an inclusive prefix.  Every wait is bounded
+// (HP_SPIN_LIMIT); on expiry the CTA sets HP_STATUS_SPIN_TIMEOUT and continues,
+// so a stalled predecessor can never hang the device.
+#include "hp_internal.cuh"
+
+namespace {
+
+constexpr int SCAN_BLOCK = 256;
+constexpr int SCAN_ITEMS = 16;
+constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;  // 4096
+constexpr unsigned long long FLAG_AGG = 1ull << 32;
+constexpr unsigned long long FLAG_PRE = 2ull << 32;
+
+__device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
+
+// Exclusive scan of in[0..n) into out[0..n] (out[n] = total); element n is a
+// virtual zero.  tile_status[ntiles] and *tile_counter must be zero on entry.
+__global__ void __launch_bounds__(SCAN_BLOCK)
+scan_excl_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n,
+                 unsigned long long *tile_status, unsigned *tile_counter, unsigned *status)
+{
+    __shared__ int32_t s[SCAN_TILE + SCAN_TILE / 32];
+    __shared__ int32_t s_warp[SCAN_BLOCK / 32];
+    __shared__ int32_t s_tile;
+    __shared__ int32_t s_excl;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+
+    if (tid == 0) s_tile = (int32_t)atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int64_t base = tile * SCAN_TILE;
+
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        int i = k * SCAN_BLOCK + tid;
+        int64_t g = base + i;
+        s[pad(i)] = (g < n) ? in[g] : 0;
+    }
+    __syncthreads();
+    int32_t v[SCAN_ITEMS];
+    int32_t local = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        v[k] = s[pad(tid * SCAN_ITEMS + k)];
+        local += v[k];
+    }
+    int32_t incl = hp::warp_incl_scan(local);
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int32_t t = lane < SCAN_BLOCK / 32 ? s_warp[lane] : 0;
+        int32_t ti = hp::warp_incl_scan(t);
+        if (lane < SCAN_BLOCK / 32) s_warp[lane] = ti - t;  // exclusive warp offsets
+        int32_t agg = __shfl_sync(HP_FULL_MASK, ti, SCAN_BLOCK / 32 - 1);
+        // look-back
+        int32_t excl = 0;
+        if (tile == 0) {
+            if (lane == 0) atomicExch(&tile_status[0], FLAG_PRE | (unsigned)agg);
+        } else {
+            if (lane == 0) atomicExch(&tile_status[tile], FLAG_AGG | (unsigned)agg);
+            int64_t pred = tile - 1;
+            for (;;) {
+                int64_t idx = pred - lane;
+                unsigned long long st = FLAG_PRE;  // virtual prefix 0 before tile 0
+                if (idx >= 0) {
+                    unsigned it = 0;
+                    for (;;) {
+                        st = *(volatile unsigned long long *)&tile_status[idx];
+                        if (st >> 32) break;
+                        if (++it > HP_SPIN_LIMIT) {
+                            atomicOr(status, HP_STATUS_SPIN_TIMEOUT);
+                            st = FLAG_PRE;
+                            break;
+                        }
+                        __nanosleep(32);
+                    }
+                }
+                unsigned pre_mask = __ballot_sync(HP_FULL_MASK, (st >> 32) == 2);
+                int32_t val = (int32_t)(unsigned)(st & 0xffffffffull);
+                if (pre_mask) {
+                    int first = __ffs(pre_mask) - 1;
+                    int32_t contrib = lane <= first ? val : 0;
+                    excl += hp::warp_sum(contrib);
+                    break;
+                }
+                excl += hp::warp_sum(val);
+                pred -= 32;
+            }
+            if (lane == 0) atomicExch(&tile_status[tile], FLAG_PRE | (unsigned)(excl + agg));
+        }
+        if (lane == 0) s_excl = excl;
+    }
+    __syncthreads();
+    int32_t run = s_excl + s_warp[wid] + incl - local;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        s[pad(tid * SCAN_ITEMS + k)] = run;
+        run += v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        int i = k * SCAN_BLOCK + tid;
+        int64_t g = base + i;
+        if (g <= n) out[g] = s[pad(i)];
+    }
+}
+
+__global__ void fill_kernel(int32_t *p, int64_t n, int32_t value)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = value;
+}
+
+__global__ void iota_kernel(int32_t *p, int64_t n)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = (int32_t)i;
+}
+
+__global__ void scatter_flags_kernel(const int32_t *flags, const int32_t *pos, int64_t n,
+                                     int32_t *out, int32_t *d_count)
+{
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        if (flags[i]) out[pos[i]] = (int32_t)i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *d_count = pos[n];
+}
+
+// Warp per vertex; int64 block partial sums.
+__global__ void __launch_bounds__(256)
+edgecut_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+               const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
+               unsigned long long *cut2)
+{
+    const int lane = threadIdx.x & 31;
+    long long acc = 0;
+    for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < n;
+         v += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int32_t wv = where[v];
+        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32)
+            if (where[adjncy[j]] != wv) acc += adjwgt[j];
+    }
+    hp::block_add_to<256>(acc, cut2);
+}
+
+inline unsigned grid_for(hp_context *c, int64_t n, int block)
+{
+    int64_t g = (n + block - 1) / block;
+    int64_t cap = (int64_t)c->sm_count * 16;
+    if (g > cap) g = cap;
+    return (unsigned)(g > 0 ? g : 1);
+}
+
+}  // namespace
+
+int hp_scan_excl(hp_context *c, const int32_t *in, int32_t *out, int64_t n)
+{
+    if (n < 0) return HP_ERR_INVALID_ARG;
+    const int64_t ntiles = (n + 1 + SCAN_TILE - 1) / SCAN_TILE;
+    size_t mark = c->hi;
+    auto *st = ralloc_t<unsigned long long>(c, ntiles + 1);
+    HP_CHECK_OOM(c);
+    unsigned *counter = (unsigned *)(st + ntiles);
+    HP_CUDA(cudaMemsetAsync(st, 0, sizeof(unsigned long long) * (size_t)(ntiles + 1), c->stream));
+    HP_LAUNCH(c, scan_excl_kernel, (unsigned)ntiles, SCAN_BLOCK, 0, in, out, n, st, counter,
+              c->d_status);
+    c->hi = mark;
+    return HP_OK;
+}
+
+int hp_fill_i32(hp_context *c, int32_t *p, int64_t n, int32_t value)
+{
+    if (n <= 0) return HP_OK;
+    HP_LAUNCH(c, fill_kernel, grid_for(c, n, 256), 256, 0, p, n, value);
+    return HP_OK;
+}
+
+int hp_iota_i32(hp_context *c, int32_t *p, int64_t n)
+{
+    if (n <= 0) return HP_OK;
+    HP_LAUNCH(c, iota_kernel, grid_for(c, n, 256), 256, 0, p, n);
+    return HP_OK;
+}
+
+int hp_compact_flags(hp_context *c, const int32_t *flags, int64_t n, int32_t *out, int32_t *d_count)
+{
+    size_t mark = c->hi;
+    int32_t *pos = ralloc_t<int32_t>(c, n + 1);
+    HP_CHECK_OOM(c);
+    HP_TRY(hp_scan_excl(c, flags, pos, n));
+    HP_LAUNCH(c, scatter_flags_kernel, grid_for(c, n, 256), 256, 0, flags, pos, n, out, d_count);
+    c->hi = mark;
+    return HP_OK;
+}
+
+int hp_edgecut_launch(hp_context *c, int32_t n, const int32_t *xadj, const int32_t *adjncy,
+                      const int32_t *adjwgt, const int32_t *where, unsigned long long *d_cut2)
+{
+    if (n <= 0) return HP_OK;
+    HP_LAUNCH(c, edgecut_kernel, grid_for(c, (int64_t)n * 32, 256), 256, 0, n, xadj, adjncy,
+              adjwgt, where, d_cut2);
+    return HP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Stable LSD radix sort of (key, value) int32 pairs, 8-bit digits.
+// Pass: per-tile digit histograms stored digit-major, one exclusive scan over
+// them, then a stable scatter in which every tile ranks its items per digit
+// (warp __match_any_sync + per-warp digit counters in shared memory).
+namespace {
+
+constexpr int RS_BLOCK = 256;
+constexpr int RS_ITEMS = 4;
+constexpr int RS_TILE = RS_BLOCK * RS_ITEMS;
+
+__global__ void __launch_bounds__(RS_BLOCK)
+radix_hist_kernel(const int32_t *__restrict__ keys, const int32_t *__restrict__ d_count,
+                  int shift, int32_t nblocks, int32_t *__restrict__ hist)
+{
+    __shared__ int32_t h[256];
+    const int32_t cnt = *d_count;
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
+    for (int r = 0; r < RS_ITEMS; r++) {
+        int64_t i = base + r * RS_BLOCK + threadIdx.x;
+        if (i < cnt) atomicAdd(&h[((unsigned)keys[i] >> shift) & 255u], 1);
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(RS_BLOCK)
+radix_scatter_kernel(const int32_t *__restrict__ kin, const int32_t *__restrict__ vin,
+                     const int32_t *__restrict__ d_count, int shift, int32_t nblocks,
+                     const int32_t *__restrict__ hscan, int32_t *__restrict__ kout,
+                     int32_t *__restrict__ vout)
+{
+    __shared__ int32_t run[256];                       // running per-digit offset of this tile
+    __shared__ int32_t wc[RS_BLOCK / 32][256];         // per-warp digit counts / offsets
+    const int32_t cnt = *d_count;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    run[threadIdx.x] = hscan[(int64_t)threadIdx.x * nblocks + blockIdx.x];
+    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
+    for (int r = 0; r < RS_ITEMS; r++) {
+        for (int w = 0; w < RS_BLOCK / 32; w++) wc[w][threadIdx.x] = 0;
+        __syncthreads();
+        int64_t i = base + r * RS_BLOCK + threadIdx.x;
+        bool valid = i < cnt;
+        int32_t k = valid ? kin[i] : 0, v = valid ? vin[i] : 0;
+        unsigned d = valid ? (((unsigned)k >> shift) & 255u) : 256u + lane;  // invalid: unique
+        unsigned peers = __match_any_sync(HP_FULL_MASK, d);
+        int rank = __popc(peers & hp::lanemask_lt());
+        if (valid && rank == 0) wc[wid][d] = __popc(peers);
+        __syncthreads();
+        {   // thread t owns digit t: turn warp counts into offsets
+            int32_t acc = run[threadIdx.x];
+            for (int w = 0; w < RS_BLOCK / 32; w++) {
+                int32_t t = wc[w][threadIdx.x];
+                wc[w][threadIdx.x] = acc;
+                acc += t;
+            }
+            run[threadIdx.x] = acc;
+        }
+        __syncthreads();
+        if (valid) {
+            int32_t p = wc[wid][d] + rank;
+            kout[p] = k;
+            vout[p] = v;
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+int hp_sort_pairs(hp_context *c, int32_t *keys, int32_t *vals, int32_t *tkeys, int32_t *tvals,
+                  int64_t bound, const int32_t *d_count, int key_bits, bool *in_tmp)
+{
+    *in_tmp = false;
+    if (bound <= 0) return HP_OK;
+    const int32_t nblocks = (int32_t)((bound + RS_TILE - 1) / RS_TILE);
+    const size_t mark = c->hi;
+    int32_t *hist = ralloc_t<int32_t>(c, (int64_t)nblocks * 256 + 1);
+    HP_CHECK_OOM(c);
+    int32_t *ka = keys, *va = vals, *kb = tkeys, *vb = tvals;
+    for (int shift = 0; shift < key_bits; shift += 8) {
+        HP_LAUNCH(c, radix_hist_kernel, (unsigned)nblocks, RS_BLOCK, 0, ka, d_count, shift, nblocks, hist);
+        HP_TRY(hp_scan_excl(c, hist, hist, (int64_t)nblocks * 256));
+        HP_LAUNCH(c, radix_scatter_kernel, (unsigned)nblocks, RS_BLOCK, 0, ka, va, d_count, shift, nblocks,
+                  hist, kb, vb);
+        std::swap(ka, kb);
+        std::swap(va, vb);
+        *in_tmp = !*in_tmp;
+    }
+    c->hi = mark;
+    return HP_OK;
+}

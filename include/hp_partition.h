@@ -1,0 +1,174 @@
+/*
+ * hp_partition.h — C ABI of the B200 multilevel k-way graph partitioner.
+ *
+ * Plain C types only: host or device pointers and sizes, int32 CSR, int64 cut.
+ * Every entry point returns HP_OK (0) or a negative HP_ERR_* code; nothing in
+ * the library calls exit().
+ *
+ * Reference interface replaced (HunyuanGraph, Elegancejiang/HunyuanSC25):
+ *   void hunyuangraph_PartitionGraph(int *nvtxs, int *xadj, int *adjncy,
+ *        int *vwgt, int *adjwgt, int *nparts, float *tpwgts, float *ubvec,
+ *        int *part)                       hunyuangraph_partitiongraph.h:284-347
+ *   prototype                             HunyuanGRAPH.h:57
+ * hp_partition() is the reentrant, error-returning form of that call; the
+ * legacy symbol hunyuangraph_PartitionGraph() below keeps the exact signature
+ * and forwards to it so existing callers relink unchanged.
+ *
+ * Behavioural differences from the reference entry point (deliberate):
+ *   - vwgt/adjwgt are honoured (the reference overwrites both with 1,
+ *     hunyuangraph_partitiongraph.h:220-221); NULL means unit weights.
+ *   - ubfactor is honoured (the reference hard-codes IMB 1.04,
+ *     hunyuangraph_define.h:8, hunyuangraph_GPU_uncoarsen.h:428-437).
+ *   - the edge cut is int64 (the reference uses int, hunyuangraph_graph.h:144).
+ *   - results are deterministic for a given seed (the reference matching is an
+ *     atomicCAS race, hunyuangraph_GPU_match.h:800-861).
+ */
+#ifndef HP_PARTITION_H
+#define HP_PARTITION_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HP_OK                   0
+#define HP_ERR_INVALID_ARG     -1  /* bad scalar argument (nparts, ubfactor, NULL pointer) */
+#define HP_ERR_INVALID_GRAPH   -2  /* CSR failed validation (range, self loop, weight) */
+#define HP_ERR_NOMEM           -3  /* device arena could not be sized or allocated */
+#define HP_ERR_CUDA            -4  /* a CUDA runtime call failed */
+#define HP_ERR_TIMEOUT         -5  /* a bounded device wait expired (status word set) */
+#define HP_ERR_NO_DEVICE       -6  /* no CUDA device / context could not be created */
+#define HP_ERR_UNSUPPORTED     -7  /* request outside the supported envelope (e.g. nparts > HP_MAX_PARTS) */
+#define HP_ERR_INTERNAL        -8  /* an internal consistency check failed (tracked vs exact cut) */
+
+#define HP_MAX_PARTS        16384  /* gain rows use a dense shared-memory part vector */
+
+#define HP_OPTIONS_VERSION      1
+
+/* Tunables; hp_options_default() fills the defaults listed beside each field. */
+typedef struct hp_options {
+    int32_t  version;          /* HP_OPTIONS_VERSION                                          */
+    int32_t  coarsen_to;       /* 0: reference rule 8k, or max(1024, 2k) if 8k > 1024
+                                  (hunyuangraph_partitiongraph.h:298-302)                     */
+    int32_t  match_rounds;     /* handshake rounds per level (default 6)                      */
+    int32_t  refine_patience;  /* refinement passes without improvement (default 5,
+                                  hunyuangraph_GPU_krefine.h:4659)                            */
+    int32_t  init_starts;      /* bisection trials per subproblem (default 256)              */
+    int32_t  fm_passes;        /* 2-way FM passes per trial (default 10,
+                                  hunyuangraph_admin.h:14)                                    */
+    int32_t  max_levels;       /* coarsening level cap (default 64)                           */
+    int32_t  learned;          /* 0 plain refinement, 1 MLP move proposals                    */
+    int32_t  validate;         /* 0 none, 1 structural check on the device (default)          */
+    int32_t  trace;            /* 1: keep every level for hp_trace_*() (tests)                */
+    uint64_t seed;             /* matching tie-break seed (default 1)                         */
+} hp_options;
+
+/* Timing and quality of the last call on a context. */
+typedef struct hp_stats {
+    int64_t edgecut;           /* exact int64 cut of the returned partition                   */
+    int64_t max_excess;        /* max_p (pwgts[p] - maxpwgt[p]); <= 0 means balanced          */
+    int64_t tvwgt;             /* total vertex weight                                         */
+    int32_t nlevels;           /* coarse levels built (level 0 = input)                       */
+    int32_t coarsest_nvtxs;
+    int64_t coarsest_nedges;
+    int32_t refine_passes;     /* total refinement passes over all levels                     */
+    int32_t kernel_launches;   /* kernels this library launched during the call              */
+    float   ms_total;          /* device time of the whole call (CUDA events)                 */
+    float   ms_coarsen;
+    float   ms_init;
+    float   ms_uncoarsen;
+    float   ms_h2d;            /* host<->device copies inside hp_partition() (0 for _device) */
+    float   ms_d2h;
+} hp_stats;
+
+typedef struct hp_context hp_context;
+
+void        hp_options_default(hp_options *opt);
+const char *hp_strerror(int code);
+
+/* A context owns one device arena and the per-call state; one context per
+ * thread (contexts share nothing). device = CUDA ordinal. */
+int  hp_context_create(int device, hp_context **out);
+void hp_context_destroy(hp_context *ctx);
+
+/* Partition a host CSR graph into nparts parts.
+ *   xadj[nvtxs+1], adjncy[xadj[nvtxs]], symmetric, 0-based, no self loops and
+ *   no duplicate edges; vwgt[nvtxs] (NULL = 1), adjwgt[xadj[nvtxs]] (NULL = 1);
+ *   tpwgts[nparts] target fractions (NULL = uniform); ubfactor >= 1.0.
+ * Output: part[nvtxs] in [0, nparts), *edgecut (may be NULL).
+ * Replaces hunyuangraph_PartitionGraph (hunyuangraph_partitiongraph.h:284). */
+int hp_partition(hp_context *ctx, int32_t nvtxs, const int32_t *xadj,
+                 const int32_t *adjncy, const int32_t *vwgt, const int32_t *adjwgt,
+                 int32_t nparts, const float *tpwgts, float ubfactor,
+                 const hp_options *opt, int32_t *part, int64_t *edgecut);
+
+/* Same, with every array already resident on the context's device (device
+ * pointers; vwgt/adjwgt may be NULL) and the work issued on `stream`
+ * (cudaStream_t, NULL = legacy default).  d_part is a device pointer. */
+int hp_partition_device(hp_context *ctx, int32_t nvtxs, int64_t nedges,
+                        const int32_t *d_xadj, const int32_t *d_adjncy,
+                        const int32_t *d_vwgt, const int32_t *d_adjwgt,
+                        int32_t nparts, const float *tpwgts, float ubfactor,
+                        const hp_options *opt, void *stream,
+                        int32_t *d_part, int64_t *edgecut);
+
+/* Statistics of the last hp_partition*() call on ctx. */
+int hp_last_stats(const hp_context *ctx, hp_stats *out);
+
+/* ---- level trace (opt.trace = 1), for parity checks of every level ----------- */
+#define HP_TRACE_XADJ         0   /* int32[n+1]  CSR of level l                      */
+#define HP_TRACE_ADJNCY       1   /* int32[m]                                        */
+#define HP_TRACE_ADJWGT       2   /* int32[m]                                        */
+#define HP_TRACE_VWGT         3   /* int32[n]                                        */
+#define HP_TRACE_MATCH        4   /* int32[n]  mate (self when unmatched), l < last  */
+#define HP_TRACE_CMAP         5   /* int32[n]  coarse id,                  l < last  */
+#define HP_TRACE_WHERE_START  6   /* int32[n]  partition entering refinement of l:
+                                     initial partition (coarsest) or projection      */
+#define HP_TRACE_WHERE_FINAL  7   /* int32[n]  partition after refinement of l        */
+
+int hp_trace_nlevels(const hp_context *ctx);
+int hp_trace_level(const hp_context *ctx, int level, int32_t *nvtxs, int64_t *nedges,
+                   int64_t *cut_start, int64_t *cut_final);
+int hp_trace_copy(const hp_context *ctx, int level, int what, int32_t *dst, int64_t count);
+
+/* ---- batched partition of many independent graphs ------------------------------
+ * Graph g has vertices [vtxdist[g], vtxdist[g+1]) and adjacency entries
+ * [edgedist[g], edgedist[g+1]) of the concatenated host arrays; xadj is the
+ * concatenation of the per-graph xadj arrays (each starting at 0, length n_g+1,
+ * so xadj has vtxdist[G] + G entries); adjncy ids are local to their graph.
+ * nparts[g], ubfactor[g] per graph; part is concatenated like vwgt. */
+int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *vtxdist,
+                       const int64_t *edgedist, const int32_t *xadj,
+                       const int32_t *adjncy, const int32_t *vwgt,
+                       const int32_t *adjwgt, const int32_t *nparts,
+                       const float *ubfactor, const hp_options *opt,
+                       int32_t *part, int64_t *edgecut);
+
+/* ---- device primitives (device pointers, issued on `stream`) ------------------- */
+/* Exclusive int32 prefix sum, single-pass decoupled look-back.  Writes n+1
+ * outputs (out[n] = total); in == out is allowed.  Replaces prefixsum()
+ * (hunyuangraph_GPU_prefixsum.h:141-188), which is inclusive and recursive. */
+int hp_scan_exclusive_i32(hp_context *ctx, const int32_t *d_in, int32_t *d_out,
+                          int64_t n, void *stream);
+
+/* Exact int64 edge cut of a device-resident partition.  Replaces
+ * compute_edgecut_gpu (hunyuangraph_graph.h:230-268). */
+int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xadj,
+                      const int32_t *d_adjncy, const int32_t *d_adjwgt,
+                      const int32_t *d_where, void *stream, int64_t *cut);
+
+/* ---- legacy drop-in ------------------------------------------------------------
+ * Identical signature to the reference (hunyuangraph_partitiongraph.h:284).
+ * Uses a process-wide context on device 0 and hp_options_default(); ubvec[0]
+ * is the imbalance factor.  On error every part[] entry is set to -1 and a
+ * message goes to stderr (the reference prints and calls exit()). */
+void hunyuangraph_PartitionGraph(int *nvtxs, int *xadj, int *adjncy, int *vwgt,
+                                 int *adjwgt, int *nparts, float *tpwgts,
+                                 float *ubvec, int *part);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HP_PARTITION_H */

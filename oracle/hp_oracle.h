@@ -1,0 +1,88 @@
+/*
+ * hp_oracle.h — CPU oracle of the multilevel k-way partition path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a sequential (optionally OpenMP) C
+ * restatement of the partition path that the CUDA library implements; it is
+ * the checker in tests/, __graft_entry__.smoke() and bench.py's CPU baseline,
+ * and nothing in the product links or calls it.
+ *
+ * Pins: the contraction and edge-cut semantics are checked against the
+ * reference's own CPU code (hunyuangraph_cpu_create_cgraph,
+ * hunyuangraph_computecut_cpu) built from /root/reference by
+ * oracle/build_ref.sh, and against committed fixtures in tests/golden/.
+ * The reference publishes no golden vectors for matching, bisection or
+ * refinement (it ships no tests); those rules are pinned only by this
+ * restatement (parity unpinned at the reference-test level).
+ */
+#ifndef HP_ORACLE_H
+#define HP_ORACLE_H
+
+#include <stdint.h>
+#include "hp_partition.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ora_trace ora_trace;
+
+void ora_set_threads(int nthreads);
+int  ora_get_threads(void);
+
+/* Full V-cycle; same contract as hp_partition(). trace may be NULL. */
+int ora_partition(int32_t n, const int32_t *xadj, const int32_t *adjncy,
+                  const int32_t *vwgt, const int32_t *adjwgt, int32_t nparts,
+                  const float *tpwgts, float ubfactor, const hp_options *opt,
+                  int32_t *part, int64_t *edgecut, ora_trace **trace);
+
+int  ora_trace_nlevels(const ora_trace *t);
+int  ora_trace_level(const ora_trace *t, int level, int32_t *n, int64_t *m,
+                     int64_t *cut_start, int64_t *cut_final);
+int  ora_trace_copy(const ora_trace *t, int level, int what, int32_t *dst, int64_t count);
+void ora_trace_free(ora_trace *t);
+
+/* ---- components (each follows the same rule as the CUDA path) ------------- */
+int64_t ora_edgecut(int32_t n, const int32_t *xadj, const int32_t *adjncy,
+                    const int32_t *adjwgt, const int32_t *where);
+
+/* One matching level: fills match[n] (self when unmatched) and cmap[n];
+ * returns the coarse vertex count. */
+int32_t ora_match(int32_t n, const int32_t *xadj, const int32_t *adjncy,
+                  const int32_t *vwgt, const int32_t *adjwgt, int32_t level,
+                  uint64_t seed, int64_t maxvwgt, int32_t rounds,
+                  int32_t *match, int32_t *cmap);
+
+/* Contraction of a matching: coarse CSR with rows sorted by neighbour id.
+ * Output arrays are malloc'ed (free with ora_free). Returns coarse m. */
+int64_t ora_contract(int32_t n, const int32_t *xadj, const int32_t *adjncy,
+                     const int32_t *vwgt, const int32_t *adjwgt,
+                     const int32_t *match, const int32_t *cmap, int32_t cn,
+                     int32_t **cxadj, int32_t **cadjncy, int32_t **cadjwgt,
+                     int32_t **cvwgt);
+void ora_free(void *p);
+
+/* Target / maximum part weights shared by initial partitioning and refinement. */
+void ora_part_targets(int64_t tvwgt, int32_t nparts, const float *tpwgts, float ubfactor,
+                      int64_t *opt, int64_t *maxp);
+int64_t ora_bisect_ub_fx(float ubfactor, int32_t nparts);
+
+/* Recursive-bisection initial partition of a (small) graph. */
+int ora_initpart(int32_t n, const int32_t *xadj, const int32_t *adjncy,
+                 const int32_t *vwgt, const int32_t *adjwgt, int32_t nparts,
+                 const int64_t *tw, int64_t ub2_fx, int32_t starts, int32_t fm_passes,
+                 int32_t *where);
+
+/* Refinement of one level in place; returns the final cut. */
+int64_t ora_refine(int32_t n, const int32_t *xadj, const int32_t *adjncy,
+                   const int32_t *vwgt, const int32_t *adjwgt, int32_t nparts,
+                   const int64_t *opt, const int64_t *maxp, int32_t finest,
+                   int32_t patience, int32_t *where, int32_t *passes);
+
+/* Weak-rebalance gain bucket (float semantics of the reference). */
+int32_t ora_gain_bucket(int32_t gain, int32_t vwgt);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,80 @@
+"""C ABI: the libraries load without a GPU and export every declared symbol;
+the Python mirror matches the header.  No compute call is made here."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+import hunyuansc25_b200 as hp
+from hunyuansc25_b200 import _abi, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions(header):
+    src = open(os.path.join(ROOT, "include", header)).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"//[^\n]*", "", src)
+    names = re.findall(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\(", src, flags=re.M)
+    return sorted(set(n for n in names if n not in ("defined",)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(hp.library_path()):
+        build.build_cuda()
+    return C.CDLL(hp.library_path())
+
+
+def test_partition_header_symbols_exported(lib):
+    names = declared_functions("hp_partition.h")
+    assert "hp_partition" in names and "hunyuangraph_PartitionGraph" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_gen_header_symbols_exported():
+    path = build.build_gen()
+    lib = C.CDLL(path)
+    names = declared_functions("hp_gen.h")
+    assert "hp_gen_rmat" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_prototypes_cover_header():
+    names = declared_functions("hp_partition.h")
+    assert sorted(_abi.PROTOTYPES) == names
+
+
+def test_load_library_binds_prototypes(lib):
+    L = hp.load_library()
+    assert L.hp_partition.restype == C.c_int
+
+
+def test_options_struct_layout():
+    # version(4) + 9 int32 + pad to 8 + seed(8)
+    assert C.sizeof(_abi.HpOptions) == 48
+    assert _abi.HpOptions.seed.offset == 40
+    assert C.sizeof(_abi.HpStats) == 8 * 3 + 4 * 2 + 8 + 4 * 2 + 4 * 6
+
+
+def test_options_default_matches_library(lib):
+    o = _abi.HpOptions()
+    lib.hp_options_default(C.byref(o))
+    d = _abi.default_options()
+    for name, _ in _abi.HpOptions._fields_:
+        assert getattr(o, name) == getattr(d, name), name
+
+
+def test_strerror(lib):
+    lib.hp_strerror.restype = C.c_char_p
+    assert lib.hp_strerror(0) == b"ok"
+    assert b"device memory" in lib.hp_strerror(_abi.HP_ERR_NOMEM)
+    assert lib.hp_strerror(-99) == b"unknown error"
+
+
+def test_legacy_symbol_signature_comment():
+    hdr = open(os.path.join(ROOT, "include", "hp_partition.h")).read()
+    assert "void hunyuangraph_PartitionGraph(int *nvtxs, int *xadj, int *adjncy, int *vwgt" in hdr

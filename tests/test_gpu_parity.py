@@ -1,0 +1,191 @@
+"""CUDA path vs the CPU oracle, through the C ABI: every level of the V-cycle
+(coarse CSR, vertex/edge weights, matching, cmap, initial and projected
+partitions, refined partitions, cuts) must be bit-identical."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import hunyuansc25_b200 as hp
+import oracle
+from hunyuansc25_b200 import graphs
+from hunyuansc25_b200._abi import (HP_ERR_INVALID_ARG, HP_ERR_INVALID_GRAPH, HP_ERR_UNSUPPORTED,
+                                   default_options)
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ["xadj", "adjncy", "adjwgt", "vwgt", "match", "cmap", "where_start", "where_final"]
+
+
+def compare_runs(ctx, g, k, ub=1.03, tpwgts=None, **optkw):
+    opt = default_options(trace=1, **optkw)
+    oracle.set_threads(8)
+    part_o, cut_o, tr = oracle.partition(g, k, ub, tpwgts=tpwgts, opt=opt, trace=True)
+    part_g, cut_g = ctx.partition_graph(g, k, ub, tpwgts=tpwgts, options=opt)
+    L = tr.nlevels
+    assert ctx.trace_nlevels == L, (ctx.trace_nlevels, L)
+    for l in range(L):
+        assert ctx.trace_level(l) == tr.level(l), f"level {l} sizes/cuts differ"
+        for what, name in enumerate(NAMES):
+            a = tr.array(l, what)
+            b = ctx.trace_array(l, what)
+            if a is None:
+                continue
+            assert b is not None, f"level {l} {name} missing on GPU"
+            if not np.array_equal(a, b):
+                bad = np.nonzero(a != b)[0]
+                raise AssertionError(f"level {l} {name}: {bad.size} entries differ, first at {bad[0]} "
+                                     f"(oracle {a[bad[0]]}, gpu {b[bad[0]]})")
+    assert np.array_equal(part_o, part_g)
+    assert cut_o == cut_g
+    assert cut_g == oracle.edgecut(g, part_g)
+    st = ctx.stats()
+    assert st.edgecut == cut_g
+    return part_g, cut_g, st
+
+
+def test_grid2d_256_k8(ctx):
+    g = graphs.config_grid2d()
+    part, cut, st = compare_runs(ctx, g, 8, coarsen_to=160)
+    assert st.max_excess <= 0
+
+
+def test_grid2d_reference_threshold(ctx):
+    compare_runs(ctx, graphs.config_grid2d(), 8)
+
+
+def test_grid3d_32_k64(ctx):
+    compare_runs(ctx, graphs.grid3d(32, 32, 32, seed=2, wmin=1, wmax=10), 64)
+
+
+def test_rmat_s14_k256(ctx):
+    compare_runs(ctx, graphs.rmat(14, 16, seed=3, wmin=1, wmax=100), 256)
+
+
+def test_rmat_s12_unit(ctx):
+    compare_runs(ctx, graphs.rmat(12, 16, seed=9, wmin=1, wmax=1), 32)
+
+
+def test_rgg_k1024(ctx):
+    compare_runs(ctx, graphs.rgg(1 << 16, 12.0, seed=4), 1024, ub=1.05)
+
+
+def test_odd_k_and_tpwgts(ctx):
+    g = graphs.grid2d(90, 70, seed=6, wmin=1, wmax=5)
+    compare_runs(ctx, g, 7)
+    tp = np.array([0.3, 0.2, 0.2, 0.1, 0.1, 0.05, 0.05], np.float32)
+    compare_runs(ctx, g, 7, tpwgts=tp)
+
+
+def test_seed_and_options(ctx):
+    g = graphs.grid3d(20, 20, 20, seed=2, wmin=1, wmax=10)
+    compare_runs(ctx, g, 16, seed=12345, match_rounds=3, refine_patience=2, init_starts=32, fm_passes=4)
+
+
+def test_hub_graph_xl_rows(ctx):
+    # a star plus a ring: one row far above the block-sort capacity
+    n = 20000
+    src = [0] * (n - 1) + list(range(1, n - 1))
+    dst = list(range(1, n)) + list(range(2, n))
+    e = np.array(src + dst, np.int64), np.array(dst + src, np.int64)
+    order = np.lexsort((e[1], e[0]))
+    s, d = e[0][order], e[1][order]
+    xadj = np.zeros(n + 1, np.int32)
+    np.add.at(xadj, s + 1, 1)
+    xadj = np.cumsum(xadj).astype(np.int32)
+    w = np.array([graphs.edge_weight(1, int(a), int(b), 1, 50) for a, b in zip(s, d)], np.int32)
+    g = graphs.Graph(xadj, d.astype(np.int32), np.ones(n, np.int32), w)
+    compare_runs(ctx, g, 8)
+
+
+def test_full_grid3d_128_k64(ctx):
+    """The 128^3 workload at full size: bit-identical to the oracle."""
+    g = graphs.config_grid3d()
+    part, cut, st = compare_runs(ctx, g, 64)
+    assert st.max_excess <= 0
+    assert part.min() >= 0 and part.max() < 64
+
+
+def test_deterministic_repeat(ctx):
+    g = graphs.rmat(13, 16, seed=3)
+    a = ctx.partition_graph(g, 64)
+    b = ctx.partition_graph(g, 64)
+    assert np.array_equal(a[0], b[0]) and a[1] == b[1]
+
+
+def test_edge_cases(ctx):
+    # empty graph
+    part, cut = ctx.partition(np.zeros(1, np.int32), np.zeros(0, np.int32), 4)
+    assert part.shape == (0,) and cut == 0
+    # single vertex, k > n, k = 1
+    g = graphs.grid2d(1, 1)
+    part, cut = ctx.partition_graph(g, 4)
+    assert cut == 0 and part.shape == (1,)
+    g = graphs.grid2d(6, 6)
+    part, cut = ctx.partition_graph(g, 1)
+    assert cut == 0 and np.all(part == 0)
+    compare_runs(ctx, g, 40)
+    # isolated vertices + two components
+    xadj = np.array([0, 1, 2, 2, 2, 4, 5, 6], np.int32)
+    adj = np.array([1, 0, 5, 6, 4, 4], np.int32)
+    gg = graphs.Graph(xadj, adj, np.ones(7, np.int32), np.ones(6, np.int32))
+    compare_runs(ctx, gg, 2)
+    compare_runs(ctx, gg, 3)
+
+
+def test_invalid_inputs(ctx):
+    bad = np.array([0, 1, 2], np.int32)
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition(bad, np.array([0, 0], np.int32), 2)         # self loop
+    assert e.value.code == HP_ERR_INVALID_GRAPH
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition(bad, np.array([5, 0], np.int32), 2)         # out of range
+    assert e.value.code == HP_ERR_INVALID_GRAPH
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition(bad, np.array([1, 0], np.int32), 2, adjwgt=np.array([0, 0], np.int32))
+    assert e.value.code == HP_ERR_INVALID_GRAPH
+    g = graphs.grid2d(4, 4)
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition_graph(g, 0)
+    assert e.value.code == HP_ERR_INVALID_ARG
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition_graph(g, 20000)
+    assert e.value.code == HP_ERR_UNSUPPORTED
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition_graph(g, 4, ubfactor=0.9)
+    assert e.value.code == HP_ERR_INVALID_ARG
+    # the context stays usable after errors
+    part, cut = ctx.partition_graph(g, 4)
+    assert cut == oracle.edgecut(g, part)
+
+
+def test_legacy_entry_point(ctx):
+    g = graphs.grid2d(40, 30, seed=3, wmin=1, wmax=9)
+    lib = hp.load_library()
+    I = C.POINTER(C.c_int32)
+    p = lambda a: a.ctypes.data_as(I)  # noqa: E731
+    n = C.c_int32(g.nvtxs)
+    k = C.c_int32(6)
+    ub = np.array([1.03], np.float32)
+    part = np.full(g.nvtxs, -7, np.int32)
+    lib.hunyuangraph_PartitionGraph(C.byref(n), p(g.xadj), p(g.adjncy), p(g.vwgt), p(g.adjwgt), C.byref(k),
+                                    None, ub.ctypes.data_as(C.POINTER(C.c_float)), p(part))
+    ref_part, _ = ctx.partition_graph(g, 6)
+    assert np.array_equal(part, ref_part)
+    # the Python mirror with the reference's argument list
+    out = np.zeros(g.nvtxs, np.int32)
+    hp.PartitionGraph(g.nvtxs, g.xadj, g.adjncy, g.vwgt, g.adjwgt, 6, None, [1.03], out)
+    assert np.array_equal(out, ref_part)
+
+
+def test_partition_device_torch(ctx):
+    import torch
+    g = graphs.grid3d(24, 24, 24, seed=2, wmin=1, wmax=10)
+    dev = torch.device("cuda", 0)
+    t = [torch.from_numpy(a).to(dev) for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt)]
+    part, cut = ctx.partition_device(t[0], t[1], 32, t[2], t[3])
+    torch.cuda.synchronize()
+    ref_part, ref_cut = ctx.partition_graph(g, 32)
+    assert cut == ref_cut
+    assert np.array_equal(part.cpu().numpy(), ref_part)
+    assert ctx.edgecut_device(t[0], t[1], t[3], part) == ref_cut
