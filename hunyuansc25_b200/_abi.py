@@ -49,6 +49,7 @@ class HpOptions(C.Structure):
         ("learned", C.c_int32),
         ("validate", C.c_int32),
         ("trace", C.c_int32),
+        ("profile", C.c_int32),
         ("seed", C.c_uint64),
     ]
 
@@ -66,6 +67,7 @@ def default_options(**overrides) -> HpOptions:
     o.learned = 0
     o.validate = 1
     o.trace = 0
+    o.profile = 0
     o.seed = 1
     for k, v in overrides.items():
         setattr(o, k, v)
@@ -88,10 +90,26 @@ class HpStats(C.Structure):
         ("ms_uncoarsen", C.c_float),
         ("ms_h2d", C.c_float),
         ("ms_d2h", C.c_float),
+        ("prof_ms", C.c_float * 8),
+        ("prof_bytes", C.c_int64 * 8),
+        ("prof_launches", C.c_int32 * 8),
     ]
 
     def as_dict(self):
-        return {name: getattr(self, name) for name, _ in self._fields_}
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if name.startswith("prof_") else v
+        return out
+
+
+HP_PROF_MATCH = 0
+HP_PROF_CONTRACT = 1
+HP_PROF_GAIN = 2
+HP_PROF_LP = 3
+HP_PROF_REBUILD = 4
+HP_PROF_INIT = 5
+PROF_NAMES = ["match", "contract", "gain_build", "lp", "rebuild", "init_trials", "", ""]
 
 
 I32P = C.POINTER(C.c_int32)

@@ -272,6 +272,7 @@ HP_API void hp_options_default(hp_options *o)
     o->learned = 0;
     o->validate = 1;
     o->trace = 0;
+    o->profile = 0;
     o->seed = 1;
 }
 

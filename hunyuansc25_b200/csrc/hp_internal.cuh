@@ -39,6 +39,12 @@ struct hp_context {
     cudaEvent_t ev[8] = {};
     int launches = 0;
 
+    // Kernel-class profiler (opt.profile): event pairs resolved at the end of a call.
+    struct ProfRec { int cls; int ev0, ev1; int64_t bytes; int launches; };
+    std::vector<cudaEvent_t> prof_events;
+    std::vector<ProfRec> prof_recs;
+    int prof_next = 0;
+
     hp_stats stats = {};
     std::vector<HpLevel> levels;
     bool trace_valid = false;
@@ -86,6 +92,12 @@ template <class T> inline T *ralloc_t(hp_context *c, int64_t n) { return (T *)hp
             }                                                                               \
         }                                                                                   \
     } while (0)
+
+// ---- kernel-class profiler ------------------------------------------------------
+// Usage: int t = hp_prof_begin(c); ...launches...; hp_prof_end(c, t, HP_PROF_X, bytes);
+int hp_prof_begin(hp_context *c);
+void hp_prof_end(hp_context *c, int token, int cls, int64_t bytes);
+void hp_prof_resolve(hp_context *c);
 
 // Blocking read of nbytes from device into the pinned mirror, then dst.
 int hp_read_scalars(hp_context *c, const void *d_src, size_t nbytes, void *dst);

@@ -15,6 +15,8 @@
 // vertex id) via a stable radix sort, the cut is int64, balance is judged
 // against integer maximum part weights, and one status read per pass replaces
 // the reference's 4-6 blocking reads.
+#include <cstdlib>
+
 #include "hp_internal.cuh"
 #include "hp_rowagg.cuh"
 
@@ -585,8 +587,10 @@ struct RefineBufs {
 };
 
 // scalar slots used by refinement
+// Slots below S_PASS_END are reset at the start of every pass; S_BIGCNT (the
+// level's list of rows longer than 32) lives above it and persists.
 enum { S_NMOVES = 0, S_C1 = 1, S_C2 = 2, S_EXCESS = 3, S_NCAND = 4, S_CUT2 = 5, S_DIRTY = 6,
-       S_BIGCNT = 7, S_LISTCNT = 8, S_NU = 9, S_NP = 10 };
+       S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_PASS_END = 12, S_BIGCNT = 16 };
 
 int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_t *small_list,
                const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt)
@@ -688,7 +692,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 16, c->stream));
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 1), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
     HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, d_bigcnt);
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
@@ -717,9 +721,11 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     const int patience = c->opt.refine_patience;
     const unsigned pg = (unsigned)(c->sm_count * 8);
     int count = 0, bal = 0, passes = 0;
+    const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     while (count++ <= patience) {
         passes++;
-        HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 16, c->stream));
+        HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * S_PASS_END, c->stream));
+        const int mode = excess <= 0 ? 0 : (bal < 2 ? 1 : 2);
         if (excess <= 0) {
             HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
                       finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND]);
@@ -753,6 +759,9 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         const int64_t c1 = st[S_C1], c2 = st[S_C2];
         excess = st[S_EXCESS];
         cut -= (c1 + c2) / 2;
+        if (dbg)
+            fprintf(stderr, "gpu pass n=%d pass=%d mode=%d moves=%lld cut=%lld excess=%lld\n", n, passes,
+                    mode, st[S_NMOVES], (long long)cut, (long long)excess);
 
         bool take = false;
         if (best_excess > 0 && excess < best_excess) {

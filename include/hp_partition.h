@@ -61,8 +61,18 @@ typedef struct hp_options {
     int32_t  learned;          /* 0 plain refinement, 1 MLP move proposals                    */
     int32_t  validate;         /* 0 none, 1 structural check on the device (default)          */
     int32_t  trace;            /* 1: keep every level for hp_trace_*() (tests)                */
+    int32_t  profile;          /* 1: time kernel classes with CUDA events into hp_stats.prof_* */
     uint64_t seed;             /* matching tie-break seed (default 1)                         */
 } hp_options;
+
+/* Kernel classes timed when hp_options.profile = 1 (hp_stats.prof_*[class]). */
+#define HP_PROF_MATCH     0   /* handshake rounds (proposal + commit)          */
+#define HP_PROF_CONTRACT  1   /* coarse-row aggregation + coarse CSR assembly  */
+#define HP_PROF_GAIN      2   /* full gain-table build of a level              */
+#define HP_PROF_LP        3   /* LP destination selection + afterburner        */
+#define HP_PROF_REBUILD   4   /* gain rows of moved vertices' neighbourhoods   */
+#define HP_PROF_INIT      5   /* bisection trials                              */
+#define HP_PROF_NCLASS    8
 
 /* Timing and quality of the last call on a context. */
 typedef struct hp_stats {
@@ -80,6 +90,9 @@ typedef struct hp_stats {
     float   ms_uncoarsen;
     float   ms_h2d;            /* host<->device copies inside hp_partition() (0 for _device) */
     float   ms_d2h;
+    float   prof_ms[8];        /* device time per kernel class (HP_PROF_*)                    */
+    int64_t prof_bytes[8];     /* algorithmic HBM bytes per kernel class                      */
+    int32_t prof_launches[8];  /* kernel launches per class                                   */
 } hp_stats;
 
 typedef struct hp_context hp_context;

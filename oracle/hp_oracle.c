@@ -29,6 +29,7 @@
 #include "hp_oracle.h"
 
 #include <limits.h>
+#include <stdio.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -986,19 +987,24 @@ int64_t ora_refine(int32_t n, const int32_t *xadj, const int32_t *adjncy,
     memcpy(best, where, sizeof(int32_t) * (size_t)n);
     int64_t best_cut = cut, best_excess = excess;
     int32_t count = 0, bal_counter = 0, passes = 0;
+    const int dbg = getenv("HP_DEBUG_PASSES") != NULL;
 
     while (count++ <= patience) {
         passes++;
         int32_t nm;
+        int mode;
         if (excess <= 0) {
             nm = lp_moves(&s, finest);
             bal_counter = 0;
+            mode = 0;
         } else if (bal_counter < 2) {
             nm = rw_moves(&s);
             bal_counter++;
+            mode = 1;
         } else {
             nm = rs_moves(&s);
             bal_counter++;
+            mode = 2;
         }
         for (int32_t i = 0; i < nm; i++) {
             int32_t v = s.moves[i];
@@ -1013,6 +1019,9 @@ int64_t ora_refine(int32_t n, const int32_t *xadj, const int32_t *adjncy,
         excess = INT64_MIN;
         for (int32_t p = 0; p < nparts; p++)
             if (s.pw[p] - maxp[p] > excess) excess = s.pw[p] - maxp[p];
+        if (dbg)
+            fprintf(stderr, "ora pass n=%d pass=%d mode=%d moves=%d cut=%lld excess=%lld\n", n, passes,
+                    mode, nm, (long long)cut, (long long)excess);
 
         if (best_excess > 0 && excess < best_excess) {
             best_excess = excess; best_cut = cut;
@@ -1109,6 +1118,7 @@ static void ora_options_default(hp_options *o)
     o->learned = 0;
     o->validate = 1;
     o->trace = 0;
+    o->profile = 0;
     o->seed = 1;
 }
 

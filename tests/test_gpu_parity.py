@@ -24,8 +24,7 @@ def compare_runs(ctx, g, k, ub=1.03, tpwgts=None, **optkw):
     part_g, cut_g = ctx.partition_graph(g, k, ub, tpwgts=tpwgts, options=opt)
     L = tr.nlevels
     assert ctx.trace_nlevels == L, (ctx.trace_nlevels, L)
-    for l in range(L):
-        assert ctx.trace_level(l) == tr.level(l), f"level {l} sizes/cuts differ"
+    for l in reversed(range(L)):       # coarsest first: the first mismatch is the cause
         for what, name in enumerate(NAMES):
             a = tr.array(l, what)
             b = ctx.trace_array(l, what)
@@ -36,6 +35,7 @@ def compare_runs(ctx, g, k, ub=1.03, tpwgts=None, **optkw):
                 bad = np.nonzero(a != b)[0]
                 raise AssertionError(f"level {l} {name}: {bad.size} entries differ, first at {bad[0]} "
                                      f"(oracle {a[bad[0]]}, gpu {b[bad[0]]})")
+        assert ctx.trace_level(l) == tr.level(l), f"level {l} sizes/cuts differ"
     assert np.array_equal(part_o, part_g)
     assert cut_o == cut_g
     assert cut_g == oracle.edgecut(g, part_g)
