@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Partition throughput of the B200 multilevel k-way partitioner: one JSON line.
+
+A step is one full multilevel k-way partition (coarsening -> initial bisection
+-> uncoarsening with refinement) of the workload graph, whose CSR is already
+resident in HBM.  value = undirected edges partitioned per second (whole job:
+N GPUs each run an independent replica, the graph does not shard).  L2 is
+flushed (256 MiB write) before every timed step; each step is timed with CUDA
+events on the stream the library launches on; the job time is the max over
+ranks.  e2e repeats the metric through the host-buffer C-ABI entry point
+(hp_partition) with pinned inputs, the H2D copies and the D2H of the partition
+inside the timed call.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload grid3d|grid2d|rmat22|rgg24]
+  python bench.py --impl reference ...   # the CPU path on the host cores
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from hunyuansc25_b200 import graphs  # noqa: E402
+from hunyuansc25_b200._abi import PROF_NAMES, default_options  # noqa: E402
+
+WORKLOADS = {
+    "grid3d": dict(desc="grid3d 128^3 7-point, edge weights U{1..10} (seed 2), unit vertex weights, "
+                        "k=64, imbalance 1.03", k=64, ub=1.03, coarsen_to=0,
+                   make=lambda: graphs.config_grid3d()),
+    "grid2d": dict(desc="grid2d 256x256 5-point, unit weights, k=8, imbalance 1.03, coarsen to k*20",
+                   k=8, ub=1.03, coarsen_to=160, make=lambda: graphs.config_grid2d()),
+    "rmat22": dict(desc="R-MAT scale 22 edge factor 16 (a,b,c=.57,.19,.19, seed 3), weights U{1..100}, "
+                        "k=256, imbalance 1.03", k=256, ub=1.03, coarsen_to=0,
+                   make=lambda: graphs.config_rmat(22)),
+    "rgg24": dict(desc="RGG 2^24 points (seed 4), mean degree 12, w=int(1000(1-d/r))+1, k=1024, "
+                       "imbalance 1.05", k=1024, ub=1.05, coarsen_to=0,
+                  make=lambda: graphs.config_rgg(1 << 24)),
+}
+METRIC = "partition ms & edges/s at equal edge cut (±1%), learned vs plain, 1 B200"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic(workload, cls_name):
+    """DRAM bytes per algorithmic byte of the dominant kernel class from the
+    committed ncu summary (profiles/traffic.json), if present."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    e = t.get(workload, {}).get(cls_name)
+    return e
+
+
+class ClockSampler:
+    """nvidia-smi SM clock / throttle-reason samples during the timed region."""
+
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 10:
+                    continue
+                try:
+                    sm.append(float(parts[2]))
+                    mx.append(float(parts[3]))
+                except ValueError:
+                    continue
+                for nm, val in zip(names, parts[6:10]):
+                    if val.lower() == "active":
+                        reasons.add(nm)
+        os.unlink(self.path)
+        if sm:
+            out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                   "samples": len(sm)}
+        return out
+
+
+def cpu_port_run(g, spec, threads):
+    import oracle
+    oracle.set_threads(threads)
+    opt = default_options(coarsen_to=spec["coarsen_to"])
+    t0 = time.perf_counter()
+    part, cut, _ = oracle.partition(g, spec["k"], spec["ub"], opt=opt)
+    dt = time.perf_counter() - t0
+    return dt, cut
+
+
+def run_reference(args, spec, g, m_und):
+    """The reference arm: the CPU implementation of the path (the oracle port
+    of the reference's CPU algorithm) on all host threads of rank 0."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_port_run(g, spec, threads)
+    times = []
+    cut = None
+    for _ in range(args.steps):
+        dt, cut = cpu_port_run(g, spec, threads)
+        times.append(dt)
+    total = sum(times)
+    value = args.steps * m_und / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic", "config": config_of(args, spec, g, m_und),
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full partitions of the workload graph"},
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "quality": {"edgecut": int(cut)},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, spec, g, m_und):
+    return {"workload": spec["desc"], "name": args.workload, "nvtxs": g.nvtxs, "nedges_undirected": m_und,
+            "nparts": spec["k"], "ubfactor": spec["ub"],
+            "coarsen_to": spec["coarsen_to"] or "reference rule (8k, or max(1024,2k) when 8k > 1024)",
+            "parallelism": f"replicas x{args.gpus} (a single graph does not shard)",
+            "l2": "flushed before every timed step (256 MiB write)"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="grid3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="skip the e2e and CPU-baseline legs (profiling runs)")
+    args = ap.parse_args()
+    spec = WORKLOADS[args.workload]
+    graphs.set_threads(os.cpu_count() or 1)
+    g = spec["make"]()
+    m_und = g.nedges // 2
+
+    if args.impl == "reference":
+        run_reference(args, spec, g, m_und)
+        return
+
+    import torch
+    import torch.distributed as dist
+    import hunyuansc25_b200 as hp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", device_id=dev, timeout=timedelta(seconds=300))
+
+    ctx = hp.Context(local)
+    opt = default_options(coarsen_to=spec["coarsen_to"], profile=1)
+    xadj, adj, vw, ew = (torch.from_numpy(a).to(dev) for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt))
+    part = torch.empty(g.nvtxs, dtype=torch.int32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        return ctx.partition_device(xadj, adj, spec["k"], vw, ew, spec["ub"], options=opt, stream=stream,
+                                    part=part)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = []
+    stats = []
+    cut = None
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        _, cut = step()
+        e1.record(stream)
+        evs.append((e0, e1))
+        stats.append(ctx.stats())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    job_ms = float(t.item())
+    value = world * args.steps * m_und / (job_ms / 1000.0)
+
+    # kernel-class roofline from the library's CUDA-event profile of the timed steps
+    prof_ms = np.zeros(8)
+    prof_bytes = np.zeros(8)
+    prof_launch = np.zeros(8)
+    launches = 0
+    for s in stats:
+        prof_ms += np.array(list(s.prof_ms))
+        prof_bytes += np.array(list(s.prof_bytes), dtype=np.float64)
+        prof_launch += np.array(list(s.prof_launches))
+        launches += s.kernel_launches
+    with_bytes = [i for i in range(8) if prof_bytes[i] > 0]
+    dom = max(with_bytes, key=lambda i: prof_ms[i]) if with_bytes else 0
+    peak, peak_kind = load_peaks()
+    achieved = prof_bytes[dom] / (prof_ms[dom] / 1000.0) / 1e9 if prof_ms[dom] > 0 else 0.0
+    traffic_ratio = load_traffic(args.workload, PROF_NAMES[dom])
+    per_launch_alg = prof_bytes[dom] / max(prof_launch[dom], 1)
+    roofline = {
+        "bound": "hbm", "kernel": PROF_NAMES[dom], "achieved": round(achieved, 1), "peak": peak,
+        "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+        "traffic": (round(traffic_ratio * per_launch_alg) if traffic_ratio else None),
+        "algorithmic_bytes_per_launch": int(per_launch_alg),
+        "classes": {PROF_NAMES[i]: {"ms_per_step": round(prof_ms[i] / args.steps, 3),
+                                    "GB/s": (round(prof_bytes[i] / (prof_ms[i] / 1e3) / 1e9, 1)
+                                             if prof_bytes[i] > 0 and prof_ms[i] > 0 else None)}
+                    for i in range(8) if PROF_NAMES[i] and prof_ms[i] > 0},
+    }
+    last = stats[-1]
+
+    # end-to-end through the host-buffer entry point with pinned inputs
+    pin = [torch.from_numpy(a).pin_memory() for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt)]
+    hn = [p.numpy() for p in pin]
+    e2e_opt = default_options(coarsen_to=spec["coarsen_to"])
+    e2e_t = []
+    for i in range(0 if args.kernel_only else args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        hpart, hcut = ctx.partition(hn[0], hn[1], spec["k"], hn[2], hn[3], spec["ub"], options=e2e_opt)
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_t.append(dt)
+    e2e_tot = torch.tensor([sum(e2e_t)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+    e2e_value = world * len(e2e_t) * m_und / float(e2e_tot.item()) if e2e_t else None
+    h2d = (g.nvtxs + 1 + g.nedges + g.nvtxs + g.nedges) * 4
+    d2h = g.nvtxs * 4 + 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.kernel_only:
+        threads = os.cpu_count() or 1
+        dt, ocut = cpu_port_run(g, spec, threads)
+        cpu = {"value": m_und / dt, "unit": "edges/s", "cores": threads, "kind": "port",
+               "sample": "one full partition of the workload graph by the CPU port (all host threads)",
+               "edgecut": int(ocut), "parity_cut_equal": int(ocut) == int(cut)}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": job_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+            "config": config_of(args, spec, g, m_und),
+            "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": 1000 * sum(e2e_t) / len(e2e_t) if e2e_t else None},
+            "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "quality": {"edgecut": int(cut), "max_excess": int(last.max_excess), "balanced": last.max_excess <= 0,
+                        "levels": last.nlevels, "coarsest_nvtxs": last.coarsest_nvtxs,
+                        "phase_ms": {"coarsen": round(last.ms_coarsen, 3), "init": round(last.ms_init, 3),
+                                     "uncoarsen": round(last.ms_uncoarsen, 3)}},
+            "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

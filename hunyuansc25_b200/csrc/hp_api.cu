@@ -194,6 +194,8 @@ int begin_call(hp_context *c, const hp_options *opt, void *stream)
     HP_CUDA(cudaSetDevice(c->device));
     c->stream = stream ? (cudaStream_t)stream : c->own_stream;
     c->launches = 0;
+    c->prof_recs.clear();
+    c->prof_next = 0;
     memset(&c->stats, 0, sizeof(c->stats));
     unsigned zero = 0;
     HP_CUDA(cudaMemcpyAsync(c->d_status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
@@ -210,10 +212,64 @@ void finish_stats(hp_context *c)
     if (cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]) == cudaSuccess) st.ms_init = ms;
     if (cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]) == cudaSuccess) st.ms_uncoarsen = ms;
     st.kernel_launches = c->launches;
+    hp_prof_resolve(c);
     c->trace_valid = c->opt.trace != 0;
 }
 
 }  // namespace
+
+// ---- kernel-class profiler ----------------------------------------------------------
+static int prof_event(hp_context *c)
+{
+    if (c->prof_next >= (int)c->prof_events.size()) {
+        for (int i = 0; i < 256; i++) {
+            cudaEvent_t e;
+            if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return -1; }
+            c->prof_events.push_back(e);
+        }
+    }
+    return c->prof_next++;
+}
+
+int hp_prof_begin(hp_context *c)
+{
+    if (!c->opt.profile) return -1;
+    int e0 = prof_event(c);
+    if (e0 < 0) return -1;
+    cudaEventRecord(c->prof_events[e0], c->stream);
+    c->prof_recs.push_back({-1, e0, -1, 0, c->launches});
+    return (int)c->prof_recs.size() - 1;
+}
+
+void hp_prof_end(hp_context *c, int token, int cls, int64_t bytes)
+{
+    if (token < 0 || token >= (int)c->prof_recs.size()) return;
+    int e1 = prof_event(c);
+    if (e1 < 0) return;
+    cudaEventRecord(c->prof_events[e1], c->stream);
+    auto &r = c->prof_recs[token];
+    r.cls = cls;
+    r.ev1 = e1;
+    r.bytes = bytes;
+    r.launches = c->launches - r.launches;
+}
+
+void hp_prof_resolve(hp_context *c)
+{
+    for (const auto &r : c->prof_recs) {
+        if (r.cls < 0 || r.cls >= 8 || r.ev1 < 0) continue;
+        float ms = 0;
+        if (cudaEventElapsedTime(&ms, c->prof_events[r.ev0], c->prof_events[r.ev1]) != cudaSuccess) {
+            cudaGetLastError();
+            continue;
+        }
+        c->stats.prof_ms[r.cls] += ms;
+        c->stats.prof_bytes[r.cls] += r.bytes;
+        c->stats.prof_launches[r.cls] += r.launches;
+    }
+    c->prof_recs.clear();
+    c->prof_next = 0;
+}
 
 // ---- shared helpers -------------------------------------------------------------
 int hp_read_scalars(hp_context *c, const void *d_src, size_t nbytes, void *dst)
@@ -335,6 +391,7 @@ HP_API void hp_context_destroy(hp_context *c)
     if (c->h_pin) cudaFreeHost(c->h_pin);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (auto e : c->prof_events) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }

@@ -398,13 +398,18 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     HP_LAUNCH(c, big_list_kernel, blocks_for(n), 256, 0, n, g.xadj, big, d_bigcnt);
 
     const int rounds = o.match_rounds < 1 ? 1 : (o.match_rounds > 30 ? 30 : o.match_rounds);
+    // algorithmic bytes of one full handshake round: xadj, adjncy, adjwgt,
+    // vwgt, match read and write (neighbour gathers not counted)
+    const int64_t round_bytes = 4 * ((int64_t)n + 1) + 8 * g.m + 12 * (int64_t)n;
     for (int r = 0; r < rounds; r++) {
+        const int tok = hp_prof_begin(c);
         const unsigned long long *prev = r == 0 ? nullptr : &sc[2 + r - 1];
         HP_LAUNCH(c, pref_small_kernel<true>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
                   g.vwgt, g.match, pref, lkey, maxvwgt, prev);
         HP_LAUNCH(c, pref_big_kernel<true>, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, pref, lkey, maxvwgt, prev);
         HP_LAUNCH(c, commit_kernel, blocks_for(n), 256, 0, n, g.match, pref, &sc[2 + r], prev);
+        hp_prof_end(c, tok, r == 0 ? HP_PROF_MATCH : 6, r == 0 ? round_bytes : 0);
     }
 
     auto matched = [&](int slot, int64_t *out) -> int {
@@ -467,9 +472,11 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     int32_t *counts = (int32_t *)sc;          // 3 class counts (+ maxlen) packed in 2 slots
     int32_t *maxlen = counts + 3;
 
+    int tok = hp_prof_begin(c);
     HP_LAUNCH(c, coarse_setup_kernel, blocks_for(n), 256, 0, n, g.match, g.cmap, g.xadj, g.vwgt,
               leader_of, cg.vwgt, toff, lists, counts, cn, maxlen);
     HP_TRY(hp_scan_excl(c, toff, toff, cn));
+    hp_prof_end(c, tok, HP_PROF_CONTRACT, 0);
     struct { int32_t cnt[3]; int32_t maxlen; } h;
     HP_TRY(hp_read_scalars(c, counts, sizeof(h), &h));
     int32_t tm = 0;
@@ -479,6 +486,7 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     int32_t *tw = ralloc_t<int32_t>(c, tm);
     HP_CHECK_OOM(c);
     ContractSrc src{g.xadj, g.adjncy, g.adjwgt, g.cmap, g.match, leader_of};
+    tok = hp_prof_begin(c);
     HP_LAUNCH(c, contract_warp_kernel, blocks_for((int64_t)cn * 32), 256, 0, cn, src, toff, tk, tw,
               ucnt);
     if (h.cnt[0] > 0)
@@ -501,6 +509,7 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
                   &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm);
     }
     HP_TRY(hp_scan_excl(c, ucnt, cg.xadj, cn));
+    hp_prof_end(c, tok, HP_PROF_CONTRACT, 0);
     int32_t mc = 0;
     HP_TRY(hp_read_scalars(c, cg.xadj + cn, sizeof(int32_t), &mc));
     cg.m = mc;
@@ -508,8 +517,14 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     cg.adjncy = lalloc_t<int32_t>(c, mc);
     cg.adjwgt = lalloc_t<int32_t>(c, mc);
     HP_CHECK_OOM(c);
+    tok = hp_prof_begin(c);
     HP_LAUNCH(c, copy_rows_kernel, blocks_for((int64_t)cn * 32), 256, 0, cn, toff, cg.xadj, tk, tw,
               cg.adjncy, cg.adjwgt);
+    // algorithmic bytes of the whole contraction: fine CSR, cmap, match,
+    // vwgt in; coarse xadj, adjacency, weights, vertex weights out
+    hp_prof_end(c, tok, HP_PROF_CONTRACT,
+                4 * ((int64_t)n + 1) + 8 * g.m + 12 * (int64_t)n + 4 * ((int64_t)cn + 1) + 8 * (int64_t)mc +
+                    4 * (int64_t)cn);
     c->hi = mark;
     return HP_OK;
 }

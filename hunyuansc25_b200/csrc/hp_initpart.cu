@@ -485,8 +485,10 @@ int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_
         HP_CHECK_OOM(c);
         HP_CUDA(cudaMemcpyAsync(d_info, info.data(), sizeof(SubInfo) * ns, cudaMemcpyHostToDevice, c->stream));
         HP_CUDA(cudaMemcpyAsync(d_tsub, trial_sub.data(), sizeof(int32_t) * tcount, cudaMemcpyHostToDevice, c->stream));
+        const int tok = hp_prof_begin(c);
         HP_LAUNCH(c, trial_kernel, nblk(tcount, 128), 128, 0, d_info, d_tsub, tcount, fxadj, fadj, fwgt,
                   fvwgt, slab, starts, fm_passes, d_cut, d_viol);
+        hp_prof_end(c, tok, HP_PROF_INIT, 0);
         HP_LAUNCH(c, select_kernel, (unsigned)ns, 256, 0, d_info, d_cut, d_viol, slab, fvwgt, side, d_res);
         std::vector<int64_t> res(2 * ns);
         HP_CUDA(cudaMemcpyAsync(res.data(), d_res, sizeof(int64_t) * 2 * ns, cudaMemcpyDeviceToHost, c->stream));

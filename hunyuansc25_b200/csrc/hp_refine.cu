@@ -701,7 +701,10 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.gpart = ralloc_t<int32_t>(c, G);
     B.gconn = ralloc_t<int32_t>(c, G);
     HP_CHECK_OOM(c);
+    int tok = hp_prof_begin(c);
     HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt));
+    // xadj, adjncy, adjwgt, where (own), goff, gain rows out
+    hp_prof_end(c, tok, HP_PROF_GAIN, 4 * ((int64_t)n + 1) + 8 * g.m + 4 * (int64_t)n + 4 * ((int64_t)n + 1) + 8 * (int64_t)G);
     HP_CUDA(cudaMemsetAsync(B.pw, 0, sizeof(unsigned long long) * (size_t)k, c->stream));
     HP_CUDA(cudaMemsetAsync(B.lock, 0, (size_t)n, c->stream));
     HP_CUDA(cudaMemsetAsync(B.dirty, 0, sizeof(int32_t) * (size_t)n, c->stream));
@@ -727,12 +730,17 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * S_PASS_END, c->stream));
         const int mode = excess <= 0 ? 0 : (bal < 2 ? 1 : 2);
         if (excess <= 0) {
+            const int ltok = hp_prof_begin(c);
             HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
                       finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND]);
             HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where,
                       B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
             HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
                       g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
+            // select: goff, rows, where, lock in; dest, pregain out.  afterburner:
+            // xadj, adjncy, adjwgt, own pregain/dest/where in, lock out
+            hp_prof_end(c, ltok, HP_PROF_LP,
+                        8 * ((int64_t)n + 1) + 8 * (int64_t)G + 8 * g.m + 26 * (int64_t)n);
             bal = 0;
         } else if (bal < 2) {
             HP_TRY(weak_rebalance(c, g, B, k));
@@ -748,10 +756,12 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw,
                   g.xadj, g.adjncy, B.dirty);
         HP_LAUNCH(c, commit_moves_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest);
+        const int rtok = hp_prof_begin(c);
         HP_LAUNCH(c, classify_dirty_kernel, nblk(n), 256, 0, n, B.dirty, g.xadj, B.small_l, B.big_l,
                   (int32_t *)&sc[S_DIRTY]);
         HP_TRY(build_rows(c, g, B, k, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
                           ((const int32_t *)&sc[S_DIRTY]) + 1));
+        hp_prof_end(c, rtok, HP_PROF_REBUILD, 0);
         HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where,
                   B.dest, B.oldp, 0, &sc[S_C2]);
         HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);

@@ -54,9 +54,9 @@ def test_load_library_binds_prototypes(lib):
 
 
 def test_options_struct_layout():
-    # version + 10 int32 fields, then the 8-byte seed
-    assert C.sizeof(_abi.HpOptions) == 48
-    assert _abi.HpOptions.seed.offset == 40
+    # version + 10 int32 fields (44 bytes), padding, then the 8-byte seed
+    assert C.sizeof(_abi.HpOptions) == 56
+    assert _abi.HpOptions.seed.offset == 48
     assert C.sizeof(_abi.HpStats) == 8 * 3 + 4 * 2 + 8 + 4 * 2 + 4 * 6 + 4 * 8 + 8 * 8 + 4 * 8
 
 
