@@ -47,6 +47,9 @@ WORKLOADS = {
                        "imbalance 1.05", k=1024, ub=1.05, coarsen_to=0,
                   make=lambda: graphs.config_rgg(1 << 24)),
 }
+WORKLOADS["batch"] = dict(desc="1,024 graphs, n log-uniform in [1e3, 2e5] (seed 5), half 2-D grids, half R-MAT "
+                               "(edge factor 8), weights U{1..100}, k from {2,4,8,16,32,64}, imbalance 1.03",
+                          k=0, ub=1.03, coarsen_to=0, make=None)
 METRIC = "partition ms & edges/s at equal edge cut (±1%), learned vs plain, 1 B200"
 L2_FLUSH_BYTES = 256 << 20
 
@@ -172,6 +175,50 @@ def config_of(args, spec, g, m_und):
             "l2": "flushed before every timed step (256 MiB write)"}
 
 
+def run_batch(args, spec):
+    """The batched workload: one hp_partition_batch call (worker contexts on
+    separate streams) against one hp_partition call per graph, same inputs."""
+    import torch
+    import hunyuansc25_b200 as hp
+    specs = graphs.batch_specs(1024, seed=5)
+    gs = [graphs.batch_graph(kind, n, seed=1000 + i) for i, (kind, n, k) in enumerate(specs)]
+    ks = [k for _, _, k in specs]
+    m_und = sum(g.nedges for g in gs) // 2
+    ctx = hp.Context(0)
+    for _ in range(max(1, args.warmup)):
+        ctx.partition_batch(gs, ks, spec["ub"])
+    t_batch = []
+    launches = 0
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        parts, cuts = ctx.partition_batch(gs, ks, spec["ub"])
+        t_batch.append(time.perf_counter() - t0)
+        launches += ctx.stats().kernel_launches
+    # per-graph launches: one hp_partition call after another
+    t0 = time.perf_counter()
+    seq_cuts = [ctx.partition_graph(g, k, spec["ub"])[1] for g, k in zip(gs, ks)]
+    t_seq = time.perf_counter() - t0
+    same = [int(a) for a in cuts] == [int(b) for b in seq_cuts]
+    tb = sum(t_batch) / len(t_batch)
+    line = {
+        "metric": METRIC, "value": m_und / tb, "unit": "edges/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * tb, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": spec["desc"], "name": "batch", "graphs": len(gs),
+                   "nvtxs_total": int(sum(g.nvtxs for g in gs)), "nedges_undirected": m_und,
+                   "parallelism": "one GPU, 16 worker streams", "l2": "inputs (host) re-copied every step"},
+        "e2e": {"value": m_und / tb, "unit": "edges/s",
+                "h2d_bytes_per_step": int(sum((2 * g.nvtxs + 1 + 2 * g.nedges) * 4 for g in gs)),
+                "d2h_bytes_per_step": int(sum(g.nvtxs * 4 + 8 for g in gs))},
+        "gpu_launches": int(launches),
+        "batch_vs_per_graph": {"per_graph_ms": 1000 * t_seq, "batch_ms": 1000 * tb, "speedup": t_seq / tb,
+                               "identical_cuts": same},
+    }
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -186,6 +233,9 @@ def main():
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
     graphs.set_threads(os.cpu_count() or 1)
+    if args.workload == "batch":
+        run_batch(args, spec)
+        return
     g = spec["make"]()
     m_und = g.nedges // 2
 

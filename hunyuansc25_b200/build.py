@@ -62,11 +62,11 @@ def _cc():
 def build_gen(force=False):
     os.makedirs(LIB, exist_ok=True)
     out = os.path.join(LIB, "libhp_gen.so")
-    src = os.path.join(CSRC, "hp_gen.c")
-    if not force and _newer(out, [src, os.path.join(INCLUDE, "hp_gen.h")]):
+    srcs = [os.path.join(CSRC, "hp_gen.c"), os.path.join(CSRC, "hp_io.c")]
+    if not force and _newer(out, srcs + [os.path.join(INCLUDE, "hp_gen.h"), os.path.join(INCLUDE, "hp_io.h")]):
         return out
     _run([_cc(), "-O2", "-fPIC", "-fopenmp", "-std=c11", "-Wall", "-I", INCLUDE, "-shared",
-          "-o", out, src, "-lm"])
+          "-o", out, *srcs, "-lm"])
     return out
 
 

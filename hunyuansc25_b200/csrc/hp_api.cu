@@ -8,9 +8,14 @@
 // unit weights and exits on error; here a context keeps one arena sized from
 // (n, m) and grown on demand, the caller's weights are used, and every failure
 // is an error code.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <numeric>
+#include <thread>
 
 #include "hp_internal.cuh"
 
@@ -372,6 +377,7 @@ HP_API int hp_context_create(int device, hp_context **out)
     ok = ok && cudaMallocHost((void **)&c->h_pin, sizeof(long long) * HP_NSCAL) == cudaSuccess;
     for (int i = 0; ok && i < 8; i++) ok = cudaEventCreate(&c->ev[i]) == cudaSuccess;
     ok = ok && hp_refine_init() == HP_OK;
+    ok = ok && hp_initpart_init() == HP_OK;
     if (!ok) {
         cudaGetLastError();
         hp_context_destroy(c);
@@ -384,6 +390,8 @@ HP_API int hp_context_create(int device, hp_context **out)
 HP_API void hp_context_destroy(hp_context *c)
 {
     if (!c) return;
+    for (hp_context *w : c->workers) hp_context_destroy(w);
+    c->workers.clear();
     cudaSetDevice(c->device);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->arena) cudaFree(c->arena);
@@ -560,18 +568,63 @@ HP_API int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *v
                               const float *ubfactor, const hp_options *opt, int32_t *part,
                               int64_t *edgecut)
 {
+    // Independent graphs are partitioned by a pool of worker contexts, each
+    // with its own stream and arena; a worker's host-side scalar reads overlap
+    // with the other workers' kernels.  Graphs are taken largest first.  Each
+    // graph's result depends only on that graph, so the batch returns exactly
+    // what one hp_partition() call per graph returns.
     if (!ctx || ngraphs < 0 || !vtxdist || !edgedist || !xadj || !nparts || !ubfactor || !part)
         return HP_ERR_INVALID_ARG;
+    if (ngraphs == 0) return HP_OK;
     for (int32_t gi = 0; gi < ngraphs; gi++) {
-        const int64_t v0 = vtxdist[gi], n = vtxdist[gi + 1] - v0, e0 = edgedist[gi];
-        int64_t cut = 0;
-        int rc = hp_partition(ctx, (int32_t)n, xadj + v0 + gi, adjncy + e0, vwgt ? vwgt + v0 : nullptr,
-                              adjwgt ? adjwgt + e0 : nullptr, nparts[gi], nullptr, ubfactor[gi], opt,
-                              part + v0, &cut);
-        if (rc != HP_OK) return rc;
-        if (edgecut) edgecut[gi] = cut;
+        if (vtxdist[gi + 1] < vtxdist[gi] || edgedist[gi + 1] < edgedist[gi]) return HP_ERR_INVALID_ARG;
+        if (vtxdist[gi + 1] - vtxdist[gi] > INT32_MAX - 1) return HP_ERR_UNSUPPORTED;
     }
-    return HP_OK;
+    const int nworkers = (int)std::min<int64_t>(ngraphs, 16);
+    HP_CUDA(cudaSetDevice(ctx->device));
+    while ((int)ctx->workers.size() < nworkers) {
+        hp_context *w = nullptr;
+        HP_TRY(hp_context_create(ctx->device, &w));
+        ctx->workers.push_back(w);
+    }
+    std::vector<int32_t> order(ngraphs);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+        return edgedist[a + 1] - edgedist[a] > edgedist[b + 1] - edgedist[b];
+    });
+    std::atomic<int32_t> next{0};
+    std::atomic<int> first_err{HP_OK};
+    std::atomic<long long> launches{0};
+    auto t0 = std::chrono::steady_clock::now();
+    auto work = [&](hp_context *w) {
+        cudaSetDevice(w->device);
+        for (;;) {
+            if (first_err.load() != HP_OK) return;
+            int32_t i = next.fetch_add(1);
+            if (i >= ngraphs) return;
+            const int32_t gi = order[i];
+            const int64_t v0 = vtxdist[gi], n = vtxdist[gi + 1] - v0, e0 = edgedist[gi];
+            int64_t cut = 0;
+            int rc = hp_partition(w, (int32_t)n, xadj + v0 + gi, adjncy + e0, vwgt ? vwgt + v0 : nullptr,
+                                  adjwgt ? adjwgt + e0 : nullptr, nparts[gi], nullptr, ubfactor[gi], opt,
+                                  part + v0, &cut);
+            if (rc != HP_OK) {
+                int expected = HP_OK;
+                first_err.compare_exchange_strong(expected, rc);
+                return;
+            }
+            launches += w->stats.kernel_launches;
+            if (edgecut) edgecut[gi] = cut;
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nworkers; t++) pool.emplace_back(work, ctx->workers[t]);
+    for (auto &t : pool) t.join();
+    memset(&ctx->stats, 0, sizeof(ctx->stats));
+    ctx->stats.ms_total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    ctx->stats.kernel_launches = (int32_t)std::min<long long>(launches.load(), INT32_MAX);
+    ctx->trace_valid = false;
+    return first_err.load();
 }
 
 HP_API int hp_scan_exclusive_i32(hp_context *ctx, const int32_t *d_in, int32_t *d_out, int64_t n,

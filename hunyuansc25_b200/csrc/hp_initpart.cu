@@ -20,6 +20,9 @@
 
 #include "hp_internal.cuh"
 
+// Shared memory for the trial states of one CTA (<= 227 KB per CTA on B200).
+#define HP_TRIAL_SMEM (200 * 1024)
+
 namespace {
 
 struct SubInfo {
@@ -29,150 +32,123 @@ struct SubInfo {
     int64_t slab_off;
 };
 
-__host__ __device__ inline int64_t slab_bytes(int32_t n)
-{
-    return (((int64_t)3 * n + 15) & ~(int64_t)15) + (int64_t)36 * n + 16;
-}
-
-// ---- device max-heap ordered by (key desc, vertex asc) ----------------------
-struct DHeap {
-    int32_t *heap, *pos, *key;
-    int32_t len;
-    __device__ __forceinline__ bool above(int32_t a, int32_t b) const
-    {
-        int32_t ka = key[a], kb = key[b];
-        return ka > kb || (ka == kb && a < b);
-    }
-    __device__ void up(int32_t i)
-    {
-        int32_t v = heap[i];
-        while (i > 0) {
-            int32_t p = (i - 1) >> 1;
-            if (!above(v, heap[p])) break;
-            heap[i] = heap[p];
-            pos[heap[i]] = i;
-            i = p;
-        }
-        heap[i] = v;
-        pos[v] = i;
-    }
-    __device__ void down(int32_t i)
-    {
-        int32_t v = heap[i];
-        for (;;) {
-            int32_t l = 2 * i + 1, r = l + 1, b = i, bv = v;
-            if (l < len && above(heap[l], bv)) { b = l; bv = heap[l]; }
-            if (r < len && above(heap[r], bv)) { b = r; bv = heap[r]; }
-            if (b == i) break;
-            heap[i] = bv;
-            pos[bv] = i;
-            i = b;
-        }
-        heap[i] = v;
-        pos[v] = i;
-    }
-    __device__ void insert(int32_t v, int32_t k)
-    {
-        key[v] = k;
-        heap[len] = v;
-        pos[v] = len;
-        len++;
-        up(len - 1);
-    }
-    __device__ void remove(int32_t v)
-    {
-        int32_t i = pos[v];
-        pos[v] = -1;
-        len--;
-        if (i == len) return;
-        int32_t last = heap[len];
-        heap[i] = last;
-        pos[last] = i;
-        up(i);
-        down(pos[last]);
-    }
-    __device__ void update(int32_t v, int32_t k)
-    {
-        key[v] = k;
-        up(pos[v]);
-        down(pos[v]);
-    }
-    __device__ int32_t pop()
-    {
-        if (len == 0) return -1;
-        int32_t v = heap[0];
-        remove(v);
-        return v;
-    }
+// One BFS-growth + FM bisection trial per warp.  Trial state lives in shared
+// memory when the largest subgraph of the depth fits (else in a global slab).
+//
+// FM without a heap: the reference's priority queues
+// (hunyuangraph_CPU_2wayrefine.h:117-225, hunyuangraph_priorityqueue.h) only
+// ever hold the vertices v with bnd[v] && moved[v] == -1, keyed by ed[v]-id[v]
+// (every insert/update/delete keeps that invariant), so popping side `from`
+// is an argmax of (ed-id desc, v asc) over {bnd, not moved, where == from}.
+// The warp computes that argmax in n/32 steps and updates the moved vertex's
+// neighbours in parallel, which is exact and needs no heap maintenance on
+// dense coarse graphs.
+struct TrialState {
+    int8_t *where, *bnd, *vis;
+    int32_t *id, *ed, *moved, *swaps;   // swaps doubles as the BFS queue
 };
 
-// One BFS-growth + FM bisection trial per thread.
-__global__ void __launch_bounds__(128)
-trial_kernel(const SubInfo *__restrict__ subs, const int32_t *__restrict__ trial_sub,
-             int32_t ntrials, const int32_t *__restrict__ fxadj, const int32_t *__restrict__ fadj,
-             const int32_t *__restrict__ fwgt, const int32_t *__restrict__ fvwgt, char *slab_base,
-             int32_t starts, int32_t fm_passes, int64_t *tr_cut, int64_t *tr_viol)
+__host__ __device__ inline int64_t state_bytes(int32_t n)
 {
-    const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    return (((int64_t)3 * n + 15) & ~(int64_t)15) + (int64_t)16 * n + 16;
+}
+
+__device__ __forceinline__ TrialState carve(char *p, int32_t n)
+{
+    TrialState t;
+    t.where = (int8_t *)p;
+    t.bnd = t.where + n;
+    t.vis = t.bnd + n;
+    int32_t *ip = (int32_t *)(p + (((int64_t)3 * n + 15) & ~(int64_t)15));
+    t.id = ip;
+    t.ed = ip + n;
+    t.moved = ip + 2 * n;
+    t.swaps = ip + 3 * n;
+    return t;
+}
+
+__global__ void __launch_bounds__(128)
+trial_warp_kernel(const SubInfo *__restrict__ subs, const int32_t *__restrict__ trial_sub,
+                  int32_t ntrials, const int32_t *__restrict__ fxadj, const int32_t *__restrict__ fadj,
+                  const int32_t *__restrict__ fwgt, const int32_t *__restrict__ fvwgt, char *slab_base,
+                  int32_t starts, int32_t fm_passes, int64_t *tr_cut, int64_t *tr_viol,
+                  int use_smem, int64_t smem_per_warp)
+{
+    extern __shared__ __align__(16) char tsm[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int32_t t = blockIdx.x * (blockDim.x >> 5) + wib;
     if (t >= ntrials) return;
     const SubInfo S = subs[trial_sub[t]];
     const int32_t lt = t - S.tbeg;
     const int32_t n = S.n;
     const int32_t *xadj = fxadj + S.vbeg;   // global edge offsets, local neighbour ids
     const int32_t *vwgt = fvwgt + S.vbeg;
-    char *slab = slab_base + S.slab_off + (int64_t)lt * slab_bytes(n);
-    int8_t *where = (int8_t *)slab;
-    int8_t *bnd = where + n;
-    int8_t *vis = bnd + n;
-    int32_t *ip = (int32_t *)(slab + (((int64_t)3 * n + 15) & ~(int64_t)15));
-    int32_t *id = ip, *ed = ip + n, *moved = ip + 2 * n, *swaps = ip + 3 * n, *pos = ip + 4 * n;
-    int32_t *key = ip + 5 * n, *heap0 = ip + 6 * n, *heap1 = ip + 7 * n, *queue = ip + 8 * n;
+    char *base = use_smem ? tsm + (int64_t)wib * smem_per_warp
+                          : slab_base + S.slab_off + (int64_t)lt * state_bytes(n);
+    TrialState T = carve(base, n);
     const int32_t start = (n <= starts) ? lt : (int32_t)(((int64_t)lt * n) / starts);
     const int64_t tv = S.tv, want1 = S.want1, onemin = S.onemin, onemax = S.onemax;
     int64_t pw0 = 0, pw1 = tv;
 
-    // BFS growth of side 0 (hunyuangraph_CPU_initialpartition.h:66-120)
-    for (int32_t v = 0; v < n; v++) { where[v] = 1; vis[v] = 0; }
+    // ---- BFS growth of side 0 (hunyuangraph_CPU_initialpartition.h:66-120)
+    for (int32_t v = lane; v < n; v += 32) { T.where[v] = 1; T.vis[v] = 0; }
+    __syncwarp();
     int32_t first = 0, last = 1, nleft = n - 1, next_unvis = 0;
     bool drain = false;
-    queue[0] = start;
-    vis[start] = 1;
+    if (lane == 0) { T.swaps[0] = start; T.vis[start] = 1; }
+    __syncwarp();
     for (;;) {
         if (first == last) {
             if (nleft == 0 || drain) break;
-            while (vis[next_unvis]) next_unvis++;
-            queue[0] = next_unvis;
-            vis[next_unvis] = 1;
+            // lowest unvisited vertex
+            for (;;) {
+                int32_t v = next_unvis + lane;
+                bool un = v < n && !T.vis[v];
+                unsigned m = __ballot_sync(HP_FULL_MASK, un);
+                if (m) { next_unvis += __ffs(m) - 1; break; }
+                next_unvis += 32;
+            }
+            if (lane == 0) { T.swaps[0] = next_unvis; T.vis[next_unvis] = 1; }
+            __syncwarp();
             first = 0; last = 1; nleft--;
         }
-        int32_t i = queue[first++];
-        if (pw0 > 0 && pw1 - vwgt[i] < onemin) { drain = true; continue; }
-        where[i] = 0;
-        pw0 += vwgt[i]; pw1 -= vwgt[i];
+        const int32_t i = T.swaps[first++];
+        const int32_t wi = vwgt[i];
+        if (pw0 > 0 && pw1 - wi < onemin) { drain = true; continue; }
+        if (lane == 0) T.where[i] = 0;
+        pw0 += wi; pw1 -= wi;
         if (pw1 <= onemax) break;
         drain = false;
-        for (int32_t j = xadj[i]; j < xadj[i + 1]; j++) {
-            int32_t k = fadj[j];
-            if (!vis[k]) { queue[last++] = k; vis[k] = 1; nleft--; }
+        for (int32_t base_j = xadj[i]; base_j < xadj[i + 1]; base_j += 32) {
+            int32_t j = base_j + lane;
+            int32_t k = -1;
+            bool un = false;
+            if (j < xadj[i + 1]) { k = fadj[j]; un = !T.vis[k]; }
+            unsigned m = __ballot_sync(HP_FULL_MASK, un);
+            if (un) { T.swaps[last + __popc(m & hp::lanemask_lt())] = k; T.vis[k] = 1; }
+            last += __popc(m);
+            nleft -= __popc(m);
+            __syncwarp();
         }
     }
+    __syncwarp();
 
-    // 2-way FM (hunyuangraph_CPU_2wayrefine.h:77-245)
-    int64_t cut = 0;
-    for (int32_t v = 0; v < n; v++) {
+    // ---- 2-way FM (hunyuangraph_CPU_2wayrefine.h:24-245)
+    long long cut2 = 0;
+    for (int32_t v = lane; v < n; v += 32) {
         int32_t tid = 0, ted = 0;
-        const int8_t wv = where[v];
+        const int8_t wv = T.where[v];
         for (int32_t j = xadj[v]; j < xadj[v + 1]; j++) {
-            if (where[fadj[j]] == wv) tid += fwgt[j];
+            if (T.where[fadj[j]] == wv) tid += fwgt[j];
             else ted += fwgt[j];
         }
-        id[v] = tid; ed[v] = ted;
-        bnd[v] = (ted > 0 || xadj[v] == xadj[v + 1]);
-        cut += ted;
-        moved[v] = -1;
-        pos[v] = -1;
+        T.id[v] = tid; T.ed[v] = ted;
+        T.bnd[v] = (ted > 0 || xadj[v] == xadj[v + 1]);
+        cut2 += ted;
+        T.moved[v] = -1;
     }
-    cut /= 2;
+    int64_t cut = hp::warp_sum64(cut2) / 2;
+    __syncwarp();
     const int64_t tpw0 = tv - want1, tpw1 = want1;
     int64_t limit = n / 100;
     if (limit < 15) limit = 15;
@@ -180,74 +156,82 @@ trial_kernel(const SubInfo *__restrict__ subs, const int32_t *__restrict__ trial
     int64_t avgvwgt = (pw0 + pw1) / 20;
     if (n > 0 && 2 * (pw0 + pw1) / n < avgvwgt) avgvwgt = 2 * (pw0 + pw1) / n;
     const int64_t origdiff = hp::iabs64(tpw0 - pw0);
-    DHeap q[2];
-    q[0].heap = heap0; q[1].heap = heap1;
-    q[0].pos = q[1].pos = pos;
-    q[0].key = q[1].key = key;
+
+    // neighbour update after h moved to `to`
+    auto relax = [&](int32_t h, int to) {
+        for (int32_t j = xadj[h] + lane; j < xadj[h + 1]; j += 32) {
+            const int32_t k = fadj[j];
+            const int32_t kw = (to == T.where[k]) ? fwgt[j] : -fwgt[j];
+            const int32_t nid = T.id[k] + kw, ned = T.ed[k] - kw;
+            T.id[k] = nid; T.ed[k] = ned;
+            if (T.bnd[k]) { if (ned == 0) T.bnd[k] = 0; }
+            else if (ned > 0) T.bnd[k] = 1;
+        }
+        __syncwarp();
+    };
+
     for (int32_t pass = 0; pass < fm_passes; pass++) {
-        q[0].len = q[1].len = 0;
-        for (int32_t v = 0; v < n; v++) pos[v] = -1;
         int64_t mincutorder = -1;
         int64_t newcut = cut, mincut = cut, initcut = cut;
         int64_t mindiff = hp::iabs64(tpw0 - pw0);
-        for (int32_t v = 0; v < n; v++)
-            if (bnd[v]) q[where[v]].insert(v, ed[v] - id[v]);
         int32_t nswaps;
         for (nswaps = 0; nswaps < n; nswaps++) {
-            int from = (tpw0 - pw0 < tpw1 - pw1) ? 0 : 1;
-            int to = 1 - from;
-            int32_t h = q[from].pop();
+            const int from = (tpw0 - pw0 < tpw1 - pw1) ? 0 : 1;
+            const int to = 1 - from;
+            // pop: argmax (ed-id desc, v asc) over {bnd, not moved, side from}
+            int32_t bh = -1, bk = 0;
+            for (int32_t v = lane; v < n; v += 32) {
+                if (T.bnd[v] && T.moved[v] == -1 && T.where[v] == from) {
+                    int32_t key = T.ed[v] - T.id[v];
+                    if (bh < 0 || key > bk) { bh = v; bk = key; }   // ascending v per lane
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                int32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
+                int32_t ok = __shfl_xor_sync(HP_FULL_MASK, bk, o);
+                if (oh >= 0 && (bh < 0 || ok > bk || (ok == bk && oh < bh))) { bh = oh; bk = ok; }
+            }
+            const int32_t h = bh;
             if (h < 0) break;
-            newcut -= (ed[h] - id[h]);
-            if (to == 0) { pw0 += vwgt[h]; pw1 -= vwgt[h]; } else { pw1 += vwgt[h]; pw0 -= vwgt[h]; }
+            const int32_t gain = bk, wh = vwgt[h];
+            newcut -= gain;
+            if (to == 0) { pw0 += wh; pw1 -= wh; } else { pw1 += wh; pw0 -= wh; }
             if ((newcut < mincut && hp::iabs64(tpw0 - pw0) <= origdiff + avgvwgt) ||
                 (newcut == mincut && hp::iabs64(tpw0 - pw0) < mindiff)) {
                 mincut = newcut;
                 mindiff = hp::iabs64(tpw0 - pw0);
                 mincutorder = nswaps;
             } else if (nswaps - mincutorder > limit) {
-                newcut += (ed[h] - id[h]);
-                if (to == 0) { pw0 -= vwgt[h]; pw1 += vwgt[h]; } else { pw1 -= vwgt[h]; pw0 += vwgt[h]; }
+                newcut += gain;
+                if (to == 0) { pw0 -= wh; pw1 += wh; } else { pw1 -= wh; pw0 += wh; }
                 break;
             }
-            where[h] = (int8_t)to;
-            moved[h] = nswaps;
-            swaps[nswaps] = h;
-            { int32_t tt = id[h]; id[h] = ed[h]; ed[h] = tt; }
-            if (ed[h] == 0 && xadj[h] < xadj[h + 1]) bnd[h] = 0;
-            for (int32_t j = xadj[h]; j < xadj[h + 1]; j++) {
-                int32_t k = fadj[j];
-                int32_t kw = (to == where[k]) ? fwgt[j] : -fwgt[j];
-                id[k] += kw; ed[k] -= kw;
-                if (bnd[k]) {
-                    if (ed[k] == 0) {
-                        bnd[k] = 0;
-                        if (moved[k] == -1 && pos[k] >= 0) q[where[k]].remove(k);
-                    } else if (moved[k] == -1 && pos[k] >= 0) {
-                        q[where[k]].update(k, ed[k] - id[k]);
-                    }
-                } else if (ed[k] > 0) {
-                    bnd[k] = 1;
-                    if (moved[k] == -1) q[where[k]].insert(k, ed[k] - id[k]);
-                }
+            if (lane == 0) {
+                T.where[h] = (int8_t)to;
+                T.moved[h] = nswaps;
+                T.swaps[nswaps] = h;
+                int32_t tt = T.id[h]; T.id[h] = T.ed[h]; T.ed[h] = tt;
+                if (T.ed[h] == 0 && xadj[h] < xadj[h + 1]) T.bnd[h] = 0;
             }
+            __syncwarp();
+            relax(h, to);
         }
-        for (int32_t i = 0; i < nswaps; i++) moved[swaps[i]] = -1;
+        for (int32_t i = lane; i < nswaps; i += 32) T.moved[T.swaps[i]] = -1;
+        __syncwarp();
         for (nswaps--; nswaps > mincutorder; nswaps--) {
-            int32_t h = swaps[nswaps];
-            int to = 1 - where[h];
-            where[h] = (int8_t)to;
-            { int32_t tt = id[h]; id[h] = ed[h]; ed[h] = tt; }
-            if (ed[h] == 0 && bnd[h] && xadj[h] < xadj[h + 1]) bnd[h] = 0;
-            else if (ed[h] > 0 && !bnd[h]) bnd[h] = 1;
-            if (to == 0) { pw0 += vwgt[h]; pw1 -= vwgt[h]; } else { pw1 += vwgt[h]; pw0 -= vwgt[h]; }
-            for (int32_t j = xadj[h]; j < xadj[h + 1]; j++) {
-                int32_t k = fadj[j];
-                int32_t kw = (to == where[k]) ? fwgt[j] : -fwgt[j];
-                id[k] += kw; ed[k] -= kw;
-                if (bnd[k] && ed[k] == 0) bnd[k] = 0;
-                if (!bnd[k] && ed[k] > 0) bnd[k] = 1;
+            const int32_t h = T.swaps[nswaps];
+            const int to = 1 - T.where[h];
+            if (lane == 0) {
+                T.where[h] = (int8_t)to;
+                int32_t tt = T.id[h]; T.id[h] = T.ed[h]; T.ed[h] = tt;
+                if (T.ed[h] == 0 && T.bnd[h] && xadj[h] < xadj[h + 1]) T.bnd[h] = 0;
+                else if (T.ed[h] > 0 && !T.bnd[h]) T.bnd[h] = 1;
             }
+            const int32_t wh = vwgt[h];
+            if (to == 0) { pw0 += wh; pw1 -= wh; } else { pw1 += wh; pw0 -= wh; }
+            __syncwarp();
+            relax(h, to);
         }
         cut = mincut;
         if (mincutorder <= 0 || mincut == initcut) break;
@@ -255,8 +239,11 @@ trial_kernel(const SubInfo *__restrict__ subs, const int32_t *__restrict__ trial
     int64_t viol = 0;
     if (pw1 > onemax) viol += pw1 - onemax;
     if (pw1 < onemin) viol += onemin - pw1;
-    tr_cut[t] = cut;
-    tr_viol[t] = viol;
+    // the trial's sides go to the global slab for the selection kernel
+    int8_t *wout = (int8_t *)(slab_base + S.slab_off + (int64_t)lt * state_bytes(n));
+    if (use_smem)
+        for (int32_t v = lane; v < n; v += 32) wout[v] = T.where[v];
+    if (lane == 0) { tr_cut[t] = cut; tr_viol[t] = viol; }
 }
 
 // Best trial of every subgraph: min (violation, cut, trial index); copies its
@@ -295,7 +282,7 @@ select_kernel(const SubInfo *__restrict__ subs, const int64_t *__restrict__ tr_c
         s_best = bt;
     }
     __syncthreads();
-    const int8_t *w = (const int8_t *)(slab_base + S.slab_off + (int64_t)s_best * slab_bytes(S.n));
+    const int8_t *w = (const int8_t *)(slab_base + S.slab_off + (int64_t)s_best * state_bytes(S.n));
     long long n0 = 0, tv0 = 0;
     for (int i = threadIdx.x; i < S.n; i += blockDim.x) {
         int sd = w[i];
@@ -410,6 +397,13 @@ inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)std::max<int64_t
 
 }  // namespace
 
+int hp_initpart_init()
+{
+    HP_CUDA(cudaFuncSetAttribute(trial_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)HP_TRIAL_SMEM));
+    return HP_OK;
+}
+
 int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_t *h_tw,
                          int64_t ub2_fx, int32_t *d_where)
 {
@@ -471,7 +465,7 @@ int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_
             I.ntr = H.n <= starts ? H.n : starts;
             I.tbeg = tcount;
             I.slab_off = slab_total;
-            slab_total += (int64_t)I.ntr * slab_bytes(H.n);
+            slab_total += (int64_t)I.ntr * state_bytes(H.n);
             for (int32_t t = 0; t < I.ntr; t++) trial_sub.push_back(s);
             tcount += I.ntr;
         }
@@ -485,9 +479,17 @@ int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_
         HP_CHECK_OOM(c);
         HP_CUDA(cudaMemcpyAsync(d_info, info.data(), sizeof(SubInfo) * ns, cudaMemcpyHostToDevice, c->stream));
         HP_CUDA(cudaMemcpyAsync(d_tsub, trial_sub.data(), sizeof(int32_t) * tcount, cudaMemcpyHostToDevice, c->stream));
+        // trial state in shared memory when the largest subgraph fits
+        int32_t maxn = 0;
+        for (const HostSub &H : subs) maxn = std::max(maxn, H.n);
+        const int64_t per = (state_bytes(maxn) + 15) & ~(int64_t)15;
+        const int wpb = (int)std::max<int64_t>(1, std::min<int64_t>(4, HP_TRIAL_SMEM / per));
+        const int use_smem = per <= HP_TRIAL_SMEM ? 1 : 0;
+        const int wpb_eff = use_smem ? wpb : 4;
         const int tok = hp_prof_begin(c);
-        HP_LAUNCH(c, trial_kernel, nblk(tcount, 128), 128, 0, d_info, d_tsub, tcount, fxadj, fadj, fwgt,
-                  fvwgt, slab, starts, fm_passes, d_cut, d_viol);
+        HP_LAUNCH(c, trial_warp_kernel, nblk(tcount, wpb_eff), 32 * wpb_eff,
+                  use_smem ? (size_t)(per * wpb_eff) : 0, d_info, d_tsub, tcount, fxadj, fadj, fwgt, fvwgt,
+                  slab, starts, fm_passes, d_cut, d_viol, use_smem, per);
         hp_prof_end(c, tok, HP_PROF_INIT, 0);
         HP_LAUNCH(c, select_kernel, (unsigned)ns, 256, 0, d_info, d_cut, d_viol, slab, fvwgt, side, d_res);
         std::vector<int64_t> res(2 * ns);

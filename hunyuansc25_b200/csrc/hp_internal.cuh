@@ -46,6 +46,7 @@ struct hp_context {
     int prof_next = 0;
 
     hp_stats stats = {};
+    std::vector<hp_context *> workers;   // batch worker contexts (own streams and arenas)
     std::vector<HpLevel> levels;
     bool trace_valid = false;
     hp_options opt = {};
@@ -133,6 +134,7 @@ int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_
 int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int64_t *h_maxp);
 // One-time kernel attributes (dynamic shared memory above 48 KB).
 int hp_refine_init();
+int hp_initpart_init();
 
 // ---- targets shared with the host driver -----------------------------------------
 void hp_part_targets(int64_t tvwgt, int32_t nparts, const float *tpwgts, float ubfactor,

@@ -54,6 +54,9 @@ def _lib():
         lib.hp_gen_set_threads.argtypes = [C.c_int]
         lib.hp_gen_edge_weight.argtypes = [C.c_uint64, C.c_int32, C.c_int32, C.c_int32, C.c_int32]
         lib.hp_gen_edge_weight.restype = C.c_int32
+        lib.hp_read_metis.argtypes = [C.c_char_p, C.POINTER(_HpGraph), C.c_char_p, C.c_int]
+        lib.hp_write_partition.argtypes = [C.c_char_p, C.POINTER(C.c_int32), C.c_int32, C.c_int32]
+        lib.hp_write_metis.argtypes = [C.c_char_p, C.POINTER(_HpGraph)]
         _LIB = lib
     return _LIB
 
@@ -98,6 +101,33 @@ def _take(g: _HpGraph, name: str) -> Graph:
 def _check(rc, what):
     if rc != 0:
         raise RuntimeError(f"{what} failed with code {rc}")
+
+
+def read_metis(path: str) -> Graph:
+    """Read a METIS .graph file (replaces hunyuangraph_readgraph, hunyuangraph_io.h:25-187)."""
+    g = _HpGraph()
+    err = C.create_string_buffer(512)
+    rc = _lib().hp_read_metis(path.encode(), C.byref(g), err, 512)
+    if rc != 0:
+        raise ValueError(f"{path}: {err.value.decode() or rc}")
+    return _take(g, os.path.basename(path))
+
+
+def write_metis(path: str, g: Graph) -> None:
+    h = _HpGraph(g.nvtxs, g.nedges, g.xadj.ctypes.data_as(C.POINTER(C.c_int32)),
+                 g.adjncy.ctypes.data_as(C.POINTER(C.c_int32)), g.vwgt.ctypes.data_as(C.POINTER(C.c_int32)),
+                 g.adjwgt.ctypes.data_as(C.POINTER(C.c_int32)))
+    if _lib().hp_write_metis(path.encode(), C.byref(h)) != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def write_partition(fname: str, part, nparts: int) -> str:
+    """Write <fname>.part.<nparts> (replaces hunyuangraph_writetofile, hunyuangraph_io.h:190-205)."""
+    p = np.ascontiguousarray(part, dtype=np.int32)
+    if _lib().hp_write_partition(fname.encode(), p.ctypes.data_as(C.POINTER(C.c_int32)), p.shape[0],
+                                 nparts) != 0:
+        raise OSError(f"cannot write {fname}.part.{nparts}")
+    return f"{fname}.part.{nparts}"
 
 
 def set_threads(n: int) -> None:
