@@ -14,6 +14,7 @@ HP_ERR_UNSUPPORTED = -7
 HP_ERR_INTERNAL = -8
 HP_MAX_PARTS = 16384
 HP_OPTIONS_VERSION = 1
+HP_SCAN_NOALLOC_MAX_N = 1 << 26
 
 HP_TRACE_XADJ = 0
 HP_TRACE_ADJNCY = 1
@@ -135,6 +136,7 @@ PROTOTYPES = {
                                      I32P, F32P, C.POINTER(HpOptions), I32P, I64P]),
     "hp_scan_exclusive_i32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                         C.c_void_p]),
+    "hp_scan_exclusive_i32_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "hp_edgecut_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, I64P]),
     "hunyuangraph_PartitionGraph": (None, [I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P]),

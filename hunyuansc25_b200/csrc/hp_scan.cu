@@ -8,6 +8,8 @@
 // time) until it meets an inclusive prefix.  Every wait is bounded
 // (HP_SPIN_LIMIT); on expiry the CTA sets HP_STATUS_SPIN_TIMEOUT and continues,
 // so a stalled predecessor can never hang the device.
+#include <mutex>
+
 #include "hp_internal.cuh"
 
 namespace {
@@ -176,6 +178,66 @@ int hp_scan_excl(hp_context *c, const int32_t *in, int32_t *out, int64_t n)
               c->d_status);
     c->hi = mark;
     return HP_OK;
+}
+
+// ---- scan without any allocation ---------------------------------------------------
+// Fixed scratch in the library's device image: the look-back tile status words
+// for up to HP_SCAN_NOALLOC_MAX_N elements, then the dynamic tile counter and a
+// status word (one 8-byte slot each).  Every GPU that loads the library holds
+// this array (about 128 KiB) until the process exits.
+#define HP_NOALLOC_TILES ((HP_SCAN_NOALLOC_MAX_N + 1 + SCAN_TILE - 1) / SCAN_TILE)
+static __device__ __align__(256) unsigned long long g_scan_noalloc_scratch[HP_NOALLOC_TILES + 2];
+
+namespace {
+std::mutex g_noalloc_mu;
+unsigned long long *g_noalloc_ptr[64] = {};   // device address per CUDA ordinal
+}
+
+extern "C" __attribute__((visibility("default")))
+int hp_scan_exclusive_i32_noalloc(const int32_t *d_in, int32_t *d_out, int64_t n, void *stream)
+{
+    if (n < 0 || (!d_in && n > 0) || !d_out) return HP_ERR_INVALID_ARG;
+    if (n > HP_SCAN_NOALLOC_MAX_N) {
+        fprintf(stderr, "hp_scan_exclusive_i32_noalloc: n = %lld exceeds the fixed scratch limit of %lld "
+                        "elements; use hp_scan_exclusive_i32 with a context\n",
+                (long long)n, (long long)HP_SCAN_NOALLOC_MAX_N);
+        return HP_ERR_UNSUPPORTED;
+    }
+    int dev = 0;
+    HP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return HP_ERR_UNSUPPORTED;
+    unsigned long long *scratch = nullptr;
+    {
+        // set-up, once per device, with that device current: the host-side
+        // name of a __device__ array is not a device address, so look it up
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[dev]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_scan_noalloc_scratch);
+            if (e != cudaSuccess || !p) {
+                fprintf(stderr, "hp_scan_exclusive_i32_noalloc: cudaGetSymbolAddress failed: %s\n",
+                        cudaGetErrorString(e));
+                return HP_ERR_CUDA;
+            }
+            g_noalloc_ptr[dev] = (unsigned long long *)p;
+        }
+        scratch = g_noalloc_ptr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t ntiles = (n + 1 + SCAN_TILE - 1) / SCAN_TILE;
+    unsigned long long *counter_slot = scratch + HP_NOALLOC_TILES;
+    unsigned long long *status_slot = scratch + HP_NOALLOC_TILES + 1;
+    // the array keeps the last call's contents: clear the tile words this call
+    // uses, the counter and the status word
+    HP_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * (size_t)ntiles, s));
+    HP_CUDA(cudaMemsetAsync(counter_slot, 0, sizeof(unsigned long long) * 2, s));
+    scan_excl_kernel<<<(unsigned)ntiles, SCAN_BLOCK, 0, s>>>(d_in, d_out, n, scratch, (unsigned *)counter_slot,
+                                                             (unsigned *)status_slot);
+    HP_CUDA(cudaGetLastError());
+    unsigned st = 0;
+    HP_CUDA(cudaMemcpyAsync(&st, status_slot, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    HP_CUDA(cudaStreamSynchronize(s));
+    return (st & HP_STATUS_SPIN_TIMEOUT) ? HP_ERR_TIMEOUT : HP_OK;
 }
 
 int hp_fill_i32(hp_context *c, int32_t *p, int64_t n, int32_t value)

@@ -165,6 +165,27 @@ int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *vtxdist,
 int hp_scan_exclusive_i32(hp_context *ctx, const int32_t *d_in, int32_t *d_out,
                           int64_t n, void *stream);
 
+/* Exclusive int32 prefix sum that allocates nothing: same result as
+ * hp_scan_exclusive_i32, without a context.  No counterpart in the reference
+ * (its prefix sum draws scratch from its device pool).
+ *
+ * For callers that cannot call cudaMalloc: code whose device memory is owned
+ * by a host framework's caching allocator that admits no outside allocations,
+ * and latency-critical pipelines that cannot take cudaMalloc's implicit device
+ * synchronisation.  The scan's look-back scratch is a fixed array in the
+ * library's device image (about 128 KiB, held by every GPU that loads the
+ * library until the process exits), so n is limited to
+ * HP_SCAN_NOALLOC_MAX_N; larger n returns HP_ERR_UNSUPPORTED with a message
+ * on stderr.  The caller still passes d_in and d_out (n + 1 entries).
+ *   - The first call on a device looks up the array's device address with that
+ *     device current; make that first call before any stream capture.
+ *   - Runs on the calling thread's current device and `stream`, and returns
+ *     after the scan completed (it reads the status word back).
+ *   - All calls share the one array: calls that overlap on the GPU (other
+ *     streams, other threads) race and must be serialised by the caller. */
+#define HP_SCAN_NOALLOC_MAX_N ((int64_t)1 << 26)
+int hp_scan_exclusive_i32_noalloc(const int32_t *d_in, int32_t *d_out, int64_t n, void *stream);
+
 /* Exact int64 edge cut of a device-resident partition.  Replaces
  * compute_edgecut_gpu (hunyuangraph_graph.h:230-268). */
 int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xadj,
