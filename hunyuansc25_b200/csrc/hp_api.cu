@@ -23,24 +23,47 @@
 
 namespace {
 
-__global__ void validate_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
-                                const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt,
-                                const int32_t *__restrict__ vwgt, unsigned *status)
+// Structural validation: vertex checks per thread, adjacency checks in
+// edge-parallel tiles of 256 x 32 entries (the owner of an entry is found by a
+// binary search over xadj, then a forward walk), so hub rows cost no more than
+// their share of the array.
+__global__ void validate_vertices_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
+                                         const int32_t *__restrict__ vwgt, unsigned *status)
 {
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     bool bad = false;
-    for (int64_t v = tid; v < n; v += stride) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         int32_t b = xadj[v], e = xadj[v + 1];
-        if (b > e || b < 0 || e > m) { bad = true; continue; }
+        if (b > e || b < 0 || e > m) bad = true;
         if (vwgt && vwgt[v] < 0) bad = true;
-        for (int32_t j = b; j < e; j++) {
-            int32_t u = adjncy[j];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (xadj[0] != 0 || xadj[n] != m)) bad = true;
+    if (bad) atomicOr(status, HP_STATUS_BAD_GRAPH);
+}
+
+// Runs after validate_vertices_kernel succeeded (xadj monotone, in range).
+__global__ void __launch_bounds__(256)
+validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
+                      const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt, unsigned *status)
+{
+    if (*status & HP_STATUS_BAD_GRAPH) return;
+    const int64_t tile = 256 * 32;
+    bool bad = false;
+    for (int64_t tb = blockIdx.x * tile; tb < m; tb += (int64_t)gridDim.x * tile) {
+        int64_t j = tb + threadIdx.x;
+        if (j >= m) continue;
+        int32_t lo = 0, hi = n - 1;
+        while (lo < hi) {
+            int32_t mid = (int32_t)(((int64_t)lo + hi + 1) / 2);
+            if (xadj[mid] <= j) lo = mid; else hi = mid - 1;
+        }
+        int32_t v = lo;
+        for (int k = 0; k < 32 && j < m; k++, j += 256) {
+            while (xadj[v + 1] <= j) v++;
+            const int32_t u = adjncy[j];
             if (u < 0 || u >= n || u == v) bad = true;
             if (adjwgt && adjwgt[j] <= 0) bad = true;
         }
     }
-    if (tid == 0 && (xadj[0] != 0 || xadj[n] != m)) bad = true;
     if (bad) atomicOr(status, HP_STATUS_BAD_GRAPH);
 }
 
@@ -55,10 +78,22 @@ __global__ void sum_kernel(int64_t n, const int32_t *__restrict__ a, unsigned lo
 __global__ void final_pw_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__restrict__ vwgt,
                                 unsigned long long *pw, int32_t k, unsigned *status)
 {
+    extern __shared__ unsigned long long fpw[];
+    const bool use_s = k <= 2048;
+    if (use_s) {
+        for (int i = threadIdx.x; i < k; i += blockDim.x) fpw[i] = 0;
+        __syncthreads();
+    }
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         int32_t p = where[v];
         if (p < 0 || p >= k) { atomicOr(status, HP_STATUS_OVERFLOW); continue; }
-        atomicAdd(&pw[p], (unsigned long long)vwgt[v]);
+        if (use_s) atomicAdd(&fpw[p], (unsigned long long)vwgt[v]);
+        else atomicAdd(&pw[p], (unsigned long long)vwgt[v]);
+    }
+    if (use_s) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < k; i += blockDim.x)
+            if (fpw[i]) atomicAdd(&pw[i], fpw[i]);
     }
 }
 
@@ -123,8 +158,9 @@ int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, i
     unsigned long long *sc = c->d_scal;
 
     if (c->opt.validate) {
-        HP_LAUNCH(c, validate_kernel, gsz(c, n), 256, 0, n, g0.m, g0.xadj, g0.adjncy, g0.adjwgt,
-                  g0.vwgt, c->d_status);
+        HP_LAUNCH(c, validate_vertices_kernel, gsz(c, n), 256, 0, n, g0.m, g0.xadj, g0.vwgt, c->d_status);
+        HP_LAUNCH(c, validate_edges_kernel, gsz(c, (g0.m + 31) / 32), 256, 0, n, g0.m, g0.xadj, g0.adjncy,
+                  g0.adjwgt, c->d_status);
     }
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 2, c->stream));
     HP_LAUNCH(c, sum_kernel, gsz(c, n), 256, 0, (int64_t)n, g0.vwgt, &sc[0]);
@@ -163,7 +199,8 @@ int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, i
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 2, c->stream));
     HpLevel &f = c->levels[0];
     HP_TRY(hp_edgecut_launch(c, n, f.xadj, f.adjncy, f.adjwgt, f.where, &sc[0]));
-    HP_LAUNCH(c, final_pw_kernel, gsz(c, n), 256, 0, n, f.where, f.vwgt, pw, nparts, c->d_status);
+    HP_LAUNCH(c, final_pw_kernel, gsz(c, n), 256, nparts <= 2048 ? sizeof(unsigned long long) * nparts : 0, n,
+              f.where, f.vwgt, pw, nparts, c->d_status);
     std::vector<unsigned long long> hpw(nparts);
     HP_CUDA(cudaMemcpyAsync(hpw.data(), pw, sizeof(unsigned long long) * nparts, cudaMemcpyDeviceToHost, c->stream));
     long long cut2 = 0;
@@ -378,6 +415,7 @@ HP_API int hp_context_create(int device, hp_context **out)
     for (int i = 0; ok && i < 8; i++) ok = cudaEventCreate(&c->ev[i]) == cudaSuccess;
     ok = ok && hp_refine_init() == HP_OK;
     ok = ok && hp_initpart_init() == HP_OK;
+    ok = ok && hp_coarsen_init() == HP_OK;
     if (!ok) {
         cudaGetLastError();
         hp_context_destroy(c);

@@ -19,7 +19,8 @@
 
 namespace {
 
-constexpr int BIG_DEG = 32;   // rows longer than this use a warp per vertex
+constexpr int BIG_DEG = 32;      // rows longer than this use a warp per vertex
+constexpr int HUGE_DEG = 4096;   // rows longer than this use a CTA per vertex
 
 // ---------------------------------------------------------------------------
 // matching
@@ -111,10 +112,98 @@ commit_kernel(int32_t n, int32_t *__restrict__ match, const int32_t *__restrict_
 }
 
 __global__ void __launch_bounds__(256)
-big_list_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t *list, int32_t *d_count)
+big_list_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t *list, int32_t *d_count,
+                int32_t *huge, int32_t *d_huge)
 {
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < n && xadj[v + 1] - xadj[v] > BIG_DEG) list[atomicAdd(d_count, 1)] = v;
+    if (v >= n) return;
+    const int32_t d = xadj[v + 1] - xadj[v];
+    if (d > HUGE_DEG) huge[atomicAdd(d_huge, 1)] = v;
+    else if (d > BIG_DEG) list[atomicAdd(d_count, 1)] = v;
+}
+
+// CTA per vertex for rows longer than HUGE_DEG (R-MAT hubs).
+template <bool ELIG>
+__global__ void __launch_bounds__(512)
+pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                 const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                 const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
+                 const int32_t *__restrict__ match, int32_t *__restrict__ pref, uint64_t lkey,
+                 int64_t maxvwgt, const unsigned long long *made_prev)
+{
+    if (made_prev && *made_prev == 0ull) return;
+    __shared__ int32_t su[16], sw[16];
+    __shared__ uint32_t sh[16];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int32_t cnt = *d_count;
+    for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
+        const int32_t v = list[li];
+        if (match[v] != -1) { if (threadIdx.x == 0) pref[v] = -1; continue; }
+        const int32_t wv = vwgt[v];
+        int32_t bu = -1, bw = 0;
+        uint32_t bh = 0;
+        for (int32_t j = xadj[v] + threadIdx.x; j < xadj[v + 1]; j += blockDim.x) {
+            int32_t u = adjncy[j];
+            if (u == v) continue;
+            if (ELIG) {
+                if (match[u] != -1) continue;
+                if ((int64_t)wv + vwgt[u] > maxvwgt) continue;
+            }
+            int32_t w = adjwgt[j];
+            uint32_t h = hp::edge_tie(lkey, v, u);
+            if (bu < 0 || hp::better(w, h, u, bw, bh, bu)) { bu = u; bw = w; bh = h; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
+            int32_t ow = __shfl_xor_sync(HP_FULL_MASK, bw, o);
+            uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
+            if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; }
+        }
+        if (lane == 0) { su[wid] = bu; sw[wid] = bw; sh[wid] = bh; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w2 = 1; w2 < (int)(blockDim.x >> 5); w2++)
+                if (su[w2] >= 0 && (bu < 0 || hp::better(sw[w2], sh[w2], su[w2], bw, bh, bu))) {
+                    bu = su[w2]; bw = sw[w2]; bh = sh[w2];
+                }
+            pref[v] = bu;
+        }
+        __syncthreads();
+    }
+}
+
+// Hub pairing for rows longer than HUGE_DEG: clients ranked by a CTA scan.
+__global__ void __launch_bounds__(512)
+pair_hub_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                     const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                     const int32_t *__restrict__ vwgt, const int32_t *__restrict__ hub,
+                     int32_t *__restrict__ match, int64_t maxvwgt)
+{
+    __shared__ int32_t s_scan[512 / 32 + 2];
+    __shared__ int32_t s_cl[512];
+    const int32_t cnt = *d_count;
+    for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
+        const int32_t h = list[li];
+        int32_t t = 0, carry = -1;
+        for (int32_t base = xadj[h]; base < xadj[h + 1]; base += 512) {
+            const int32_t j = base + threadIdx.x;
+            int32_t c = -1;
+            int isc = 0;
+            if (j < xadj[h + 1]) { c = adjncy[j]; isc = hub[c] == h; }
+            int tot;
+            const int ex = hp::block_excl_scan<512>(isc, &tot, s_scan);
+            if (isc) s_cl[ex] = c;
+            __syncthreads();
+            if (isc && ((t + ex) & 1)) {
+                const int32_t first = ex > 0 ? s_cl[ex - 1] : carry;
+                if ((int64_t)vwgt[first] + vwgt[c] <= maxvwgt) { match[first] = c; match[c] = first; }
+            }
+            if (tot > 0 && ((t + tot - 1) & 1) == 0) carry = s_cl[tot - 1];
+            t += tot;
+            __syncthreads();
+        }
+    }
 }
 
 __global__ void __launch_bounds__(256)
@@ -287,33 +376,61 @@ contract_warp_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict__ to
     }
 }
 
-template <int NT, int CAP>
+// Rows of 33..HCAP/2 entries: one CTA merges equal coarse ids in a
+// shared-memory hash table (linear probing, atomicCAS keys, atomicAdd
+// weights), compacts the unique keys, and bitonic-sorts only those.
+template <int NT, int HCAP>
 __global__ void __launch_bounds__(NT)
-contract_block_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
-                      ContractSrc src, const int32_t *__restrict__ toff, int32_t *__restrict__ tk,
-                      int32_t *__restrict__ tw, int32_t *__restrict__ ucnt)
+contract_hash_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                     ContractSrc src, const int32_t *__restrict__ toff, int32_t *__restrict__ tk,
+                     int32_t *__restrict__ tw, int32_t *__restrict__ ucnt)
 {
-    __shared__ int32_t sk[CAP], sw[CAP];
+    extern __shared__ int32_t hsm[];
+    int32_t *hk = hsm, *hw = hsm + HCAP;                  // hash table
+    int32_t *sk = hsm + 2 * HCAP, *sw = sk + HCAP / 2;    // unique entries to sort
     __shared__ int32_t s_scan[NT / 32 + 2];
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t c = list[li];
         int32_t v, u, lv, len;
         src.row(c, v, u, lv, len);
-        int P = 32;
-        while (P < len) P <<= 1;
-        for (int i = threadIdx.x; i < P; i += NT) {
-            int32_t k = hp::KEY_NONE, w = 0;
-            if (i < len) src.get(c, v, u, lv, i, k, w);
-            sk[i] = k;
-            sw[i] = w;
+        // table sized to the row: H = pow2 >= 2 len (load factor <= 1/2)
+        int H = 64;
+        while (H < 2 * len) H <<= 1;
+        for (int i = threadIdx.x; i < H; i += NT) { hk[i] = hp::KEY_NONE; hw[i] = 0; }
+        __syncthreads();
+        for (int32_t i = threadIdx.x; i < len; i += NT) {
+            int32_t k, w;
+            src.get(c, v, u, lv, i, k, w);
+            if (k == hp::KEY_NONE) continue;
+            uint32_t h = ((uint32_t)k * 2654435761u) & (H - 1);
+            for (;;) {
+                int32_t prev = atomicCAS(&hk[h], hp::KEY_NONE, k);
+                if (prev == hp::KEY_NONE || prev == k) { atomicAdd(&hw[h], w); break; }
+                h = (h + 1) & (H - 1);
+            }
         }
         __syncthreads();
+        // compact occupied slots; thread t owns slots [t*per, (t+1)*per)
+        const int per = (H + NT - 1) / NT;
+        const int lo = threadIdx.x * per, hi = min(lo + per, H);
+        int cntl = 0;
+        for (int i = lo; i < hi; i++) cntl += hk[i] != hp::KEY_NONE;
+        int U;
+        int pos = hp::block_excl_scan<NT>(cntl, &U, s_scan);
+        for (int i = lo; i < hi; i++)
+            if (hk[i] != hp::KEY_NONE) { sk[pos] = hk[i]; sw[pos] = hw[i]; pos++; }
+        int P = 32;
+        while (P < U) P <<= 1;
+        for (int i = U + threadIdx.x; i < P; i += NT) { sk[i] = hp::KEY_NONE; sw[i] = 0; }
+        __syncthreads();
         int32_t off = toff[c];
-        int tot = hp::block_aggregate_smem<NT, CAP>(sk, sw, P, tk + off, tw + off, s_scan);
+        int tot = hp::block_aggregate_smem<NT, HCAP / 2>(sk, sw, P, tk + off, tw + off, s_scan);
         if (threadIdx.x == 0) ucnt[c] = tot;
     }
 }
+
+constexpr size_t hash_smem(int hcap) { return sizeof(int32_t) * (size_t)(3 * hcap); }
 
 // Rows longer than 4096 entries: dense accumulator over the coarse id space in
 // a per-CTA global slab (dw: cn ints, bm: cn/32 words; zero on entry/exit).
@@ -346,18 +463,31 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
     }
 }
 
+// Compacts the unique coarse rows (at upper-bound offsets toff[c]) to their
+// final places cxadj[c]: edge-parallel over the coarse adjacency in tiles of
+// 256 x 32 entries; the owner of an entry is found by binary search over cxadj
+// and a forward walk, so long rows cost their length, not one warp's time.
 __global__ void __launch_bounds__(256)
 copy_rows_kernel(int32_t cn, const int32_t *__restrict__ toff, const int32_t *__restrict__ cxadj,
                  const int32_t *__restrict__ tk, const int32_t *__restrict__ tw,
                  int32_t *__restrict__ cadjncy, int32_t *__restrict__ cadjwgt)
 {
-    const int lane = threadIdx.x & 31;
-    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < cn;
-         c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int32_t s = toff[c], d = cxadj[c], len = cxadj[c + 1] - d;
-        for (int32_t i = lane; i < len; i += 32) {
-            cadjncy[d + i] = tk[s + i];
-            cadjwgt[d + i] = tw[s + i];
+    const int64_t mc = cxadj[cn];
+    const int64_t tile = 256 * 32;
+    for (int64_t tb = blockIdx.x * tile; tb < mc; tb += (int64_t)gridDim.x * tile) {
+        int64_t j = tb + threadIdx.x;
+        if (j >= mc) continue;
+        int32_t lo = 0, hi = cn - 1;
+        while (lo < hi) {
+            int32_t mid = (int32_t)(((int64_t)lo + hi + 1) / 2);
+            if (cxadj[mid] <= j) lo = mid; else hi = mid - 1;
+        }
+        int32_t c = lo;
+        for (int k = 0; k < 32 && j < mc; k++, j += 256) {
+            while (cxadj[c + 1] <= j) c++;
+            const int64_t src = toff[c] + (j - cxadj[c]);
+            cadjncy[j] = tk[src];
+            cadjwgt[j] = tw[src];
         }
     }
 }
@@ -385,6 +515,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
 
     int32_t *pref = ralloc_t<int32_t>(c, n);
     int32_t *big = ralloc_t<int32_t>(c, n);
+    int32_t *huge = ralloc_t<int32_t>(c, n);
     int32_t *flags = ralloc_t<int32_t>(c, n + 1);
     int32_t *list = ralloc_t<int32_t>(c, n + 1);
     HP_CHECK_OOM(c);
@@ -393,9 +524,10 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * HP_NSCAL, c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[0];
     int32_t *d_listcnt = (int32_t *)&sc[1];
+    int32_t *d_hugecnt = (int32_t *)&sc[38];
 
     HP_TRY(hp_fill_i32(c, g.match, n, -1));
-    HP_LAUNCH(c, big_list_kernel, blocks_for(n), 256, 0, n, g.xadj, big, d_bigcnt);
+    HP_LAUNCH(c, big_list_kernel, blocks_for(n), 256, 0, n, g.xadj, big, d_bigcnt, huge, d_hugecnt);
 
     const int rounds = o.match_rounds < 1 ? 1 : (o.match_rounds > 30 ? 30 : o.match_rounds);
     // algorithmic bytes of one full handshake round: xadj, adjncy, adjwgt,
@@ -407,6 +539,8 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
         HP_LAUNCH(c, pref_small_kernel<true>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
                   g.vwgt, g.match, pref, lkey, maxvwgt, prev);
         HP_LAUNCH(c, pref_big_kernel<true>, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj,
+                  g.adjncy, g.adjwgt, g.vwgt, g.match, pref, lkey, maxvwgt, prev);
+        HP_LAUNCH(c, pref_huge_kernel<true>, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, pref, lkey, maxvwgt, prev);
         HP_LAUNCH(c, commit_kernel, blocks_for(n), 256, 0, n, g.match, pref, &sc[2 + r], prev);
         hp_prof_end(c, tok, r == 0 ? HP_PROF_MATCH : 6, r == 0 ? round_bytes : 0);
@@ -429,10 +563,15 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
         HP_LAUNCH(c, pref_big_kernel<false>, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, hub, lkey, maxvwgt,
                   (const unsigned long long *)nullptr);
+        HP_LAUNCH(c, pref_huge_kernel<false>, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
+                  g.adjncy, g.adjwgt, g.vwgt, g.match, hub, lkey, maxvwgt,
+                  (const unsigned long long *)nullptr);
         HP_LAUNCH(c, pair_hub_small_kernel, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.vwgt, hub,
                   g.match, maxvwgt);
         HP_LAUNCH(c, pair_hub_big_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy,
                   g.vwgt, hub, g.match, maxvwgt);
+        HP_LAUNCH(c, pair_hub_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
+                  g.adjncy, g.vwgt, hub, g.match, maxvwgt);
         HP_TRY(matched(41, &nm));
     }
     for (int pass = 0; pass < 2; pass++) {
@@ -490,11 +629,11 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     HP_LAUNCH(c, contract_warp_kernel, blocks_for((int64_t)cn * 32), 256, 0, cn, src, toff, tk, tw,
               ucnt);
     if (h.cnt[0] > 0)
-        HP_LAUNCH(c, (contract_block_kernel<128, 512>), (unsigned)std::min<int64_t>(h.cnt[0], c->sm_count * 16),
-                  128, 0, lists, &counts[0], src, toff, tk, tw, ucnt);
+        HP_LAUNCH(c, (contract_hash_kernel<128, 1024>), (unsigned)std::min<int64_t>(h.cnt[0], c->sm_count * 16),
+                  128, hash_smem(1024), lists, &counts[0], src, toff, tk, tw, ucnt);
     if (h.cnt[1] > 0)
-        HP_LAUNCH(c, (contract_block_kernel<512, 4096>), (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 4),
-                  512, 0, lists + cn, &counts[1], src, toff, tk, tw, ucnt);
+        HP_LAUNCH(c, (contract_hash_kernel<512, 8192>), (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 2),
+                  512, hash_smem(8192), lists + cn, &counts[1], src, toff, tk, tw, ucnt);
     if (h.cnt[2] > 0) {
         // slab per CTA: cn ints + cn/32 words; bounded to ~512 MB
         int64_t slab = (int64_t)cn * 4 + ((int64_t)cn + 31) / 32 * 4;
@@ -518,8 +657,8 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     cg.adjwgt = lalloc_t<int32_t>(c, mc);
     HP_CHECK_OOM(c);
     tok = hp_prof_begin(c);
-    HP_LAUNCH(c, copy_rows_kernel, blocks_for((int64_t)cn * 32), 256, 0, cn, toff, cg.xadj, tk, tw,
-              cg.adjncy, cg.adjwgt);
+    HP_LAUNCH(c, copy_rows_kernel, std::min<unsigned>(blocks_for(((int64_t)mc + 31) / 32), c->sm_count * 16), 256,
+              0, cn, toff, cg.xadj, tk, tw, cg.adjncy, cg.adjwgt);
     // algorithmic bytes of the whole contraction: fine CSR, cmap, match,
     // vwgt in; coarse xadj, adjacency, weights, vertex weights out
     hp_prof_end(c, tok, HP_PROF_CONTRACT,
@@ -530,6 +669,13 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
 }
 
 }  // namespace
+
+int hp_coarsen_init()
+{
+    HP_CUDA(cudaFuncSetAttribute(contract_hash_kernel<512, 8192>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)hash_smem(8192)));
+    return HP_OK;
+}
 
 int hp_coarsen(hp_context *c, int32_t coarsen_to, int64_t maxvwgt)
 {

@@ -135,6 +135,7 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
 // One-time kernel attributes (dynamic shared memory above 48 KB).
 int hp_refine_init();
 int hp_initpart_init();
+int hp_coarsen_init();
 
 // ---- targets shared with the host driver -----------------------------------------
 void hp_part_targets(int64_t tvwgt, int32_t nparts, const float *tpwgts, float ubfactor,

@@ -23,6 +23,7 @@
 namespace {
 
 constexpr int BIGD = 32;
+constexpr int HUGED = 4096;   // afterburner rows longer than this use a CTA per vertex
 constexpr int32_t NEG = INT_MIN;
 
 inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)std::max<int64_t>(1, (n + b - 1) / b); }
@@ -45,24 +46,31 @@ __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int
 }
 
 // Gain row of v: (part, connectivity) for every part adjacent to v, ascending
-// by part, padded with part -1 up to min(deg, k).
+// by part, padded with part -1 up to min(deg, k).  A vertex with deg >= k has a
+// dense row instead: entry q is (q, conn to part q), zeros included; dense rows
+// are updated in place by atomics when a neighbour moves and never rebuilt.
 __global__ void __launch_bounds__(256)
 gain_warp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, int32_t n,
                  const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                  const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                  const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
-                 int32_t *__restrict__ gconn)
+                 int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty)
 {
     const int lane = threadIdx.x & 31;
     const int32_t cnt = list ? *d_count : n;
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = list ? list[i] : (int32_t)i;
+        if (dirty && lane == 0) dirty[v] = 0;
         const int32_t b = xadj[v], d = xadj[v + 1] - b;
         if (d > BIGD) continue;
         int32_t key = hp::KEY_NONE, w = 0;
         if (lane < d) { key = where[adjncy[b + lane]]; w = adjwgt[b + lane]; }
         const int32_t o = goff[v], cap = goff[v + 1] - o;
+        if (d >= k) {   // dense row: entry q is part q (cap == k)
+            hp::warp_aggregate32_dense(key, w, k, gpart + o, gconn + o);
+            continue;
+        }
         int c = hp::warp_aggregate32(key, w, gpart + o, gconn + o);
         for (int32_t t = c + lane; t < cap; t += 32) { gpart[o + t] = -1; gconn[o + t] = 0; }
     }
@@ -74,7 +82,7 @@ gain_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ 
                   const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                   const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
-                  int32_t *__restrict__ gconn, int32_t k)
+                  int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty)
 {
     extern __shared__ int32_t dsm[];
     __shared__ int32_t s_scan[NT / 32 + 2];
@@ -89,6 +97,7 @@ gain_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ 
         const int32_t v = list[li];
         const int32_t b = xadj[v], e = xadj[v + 1];
         if (e - b <= BIGD) continue;
+        if (dirty && threadIdx.x == 0) dirty[v] = 0;
         for (int32_t j = b + threadIdx.x; j < e; j += NT) {
             int32_t q = where[adjncy[j]];
             atomicAdd(&dw[q], adjwgt[j]);
@@ -96,14 +105,26 @@ gain_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ 
         }
         __syncthreads();
         const int32_t o = goff[v], cap = goff[v + 1] - o;
+        if (e - b >= k) {   // dense row
+            for (int32_t q = threadIdx.x; q < k; q += NT) {
+                gpart[o + q] = q;
+                gconn[o + q] = dw[q];
+                dw[q] = 0;
+            }
+            for (int32_t q = threadIdx.x; q < nwords; q += NT) bm[q] = 0;
+            __syncthreads();
+            continue;
+        }
         int c = hp::dense_extract<NT>(dw, bm, k, gpart + o, gconn + o, s_scan);
         for (int32_t t = c + threadIdx.x; t < cap; t += NT) { gpart[o + t] = -1; gconn[o + t] = 0; }
         __syncthreads();
     }
 }
 
-__device__ __forceinline__ int32_t row_conn(const int32_t *gp, const int32_t *gc, int32_t len, int32_t q)
+__device__ __forceinline__ int32_t row_conn(const int32_t *gp, const int32_t *gc, int32_t len, int32_t q,
+                                            int32_t k)
 {
+    if (len == k) return gc[q];   // dense row
     for (int32_t j = 0; j < len; j++) {
         int32_t p = gp[j];
         if (p == q) return gc[j];
@@ -258,6 +279,7 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = big[i];
+        if (xadj[v + 1] - xadj[v] > HUGED) continue;
         const int32_t g = pregain[v];
         int8_t sel = 0;
         if (g != NEG) {
@@ -275,13 +297,49 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
     }
 }
 
+__global__ void __launch_bounds__(512)
+afterburner_huge_kernel(const int32_t *__restrict__ big, const int32_t *__restrict__ d_bigcnt,
+                        const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                        const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
+                        const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
+                        int8_t *__restrict__ lock, const unsigned long long *d_ncand,
+                        int32_t *__restrict__ moves, unsigned long long *d_nmoves)
+{
+    if (*d_ncand == 0ull) return;
+    __shared__ long long s_ch[16];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int32_t cnt = *d_bigcnt;
+    for (int32_t i = blockIdx.x; i < cnt; i += gridDim.x) {
+        const int32_t v = big[i];
+        if (xadj[v + 1] - xadj[v] <= HUGED) continue;
+        const int32_t g = pregain[v];
+        long long ch = 0;
+        if (g != NEG) {
+            const int32_t p = where[v], b = dest[v];
+            for (int32_t j = xadj[v] + threadIdx.x; j < xadj[v + 1]; j += blockDim.x)
+                ch += ab_change(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where);
+        }
+        ch = hp::warp_sum64(ch);
+        if (lane == 0) s_ch[wid] = ch;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            long long tot = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += s_ch[w];
+            int8_t sel = (g != NEG) && ((long long)g + tot >= 0);
+            lock[v] = sel;
+            if (sel) moves[atomicAdd(d_nmoves, 1ull)] = v;
+        }
+        __syncthreads();
+    }
+}
+
 // ---- applying moves -------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 c_delta_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
                const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
                const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
                const int32_t *__restrict__ dest, int32_t *__restrict__ oldp, int before,
-               unsigned long long *d_c)
+               unsigned long long *d_c, int32_t k)
 {
     const int64_t nm = (int64_t)*d_nmoves;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -292,31 +350,73 @@ c_delta_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nm
         int32_t from, to;
         if (before) { from = where[v]; to = dest[v]; oldp[i] = from; }
         else { from = oldp[i]; to = where[v]; }
-        acc = (long long)row_conn(gpart + o, gconn + o, len, to) - row_conn(gpart + o, gconn + o, len, from);
+        acc = (long long)row_conn(gpart + o, gconn + o, len, to, k) - row_conn(gpart + o, gconn + o, len, from, k);
     }
     hp::block_add_to<256>(acc, d_c);
 }
 
+// Effect of one move on its neighbours' gain rows.  A vertex's own row does
+// not depend on its own part: only neighbours' rows change.  Dense neighbour
+// rows (deg >= k) take the change in place; a sparse neighbour is queued once
+// (atomicExch on its dirty flag) on the small or big rebuild list.
+__device__ __forceinline__ void touch_neighbour(int32_t u, int32_t w, int32_t p, int32_t d,
+                                                const int32_t *__restrict__ xadj,
+                                                const int32_t *__restrict__ goff,
+                                                int32_t *__restrict__ gconn, int32_t *__restrict__ dirty,
+                                                int32_t *__restrict__ small_l, int32_t *__restrict__ big_l,
+                                                int32_t *counts, int32_t k)
+{
+    const int32_t o = goff[u];
+    if (goff[u + 1] - o == k) {
+        atomicAdd(&gconn[o + p], -w);
+        atomicAdd(&gconn[o + d], w);
+    } else if (atomicExch(&dirty[u], 1) == 0) {
+        if (xadj[u + 1] - xadj[u] > BIGD) big_l[atomicAdd(&counts[1], 1)] = u;
+        else small_l[atomicAdd(&counts[0], 1)] = u;
+    }
+}
+
 __global__ void __launch_bounds__(256)
 apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
-                   int32_t *__restrict__ where, const int32_t *__restrict__ dest,
+                   const int32_t *__restrict__ where, const int32_t *__restrict__ dest,
                    const int32_t *__restrict__ vwgt, unsigned long long *__restrict__ pw,
                    const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
-                   int32_t *__restrict__ dirty)
+                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
+                   int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
+                   int32_t *__restrict__ big_l, int32_t *counts, int32_t k)
 {
     const int64_t nm = (int64_t)*d_nmoves;
     const int lane = threadIdx.x & 31;
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nm;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = moves[i];
+        const int32_t p = where[v], d = dest[v];
         if (lane == 0) {
-            const int32_t p = where[v], d = dest[v];
             const unsigned long long w = (unsigned long long)vwgt[v];
             atomicAdd(&pw[d], w);
             atomicAdd(&pw[p], (unsigned long long)(-(long long)w));
-            dirty[v] = 1;
         }
-        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32) dirty[adjncy[j]] = 1;
+        if (xadj[v + 1] - xadj[v] > HUGED) continue;   // CTA kernel below
+        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32)
+            touch_neighbour(adjncy[j], adjwgt[j], p, d, xadj, goff, gconn, dirty, small_l, big_l, counts, k);
+    }
+}
+
+__global__ void __launch_bounds__(512)
+apply_moves_huge_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
+                        const int32_t *__restrict__ where, const int32_t *__restrict__ dest,
+                        const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                        const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
+                        int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
+                        int32_t *__restrict__ big_l, int32_t *counts, int32_t k)
+{
+    const int64_t nm = (int64_t)*d_nmoves;
+    for (int64_t i = blockIdx.x; i < nm; i += gridDim.x) {
+        const int32_t v = moves[i];
+        if (xadj[v + 1] - xadj[v] <= HUGED) continue;
+        const int32_t p = where[v], d = dest[v];
+        for (int32_t j = xadj[v] + threadIdx.x; j < xadj[v + 1]; j += blockDim.x)
+            touch_neighbour(adjncy[j], adjwgt[j], p, d, xadj, goff, gconn, dirty, small_l, big_l, counts, k);
     }
 }
 
@@ -327,17 +427,6 @@ commit_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long 
     const int64_t nm = (int64_t)*d_nmoves;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < nm) { int32_t v = moves[i]; where[v] = dest[v]; }
-}
-
-__global__ void __launch_bounds__(256)
-classify_dirty_kernel(int32_t n, int32_t *__restrict__ dirty, const int32_t *__restrict__ xadj,
-                      int32_t *__restrict__ small, int32_t *__restrict__ bigl, int32_t *counts)
-{
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n || !dirty[v]) return;
-    dirty[v] = 0;
-    if (xadj[v + 1] - xadj[v] > BIGD) bigl[atomicAdd(&counts[1], 1)] = v;
-    else small[atomicAdd(&counts[0], 1)] = v;
 }
 
 // ---- rebalancing ------------------------------------------------------------------
@@ -407,7 +496,7 @@ rs_key_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__res
               const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
               const int64_t *__restrict__ opt, const int32_t *__restrict__ goff,
               const int32_t *__restrict__ gpart, const int32_t *__restrict__ gconn,
-              int32_t *__restrict__ key, int32_t *__restrict__ flag, int32_t *__restrict__ dest)
+              int32_t *__restrict__ key, int32_t *__restrict__ flag, int32_t *__restrict__ dest, int32_t k)
 {
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
@@ -416,7 +505,7 @@ rs_key_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__res
     const int64_t pwp = (int64_t)pw[p];
     if (pwp > maxp[p] && (int64_t)vwgt[v] < 2 * (pwp - opt[p])) {
         int32_t o = goff[v];
-        int32_t pc = row_conn(gpart + o, gconn + o, goff[v + 1] - o, p);
+        int32_t pc = row_conn(gpart + o, gconn + o, goff[v + 1] - o, p, k);
         kk = p * 64 + hp::gain_bucket(-pc, vwgt[v]);
     }
     key[v] = kk;
@@ -593,14 +682,17 @@ enum { S_NMOVES = 0, S_C1 = 1, S_C2 = 2, S_EXCESS = 3, S_NCAND = 4, S_CUT2 = 5, 
        S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_PASS_END = 12, S_BIGCNT = 16 };
 
 int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_t *small_list,
-               const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt)
+               const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt,
+               bool any_big, int32_t *dirty)
 {
     const unsigned pg = (unsigned)(c->sm_count * 8);
     HP_LAUNCH(c, gain_warp_kernel, small_list ? pg : nblk((int64_t)g.n * 32), 256, 0, small_list,
-              d_small_cnt, g.n, g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn);
-    const size_t smem = sizeof(int32_t) * (size_t)k + sizeof(unsigned) * (size_t)((k + 31) / 32);
-    HP_LAUNCH(c, gain_dense_kernel<256>, (unsigned)(c->sm_count * 2), 256, smem, big_list, d_big_cnt,
-              g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k);
+              d_small_cnt, g.n, g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
+    if (any_big) {
+        const size_t smem = sizeof(int32_t) * (size_t)k + sizeof(unsigned) * (size_t)((k + 31) / 32);
+        HP_LAUNCH(c, gain_dense_kernel<256>, (unsigned)(c->sm_count * 2), 256, smem, big_list, d_big_cnt,
+                  g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
+    }
     return HP_OK;
 }
 
@@ -654,7 +746,7 @@ int strong_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
     const int32_t n = g.n;
     unsigned long long *sc = c->d_scal;
     HP_LAUNCH(c, rs_key_kernel, nblk(n), 256, 0, n, g.where, g.vwgt, B.pw, B.maxp, B.opt, B.goff,
-              B.gpart, B.gconn, B.key, B.flag, B.dest);
+              B.gpart, B.gconn, B.key, B.flag, B.dest, k);
     int32_t *Ks, *Vs;
     HP_TRY(sort_candidates(c, g, B, k, &Ks, &Vs));
     const unsigned pg = (unsigned)(c->sm_count * 8);
@@ -701,8 +793,12 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.gpart = ralloc_t<int32_t>(c, G);
     B.gconn = ralloc_t<int32_t>(c, G);
     HP_CHECK_OOM(c);
+    // the level's counts of rows longer than 32 / 4096 (lets empty classes skip their launches)
+    int32_t nbig = 0;
+    HP_TRY(hp_read_scalars(c, d_bigcnt, sizeof(int32_t), &nbig));
+    const bool any_big = nbig > 0;
     int tok = hp_prof_begin(c);
-    HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt));
+    HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt, any_big, nullptr));
     // xadj, adjncy, adjwgt, where (own), goff, gain rows out
     hp_prof_end(c, tok, HP_PROF_GAIN, 4 * ((int64_t)n + 1) + 8 * g.m + 4 * (int64_t)n + 4 * ((int64_t)n + 1) + 8 * (int64_t)G);
     HP_CUDA(cudaMemsetAsync(B.pw, 0, sizeof(unsigned long long) * (size_t)k, c->stream));
@@ -724,6 +820,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     const int patience = c->opt.refine_patience;
     const unsigned pg = (unsigned)(c->sm_count * 8);
     int count = 0, bal = 0, passes = 0;
+    bool lp_idle = false;   // previous pass was an LP pass without moves (locks now clear)
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     while (count++ <= patience) {
         passes++;
@@ -735,8 +832,13 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
                       finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND]);
             HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where,
                       B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
-            HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
-                      g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
+            if (any_big) {
+                HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
+                          g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
+                HP_LAUNCH(c, afterburner_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.big, d_bigcnt,
+                          g.xadj, g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND],
+                          B.moves, &sc[S_NMOVES]);
+            }
             // select: goff, rows, where, lock in; dest, pregain out.  afterburner:
             // xadj, adjncy, adjwgt, own pregain/dest/where in, lock out
             hp_prof_end(c, ltok, HP_PROF_LP,
@@ -752,20 +854,23 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         // apply the move set simultaneously; exact cut change from the gain rows
         const unsigned mg = nblk(n);
         HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where,
-                  B.dest, B.oldp, 1, &sc[S_C1]);
+                  B.dest, B.oldp, 1, &sc[S_C1], k);
         HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw,
-                  g.xadj, g.adjncy, B.dirty);
+                  g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l,
+                  (int32_t *)&sc[S_DIRTY], k);
+        if (any_big)
+            HP_LAUNCH(c, apply_moves_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.moves, &sc[S_NMOVES],
+                      g.where, B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l,
+                      (int32_t *)&sc[S_DIRTY], k);
         HP_LAUNCH(c, commit_moves_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest);
         const int rtok = hp_prof_begin(c);
-        HP_LAUNCH(c, classify_dirty_kernel, nblk(n), 256, 0, n, B.dirty, g.xadj, B.small_l, B.big_l,
-                  (int32_t *)&sc[S_DIRTY]);
         HP_TRY(build_rows(c, g, B, k, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
-                          ((const int32_t *)&sc[S_DIRTY]) + 1));
+                          ((const int32_t *)&sc[S_DIRTY]) + 1, any_big, B.dirty));
         hp_prof_end(c, rtok, HP_PROF_REBUILD, 0);
         HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where,
-                  B.dest, B.oldp, 0, &sc[S_C2]);
+                  B.dest, B.oldp, 0, &sc[S_C2], k);
         HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);
-        HP_TRY(hp_read_scalars(c, sc, sizeof(long long) * 4, st));
+        HP_TRY(hp_read_scalars(c, sc, sizeof(long long) * 5, st));
         const int64_t c1 = st[S_C1], c2 = st[S_C2];
         excess = st[S_EXCESS];
         cut -= (c1 + c2) / 2;
@@ -773,6 +878,12 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
             fprintf(stderr, "gpu pass n=%d pass=%d mode=%d moves=%lld cut=%lld excess=%lld\n", n, passes,
                     mode, st[S_NMOVES], (long long)cut, (long long)excess);
 
+        // A pass that changed nothing (no moves, no lock change) is repeated
+        // identically by every later pass and can never improve the best
+        // partition: stop now; the result is the same as running on.
+        const bool stalled = st[S_NMOVES] == 0 &&
+                             ((mode == 2) || (mode == 0 && (st[S_NCAND] == 0 || lp_idle)));
+        lp_idle = (mode == 0 && st[S_NMOVES] == 0);
         bool take = false;
         if (best_excess > 0 && excess < best_excess) {
             take = true;
@@ -790,6 +901,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         } else {
             best_current = false;
         }
+        if (stalled) break;
     }
     if (!best_current)
         HP_CUDA(cudaMemcpyAsync(g.where, B.best_where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));

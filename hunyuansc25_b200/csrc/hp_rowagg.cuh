@@ -57,6 +57,19 @@ __device__ __forceinline__ int warp_aggregate32(int32_t key, int32_t w, int32_t 
     return __popc(hm);
 }
 
+// Same aggregation written as a dense vector over keys [0, nkeys):
+// out_k[q] = q, out_w[q] = sum of the weights with key q (0 if none).
+__device__ __forceinline__ void warp_aggregate32_dense(int32_t key, int32_t w, int32_t nkeys,
+                                                       int32_t *out_k, int32_t *out_w)
+{
+    const int lane = threadIdx.x & 31;
+    for (int32_t q = lane; q < nkeys; q += 32) { out_k[q] = q; out_w[q] = 0; }
+    __syncwarp();
+    // duplicates of a key are summed with one atomic per entry (order-free)
+    if (key != KEY_NONE) atomicAdd(&out_w[key], w);
+    __syncwarp();
+}
+
 // CTA-wide shared-memory aggregation of len <= CAP entries staged in sk/sw
 // (entries beyond len must already be KEY_NONE up to the pow2 size P).
 template <int NT, int CAP>

@@ -8,6 +8,7 @@
 // time) until it meets an inclusive prefix.  Every wait is bounded
 // (HP_SPIN_LIMIT); on expiry the CTA sets HP_STATUS_SPIN_TIMEOUT and continues,
 // so a stalled predecessor can never hang the device.
+#include <cstring>
 #include <mutex>
 
 #include "hp_internal.cuh"
@@ -138,19 +139,32 @@ __global__ void scatter_flags_kernel(const int32_t *flags, const int32_t *pos, i
     if (blockIdx.x == 0 && threadIdx.x == 0) *d_count = pos[n];
 }
 
-// Warp per vertex; int64 block partial sums.
+// Edge-parallel over the adjacency array in tiles of 256 x 32 entries
+// (coalesced reads of adjncy/adjwgt); each thread finds the owner of its first
+// entry by binary search over xadj and walks forward 256 entries at a time.
+// int64 block partial sums of 2 x cut.
+constexpr int CUT_ITEMS = 32;
 __global__ void __launch_bounds__(256)
 edgecut_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                unsigned long long *cut2)
 {
-    const int lane = threadIdx.x & 31;
+    const int64_t m = xadj[n];
+    const int64_t tile = 256 * CUT_ITEMS;
     long long acc = 0;
-    for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < n;
-         v += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int32_t wv = where[v];
-        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32)
-            if (where[adjncy[j]] != wv) acc += adjwgt[j];
+    for (int64_t tb = blockIdx.x * tile; tb < m; tb += (int64_t)gridDim.x * tile) {
+        int64_t j = tb + threadIdx.x;
+        if (j >= m) continue;
+        int32_t lo = 0, hi = n - 1;
+        while (lo < hi) {
+            int32_t mid = (int32_t)(((int64_t)lo + hi + 1) / 2);
+            if (xadj[mid] <= j) lo = mid; else hi = mid - 1;
+        }
+        int32_t v = lo;
+        for (int k = 0; k < CUT_ITEMS && j < m; k++, j += 256) {
+            while (xadj[v + 1] <= j) v++;
+            if (where[adjncy[j]] != where[v]) acc += adjwgt[j];
+        }
     }
     hp::block_add_to<256>(acc, cut2);
 }
@@ -269,8 +283,12 @@ int hp_edgecut_launch(hp_context *c, int32_t n, const int32_t *xadj, const int32
                       const int32_t *adjwgt, const int32_t *where, unsigned long long *d_cut2)
 {
     if (n <= 0) return HP_OK;
-    HP_LAUNCH(c, edgecut_kernel, grid_for(c, (int64_t)n * 32, 256), 256, 0, n, xadj, adjncy,
-              adjwgt, where, d_cut2);
+    int32_t m = 0;
+    HP_CUDA(cudaMemcpyAsync(c->h_pin, xadj + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    HP_CUDA(cudaStreamSynchronize(c->stream));
+    memcpy(&m, c->h_pin, sizeof(int32_t));
+    HP_LAUNCH(c, edgecut_kernel, grid_for(c, ((int64_t)m + CUT_ITEMS - 1) / CUT_ITEMS, 256), 256, 0, n, xadj,
+              adjncy, adjwgt, where, d_cut2);
     return HP_OK;
 }
 

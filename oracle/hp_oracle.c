@@ -752,8 +752,9 @@ typedef struct {
     int32_t **parts_t;
 } rstate;
 
-/* Label-propagation move set with afterburner (jetlp). Returns #moves. */
-static int32_t lp_moves(rstate *s, int32_t finest)
+/* Label-propagation move set with afterburner (jetlp). Returns #moves;
+ * *ncand_out = number of candidates before the afterburner. */
+static int32_t lp_moves(rstate *s, int32_t finest, int32_t *ncand_out)
 {
     const int32_t n = s->n;
     int32_t ncand = 0;
@@ -785,6 +786,7 @@ static int32_t lp_moves(rstate *s, int32_t finest)
             ncand++;
         }
     }
+    *ncand_out = ncand;
     if (ncand == 0) return 0;
     int32_t nm = 0;
     int8_t *sel = (int8_t *)xmalloc((size_t)n);
@@ -987,14 +989,15 @@ int64_t ora_refine(int32_t n, const int32_t *xadj, const int32_t *adjncy,
     memcpy(best, where, sizeof(int32_t) * (size_t)n);
     int64_t best_cut = cut, best_excess = excess;
     int32_t count = 0, bal_counter = 0, passes = 0;
+    int lp_idle = 0;
     const int dbg = getenv("HP_DEBUG_PASSES") != NULL;
 
     while (count++ <= patience) {
         passes++;
-        int32_t nm;
+        int32_t nm, ncand = -1;
         int mode;
         if (excess <= 0) {
-            nm = lp_moves(&s, finest);
+            nm = lp_moves(&s, finest, &ncand);
             bal_counter = 0;
             mode = 0;
         } else if (bal_counter < 2) {
@@ -1032,6 +1035,10 @@ int64_t ora_refine(int32_t n, const int32_t *xadj, const int32_t *adjncy,
             best_excess = excess; best_cut = cut;
             memcpy(best, where, sizeof(int32_t) * (size_t)n);
         }
+        /* A pass that changed nothing repeats identically: stop (same result). */
+        int stalled = nm == 0 && (mode == 2 || (mode == 0 && (ncand == 0 || lp_idle)));
+        lp_idle = (mode == 0 && nm == 0);
+        if (stalled) break;
     }
     memcpy(where, best, sizeof(int32_t) * (size_t)n);
     for (int t = 0; t < nt; t++) { free(s.conn_t[t]); free(s.parts_t[t]); }
