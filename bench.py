@@ -228,6 +228,11 @@ def main():
     ap.add_argument("--workload", default="grid3d", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--learned", action="store_true",
+                    help="time the learned move proposals (MLP) instead of the plain refiner")
+    ap.add_argument("--compare-learned", action="store_true",
+                    help="also time the learned refiner and report learned vs plain")
+    ap.add_argument("--learned-threshold", type=float, default=None)
     ap.add_argument("--kernel-only", action="store_true",
                     help="skip the e2e and CPU-baseline legs (profiling runs)")
     args = ap.parse_args()
@@ -257,7 +262,11 @@ def main():
         dist.init_process_group("nccl", device_id=dev, timeout=timedelta(seconds=300))
 
     ctx = hp.Context(local)
-    opt = default_options(coarsen_to=spec["coarsen_to"], profile=1)
+    from hunyuansc25_b200 import learn
+    if args.learned or args.compare_learned:
+        mparams, mthr, _ = learn.load_params()
+        ctx.mlp_set_params(mparams, mthr if args.learned_threshold is None else args.learned_threshold)
+    opt = default_options(coarsen_to=spec["coarsen_to"], profile=1, learned=1 if args.learned else 0)
     xadj, adj, vw, ew = (torch.from_numpy(a).to(dev) for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt))
     part = torch.empty(g.nvtxs, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
@@ -329,6 +338,28 @@ def main():
     }
     last = stats[-1]
 
+    learned_cmp = None
+    if args.compare_learned:
+        lopt = default_options(coarsen_to=spec["coarsen_to"], learned=1)
+        lms, lcut = [], None
+        for i in range(args.warmup + args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, lcut = ctx.partition_device(xadj, adj, spec["k"], vw, ew, spec["ub"], options=lopt, stream=stream,
+                                           part=part)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                lms.append(e0.elapsed_time(e1))
+        plain_ms = job_ms / args.steps
+        learned_ms = sum(lms) / len(lms)
+        learned_cmp = {"plain_ms": round(plain_ms, 3), "learned_ms": round(learned_ms, 3),
+                       "speedup": round(plain_ms / learned_ms, 4), "plain_cut": int(cut), "learned_cut": int(lcut),
+                       "cut_ratio": round(int(lcut) / max(1, int(cut)), 5),
+                       "learned_balanced": ctx.stats().max_excess <= 0}
+
     # end-to-end through the host-buffer entry point with pinned inputs
     pin = [torch.from_numpy(a).pin_memory() for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt)]
     hn = [p.numpy() for p in pin]
@@ -370,7 +401,10 @@ def main():
                         "phase_ms": {"coarsen": round(last.ms_coarsen, 3), "init": round(last.ms_init, 3),
                                      "uncoarsen": round(last.ms_uncoarsen, 3)}},
             "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
+            "refiner": "learned" if args.learned else "plain",
         }
+        if learned_cmp:
+            line["learned_vs_plain"] = learned_cmp
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:

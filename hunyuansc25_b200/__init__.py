@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-from ._abi import (ERROR_NAMES, HP_OK, HP_TRACE_ADJNCY, HP_TRACE_ADJWGT, HP_TRACE_CMAP,
+from ._abi import (ERROR_NAMES, HP_MLP_NPARAM, HP_OK, HP_TRACE_ADJNCY, HP_TRACE_ADJWGT, HP_TRACE_CMAP,
                    HP_TRACE_MATCH, HP_TRACE_VWGT, HP_TRACE_WHERE_FINAL, HP_TRACE_WHERE_START,
                    HP_TRACE_XADJ, PROTOTYPES, HpOptions, HpStats, default_options)
 
@@ -196,6 +196,58 @@ class Context:
         if rc != HP_OK:
             return None
         return out[:size]
+
+    # ---- learned move proposals -------------------------------------------------------
+    def mlp_set_params(self, params, threshold: float = 0.0):
+        params = np.ascontiguousarray(params, dtype=np.float32)
+        _check(self.lib.hp_mlp_set_params(self.h, params.ctypes.data_as(C.POINTER(C.c_float)), params.shape[0],
+                                          C.c_float(threshold)), "hp_mlp_set_params")
+
+    def mlp_get_params(self):
+        out = np.empty(HP_MLP_NPARAM, np.float32)
+        _check(self.lib.hp_mlp_get_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), HP_MLP_NPARAM),
+               "hp_mlp_get_params")
+        return out
+
+    def mlp_loss_grad(self, x, y):
+        """x: CUDA float32 [n, 8], y: CUDA float32 [n] -> (loss, grad numpy)."""
+        g = np.empty(HP_MLP_NPARAM, np.float32)
+        loss = C.c_float()
+        _check(self.lib.hp_mlp_loss_grad(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()), y.numel(),
+                                         g.ctypes.data_as(C.POINTER(C.c_float)), C.byref(loss)),
+               "hp_mlp_loss_grad")
+        return loss.value, g
+
+    def mlp_train(self, x, y, perm=None, epochs=1, batch=4096, lr=3e-3):
+        loss = C.c_float()
+        _check(self.lib.hp_mlp_train(self.h, C.c_void_p(x.data_ptr()), C.c_void_p(y.data_ptr()),
+                                     C.c_void_p(perm.data_ptr()) if perm is not None else None, y.numel(),
+                                     epochs, batch, C.c_float(lr), C.byref(loss)), "hp_mlp_train")
+        return loss.value
+
+    def mlp_infer(self, x, tensor_cores=True):
+        import torch
+        out = torch.empty(x.shape[0], dtype=torch.float32, device=x.device)
+        _check(self.lib.hp_mlp_infer(self.h, C.c_void_p(x.data_ptr()), x.shape[0], C.c_void_p(out.data_ptr()),
+                                     1 if tensor_cores else 0), "hp_mlp_infer")
+        return out
+
+    def movelog_enable(self, capacity: int):
+        _check(self.lib.hp_movelog_enable(self.h, capacity), "hp_movelog_enable")
+
+    def movelog_count(self) -> int:
+        return int(self.lib.hp_movelog_count(self.h))
+
+    def movelog_fetch(self):
+        n = self.movelog_count()
+        x = np.empty((max(n, 1), 8), np.float32)
+        y = np.empty(max(n, 1), np.float32)
+        _check(self.lib.hp_movelog_copy(self.h, x.ctypes.data_as(C.POINTER(C.c_float)),
+                                        y.ctypes.data_as(C.POINTER(C.c_float)), n), "hp_movelog_copy")
+        return x[:n], y[:n]
+
+    def movelog_reset(self):
+        _check(self.lib.hp_movelog_reset(self.h), "hp_movelog_reset")
 
     # ---- primitives -------------------------------------------------------------------
     def scan_exclusive(self, d_in, d_out=None, stream=None):

@@ -15,6 +15,7 @@ HP_ERR_INTERNAL = -8
 HP_MAX_PARTS = 16384
 HP_OPTIONS_VERSION = 1
 HP_SCAN_NOALLOC_MAX_N = 1 << 26
+HP_MLP_NPARAM = 1377
 
 HP_TRACE_XADJ = 0
 HP_TRACE_ADJNCY = 1
@@ -134,6 +135,16 @@ PROTOTYPES = {
     "hp_trace_copy": (C.c_int, [C.c_void_p, C.c_int, C.c_int, I32P, C.c_int64]),
     "hp_partition_batch": (C.c_int, [C.c_void_p, C.c_int32, I64P, I64P, I32P, I32P, I32P, I32P,
                                      I32P, F32P, C.POINTER(HpOptions), I32P, I64P]),
+    "hp_mlp_set_params": (C.c_int, [C.c_void_p, F32P, C.c_int32, C.c_float]),
+    "hp_mlp_get_params": (C.c_int, [C.c_void_p, F32P, C.c_int32]),
+    "hp_mlp_loss_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, F32P, F32P]),
+    "hp_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32,
+                               C.c_int32, C.c_float, F32P]),
+    "hp_mlp_infer": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_int32]),
+    "hp_movelog_enable": (C.c_int, [C.c_void_p, C.c_int64]),
+    "hp_movelog_count": (C.c_int64, [C.c_void_p]),
+    "hp_movelog_copy": (C.c_int, [C.c_void_p, F32P, F32P, C.c_int64]),
+    "hp_movelog_reset": (C.c_int, [C.c_void_p]),
     "hp_scan_exclusive_i32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                         C.c_void_p]),
     "hp_scan_exclusive_i32_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),

@@ -33,6 +33,7 @@ CU_SOURCES = [
     "hp_coarsen.cu",
     "hp_initpart.cu",
     "hp_refine.cu",
+    "hp_mlp.cu",
 ]
 
 

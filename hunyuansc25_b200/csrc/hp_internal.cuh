@@ -46,6 +46,17 @@ struct hp_context {
     int prof_next = 0;
 
     hp_stats stats = {};
+
+    // move-scoring MLP (hp_mlp.cu): params, gradient, Adam moments
+    float *mlp_params = nullptr, *mlp_grad = nullptr, *mlp_m = nullptr, *mlp_v = nullptr;
+    float mlp_threshold = 0.0f;
+    bool mlp_ready = false;
+    // move log recorded by the plain refiner (opt.learned = 2)
+    float *log_x = nullptr, *log_y = nullptr;
+    int32_t *log_v = nullptr, *log_d = nullptr, *log_acc = nullptr;
+    unsigned long long *log_count = nullptr;
+    int64_t log_cap = 0;
+
     std::vector<hp_context *> workers;   // batch worker contexts (own streams and arenas)
     std::vector<HpLevel> levels;
     bool trace_valid = false;
@@ -136,6 +147,7 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
 int hp_refine_init();
 int hp_initpart_init();
 int hp_coarsen_init();
+int hp_mlp_ensure(hp_context *c);
 
 // ---- targets shared with the host driver -----------------------------------------
 void hp_part_targets(int64_t tvwgt, int32_t nparts, const float *tpwgts, float ubfactor,

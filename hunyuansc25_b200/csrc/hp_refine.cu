@@ -18,6 +18,7 @@
 #include <cstdlib>
 
 #include "hp_internal.cuh"
+#include "hp_mlp.cuh"
 #include "hp_rowagg.cuh"
 
 namespace {
@@ -223,6 +224,113 @@ lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__r
         dest[v] = d;
     }
     hp::block_add_to<256>(cand, d_ncand);
+}
+
+// Learned LP selection: the plain rule first, then the MLP scores every
+// candidate (all lanes of a warp run the tensor-core inference together) and
+// drops candidates scoring below the threshold.  Dropped candidates simply
+// stay; nothing the network says bypasses the exact afterburner.
+__global__ void __launch_bounds__(256)
+lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
+                         const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
+                         const int32_t *__restrict__ xadj, const int8_t *__restrict__ lock, int finest,
+                         const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
+                         const int64_t *__restrict__ opt, const float *__restrict__ params, float threshold,
+                         int32_t *__restrict__ dest, int32_t *__restrict__ pregain, unsigned long long *d_ncand)
+{
+    __shared__ hp::MlpSmem sm;
+    hp::mlp_load_smem(sm, params);
+    __syncthreads();
+    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    int cand = 0;
+    float f[HP_MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int32_t g = NEG, d = 0;
+    if (v < n) {
+        const int32_t p = where[v];
+        int64_t pc = 0, bc = 0, wd = 0;
+        int32_t b = -1, np = 0;
+        for (int32_t j = goff[v]; j < goff[v + 1]; j++) {
+            int32_t q = gpart[j];
+            if (q < 0) break;
+            int32_t cq = gconn[j];
+            wd += cq;
+            np += cq > 0;
+            if (q == p) { pc = cq; continue; }
+            if (cq > bc) { bc = cq; b = q; }
+        }
+        d = p;
+        if (b >= 0) {
+            int64_t thr = finest ? pc / 4 : (3 * pc) / 4;
+            if ((bc >= pc || (pc - bc) < thr) && !lock[v]) {
+                g = (int32_t)(bc - pc);
+                d = b;
+                cand = 1;
+                hp::mlp_features(pc, bc, wd, np, xadj[v + 1] - xadj[v], maxp[b] - (int64_t)pw[b], opt[b],
+                                 maxp[p] - (int64_t)pw[p], opt[p], finest, f);
+            }
+        }
+    }
+    const float logit = hp::mlp_warp_logit(sm, f);
+    if (cand && logit < threshold) { cand = 0; g = NEG; d = where[v]; }
+    if (v < n) { pregain[v] = g; dest[v] = d; }
+    hp::block_add_to<256>(cand, d_ncand);
+}
+
+// Move log (record mode): features of every LP candidate, its vertex and
+// destination; rec_of[v] links the vertex to its record for the afterburner.
+__global__ void __launch_bounds__(256)
+log_candidates_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
+                      const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
+                      const int32_t *__restrict__ xadj, int finest, const unsigned long long *__restrict__ pw,
+                      const int64_t *__restrict__ maxp, const int64_t *__restrict__ opt,
+                      const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
+                      int32_t *__restrict__ rec_of, float *__restrict__ lx, int32_t *__restrict__ lv,
+                      int32_t *__restrict__ ld, int32_t *__restrict__ lacc, unsigned long long *lcount, int64_t cap)
+{
+    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= n) return;
+    rec_of[v] = -1;
+    if (pregain[v] == NEG) return;
+    const int32_t p = where[v], b = dest[v];
+    int64_t pc = 0, bc = 0, wd = 0;
+    int32_t np = 0;
+    for (int32_t j = goff[v]; j < goff[v + 1]; j++) {
+        int32_t q = gpart[j];
+        if (q < 0) break;
+        int32_t cq = gconn[j];
+        wd += cq;
+        np += cq > 0;
+        if (q == p) pc = cq;
+        if (q == b) bc = cq;
+    }
+    const unsigned long long r = atomicAdd(lcount, 1ull);
+    if ((int64_t)r >= cap) return;
+    float f[HP_MLP_IN];
+    hp::mlp_features(pc, bc, wd, np, xadj[v + 1] - xadj[v], maxp[b] - (int64_t)pw[b], opt[b],
+                     maxp[p] - (int64_t)pw[p], opt[p], finest, f);
+    for (int i = 0; i < HP_MLP_IN; i++) lx[r * HP_MLP_IN + i] = f[i];
+    lv[r] = v;
+    ld[r] = b;
+    lacc[r] = 0;
+    rec_of[v] = (int32_t)r;
+}
+
+__global__ void log_accept_kernel(int32_t n, const int32_t *__restrict__ rec_of, const int8_t *__restrict__ lock,
+                                  const unsigned long long *d_ncand, int32_t *__restrict__ lacc)
+{
+    if (*d_ncand == 0ull) return;
+    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n && rec_of[v] >= 0) lacc[rec_of[v]] = lock[v];
+}
+
+// Label of a record once its level is final: the afterburner accepted the
+// move and the vertex ends the level in that destination.
+__global__ void log_label_kernel(int64_t r0, int64_t r1, const int32_t *__restrict__ where,
+                                 const int32_t *__restrict__ lv, const int32_t *__restrict__ ld,
+                                 const int32_t *__restrict__ lacc, float *__restrict__ ly)
+{
+    int64_t r = r0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (r < r1) ly[r] = (lacc[r] && where[lv[r]] == ld[r]) ? 1.f : 0.f;
 }
 
 __device__ __forceinline__ long long ab_change(int32_t v, int32_t g, int32_t p, int32_t b,
@@ -821,15 +929,36 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     const unsigned pg = (unsigned)(c->sm_count * 8);
     int count = 0, bal = 0, passes = 0;
     bool lp_idle = false;   // previous pass was an LP pass without moves (locks now clear)
+    // learned LP proposals (opt.learned = 1) until a learned pass fails to
+    // improve the exact cut; then the plain rule for the rest of the level
+    bool learned_active = c->opt.learned == 1 && c->mlp_ready;
+    const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
+    int64_t log_r0 = 0;
+    if (recording) {
+        unsigned long long lc = 0;
+        HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
+        log_r0 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
+    }
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     while (count++ <= patience) {
         passes++;
         HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * S_PASS_END, c->stream));
         const int mode = excess <= 0 ? 0 : (bal < 2 ? 1 : 2);
+        const bool learned_pass = excess <= 0 && learned_active;
+        const int64_t cut_before = cut;
         if (excess <= 0) {
             const int ltok = hp_prof_begin(c);
-            HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
-                      finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND]);
+            if (learned_pass)
+                HP_LAUNCH(c, lp_select_learned_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where,
+                          g.xadj, B.lock, finest ? 1 : 0, B.pw, B.maxp, B.opt, c->mlp_params, c->mlp_threshold,
+                          B.dest, B.pregain, &sc[S_NCAND]);
+            else
+                HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
+                          finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND]);
+            if (recording)
+                HP_LAUNCH(c, log_candidates_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where,
+                          g.xadj, finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.oldp, c->log_x,
+                          c->log_v, c->log_d, c->log_acc, c->log_count, c->log_cap);
             HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where,
                       B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
             if (any_big) {
@@ -839,6 +968,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
                           g.xadj, g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND],
                           B.moves, &sc[S_NMOVES]);
             }
+            if (recording)
+                HP_LAUNCH(c, log_accept_kernel, nblk(n), 256, 0, n, B.oldp, B.lock, &sc[S_NCAND], c->log_acc);
             // select: goff, rows, where, lock in; dest, pregain out.  afterburner:
             // xadj, adjncy, adjwgt, own pregain/dest/where in, lock out
             hp_prof_end(c, ltok, HP_PROF_LP,
@@ -874,6 +1005,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         const int64_t c1 = st[S_C1], c2 = st[S_C2];
         excess = st[S_EXCESS];
         cut -= (c1 + c2) / 2;
+        if (learned_pass && cut >= cut_before) learned_active = false;
         if (dbg)
             fprintf(stderr, "gpu pass n=%d pass=%d mode=%d moves=%lld cut=%lld excess=%lld\n", n, passes,
                     mode, st[S_NMOVES], (long long)cut, (long long)excess);
@@ -905,6 +1037,14 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     }
     if (!best_current)
         HP_CUDA(cudaMemcpyAsync(g.where, B.best_where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
+    if (recording) {
+        unsigned long long lc = 0;
+        HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
+        const int64_t r1 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
+        if (r1 > log_r0)
+            HP_LAUNCH(c, log_label_kernel, nblk(r1 - log_r0), 256, 0, log_r0, r1, g.where, c->log_v, c->log_d,
+                      c->log_acc, c->log_y);
+    }
     *cut_final = best_cut;
     *passes_out = passes;
     HP_TRY(hp_check_status(c));

@@ -1,0 +1,144 @@
+"""Training of the move-scoring MLP on move logs of the plain refiner.
+
+  python -m hunyuansc25_b200.learn [--out hunyuansc25_b200/data/mlp_default.bin]
+
+1. The plain GPU refiner partitions seeded synthetic graphs (R-MAT, 3-D grids,
+   RGG; seeds disjoint from the benchmark workloads) with hp_options.learned = 2
+   and records every label-propagation candidate: eight integer-derived
+   features and a label (the exact afterburner accepted the move and the vertex
+   ends its level in the proposed part).
+2. The network is trained on the device by the library's own FP32 kernels
+   (forward, backward, Adam; hp_mlp_train), one shuffled pass per epoch.
+3. The pruning threshold keeps 95 % of the good moves of a held-out split.
+4. Parameters + threshold go to a small versioned blob with a SHA-256 checksum.
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import os
+import struct
+import sys
+
+import numpy as np
+
+from . import graphs
+from ._abi import HP_MLP_NPARAM, default_options
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_WEIGHTS = os.path.join(HERE, "data", "mlp_default.bin")
+MAGIC = b"HPMLP\x00\x01\x00"
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-initialised parameters (biases zero)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(HP_MLP_NPARAM, np.float32)
+    p[0:256] = rng.normal(0, np.sqrt(2 / 8), 256)                 # W1[32][8]
+    p[288:288 + 1024] = rng.normal(0, np.sqrt(2 / 32), 1024)       # W2[32][32]
+    p[1344:1376] = rng.normal(0, np.sqrt(1 / 32), 32)              # w3
+    return p
+
+
+def save_params(path: str, params: np.ndarray, threshold: float, meta: str = "") -> None:
+    params = np.ascontiguousarray(params, np.float32)
+    body = struct.pack("<if", params.shape[0], float(threshold)) + params.tobytes()
+    mb = meta.encode()[:255]
+    body += struct.pack("<B", len(mb)) + mb
+    digest = hashlib.sha256(body).digest()
+    with open(path, "wb") as f:
+        f.write(MAGIC + digest + body)
+
+
+def load_params(path: str = DEFAULT_WEIGHTS):
+    """Returns (params, threshold, meta); raises on a bad magic or checksum."""
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:8] != MAGIC:
+        raise ValueError(f"{path}: not an MLP weight blob")
+    digest, body = data[8:40], data[40:]
+    if hashlib.sha256(body).digest() != digest:
+        raise ValueError(f"{path}: checksum mismatch")
+    n, thr = struct.unpack("<if", body[:8])
+    if n != HP_MLP_NPARAM:
+        raise ValueError(f"{path}: {n} parameters, expected {HP_MLP_NPARAM}")
+    params = np.frombuffer(body[8:8 + 4 * n], np.float32).copy()
+    ml = body[8 + 4 * n]
+    meta = body[9 + 4 * n:9 + 4 * n + ml].decode()
+    return params, float(thr), meta
+
+
+def training_graphs():
+    """Seeded synthetic graphs for the move logs (seeds differ from the workloads)."""
+    out = []
+    for i, s in enumerate((14, 15, 16)):
+        out.append((graphs.rmat(s, 16, seed=100 + i, wmin=1, wmax=100), 256 if s >= 15 else 64, 1.03))
+    for i, side in enumerate((32, 48)):
+        out.append((graphs.grid3d(side, side, side, seed=200 + i, wmin=1, wmax=10), 64 if side > 32 else 16, 1.03))
+    out.append((graphs.rgg(1 << 16, 12.0, seed=300), 256, 1.05))
+    return out
+
+
+def collect(ctx, items, capacity=8_000_000):
+    ctx.movelog_enable(capacity)
+    opt = default_options(learned=2)
+    for g, k, ub in items:
+        ctx.partition_graph(g, k, ub, options=opt)
+    return ctx.movelog_fetch()
+
+
+def train(ctx, x, y, epochs=12, batch=4096, lr=3e-3, seed=0, params=None):
+    import torch
+    dev = torch.device("cuda", ctx.device)
+    ctx.mlp_set_params(init_params(seed) if params is None else params, 0.0)
+    xt = torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+    yt = torch.from_numpy(np.ascontiguousarray(y)).to(dev)
+    rng = np.random.default_rng(seed)
+    losses = []
+    for _ in range(epochs):
+        perm = torch.from_numpy(rng.permutation(x.shape[0]).astype(np.int32)).to(dev)
+        losses.append(ctx.mlp_train(xt, yt, perm, epochs=1, batch=batch, lr=lr))
+    return ctx.mlp_get_params(), losses
+
+
+def pick_threshold(ctx, x, y, keep=0.95):
+    """Largest threshold that still proposes `keep` of the good moves."""
+    import torch
+    xt = torch.from_numpy(np.ascontiguousarray(x)).to(torch.device("cuda", ctx.device))
+    logits = ctx.mlp_infer(xt, tensor_cores=True).cpu().numpy()
+    pos = np.sort(logits[y > 0.5])
+    if pos.size == 0:
+        return 0.0, logits
+    return float(pos[int((1.0 - keep) * pos.size)]), logits
+
+
+def main(argv=None):
+    import hunyuansc25_b200 as hp
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=DEFAULT_WEIGHTS)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args(argv)
+    ctx = hp.Context(0)
+    x, y = collect(ctx, training_graphs())
+    n = x.shape[0]
+    rng = np.random.default_rng(args.seed)
+    order = rng.permutation(n)
+    nval = max(1, n // 10)
+    val, tr = order[:nval], order[nval:]
+    params, losses = train(ctx, x[tr], y[tr], epochs=args.epochs, seed=args.seed)
+    thr, logits = pick_threshold(ctx, x[val], y[val])
+    yv = y[val]
+    kept = logits >= thr
+    stats = (f"samples={n} pos_rate={y.mean():.3f} loss0={losses[0]:.4f} loss={losses[-1]:.4f} "
+             f"threshold={thr:.3f} val_pruned={1 - kept.mean():.3f} "
+             f"val_bad_pruned={((~kept) & (yv < 0.5)).sum() / max(1, (yv < 0.5).sum()):.3f}")
+    print(stats)
+    os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
+    save_params(args.out, params, thr, stats)
+    print(args.out)
+    ctx.close()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

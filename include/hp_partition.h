@@ -58,7 +58,7 @@ typedef struct hp_options {
     int32_t  fm_passes;        /* 2-way FM passes per trial (default 10,
                                   hunyuangraph_admin.h:14)                                    */
     int32_t  max_levels;       /* coarsening level cap (default 64)                           */
-    int32_t  learned;          /* 0 plain refinement, 1 MLP move proposals                    */
+    int32_t  learned;          /* 0 plain refinement, 1 MLP move proposals, 2 record move log */
     int32_t  validate;         /* 0 none, 1 structural check on the device (default)          */
     int32_t  trace;            /* 1: keep every level for hp_trace_*() (tests)                */
     int32_t  profile;          /* 1: time kernel classes with CUDA events into hp_stats.prof_* */
@@ -157,6 +157,39 @@ int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *vtxdist,
                        const int32_t *adjwgt, const int32_t *nparts,
                        const float *ubfactor, const hp_options *opt,
                        int32_t *part, int64_t *edgecut);
+
+/* ---- learned move proposals --------------------------------------------------------
+ * No counterpart in the reference (its refinement has no learned component).
+ * An MLP 8 -> 32 -> 32 -> 1 scores each label-propagation candidate from eight
+ * integer-derived features (normalised gain, own/best connectivity fractions,
+ * adjacent-part count, log degree, target/own part slack, finest-level flag).
+ * With hp_options.learned = 1, candidates scoring below `threshold` are not
+ * proposed; the exact integer afterburner and balance rules still decide
+ * every move, and a level returns to the plain rule as soon as a learned pass
+ * fails to lower the exact cut.  Inference runs on BF16 tensor cores with FP32
+ * accumulation inside the LP kernel; training is FP32 (forward, backward,
+ * Adam) on the device.  Parameters are HP_MLP_NPARAM floats:
+ * W1[32][8], b1[32], W2[32][32], b2[32], w3[32], b3. */
+#define HP_MLP_NPARAM 1377
+int hp_mlp_set_params(hp_context *ctx, const float *params, int32_t count, float threshold);
+int hp_mlp_get_params(hp_context *ctx, float *params, int32_t count);
+/* Mean BCE-with-logits loss and its gradient over n samples (device arrays
+ * d_x[n][8], d_y[n] in {0,1}); grad and loss are host outputs. */
+int hp_mlp_loss_grad(hp_context *ctx, const float *d_x, const float *d_y, int64_t n, float *grad,
+                     float *loss);
+/* Mini-batch Adam on the device; d_perm (nullable) orders the samples. */
+int hp_mlp_train(hp_context *ctx, const float *d_x, const float *d_y, const int32_t *d_perm, int64_t n,
+                 int32_t epochs, int32_t batch, float lr, float *final_loss);
+/* Logits of n samples (device arrays); tensor_cores = 1 uses the BF16 MMA path
+ * of the LP kernel, 0 the FP32 path. */
+int hp_mlp_infer(hp_context *ctx, const float *d_x, int64_t n, float *d_out, int32_t tensor_cores);
+/* Move log of the plain refiner (hp_options.learned = 2): every LP candidate's
+ * features, labelled 1 when the afterburner accepted the move and the vertex
+ * ends its level in that part. */
+int     hp_movelog_enable(hp_context *ctx, int64_t capacity);
+int64_t hp_movelog_count(hp_context *ctx);
+int     hp_movelog_copy(hp_context *ctx, float *features, float *labels, int64_t count);
+int     hp_movelog_reset(hp_context *ctx);
 
 /* ---- device primitives (device pointers, issued on `stream`) ------------------- */
 /* Exclusive int32 prefix sum, single-pass decoupled look-back.  Writes n+1

@@ -72,6 +72,10 @@ def lib():
         L.ora_refine.argtypes = [C.c_int32, I32P, I32P, I32P, I32P, C.c_int32, I64P, I64P, C.c_int32,
                                  C.c_int32, I32P, I32P]
         L.ora_refine.restype = C.c_int64
+        F32 = C.POINTER(C.c_float)
+        L.ora_mlp_forward.argtypes = [F32, F32, C.c_int64, F32]
+        L.ora_mlp_loss_grad.argtypes = [F32, F32, F32, C.c_int64, F32]
+        L.ora_mlp_loss_grad.restype = C.c_float
         L.ora_gain_bucket.argtypes = [C.c_int32, C.c_int32]
         L.ora_gain_bucket.restype = C.c_int32
         _LIB = L
@@ -182,3 +186,23 @@ def part_targets(tvwgt, nparts, ubfactor, tpwgts=None):
 
 def gain_bucket(gain, vwgt):
     return int(lib().ora_gain_bucket(gain, vwgt))
+
+
+def mlp_forward(params, x):
+    params = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.empty(x.shape[0], np.float32)
+    F32 = C.POINTER(C.c_float)
+    lib().ora_mlp_forward(params.ctypes.data_as(F32), x.ctypes.data_as(F32), x.shape[0], out.ctypes.data_as(F32))
+    return out
+
+
+def mlp_loss_grad(params, x, y):
+    params = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(x, np.float32)
+    y = np.ascontiguousarray(y, np.float32)
+    g = np.empty(params.shape[0], np.float32)
+    F32 = C.POINTER(C.c_float)
+    loss = lib().ora_mlp_loss_grad(params.ctypes.data_as(F32), x.ctypes.data_as(F32), y.ctypes.data_as(F32),
+                                   x.shape[0], g.ctypes.data_as(F32))
+    return float(loss), g

@@ -1245,3 +1245,78 @@ int ora_partition(int32_t n, const int32_t *xadj, const int32_t *adjncy,
     }
     return HP_OK;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Move-scoring MLP, FP32 (the reference for the device forward/backward).   */
+/* Parameters: W1[32][8], b1[32], W2[32][32], b2[32], w3[32], b3.            */
+
+#define OMLP_IN 8
+#define OMLP_H 32
+#define OMLP_W1 0
+#define OMLP_B1 (OMLP_W1 + OMLP_H * OMLP_IN)
+#define OMLP_W2 (OMLP_B1 + OMLP_H)
+#define OMLP_B2 (OMLP_W2 + OMLP_H * OMLP_H)
+#define OMLP_W3 (OMLP_B2 + OMLP_H)
+#define OMLP_B3 (OMLP_W3 + OMLP_H)
+#define OMLP_N (OMLP_B3 + 1)
+
+static float omlp_fwd(const float *P, const float *x, float *z1, float *z2)
+{
+    float a1[OMLP_H];
+    for (int j = 0; j < OMLP_H; j++) {
+        float s = P[OMLP_B1 + j];
+        for (int i = 0; i < OMLP_IN; i++) s += P[OMLP_W1 + j * OMLP_IN + i] * x[i];
+        z1[j] = s;
+        a1[j] = s > 0.f ? s : 0.f;
+    }
+    float y = P[OMLP_B3];
+    for (int j = 0; j < OMLP_H; j++) {
+        float s = P[OMLP_B2 + j];
+        for (int i = 0; i < OMLP_H; i++) s += P[OMLP_W2 + j * OMLP_H + i] * a1[i];
+        z2[j] = s;
+        y += P[OMLP_W3 + j] * (s > 0.f ? s : 0.f);
+    }
+    return y;
+}
+
+void ora_mlp_forward(const float *P, const float *X, int64_t n, float *out)
+{
+    float z1[OMLP_H], z2[OMLP_H];
+    for (int64_t r = 0; r < n; r++) out[r] = omlp_fwd(P, X + r * OMLP_IN, z1, z2);
+}
+
+/* Mean binary cross-entropy with logits and its gradient (double accumulators). */
+float ora_mlp_loss_grad(const float *P, const float *X, const float *Y, int64_t n, float *grad)
+{
+    double g[OMLP_N];
+    memset(g, 0, sizeof(g));
+    double loss = 0.0;
+    for (int64_t r = 0; r < n; r++) {
+        const float *x = X + r * OMLP_IN;
+        float z1[OMLP_H], z2[OMLP_H];
+        const float y = omlp_fwd(P, x, z1, z2);
+        const float t = Y[r];
+        const double sp = y > 0 ? y + log1p(exp(-(double)y)) : log1p(exp((double)y));
+        loss += sp - (double)t * y;
+        const double dy = 1.0 / (1.0 + exp(-(double)y)) - t;
+        g[OMLP_B3] += dy;
+        double da1[OMLP_H];
+        memset(da1, 0, sizeof(da1));
+        for (int j = 0; j < OMLP_H; j++) {
+            g[OMLP_W3 + j] += dy * (z2[j] > 0.f ? z2[j] : 0.f);
+            const double dz2 = z2[j] > 0.f ? dy * P[OMLP_W3 + j] : 0.0;
+            g[OMLP_B2 + j] += dz2;
+            for (int i = 0; i < OMLP_H; i++) {
+                g[OMLP_W2 + j * OMLP_H + i] += dz2 * (z1[i] > 0.f ? z1[i] : 0.f);
+                da1[i] += dz2 * P[OMLP_W2 + j * OMLP_H + i];
+            }
+        }
+        for (int i = 0; i < OMLP_H; i++) {
+            const double dz1 = z1[i] > 0.f ? da1[i] : 0.0;
+            g[OMLP_B1 + i] += dz1;
+            for (int c = 0; c < OMLP_IN; c++) g[OMLP_W1 + i * OMLP_IN + c] += dz1 * x[c];
+        }
+    }
+    for (int i = 0; i < OMLP_N; i++) grad[i] = (float)(g[i] / (double)n);
+    return (float)(loss / (double)n);
+}

@@ -78,6 +78,10 @@ int64_t ora_refine(int32_t n, const int32_t *xadj, const int32_t *adjncy,
                    const int64_t *opt, const int64_t *maxp, int32_t finest,
                    int32_t patience, int32_t *where, int32_t *passes);
 
+/* Move-scoring MLP in FP32 (parameters as in hp_mlp_set_params). */
+void  ora_mlp_forward(const float *params, const float *x, int64_t n, float *out);
+float ora_mlp_loss_grad(const float *params, const float *x, const float *y, int64_t n, float *grad);
+
 /* Weak-rebalance gain bucket (float semantics of the reference). */
 int32_t ora_gain_bucket(int32_t gain, int32_t vwgt);
 

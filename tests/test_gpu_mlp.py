@@ -1,0 +1,95 @@
+"""Learned move proposals: device training kernels against the CPU oracle,
+tensor-core inference against FP32, the move log, and a learned partition
+that stays exact (cut recomputed, balance honoured) and deterministic."""
+import numpy as np
+import pytest
+
+import oracle
+from hunyuansc25_b200 import graphs, learn
+from hunyuansc25_b200._abi import HP_MLP_NPARAM, default_options
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(n, seed=0):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(0, 0.6, size=(n, 8)).astype(np.float32)
+    y = ((x[:, 0] + 0.5 * x[:, 5] - 0.3 * x[:, 1]) > 0).astype(np.float32)
+    return x, y
+
+
+def test_gradient_matches_oracle(ctx):
+    import torch
+    x, y = _data(5000, 1)
+    p = learn.init_params(3)
+    p[256:288] = 0.05   # nonzero biases exercise their gradients
+    ctx.mlp_set_params(p)
+    loss, g = ctx.mlp_loss_grad(torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda())
+    oloss, og = oracle.mlp_loss_grad(p, x, y)
+    # FP32 device sums (atomics, any order) vs double-accumulated CPU: rel-err <= 1e-3
+    assert abs(loss - oloss) <= 1e-3 * max(1.0, abs(oloss))
+    scale = np.abs(og).max()
+    assert np.max(np.abs(g - og)) <= 1e-3 * scale, (np.max(np.abs(g - og)), scale)
+
+
+def test_inference_tensor_cores_vs_fp32(ctx):
+    import torch
+    x, _ = _data(10007, 2)
+    p = learn.init_params(4)
+    ctx.mlp_set_params(p)
+    xt = torch.from_numpy(x).cuda()
+    ref = oracle.mlp_forward(p, x)
+    fp32 = ctx.mlp_infer(xt, tensor_cores=False).cpu().numpy()
+    bf16 = ctx.mlp_infer(xt, tensor_cores=True).cpu().numpy()
+    assert np.allclose(fp32, ref, rtol=1e-4, atol=1e-4)
+    # BF16 operands (8-bit mantissa), FP32 accumulation: |err| <= 0.03 + 0.03 |y|
+    err = np.abs(bf16 - ref)
+    assert np.all(err <= 0.03 + 0.03 * np.abs(ref)), err.max()
+    assert np.mean(np.sign(bf16) == np.sign(ref)) > 0.99
+
+
+def test_training_lowers_loss(ctx):
+    import torch
+    x, y = _data(40000, 5)
+    p0 = learn.init_params(7)
+    ctx.mlp_set_params(p0)
+    xt, yt = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    l0, _ = ctx.mlp_loss_grad(xt, yt)
+    params, losses = learn.train(ctx, x, y, epochs=8, batch=2048, lr=3e-3, seed=7, params=p0)
+    l1, _ = ctx.mlp_loss_grad(xt, yt)
+    assert l1 < 0.5 * l0
+    acc = np.mean((oracle.mlp_forward(params, x) > 0) == (y > 0.5))
+    assert acc > 0.95
+
+
+def test_move_log_does_not_change_the_partition(ctx):
+    g = graphs.rmat(13, 16, seed=11)
+    plain_part, plain_cut = ctx.partition_graph(g, 64)
+    ctx.movelog_enable(1 << 20)
+    part, cut = ctx.partition_graph(g, 64, options=default_options(learned=2))
+    assert cut == plain_cut and np.array_equal(part, plain_part)
+    x, y = ctx.movelog_fetch()
+    assert x.shape[0] > 100 and np.all(np.isfinite(x))
+    assert set(np.unique(y)).issubset({0.0, 1.0})
+    assert 0.0 < y.mean() < 1.0
+    ctx.movelog_enable(0)
+
+
+def test_learned_partition_exact_and_deterministic(ctx):
+    g = graphs.rmat(13, 16, seed=21)
+    ctx.movelog_enable(1 << 21)
+    ctx.partition_graph(graphs.rmat(12, 16, seed=22), 64, options=default_options(learned=2))
+    x, y = ctx.movelog_fetch()
+    ctx.movelog_enable(0)
+    params, _ = learn.train(ctx, x, y, epochs=4, batch=2048, seed=1)
+    thr, _ = learn.pick_threshold(ctx, x, y)
+    ctx.mlp_set_params(params, thr)
+    plain_part, plain_cut = ctx.partition_graph(g, 64)
+    lopt = default_options(learned=1)
+    a_part, a_cut = ctx.partition_graph(g, 64, options=lopt)
+    st = ctx.stats()
+    b_part, b_cut = ctx.partition_graph(g, 64, options=lopt)
+    assert a_cut == b_cut and np.array_equal(a_part, b_part)
+    assert a_cut == oracle.edgecut(g, a_part)           # exact int64 cut
+    assert st.max_excess <= 0                            # balance bound honoured exactly
+    assert a_cut <= 1.10 * plain_cut
