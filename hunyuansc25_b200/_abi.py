@@ -52,6 +52,7 @@ class HpOptions(C.Structure):
         ("validate", C.c_int32),
         ("trace", C.c_int32),
         ("profile", C.c_int32),
+        ("eager", C.c_int32),
         ("seed", C.c_uint64),
     ]
 
@@ -70,6 +71,7 @@ def default_options(**overrides) -> HpOptions:
     o.validate = 1
     o.trace = 0
     o.profile = 0
+    o.eager = 0
     o.seed = 1
     for k, v in overrides.items():
         setattr(o, k, v)

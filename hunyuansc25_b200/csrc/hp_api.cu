@@ -275,7 +275,7 @@ static int prof_event(hp_context *c)
 
 int hp_prof_begin(hp_context *c)
 {
-    if (!c->opt.profile) return -1;
+    if (!c->opt.profile || c->prof_suspended) return -1;
     int e0 = prof_event(c);
     if (e0 < 0) return -1;
     cudaEventRecord(c->prof_events[e0], c->stream);
@@ -371,6 +371,7 @@ HP_API void hp_options_default(hp_options *o)
     o->validate = 1;
     o->trace = 0;
     o->profile = 0;
+    o->eager = 0;
     o->seed = 1;
 }
 

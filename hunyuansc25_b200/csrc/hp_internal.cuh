@@ -44,6 +44,7 @@ struct hp_context {
     std::vector<cudaEvent_t> prof_events;
     std::vector<ProfRec> prof_recs;
     int prof_next = 0;
+    bool prof_suspended = false;   // set while launches are captured into a CUDA graph
 
     hp_stats stats = {};
 

@@ -200,8 +200,9 @@ __global__ void __launch_bounds__(256)
 lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
                  const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
                  const int8_t *__restrict__ lock, int finest, int32_t *__restrict__ dest,
-                 int32_t *__restrict__ pregain, unsigned long long *d_ncand)
+                 int32_t *__restrict__ pregain, unsigned long long *d_ncand, const int32_t *gate)
 {
+    if (gate && *gate != 0) return;   // graph mode: the learned kernel runs this pass
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int cand = 0;
     if (v < n) {
@@ -236,8 +237,10 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
                          const int32_t *__restrict__ xadj, const int8_t *__restrict__ lock, int finest,
                          const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
                          const int64_t *__restrict__ opt, const float *__restrict__ params, float threshold,
-                         int32_t *__restrict__ dest, int32_t *__restrict__ pregain, unsigned long long *d_ncand)
+                         int32_t *__restrict__ dest, int32_t *__restrict__ pregain, unsigned long long *d_ncand,
+                         const int32_t *gate)
 {
+    if (gate && *gate != 1) return;   // graph mode: the plain kernel runs this pass
     __shared__ hp::MlpSmem sm;
     hp::mlp_load_smem(sm, params);
     __syncthreads();
@@ -781,6 +784,7 @@ struct RefineBufs {
     int32_t *pstart, *pend, *und, *ev_end, *es, *ee;
     unsigned long long *pw;
     const int64_t *opt, *maxp;
+    int32_t G;   // gain-row entries of the level
 };
 
 // scalar slots used by refinement
@@ -871,6 +875,299 @@ int strong_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
     return HP_OK;
 }
 
+// ---- pass control ------------------------------------------------------------------
+// The pass loop's bookkeeping (exact cut, best partition, patience, stall rule,
+// next mode) lives in device memory and is advanced by one-thread kernels.  The
+// same rule therefore drives both loops: the eager loop reads the block after
+// every pass, the CUDA-graph loop lets the block set its own WHILE and SWITCH
+// conditions.  Passes per level are capped (a bound on the device-side loop).
+constexpr int32_t HP_MAX_REFINE_PASSES = 1 << 14;
+
+struct RefineCtl {
+    long long cut, excess, best_cut, best_excess, cut_before, cut_start, last_moves;
+    int32_t count, bal, passes, lp_idle;
+    int32_t learned_active, learned_pass, mode, best_current;
+    int32_t take, cont, patience, last_mode;
+    int32_t mode_passes[4];
+};
+
+__device__ void ctl_prepare(RefineCtl *s)
+{
+    s->passes++;
+    s->mode = s->excess <= 0 ? 0 : (s->bal < 2 ? 1 : 2);
+    s->learned_pass = (s->excess <= 0 && s->learned_active) ? 1 : 0;
+    s->cut_before = s->cut;
+    s->bal = s->mode == 0 ? 0 : s->bal + 1;
+    s->mode_passes[s->mode]++;
+}
+
+__global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned)
+{
+    s->cut = (long long)sc[S_CUT2] / 2;
+    s->excess = (long long)sc[S_EXCESS];
+    s->cut_start = s->cut;
+    s->best_cut = s->cut;
+    s->best_excess = s->excess;
+    s->best_current = 1;
+    s->count = 0;
+    s->bal = 0;
+    s->passes = 0;
+    s->lp_idle = 0;
+    s->learned_active = learned;
+    s->learned_pass = 0;
+    s->take = 0;
+    s->last_moves = 0;
+    s->last_mode = -1;
+    s->patience = patience;
+    s->mode = 0;
+    for (int i = 0; i < 4; i++) s->mode_passes[i] = 0;
+    s->cont = s->count <= patience;   // while (count++ <= patience)
+    s->count++;
+    if (s->cont) ctl_prepare(s);
+}
+
+// End of a pass: the exact cut change, the learned fallback, the stall rule, the
+// best partition and the loop condition, in the order of the host loop they replace.
+__global__ void ctl_end_kernel(RefineCtl *s, const unsigned long long *sc, cudaGraphConditionalHandle hloop,
+                               int graph)
+{
+    const long long c1 = (long long)sc[S_C1], c2 = (long long)sc[S_C2];
+    const long long nmoves = (long long)sc[S_NMOVES], ncand = (long long)sc[S_NCAND];
+    s->excess = (long long)sc[S_EXCESS];
+    s->cut -= (c1 + c2) / 2;
+    s->last_moves = nmoves;
+    s->last_mode = s->mode;
+    if (s->learned_pass && s->cut >= s->cut_before) s->learned_active = 0;
+    const int mode = s->mode;
+    // A pass that changed nothing (no moves, no lock change) is repeated
+    // identically by every later pass and can never improve the best
+    // partition: stop now; the result is the same as running on.
+    const bool stalled = nmoves == 0 && (mode == 2 || (mode == 0 && (ncand == 0 || s->lp_idle)));
+    s->lp_idle = (mode == 0 && nmoves == 0) ? 1 : 0;
+    int take = 0;
+    if (s->best_excess > 0 && s->excess < s->best_excess) {
+        take = 1;
+        s->count = 0;
+    } else if (s->cut < s->best_cut && (s->excess <= 0 || s->excess <= s->best_excess)) {
+        if (1000 * s->cut < 999 * s->best_cut) s->count = 0;
+        take = 1;
+    }
+    if (take) {
+        s->best_cut = s->cut;
+        s->best_excess = s->excess;
+    }
+    s->best_current = take;
+    s->take = take;
+    int cont = 0;
+    if (!stalled) {
+        cont = s->count <= s->patience;
+        s->count++;
+    }
+    if (s->passes >= HP_MAX_REFINE_PASSES) cont = 0;
+    s->cont = cont;
+    if (cont) ctl_prepare(s);
+    if (graph) cudaGraphSetConditional(hloop, cont ? 1u : 0u);
+}
+
+// Start of a pass in the graph loop: clear the per-pass scalar slots and select
+// the proposal body (0 LP, 1 weak rebalance, 2 strong rebalance).
+__global__ void ctl_begin_kernel(const RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle hmode)
+{
+    if (threadIdx.x < S_PASS_END) sc[threadIdx.x] = 0;
+    if (threadIdx.x == 0) cudaGraphSetConditional(hmode, (unsigned)s->mode);
+}
+
+__global__ void save_best_kernel(const RefineCtl *s, int32_t n, const int32_t *__restrict__ where,
+                                 int32_t *__restrict__ best_where, int32_t k,
+                                 const unsigned long long *__restrict__ pw, unsigned long long *__restrict__ best_pw)
+{
+    if (!s->take) return;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) best_where[i] = where[i];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += stride) best_pw[i] = pw[i];
+}
+
+__global__ void restore_best_kernel(const RefineCtl *s, int32_t n, const int32_t *__restrict__ best_where,
+                                    int32_t *__restrict__ where)
+{
+    if (s->best_current) return;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) where[i] = best_where[i];
+}
+
+struct PassCfg {
+    int32_t k;
+    bool finest, any_big, recording;
+    RefineCtl *ctl;
+    unsigned long long *best_pw;
+};
+
+// Proposal phase of one pass.  Eager mode launches the LP selection kernel the
+// host chose; graph mode launches both when the MLP is loaded, gated by the
+// control block's learned_pass flag.
+int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int mode, bool learned_pass,
+                 bool both_lp)
+{
+    const int32_t n = g.n, k = P.k;
+    unsigned long long *sc = c->d_scal;
+    int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
+    const unsigned pg = (unsigned)(c->sm_count * 8);
+    const int32_t *gate = both_lp ? &P.ctl->learned_pass : nullptr;
+    if (mode == 0) {
+        const int ltok = hp_prof_begin(c);
+        if (both_lp || learned_pass)
+            HP_LAUNCH(c, lp_select_learned_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, g.xadj,
+                      B.lock, P.finest ? 1 : 0, B.pw, B.maxp, B.opt, c->mlp_params, c->mlp_threshold, B.dest,
+                      B.pregain, &sc[S_NCAND], gate);
+        if (both_lp || !learned_pass)
+            HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
+                      P.finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND], gate);
+        if (P.recording)
+            HP_LAUNCH(c, log_candidates_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, g.xadj,
+                      P.finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.oldp, c->log_x, c->log_v,
+                      c->log_d, c->log_acc, c->log_count, c->log_cap);
+        HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest,
+                  B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
+        if (P.any_big) {
+            HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt, g.where,
+                      B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
+            HP_LAUNCH(c, afterburner_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.big, d_bigcnt, g.xadj,
+                      g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves,
+                      &sc[S_NMOVES]);
+        }
+        if (P.recording)
+            HP_LAUNCH(c, log_accept_kernel, nblk(n), 256, 0, n, B.oldp, B.lock, &sc[S_NCAND], c->log_acc);
+        // select: goff, rows, where, lock in; dest, pregain out.  afterburner:
+        // xadj, adjncy, adjwgt, own pregain/dest/where in, lock out
+        hp_prof_end(c, ltok, HP_PROF_LP, 8 * ((int64_t)n + 1) + 8 * (int64_t)(B.G) + 8 * g.m + 26 * (int64_t)n);
+    } else if (mode == 1) {
+        HP_TRY(weak_rebalance(c, g, B, k));
+    } else {
+        HP_TRY(strong_rebalance(c, g, B, k));
+    }
+    return HP_OK;
+}
+
+// Apply phase of one pass: simultaneous moves, exact cut change from the gain
+// rows before and after, gain-row maintenance, balance, then the control step.
+int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaGraphConditionalHandle hloop,
+               int graph)
+{
+    const int32_t n = g.n, k = P.k;
+    unsigned long long *sc = c->d_scal;
+    const unsigned pg = (unsigned)(c->sm_count * 8);
+    const unsigned mg = nblk(n);
+    HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
+              B.oldp, 1, &sc[S_C1], k);
+    HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw, g.xadj,
+              g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k);
+    if (P.any_big)
+        HP_LAUNCH(c, apply_moves_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.moves, &sc[S_NMOVES], g.where,
+                  B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l,
+                  (int32_t *)&sc[S_DIRTY], k);
+    HP_LAUNCH(c, commit_moves_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest);
+    const int rtok = hp_prof_begin(c);
+    HP_TRY(build_rows(c, g, B, k, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
+                      ((const int32_t *)&sc[S_DIRTY]) + 1, P.any_big, B.dirty));
+    hp_prof_end(c, rtok, HP_PROF_REBUILD, 0);
+    HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
+              B.oldp, 0, &sc[S_C2], k);
+    HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);
+    HP_LAUNCH(c, ctl_end_kernel, 1, 1, 0, P.ctl, (const unsigned long long *)sc, hloop, graph);
+    HP_LAUNCH(c, save_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, P.ctl, n,
+              g.where, B.best_where, k, B.pw, P.best_pw);
+    return HP_OK;
+}
+
+// Graph-capture helper: records the launches of body() into `graph`.  The capture
+// is always ended, also when body() fails.
+template <class F>
+int capture_into(hp_context *c, cudaGraph_t graph, F &&body)
+{
+    HP_CUDA(cudaStreamBeginCaptureToGraph(c->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    // event records cannot sit in conditional bodies: the kernel-class profiler
+    // skips the captured launches (eager calls time them)
+    c->prof_suspended = true;
+    const int rc = body();
+    c->prof_suspended = false;
+    cudaGraph_t out = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &out);
+    if (rc != HP_OK) {
+        cudaGetLastError();
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        fprintf(stderr, "hp: graph capture failed: %s\n", cudaGetErrorString(e));
+        return HP_ERR_CUDA;
+    }
+    return HP_OK;
+}
+
+struct GraphHold {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t x = nullptr;
+    ~GraphHold()
+    {
+        if (x) cudaGraphExecDestroy(x);
+        if (g) cudaGraphDestroy(g);
+    }
+};
+
+// The level's pass loop as one CUDA graph:
+//   WHILE (cont) { ctl_begin; SWITCH (mode) { LP | weak | strong }; apply; ctl_end; save_best }
+// ctl_end sets the WHILE condition, ctl_begin the SWITCH value; nothing returns to
+// the host between passes.  Launch accounting: kernels per body x passes per mode,
+// read back from the control block.
+int run_passes_graph(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, bool both_lp, int *n_common,
+                     int n_mode[3])
+{
+    GraphHold H;
+    HP_CUDA(cudaGraphCreate(&H.g, 0));
+    cudaGraphConditionalHandle hloop;
+    HP_CUDA(cudaGraphConditionalHandleCreate(&hloop, H.g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hloop;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    HP_CUDA(cudaGraphAddNode(&wnode, H.g, nullptr, 0, &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    cudaGraphConditionalHandle hmode;
+    HP_CUDA(cudaGraphConditionalHandleCreate(&hmode, body, 0, 0));
+    cudaGraph_t mode_body[3] = {nullptr, nullptr, nullptr};
+    const int l0 = c->launches;
+    HP_TRY(capture_into(c, body, [&]() -> int {
+        HP_LAUNCH(c, ctl_begin_kernel, 1, 32, 0, P.ctl, c->d_scal, hmode);
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t capg = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        HP_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &capg, &deps, &ndeps));
+        cudaGraphNodeParams sp = {};
+        sp.type = cudaGraphNodeTypeConditional;
+        sp.conditional.handle = hmode;
+        sp.conditional.type = cudaGraphCondTypeSwitch;
+        sp.conditional.size = 3;
+        cudaGraphNode_t snode;
+        HP_CUDA(cudaGraphAddNode(&snode, capg, deps, ndeps, &sp));
+        for (int i = 0; i < 3; i++) mode_body[i] = sp.conditional.phGraph_out[i];
+        HP_CUDA(cudaStreamUpdateCaptureDependencies(c->stream, &snode, 1, cudaStreamSetCaptureDependencies));
+        return pass_apply(c, g, B, P, hloop, 1);
+    }));
+    *n_common = c->launches - l0;
+    for (int m = 0; m < 3; m++) {
+        const int l1 = c->launches;
+        HP_TRY(capture_into(c, mode_body[m], [&]() -> int { return pass_propose(c, g, B, P, m, false, both_lp); }));
+        n_mode[m] = c->launches - l1;
+    }
+    c->launches = l0;
+    HP_CUDA(cudaGraphInstantiate(&H.x, H.g, 0));
+    HP_CUDA(cudaGraphLaunch(H.x, c->stream));
+    // the exec graph may be destroyed once its launch is enqueued
+    return HP_OK;
+}
+
 int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_t *d_opt,
                  const int64_t *d_maxp, int64_t *cut_start, int64_t *cut_final, int *passes_out)
 {
@@ -890,21 +1187,24 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.lock = ralloc_t<int8_t>(c, n);
     B.pw = ralloc_t<unsigned long long>(c, k);
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
+    RefineCtl *ctl = ralloc_t<RefineCtl>(c, 1);
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 1), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
     HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, d_bigcnt);
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
-    int32_t G = 0;
-    HP_TRY(hp_read_scalars(c, B.goff + n, sizeof(int32_t), &G));
+    // gain-row total and the level's count of rows longer than 32 (lets empty
+    // classes skip their launches)
+    int32_t gb[2] = {0, 0};
+    HP_TRY(hp_read_scalars(c, B.goff + n, sizeof(int32_t), &gb[0]));
+    HP_TRY(hp_read_scalars(c, d_bigcnt, sizeof(int32_t), &gb[1]));
+    const int32_t G = gb[0];
+    B.G = G;
     B.gpart = ralloc_t<int32_t>(c, G);
     B.gconn = ralloc_t<int32_t>(c, G);
     HP_CHECK_OOM(c);
-    // the level's counts of rows longer than 32 / 4096 (lets empty classes skip their launches)
-    int32_t nbig = 0;
-    HP_TRY(hp_read_scalars(c, d_bigcnt, sizeof(int32_t), &nbig));
-    const bool any_big = nbig > 0;
+    const bool any_big = gb[1] > 0;
     int tok = hp_prof_begin(c);
     HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt, any_big, nullptr));
     // xadj, adjncy, adjwgt, where (own), goff, gain rows out
@@ -916,127 +1216,50 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
               k <= 2048 ? sizeof(unsigned long long) * k : 0, n, g.where, g.vwgt, B.pw, k);
     HP_LAUNCH(c, rowcut_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, &sc[S_CUT2]);
     HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);
-    long long st[16];
-    HP_TRY(hp_read_scalars(c, sc, sizeof(st), st));
-    int64_t cut = st[S_CUT2] / 2, excess = st[S_EXCESS];
-    *cut_start = cut;
-    int64_t best_cut = cut, best_excess = excess;
-    bool best_current = true;
     HP_CUDA(cudaMemcpyAsync(B.best_where, g.where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
     HP_CUDA(cudaMemcpyAsync(best_pw, B.pw, sizeof(unsigned long long) * k, cudaMemcpyDeviceToDevice, c->stream));
 
-    const int patience = c->opt.refine_patience;
-    const unsigned pg = (unsigned)(c->sm_count * 8);
-    int count = 0, bal = 0, passes = 0;
-    bool lp_idle = false;   // previous pass was an LP pass without moves (locks now clear)
     // learned LP proposals (opt.learned = 1) until a learned pass fails to
     // improve the exact cut; then the plain rule for the rest of the level
-    bool learned_active = c->opt.learned == 1 && c->mlp_ready;
+    const bool learned = c->opt.learned == 1 && c->mlp_ready;
     const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
+    const int patience = c->opt.refine_patience;
+    HP_LAUNCH(c, ctl_init_kernel, 1, 1, 0, ctl, (const unsigned long long *)sc, patience, learned ? 1 : 0);
     int64_t log_r0 = 0;
     if (recording) {
         unsigned long long lc = 0;
         HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
         log_r0 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
     }
+    PassCfg P{k, finest, any_big, recording, ctl, best_pw};
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
-    while (count++ <= patience) {
-        passes++;
-        HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * S_PASS_END, c->stream));
-        const int mode = excess <= 0 ? 0 : (bal < 2 ? 1 : 2);
-        const bool learned_pass = excess <= 0 && learned_active;
-        const int64_t cut_before = cut;
-        if (excess <= 0) {
-            const int ltok = hp_prof_begin(c);
-            if (learned_pass)
-                HP_LAUNCH(c, lp_select_learned_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where,
-                          g.xadj, B.lock, finest ? 1 : 0, B.pw, B.maxp, B.opt, c->mlp_params, c->mlp_threshold,
-                          B.dest, B.pregain, &sc[S_NCAND]);
-            else
-                HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
-                          finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND]);
-            if (recording)
-                HP_LAUNCH(c, log_candidates_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where,
-                          g.xadj, finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.oldp, c->log_x,
-                          c->log_v, c->log_d, c->log_acc, c->log_count, c->log_cap);
-            HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where,
-                      B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
-            if (any_big) {
-                HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
-                          g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
-                HP_LAUNCH(c, afterburner_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.big, d_bigcnt,
-                          g.xadj, g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND],
-                          B.moves, &sc[S_NMOVES]);
-            }
-            if (recording)
-                HP_LAUNCH(c, log_accept_kernel, nblk(n), 256, 0, n, B.oldp, B.lock, &sc[S_NCAND], c->log_acc);
-            // select: goff, rows, where, lock in; dest, pregain out.  afterburner:
-            // xadj, adjncy, adjwgt, own pregain/dest/where in, lock out
-            hp_prof_end(c, ltok, HP_PROF_LP,
-                        8 * ((int64_t)n + 1) + 8 * (int64_t)G + 8 * g.m + 26 * (int64_t)n);
-            bal = 0;
-        } else if (bal < 2) {
-            HP_TRY(weak_rebalance(c, g, B, k));
-            bal++;
-        } else {
-            HP_TRY(strong_rebalance(c, g, B, k));
-            bal++;
+    // CUDA-graph pass loop unless the caller asked for eager launches, the move
+    // log or the per-pass debug log is on, or the stream is the legacy one
+    const bool use_graph = !c->opt.eager && !recording && !dbg && patience >= 0 && c->stream != nullptr &&
+                           c->stream != cudaStreamLegacy;
+    RefineCtl h{};
+    if (use_graph) {
+        int n_common = 0, n_mode[3] = {0, 0, 0};
+        HP_TRY(run_passes_graph(c, g, B, P, learned, &n_common, n_mode));
+        HP_LAUNCH(c, restore_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, ctl, n,
+                  B.best_where, g.where);
+        HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));
+        c->launches += 1 + h.passes * n_common + h.mode_passes[0] * n_mode[0] + h.mode_passes[1] * n_mode[1] +
+                       h.mode_passes[2] * n_mode[2];   // + the graph's own launch
+    } else {
+        HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));
+        while (h.cont) {
+            HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * S_PASS_END, c->stream));
+            HP_TRY(pass_propose(c, g, B, P, h.mode, h.learned_pass != 0, false));
+            HP_TRY(pass_apply(c, g, B, P, 0, 0));
+            HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));
+            if (dbg)
+                fprintf(stderr, "gpu pass n=%d pass=%d mode=%d moves=%lld cut=%lld excess=%lld\n", n,
+                        h.passes - (h.cont ? 1 : 0), h.last_mode, h.last_moves, h.cut, h.excess);
         }
-        // apply the move set simultaneously; exact cut change from the gain rows
-        const unsigned mg = nblk(n);
-        HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where,
-                  B.dest, B.oldp, 1, &sc[S_C1], k);
-        HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw,
-                  g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l,
-                  (int32_t *)&sc[S_DIRTY], k);
-        if (any_big)
-            HP_LAUNCH(c, apply_moves_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.moves, &sc[S_NMOVES],
-                      g.where, B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l,
-                      (int32_t *)&sc[S_DIRTY], k);
-        HP_LAUNCH(c, commit_moves_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest);
-        const int rtok = hp_prof_begin(c);
-        HP_TRY(build_rows(c, g, B, k, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
-                          ((const int32_t *)&sc[S_DIRTY]) + 1, any_big, B.dirty));
-        hp_prof_end(c, rtok, HP_PROF_REBUILD, 0);
-        HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where,
-                  B.dest, B.oldp, 0, &sc[S_C2], k);
-        HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);
-        HP_TRY(hp_read_scalars(c, sc, sizeof(long long) * 5, st));
-        const int64_t c1 = st[S_C1], c2 = st[S_C2];
-        excess = st[S_EXCESS];
-        cut -= (c1 + c2) / 2;
-        if (learned_pass && cut >= cut_before) learned_active = false;
-        if (dbg)
-            fprintf(stderr, "gpu pass n=%d pass=%d mode=%d moves=%lld cut=%lld excess=%lld\n", n, passes,
-                    mode, st[S_NMOVES], (long long)cut, (long long)excess);
-
-        // A pass that changed nothing (no moves, no lock change) is repeated
-        // identically by every later pass and can never improve the best
-        // partition: stop now; the result is the same as running on.
-        const bool stalled = st[S_NMOVES] == 0 &&
-                             ((mode == 2) || (mode == 0 && (st[S_NCAND] == 0 || lp_idle)));
-        lp_idle = (mode == 0 && st[S_NMOVES] == 0);
-        bool take = false;
-        if (best_excess > 0 && excess < best_excess) {
-            take = true;
-            count = 0;
-        } else if (cut < best_cut && (excess <= 0 || excess <= best_excess)) {
-            if (1000 * cut < 999 * best_cut) count = 0;
-            take = true;
-        }
-        if (take) {
-            best_cut = cut;
-            best_excess = excess;
-            best_current = true;
-            HP_CUDA(cudaMemcpyAsync(B.best_where, g.where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
-            HP_CUDA(cudaMemcpyAsync(best_pw, B.pw, sizeof(unsigned long long) * k, cudaMemcpyDeviceToDevice, c->stream));
-        } else {
-            best_current = false;
-        }
-        if (stalled) break;
+        HP_LAUNCH(c, restore_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, ctl, n,
+                  B.best_where, g.where);
     }
-    if (!best_current)
-        HP_CUDA(cudaMemcpyAsync(g.where, B.best_where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
     if (recording) {
         unsigned long long lc = 0;
         HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
@@ -1045,8 +1268,9 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
             HP_LAUNCH(c, log_label_kernel, nblk(r1 - log_r0), 256, 0, log_r0, r1, g.where, c->log_v, c->log_d,
                       c->log_acc, c->log_y);
     }
-    *cut_final = best_cut;
-    *passes_out = passes;
+    *cut_start = h.cut_start;
+    *cut_final = h.best_cut;
+    *passes_out = h.passes;
     HP_TRY(hp_check_status(c));
     c->hi = mark;
     return HP_OK;

@@ -62,6 +62,11 @@ typedef struct hp_options {
     int32_t  validate;         /* 0 none, 1 structural check on the device (default)          */
     int32_t  trace;            /* 1: keep every level for hp_trace_*() (tests)                */
     int32_t  profile;          /* 1: time kernel classes with CUDA events into hp_stats.prof_* */
+    int32_t  eager;            /* 0: each level's refinement passes run as one CUDA graph
+                                  (device-side WHILE/SWITCH control, default); 1: passes
+                                  launched one by one with a host read per pass.  Results
+                                  are identical.  With profile = 1 the graphed LP and
+                                  gain-rebuild launches are not timed (eager ones are).    */
     uint64_t seed;             /* matching tie-break seed (default 1)                         */
 } hp_options;
 

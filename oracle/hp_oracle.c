@@ -28,6 +28,8 @@
  */
 #include "hp_oracle.h"
 
+#define ORA_MAX_REFINE_PASSES (1 << 14)
+
 #include <limits.h>
 #include <stdio.h>
 #include <math.h>
@@ -1039,6 +1041,8 @@ int64_t ora_refine(int32_t n, const int32_t *xadj, const int32_t *adjncy,
         int stalled = nm == 0 && (mode == 2 || (mode == 0 && (ncand == 0 || lp_idle)));
         lp_idle = (mode == 0 && nm == 0);
         if (stalled) break;
+        /* hard bound on passes per level, the same as the device-side loop's */
+        if (passes >= ORA_MAX_REFINE_PASSES) break;
     }
     memcpy(where, best, sizeof(int32_t) * (size_t)n);
     for (int t = 0; t < nt; t++) { free(s.conn_t[t]); free(s.parts_t[t]); }

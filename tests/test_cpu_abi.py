@@ -54,8 +54,10 @@ def test_load_library_binds_prototypes(lib):
 
 
 def test_options_struct_layout():
-    # version + 10 int32 fields (44 bytes), padding, then the 8-byte seed
+    # version + 11 int32 fields (48 bytes), then the 8-byte seed; `eager` took the
+    # padding slot, so the layout of version-1 callers is unchanged
     assert C.sizeof(_abi.HpOptions) == 56
+    assert _abi.HpOptions.eager.offset == 44
     assert _abi.HpOptions.seed.offset == 48
     assert C.sizeof(_abi.HpStats) == 8 * 3 + 4 * 2 + 8 + 4 * 2 + 4 * 6 + 4 * 8 + 8 * 8 + 4 * 8
 

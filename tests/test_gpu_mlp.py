@@ -93,3 +93,7 @@ def test_learned_partition_exact_and_deterministic(ctx):
     assert a_cut == oracle.edgecut(g, a_part)           # exact int64 cut
     assert st.max_excess <= 0                            # balance bound honoured exactly
     assert a_cut <= 1.10 * plain_cut
+    # the CUDA-graph pass loop (both LP kernels captured, gated on the device by
+    # the learned flag) gives the same partition as the eager loop
+    e_part, e_cut = ctx.partition_graph(g, 64, options=default_options(learned=1, eager=1))
+    assert e_cut == a_cut and np.array_equal(e_part, a_part)

@@ -106,6 +106,40 @@ def test_full_grid3d_128_k64(ctx):
     assert part.min() >= 0 and part.max() < 64
 
 
+def test_eager_passes_match_oracle(ctx):
+    """The eager pass loop (one launch per kernel, a host read per pass) against
+    the oracle, on the graphs the graph-mode tests above use."""
+    compare_runs(ctx, graphs.config_grid2d(), 8, coarsen_to=160, eager=1)
+    compare_runs(ctx, graphs.rmat(14, 16, seed=3, wmin=1, wmax=100), 256, eager=1)
+
+
+@pytest.mark.parametrize("name", ["grid3d_48", "rmat13_hubs", "rgg17", "star"])
+def test_graph_loop_equals_eager_loop(ctx, name):
+    """CUDA-graph pass loop (device-side WHILE/SWITCH control) and the eager loop
+    give the same partition, cut and pass count."""
+    if name == "grid3d_48":
+        g, k = graphs.grid3d(48, 48, 48, seed=2, wmin=1, wmax=10), 64
+    elif name == "rmat13_hubs":
+        g, k = graphs.rmat(13, 16, seed=5, wmin=1, wmax=100), 128
+    elif name == "rgg17":
+        g, k = graphs.rgg(1 << 17, 12.0, seed=4), 512
+    else:
+        n = 20001
+        xadj = np.zeros(n + 1, np.int32)
+        xadj[1] = n - 1
+        xadj[2:] = n - 1 + np.arange(1, n)
+        adj = np.concatenate([np.arange(1, n), np.zeros(n - 1)]).astype(np.int32)
+        g = graphs.Graph(xadj, adj, np.ones(n, np.int32), np.ones(2 * (n - 1), np.int32), "star")
+        k = 16
+    pe, ce = ctx.partition_graph(g, k, options=default_options(eager=1))
+    se = ctx.stats()
+    pg, cg = ctx.partition_graph(g, k, options=default_options(eager=0))
+    sg = ctx.stats()
+    assert ce == cg and np.array_equal(pe, pg)
+    assert se.refine_passes == sg.refine_passes
+    assert sg.max_excess == se.max_excess
+
+
 def test_deterministic_repeat(ctx):
     g = graphs.rmat(13, 16, seed=3)
     a = ctx.partition_graph(g, 64)
