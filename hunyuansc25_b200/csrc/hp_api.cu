@@ -296,6 +296,12 @@ void hp_prof_end(hp_context *c, int token, int cls, int64_t bytes)
     r.launches = c->launches - r.launches;
 }
 
+void hp_prof_add_bytes(hp_context *c, int token, int64_t bytes)
+{
+    if (token < 0 || token >= (int)c->prof_recs.size()) return;
+    c->prof_recs[token].bytes += bytes;
+}
+
 void hp_prof_resolve(hp_context *c)
 {
     for (const auto &r : c->prof_recs) {

@@ -8,9 +8,17 @@
 //     leaf, relative, isolate, forced  :1374-1716 (gated at 75 % matched, :2577)
 //     cmap / cvwgt / coarse row bound  :1012-1096
 //   contraction                        hunyuangraph_GPU_contraction.h:715-1247
-//     (scatter -> segmented sort -> mark -> scan -> write; here one pass per
-//      coarse vertex that gathers both fine rows, merges equal coarse
-//      neighbours and writes them sorted, by size class; hp_rowagg.cuh)
+//     (scatter -> segmented sort -> mark -> scan -> write; here each coarse
+//      row gathers both fine rows, merges equal coarse neighbours and is
+//      written sorted, by size class:
+//        <= 32 entries    one thread, bitonic network in registers, written in
+//                         place by one ordered pass with a decoupled look-back
+//                         that also produces the coarse xadj
+//        33..256          one warp, LSD radix sort in shared memory
+//        257..4096        one CTA, LSD radix sort in shared memory
+//        larger           one CTA, dense accumulator + presence bitmap
+//      the long classes go through a temporary buffer and are copied to their
+//      final offsets)
 // The reference's matching is an atomicCAS race (nondeterministic); every
 // decision here is a pure function of the level's CSR and the seed, so the
 // CPU oracle reproduces each level bit for bit.
@@ -27,6 +35,20 @@ constexpr int HUGE_DEG = 4096;   // rows longer than this use a CTA per vertex
 
 // ELIG: handshake proposal (unmatched neighbour, weight cap).  !ELIG: hub
 // choice for two-hop matching (any neighbour).
+//
+// Rounds after the first keep a proposal that is still valid: between rounds
+// the eligible set of a vertex only shrinks (neighbours get matched; weights
+// and the cap do not change), so if the previous best neighbour is still
+// unmatched it is still the best, and an empty set stays empty.  Only vertices
+// whose choice was matched away rescan their row (same result as a full rescan).
+__device__ __forceinline__ bool keep_proposal(bool later_round, int32_t v, const int32_t *__restrict__ pref,
+                                              const int32_t *__restrict__ match)
+{
+    if (!later_round) return false;
+    const int32_t pu = pref[v];
+    return pu < 0 || match[pu] == -1;
+}
+
 template <bool ELIG>
 __global__ void __launch_bounds__(256)
 pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
@@ -40,19 +62,35 @@ pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__
     const int32_t b = xadj[v], e = xadj[v + 1];
     if (e - b > BIG_DEG) return;
     if (match[v] != -1) { pref[v] = -1; return; }
+    if (ELIG && keep_proposal(made_prev != nullptr, v, pref, match)) return;
     const int32_t wv = vwgt[v];
     int32_t bu = -1, bw = 0;
     uint32_t bh = 0;
-    for (int32_t j = b; j < e; j++) {
-        int32_t u = adjncy[j];
-        if (u == v) continue;
-        if (ELIG) {
-            if (match[u] != -1) continue;
-            if ((int64_t)wv + vwgt[u] > maxvwgt) continue;
+    // four entries at a time: the row loads, then the neighbour gathers, are
+    // issued together so each thread keeps several misses in flight
+    for (int32_t j0 = b; j0 < e; j0 += 4) {
+        int32_t u[4], w[4], mu[4], vu[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const bool in = j0 + q < e;
+            u[q] = in ? adjncy[j0 + q] : v;
+            w[q] = in ? adjwgt[j0 + q] : 0;
         }
-        int32_t w = adjwgt[j];
-        uint32_t h = hp::edge_tie(lkey, v, u);
-        if (bu < 0 || hp::better(w, h, u, bw, bh, bu)) { bu = u; bw = w; bh = h; }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            mu[q] = (ELIG && u[q] != v) ? match[u[q]] : -1;
+            vu[q] = (ELIG && u[q] != v) ? vwgt[u[q]] : 0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (u[q] == v) continue;
+            if (ELIG) {
+                if (mu[q] != -1) continue;
+                if ((int64_t)wv + vu[q] > maxvwgt) continue;
+            }
+            uint32_t h = hp::edge_tie(lkey, v, u[q]);
+            if (bu < 0 || hp::better(w[q], h, u[q], bw, bh, bu)) { bu = u[q]; bw = w[q]; bh = h; }
+        }
     }
     pref[v] = bu;
 }
@@ -72,6 +110,7 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = list[i];
         if (match[v] != -1) { if (lane == 0) pref[v] = -1; continue; }
+        if (ELIG && keep_proposal(made_prev != nullptr, v, pref, match)) continue;
         const int32_t wv = vwgt[v];
         int32_t bu = -1, bw = 0;
         uint32_t bh = 0;
@@ -139,6 +178,7 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t v = list[li];
         if (match[v] != -1) { if (threadIdx.x == 0) pref[v] = -1; continue; }
+        if (ELIG && keep_proposal(made_prev != nullptr, v, pref, match)) continue;
         const int32_t wv = vwgt[v];
         int32_t bu = -1, bw = 0;
         uint32_t bh = 0;
@@ -309,128 +349,440 @@ finalize_match_kernel(int32_t n, int32_t *__restrict__ match, int32_t *__restric
     leader_flag[v] = (v <= u);
 }
 
-// Followers copy the leader's coarse id; leaders fill the coarse vertex.
+// Followers copy the leader's coarse id; leaders describe the coarse row: the
+// fine rows it merges (start and length of the leader's and the mate's row)
+// and its vertex weight.  Rows longer than SMALL_ROW entries are appended to
+// their class list and their length is counted for the temporary row buffer.
+constexpr int32_t SMALL_ROW = 32;
+
+struct RowInfo {
+    int32_t s0, l0, s1, l1;   // leader row start/length, mate row start/length (l1 = 0 if unmatched)
+};
+
 __global__ void __launch_bounds__(256)
 coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__restrict__ cmap,
                     const int32_t *__restrict__ xadj, const int32_t *__restrict__ vwgt,
-                    int32_t *__restrict__ leader_of, int32_t *__restrict__ cvwgt,
-                    int32_t *__restrict__ tlen, int32_t *__restrict__ lists,
-                    int32_t *__restrict__ counts, int32_t cn, int32_t *__restrict__ maxlen)
+                    int4 *__restrict__ rinfo, int32_t *__restrict__ cvwgt, int32_t *__restrict__ ltlen,
+                    int32_t *__restrict__ lists, int32_t *__restrict__ counts, int32_t cn,
+                    int32_t *__restrict__ maxlen, unsigned long long *__restrict__ long_total,
+                    int32_t *__restrict__ small_max)
 {
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     int32_t u = match[v];
     if (v > u) { cmap[v] = cmap[u]; return; }
     int32_t c = cmap[v];
-    leader_of[c] = v;
-    int32_t len = xadj[v + 1] - xadj[v];
+    const int32_t s0 = xadj[v], l0 = xadj[v + 1] - s0;
+    int32_t s1 = 0, l1 = 0;
     int32_t w = vwgt[v];
-    if (u != v) { len += xadj[u + 1] - xadj[u]; w += vwgt[u]; }
+    if (u != v) {
+        s1 = xadj[u];
+        l1 = xadj[u + 1] - s1;
+        w += vwgt[u];
+    }
+    rinfo[c] = make_int4(s0, l0, s1, l1);
     cvwgt[c] = w;
-    tlen[c] = len;
-    if (len > 32) {
-        int cls = len <= 512 ? 0 : (len <= 4096 ? 1 : 2);
+    const int32_t len = l0 + l1;
+    ltlen[c] = len > SMALL_ROW ? len : 0;
+    if (len <= SMALL_ROW && len > 8) atomicMax(small_max, len);   // picks the assembly kernel's network
+    if (len > SMALL_ROW) {
+        int cls = len <= 256 ? 0 : (len <= 4096 ? 1 : 2);   // warp radix, CTA radix, dense
         int32_t pos = atomicAdd(&counts[cls], 1);
         lists[(int64_t)cls * cn + pos] = c;
         if (cls == 2) atomicMax(maxlen, len);
+        atomicAdd(long_total, (unsigned long long)len);
     }
 }
 
 // Entry i of coarse vertex c: the i-th entry of the leader's row, then of the
 // mate's row, mapped through cmap; the coarse self key is dropped.
 struct ContractSrc {
-    const int32_t *xadj, *adjncy, *adjwgt, *cmap, *match, *leader_of;
-    __device__ __forceinline__ void row(int32_t c, int32_t &v, int32_t &u, int32_t &lv,
-                                        int32_t &len) const
+    const int4 *rinfo;
+    const int32_t *adjncy, *adjwgt, *cmap;
+    __device__ __forceinline__ void row(int32_t c, RowInfo &r, int32_t &len) const
     {
-        v = leader_of[c];
-        u = match[v];
-        lv = xadj[v + 1] - xadj[v];
-        len = lv + (u != v ? xadj[u + 1] - xadj[u] : 0);
+        const int4 q = rinfo[c];
+        r = RowInfo{q.x, q.y, q.z, q.w};
+        len = r.l0 + r.l1;
     }
-    __device__ __forceinline__ void get(int32_t c, int32_t v, int32_t u, int32_t lv, int32_t i,
-                                        int32_t &k, int32_t &w) const
+    __device__ __forceinline__ void get(int32_t c, const RowInfo &r, int32_t i, int32_t &k, int32_t &w) const
     {
-        int32_t j = i < lv ? xadj[v] + i : xadj[u] + (i - lv);
+        int32_t j = i < r.l0 ? r.s0 + i : r.s1 + (i - r.l0);
         k = cmap[adjncy[j]];
         w = adjwgt[j];
         if (k == c) { k = hp::KEY_NONE; w = 0; }
     }
 };
 
-__global__ void __launch_bounds__(256)
-contract_warp_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict__ toff,
-                     int32_t *__restrict__ tk, int32_t *__restrict__ tw, int32_t *__restrict__ ucnt)
+// ---- short rows: one thread per coarse row, aggregation in registers ------------
+// Entries are packed as key << 32 | weight (keys are coarse ids < 2^31, the
+// dropped self key and padding are KEY_NONE), sorted ascending by a bitonic
+// network over the first NET of 32 registers (compile-time indices only), and
+// equal keys are merged by summing the low halves.
+template <int NET, int XN>
+__device__ __forceinline__ void sort_regs(unsigned long long (&x)[XN])
 {
-    const int lane = threadIdx.x & 31;
-    for (int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; c < cn;
-         c += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        int32_t v, u, lv, len;
-        src.row((int32_t)c, v, u, lv, len);
-        if (len > 32) continue;
-        int32_t k = hp::KEY_NONE, w = 0;
-        if (lane < len) src.get((int32_t)c, v, u, lv, lane, k, w);
-        int32_t off = toff[c];
-        int cnt = hp::warp_aggregate32(k, w, tk + off, tw + off);
-        if (lane == 0) ucnt[c] = cnt;
+#pragma unroll
+    for (int size = 2; size <= NET; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+#pragma unroll
+            for (int i = 0; i < NET; i++) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const unsigned long long a = x[i], b = x[j];
+                    const unsigned long long lo = a < b ? a : b, hi = a < b ? b : a;
+                    if ((i & size) == 0) { x[i] = lo; x[j] = hi; }
+                    else { x[i] = hi; x[j] = lo; }
+                }
+            }
+}
+
+constexpr unsigned long long PACK_NONE = (unsigned long long)(uint32_t)hp::KEY_NONE << 32;
+
+template <int NET, int XN>
+__device__ __forceinline__ int gather_sort_row(const ContractSrc &src, int32_t c, const RowInfo &r, int32_t len,
+                                               unsigned long long (&x)[XN])
+{
+#pragma unroll
+    for (int i = 0; i < NET; i++) {
+        unsigned long long e = PACK_NONE;
+        if (i < len) {
+            int32_t k, w;
+            src.get(c, r, i, k, w);
+            if (k != hp::KEY_NONE) e = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)w;
+        }
+        x[i] = e;
+    }
+    sort_regs<NET, XN>(x);
+    int u = 0;
+#pragma unroll
+    for (int i = 0; i < NET; i++) {
+        const uint32_t k = (uint32_t)(x[i] >> 32);
+        const bool head = k != (uint32_t)hp::KEY_NONE && (i == 0 || (uint32_t)(x[i - 1] >> 32) != k);
+        u += head;
+    }
+    return u;
+}
+
+template <int NET, int XN>
+__device__ __forceinline__ void emit_row(const unsigned long long (&x)[XN], int32_t *__restrict__ out_k,
+                                         int32_t *__restrict__ out_w)
+{
+    int r = -1;
+    uint32_t prev = 0xffffffffu;
+    int32_t acc = 0;
+#pragma unroll
+    for (int i = 0; i < NET; i++) {
+        const uint32_t k = (uint32_t)(x[i] >> 32);
+        const int32_t w = (int32_t)(uint32_t)x[i];
+        if (k == (uint32_t)hp::KEY_NONE) continue;
+        if (k != prev) {
+            if (r >= 0) out_w[r] = acc;
+            r++;
+            out_k[r] = (int32_t)k;
+            acc = w;
+            prev = k;
+        } else {
+            acc += w;
+        }
+    }
+    if (r >= 0) out_w[r] = acc;
+}
+
+// Coarse CSR assembly in one ordered pass: tiles of ASM_TILE coarse rows are
+// taken in order (dynamic tile counter); each thread aggregates its short row in
+// registers (network of 8, 16 or 32 by the longest short row in the warp) or
+// reads the unique count of a long row aggregated before; a block scan plus a
+// decoupled look-back across tiles gives every row its final offset, so cxadj
+// and the short rows' entries are written directly, with no second scan and no
+// compaction copy.  Long rows are placed afterwards by copy_long_rows_kernel.
+constexpr int ASM_TILE = 256;
+
+// XN: the longest network the level needs (8, 16 or 32; the host reads the
+// longest short row) -- the register array, and so the occupancy, follow it.
+template <int XN>
+__global__ void __launch_bounds__(ASM_TILE)
+contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict__ ucnt,
+                         int32_t *__restrict__ cxadj, int32_t *__restrict__ cadjncy,
+                         int32_t *__restrict__ cadjwgt, unsigned long long *tile_status,
+                         unsigned *tile_counter, unsigned *status)
+{
+    __shared__ int32_t s_scan[ASM_TILE / 32 + 2];
+    __shared__ int32_t s_tile, s_excl;
+    if (threadIdx.x == 0) s_tile = (int32_t)atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const int64_t tile = s_tile;
+    const int32_t c = (int32_t)(tile * ASM_TILE + threadIdx.x);
+    RowInfo r{0, 0, 0, 0};
+    int32_t len = 0;
+    if (c < cn) src.row(c, r, len);
+    const bool small = c < cn && len <= SMALL_ROW;
+    const unsigned wmax = __reduce_max_sync(HP_FULL_MASK, small ? (unsigned)len : 0u);
+    unsigned long long x[XN];
+    int u = 0;
+    if (c < cn && !small) u = ucnt[c];
+    if (XN == 8 || wmax <= 8) {
+        if (small) u = gather_sort_row<8, XN>(src, c, r, len, x);
+    } else if (XN == 16 || wmax <= 16) {
+        if (small) u = gather_sort_row<(XN < 16 ? XN : 16), XN>(src, c, r, len, x);
+    } else {
+        if (small) u = gather_sort_row<XN, XN>(src, c, r, len, x);
+    }
+    int agg;
+    const int local = hp::block_excl_scan<ASM_TILE>(u, &agg, s_scan);
+    if (threadIdx.x < 32) {
+        const int32_t excl = hp::lookback_exclusive(tile_status, tile, agg, status);
+        if (threadIdx.x == 0) s_excl = excl;
+    }
+    __syncthreads();
+    const int32_t off = s_excl + local;
+    if (c < cn) {
+        cxadj[c] = off;
+        if (c == cn - 1) cxadj[cn] = off + u;
+    }
+    if (small) {
+        if (XN == 8 || wmax <= 8) emit_row<8, XN>(x, cadjncy + off, cadjwgt + off);
+        else if (XN == 16 || wmax <= 16) emit_row<(XN < 16 ? XN : 16), XN>(x, cadjncy + off, cadjwgt + off);
+        else emit_row<XN, XN>(x, cadjncy + off, cadjwgt + off);
     }
 }
 
-// Rows of 33..HCAP/2 entries: one CTA merges equal coarse ids in a
-// shared-memory hash table (linear probing, atomicCAS keys, atomicAdd
-// weights), compacts the unique keys, and bitonic-sorts only those.
-template <int NT, int HCAP>
-__global__ void __launch_bounds__(NT)
-contract_hash_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
-                     ContractSrc src, const int32_t *__restrict__ toff, int32_t *__restrict__ tk,
-                     int32_t *__restrict__ tw, int32_t *__restrict__ ucnt)
+// Long rows (aggregated into the temporary buffer at toff[c]) to their final
+// place cxadj[c]: one warp per row, coalesced.
+__global__ void __launch_bounds__(256)
+copy_long_rows_kernel(const int32_t *__restrict__ lists, const int32_t *__restrict__ counts, int32_t cn,
+                      const int32_t *__restrict__ toff, const int32_t *__restrict__ ucnt,
+                      const int32_t *__restrict__ cxadj, const int32_t *__restrict__ tk,
+                      const int32_t *__restrict__ tw, int32_t *__restrict__ cadjncy, int32_t *__restrict__ cadjwgt)
 {
-    extern __shared__ int32_t hsm[];
-    int32_t *hk = hsm, *hw = hsm + HCAP;                  // hash table
-    int32_t *sk = hsm + 2 * HCAP, *sw = sk + HCAP / 2;    // unique entries to sort
-    __shared__ int32_t s_scan[NT / 32 + 2];
+    const int lane = threadIdx.x & 31;
+    const int64_t total = (int64_t)counts[0] + counts[1] + counts[2];
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < total;
+         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int cls = i < counts[0] ? 0 : (i < (int64_t)counts[0] + counts[1] ? 1 : 2);
+        const int64_t pos = cls == 0 ? i : (cls == 1 ? i - counts[0] : i - counts[0] - counts[1]);
+        const int32_t c = lists[(int64_t)cls * cn + pos];
+        const int32_t src = toff[c], dst = cxadj[c], cnt = ucnt[c];
+        for (int32_t j = lane; j < cnt; j += 32) {
+            cadjncy[dst + j] = tk[src + j];
+            cadjwgt[dst + j] = tw[src + j];
+        }
+    }
+}
+
+// ---- long rows: stable LSD radix sort of packed entries in shared memory -------
+// A group of G threads (one warp, or the whole CTA) sorts the entries of one
+// coarse row, packed as key << 32 | weight with the self key already dropped,
+// by the low `kbits` bits of the key (8-bit digits), then merges equal keys.
+// Per pass: per-warp digit histograms, one exclusive scan over them in
+// digit-major order (digit d of warp w before digit d of warp w+1), and a stable
+// scatter in which each warp walks its contiguous chunk 32 items at a time and
+// ranks equal digits with __match_any_sync.
+template <int G>
+__device__ __forceinline__ void group_sync()
+{
+    if (G == 32) __syncwarp();
+    else __syncthreads();
+}
+
+// Exclusive scan across the G threads of a group (one value per thread).
+template <int G>
+__device__ __forceinline__ int group_excl_scan(int v, int *total, int32_t *s_scan /* G/32 + 1 */)
+{
+    const int lane = threadIdx.x & 31;
+    const int incl = hp::warp_incl_scan(v);
+    if (G == 32) {
+        *total = __shfl_sync(HP_FULL_MASK, incl, 31);
+        return incl - v;
+    }
+    const int wid = (threadIdx.x % G) >> 5;
+    if (lane == 31) s_scan[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int t = lane < G / 32 ? s_scan[lane] : 0;
+        int ti = hp::warp_incl_scan(t);
+        if (lane < G / 32) s_scan[lane] = ti - t;
+        if (lane == G / 32 - 1) s_scan[G / 32] = ti;
+    }
+    __syncthreads();
+    const int r = s_scan[wid] + incl - v;
+    *total = s_scan[G / 32];
+    __syncthreads();
+    return r;
+}
+
+// Sorts A[0..N) (result in A; B is scratch of the same size); hist holds
+// 256 * G/32 counters.  All G threads call it.
+template <int G>
+__device__ void group_radix_sort(unsigned long long *A, unsigned long long *B, int N, int kbits, int32_t *hist,
+                                 int32_t *s_scan)
+{
+    constexpr int W = G / 32;
+    const int t = threadIdx.x % G, lane = t & 31, w = t >> 5;
+    const int chunk = (N + W - 1) / W;
+    const int beg = min(N, w * chunk), end = min(N, beg + chunk);
+    for (int shift = 0; shift < kbits; shift += 8) {
+        for (int i = t; i < 256 * W; i += G) hist[i] = 0;
+        group_sync<G>();
+        for (int i = beg + lane; i < end; i += 32) atomicAdd(&hist[((unsigned)(A[i] >> (32 + shift)) & 255u) * W + w], 1);
+        group_sync<G>();
+        // digit-major exclusive offsets: thread t owns counters [8t, 8t+8)
+        int s = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) s += hist[8 * t + q];
+        int tot;
+        int run = group_excl_scan<G>(s, &tot, s_scan);
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int h = hist[8 * t + q];
+            hist[8 * t + q] = run;
+            run += h;
+        }
+        group_sync<G>();
+        for (int base = beg; base < end; base += 32) {
+            const int i = base + lane;
+            const bool valid = i < end;
+            const unsigned long long x = valid ? A[i] : 0ull;
+            const unsigned d = valid ? ((unsigned)(x >> (32 + shift)) & 255u) : 256u + lane;
+            const unsigned peers = __match_any_sync(HP_FULL_MASK, d);
+            const int rank = __popc(peers & hp::lanemask_lt());
+            int *slot = &hist[(d & 255u) * W + w];
+            if (valid) B[*slot + rank] = x;
+            __syncwarp();
+            if (valid && rank == 0) *slot += __popc(peers);
+            __syncwarp();
+        }
+        group_sync<G>();
+        unsigned long long *tmp = A; A = B; B = tmp;
+    }
+    // an odd number of passes leaves the result in the scratch buffer
+    if (((kbits + 7) / 8) & 1) {
+        for (int i = t; i < N; i += G) B[i] = A[i];
+        group_sync<G>();
+    }
+}
+
+// Merges equal keys of the sorted A[0..N): unique keys in order to out_k, the
+// weight sums to out_w (a wrapping 32-bit prefix of the weights; every run sum
+// is itself an int32 edge weight).  Returns the unique count (all threads).
+// pre is scratch for N ints.
+template <int G>
+__device__ int group_merge_emit(const unsigned long long *A, int N, int32_t *out_k, int32_t *out_w, uint32_t *pre,
+                                int32_t *s_scan)
+{
+    const int t = threadIdx.x % G;
+    const int per = (N + G - 1) / G;
+    const int lo = min(N, t * per), hi = min(N, lo + per);
+    int heads = 0;
+    uint32_t wsum = 0;
+    for (int i = lo; i < hi; i++) {
+        heads += (i == 0 || (uint32_t)(A[i] >> 32) != (uint32_t)(A[i - 1] >> 32));
+        wsum += (uint32_t)A[i];
+    }
+    int U;
+    int o = group_excl_scan<G>(heads, &U, s_scan) - 1;   // ordinal of the current run
+    int dummy;
+    uint32_t p = (uint32_t)group_excl_scan<G>((int)wsum, &dummy, s_scan);   // weights before lo
+    for (int i = lo; i < hi; i++) {
+        const uint32_t k = (uint32_t)(A[i] >> 32);
+        if (i == 0 || k != (uint32_t)(A[i - 1] >> 32)) {
+            o++;
+            out_k[o] = (int32_t)k;
+            pre[o] = p;
+        }
+        p += (uint32_t)A[i];
+    }
+    group_sync<G>();
+    // second walk: the last entry of every run closes it
+    p = (uint32_t)group_excl_scan<G>((int)wsum, &dummy, s_scan);
+    o = group_excl_scan<G>(heads, &dummy, s_scan) - 1;
+    for (int i = lo; i < hi; i++) {
+        const uint32_t k = (uint32_t)(A[i] >> 32);
+        if (i == 0 || k != (uint32_t)(A[i - 1] >> 32)) o++;
+        p += (uint32_t)A[i];
+        if (i == N - 1 || (uint32_t)(A[i + 1] >> 32) != k) out_w[o] = (int32_t)(p - pre[o]);
+    }
+    return U;
+}
+
+// Gathers row c (self key dropped) into A, compacted, in entry order; returns N.
+template <int G>
+__device__ int group_gather_row(const ContractSrc &src, int32_t c, const RowInfo &r, int32_t len,
+                                unsigned long long *A, int32_t *s_scan)
+{
+    const int t = threadIdx.x % G;
+    int base = 0;
+    for (int i0 = 0; i0 < len; i0 += G) {
+        const int i = i0 + t;
+        int32_t k = hp::KEY_NONE, w = 0;
+        if (i < len) src.get(c, r, i, k, w);
+        const int keep = k != hp::KEY_NONE;
+        int tot;
+        const int pos = group_excl_scan<G>(keep, &tot, s_scan);
+        if (keep) A[base + pos] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)w;
+        base += tot;
+    }
+    group_sync<G>();
+    return base;
+}
+
+constexpr int WROW_MAX = 256;    // warp class: 33..256 entries
+constexpr int CROW_MAX = 4096;   // CTA class: 257..4096 entries
+constexpr int WROW_WARPS = 8;
+
+// Warp class: 8 warps per CTA, one row per warp at a time.
+__global__ void __launch_bounds__(32 * WROW_WARPS)
+contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, ContractSrc src,
+                           const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
+                           int32_t *__restrict__ ucnt, int kbits)
+{
+    __shared__ unsigned long long sA[WROW_WARPS][WROW_MAX], sB[WROW_WARPS][WROW_MAX];
+    __shared__ int32_t sH[WROW_WARPS][256];
+    const int wid = threadIdx.x >> 5;
+    const int32_t cnt = *d_count;
+    for (int64_t li = (int64_t)blockIdx.x * WROW_WARPS + wid; li < cnt; li += (int64_t)gridDim.x * WROW_WARPS) {
+        const int32_t c = list[li];
+        RowInfo r;
+        int32_t len;
+        src.row(c, r, len);
+        const int N = group_gather_row<32>(src, c, r, len, sA[wid], nullptr);
+        group_radix_sort<32>(sA[wid], sB[wid], N, kbits, sH[wid], nullptr);
+        const int32_t off = toff[c];
+        const int U = group_merge_emit<32>(sA[wid], N, tk + off, tw + off, (uint32_t *)sB[wid], nullptr);
+        if ((threadIdx.x & 31) == 0) ucnt[c] = U;
+        __syncwarp();
+    }
+}
+
+// CTA class: 256 threads per row.
+constexpr int CROW_THREADS = 256;
+__global__ void __launch_bounds__(CROW_THREADS)
+contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, ContractSrc src,
+                          const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
+                          int32_t *__restrict__ ucnt, int kbits)
+{
+    extern __shared__ unsigned long long dsm[];
+    unsigned long long *A = dsm, *B = dsm + CROW_MAX;
+    int32_t *hist = (int32_t *)(dsm + 2 * CROW_MAX);
+    __shared__ int32_t s_scan[CROW_THREADS / 32 + 2];
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t c = list[li];
-        int32_t v, u, lv, len;
-        src.row(c, v, u, lv, len);
-        // table sized to the row: H = pow2 >= 2 len (load factor <= 1/2)
-        int H = 64;
-        while (H < 2 * len) H <<= 1;
-        for (int i = threadIdx.x; i < H; i += NT) { hk[i] = hp::KEY_NONE; hw[i] = 0; }
+        RowInfo r;
+        int32_t len;
+        src.row(c, r, len);
+        const int N = group_gather_row<CROW_THREADS>(src, c, r, len, A, s_scan);
+        group_radix_sort<CROW_THREADS>(A, B, N, kbits, hist, s_scan);
+        const int32_t off = toff[c];
+        const int U = group_merge_emit<CROW_THREADS>(A, N, tk + off, tw + off, (uint32_t *)B, s_scan);
+        if (threadIdx.x == 0) ucnt[c] = U;
         __syncthreads();
-        for (int32_t i = threadIdx.x; i < len; i += NT) {
-            int32_t k, w;
-            src.get(c, v, u, lv, i, k, w);
-            if (k == hp::KEY_NONE) continue;
-            uint32_t h = ((uint32_t)k * 2654435761u) & (H - 1);
-            for (;;) {
-                int32_t prev = atomicCAS(&hk[h], hp::KEY_NONE, k);
-                if (prev == hp::KEY_NONE || prev == k) { atomicAdd(&hw[h], w); break; }
-                h = (h + 1) & (H - 1);
-            }
-        }
-        __syncthreads();
-        // compact occupied slots; thread t owns slots [t*per, (t+1)*per)
-        const int per = (H + NT - 1) / NT;
-        const int lo = threadIdx.x * per, hi = min(lo + per, H);
-        int cntl = 0;
-        for (int i = lo; i < hi; i++) cntl += hk[i] != hp::KEY_NONE;
-        int U;
-        int pos = hp::block_excl_scan<NT>(cntl, &U, s_scan);
-        for (int i = lo; i < hi; i++)
-            if (hk[i] != hp::KEY_NONE) { sk[pos] = hk[i]; sw[pos] = hw[i]; pos++; }
-        int P = 32;
-        while (P < U) P <<= 1;
-        for (int i = U + threadIdx.x; i < P; i += NT) { sk[i] = hp::KEY_NONE; sw[i] = 0; }
-        __syncthreads();
-        int32_t off = toff[c];
-        int tot = hp::block_aggregate_smem<NT, HCAP / 2>(sk, sw, P, tk + off, tw + off, s_scan);
-        if (threadIdx.x == 0) ucnt[c] = tot;
     }
 }
 
-constexpr size_t hash_smem(int hcap) { return sizeof(int32_t) * (size_t)(3 * hcap); }
+constexpr size_t cta_radix_smem() { return sizeof(unsigned long long) * 2 * CROW_MAX + sizeof(int32_t) * 256 * (CROW_THREADS / 32); }
+
 
 // Rows longer than 4096 entries: dense accumulator over the coarse id space in
 // a per-CTA global slab (dw: cn ints, bm: cn/32 words; zero on entry/exit).
@@ -447,11 +799,12 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t c = list[li];
-        int32_t v, u, lv, len;
-        src.row(c, v, u, lv, len);
+        RowInfo r;
+        int32_t len;
+        src.row(c, r, len);
         for (int32_t i = threadIdx.x; i < len; i += NT) {
             int32_t k, w;
-            src.get(c, v, u, lv, i, k, w);
+            src.get(c, r, i, k, w);
             if (k == hp::KEY_NONE) continue;
             atomicAdd(&dw[k], w);
             atomicOr(&bm[k >> 5], 1u << (k & 31));
@@ -460,35 +813,6 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
         int32_t off = toff[c];
         int tot = hp::dense_extract<NT>(dw, bm, cn, tk + off, tw + off, s_scan);
         if (threadIdx.x == 0) ucnt[c] = tot;
-    }
-}
-
-// Compacts the unique coarse rows (at upper-bound offsets toff[c]) to their
-// final places cxadj[c]: edge-parallel over the coarse adjacency in tiles of
-// 256 x 32 entries; the owner of an entry is found by binary search over cxadj
-// and a forward walk, so long rows cost their length, not one warp's time.
-__global__ void __launch_bounds__(256)
-copy_rows_kernel(int32_t cn, const int32_t *__restrict__ toff, const int32_t *__restrict__ cxadj,
-                 const int32_t *__restrict__ tk, const int32_t *__restrict__ tw,
-                 int32_t *__restrict__ cadjncy, int32_t *__restrict__ cadjwgt)
-{
-    const int64_t mc = cxadj[cn];
-    const int64_t tile = 256 * 32;
-    for (int64_t tb = blockIdx.x * tile; tb < mc; tb += (int64_t)gridDim.x * tile) {
-        int64_t j = tb + threadIdx.x;
-        if (j >= mc) continue;
-        int32_t lo = 0, hi = cn - 1;
-        while (lo < hi) {
-            int32_t mid = (int32_t)(((int64_t)lo + hi + 1) / 2);
-            if (cxadj[mid] <= j) lo = mid; else hi = mid - 1;
-        }
-        int32_t c = lo;
-        for (int k = 0; k < 32 && j < mc; k++, j += 256) {
-            while (cxadj[c + 1] <= j) c++;
-            const int64_t src = toff[c] + (j - cxadj[c]);
-            cadjncy[j] = tk[src];
-            cadjwgt[j] = tw[src];
-        }
     }
 }
 
@@ -599,71 +923,92 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     cg.n = cn;
     cg.xadj = lalloc_t<int32_t>(c, cn + 1);
     cg.vwgt = lalloc_t<int32_t>(c, cn);
+    // coarse adjacency at the low end with the fine entry count as capacity (an
+    // upper bound); the unused tail of the weights is released once m_c is known
+    const int64_t cap = std::max<int64_t>(g.m, 1);
+    cg.adjncy = lalloc_t<int32_t>(c, cap);
+    cg.adjwgt = lalloc_t<int32_t>(c, cap);
     HP_CHECK_OOM(c);
     const size_t mark = c->hi;
-    int32_t *leader_of = ralloc_t<int32_t>(c, cn);
-    int32_t *toff = ralloc_t<int32_t>(c, cn + 1);
-    int32_t *ucnt = ralloc_t<int32_t>(c, cn + 1);
+    int4 *rinfo = ralloc_t<int4>(c, cn);
+    int32_t *toff = ralloc_t<int32_t>(c, (int64_t)cn + 1);
+    int32_t *ucnt = ralloc_t<int32_t>(c, (int64_t)cn + 1);
     int32_t *lists = ralloc_t<int32_t>(c, 3 * (int64_t)cn);
+    const int64_t ntiles = ((int64_t)cn + ASM_TILE - 1) / ASM_TILE;
+    unsigned long long *tstat = ralloc_t<unsigned long long>(c, ntiles + 1);
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 4, c->stream));
-    int32_t *counts = (int32_t *)sc;          // 3 class counts (+ maxlen) packed in 2 slots
+    int32_t *counts = (int32_t *)sc;          // 3 long-row class counts + max length in slots 0-1
     int32_t *maxlen = counts + 3;
+    unsigned long long *long_total = &sc[2];  // entries of the long rows
+    int32_t *small_max = (int32_t *)&sc[3];   // longest short row above 8 entries (0: none)
 
     int tok = hp_prof_begin(c);
-    HP_LAUNCH(c, coarse_setup_kernel, blocks_for(n), 256, 0, n, g.match, g.cmap, g.xadj, g.vwgt,
-              leader_of, cg.vwgt, toff, lists, counts, cn, maxlen);
-    HP_TRY(hp_scan_excl(c, toff, toff, cn));
+    HP_LAUNCH(c, coarse_setup_kernel, blocks_for(n), 256, 0, n, g.match, g.cmap, g.xadj, g.vwgt, rinfo, cg.vwgt,
+              toff, lists, counts, cn, maxlen, long_total, small_max);
     hp_prof_end(c, tok, HP_PROF_CONTRACT, 0);
-    struct { int32_t cnt[3]; int32_t maxlen; } h;
-    HP_TRY(hp_read_scalars(c, counts, sizeof(h), &h));
-    int32_t tm = 0;
-    HP_TRY(hp_read_scalars(c, toff + cn, sizeof(int32_t), &tm));
-
-    int32_t *tk = ralloc_t<int32_t>(c, tm);
-    int32_t *tw = ralloc_t<int32_t>(c, tm);
-    HP_CHECK_OOM(c);
-    ContractSrc src{g.xadj, g.adjncy, g.adjwgt, g.cmap, g.match, leader_of};
+    struct { int32_t cnt[3]; int32_t maxlen; unsigned long long total; int32_t small_max, pad; } h;
+    HP_TRY(hp_read_scalars(c, sc, sizeof(h), &h));
+    const bool any_long = h.cnt[0] + h.cnt[1] + h.cnt[2] > 0;
+    ContractSrc src{rinfo, g.adjncy, g.adjwgt, g.cmap};
+    int32_t *tk = nullptr, *tw = nullptr;
     tok = hp_prof_begin(c);
-    HP_LAUNCH(c, contract_warp_kernel, blocks_for((int64_t)cn * 32), 256, 0, cn, src, toff, tk, tw,
-              ucnt);
-    if (h.cnt[0] > 0)
-        HP_LAUNCH(c, (contract_hash_kernel<128, 1024>), (unsigned)std::min<int64_t>(h.cnt[0], c->sm_count * 16),
-                  128, hash_smem(1024), lists, &counts[0], src, toff, tk, tw, ucnt);
-    if (h.cnt[1] > 0)
-        HP_LAUNCH(c, (contract_hash_kernel<512, 8192>), (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 2),
-                  512, hash_smem(8192), lists + cn, &counts[1], src, toff, tk, tw, ucnt);
-    if (h.cnt[2] > 0) {
-        // slab per CTA: cn ints + cn/32 words; bounded to ~512 MB
-        int64_t slab = (int64_t)cn * 4 + ((int64_t)cn + 31) / 32 * 4;
-        int64_t nb = std::min<int64_t>(h.cnt[2], 2 * (int64_t)c->sm_count);
-        nb = std::max<int64_t>(1, std::min<int64_t>(nb, (512ll << 20) / std::max<int64_t>(slab, 1)));
-        int32_t *sw = ralloc_t<int32_t>(c, nb * (int64_t)cn);
-        unsigned *sbm = ralloc_t<unsigned>(c, nb * (((int64_t)cn + 31) / 32));
+    if (any_long) {
+        // long rows: aggregated into a temporary buffer (offsets by a scan of
+        // their lengths), unique counts in ucnt
+        HP_TRY(hp_scan_excl(c, toff, toff, cn));
+        tk = ralloc_t<int32_t>(c, (int64_t)h.total);
+        tw = ralloc_t<int32_t>(c, (int64_t)h.total);
         HP_CHECK_OOM(c);
-        HP_CUDA(cudaMemsetAsync(sw, 0, sizeof(int32_t) * (size_t)(nb * cn), c->stream));
-        HP_CUDA(cudaMemsetAsync(sbm, 0, sizeof(unsigned) * (size_t)(nb * ((cn + 31) / 32)), c->stream));
-        HP_LAUNCH(c, contract_dense_kernel<1024>, (unsigned)nb, 1024, 0, lists + 2 * (int64_t)cn,
-                  &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm);
+        int kbits = 0;   // key bits of the coarse ids (< cn)
+        while ((1ll << kbits) < (int64_t)cn) kbits++;
+        if (h.cnt[0] > 0)
+            HP_LAUNCH(c, contract_warp_radix_kernel,
+                      (unsigned)std::min<int64_t>((h.cnt[0] + WROW_WARPS - 1) / WROW_WARPS, c->sm_count * 6),
+                      32 * WROW_WARPS, 0, lists, &counts[0], src, toff, tk, tw, ucnt, kbits);
+        if (h.cnt[1] > 0)
+            HP_LAUNCH(c, contract_cta_radix_kernel, (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 3),
+                      CROW_THREADS, cta_radix_smem(), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits);
+        if (h.cnt[2] > 0) {
+            // slab per CTA: cn ints + cn/32 words; bounded to ~512 MB
+            int64_t slab = (int64_t)cn * 4 + ((int64_t)cn + 31) / 32 * 4;
+            int64_t nb = std::min<int64_t>(h.cnt[2], 2 * (int64_t)c->sm_count);
+            nb = std::max<int64_t>(1, std::min<int64_t>(nb, (512ll << 20) / std::max<int64_t>(slab, 1)));
+            int32_t *sw = ralloc_t<int32_t>(c, nb * (int64_t)cn);
+            unsigned *sbm = ralloc_t<unsigned>(c, nb * (((int64_t)cn + 31) / 32));
+            HP_CHECK_OOM(c);
+            HP_CUDA(cudaMemsetAsync(sw, 0, sizeof(int32_t) * (size_t)(nb * cn), c->stream));
+            HP_CUDA(cudaMemsetAsync(sbm, 0, sizeof(unsigned) * (size_t)(nb * ((cn + 31) / 32)), c->stream));
+            HP_LAUNCH(c, contract_dense_kernel<1024>, (unsigned)nb, 1024, 0, lists + 2 * (int64_t)cn,
+                      &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm);
+        }
     }
-    HP_TRY(hp_scan_excl(c, ucnt, cg.xadj, cn));
+    // short rows + coarse xadj in one ordered pass, then the long rows' copies
+    HP_CUDA(cudaMemsetAsync(tstat, 0, sizeof(unsigned long long) * (size_t)(ntiles + 1), c->stream));
+    if (h.small_max <= 8)
+        HP_LAUNCH(c, contract_assemble_kernel<8>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
+                  cg.adjncy, cg.adjwgt, tstat, (unsigned *)(tstat + ntiles), c->d_status);
+    else if (h.small_max <= 16)
+        HP_LAUNCH(c, contract_assemble_kernel<16>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
+                  cg.adjncy, cg.adjwgt, tstat, (unsigned *)(tstat + ntiles), c->d_status);
+    else
+        HP_LAUNCH(c, contract_assemble_kernel<32>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
+                  cg.adjncy, cg.adjwgt, tstat, (unsigned *)(tstat + ntiles), c->d_status);
+    if (any_long)
+        HP_LAUNCH(c, copy_long_rows_kernel,
+                  std::min<unsigned>(blocks_for((int64_t)(h.cnt[0] + h.cnt[1] + h.cnt[2]) * 32), c->sm_count * 16),
+                  256, 0, lists, counts, cn, toff, ucnt, cg.xadj, tk, tw, cg.adjncy, cg.adjwgt);
     hp_prof_end(c, tok, HP_PROF_CONTRACT, 0);
     int32_t mc = 0;
     HP_TRY(hp_read_scalars(c, cg.xadj + cn, sizeof(int32_t), &mc));
+    // algorithmic bytes of the whole contraction: fine CSR, cmap, match, vwgt in;
+    // coarse xadj, adjacency, weights, vertex weights out
+    hp_prof_add_bytes(c, tok, 4 * ((int64_t)n + 1) + 8 * g.m + 12 * (int64_t)n + 4 * ((int64_t)cn + 1) +
+                                  8 * (int64_t)mc + 4 * (int64_t)cn);
+    if (mc < 0 || mc > cap) return HP_ERR_INTERNAL;
     cg.m = mc;
-    // the coarse adjacency goes to the low end; temporaries stay on the high end
-    cg.adjncy = lalloc_t<int32_t>(c, mc);
-    cg.adjwgt = lalloc_t<int32_t>(c, mc);
-    HP_CHECK_OOM(c);
-    tok = hp_prof_begin(c);
-    HP_LAUNCH(c, copy_rows_kernel, std::min<unsigned>(blocks_for(((int64_t)mc + 31) / 32), c->sm_count * 16), 256,
-              0, cn, toff, cg.xadj, tk, tw, cg.adjncy, cg.adjwgt);
-    // algorithmic bytes of the whole contraction: fine CSR, cmap, match,
-    // vwgt in; coarse xadj, adjacency, weights, vertex weights out
-    hp_prof_end(c, tok, HP_PROF_CONTRACT,
-                4 * ((int64_t)n + 1) + 8 * g.m + 12 * (int64_t)n + 4 * ((int64_t)cn + 1) + 8 * (int64_t)mc +
-                    4 * (int64_t)cn);
+    c->lo = (size_t)((char *)cg.adjwgt - c->arena) + ((size_t)std::max<int64_t>(mc, 1) * 4 + HP_ALIGN - 1) / HP_ALIGN * HP_ALIGN;
     c->hi = mark;
     return HP_OK;
 }
@@ -672,8 +1017,8 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
 
 int hp_coarsen_init()
 {
-    HP_CUDA(cudaFuncSetAttribute(contract_hash_kernel<512, 8192>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)hash_smem(8192)));
+    HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_radix_smem()));
     return HP_OK;
 }
 

@@ -108,6 +108,59 @@ __device__ __forceinline__ void block_add_to(long long v, unsigned long long *ou
     }
 }
 
+// Decoupled look-back (single-pass scan across CTAs).  tile_status[t] holds
+// flag << 32 | value: flag 1 = the tile's own aggregate, flag 2 = its inclusive
+// prefix.  Called by all 32 lanes of one warp of tile `tile` with the tile's
+// aggregate; publishes it, walks back over predecessors 32 at a time until an
+// inclusive prefix is found, publishes its own inclusive prefix and returns the
+// exclusive prefix (same value in every lane).  Tiles must be taken in launch
+// order (a dynamic tile counter), so every predecessor is running or done.  Each
+// wait is bounded by HP_SPIN_LIMIT; on expiry HP_STATUS_SPIN_TIMEOUT is set in
+// *status and the predecessor counts as zero, so the kernel always finishes.
+constexpr unsigned long long LB_FLAG_AGG = 1ull << 32;
+constexpr unsigned long long LB_FLAG_PRE = 2ull << 32;
+
+__device__ __forceinline__ int32_t lookback_exclusive(unsigned long long *tile_status, int64_t tile, int32_t agg,
+                                                      unsigned *status)
+{
+    const int lane = threadIdx.x & 31;
+    if (tile == 0) {
+        if (lane == 0) atomicExch(&tile_status[0], LB_FLAG_PRE | (unsigned)agg);
+        return 0;
+    }
+    if (lane == 0) atomicExch(&tile_status[tile], LB_FLAG_AGG | (unsigned)agg);
+    int32_t excl = 0;
+    int64_t pred = tile - 1;
+    for (;;) {
+        const int64_t idx = pred - lane;
+        unsigned long long st = LB_FLAG_PRE;  // virtual prefix 0 before tile 0
+        if (idx >= 0) {
+            unsigned it = 0;
+            for (;;) {
+                st = *(volatile unsigned long long *)&tile_status[idx];
+                if (st >> 32) break;
+                if (++it > HP_SPIN_LIMIT) {
+                    atomicOr(status, HP_STATUS_SPIN_TIMEOUT);
+                    st = LB_FLAG_PRE;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        const unsigned pre_mask = __ballot_sync(HP_FULL_MASK, (st >> 32) == 2);
+        const int32_t val = (int32_t)(unsigned)(st & 0xffffffffull);
+        if (pre_mask) {
+            const int first = __ffs(pre_mask) - 1;
+            excl += warp_sum(lane <= first ? val : 0);
+            break;
+        }
+        excl += warp_sum(val);
+        pred -= 32;
+    }
+    if (lane == 0) atomicExch(&tile_status[tile], LB_FLAG_PRE | (unsigned)(excl + agg));
+    return excl;
+}
+
 __host__ __device__ __forceinline__ int64_t iabs64(int64_t x) { return x < 0 ? -x : x; }
 
 // Weak-rebalance gain bucket with the float semantics of the reference's

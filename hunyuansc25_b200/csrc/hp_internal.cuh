@@ -110,6 +110,8 @@ template <class T> inline T *ralloc_t(hp_context *c, int64_t n) { return (T *)hp
 // Usage: int t = hp_prof_begin(c); ...launches...; hp_prof_end(c, t, HP_PROF_X, bytes);
 int hp_prof_begin(hp_context *c);
 void hp_prof_end(hp_context *c, int token, int cls, int64_t bytes);
+// Algorithmic bytes of an interval that are known only after it was closed.
+void hp_prof_add_bytes(hp_context *c, int token, int64_t bytes);
 void hp_prof_resolve(hp_context *c);
 
 // Blocking read of nbytes from device into the pinned mirror, then dst.

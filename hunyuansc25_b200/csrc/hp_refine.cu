@@ -1294,9 +1294,15 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
     HP_CUDA(cudaMemcpyAsync(d_opt, h_opt, sizeof(int64_t) * nparts, cudaMemcpyHostToDevice, c->stream));
     HP_CUDA(cudaMemcpyAsync(d_maxp, h_maxp, sizeof(int64_t) * nparts, cudaMemcpyHostToDevice, c->stream));
     const bool trace = c->opt.trace != 0;
+    // HP_DEBUG_LEVELS: per-level size, passes and device time on stderr
+    const bool dbg_levels = getenv("HP_DEBUG_LEVELS") != nullptr;
+    cudaEvent_t lev[2] = {nullptr, nullptr};
+    if (dbg_levels)
+        for (auto &e : lev) HP_CUDA(cudaEventCreate(&e));
     int total_passes = 0;
     for (int l = L; l >= 0; l--) {
         HpLevel &g = c->levels[l];
+        if (dbg_levels) HP_CUDA(cudaEventRecord(lev[0], c->stream));
         if (l < L)
             HP_LAUNCH(c, project_kernel, nblk(g.n), 256, 0, g.n, g.cmap, c->levels[l + 1].where, g.where);
         if (trace) {
@@ -1308,9 +1314,18 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
         int passes = 0;
         HP_TRY(refine_level(c, g, nparts, l == 0, d_opt, d_maxp, &g.cut_start, &g.cut_final, &passes));
         total_passes += passes;
+        if (dbg_levels) {
+            HP_CUDA(cudaEventRecord(lev[1], c->stream));
+            HP_CUDA(cudaEventSynchronize(lev[1]));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, lev[0], lev[1]);
+            fprintf(stderr, "gpu level %d n=%d m=%lld passes=%d ms=%.3f\n", l, g.n, (long long)g.m, passes, ms);
+        }
         if (trace)
             HP_CUDA(cudaMemcpyAsync(g.where_final, g.where, sizeof(int32_t) * g.n, cudaMemcpyDeviceToDevice, c->stream));
     }
+    for (auto e : lev)
+        if (e) cudaEventDestroy(e);
     c->stats.refine_passes = total_passes;
     return HP_OK;
 }

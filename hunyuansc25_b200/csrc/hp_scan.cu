@@ -18,8 +18,6 @@ namespace {
 constexpr int SCAN_BLOCK = 256;
 constexpr int SCAN_ITEMS = 16;
 constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;  // 4096
-constexpr unsigned long long FLAG_AGG = 1ull << 32;
-constexpr unsigned long long FLAG_PRE = 2ull << 32;
 
 __device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
 
@@ -62,42 +60,7 @@ scan_excl_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int6
         int32_t ti = hp::warp_incl_scan(t);
         if (lane < SCAN_BLOCK / 32) s_warp[lane] = ti - t;  // exclusive warp offsets
         int32_t agg = __shfl_sync(HP_FULL_MASK, ti, SCAN_BLOCK / 32 - 1);
-        // look-back
-        int32_t excl = 0;
-        if (tile == 0) {
-            if (lane == 0) atomicExch(&tile_status[0], FLAG_PRE | (unsigned)agg);
-        } else {
-            if (lane == 0) atomicExch(&tile_status[tile], FLAG_AGG | (unsigned)agg);
-            int64_t pred = tile - 1;
-            for (;;) {
-                int64_t idx = pred - lane;
-                unsigned long long st = FLAG_PRE;  // virtual prefix 0 before tile 0
-                if (idx >= 0) {
-                    unsigned it = 0;
-                    for (;;) {
-                        st = *(volatile unsigned long long *)&tile_status[idx];
-                        if (st >> 32) break;
-                        if (++it > HP_SPIN_LIMIT) {
-                            atomicOr(status, HP_STATUS_SPIN_TIMEOUT);
-                            st = FLAG_PRE;
-                            break;
-                        }
-                        __nanosleep(32);
-                    }
-                }
-                unsigned pre_mask = __ballot_sync(HP_FULL_MASK, (st >> 32) == 2);
-                int32_t val = (int32_t)(unsigned)(st & 0xffffffffull);
-                if (pre_mask) {
-                    int first = __ffs(pre_mask) - 1;
-                    int32_t contrib = lane <= first ? val : 0;
-                    excl += hp::warp_sum(contrib);
-                    break;
-                }
-                excl += hp::warp_sum(val);
-                pred -= 32;
-            }
-            if (lane == 0) atomicExch(&tile_status[tile], FLAG_PRE | (unsigned)(excl + agg));
-        }
+        const int32_t excl = hp::lookback_exclusive(tile_status, tile, agg, status);
         if (lane == 0) s_excl = excl;
     }
     __syncthreads();
