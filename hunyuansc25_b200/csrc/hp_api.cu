@@ -320,6 +320,23 @@ void hp_prof_resolve(hp_context *c)
 }
 
 // ---- shared helpers -------------------------------------------------------------
+int hp_lb_reserve(hp_context *c, int64_t tiles)
+{
+    if (tiles <= c->lb_cap && c->lb_ctl) return HP_OK;
+    // between calls: nothing of this context is in flight
+    HP_CUDA(cudaStreamSynchronize(c->stream));
+    const int64_t cap = std::max<int64_t>(tiles, std::max<int64_t>(2 * c->lb_cap, 4096));
+    if (c->lb_status) cudaFree(c->lb_status);
+    c->lb_status = nullptr;
+    c->lb_cap = 0;
+    HP_CUDA(cudaMalloc((void **)&c->lb_status, sizeof(unsigned long long) * (size_t)cap));
+    HP_CUDA(cudaMemset(c->lb_status, 0, sizeof(unsigned long long) * (size_t)cap));
+    if (!c->lb_ctl) HP_CUDA(cudaMalloc((void **)&c->lb_ctl, sizeof(hp::LbCtl)));
+    HP_CUDA(cudaMemset(c->lb_ctl, 0, sizeof(hp::LbCtl)));
+    c->lb_cap = cap;
+    return HP_OK;
+}
+
 int hp_read_scalars(hp_context *c, const void *d_src, size_t nbytes, void *dst)
 {
     if (nbytes > sizeof(long long) * HP_NSCAL) return HP_ERR_INVALID_ARG;
@@ -441,6 +458,8 @@ HP_API void hp_context_destroy(hp_context *c)
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->arena) cudaFree(c->arena);
     if (c->d_status) cudaFree(c->d_status);
+    if (c->lb_status) cudaFree(c->lb_status);
+    if (c->lb_ctl) cudaFree(c->lb_ctl);
     if (c->h_pin) cudaFreeHost(c->h_pin);
     for (int i = 0; i < 8; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -495,6 +514,9 @@ static int partition_common(hp_context *c, int32_t n, int64_t m, const int32_t *
                             int32_t nparts, const float *tpwgts, float ubfactor, bool host,
                             int32_t *part, int64_t *edgecut)
 {
+    // look-back tiles of every single-pass kernel of the call: at most one per
+    // 256 vertices (the smallest tile), plus the scans' slack
+    HP_TRY(hp_lb_reserve(c, ((int64_t)n + 255) / 256 + 1024));
     size_t want = estimate_arena(n, m);
     int rc = HP_ERR_NOMEM;
     for (int attempt = 0; attempt < 4 && rc == HP_ERR_NOMEM; attempt++) {
@@ -684,6 +706,7 @@ HP_API int hp_scan_exclusive_i32(hp_context *ctx, const int32_t *d_in, int32_t *
     size_t need = (size_t)((n + 4096) / 4096 + 2) * 8 + ((size_t)1 << 20);
     if (!ctx->arena || ctx->arena_cap < need) HP_TRY(ensure_arena(ctx, std::max(need, (size_t)64 << 20)));
     reset_arena(ctx);
+    HP_TRY(hp_lb_reserve(ctx, (n + 4096) / 4096 + 2));
     unsigned zero = 0;
     HP_CUDA(cudaMemcpyAsync(ctx->d_status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
     HP_TRY(hp_scan_excl(ctx, d_in, d_out, n));

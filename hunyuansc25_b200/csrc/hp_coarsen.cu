@@ -415,38 +415,13 @@ struct ContractSrc {
 };
 
 // ---- short rows: one thread per coarse row, aggregation in registers ------------
-// Entries are packed as key << 32 | weight (keys are coarse ids < 2^31, the
-// dropped self key and padding are KEY_NONE), sorted ascending by a bitonic
-// network over the first NET of 32 registers (compile-time indices only), and
-// equal keys are merged by summing the low halves.
-template <int NET, int XN>
-__device__ __forceinline__ void sort_regs(unsigned long long (&x)[XN])
-{
-#pragma unroll
-    for (int size = 2; size <= NET; size <<= 1)
-#pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1)
-#pragma unroll
-            for (int i = 0; i < NET; i++) {
-                const int j = i ^ stride;
-                if (j > i) {
-                    const unsigned long long a = x[i], b = x[j];
-                    const unsigned long long lo = a < b ? a : b, hi = a < b ? b : a;
-                    if ((i & size) == 0) { x[i] = lo; x[j] = hi; }
-                    else { x[i] = hi; x[j] = lo; }
-                }
-            }
-}
-
-constexpr unsigned long long PACK_NONE = (unsigned long long)(uint32_t)hp::KEY_NONE << 32;
-
 template <int NET, int XN>
 __device__ __forceinline__ int gather_sort_row(const ContractSrc &src, int32_t c, const RowInfo &r, int32_t len,
                                                unsigned long long (&x)[XN])
 {
 #pragma unroll
     for (int i = 0; i < NET; i++) {
-        unsigned long long e = PACK_NONE;
+        unsigned long long e = hp::PACK_NONE;
         if (i < len) {
             int32_t k, w;
             src.get(c, r, i, k, w);
@@ -454,7 +429,7 @@ __device__ __forceinline__ int gather_sort_row(const ContractSrc &src, int32_t c
         }
         x[i] = e;
     }
-    sort_regs<NET, XN>(x);
+    hp::sort_regs<NET, XN>(x);
     int u = 0;
 #pragma unroll
     for (int i = 0; i < NET; i++) {
@@ -505,14 +480,14 @@ template <int XN>
 __global__ void __launch_bounds__(ASM_TILE)
 contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict__ ucnt,
                          int32_t *__restrict__ cxadj, int32_t *__restrict__ cadjncy,
-                         int32_t *__restrict__ cadjwgt, unsigned long long *tile_status,
-                         unsigned *tile_counter, unsigned *status)
+                         int32_t *__restrict__ cadjwgt, unsigned long long *tile_status, hp::LbCtl *lb,
+                         unsigned *status)
 {
     __shared__ int32_t s_scan[ASM_TILE / 32 + 2];
-    __shared__ int32_t s_tile, s_excl;
-    if (threadIdx.x == 0) s_tile = (int32_t)atomicAdd(tile_counter, 1u);
-    __syncthreads();
-    const int64_t tile = s_tile;
+    __shared__ int32_t s_excl;
+    int64_t tile;
+    unsigned epoch;
+    hp::lb_begin(lb, &tile, &epoch);
     const int32_t c = (int32_t)(tile * ASM_TILE + threadIdx.x);
     RowInfo r{0, 0, 0, 0};
     int32_t len = 0;
@@ -532,7 +507,7 @@ contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict_
     int agg;
     const int local = hp::block_excl_scan<ASM_TILE>(u, &agg, s_scan);
     if (threadIdx.x < 32) {
-        const int32_t excl = hp::lookback_exclusive(tile_status, tile, agg, status);
+        const int32_t excl = hp::lookback_epoch(tile_status, tile, agg, epoch, status);
         if (threadIdx.x == 0) s_excl = excl;
     }
     __syncthreads();
@@ -546,25 +521,29 @@ contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict_
         else if (XN == 16 || wmax <= 16) emit_row<(XN < 16 ? XN : 16), XN>(x, cadjncy + off, cadjwgt + off);
         else emit_row<XN, XN>(x, cadjncy + off, cadjwgt + off);
     }
+    hp::lb_end(lb);
 }
 
 // Long rows (aggregated into the temporary buffer at toff[c]) to their final
-// place cxadj[c]: one warp per row, coalesced.
+// place cxadj[c], coalesced: a warp per row for the warp class (list 0), a CTA
+// per row for the longer classes (lists 1 and 2).
+template <bool CTA>
 __global__ void __launch_bounds__(256)
 copy_long_rows_kernel(const int32_t *__restrict__ lists, const int32_t *__restrict__ counts, int32_t cn,
                       const int32_t *__restrict__ toff, const int32_t *__restrict__ ucnt,
                       const int32_t *__restrict__ cxadj, const int32_t *__restrict__ tk,
                       const int32_t *__restrict__ tw, int32_t *__restrict__ cadjncy, int32_t *__restrict__ cadjwgt)
 {
-    const int lane = threadIdx.x & 31;
-    const int64_t total = (int64_t)counts[0] + counts[1] + counts[2];
-    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < total;
-         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int cls = i < counts[0] ? 0 : (i < (int64_t)counts[0] + counts[1] ? 1 : 2);
-        const int64_t pos = cls == 0 ? i : (cls == 1 ? i - counts[0] : i - counts[0] - counts[1]);
-        const int32_t c = lists[(int64_t)cls * cn + pos];
+    const int lane = CTA ? threadIdx.x : (threadIdx.x & 31);
+    const int width = CTA ? blockDim.x : 32;
+    const int64_t total = CTA ? (int64_t)counts[1] + counts[2] : (int64_t)counts[0];
+    const int64_t first = CTA ? blockIdx.x : (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t step = CTA ? gridDim.x : ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i = first; i < total; i += step) {
+        const int64_t slot = CTA ? (i < counts[1] ? (int64_t)cn + i : 2 * (int64_t)cn + (i - counts[1])) : i;
+        const int32_t c = lists[slot];
         const int32_t src = toff[c], dst = cxadj[c], cnt = ucnt[c];
-        for (int32_t j = lane; j < cnt; j += 32) {
+        for (int32_t j = lane; j < cnt; j += width) {
             cadjncy[dst + j] = tk[src + j];
             cadjwgt[dst + j] = tw[src + j];
         }
@@ -610,6 +589,51 @@ __device__ __forceinline__ int group_excl_scan(int v, int *total, int32_t *s_sca
     *total = s_scan[G / 32];
     __syncthreads();
     return r;
+}
+
+// Two exclusive scans across a group in one pass (a: int, b: wrapping uint32).
+template <int G>
+__device__ __forceinline__ void group_excl_scan2(int a, uint32_t b, int *ea, uint32_t *eb, int *ta,
+                                                 int32_t *s_scan /* 2 * (G/32) + 2 */)
+{
+    const int lane = threadIdx.x & 31;
+    int ia = a;
+    uint32_t ib = b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int xa = __shfl_up_sync(HP_FULL_MASK, ia, o);
+        const uint32_t xb = __shfl_up_sync(HP_FULL_MASK, ib, o);
+        if (lane >= o) { ia += xa; ib += xb; }
+    }
+    if (G == 32) {
+        *ta = __shfl_sync(HP_FULL_MASK, ia, 31);
+        *ea = ia - a;
+        *eb = ib - b;
+        return;
+    }
+    constexpr int W = G / 32;
+    const int wid = (threadIdx.x % G) >> 5;
+    if (lane == 31) { s_scan[wid] = ia; s_scan[W + wid] = (int32_t)ib; }
+    __syncthreads();
+    if (wid == 0) {
+        int t = lane < W ? s_scan[lane] : 0;
+        uint32_t u = lane < W ? (uint32_t)s_scan[W + lane] : 0u;
+        int ti = t;
+        uint32_t ui = u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int xa = __shfl_up_sync(HP_FULL_MASK, ti, o);
+            const uint32_t xb = __shfl_up_sync(HP_FULL_MASK, ui, o);
+            if (lane >= o) { ti += xa; ui += xb; }
+        }
+        if (lane < W) { s_scan[lane] = ti - t; s_scan[W + lane] = (int32_t)(ui - u); }
+        if (lane == W - 1) s_scan[2 * W] = ti;
+    }
+    __syncthreads();
+    *ea = s_scan[wid] + ia - a;
+    *eb = (uint32_t)s_scan[W + wid] + ib - b;
+    *ta = s_scan[2 * W];
+    __syncthreads();
 }
 
 // Sorts A[0..N) (result in A; B is scratch of the same size); hist holds
@@ -680,10 +704,11 @@ __device__ int group_merge_emit(const unsigned long long *A, int N, int32_t *out
         heads += (i == 0 || (uint32_t)(A[i] >> 32) != (uint32_t)(A[i - 1] >> 32));
         wsum += (uint32_t)A[i];
     }
-    int U;
-    int o = group_excl_scan<G>(heads, &U, s_scan) - 1;   // ordinal of the current run
-    int dummy;
-    uint32_t p = (uint32_t)group_excl_scan<G>((int)wsum, &dummy, s_scan);   // weights before lo
+    int o0, U;
+    uint32_t p0;
+    group_excl_scan2<G>(heads, wsum, &o0, &p0, &U, s_scan);
+    int o = o0 - 1;   // ordinal of the current run
+    uint32_t p = p0;  // weights before entry i
     for (int i = lo; i < hi; i++) {
         const uint32_t k = (uint32_t)(A[i] >> 32);
         if (i == 0 || k != (uint32_t)(A[i - 1] >> 32)) {
@@ -695,8 +720,8 @@ __device__ int group_merge_emit(const unsigned long long *A, int N, int32_t *out
     }
     group_sync<G>();
     // second walk: the last entry of every run closes it
-    p = (uint32_t)group_excl_scan<G>((int)wsum, &dummy, s_scan);
-    o = group_excl_scan<G>(heads, &dummy, s_scan) - 1;
+    o = o0 - 1;
+    p = p0;
     for (int i = lo; i < hi; i++) {
         const uint32_t k = (uint32_t)(A[i] >> 32);
         if (i == 0 || k != (uint32_t)(A[i - 1] >> 32)) o++;
@@ -706,25 +731,25 @@ __device__ int group_merge_emit(const unsigned long long *A, int N, int32_t *out
     return U;
 }
 
-// Gathers row c (self key dropped) into A, compacted, in entry order; returns N.
+// Gathers row c into A in entry order; the coarse self key stays in as
+// KEY_NONE (whose low kbits bits exceed every coarse id, so it sorts last) and
+// the count of real entries is returned.
 template <int G>
 __device__ int group_gather_row(const ContractSrc &src, int32_t c, const RowInfo &r, int32_t len,
                                 unsigned long long *A, int32_t *s_scan)
 {
     const int t = threadIdx.x % G;
-    int base = 0;
-    for (int i0 = 0; i0 < len; i0 += G) {
-        const int i = i0 + t;
-        int32_t k = hp::KEY_NONE, w = 0;
-        if (i < len) src.get(c, r, i, k, w);
-        const int keep = k != hp::KEY_NONE;
-        int tot;
-        const int pos = group_excl_scan<G>(keep, &tot, s_scan);
-        if (keep) A[base + pos] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)w;
-        base += tot;
+    int self = 0;
+    for (int i = t; i < len; i += G) {
+        int32_t k, w;
+        src.get(c, r, i, k, w);
+        self += k == hp::KEY_NONE;
+        A[i] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)w;
     }
+    int tot;
+    group_excl_scan<G>(self, &tot, s_scan);
     group_sync<G>();
-    return base;
+    return len - tot;
 }
 
 constexpr int WROW_MAX = 256;    // warp class: 33..256 entries
@@ -747,7 +772,7 @@ contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__re
         int32_t len;
         src.row(c, r, len);
         const int N = group_gather_row<32>(src, c, r, len, sA[wid], nullptr);
-        group_radix_sort<32>(sA[wid], sB[wid], N, kbits, sH[wid], nullptr);
+        group_radix_sort<32>(sA[wid], sB[wid], len, kbits, sH[wid], nullptr);
         const int32_t off = toff[c];
         const int U = group_merge_emit<32>(sA[wid], N, tk + off, tw + off, (uint32_t *)sB[wid], nullptr);
         if ((threadIdx.x & 31) == 0) ucnt[c] = U;
@@ -765,7 +790,7 @@ contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__res
     extern __shared__ unsigned long long dsm[];
     unsigned long long *A = dsm, *B = dsm + CROW_MAX;
     int32_t *hist = (int32_t *)(dsm + 2 * CROW_MAX);
-    __shared__ int32_t s_scan[CROW_THREADS / 32 + 2];
+    __shared__ int32_t s_scan[2 * (CROW_THREADS / 32) + 2];
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t c = list[li];
@@ -773,7 +798,7 @@ contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__res
         int32_t len;
         src.row(c, r, len);
         const int N = group_gather_row<CROW_THREADS>(src, c, r, len, A, s_scan);
-        group_radix_sort<CROW_THREADS>(A, B, N, kbits, hist, s_scan);
+        group_radix_sort<CROW_THREADS>(A, B, len, kbits, hist, s_scan);
         const int32_t off = toff[c];
         const int U = group_merge_emit<CROW_THREADS>(A, N, tk + off, tw + off, (uint32_t *)B, s_scan);
         if (threadIdx.x == 0) ucnt[c] = U;
@@ -791,27 +816,36 @@ __global__ void __launch_bounds__(NT)
 contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                       ContractSrc src, const int32_t *__restrict__ toff, int32_t *__restrict__ tk,
                       int32_t *__restrict__ tw, int32_t *__restrict__ ucnt, int32_t cn,
-                      int32_t *slab_w, unsigned *slab_bm)
+                      int32_t *slab_w, unsigned *slab_bm, unsigned *slab_bm2)
 {
     __shared__ int32_t s_scan[NT / 32 + 2];
     int32_t *dw = slab_w + (int64_t)blockIdx.x * cn;
     unsigned *bm = slab_bm + (int64_t)blockIdx.x * ((cn + 31) / 32);
+    unsigned *bm2 = slab_bm2 + (int64_t)blockIdx.x * ((cn + 1023) / 1024);
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t c = list[li];
         RowInfo r;
         int32_t len;
         src.row(c, r, len);
+        // a row much shorter than the bitmap walks the occupied words through
+        // the second level; a denser row scans the bitmap directly
+        const bool two_level = (int64_t)len * 4 < ((int64_t)cn + 31) / 32;
         for (int32_t i = threadIdx.x; i < len; i += NT) {
             int32_t k, w;
             src.get(c, r, i, k, w);
             if (k == hp::KEY_NONE) continue;
-            atomicAdd(&dw[k], w);
-            atomicOr(&bm[k >> 5], 1u << (k & 31));
+            if (two_level) {
+                hp::dense_mark2(dw, bm, bm2, k, w);
+            } else {
+                atomicAdd(&dw[k], w);
+                atomicOr(&bm[k >> 5], 1u << (k & 31));
+            }
         }
         __syncthreads();
         int32_t off = toff[c];
-        int tot = hp::dense_extract<NT>(dw, bm, cn, tk + off, tw + off, s_scan);
+        int tot = two_level ? hp::dense_extract2<NT>(dw, bm, bm2, cn, tk + off, tw + off, s_scan)
+                            : hp::dense_extract<NT>(dw, bm, cn, tk + off, tw + off, s_scan);
         if (threadIdx.x == 0) ucnt[c] = tot;
     }
 }
@@ -935,7 +969,7 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     int32_t *ucnt = ralloc_t<int32_t>(c, (int64_t)cn + 1);
     int32_t *lists = ralloc_t<int32_t>(c, 3 * (int64_t)cn);
     const int64_t ntiles = ((int64_t)cn + ASM_TILE - 1) / ASM_TILE;
-    unsigned long long *tstat = ralloc_t<unsigned long long>(c, ntiles + 1);
+    if (ntiles > c->lb_cap) return HP_ERR_INTERNAL;   // reserved at the start of every call
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 4, c->stream));
@@ -961,8 +995,10 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
         tk = ralloc_t<int32_t>(c, (int64_t)h.total);
         tw = ralloc_t<int32_t>(c, (int64_t)h.total);
         HP_CHECK_OOM(c);
-        int kbits = 0;   // key bits of the coarse ids (< cn)
-        while ((1ll << kbits) < (int64_t)cn) kbits++;
+        // key bits: 2^kbits > cn, so every coarse id (< cn) is below the low
+        // kbits bits of KEY_NONE and the dropped self key sorts last
+        int kbits = 0;
+        while ((1ll << kbits) <= (int64_t)cn) kbits++;
         if (h.cnt[0] > 0)
             HP_LAUNCH(c, contract_warp_radix_kernel,
                       (unsigned)std::min<int64_t>((h.cnt[0] + WROW_WARPS - 1) / WROW_WARPS, c->sm_count * 6),
@@ -971,33 +1007,38 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
             HP_LAUNCH(c, contract_cta_radix_kernel, (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 3),
                       CROW_THREADS, cta_radix_smem(), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits);
         if (h.cnt[2] > 0) {
-            // slab per CTA: cn ints + cn/32 words; bounded to ~512 MB
-            int64_t slab = (int64_t)cn * 4 + ((int64_t)cn + 31) / 32 * 4;
+            // slab per CTA: cn ints + cn/32 + cn/1024 words; bounded to ~512 MB
+            const int64_t nw = ((int64_t)cn + 31) / 32, nw2 = ((int64_t)cn + 1023) / 1024;
+            int64_t slab = (int64_t)cn * 4 + nw * 4 + nw2 * 4;
             int64_t nb = std::min<int64_t>(h.cnt[2], 2 * (int64_t)c->sm_count);
             nb = std::max<int64_t>(1, std::min<int64_t>(nb, (512ll << 20) / std::max<int64_t>(slab, 1)));
             int32_t *sw = ralloc_t<int32_t>(c, nb * (int64_t)cn);
-            unsigned *sbm = ralloc_t<unsigned>(c, nb * (((int64_t)cn + 31) / 32));
+            unsigned *sbm = ralloc_t<unsigned>(c, nb * nw);
+            unsigned *sbm2 = ralloc_t<unsigned>(c, nb * nw2);
             HP_CHECK_OOM(c);
             HP_CUDA(cudaMemsetAsync(sw, 0, sizeof(int32_t) * (size_t)(nb * cn), c->stream));
-            HP_CUDA(cudaMemsetAsync(sbm, 0, sizeof(unsigned) * (size_t)(nb * ((cn + 31) / 32)), c->stream));
+            HP_CUDA(cudaMemsetAsync(sbm, 0, sizeof(unsigned) * (size_t)(nb * nw), c->stream));
+            HP_CUDA(cudaMemsetAsync(sbm2, 0, sizeof(unsigned) * (size_t)(nb * nw2), c->stream));
             HP_LAUNCH(c, contract_dense_kernel<1024>, (unsigned)nb, 1024, 0, lists + 2 * (int64_t)cn,
-                      &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm);
+                      &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm, sbm2);
         }
     }
     // short rows + coarse xadj in one ordered pass, then the long rows' copies
-    HP_CUDA(cudaMemsetAsync(tstat, 0, sizeof(unsigned long long) * (size_t)(ntiles + 1), c->stream));
     if (h.small_max <= 8)
         HP_LAUNCH(c, contract_assemble_kernel<8>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, tstat, (unsigned *)(tstat + ntiles), c->d_status);
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status);
     else if (h.small_max <= 16)
         HP_LAUNCH(c, contract_assemble_kernel<16>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, tstat, (unsigned *)(tstat + ntiles), c->d_status);
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status);
     else
         HP_LAUNCH(c, contract_assemble_kernel<32>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, tstat, (unsigned *)(tstat + ntiles), c->d_status);
-    if (any_long)
-        HP_LAUNCH(c, copy_long_rows_kernel,
-                  std::min<unsigned>(blocks_for((int64_t)(h.cnt[0] + h.cnt[1] + h.cnt[2]) * 32), c->sm_count * 16),
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status);
+    if (h.cnt[0] > 0)
+        HP_LAUNCH(c, copy_long_rows_kernel<false>, std::min<unsigned>(blocks_for((int64_t)h.cnt[0] * 32),
+                                                                     c->sm_count * 16),
+                  256, 0, lists, counts, cn, toff, ucnt, cg.xadj, tk, tw, cg.adjncy, cg.adjwgt);
+    if (h.cnt[1] + h.cnt[2] > 0)
+        HP_LAUNCH(c, copy_long_rows_kernel<true>, (unsigned)std::min<int64_t>(h.cnt[1] + h.cnt[2], c->sm_count * 8),
                   256, 0, lists, counts, cn, toff, ucnt, cg.xadj, tk, tw, cg.adjncy, cg.adjwgt);
     hp_prof_end(c, tok, HP_PROF_CONTRACT, 0);
     int32_t mc = 0;

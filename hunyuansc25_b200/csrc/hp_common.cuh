@@ -161,6 +161,103 @@ __device__ __forceinline__ int32_t lookback_exclusive(unsigned long long *tile_s
     return excl;
 }
 
+// ---- epoch look-back (no zeroing between uses) ------------------------------------
+// Single-pass kernels of a context share one tile-status region that only they
+// write.  A tile word is epoch (bits 34-63) | flag (bits 32-33: 1 aggregate,
+// 2 inclusive prefix) | value (bits 0-31); a word of another epoch counts as
+// not yet published, so the region never needs clearing.  LbCtl holds the
+// dynamic tile counter, the count of finished CTAs and the current epoch: the
+// last CTA of a launch resets the first two and advances the epoch, so the next
+// launch (stream order) starts clean -- also when both are replayed from a
+// CUDA graph.
+struct LbCtl {
+    unsigned tile_counter, done, epoch, pad;
+};
+
+__device__ __forceinline__ unsigned long long lb_word(unsigned epoch, unsigned flag, int32_t v)
+{
+    return ((unsigned long long)(epoch & 0x3fffffffu) << 34) | ((unsigned long long)flag << 32) | (uint32_t)v;
+}
+
+// All threads of the CTA: its tile (in launch order) and the launch's epoch.
+__device__ __forceinline__ void lb_begin(LbCtl *ctl, int64_t *tile, unsigned *epoch)
+{
+    __shared__ unsigned s_t, s_e;
+    if (threadIdx.x == 0) {
+        s_t = atomicAdd(&ctl->tile_counter, 1u);
+        s_e = *(volatile unsigned *)&ctl->epoch;
+    }
+    __syncthreads();
+    *tile = s_t;
+    *epoch = s_e;
+}
+
+// All threads of the CTA, after its last write: the last CTA to finish resets
+// the counters and advances the epoch.
+__device__ __forceinline__ void lb_end(LbCtl *ctl)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned d = atomicAdd(&ctl->done, 1u);
+        if (d == gridDim.x - 1) {
+            ctl->tile_counter = 0u;
+            ctl->done = 0u;
+            ctl->epoch = ctl->epoch + 1u;
+            __threadfence();
+        }
+    }
+}
+
+// lookback_exclusive over epoch-tagged words (same contract: one full warp,
+// bounded waits, returns the exclusive prefix of `tile`).
+__device__ __forceinline__ int32_t lookback_epoch(unsigned long long *tile_status, int64_t tile, int32_t agg,
+                                                  unsigned epoch, unsigned *status)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned long long tag = (unsigned long long)(epoch & 0x3fffffffu);
+    if (tile == 0) {
+        if (lane == 0) atomicExch(&tile_status[0], lb_word(epoch, 2u, agg));
+        return 0;
+    }
+    if (lane == 0) atomicExch(&tile_status[tile], lb_word(epoch, 1u, agg));
+    int32_t excl = 0;
+    int64_t pred = tile - 1;
+    for (;;) {
+        const int64_t idx = pred - lane;
+        unsigned flag = 2u;   // virtual inclusive prefix 0 before tile 0
+        int32_t val = 0;
+        if (idx >= 0) {
+            unsigned it = 0;
+            for (;;) {
+                const unsigned long long st = *(volatile unsigned long long *)&tile_status[idx];
+                flag = (st >> 34) == tag ? (unsigned)(st >> 32) & 3u : 0u;
+                if (flag) {
+                    val = (int32_t)(unsigned)(st & 0xffffffffull);
+                    break;
+                }
+                if (++it > HP_SPIN_LIMIT) {
+                    atomicOr(status, HP_STATUS_SPIN_TIMEOUT);
+                    flag = 2u;
+                    val = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        const unsigned pre_mask = __ballot_sync(HP_FULL_MASK, flag == 2u);
+        if (pre_mask) {
+            const int first = __ffs(pre_mask) - 1;
+            excl += warp_sum(lane <= first ? val : 0);
+            break;
+        }
+        excl += warp_sum(val);
+        pred -= 32;
+    }
+    if (lane == 0) atomicExch(&tile_status[tile], lb_word(epoch, 2u, excl + agg));
+    return excl;
+}
+
 __host__ __device__ __forceinline__ int64_t iabs64(int64_t x) { return x < 0 ? -x : x; }
 
 // Weak-rebalance gain bucket with the float semantics of the reference's

@@ -39,6 +39,12 @@ struct hp_context {
     cudaEvent_t ev[8] = {};
     int launches = 0;
 
+    // Epoch look-back region of the single-pass kernels (hp_common.cuh): tile
+    // words (only those kernels write them) and the tile counter / epoch block.
+    unsigned long long *lb_status = nullptr;
+    int64_t lb_cap = 0;
+    hp::LbCtl *lb_ctl = nullptr;
+
     // Kernel-class profiler (opt.profile): event pairs resolved at the end of a call.
     struct ProfRec { int cls; int ev0, ev1; int64_t bytes; int launches; };
     std::vector<cudaEvent_t> prof_events;
@@ -113,6 +119,10 @@ void hp_prof_end(hp_context *c, int token, int cls, int64_t bytes);
 // Algorithmic bytes of an interval that are known only after it was closed.
 void hp_prof_add_bytes(hp_context *c, int token, int64_t bytes);
 void hp_prof_resolve(hp_context *c);
+
+// Ensures room for `tiles` look-back words (called at the start of a call,
+// before any launch that could use them).
+int hp_lb_reserve(hp_context *c, int64_t tiles);
 
 // Blocking read of nbytes from device into the pinned mirror, then dst.
 int hp_read_scalars(hp_context *c, const void *d_src, size_t nbytes, void *dst);

@@ -5,6 +5,7 @@
 #include <cuda_bf16.h>
 
 #include "hp_common.cuh"
+#include "hp_partition.h"
 
 #define HP_MLP_IN 8
 #define HP_MLP_H 32
@@ -15,7 +16,8 @@
 #define HP_MLP_OFF_B2 (HP_MLP_OFF_W2 + HP_MLP_H * HP_MLP_H)
 #define HP_MLP_OFF_W3 (HP_MLP_OFF_B2 + HP_MLP_H)
 #define HP_MLP_OFF_B3 (HP_MLP_OFF_W3 + HP_MLP_H)
-#define HP_MLP_NPARAM (HP_MLP_OFF_B3 + 1)   // 1377
+// the public count (HP_MLP_NPARAM, include/hp_partition.h) is this layout's size
+static_assert(HP_MLP_OFF_B3 + 1 == HP_MLP_NPARAM, "parameter layout and HP_MLP_NPARAM disagree");
 
 namespace hp {
 

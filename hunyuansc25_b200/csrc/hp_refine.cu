@@ -36,6 +36,9 @@ __global__ void project_kernel(int32_t n, const int32_t *__restrict__ cmap,
     if (v < n) where[v] = cwhere[cmap[v]];
 }
 
+// Row capacities min(deg, k); rows longer than BIGD go on the big list;
+// d_bigcnt[1] records the longest short row above 8 entries (picks the
+// network of gain_thread_kernel), d_bigcnt[2] the longest row above HUGED.
 __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t k,
                                 int32_t *__restrict__ cap, int32_t *big, int32_t *d_bigcnt)
 {
@@ -43,37 +46,214 @@ __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int
     if (v >= n) return;
     int32_t d = xadj[v + 1] - xadj[v];
     cap[v] = d < k ? d : k;
-    if (d > BIGD) big[atomicAdd(d_bigcnt, 1)] = v;
+    if (d > BIGD) {
+        big[atomicAdd(d_bigcnt, 1)] = v;
+        if (d > HUGED) atomicMax(d_bigcnt + 2, d);
+    } else if (d > 8) {
+        atomicMax(d_bigcnt + 1, d);
+    }
+}
+
+// Gain row of a vertex with at most BIGD neighbours, one thread per row: the
+// (part, weight) pairs are sorted by a register network and merged, then
+// written as the sparse row (ascending parts, part -1 padding up to the
+// capacity) or, when deg >= k, as the dense row (entry q = part q).
+template <int NET, int XN>
+__device__ __forceinline__ void gain_row_thread(int32_t b, int32_t d, const int32_t *__restrict__ adjncy,
+                                                const int32_t *__restrict__ adjwgt,
+                                                const int32_t *__restrict__ where, int32_t *__restrict__ gp,
+                                                int32_t *__restrict__ gc, int32_t cap, int32_t k)
+{
+    unsigned long long x[XN];
+#pragma unroll
+    for (int i = 0; i < NET; i++)
+        x[i] = i < d ? (((unsigned long long)(uint32_t)where[adjncy[b + i]] << 32) | (uint32_t)adjwgt[b + i])
+                     : hp::PACK_NONE;
+    hp::sort_regs<NET, XN>(x);
+    const bool dense = d >= k;
+    int32_t r = 0, next = 0;
+    uint32_t prev = 0xffffffffu;
+    int32_t acc = 0;
+    auto flush = [&](int32_t q, int32_t sum) {
+        if (dense) {
+            for (; next < q; next++) { gp[next] = next; gc[next] = 0; }
+            gp[q] = q;
+            gc[q] = sum;
+            next = q + 1;
+        } else {
+            gp[r] = q;
+            gc[r] = sum;
+            r++;
+        }
+    };
+#pragma unroll
+    for (int i = 0; i < NET; i++) {
+        const uint32_t q = (uint32_t)(x[i] >> 32);
+        const int32_t w = (int32_t)(uint32_t)x[i];
+        if (q == (uint32_t)hp::KEY_NONE) continue;
+        if (q != prev) {
+            if (prev != 0xffffffffu) flush((int32_t)prev, acc);
+            prev = q;
+            acc = w;
+        } else {
+            acc += w;
+        }
+    }
+    if (prev != 0xffffffffu) flush((int32_t)prev, acc);
+    if (dense) {
+        for (; next < k; next++) { gp[next] = next; gc[next] = 0; }
+    } else {
+        for (; r < cap; r++) { gp[r] = -1; gc[r] = 0; }
+    }
+}
+
+// list == nullptr: every vertex (rows longer than BIGD are skipped: the big-row
+// kernel builds them); else the listed vertices, whose dirty flags are cleared.
+template <int XN>
+__global__ void __launch_bounds__(256)
+gain_thread_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, int32_t n,
+                   const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
+                   const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
+                   int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty)
+{
+    const int32_t cnt = list ? *d_count : n;
+    for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < cnt; i0 += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = i0 + threadIdx.x;
+        int32_t v = -1, b = 0, d = 0;
+        if (i < cnt) {
+            v = list ? list[i] : (int32_t)i;
+            b = xadj[v];
+            d = xadj[v + 1] - b;
+            if (dirty) dirty[v] = 0;
+        }
+        const bool mine = v >= 0 && d <= BIGD;
+        const unsigned wmax = __reduce_max_sync(HP_FULL_MASK, mine ? (unsigned)d : 0u);
+        if (!mine) continue;
+        const int32_t o = goff[v], cap = goff[v + 1] - o;
+        if (XN == 8 || wmax <= 8)
+            gain_row_thread<8, XN>(b, d, adjncy, adjwgt, where, gpart + o, gconn + o, cap, k);
+        else if (XN == 16 || wmax <= 16)
+            gain_row_thread<(XN < 16 ? XN : 16), XN>(b, d, adjncy, adjwgt, where, gpart + o, gconn + o, cap, k);
+        else
+            gain_row_thread<XN, XN>(b, d, adjncy, adjwgt, where, gpart + o, gconn + o, cap, k);
+    }
 }
 
 // Gain row of v: (part, connectivity) for every part adjacent to v, ascending
 // by part, padded with part -1 up to min(deg, k).  A vertex with deg >= k has a
 // dense row instead: entry q is (q, conn to part q), zeros included; dense rows
 // are updated in place by atomics when a neighbour moves and never rebuilt.
+// Rebuild of the listed (dirty) rows of at most S entries (S >= the level's
+// longest short row): 32/S rows per warp, one segment of S lanes per row,
+// sorted and merged by seg_aggregate; dirty flags are cleared.  Rows with
+// deg >= k (k <= S here) are written dense.
+template <int S>
 __global__ void __launch_bounds__(256)
-gain_warp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, int32_t n,
-                 const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
-                 const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
-                 const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
-                 int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty)
+gain_seg_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
+                const int32_t *__restrict__ goff, int32_t *__restrict__ gpart, int32_t *__restrict__ gconn,
+                int32_t k, int32_t *__restrict__ dirty)
 {
-    const int lane = threadIdx.x & 31;
-    const int32_t cnt = list ? *d_count : n;
-    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
-         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int32_t v = list ? list[i] : (int32_t)i;
-        if (dirty && lane == 0) dirty[v] = 0;
-        const int32_t b = xadj[v], d = xadj[v + 1] - b;
-        if (d > BIGD) continue;
+    constexpr int R = 32 / S;
+    const int lane = threadIdx.x & 31, sl = lane & (S - 1);
+    const int32_t cnt = *d_count;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t i0 = warp * R; i0 < cnt; i0 += nwarps * R) {
+        const int64_t i = i0 + lane / S;
+        int32_t v = -1, b = 0, d = 0;
+        if (i < cnt) {
+            v = list[i];
+            b = xadj[v];
+            d = xadj[v + 1] - b;
+            if (sl == 0) dirty[v] = 0;
+        }
         int32_t key = hp::KEY_NONE, w = 0;
-        if (lane < d) { key = where[adjncy[b + lane]]; w = adjwgt[b + lane]; }
+        if (v >= 0 && sl < d) {
+            key = where[adjncy[b + sl]];
+            w = adjwgt[b + sl];
+        }
+        const int32_t o = v >= 0 ? goff[v] : 0, cap = v >= 0 ? goff[v + 1] - o : 0;
+        const bool dense = v >= 0 && d >= k;
+        if (dense && sl < k) { gpart[o + sl] = sl; gconn[o + sl] = 0; }
+        __syncwarp();
+        if (dense && key != hp::KEY_NONE) atomicAdd(&gconn[o + key], w);
+        const int c = hp::seg_aggregate<S>(key, w, (v >= 0 && !dense) ? gpart + o : nullptr,
+                                            (v >= 0 && !dense) ? gconn + o : nullptr);
+        if (v >= 0 && !dense)
+            for (int32_t t = c + sl; t < cap; t += S) { gpart[o + t] = -1; gconn[o + t] = 0; }
+    }
+}
+
+// Gain rows of BIGD+1 .. HUGED entries when k <= WARP_DENSE_K: one warp per
+// row with its own dense accumulator and presence bitmap over the k parts in
+// shared memory (k + k/32 words per warp), extracted in part order; only warp
+// synchronisation.  Longer rows (and any row when k is larger) use
+// gain_dense_kernel.
+constexpr int WARP_DENSE_K = 1024;
+constexpr int GW_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * GW_WARPS)
+gain_bigwarp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                    const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                    const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
+                    const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
+                    int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty)
+{
+    extern __shared__ int32_t gsm[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nwords = (k + 31) >> 5;
+    int32_t *dw = gsm + wid * (k + nwords);
+    unsigned *bm = (unsigned *)(dw + k);
+    for (int i = lane; i < k; i += 32) dw[i] = 0;
+    for (int i = lane; i < nwords; i += 32) bm[i] = 0u;
+    __syncwarp();
+    const int32_t cnt = *d_count;
+    for (int64_t li = (int64_t)blockIdx.x * GW_WARPS + wid; li < cnt; li += (int64_t)gridDim.x * GW_WARPS) {
+        const int32_t v = list[li];
+        const int32_t b = xadj[v], e = xadj[v + 1];
+        if (e - b <= BIGD || e - b > HUGED) continue;
+        if (dirty && lane == 0) dirty[v] = 0;
+        for (int32_t j = b + lane; j < e; j += 32) {
+            const int32_t q = where[adjncy[j]];
+            atomicAdd(&dw[q], adjwgt[j]);
+            atomicOr(&bm[q >> 5], 1u << (q & 31));
+        }
+        __syncwarp();
         const int32_t o = goff[v], cap = goff[v + 1] - o;
-        if (d >= k) {   // dense row: entry q is part q (cap == k)
-            hp::warp_aggregate32_dense(key, w, k, gpart + o, gconn + o);
+        if (e - b >= k) {   // dense row
+            for (int32_t q = lane; q < k; q += 32) {
+                gpart[o + q] = q;
+                gconn[o + q] = dw[q];
+                dw[q] = 0;
+            }
+            for (int32_t q = lane; q < nwords; q += 32) bm[q] = 0u;
+            __syncwarp();
             continue;
         }
-        int c = hp::warp_aggregate32(key, w, gpart + o, gconn + o);
-        for (int32_t t = c + lane; t < cap; t += 32) { gpart[o + t] = -1; gconn[o + t] = 0; }
+        int32_t run = 0;
+        for (int wb = 0; wb < nwords; wb += 32) {
+            const int wi = wb + lane;
+            unsigned word = wi < nwords ? bm[wi] : 0u;
+            const int c = __popc(word);
+            const int incl = hp::warp_incl_scan(c);
+            int32_t pos = run + incl - c;
+            run += __shfl_sync(HP_FULL_MASK, incl, 31);
+            if (word) bm[wi] = 0u;
+            while (word) {
+                const int bit = __ffs(word) - 1;
+                word &= word - 1;
+                const int32_t q = (wi << 5) + bit;
+                gpart[o + pos] = q;
+                gconn[o + pos] = dw[q];
+                dw[q] = 0;
+                pos++;
+            }
+        }
+        for (int32_t t = run + lane; t < cap; t += 32) { gpart[o + t] = -1; gconn[o + t] = 0; }
+        __syncwarp();
     }
 }
 
@@ -98,6 +278,7 @@ gain_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ 
         const int32_t v = list[li];
         const int32_t b = xadj[v], e = xadj[v + 1];
         if (e - b <= BIGD) continue;
+        if (k <= WARP_DENSE_K && e - b <= HUGED) continue;   // gain_bigwarp_kernel's rows
         if (dirty && threadIdx.x == 0) dirty[v] = 0;
         for (int32_t j = b + threadIdx.x; j < e; j += NT) {
             int32_t q = where[adjncy[j]];
@@ -470,26 +651,43 @@ c_delta_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nm
 // not depend on its own part: only neighbours' rows change.  Dense neighbour
 // rows (deg >= k) take the change in place; a sparse neighbour is queued once
 // (atomicExch on its dirty flag) on the small or big rebuild list.
-__device__ __forceinline__ void touch_neighbour(int32_t u, int32_t w, int32_t p, int32_t d,
+__device__ __forceinline__ void touch_neighbour(bool valid, int32_t u, int32_t w, int32_t p, int32_t d,
                                                 const int32_t *__restrict__ xadj,
                                                 const int32_t *__restrict__ goff,
                                                 int32_t *__restrict__ gconn, int32_t *__restrict__ dirty,
                                                 int32_t *__restrict__ small_l, int32_t *__restrict__ big_l,
                                                 int32_t *counts, int32_t k)
 {
-    const int32_t o = goff[u];
-    if (goff[u + 1] - o == k) {
-        atomicAdd(&gconn[o + p], -w);
-        atomicAdd(&gconn[o + d], w);
-    } else if (atomicExch(&dirty[u], 1) == 0) {
-        if (xadj[u + 1] - xadj[u] > BIGD) big_l[atomicAdd(&counts[1], 1)] = u;
-        else small_l[atomicAdd(&counts[0], 1)] = u;
+    // all 32 lanes call (valid marks the lanes with a neighbour); list appends
+    // take one counter atomic per warp and list (ballot ranks inside the warp)
+    bool sm = false, bg = false;
+    if (valid) {
+        const int32_t o = goff[u];
+        if (goff[u + 1] - o == k) {
+            atomicAdd(&gconn[o + p], -w);
+            atomicAdd(&gconn[o + d], w);
+        } else if (atomicExch(&dirty[u], 1) == 0) {
+            if (xadj[u + 1] - xadj[u] > BIGD) bg = true;
+            else sm = true;
+        }
     }
+    const unsigned lt = hp::lanemask_lt();
+    const unsigned ms = __ballot_sync(HP_FULL_MASK, sm), mb = __ballot_sync(HP_FULL_MASK, bg);
+    const int lane = threadIdx.x & 31;
+    int32_t bs = 0, bb = 0;
+    if (lane == 0) {
+        if (ms) bs = atomicAdd(&counts[0], __popc(ms));
+        if (mb) bb = atomicAdd(&counts[1], __popc(mb));
+    }
+    bs = __shfl_sync(HP_FULL_MASK, bs, 0);
+    bb = __shfl_sync(HP_FULL_MASK, bb, 0);
+    if (sm) small_l[bs + __popc(ms & lt)] = u;
+    if (bg) big_l[bb + __popc(mb & lt)] = u;
 }
 
 __global__ void __launch_bounds__(256)
 apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
-                   const int32_t *__restrict__ where, const int32_t *__restrict__ dest,
+                   int32_t *__restrict__ where, const int32_t *__restrict__ dest,
                    const int32_t *__restrict__ vwgt, unsigned long long *__restrict__ pw,
                    const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                    const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
@@ -502,20 +700,27 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = moves[i];
         const int32_t p = where[v], d = dest[v];
+        __syncwarp();
         if (lane == 0) {
             const unsigned long long w = (unsigned long long)vwgt[v];
             atomicAdd(&pw[d], w);
             atomicAdd(&pw[p], (unsigned long long)(-(long long)w));
         }
-        if (xadj[v + 1] - xadj[v] > HUGED) continue;   // CTA kernel below
-        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32)
-            touch_neighbour(adjncy[j], adjwgt[j], p, d, xadj, goff, gconn, dirty, small_l, big_l, counts, k);
+        const int32_t b = xadj[v], e = xadj[v + 1];
+        if (e - b > HUGED) continue;   // CTA kernel below (it commits v)
+        for (int32_t j0 = b; j0 < e; j0 += 32) {
+            const int32_t j = j0 + lane;
+            const bool valid = j < e;
+            touch_neighbour(valid, valid ? adjncy[j] : 0, valid ? adjwgt[j] : 0, p, d, xadj, goff, gconn, dirty,
+                            small_l, big_l, counts, k);
+        }
+        if (lane == 0) where[v] = d;   // the move itself (every lane has read where[v])
     }
 }
 
 __global__ void __launch_bounds__(512)
 apply_moves_huge_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
-                        const int32_t *__restrict__ where, const int32_t *__restrict__ dest,
+                        int32_t *__restrict__ where, const int32_t *__restrict__ dest,
                         const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                         const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
                         int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
@@ -526,26 +731,24 @@ apply_moves_huge_kernel(const int32_t *__restrict__ moves, const unsigned long l
         const int32_t v = moves[i];
         if (xadj[v + 1] - xadj[v] <= HUGED) continue;
         const int32_t p = where[v], d = dest[v];
-        for (int32_t j = xadj[v] + threadIdx.x; j < xadj[v + 1]; j += blockDim.x)
-            touch_neighbour(adjncy[j], adjwgt[j], p, d, xadj, goff, gconn, dirty, small_l, big_l, counts, k);
+        const int32_t b = xadj[v], e = xadj[v + 1];
+        for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
+            const int32_t j = j0 + threadIdx.x;
+            const bool valid = j < e;
+            touch_neighbour(valid, valid ? adjncy[j] : 0, valid ? adjwgt[j] : 0, p, d, xadj, goff, gconn, dirty,
+                            small_l, big_l, counts, k);
+        }
+        __syncthreads();   // every thread has read where[v]
+        if (threadIdx.x == 0) where[v] = d;
     }
 }
 
-__global__ void __launch_bounds__(256)
-commit_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
-                    int32_t *__restrict__ where, const int32_t *__restrict__ dest)
-{
-    const int64_t nm = (int64_t)*d_nmoves;
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < nm) { int32_t v = moves[i]; where[v] = dest[v]; }
-}
-
 // ---- rebalancing ------------------------------------------------------------------
-__global__ void undersized_kernel(int32_t k, const unsigned long long *__restrict__ pw,
-                                  const int64_t *__restrict__ maxp, int32_t *__restrict__ und,
-                                  int32_t *d_nu)
+// Undersized parts (pw < max(0.99 maxp, maxp - 100)) in part order; one CTA.
+__device__ __forceinline__ void undersized_block(int32_t k, const unsigned long long *__restrict__ pw,
+                                                 const int64_t *__restrict__ maxp, int32_t *__restrict__ und,
+                                                 int32_t *d_nu, int32_t *s_scan /* 1024/32 + 2 */)
 {
-    __shared__ int32_t s_scan[1024 / 32 + 2];
     int running = 0;
     for (int base = 0; base < k; base += 1024) {
         int p = base + threadIdx.x;
@@ -563,100 +766,141 @@ __global__ void undersized_kernel(int32_t k, const unsigned long long *__restric
     if (threadIdx.x == 0) *d_nu = running;
 }
 
-// key = part * 64 + bucket for a rebalance candidate, else -1.
-__global__ void __launch_bounds__(256)
-rw_key_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__restrict__ vwgt,
-              const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
-              const int64_t *__restrict__ opt, const int32_t *__restrict__ goff,
-              const int32_t *__restrict__ gpart, const int32_t *__restrict__ gconn,
-              const int32_t *__restrict__ und, const int32_t *__restrict__ d_nu,
-              int32_t *__restrict__ key, int32_t *__restrict__ flag, int32_t *__restrict__ dest)
-{
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const int32_t p = where[v];
-    int32_t kk = -1, d = p;
-    const int64_t pwp = (int64_t)pw[p];
-    if (pwp > maxp[p] && 2 * (int64_t)vwgt[v] < 3 * (pwp - opt[p])) {
-        int64_t pc = 0, bc = 0;
-        int32_t b = -1;
-        for (int32_t j = goff[v]; j < goff[v + 1]; j++) {
-            int32_t q = gpart[j];
-            if (q < 0) break;
-            int32_t cq = gconn[j];
-            if (q == p) pc = cq;
-            if ((int64_t)pw[q] < maxp[q] && cq > bc) { bc = cq; b = q; }
-        }
-        int64_t g = 0;
-        bool ok = true;
-        if (b >= 0) g = bc - pc;
-        else {
-            const int32_t nu = *d_nu;
-            if (nu == 0) ok = false;
-            else { b = und[v % nu]; g = -pc; }
-        }
-        if (ok) { d = b; kk = p * 64 + hp::gain_bucket((int32_t)g, vwgt[v]); }
-    }
-    key[v] = kk;
-    flag[v] = kk >= 0;
-    dest[v] = d;
-}
+// Rebalance candidates of a pass in one ordered pass over the vertices, tiles
+// of RB_TILE in launch order with an epoch look-back: the key (part * 64 + gain
+// bucket) of every candidate, compacted in vertex order into K/V, the count
+// into *d_cnt, and dest[v] for every vertex (the proposed part, or its own).
+//   weak  (jetrw, hunyuangraph_GPU_krefine.h:3381-3563): v in an overweight part
+//         with 2 vwgt < 3 (pw - opt); destination = most connected part that
+//         is not overweight (first max in part order), else an undersized part
+//         (und[v % nu]); gain = conn(dest) - conn(own)
+//   strong (jetrs, :2774-3135): v in an overweight part with vwgt < 2 (pw - opt);
+//         loss = -conn(own)
+// The part bounds pstart/pend are reset to -1 here for the rank kernel.
+constexpr int RB_TILE = 256;
 
-__global__ void __launch_bounds__(256)
-rs_key_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__restrict__ vwgt,
-              const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
-              const int64_t *__restrict__ opt, const int32_t *__restrict__ goff,
-              const int32_t *__restrict__ gpart, const int32_t *__restrict__ gconn,
-              int32_t *__restrict__ key, int32_t *__restrict__ flag, int32_t *__restrict__ dest, int32_t k)
+template <bool STRONG>
+__global__ void __launch_bounds__(RB_TILE)
+rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__restrict__ vwgt,
+                     const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
+                     const int64_t *__restrict__ opt, const int32_t *__restrict__ goff,
+                     const int32_t *__restrict__ gpart, const int32_t *__restrict__ gconn,
+                     const int32_t *__restrict__ und, const int32_t *__restrict__ d_nu, int32_t k,
+                     int32_t *__restrict__ K, int32_t *__restrict__ V, int32_t *__restrict__ dest,
+                     int32_t *__restrict__ d_cnt, int32_t *__restrict__ pstart, int32_t *__restrict__ pend,
+                     unsigned long long *tile_status, hp::LbCtl *lb, unsigned *status)
 {
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const int32_t p = where[v];
+    __shared__ int32_t s_scan[RB_TILE / 32 + 2];
+    __shared__ int32_t s_excl;
+    int64_t tile;
+    unsigned epoch;
+    hp::lb_begin(lb, &tile, &epoch);
+    for (int64_t q = tile * RB_TILE + threadIdx.x; q < k; q += (int64_t)gridDim.x * RB_TILE) {
+        pstart[q] = -1;
+        pend[q] = -1;
+    }
+    const int64_t v64 = tile * RB_TILE + threadIdx.x;
     int32_t kk = -1;
-    const int64_t pwp = (int64_t)pw[p];
-    if (pwp > maxp[p] && (int64_t)vwgt[v] < 2 * (pwp - opt[p])) {
-        int32_t o = goff[v];
-        int32_t pc = row_conn(gpart + o, gconn + o, goff[v + 1] - o, p, k);
-        kk = p * 64 + hp::gain_bucket(-pc, vwgt[v]);
+    if (v64 < n) {
+        const int32_t v = (int32_t)v64;
+        const int32_t p = where[v];
+        int32_t d = p;
+        const int64_t pwp = (int64_t)pw[p];
+        if (!STRONG) {
+            if (pwp > maxp[p] && 2 * (int64_t)vwgt[v] < 3 * (pwp - opt[p])) {
+                int64_t pc = 0, bc = 0;
+                int32_t b = -1;
+                for (int32_t j = goff[v]; j < goff[v + 1]; j++) {
+                    int32_t q = gpart[j];
+                    if (q < 0) break;
+                    int32_t cq = gconn[j];
+                    if (q == p) pc = cq;
+                    if ((int64_t)pw[q] < maxp[q] && cq > bc) { bc = cq; b = q; }
+                }
+                int64_t g = 0;
+                bool ok = true;
+                if (b >= 0) g = bc - pc;
+                else {
+                    const int32_t nu = *d_nu;
+                    if (nu == 0) ok = false;
+                    else { b = und[v % nu]; g = -pc; }
+                }
+                if (ok) { d = b; kk = p * 64 + hp::gain_bucket((int32_t)g, vwgt[v]); }
+            }
+        } else {
+            if (pwp > maxp[p] && (int64_t)vwgt[v] < 2 * (pwp - opt[p])) {
+                int32_t o = goff[v];
+                int32_t pc = row_conn(gpart + o, gconn + o, goff[v + 1] - o, p, k);
+                kk = p * 64 + hp::gain_bucket(-pc, vwgt[v]);
+            }
+        }
+        dest[v] = d;
     }
-    key[v] = kk;
-    flag[v] = kk >= 0;
-    dest[v] = p;
+    int tot;
+    const int local = hp::block_excl_scan<RB_TILE>(kk >= 0 ? 1 : 0, &tot, s_scan);
+    if (threadIdx.x < 32) {
+        const int32_t ex = hp::lookback_epoch(tile_status, tile, tot, epoch, status);
+        if (threadIdx.x == 0) s_excl = ex;
+    }
+    __syncthreads();
+    if (kk >= 0) {
+        const int32_t pos = s_excl + local;
+        K[pos] = kk;
+        V[pos] = (int32_t)v64;
+    }
+    if (tile == gridDim.x - 1 && threadIdx.x == 0) *d_cnt = s_excl + tot;
+    hp::lb_end(lb);
 }
 
-__global__ void gather_pairs_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_cnt,
-                                    const int32_t *__restrict__ key, int32_t *__restrict__ K,
-                                    int32_t *__restrict__ V)
-{
-    const int32_t cnt = *d_cnt;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        int32_t v = list[i];
-        K[i] = key[v];
-        V[i] = v;
-    }
-}
+// Over the sorted candidates: pre[i] = weight of the candidates before i in
+// the sorted order (pre[cnt] = total), and the part bounds pstart/pend (first
+// index, one past the last) from the sorted keys.  Tiles of RK_TILE items in
+// launch order with an epoch look-back; tiles beyond the count only take part
+// in the tile accounting.
+constexpr int RK_THREADS = 256, RK_ITEMS = 4, RK_TILE = RK_THREADS * RK_ITEMS;
 
-__global__ void weights_of_kernel(const int32_t *__restrict__ idx, const int32_t *__restrict__ V,
-                                  const int32_t *__restrict__ d_cnt, const int32_t *__restrict__ vwgt,
-                                  int32_t *__restrict__ W)
+__global__ void __launch_bounds__(RK_THREADS)
+rb_rank_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, const int32_t *__restrict__ d_cnt,
+               const int32_t *__restrict__ vwgt, int32_t *__restrict__ pre, int32_t *__restrict__ pstart,
+               int32_t *__restrict__ pend, unsigned long long *tile_status, hp::LbCtl *lb, unsigned *status)
 {
+    __shared__ int32_t s_scan[RK_THREADS / 32 + 2];
+    __shared__ int32_t s_excl;
+    int64_t tile;
+    unsigned epoch;
+    hp::lb_begin(lb, &tile, &epoch);
     const int32_t cnt = *d_cnt;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt;
-         i += (int64_t)gridDim.x * blockDim.x)
-        W[i] = vwgt[V[idx ? idx[i] : i]];
-}
-
-__global__ void part_bounds_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ d_cnt,
-                                   int32_t *__restrict__ pstart, int32_t *__restrict__ pend)
-{
-    const int32_t cnt = *d_cnt;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        int32_t p = K[i] >> 6;
-        if (i == 0 || (K[i - 1] >> 6) != p) pstart[p] = (int32_t)i;
-        if (i == cnt - 1 || (K[i + 1] >> 6) != p) pend[p] = (int32_t)i + 1;
+    const int64_t base = tile * RK_TILE;
+    if (base <= cnt) {
+        const int64_t i0 = base + (int64_t)threadIdx.x * RK_ITEMS;
+        int32_t w[RK_ITEMS];
+        int32_t sum = 0;
+#pragma unroll
+        for (int q = 0; q < RK_ITEMS; q++) {
+            w[q] = i0 + q < cnt ? vwgt[V[i0 + q]] : 0;
+            sum += w[q];
+        }
+        int tot;
+        int32_t run = hp::block_excl_scan<RK_THREADS>(sum, &tot, s_scan);
+        if (threadIdx.x < 32) {
+            const int32_t ex = hp::lookback_epoch(tile_status, tile, tot, epoch, status);
+            if (threadIdx.x == 0) s_excl = ex;
+        }
+        __syncthreads();
+        run += s_excl;
+#pragma unroll
+        for (int q = 0; q < RK_ITEMS; q++) {
+            const int64_t i = i0 + q;
+            if (i <= cnt) pre[i] = run;
+            run += w[q];
+            if (i < cnt) {
+                const int32_t p = K[i] >> 6;
+                if (i == 0 || (K[i - 1] >> 6) != p) pstart[p] = (int32_t)i;
+                if (i == cnt - 1 || (K[i + 1] >> 6) != p) pend[p] = (int32_t)i + 1;
+            }
+        }
     }
+    hp::lb_end(lb);
 }
 
 __global__ void rw_select_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V,
@@ -695,16 +939,73 @@ __global__ void evict_end_kernel(int32_t k, const int32_t *__restrict__ pstart,
     ev_end[p] = hi;
 }
 
-__global__ void evict_flag_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ d_cnt,
-                                  const int32_t *__restrict__ ev_end, int32_t *__restrict__ flag, int64_t bound)
+// Strong rebalance: the evicted prefix of every overweight part (sorted index
+// i < ev_end[part]) compacted in sorted order -- P[j] = i and sp[j] = weight of
+// the evicted candidates before j (sp[np] = total), *d_np = np -- in one pass
+// with two epoch look-back chains (count: tile words [0, half); weight: words
+// [half, 2 half)).
+__global__ void __launch_bounds__(RK_THREADS)
+rs_evict_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, const int32_t *__restrict__ d_cnt,
+                const int32_t *__restrict__ ev_end, const int32_t *__restrict__ vwgt, int32_t *__restrict__ P,
+                int32_t *__restrict__ sp, int32_t *__restrict__ d_np, unsigned long long *tile_status,
+                int64_t half, hp::LbCtl *lb, unsigned *status)
 {
+    __shared__ int32_t s_scan[RK_THREADS / 32 + 2];
+    __shared__ int32_t s_excl[2];
+    int64_t tile;
+    unsigned epoch;
+    hp::lb_begin(lb, &tile, &epoch);
     const int32_t cnt = *d_cnt;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < bound;
-         i += (int64_t)gridDim.x * blockDim.x)
-        flag[i] = i < cnt ? (i < ev_end[K[i] >> 6]) : 0;
+    const int64_t base = tile * RK_TILE;
+    if (base <= cnt) {
+        const int64_t i0 = base + (int64_t)threadIdx.x * RK_ITEMS;
+        int32_t w[RK_ITEMS];
+        bool f[RK_ITEMS];
+        int32_t nf = 0, sw = 0;
+#pragma unroll
+        for (int q = 0; q < RK_ITEMS; q++) {
+            const int64_t i = i0 + q;
+            f[q] = i < cnt && i < ev_end[K[i] >> 6];
+            w[q] = f[q] ? vwgt[V[i]] : 0;
+            nf += f[q];
+            sw += w[q];
+        }
+        int tc, tw;
+        int32_t pos = hp::block_excl_scan<RK_THREADS>(nf, &tc, s_scan);
+        int32_t run = hp::block_excl_scan<RK_THREADS>(sw, &tw, s_scan);
+        if (threadIdx.x < 32) {
+            const int32_t ex = hp::lookback_epoch(tile_status, tile, tc, epoch, status);
+            if (threadIdx.x == 0) s_excl[0] = ex;
+        } else if (threadIdx.x < 64) {
+            const int32_t ex = hp::lookback_epoch(tile_status + half, tile, tw, epoch, status);
+            if (threadIdx.x == 32) s_excl[1] = ex;
+        }
+        __syncthreads();
+        pos += s_excl[0];
+        run += s_excl[1];
+#pragma unroll
+        for (int q = 0; q < RK_ITEMS; q++) {
+            if (f[q]) {
+                P[pos] = (int32_t)(i0 + q);
+                sp[pos] = run;
+                pos++;
+            }
+            run += w[q];
+        }
+        if (cnt >= base && cnt < base + RK_TILE && threadIdx.x == 0) {
+            *d_np = s_excl[0] + tc;
+            sp[s_excl[0] + tc] = s_excl[1] + tw;
+        }
+    }
+    hp::lb_end(lb);
 }
 
-// Sequential cookie cutter over the parts (one warp; each search is 32-ary).
+// Sequential cookie cutter over the parts (one warp), as in the reference
+// (hunyuangraph_GPU_krefine.h:3075): part p takes the evicted range starting
+// at the previous end whose weight is closest to its room maxp[p] - pw[p].
+// Rooms are read 32 parts at a time; a part without room keeps an empty range
+// (the rule gives end = start there); otherwise the end is searched first among
+// the 32 entries after the start (one coalesced read), then 32-ary over the rest.
 __global__ void cookie_cutter_kernel(int32_t k, const unsigned long long *__restrict__ pw,
                                      const int64_t *__restrict__ maxp, const int32_t *__restrict__ sp,
                                      const int32_t *__restrict__ d_np, int32_t *__restrict__ es,
@@ -713,35 +1014,56 @@ __global__ void cookie_cutter_kernel(int32_t k, const unsigned long long *__rest
     const int lane = threadIdx.x & 31;
     const int32_t np = *d_np;
     int32_t st = 0;
-    for (int32_t p = 0; p < k; p++) {
-        const int64_t room = maxp[p] > (int64_t)pw[p] ? maxp[p] - (int64_t)pw[p] : 0;
-        const int32_t lo0 = st, hi0 = np;
-        const int64_t find = (int64_t)sp[lo0] + room;
-        // first idx in (lo0, hi0] with sp[idx] >= find, else hi0
-        int32_t lo = lo0, hi = hi0;   // answer in (lo, hi]
-        while (hi - lo > 32) {
-            int64_t span = hi - lo;
-            int32_t pos = lo + (int32_t)((span * (lane + 1)) / 32);
-            bool ge = (int64_t)sp[pos] >= find;
-            unsigned m = __ballot_sync(HP_FULL_MASK, ge);
-            if (m == 0) { lo = __shfl_sync(HP_FULL_MASK, pos, 31); break; }
-            int f = __ffs(m) - 1;
-            int32_t nhi = __shfl_sync(HP_FULL_MASK, pos, f);
-            int32_t nlo = f == 0 ? lo : __shfl_sync(HP_FULL_MASK, pos, f - 1);
-            lo = nlo; hi = nhi;
+    for (int32_t p0 = 0; p0 < k; p0 += 32) {
+        const int32_t pl = p0 + lane;
+        const int64_t my_room = pl < k && maxp[pl] > (int64_t)pw[pl] ? maxp[pl] - (int64_t)pw[pl] : 0;
+        const int cnt = min(32, k - p0);
+        for (int q = 0; q < cnt; q++) {
+            const int64_t room = __shfl_sync(HP_FULL_MASK, my_room, q);
+            const int32_t p = p0 + q;
+            const int32_t lo0 = st;
+            int32_t end = lo0;
+            if (room > 0) {
+                const int32_t hi0 = np;
+                const int64_t find = (int64_t)sp[lo0] + room;
+                // first idx in (lo0, hi0] with sp[idx] >= find, else hi0
+                int32_t lo = lo0, hi = hi0, e = hi0;
+                bool found = false;
+                {
+                    const int32_t pos = lo0 + 1 + lane;
+                    const bool ge = pos <= hi0 && (int64_t)sp[pos] >= find;
+                    const unsigned m = __ballot_sync(HP_FULL_MASK, ge);
+                    if (m) { e = lo0 + 1 + (__ffs(m) - 1); found = true; }
+                    else if (lo0 + 32 >= hi0) { e = hi0; found = true; }
+                    else lo = lo0 + 32;   // sp[lo0+32] < find: the answer lies in (lo0+32, hi0]
+                }
+                if (!found) {
+                    while (hi - lo > 32) {
+                        int64_t span = hi - lo;
+                        int32_t pos = lo + (int32_t)((span * (lane + 1)) / 32);
+                        bool ge = (int64_t)sp[pos] >= find;
+                        unsigned m = __ballot_sync(HP_FULL_MASK, ge);
+                        if (m == 0) { lo = __shfl_sync(HP_FULL_MASK, pos, 31); break; }
+                        int f = __ffs(m) - 1;
+                        int32_t nhi = __shfl_sync(HP_FULL_MASK, pos, f);
+                        int32_t nlo = f == 0 ? lo : __shfl_sync(HP_FULL_MASK, pos, f - 1);
+                        lo = nlo; hi = nhi;
+                    }
+                    e = hi;
+                    if (lo < hi) {
+                        int32_t pos = lo + 1 + lane;
+                        bool ge = pos <= hi && (int64_t)sp[pos] >= find;
+                        unsigned m = __ballot_sync(HP_FULL_MASK, ge);
+                        e = m ? lo + 1 + (__ffs(m) - 1) : hi;
+                    }
+                }
+                int32_t s0 = e > lo0 ? e - 1 : lo0;
+                int64_t dh = hp::iabs64((int64_t)sp[e] - find), dl = hp::iabs64((int64_t)sp[s0] - find);
+                end = dh < dl ? e : s0;
+            }
+            if (lane == 0) { es[p] = lo0; ee[p] = end; }
+            st = end;
         }
-        int32_t e = hi;
-        if (lo < hi) {
-            int32_t pos = lo + 1 + lane;
-            bool ge = pos <= hi && (int64_t)sp[pos] >= find;
-            unsigned m = __ballot_sync(HP_FULL_MASK, ge);
-            e = m ? lo + 1 + (__ffs(m) - 1) : hi;
-        }
-        int32_t s = e > lo0 ? e - 1 : lo0;
-        int64_t dh = hp::iabs64((int64_t)sp[e] - find), dl = hp::iabs64((int64_t)sp[s] - find);
-        int32_t end = dh < dl ? e : s;
-        if (lane == 0) { es[p] = lo0; ee[p] = end; }
-        st = end;
     }
 }
 
@@ -769,27 +1091,26 @@ __global__ void rs_assign_kernel(int32_t k, const int32_t *__restrict__ P, const
     }
 }
 
-__global__ void copy_i32_kernel(int64_t n, const int32_t *src, int32_t *dst)
-{
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        dst[i] = src[i];
-}
 
 // ---------------------------------------------------------------------------------
 struct RefineBufs {
     int32_t *goff, *gpart, *gconn, *big, *dest, *pregain, *moves, *oldp, *dirty;
     int32_t *small_l, *big_l, *best_where;
     int8_t *lock;
-    int32_t *key, *flag, *list, *K, *V, *K2, *V2, *pre, *W, *P, *sp;
+    int32_t *K, *V, *K2, *V2, *pre, *P, *sp;
     int32_t *pstart, *pend, *und, *ev_end, *es, *ee;
     unsigned long long *pw;
     const int64_t *opt, *maxp;
-    int32_t G;   // gain-row entries of the level
+    int32_t G;          // gain-row entries of the level
+    int32_t small_max;  // longest row of at most BIGD entries (picks the gain kernel's network)
+    bool huge_rows;     // the level has rows longer than HUGED
 };
 
 // scalar slots used by refinement
 // Slots below S_PASS_END are reset at the start of every pass; S_BIGCNT (the
 // level's list of rows longer than 32) lives above it and persists.
+// S_BIGCNT (slots 16-17) holds the big-row count, the longest short row and the
+// longest row above HUGED.
 enum { S_NMOVES = 0, S_C1 = 1, S_C2 = 2, S_EXCESS = 3, S_NCAND = 4, S_CUT2 = 5, S_DIRTY = 6,
        S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_PASS_END = 12, S_BIGCNT = 16 };
 
@@ -797,13 +1118,40 @@ int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_
                const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt,
                bool any_big, int32_t *dirty)
 {
-    const unsigned pg = (unsigned)(c->sm_count * 8);
-    HP_LAUNCH(c, gain_warp_kernel, small_list ? pg : nblk((int64_t)g.n * 32), 256, 0, small_list,
-              d_small_cnt, g.n, g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
+    if (small_list) {
+        // rebuild of dirty rows: segments of S lanes per row (latency of a warp
+        // per row, 32/S rows per warp)
+        const unsigned grid = (unsigned)(c->sm_count * 8);
+        if (B.small_max <= 8)
+            HP_LAUNCH(c, gain_seg_kernel<8>, grid, 256, 0, small_list, d_small_cnt, g.xadj, g.adjncy, g.adjwgt,
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+        else if (B.small_max <= 16)
+            HP_LAUNCH(c, gain_seg_kernel<16>, grid, 256, 0, small_list, d_small_cnt, g.xadj, g.adjncy, g.adjwgt,
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+        else
+            HP_LAUNCH(c, gain_seg_kernel<32>, grid, 256, 0, small_list, d_small_cnt, g.xadj, g.adjncy, g.adjwgt,
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+    } else {
+        // full build of the level: one thread per row, register network
+        const unsigned grid = nblk(g.n);
+        if (B.small_max <= 8)
+            HP_LAUNCH(c, gain_thread_kernel<8>, grid, 256, 0, nullptr, nullptr, g.n, g.xadj, g.adjncy, g.adjwgt,
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+        else if (B.small_max <= 16)
+            HP_LAUNCH(c, gain_thread_kernel<16>, grid, 256, 0, nullptr, nullptr, g.n, g.xadj, g.adjncy, g.adjwgt,
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+        else
+            HP_LAUNCH(c, gain_thread_kernel<32>, grid, 256, 0, nullptr, nullptr, g.n, g.xadj, g.adjncy, g.adjwgt,
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+    }
     if (any_big) {
         const size_t smem = sizeof(int32_t) * (size_t)k + sizeof(unsigned) * (size_t)((k + 31) / 32);
-        HP_LAUNCH(c, gain_dense_kernel<256>, (unsigned)(c->sm_count * 2), 256, smem, big_list, d_big_cnt,
-                  g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
+        if (k <= WARP_DENSE_K)
+            HP_LAUNCH(c, gain_bigwarp_kernel, (unsigned)(c->sm_count * 4), 32 * GW_WARPS, GW_WARPS * smem, big_list,
+                      d_big_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
+        if (k > WARP_DENSE_K || B.huge_rows)
+            HP_LAUNCH(c, gain_dense_kernel<256>, (unsigned)(c->sm_count * 2), 256, smem, big_list, d_big_cnt,
+                      g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
     }
     return HP_OK;
 }
@@ -816,38 +1164,36 @@ int key_bits_for(int32_t k)
     return (bits + 7) / 8 * 8;
 }
 
-// Candidates flagged in B.flag with keys in B.key -> sorted (K, V) by key,
-// stable in vertex order; prefix weights in B.pre; part bounds.  Returns the
-// arrays holding the sorted result.
-int sort_candidates(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, int32_t **Ks, int32_t **Vs)
+// Candidates of the pass (rb_candidates_kernel, K/V in vertex order) -> stable
+// radix sort by key -> prefix weights and part bounds (rb_rank_kernel).
+// Returns the arrays holding the sorted pairs.
+template <bool STRONG>
+int rank_candidates(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, int32_t **Ks, int32_t **Vs)
 {
     const int32_t n = g.n;
     unsigned long long *sc = c->d_scal;
     int32_t *d_cnt = (int32_t *)&sc[S_LISTCNT];
-    HP_TRY(hp_compact_flags(c, B.flag, n, B.list, d_cnt));
-    const unsigned pg = (unsigned)(c->sm_count * 8);
-    HP_LAUNCH(c, gather_pairs_kernel, pg, 256, 0, B.list, d_cnt, B.key, B.K, B.V);
+    const int64_t ct = ((int64_t)n + RB_TILE - 1) / RB_TILE;
+    const int64_t rt = ((int64_t)n + RK_TILE) / RK_TILE;   // a tile holds index cnt <= n
+    if (ct > c->lb_cap || 2 * rt > c->lb_cap) return HP_ERR_INTERNAL;
+    HP_LAUNCH(c, rb_candidates_kernel<STRONG>, (unsigned)ct, RB_TILE, 0, n, g.where, g.vwgt, B.pw, B.maxp, B.opt,
+              B.goff, B.gpart, B.gconn, B.und, (const int32_t *)&sc[S_NU], k, B.K, B.V, B.dest, d_cnt, B.pstart,
+              B.pend, c->lb_status, c->lb_ctl, c->d_status);
     bool in_tmp = false;
     HP_TRY(hp_sort_pairs(c, B.K, B.V, B.K2, B.V2, n, d_cnt, key_bits_for(k), &in_tmp));
     *Ks = in_tmp ? B.K2 : B.K;
     *Vs = in_tmp ? B.V2 : B.V;
-    HP_LAUNCH(c, weights_of_kernel, pg, 256, 0, (const int32_t *)nullptr, *Vs, d_cnt, g.vwgt, B.W);
-    HP_TRY(hp_scan_excl(c, B.W, B.pre, n));
-    HP_TRY(hp_fill_i32(c, B.pstart, k, -1));
-    HP_TRY(hp_fill_i32(c, B.pend, k, -1));
-    HP_LAUNCH(c, part_bounds_kernel, pg, 256, 0, *Ks, d_cnt, B.pstart, B.pend);
+    HP_LAUNCH(c, rb_rank_kernel, (unsigned)rt, RK_THREADS, 0, *Ks, *Vs, d_cnt, g.vwgt, B.pre, B.pstart, B.pend,
+              c->lb_status, c->lb_ctl, c->d_status);
     return HP_OK;
 }
 
+// The undersized-part list of a weak pass is built by ctl_begin_kernel.
 int weak_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
 {
-    const int32_t n = g.n;
     unsigned long long *sc = c->d_scal;
-    HP_LAUNCH(c, undersized_kernel, 1, 1024, 0, k, B.pw, B.maxp, B.und, (int32_t *)&sc[S_NU]);
-    HP_LAUNCH(c, rw_key_kernel, nblk(n), 256, 0, n, g.where, g.vwgt, B.pw, B.maxp, B.opt, B.goff,
-              B.gpart, B.gconn, B.und, (const int32_t *)&sc[S_NU], B.key, B.flag, B.dest);
     int32_t *Ks, *Vs;
-    HP_TRY(sort_candidates(c, g, B, k, &Ks, &Vs));
+    HP_TRY(rank_candidates<false>(c, g, B, k, &Ks, &Vs));
     HP_LAUNCH(c, rw_select_kernel, (unsigned)(c->sm_count * 8), 256, 0, Ks, Vs,
               (const int32_t *)&sc[S_LISTCNT], B.pre, B.pstart, B.pw, B.maxp, B.moves, &sc[S_NMOVES]);
     return HP_OK;
@@ -857,18 +1203,15 @@ int strong_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
 {
     const int32_t n = g.n;
     unsigned long long *sc = c->d_scal;
-    HP_LAUNCH(c, rs_key_kernel, nblk(n), 256, 0, n, g.where, g.vwgt, B.pw, B.maxp, B.opt, B.goff,
-              B.gpart, B.gconn, B.key, B.flag, B.dest, k);
     int32_t *Ks, *Vs;
-    HP_TRY(sort_candidates(c, g, B, k, &Ks, &Vs));
+    HP_TRY(rank_candidates<true>(c, g, B, k, &Ks, &Vs));
     const unsigned pg = (unsigned)(c->sm_count * 8);
     const int32_t *d_cnt = (const int32_t *)&sc[S_LISTCNT];
     int32_t *d_np = (int32_t *)&sc[S_NP];
     HP_LAUNCH(c, evict_end_kernel, nblk(k), 256, 0, k, B.pstart, B.pend, B.pre, B.pw, B.maxp, B.ev_end);
-    HP_LAUNCH(c, evict_flag_kernel, pg, 256, 0, Ks, d_cnt, B.ev_end, B.flag, (int64_t)n);
-    HP_TRY(hp_compact_flags(c, B.flag, n, B.P, d_np));
-    HP_LAUNCH(c, weights_of_kernel, pg, 256, 0, B.P, Vs, d_np, g.vwgt, B.W);
-    HP_TRY(hp_scan_excl(c, B.W, B.sp, n));
+    const int64_t rt = ((int64_t)n + RK_TILE) / RK_TILE;
+    HP_LAUNCH(c, rs_evict_kernel, (unsigned)rt, RK_THREADS, 0, Ks, Vs, d_cnt, B.ev_end, g.vwgt, B.P, B.sp, d_np,
+              c->lb_status, c->lb_cap / 2, c->lb_ctl, c->d_status);
     HP_LAUNCH(c, cookie_cutter_kernel, 1, 32, 0, k, B.pw, B.maxp, B.sp, d_np, B.es, B.ee);
     HP_LAUNCH(c, rs_assign_kernel, pg, 256, 0, k, B.P, d_np, Vs, B.es, B.ee, g.where, B.dest,
               B.moves, &sc[S_NMOVES]);
@@ -928,12 +1271,28 @@ __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int3
 
 // End of a pass: the exact cut change, the learned fallback, the stall rule, the
 // best partition and the loop condition, in the order of the host loop they replace.
-__global__ void ctl_end_kernel(RefineCtl *s, const unsigned long long *sc, cudaGraphConditionalHandle hloop,
-                               int graph)
+// One CTA of 1024 threads: the block first reduces the max excess over the
+// parts (max_p pw[p] - maxp[p]) into the status slot, then thread 0 advances
+// the control block.
+__global__ void __launch_bounds__(1024)
+ctl_end_kernel(RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle hloop, int graph, int32_t k,
+               const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp)
 {
+    long long m = LLONG_MIN;
+    for (int p = threadIdx.x; p < k; p += blockDim.x) {
+        const long long e = (long long)pw[p] - maxp[p];
+        m = e > m ? e : m;
+    }
+    m = hp::warp_max64(m);
+    __shared__ long long s_max[32];
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = s_max[w] > m ? s_max[w] : m;
+    sc[S_EXCESS] = (unsigned long long)m;
     const long long c1 = (long long)sc[S_C1], c2 = (long long)sc[S_C2];
     const long long nmoves = (long long)sc[S_NMOVES], ncand = (long long)sc[S_NCAND];
-    s->excess = (long long)sc[S_EXCESS];
+    s->excess = m;
     s->cut -= (c1 + c2) / 2;
     s->last_moves = nmoves;
     s->last_mode = s->mode;
@@ -969,12 +1328,20 @@ __global__ void ctl_end_kernel(RefineCtl *s, const unsigned long long *sc, cudaG
     if (graph) cudaGraphSetConditional(hloop, cont ? 1u : 0u);
 }
 
-// Start of a pass in the graph loop: clear the per-pass scalar slots and select
-// the proposal body (0 LP, 1 weak rebalance, 2 strong rebalance).
-__global__ void ctl_begin_kernel(const RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle hmode)
+// Start of a pass (one CTA of 1024 threads): clear the per-pass scalar slots,
+// in the graph loop select the proposal body (0 LP, 1 weak rebalance, 2 strong
+// rebalance), and for a weak pass build the undersized-part list.
+__global__ void __launch_bounds__(1024)
+ctl_begin_kernel(const RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle hmode, int graph, int32_t k,
+                 const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
+                 int32_t *__restrict__ und)
 {
+    __shared__ int32_t s_scan[1024 / 32 + 2];
     if (threadIdx.x < S_PASS_END) sc[threadIdx.x] = 0;
-    if (threadIdx.x == 0) cudaGraphSetConditional(hmode, (unsigned)s->mode);
+    const int mode = s->mode;
+    if (graph && threadIdx.x == 0) cudaGraphSetConditional(hmode, (unsigned)mode);
+    __syncthreads();
+    if (mode == 1) undersized_block(k, pw, maxp, und, (int32_t *)&sc[S_NU], s_scan);
 }
 
 __global__ void save_best_kernel(const RefineCtl *s, int32_t n, const int32_t *__restrict__ where,
@@ -1065,15 +1432,13 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
         HP_LAUNCH(c, apply_moves_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.moves, &sc[S_NMOVES], g.where,
                   B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l,
                   (int32_t *)&sc[S_DIRTY], k);
-    HP_LAUNCH(c, commit_moves_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest);
     const int rtok = hp_prof_begin(c);
     HP_TRY(build_rows(c, g, B, k, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
                       ((const int32_t *)&sc[S_DIRTY]) + 1, P.any_big, B.dirty));
     hp_prof_end(c, rtok, HP_PROF_REBUILD, 0);
     HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
               B.oldp, 0, &sc[S_C2], k);
-    HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);
-    HP_LAUNCH(c, ctl_end_kernel, 1, 1, 0, P.ctl, (const unsigned long long *)sc, hloop, graph);
+    HP_LAUNCH(c, ctl_end_kernel, 1, 1024, 0, P.ctl, sc, hloop, graph, k, B.pw, B.maxp);
     HP_LAUNCH(c, save_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, P.ctl, n,
               g.where, B.best_where, k, B.pw, P.best_pw);
     return HP_OK;
@@ -1138,7 +1503,7 @@ int run_passes_graph(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P,
     cudaGraph_t mode_body[3] = {nullptr, nullptr, nullptr};
     const int l0 = c->launches;
     HP_TRY(capture_into(c, body, [&]() -> int {
-        HP_LAUNCH(c, ctl_begin_kernel, 1, 32, 0, P.ctl, c->d_scal, hmode);
+        HP_LAUNCH(c, ctl_begin_kernel, 1, 1024, 0, P.ctl, c->d_scal, hmode, 1, P.k, B.pw, B.maxp, B.und);
         cudaStreamCaptureStatus cs;
         cudaGraph_t capg = nullptr;
         const cudaGraphNode_t *deps = nullptr;
@@ -1179,8 +1544,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.opt = d_opt;
     B.maxp = d_maxp;
     int32_t **n_arrays[] = {&B.goff, &B.big, &B.dest, &B.pregain, &B.moves, &B.oldp, &B.dirty,
-                            &B.small_l, &B.big_l, &B.best_where, &B.key, &B.flag, &B.list, &B.K,
-                            &B.V, &B.K2, &B.V2, &B.pre, &B.W, &B.P, &B.sp};
+                            &B.small_l, &B.big_l, &B.best_where, &B.K, &B.V, &B.K2, &B.V2, &B.pre,
+                            &B.P, &B.sp};
     for (auto pp : n_arrays) *pp = ralloc_t<int32_t>(c, (int64_t)n + 1);
     int32_t **k_arrays[] = {&B.pstart, &B.pend, &B.und, &B.ev_end, &B.es, &B.ee};
     for (auto pp : k_arrays) *pp = ralloc_t<int32_t>(c, k);
@@ -1190,17 +1555,19 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     RefineCtl *ctl = ralloc_t<RefineCtl>(c, 1);
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 1), c->stream));
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 2), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
     HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, d_bigcnt);
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
     // gain-row total and the level's count of rows longer than 32 (lets empty
     // classes skip their launches)
-    int32_t gb[2] = {0, 0};
+    int32_t gb[4] = {0, 0, 0, 0};
     HP_TRY(hp_read_scalars(c, B.goff + n, sizeof(int32_t), &gb[0]));
-    HP_TRY(hp_read_scalars(c, d_bigcnt, sizeof(int32_t), &gb[1]));
+    HP_TRY(hp_read_scalars(c, d_bigcnt, 3 * sizeof(int32_t), &gb[1]));
     const int32_t G = gb[0];
     B.G = G;
+    B.small_max = gb[2];
+    B.huge_rows = gb[3] > 0;
     B.gpart = ralloc_t<int32_t>(c, G);
     B.gconn = ralloc_t<int32_t>(c, G);
     HP_CHECK_OOM(c);
@@ -1249,7 +1616,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     } else {
         HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));
         while (h.cont) {
-            HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * S_PASS_END, c->stream));
+            HP_LAUNCH(c, ctl_begin_kernel, 1, 1024, 0, ctl, sc, cudaGraphConditionalHandle{}, 0, k, B.pw, B.maxp,
+                      B.und);
             HP_TRY(pass_propose(c, g, B, P, h.mode, h.learned_pass != 0, false));
             HP_TRY(pass_apply(c, g, B, P, 0, 0));
             HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));

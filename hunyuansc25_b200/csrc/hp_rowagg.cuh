@@ -57,6 +57,72 @@ __device__ __forceinline__ int warp_aggregate32(int32_t key, int32_t w, int32_t 
     return __popc(hm);
 }
 
+// ---- one row per thread, in registers ---------------------------------------
+// Entries are packed as key << 32 | weight (padding and dropped keys are
+// KEY_NONE) and sorted ascending by a bitonic network over the first NET of XN
+// registers (compile-time indices only, so the array stays in registers);
+// equal keys are then merged by summing the low halves.
+template <int NET, int XN>
+__device__ __forceinline__ void sort_regs(unsigned long long (&x)[XN])
+{
+#pragma unroll
+    for (int size = 2; size <= NET; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+#pragma unroll
+            for (int i = 0; i < NET; i++) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const unsigned long long a = x[i], b = x[j];
+                    const unsigned long long lo = a < b ? a : b, hi = a < b ? b : a;
+                    if ((i & size) == 0) { x[i] = lo; x[j] = hi; }
+                    else { x[i] = hi; x[j] = lo; }
+                }
+            }
+}
+
+constexpr unsigned long long PACK_NONE = (unsigned long long)(uint32_t)KEY_NONE << 32;
+
+// Segmented version: the warp holds 32/S independent rows of up to S entries
+// (lanes [S*r, S*r+S) hold row r); each segment is sorted by its own bitonic
+// network (log2 S stages), equal keys are merged, and every segment writes its
+// unique keys to its own out_k/out_w.  Returns the segment's unique count.
+template <int S>
+__device__ __forceinline__ int seg_aggregate(int32_t key, int32_t w, int32_t *out_k, int32_t *out_w)
+{
+    const int lane = threadIdx.x & 31;
+    const int sl = lane & (S - 1);
+#pragma unroll
+    for (int k = 2; k <= S; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int32_t pk = __shfl_xor_sync(HP_FULL_MASK, key, j);
+            const int32_t pw = __shfl_xor_sync(HP_FULL_MASK, w, j);
+            const bool up = (sl & k) == 0;
+            const bool lower = (sl & j) == 0;
+            const bool take = lower ? (up ? pk < key : pk > key) : (up ? pk > key : pk < key);
+            if (take) { key = pk; w = pw; }
+        }
+    }
+    int32_t s = w;
+#pragma unroll
+    for (int o = 1; o < S; o <<= 1) {
+        const int32_t t = __shfl_down_sync(HP_FULL_MASK, s, o, S);
+        const int32_t kk = __shfl_down_sync(HP_FULL_MASK, key, o, S);
+        if (sl + o < S && kk == key) s += t;
+    }
+    const int32_t prev = __shfl_up_sync(HP_FULL_MASK, key, 1, S);
+    const bool head = key != KEY_NONE && (sl == 0 || prev != key);
+    const unsigned seg = S == 32 ? 0xffffffffu : (((1u << S) - 1u) << (lane & ~(S - 1)));
+    const unsigned hm = __ballot_sync(HP_FULL_MASK, head) & seg;
+    if (head && out_k) {
+        const int r = __popc(hm & lanemask_lt());
+        out_k[r] = key;
+        out_w[r] = s;
+    }
+    return __popc(hm);
+}
+
 // Same aggregation written as a dense vector over keys [0, nkeys):
 // out_k[q] = q, out_w[q] = sum of the weights with key q (0 if none).
 __device__ __forceinline__ void warp_aggregate32_dense(int32_t key, int32_t w, int32_t nkeys,
@@ -174,6 +240,54 @@ __device__ __forceinline__ int dense_extract(int32_t *dw, unsigned *bm, int32_t 
                 out_w[p] = dw[k];
                 dw[k] = 0;
                 p++;
+            }
+        }
+        running += tot;
+    }
+    __syncthreads();
+    return running;
+}
+
+// Two-level variant for large key spaces: bm2[(nwords+31)/32] has one bit per
+// non-zero word of bm (set by the accumulating thread that turned the word
+// non-zero), so the extraction walks nkeys/1024 words plus the occupied bm
+// words instead of all nkeys/32.  dw, bm and bm2 are zero again on exit.
+__device__ __forceinline__ void dense_mark2(int32_t *dw, unsigned *bm, unsigned *bm2, int32_t k, int32_t w)
+{
+    atomicAdd(&dw[k], w);
+    const unsigned bit = 1u << (k & 31);
+    if (atomicOr(&bm[k >> 5], bit) == 0u) atomicOr(&bm2[k >> 10], 1u << ((k >> 5) & 31));
+}
+
+template <int NT>
+__device__ __forceinline__ int dense_extract2(int32_t *dw, unsigned *bm, unsigned *bm2, int32_t nkeys,
+                                              int32_t *out_k, int32_t *out_w, int32_t *s_scan)
+{
+    const int nwords = (nkeys + 31) >> 5;
+    const int nw2 = (nwords + 31) >> 5;
+    int running = 0;
+    for (int wb = 0; wb < nw2; wb += NT) {
+        const int i2 = wb + threadIdx.x;
+        const unsigned top = i2 < nw2 ? bm2[i2] : 0u;
+        int cnt = 0;
+        for (unsigned t = top; t; t &= t - 1) cnt += __popc(bm[(i2 << 5) + __ffs(t) - 1]);
+        int tot;
+        int p = running + block_excl_scan<NT>(cnt, &tot, s_scan);
+        if (top) {
+            bm2[i2] = 0u;
+            for (unsigned t = top; t; t &= t - 1) {
+                const int wi = (i2 << 5) + __ffs(t) - 1;
+                unsigned word = bm[wi];
+                bm[wi] = 0u;
+                while (word) {
+                    const int b = __ffs(word) - 1;
+                    word &= word - 1;
+                    const int32_t k = (wi << 5) + b;
+                    out_k[p] = k;
+                    out_w[p] = dw[k];
+                    dw[k] = 0;
+                    p++;
+                }
             }
         }
         running += tot;

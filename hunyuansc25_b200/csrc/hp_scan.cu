@@ -22,20 +22,21 @@ constexpr int SCAN_TILE = SCAN_BLOCK * SCAN_ITEMS;  // 4096
 __device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
 
 // Exclusive scan of in[0..n) into out[0..n] (out[n] = total); element n is a
-// virtual zero.  tile_status[ntiles] and *tile_counter must be zero on entry.
+// virtual zero.  EPOCH: the context's epoch look-back region (no clearing);
+// else tile_status[ntiles] and ctl->tile_counter must be zero on entry.
+template <bool EPOCH>
 __global__ void __launch_bounds__(SCAN_BLOCK)
 scan_excl_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n,
-                 unsigned long long *tile_status, unsigned *tile_counter, unsigned *status)
+                 unsigned long long *tile_status, hp::LbCtl *ctl, unsigned *status)
 {
     __shared__ int32_t s[SCAN_TILE + SCAN_TILE / 32];
     __shared__ int32_t s_warp[SCAN_BLOCK / 32];
-    __shared__ int32_t s_tile;
     __shared__ int32_t s_excl;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
 
-    if (tid == 0) s_tile = (int32_t)atomicAdd(tile_counter, 1u);
-    __syncthreads();
-    const int64_t tile = s_tile;
+    int64_t tile;
+    unsigned epoch;
+    hp::lb_begin(ctl, &tile, &epoch);
     const int64_t base = tile * SCAN_TILE;
 
 #pragma unroll
@@ -60,7 +61,8 @@ scan_excl_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int6
         int32_t ti = hp::warp_incl_scan(t);
         if (lane < SCAN_BLOCK / 32) s_warp[lane] = ti - t;  // exclusive warp offsets
         int32_t agg = __shfl_sync(HP_FULL_MASK, ti, SCAN_BLOCK / 32 - 1);
-        const int32_t excl = hp::lookback_exclusive(tile_status, tile, agg, status);
+        const int32_t excl = EPOCH ? hp::lookback_epoch(tile_status, tile, agg, epoch, status)
+                                   : hp::lookback_exclusive(tile_status, tile, agg, status);
         if (lane == 0) s_excl = excl;
     }
     __syncthreads();
@@ -77,6 +79,7 @@ scan_excl_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int6
         int64_t g = base + i;
         if (g <= n) out[g] = s[pad(i)];
     }
+    if (EPOCH) hp::lb_end(ctl);
 }
 
 __global__ void fill_kernel(int32_t *p, int64_t n, int32_t value)
@@ -146,24 +149,19 @@ int hp_scan_excl(hp_context *c, const int32_t *in, int32_t *out, int64_t n)
 {
     if (n < 0) return HP_ERR_INVALID_ARG;
     const int64_t ntiles = (n + 1 + SCAN_TILE - 1) / SCAN_TILE;
-    size_t mark = c->hi;
-    auto *st = ralloc_t<unsigned long long>(c, ntiles + 1);
-    HP_CHECK_OOM(c);
-    unsigned *counter = (unsigned *)(st + ntiles);
-    HP_CUDA(cudaMemsetAsync(st, 0, sizeof(unsigned long long) * (size_t)(ntiles + 1), c->stream));
-    HP_LAUNCH(c, scan_excl_kernel, (unsigned)ntiles, SCAN_BLOCK, 0, in, out, n, st, counter,
+    if (ntiles > c->lb_cap) return HP_ERR_INTERNAL;   // reserved at the start of every call
+    HP_LAUNCH(c, scan_excl_kernel<true>, (unsigned)ntiles, SCAN_BLOCK, 0, in, out, n, c->lb_status, c->lb_ctl,
               c->d_status);
-    c->hi = mark;
     return HP_OK;
 }
 
 // ---- scan without any allocation ---------------------------------------------------
 // Fixed scratch in the library's device image: the look-back tile status words
-// for up to HP_SCAN_NOALLOC_MAX_N elements, then the dynamic tile counter and a
-// status word (one 8-byte slot each).  Every GPU that loads the library holds
-// this array (about 128 KiB) until the process exits.
+// for up to HP_SCAN_NOALLOC_MAX_N elements, then the tile-counter block (two
+// 8-byte slots) and a status word (one slot).  Every GPU that loads the library
+// holds this array (about 128 KiB) until the process exits.
 #define HP_NOALLOC_TILES ((HP_SCAN_NOALLOC_MAX_N + 1 + SCAN_TILE - 1) / SCAN_TILE)
-static __device__ __align__(256) unsigned long long g_scan_noalloc_scratch[HP_NOALLOC_TILES + 2];
+static __device__ __align__(256) unsigned long long g_scan_noalloc_scratch[HP_NOALLOC_TILES + 3];
 
 namespace {
 std::mutex g_noalloc_mu;
@@ -202,14 +200,15 @@ int hp_scan_exclusive_i32_noalloc(const int32_t *d_in, int32_t *d_out, int64_t n
     }
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t ntiles = (n + 1 + SCAN_TILE - 1) / SCAN_TILE;
-    unsigned long long *counter_slot = scratch + HP_NOALLOC_TILES;
-    unsigned long long *status_slot = scratch + HP_NOALLOC_TILES + 1;
+    unsigned long long *counter_slot = scratch + HP_NOALLOC_TILES;     // hp::LbCtl (two slots)
+    unsigned long long *status_slot = scratch + HP_NOALLOC_TILES + 2;
     // the array keeps the last call's contents: clear the tile words this call
     // uses, the counter and the status word
     HP_CUDA(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * (size_t)ntiles, s));
-    HP_CUDA(cudaMemsetAsync(counter_slot, 0, sizeof(unsigned long long) * 2, s));
-    scan_excl_kernel<<<(unsigned)ntiles, SCAN_BLOCK, 0, s>>>(d_in, d_out, n, scratch, (unsigned *)counter_slot,
-                                                             (unsigned *)status_slot);
+    HP_CUDA(cudaMemsetAsync(counter_slot, 0, sizeof(unsigned long long) * 3, s));
+    scan_excl_kernel<false><<<(unsigned)ntiles, SCAN_BLOCK, 0, s>>>(d_in, d_out, n, scratch,
+                                                                    (hp::LbCtl *)counter_slot,
+                                                                    (unsigned *)status_slot);
     HP_CUDA(cudaGetLastError());
     unsigned st = 0;
     HP_CUDA(cudaMemcpyAsync(&st, status_slot, sizeof(unsigned), cudaMemcpyDeviceToHost, s));

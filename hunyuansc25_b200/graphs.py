@@ -57,6 +57,7 @@ def _lib():
         lib.hp_read_metis.argtypes = [C.c_char_p, C.POINTER(_HpGraph), C.c_char_p, C.c_int]
         lib.hp_write_partition.argtypes = [C.c_char_p, C.POINTER(C.c_int32), C.c_int32, C.c_int32]
         lib.hp_write_metis.argtypes = [C.c_char_p, C.POINTER(_HpGraph)]
+        lib.hp_read_mtx.argtypes = [C.c_char_p, C.POINTER(_HpGraph), C.c_char_p, C.c_int]
         _LIB = lib
     return _LIB
 
@@ -111,6 +112,29 @@ def read_metis(path: str) -> Graph:
     if rc != 0:
         raise ValueError(f"{path}: {err.value.decode() or rc}")
     return _take(g, os.path.basename(path))
+
+
+def read_mtx(path: str) -> Graph:
+    """Read a square MatrixMarket coordinate matrix as the graph of its
+    symmetrised pattern (diagonal dropped, unit weights); replaces the
+    reference's converter matrix_to_graph/matrix_to_graph.c."""
+    g = _HpGraph()
+    err = C.create_string_buffer(512)
+    rc = _lib().hp_read_mtx(path.encode(), C.byref(g), err, 512)
+    if rc != 0:
+        raise ValueError(f"{path}: {err.value.decode() or rc}")
+    return _take(g, os.path.basename(path))
+
+
+def mtx_to_metis(mtx_path: str, graph_path: str | None = None) -> str:
+    """Convert a .mtx file to a METIS .graph file (by default next to it, with
+    the extension replaced, as the reference's converter names it)."""
+    if graph_path is None:
+        base = mtx_path[:-4] if mtx_path.endswith(".mtx") else mtx_path
+        graph_path = base + ".graph"
+    g = read_mtx(mtx_path)
+    write_metis(graph_path, Graph(g.xadj, g.adjncy, g.vwgt, g.adjwgt))
+    return graph_path
 
 
 def write_metis(path: str, g: Graph) -> None:

@@ -1,5 +1,5 @@
 /*
- * hp_io.h — METIS .graph reader and .part writer (host, C ABI).
+ * hp_io.h — METIS .graph reader and .part writer, MatrixMarket reader (host, C ABI).
  *
  * Reference interface replaced:
  *   hunyuangraph_graph_t *hunyuangraph_readgraph(char *filename)   hunyuangraph_io.h:25-187
@@ -31,6 +31,15 @@ int hp_write_partition(const char *fname, const int32_t *part, int32_t n, int32_
 
 /* Writes a graph in METIS format (fmt 011 when weights are present). */
 int hp_write_metis(const char *path, const hp_graph *g);
+
+/* Reads a square MatrixMarket coordinate matrix (pattern, integer, real or
+ * complex; general, symmetric, skew-symmetric or hermitian) as the graph of
+ * its symmetrised pattern: an edge {i, j} for every stored entry off the
+ * diagonal, duplicates merged, rows sorted, unit vertex and edge weights.
+ * Replaces the reference's converter (matrix_to_graph/matrix_to_graph.c:
+ * union of the rows of A and A^T, diagonal removed, written as METIS).
+ * Returns 0, -1 (cannot open), -2 (format error; message in err), -3 (memory). */
+int hp_read_mtx(const char *path, hp_graph *out, char *err, int errlen);
 
 #ifdef __cplusplus
 }
