@@ -320,6 +320,54 @@ void hp_prof_resolve(hp_context *c)
 }
 
 // ---- shared helpers -------------------------------------------------------------
+static void reaper_main(hp_context *c)
+{
+    cudaSetDevice(c->device);
+    for (;;) {
+        hp_context::Retired r;
+        {
+            std::unique_lock<std::mutex> lk(c->reaper_mu);
+            c->reaper_cv.wait(lk, [c] { return c->reaper_stop || !c->reaper_q.empty(); });
+            if (c->reaper_q.empty()) return;   // stop requested and nothing left
+            r = std::move(c->reaper_q.front());
+            c->reaper_q.pop_front();
+        }
+        cudaEventSynchronize(r.done);
+        for (auto &it : r.graphs) {
+            if (it.second) cudaGraphExecDestroy(it.second);
+            if (it.first) cudaGraphDestroy(it.first);
+        }
+        cudaEventDestroy(r.done);
+    }
+}
+
+int hp_graph_retire(hp_context *c, std::vector<std::pair<cudaGraph_t, cudaGraphExec_t>> &&graphs)
+{
+    if (graphs.empty()) return HP_OK;
+    hp_context::Retired r;
+    r.graphs = std::move(graphs);
+    cudaError_t e = cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(r.done, c->stream);
+    if (e != cudaSuccess) {
+        // fall back to a synchronous release
+        cudaGetLastError();
+        cudaStreamSynchronize(c->stream);
+        for (auto &it : r.graphs) {
+            if (it.second) cudaGraphExecDestroy(it.second);
+            if (it.first) cudaGraphDestroy(it.first);
+        }
+        if (r.done) cudaEventDestroy(r.done);
+        return HP_OK;
+    }
+    {
+        std::lock_guard<std::mutex> lk(c->reaper_mu);
+        if (!c->reaper.joinable()) c->reaper = std::thread(reaper_main, c);
+        c->reaper_q.push_back(std::move(r));
+    }
+    c->reaper_cv.notify_one();
+    return HP_OK;
+}
+
 int hp_lb_reserve(hp_context *c, int64_t tiles)
 {
     if (tiles <= c->lb_cap && c->lb_ctl) return HP_OK;
@@ -454,6 +502,14 @@ HP_API void hp_context_destroy(hp_context *c)
     if (!c) return;
     for (hp_context *w : c->workers) hp_context_destroy(w);
     c->workers.clear();
+    if (c->reaper.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(c->reaper_mu);
+            c->reaper_stop = true;
+        }
+        c->reaper_cv.notify_one();
+        c->reaper.join();   // releases every queued graph first
+    }
     cudaSetDevice(c->device);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->arena) cudaFree(c->arena);

@@ -2,6 +2,11 @@
 #pragma once
 
 #include <algorithm>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <utility>
 #include <vector>
 
 #include "hp_common.cuh"
@@ -64,6 +69,19 @@ struct hp_context {
     unsigned long long *log_count = nullptr;
     int64_t log_cap = 0;
 
+    // Graph reaper: executable graphs are released by a background thread once
+    // the event recorded after their last launch has completed, so that their
+    // destruction never delays the stream (hp_graph_retire, hp_api.cu).
+    struct Retired {
+        cudaEvent_t done;
+        std::vector<std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
+    };
+    std::thread reaper;
+    std::mutex reaper_mu;
+    std::condition_variable reaper_cv;
+    std::deque<Retired> reaper_q;
+    bool reaper_stop = false;
+
     std::vector<hp_context *> workers;   // batch worker contexts (own streams and arenas)
     std::vector<HpLevel> levels;
     bool trace_valid = false;
@@ -119,6 +137,10 @@ void hp_prof_end(hp_context *c, int token, int cls, int64_t bytes);
 // Algorithmic bytes of an interval that are known only after it was closed.
 void hp_prof_add_bytes(hp_context *c, int token, int64_t bytes);
 void hp_prof_resolve(hp_context *c);
+
+// Hands graphs whose last launch is enqueued on c->stream to the reaper thread
+// (started on first use); they are destroyed once that work has completed.
+int hp_graph_retire(hp_context *c, std::vector<std::pair<cudaGraph_t, cudaGraphExec_t>> &&graphs);
 
 // Ensures room for `tiles` look-back words (called at the start of a call,
 // before any launch that could use them).

@@ -15,6 +15,7 @@
 // vertex id) via a stable radix sort, the cut is int64, balance is judged
 // against integer maximum part weights, and one status read per pass replaces
 // the reference's 4-6 blocking reads.
+#include <chrono>
 #include <cstdlib>
 
 #include "hp_internal.cuh"
@@ -51,6 +52,34 @@ __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int
         if (d > HUGED) atomicMax(d_bigcnt + 2, d);
     } else if (d > 8) {
         atomicMax(d_bigcnt + 1, d);
+    }
+}
+
+// Degree statistics of a level, computed for every level at the start of
+// uncoarsening so that the host chooses each level's kernels without reading
+// anything back per level: rows longer than BIGD, the longest row of 9..BIGD
+// entries, the longest row overall.
+struct LevelStat {
+    int32_t nbig, small_max, maxdeg, pad;
+};
+
+__global__ void __launch_bounds__(256)
+level_stats_kernel(int32_t n, const int32_t *__restrict__ xadj, LevelStat *st)
+{
+    int32_t nbig = 0, smax = 0, dmax = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t d = xadj[v + 1] - xadj[v];
+        if (d > BIGD) nbig++;
+        else if (d > 8) smax = d > smax ? d : smax;
+        dmax = d > dmax ? d : dmax;
+    }
+    nbig = hp::warp_sum(nbig);
+    smax = __reduce_max_sync(HP_FULL_MASK, (unsigned)smax);
+    dmax = __reduce_max_sync(HP_FULL_MASK, (unsigned)dmax);
+    if ((threadIdx.x & 31) == 0) {
+        if (nbig) atomicAdd(&st->nbig, nbig);
+        if (smax) atomicMax(&st->small_max, smax);
+        if (dmax) atomicMax(&st->maxdeg, dmax);
     }
 }
 
@@ -1232,6 +1261,7 @@ struct RefineCtl {
     int32_t learned_active, learned_pass, mode, best_current;
     int32_t take, cont, patience, last_mode;
     int32_t mode_passes[4];
+    int32_t gain_entries, pad;   // G of the level (for the profiler's byte counts)
 };
 
 __device__ void ctl_prepare(RefineCtl *s)
@@ -1244,8 +1274,10 @@ __device__ void ctl_prepare(RefineCtl *s)
     s->mode_passes[s->mode]++;
 }
 
-__global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned)
+__global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned,
+                                const int32_t *gain_total)
 {
+    s->gain_entries = *gain_total;
     s->cut = (long long)sc[S_CUT2] / 2;
     s->excess = (long long)sc[S_EXCESS];
     s->cut_start = s->cut;
@@ -1478,14 +1510,34 @@ struct GraphHold {
     }
 };
 
+// The pass graphs of one uncoarsening.  Destroying a graph that is still
+// running waits for it, so they go to the context's reaper thread, which
+// releases them once the stream has passed their launches (also on error paths).
+struct GraphKeep {
+    hp_context *c = nullptr;
+    std::vector<std::pair<cudaGraph_t, cudaGraphExec_t>> items;
+    ~GraphKeep() { hp_graph_retire(c, std::move(items)); }
+};
+
 // The level's pass loop as one CUDA graph:
 //   WHILE (cont) { ctl_begin; SWITCH (mode) { LP | weak | strong }; apply; ctl_end; save_best }
 // ctl_end sets the WHILE condition, ctl_begin the SWITCH value; nothing returns to
 // the host between passes.  Launch accounting: kernels per body x passes per mode,
 // read back from the control block.
+// host milliseconds per step of run_passes_graph (HP_DEBUG_LEVELS diagnostics):
+// create+handles, body capture, mode captures, instantiate, launch, destroy
+double g_graph_host_ms[6];
+
 int run_passes_graph(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, bool both_lp, int *n_common,
-                     int n_mode[3])
+                     int n_mode[3], GraphKeep *keep)
 {
+    using clk = std::chrono::steady_clock;
+    auto tick = [](clk::time_point &t, int slot) {
+        const auto now = clk::now();
+        g_graph_host_ms[slot] += std::chrono::duration<double, std::milli>(now - t).count();
+        t = now;
+    };
+    auto t = clk::now();
     GraphHold H;
     HP_CUDA(cudaGraphCreate(&H.g, 0));
     cudaGraphConditionalHandle hloop;
@@ -1501,6 +1553,7 @@ int run_passes_graph(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P,
     cudaGraphConditionalHandle hmode;
     HP_CUDA(cudaGraphConditionalHandleCreate(&hmode, body, 0, 0));
     cudaGraph_t mode_body[3] = {nullptr, nullptr, nullptr};
+    tick(t, 0);
     const int l0 = c->launches;
     HP_TRY(capture_into(c, body, [&]() -> int {
         HP_LAUNCH(c, ctl_begin_kernel, 1, 1024, 0, P.ctl, c->d_scal, hmode, 1, P.k, B.pw, B.maxp, B.und);
@@ -1521,24 +1574,50 @@ int run_passes_graph(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P,
         return pass_apply(c, g, B, P, hloop, 1);
     }));
     *n_common = c->launches - l0;
+    tick(t, 1);
     for (int m = 0; m < 3; m++) {
         const int l1 = c->launches;
         HP_TRY(capture_into(c, mode_body[m], [&]() -> int { return pass_propose(c, g, B, P, m, false, both_lp); }));
         n_mode[m] = c->launches - l1;
     }
     c->launches = l0;
+    tick(t, 2);
     HP_CUDA(cudaGraphInstantiate(&H.x, H.g, 0));
+    tick(t, 3);
     HP_CUDA(cudaGraphLaunch(H.x, c->stream));
-    // the exec graph may be destroyed once its launch is enqueued
+    tick(t, 4);
+    keep->items.emplace_back(H.g, H.x);   // released after the stream has finished
+    H.g = nullptr;
+    H.x = nullptr;
+    tick(t, 5);
     return HP_OK;
 }
 
+// Enqueues the refinement of one level; nothing is read back unless the eager
+// loop, the kernel-class profiler or the move log needs it.  The level's control
+// block (ctl) holds its cuts and pass count when the stream reaches the end.
+// CUDA-graph pass loop unless the caller asked for eager launches, the move log
+// or the per-pass debug log is on, or the stream is the legacy one.
+bool graph_loop(const hp_context *c)
+{
+    const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
+    return !c->opt.eager && !recording && getenv("HP_DEBUG_PASSES") == nullptr && c->opt.refine_patience >= 0 &&
+           c->stream != nullptr && c->stream != cudaStreamLegacy;
+}
+
+// Kernels per pass body of a graphed level (for the launch count, resolved
+// with the control block's pass counts once the stream has finished).
+struct LevelLaunches {
+    bool graph = false;
+    int n_common = 0, n_mode[3] = {0, 0, 0};
+    int gain_tok = -1;   // profiler interval of the level's gain build (bytes completed at the end)
+};
+
 int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_t *d_opt,
-                 const int64_t *d_maxp, int64_t *cut_start, int64_t *cut_final, int *passes_out)
+                 const int64_t *d_maxp, const LevelStat &ls, RefineCtl *ctl, LevelLaunches *ll, GraphKeep *keep)
 {
     const int32_t n = g.n;
-    *passes_out = 0;
-    if (n == 0) { *cut_start = *cut_final = 0; return HP_OK; }
+    if (n == 0) return HP_OK;
     const size_t mark = c->hi;
     RefineBufs B{};
     B.opt = d_opt;
@@ -1552,30 +1631,32 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.lock = ralloc_t<int8_t>(c, n);
     B.pw = ralloc_t<unsigned long long>(c, k);
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
-    RefineCtl *ctl = ralloc_t<RefineCtl>(c, 1);
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 2), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
     HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, d_bigcnt);
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
-    // gain-row total and the level's count of rows longer than 32 (lets empty
-    // classes skip their launches)
-    int32_t gb[4] = {0, 0, 0, 0};
-    HP_TRY(hp_read_scalars(c, B.goff + n, sizeof(int32_t), &gb[0]));
-    HP_TRY(hp_read_scalars(c, d_bigcnt, 3 * sizeof(int32_t), &gb[1]));
-    const int32_t G = gb[0];
+    // the gain rows take G = sum min(deg, k) <= m entries: allocated for m, so
+    // that no count is read back (the profiler reads G for its byte count)
+    // (the eager loop, which reads back every pass anyway, reads G for the LP
+    // class's byte count; the graphed levels complete their gain-build bytes
+    // from the control block at the end of uncoarsening)
+    const bool eager_loop = !graph_loop(c);
+    int32_t G = (int32_t)std::max<int64_t>(g.m, 1);
+    if (c->opt.profile && eager_loop) HP_TRY(hp_read_scalars(c, B.goff + n, sizeof(int32_t), &G));
     B.G = G;
-    B.small_max = gb[2];
-    B.huge_rows = gb[3] > 0;
-    B.gpart = ralloc_t<int32_t>(c, G);
-    B.gconn = ralloc_t<int32_t>(c, G);
+    B.small_max = ls.small_max;
+    B.huge_rows = ls.maxdeg > HUGED;
+    B.gpart = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
+    B.gconn = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
     HP_CHECK_OOM(c);
-    const bool any_big = gb[1] > 0;
+    const bool any_big = ls.nbig > 0;
     int tok = hp_prof_begin(c);
     HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt, any_big, nullptr));
-    // xadj, adjncy, adjwgt, where (own), goff, gain rows out
-    hp_prof_end(c, tok, HP_PROF_GAIN, 4 * ((int64_t)n + 1) + 8 * g.m + 4 * (int64_t)n + 4 * ((int64_t)n + 1) + 8 * (int64_t)G);
+    // xadj, adjncy, adjwgt, where (own), goff in; gain rows (8 G) out
+    hp_prof_end(c, tok, HP_PROF_GAIN, 4 * ((int64_t)n + 1) + 8 * g.m + 4 * (int64_t)n + 4 * ((int64_t)n + 1));
+    ll->gain_tok = tok;
     HP_CUDA(cudaMemsetAsync(B.pw, 0, sizeof(unsigned long long) * (size_t)k, c->stream));
     HP_CUDA(cudaMemsetAsync(B.lock, 0, (size_t)n, c->stream));
     HP_CUDA(cudaMemsetAsync(B.dirty, 0, sizeof(int32_t) * (size_t)n, c->stream));
@@ -1591,7 +1672,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     const bool learned = c->opt.learned == 1 && c->mlp_ready;
     const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
     const int patience = c->opt.refine_patience;
-    HP_LAUNCH(c, ctl_init_kernel, 1, 1, 0, ctl, (const unsigned long long *)sc, patience, learned ? 1 : 0);
+    HP_LAUNCH(c, ctl_init_kernel, 1, 1, 0, ctl, (const unsigned long long *)sc, patience, learned ? 1 : 0,
+              (const int32_t *)(B.goff + n));
     int64_t log_r0 = 0;
     if (recording) {
         unsigned long long lc = 0;
@@ -1600,19 +1682,13 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     }
     PassCfg P{k, finest, any_big, recording, ctl, best_pw};
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
-    // CUDA-graph pass loop unless the caller asked for eager launches, the move
-    // log or the per-pass debug log is on, or the stream is the legacy one
-    const bool use_graph = !c->opt.eager && !recording && !dbg && patience >= 0 && c->stream != nullptr &&
-                           c->stream != cudaStreamLegacy;
+    const bool use_graph = graph_loop(c);
     RefineCtl h{};
     if (use_graph) {
-        int n_common = 0, n_mode[3] = {0, 0, 0};
-        HP_TRY(run_passes_graph(c, g, B, P, learned, &n_common, n_mode));
+        ll->graph = true;
+        HP_TRY(run_passes_graph(c, g, B, P, learned, &ll->n_common, ll->n_mode, keep));
         HP_LAUNCH(c, restore_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, ctl, n,
                   B.best_where, g.where);
-        HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));
-        c->launches += 1 + h.passes * n_common + h.mode_passes[0] * n_mode[0] + h.mode_passes[1] * n_mode[1] +
-                       h.mode_passes[2] * n_mode[2];   // + the graph's own launch
     } else {
         HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));
         while (h.cont) {
@@ -1636,10 +1712,6 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
             HP_LAUNCH(c, log_label_kernel, nblk(r1 - log_r0), 256, 0, log_r0, r1, g.where, c->log_v, c->log_d,
                       c->log_acc, c->log_y);
     }
-    *cut_start = h.cut_start;
-    *cut_final = h.best_cut;
-    *passes_out = h.passes;
-    HP_TRY(hp_check_status(c));
     c->hi = mark;
     return HP_OK;
 }
@@ -1658,19 +1730,46 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
     const int L = (int)c->levels.size() - 1;
     int64_t *d_opt = lalloc_t<int64_t>(c, nparts);
     int64_t *d_maxp = lalloc_t<int64_t>(c, nparts);
+    LevelStat *d_ls = lalloc_t<LevelStat>(c, L + 1);
+    RefineCtl *d_ctl = lalloc_t<RefineCtl>(c, L + 1);
     HP_CHECK_OOM(c);
     HP_CUDA(cudaMemcpyAsync(d_opt, h_opt, sizeof(int64_t) * nparts, cudaMemcpyHostToDevice, c->stream));
     HP_CUDA(cudaMemcpyAsync(d_maxp, h_maxp, sizeof(int64_t) * nparts, cudaMemcpyHostToDevice, c->stream));
+    // every level's degree statistics in one read: afterwards the levels are
+    // enqueued without waiting, so the host builds level l-1's pass graph while
+    // the device runs level l
+    HP_CUDA(cudaMemsetAsync(d_ls, 0, sizeof(LevelStat) * (size_t)(L + 1), c->stream));
+    HP_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(RefineCtl) * (size_t)(L + 1), c->stream));
+    for (int l = 0; l <= L; l++)
+        if (c->levels[l].n > 0)
+            HP_LAUNCH(c, level_stats_kernel, std::min<unsigned>(nblk(c->levels[l].n), (unsigned)(c->sm_count * 8)),
+                      256, 0, c->levels[l].n, c->levels[l].xadj, d_ls + l);
+    std::vector<LevelStat> ls(L + 1);
+    HP_CUDA(cudaMemcpyAsync(ls.data(), d_ls, sizeof(LevelStat) * (size_t)(L + 1), cudaMemcpyDeviceToHost,
+                            c->stream));
+    HP_CUDA(cudaStreamSynchronize(c->stream));
+    std::vector<LevelLaunches> ll(L + 1);
+    GraphKeep keep;
+    keep.c = c;
     const bool trace = c->opt.trace != 0;
-    // HP_DEBUG_LEVELS: per-level size, passes and device time on stderr
+    // HP_DEBUG_LEVELS: per-level size, passes, device time, host enqueue time and
+    // whether the device had gone idle before the level was enqueued (stderr,
+    // printed after the last level so that nothing is serialised)
     const bool dbg_levels = getenv("HP_DEBUG_LEVELS") != nullptr;
-    cudaEvent_t lev[2] = {nullptr, nullptr};
-    if (dbg_levels)
+    std::vector<cudaEvent_t> lev;
+    std::vector<double> host_ms(L + 1, 0.0);
+    std::vector<int> idle(L + 1, 0);
+    if (dbg_levels) {
+        lev.resize(2 * (L + 1));
         for (auto &e : lev) HP_CUDA(cudaEventCreate(&e));
-    int total_passes = 0;
+    }
     for (int l = L; l >= 0; l--) {
         HpLevel &g = c->levels[l];
-        if (dbg_levels) HP_CUDA(cudaEventRecord(lev[0], c->stream));
+        const auto t0 = std::chrono::steady_clock::now();
+        if (dbg_levels) {
+            idle[l] = cudaStreamQuery(c->stream) == cudaSuccess;
+            HP_CUDA(cudaEventRecord(lev[2 * l], c->stream));
+        }
         if (l < L)
             HP_LAUNCH(c, project_kernel, nblk(g.n), 256, 0, g.n, g.cmap, c->levels[l + 1].where, g.where);
         if (trace) {
@@ -1679,21 +1778,43 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
             HP_CHECK_OOM(c);
             HP_CUDA(cudaMemcpyAsync(g.where_start, g.where, sizeof(int32_t) * g.n, cudaMemcpyDeviceToDevice, c->stream));
         }
-        int passes = 0;
-        HP_TRY(refine_level(c, g, nparts, l == 0, d_opt, d_maxp, &g.cut_start, &g.cut_final, &passes));
-        total_passes += passes;
+        HP_TRY(refine_level(c, g, nparts, l == 0, d_opt, d_maxp, ls[l], d_ctl + l, &ll[l], &keep));
         if (dbg_levels) {
-            HP_CUDA(cudaEventRecord(lev[1], c->stream));
-            HP_CUDA(cudaEventSynchronize(lev[1]));
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, lev[0], lev[1]);
-            fprintf(stderr, "gpu level %d n=%d m=%lld passes=%d ms=%.3f\n", l, g.n, (long long)g.m, passes, ms);
+            HP_CUDA(cudaEventRecord(lev[2 * l + 1], c->stream));
+            host_ms[l] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         }
         if (trace)
             HP_CUDA(cudaMemcpyAsync(g.where_final, g.where, sizeof(int32_t) * g.n, cudaMemcpyDeviceToDevice, c->stream));
     }
-    for (auto e : lev)
-        if (e) cudaEventDestroy(e);
+    // results of every level: cuts and pass counts from the control blocks
+    std::vector<RefineCtl> hc(L + 1);
+    HP_CUDA(cudaMemcpyAsync(hc.data(), d_ctl, sizeof(RefineCtl) * (size_t)(L + 1), cudaMemcpyDeviceToHost,
+                            c->stream));
+    HP_CUDA(cudaStreamSynchronize(c->stream));
+    if (dbg_levels) {
+        for (int l = L; l >= 0; l--) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, lev[2 * l], lev[2 * l + 1]);
+            fprintf(stderr, "gpu level %d n=%d m=%lld passes=%d ms=%.3f host_ms=%.3f idle_before=%d\n", l,
+                    c->levels[l].n, (long long)c->levels[l].m, hc[l].passes, ms, host_ms[l], idle[l]);
+        }
+        for (auto e : lev) cudaEventDestroy(e);
+        fprintf(stderr, "graph host ms: create %.3f body %.3f modes %.3f instantiate %.3f launch %.3f destroy %.3f\n",
+                g_graph_host_ms[0], g_graph_host_ms[1], g_graph_host_ms[2], g_graph_host_ms[3], g_graph_host_ms[4],
+                g_graph_host_ms[5]);
+        for (double &x : g_graph_host_ms) x = 0.0;
+    }
+    int total_passes = 0;
+    for (int l = 0; l <= L; l++) {
+        HpLevel &g = c->levels[l];
+        g.cut_start = g.n > 0 ? hc[l].cut_start : 0;
+        g.cut_final = g.n > 0 ? hc[l].best_cut : 0;
+        total_passes += hc[l].passes;
+        hp_prof_add_bytes(c, ll[l].gain_tok, 8 * (int64_t)hc[l].gain_entries);
+        if (ll[l].graph)   // the graph's own launch + its kernels per pass
+            c->launches += 1 + hc[l].passes * ll[l].n_common + hc[l].mode_passes[0] * ll[l].n_mode[0] +
+                           hc[l].mode_passes[1] * ll[l].n_mode[1] + hc[l].mode_passes[2] * ll[l].n_mode[2];
+    }
     c->stats.refine_passes = total_passes;
-    return HP_OK;
+    return hp_check_status(c);
 }
