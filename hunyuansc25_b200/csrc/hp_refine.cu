@@ -37,11 +37,12 @@ __global__ void project_kernel(int32_t n, const int32_t *__restrict__ cmap,
     if (v < n) where[v] = cwhere[cmap[v]];
 }
 
-// Row capacities min(deg, k); rows longer than BIGD go on the big list;
-// d_bigcnt[1] records the longest short row above 8 entries (picks the
-// network of gain_thread_kernel), d_bigcnt[2] the longest row above HUGED.
+// Row capacities min(deg, k); rows longer than BIGD go on the big list, rows
+// longer than HUGED also on the hub list (count d_bigcnt[3]); d_bigcnt[1]
+// records the longest short row above 8 entries, d_bigcnt[2] the longest row
+// above HUGED.
 __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t k,
-                                int32_t *__restrict__ cap, int32_t *big, int32_t *d_bigcnt)
+                                int32_t *__restrict__ cap, int32_t *big, int32_t *huge, int32_t *d_bigcnt)
 {
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
@@ -49,7 +50,10 @@ __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int
     cap[v] = d < k ? d : k;
     if (d > BIGD) {
         big[atomicAdd(d_bigcnt, 1)] = v;
-        if (d > HUGED) atomicMax(d_bigcnt + 2, d);
+        if (d > HUGED) {
+            atomicMax(d_bigcnt + 2, d);
+            huge[atomicAdd(d_bigcnt + 3, 1)] = v;
+        }
     } else if (d > 8) {
         atomicMax(d_bigcnt + 1, d);
     }
@@ -618,39 +622,102 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
     }
 }
 
-__global__ void __launch_bounds__(512)
-afterburner_huge_kernel(const int32_t *__restrict__ big, const int32_t *__restrict__ d_bigcnt,
+// ---- hub rows (longer than HUGED): chunk plans ----------------------------------
+// The work on hub rows is cut into chunks of HUB_CHUNK entries dealt over the
+// whole grid.  A one-CTA kernel plans it per pass: it selects the hubs that have
+// work (afterburner: candidates; moves: moved hubs), writes each one's vertex,
+// its item (hub-list position or move index) and the exclusive prefix of the
+// chunk counts, so that a chunk finds its hub by a binary search.
+constexpr int HUB_CHUNK = 512;
+
+template <bool MOVES>
+__global__ void __launch_bounds__(1024)
+hub_plan_kernel(const int32_t *__restrict__ items, const int32_t *__restrict__ d_nitems,
+                const int32_t *__restrict__ moves, const int32_t *__restrict__ pregain,
+                const int32_t *__restrict__ xadj, int32_t *__restrict__ plan_v, int32_t *__restrict__ plan_item,
+                int32_t *__restrict__ plan_off, int32_t *__restrict__ d_plan)
+{
+    __shared__ int32_t s_scan[1024 / 32 + 2];
+    const int32_t ni = *d_nitems;
+    int32_t nsel = 0, nch = 0;
+    for (int32_t base = 0; base < ni; base += 1024) {
+        const int32_t t = base + threadIdx.x;
+        int32_t v = -1, c = 0;
+        if (t < ni) {
+            v = MOVES ? moves[items[t]] : items[t];
+            const bool take = MOVES || pregain[v] != NEG;
+            if (take) c = (xadj[v + 1] - xadj[v] + HUB_CHUNK - 1) / HUB_CHUNK;
+            else v = -1;
+        }
+        int tsel, tch;
+        const int psel = nsel + hp::block_excl_scan<1024>(v >= 0 ? 1 : 0, &tsel, s_scan);
+        const int pch = nch + hp::block_excl_scan<1024>(c, &tch, s_scan);
+        if (v >= 0) {
+            plan_v[psel] = v;
+            plan_item[psel] = MOVES ? items[t] : t;
+            plan_off[psel] = pch;
+        }
+        nsel += tsel;
+        nch += tch;
+    }
+    if (threadIdx.x == 0) {
+        d_plan[0] = nsel;
+        d_plan[1] = nch;
+    }
+}
+
+// chunk gc -> selected hub j (the last j with plan_off[j] <= gc)
+__device__ __forceinline__ int32_t plan_find(const int32_t *__restrict__ plan_off, int32_t nsel, int64_t gc)
+{
+    int32_t lo = 0, hi = nsel - 1;
+    while (lo < hi) {
+        const int32_t mid = (lo + hi + 1) >> 1;
+        if (plan_off[mid] <= gc) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Afterburner of the candidate hubs: every chunk adds its part of the change to
+// the hub's accumulator (ab_acc, indexed by hub-list position, zero on entry);
+// afterburner_huge_final_kernel then decides from the full sums.
+__global__ void __launch_bounds__(HUB_CHUNK)
+afterburner_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__restrict__ plan_item,
+                        const int32_t *__restrict__ plan_off, const int32_t *__restrict__ d_plan,
                         const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                         const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                         const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
-                        int8_t *__restrict__ lock, const unsigned long long *d_ncand,
-                        int32_t *__restrict__ moves, unsigned long long *d_nmoves)
+                        const unsigned long long *d_ncand, unsigned long long *__restrict__ ab_acc)
 {
     if (*d_ncand == 0ull) return;
-    __shared__ long long s_ch[16];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int32_t cnt = *d_bigcnt;
-    for (int32_t i = blockIdx.x; i < cnt; i += gridDim.x) {
-        const int32_t v = big[i];
-        if (xadj[v + 1] - xadj[v] <= HUGED) continue;
+    const int lane = threadIdx.x & 31;
+    const int32_t nsel = d_plan[0], nch = d_plan[1];
+    for (int64_t gc = blockIdx.x; gc < nch; gc += gridDim.x) {
+        const int32_t jp = plan_find(plan_off, nsel, gc);
+        const int32_t v = plan_v[jp];
+        const int32_t g = pregain[v], p = where[v], b = dest[v];
+        const int32_t e0 = xadj[v + 1];
+        const int32_t j = xadj[v] + (int32_t)(gc - plan_off[jp]) * HUB_CHUNK + threadIdx.x;
+        long long c = j < e0 ? ab_change(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where) : 0;
+        c = hp::warp_sum64(c);
+        if (lane == 0 && c != 0) atomicAdd(&ab_acc[plan_item[jp]], (unsigned long long)c);
+    }
+}
+
+__global__ void afterburner_huge_final_kernel(const int32_t *__restrict__ huge, const int32_t *__restrict__ d_nhuge,
+                                              const int32_t *__restrict__ pregain, const unsigned long long *d_ncand,
+                                              unsigned long long *__restrict__ ab_acc, int8_t *__restrict__ lock,
+                                              int32_t *__restrict__ moves, unsigned long long *d_nmoves)
+{
+    if (*d_ncand == 0ull) return;
+    const int32_t nh = *d_nhuge;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += gridDim.x * blockDim.x) {
+        const int32_t v = huge[i];
         const int32_t g = pregain[v];
-        long long ch = 0;
-        if (g != NEG) {
-            const int32_t p = where[v], b = dest[v];
-            for (int32_t j = xadj[v] + threadIdx.x; j < xadj[v + 1]; j += blockDim.x)
-                ch += ab_change(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where);
-        }
-        ch = hp::warp_sum64(ch);
-        if (lane == 0) s_ch[wid] = ch;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            long long tot = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); w++) tot += s_ch[w];
-            int8_t sel = (g != NEG) && ((long long)g + tot >= 0);
-            lock[v] = sel;
-            if (sel) moves[atomicAdd(d_nmoves, 1ull)] = v;
-        }
-        __syncthreads();
+        const long long tot = (long long)ab_acc[i];
+        ab_acc[i] = 0ull;
+        const int8_t sel = (g != NEG) && ((long long)g + tot >= 0);
+        lock[v] = sel;
+        if (sel) moves[atomicAdd(d_nmoves, 1ull)] = v;
     }
 }
 
@@ -721,7 +788,8 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
                    const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                    const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
                    int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
-                   int32_t *__restrict__ big_l, int32_t *counts, int32_t k)
+                   int32_t *__restrict__ big_l, int32_t *counts, int32_t k, int32_t *__restrict__ huge_mv,
+                   int32_t *__restrict__ d_nhuge)
 {
     const int64_t nm = (int64_t)*d_nmoves;
     const int lane = threadIdx.x & 31;
@@ -736,7 +804,15 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
             atomicAdd(&pw[p], (unsigned long long)(-(long long)w));
         }
         const int32_t b = xadj[v], e = xadj[v + 1];
-        if (e - b > HUGED) continue;   // CTA kernel below (it commits v)
+        if (e - b > HUGED) {
+            // neighbours of a hub are touched by apply_moves_huge_kernel, spread
+            // over the whole grid (it reads the old part from oldp)
+            if (lane == 0) {
+                huge_mv[atomicAdd(d_nhuge, 1)] = (int32_t)i;
+                where[v] = d;
+            }
+            continue;
+        }
         for (int32_t j0 = b; j0 < e; j0 += 32) {
             const int32_t j = j0 + lane;
             const bool valid = j < e;
@@ -747,28 +823,28 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
     }
 }
 
-__global__ void __launch_bounds__(512)
-apply_moves_huge_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
-                        int32_t *__restrict__ where, const int32_t *__restrict__ dest,
+// Neighbours of the moved hubs (queued by apply_moves_kernel, planned by
+// hub_plan_kernel<true>): chunks of HUB_CHUNK entries over the whole grid.  A
+// hub's old part comes from oldp (the hub itself is already committed).
+__global__ void __launch_bounds__(HUB_CHUNK)
+apply_moves_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__restrict__ plan_item,
+                        const int32_t *__restrict__ plan_off, const int32_t *__restrict__ d_plan,
+                        const int32_t *__restrict__ oldp, const int32_t *__restrict__ dest,
                         const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                         const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
                         int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
                         int32_t *__restrict__ big_l, int32_t *counts, int32_t k)
 {
-    const int64_t nm = (int64_t)*d_nmoves;
-    for (int64_t i = blockIdx.x; i < nm; i += gridDim.x) {
-        const int32_t v = moves[i];
-        if (xadj[v + 1] - xadj[v] <= HUGED) continue;
-        const int32_t p = where[v], d = dest[v];
-        const int32_t b = xadj[v], e = xadj[v + 1];
-        for (int32_t j0 = b; j0 < e; j0 += blockDim.x) {
-            const int32_t j = j0 + threadIdx.x;
-            const bool valid = j < e;
-            touch_neighbour(valid, valid ? adjncy[j] : 0, valid ? adjwgt[j] : 0, p, d, xadj, goff, gconn, dirty,
-                            small_l, big_l, counts, k);
-        }
-        __syncthreads();   // every thread has read where[v]
-        if (threadIdx.x == 0) where[v] = d;
+    const int32_t nsel = d_plan[0], nch = d_plan[1];
+    for (int64_t gc = blockIdx.x; gc < nch; gc += gridDim.x) {
+        const int32_t jp = plan_find(plan_off, nsel, gc);
+        const int32_t v = plan_v[jp];
+        const int32_t p = oldp[plan_item[jp]], d = dest[v];
+        const int32_t e = xadj[v + 1];
+        const int32_t j = xadj[v] + (int32_t)(gc - plan_off[jp]) * HUB_CHUNK + threadIdx.x;
+        const bool valid = j < e;
+        touch_neighbour(valid, valid ? adjncy[j] : 0, valid ? adjwgt[j] : 0, p, d, xadj, goff, gconn, dirty, small_l,
+                        big_l, counts, k);
     }
 }
 
@@ -1124,7 +1200,9 @@ __global__ void rs_assign_kernel(int32_t k, const int32_t *__restrict__ P, const
 // ---------------------------------------------------------------------------------
 struct RefineBufs {
     int32_t *goff, *gpart, *gconn, *big, *dest, *pregain, *moves, *oldp, *dirty;
-    int32_t *small_l, *big_l, *best_where;
+    int32_t *small_l, *big_l, *best_where, *huge_mv, *huge;
+    int32_t *plan_v, *plan_item, *plan_off, *plan_cnt;   // hub chunk plan of the current step
+    unsigned long long *ab_acc;   // afterburner sums of the hub rows (zero between passes)
     int8_t *lock;
     int32_t *K, *V, *K2, *V2, *pre, *P, *sp;
     int32_t *pstart, *pend, *und, *ev_end, *es, *ee;
@@ -1141,7 +1219,7 @@ struct RefineBufs {
 // S_BIGCNT (slots 16-17) holds the big-row count, the longest short row and the
 // longest row above HUGED.
 enum { S_NMOVES = 0, S_C1 = 1, S_C2 = 2, S_EXCESS = 3, S_NCAND = 4, S_CUT2 = 5, S_DIRTY = 6,
-       S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_PASS_END = 12, S_BIGCNT = 16 };
+       S_HUGEMV = 7, S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_PASS_END = 12, S_BIGCNT = 16 };
 
 int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_t *small_list,
                const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt,
@@ -1178,7 +1256,10 @@ int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_
         if (k <= WARP_DENSE_K)
             HP_LAUNCH(c, gain_bigwarp_kernel, (unsigned)(c->sm_count * 4), 32 * GW_WARPS, GW_WARPS * smem, big_list,
                       d_big_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
-        if (k > WARP_DENSE_K || B.huge_rows)
+        // rows longer than HUGED: every such row in a full build; in a rebuild only
+        // sparse ones (deg < k), which exist only when k > HUGED
+        const bool dense_rows = dirty ? (B.huge_rows && k > HUGED) : B.huge_rows;
+        if (k > WARP_DENSE_K || dense_rows)
             HP_LAUNCH(c, gain_dense_kernel<256>, (unsigned)(c->sm_count * 2), 256, smem, big_list, d_big_cnt,
                       g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
     }
@@ -1396,7 +1477,7 @@ __global__ void restore_best_kernel(const RefineCtl *s, int32_t n, const int32_t
 
 struct PassCfg {
     int32_t k;
-    bool finest, any_big, recording;
+    bool finest, any_big, recording, huge_rows;
     RefineCtl *ctl;
     unsigned long long *best_pw;
 };
@@ -1427,12 +1508,18 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
                       c->log_d, c->log_acc, c->log_count, c->log_cap);
         HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest,
                   B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
-        if (P.any_big) {
+        if (P.any_big)
             HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt, g.where,
                       B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
-            HP_LAUNCH(c, afterburner_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.big, d_bigcnt, g.xadj,
-                      g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves,
-                      &sc[S_NMOVES]);
+        if (P.huge_rows) {
+            const int32_t *d_nhuge = d_bigcnt + 3;
+            HP_LAUNCH(c, hub_plan_kernel<false>, 1, 1024, 0, B.huge, d_nhuge, B.moves, B.pregain, g.xadj, B.plan_v,
+                      B.plan_item, B.plan_off, B.plan_cnt);
+            HP_LAUNCH(c, afterburner_huge_kernel, (unsigned)(4 * c->sm_count), HUB_CHUNK, 0, B.plan_v, B.plan_item,
+                      B.plan_off, B.plan_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, &sc[S_NCAND],
+                      B.ab_acc);
+            HP_LAUNCH(c, afterburner_huge_final_kernel, (unsigned)c->sm_count, 256, 0, B.huge, d_nhuge, B.pregain,
+                      &sc[S_NCAND], B.ab_acc, B.lock, B.moves, &sc[S_NMOVES]);
         }
         if (P.recording)
             HP_LAUNCH(c, log_accept_kernel, nblk(n), 256, 0, n, B.oldp, B.lock, &sc[S_NCAND], c->log_acc);
@@ -1459,11 +1546,15 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
     HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
               B.oldp, 1, &sc[S_C1], k);
     HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw, g.xadj,
-              g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k);
-    if (P.any_big)
-        HP_LAUNCH(c, apply_moves_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, B.moves, &sc[S_NMOVES], g.where,
-                  B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l,
-                  (int32_t *)&sc[S_DIRTY], k);
+              g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k,
+              B.huge_mv, (int32_t *)&sc[S_HUGEMV]);
+    if (P.huge_rows) {
+        HP_LAUNCH(c, hub_plan_kernel<true>, 1, 1024, 0, B.huge_mv, (const int32_t *)&sc[S_HUGEMV], B.moves,
+                  B.pregain, g.xadj, B.plan_v, B.plan_item, B.plan_off, B.plan_cnt);
+        HP_LAUNCH(c, apply_moves_huge_kernel, (unsigned)(4 * c->sm_count), HUB_CHUNK, 0, B.plan_v, B.plan_item,
+                  B.plan_off, B.plan_cnt, B.oldp, B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty,
+                  B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k);
+    }
     const int rtok = hp_prof_begin(c);
     HP_TRY(build_rows(c, g, B, k, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
                       ((const int32_t *)&sc[S_DIRTY]) + 1, P.any_big, B.dirty));
@@ -1624,18 +1715,27 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.maxp = d_maxp;
     int32_t **n_arrays[] = {&B.goff, &B.big, &B.dest, &B.pregain, &B.moves, &B.oldp, &B.dirty,
                             &B.small_l, &B.big_l, &B.best_where, &B.K, &B.V, &B.K2, &B.V2, &B.pre,
-                            &B.P, &B.sp};
+                            &B.P, &B.sp, &B.huge_mv, &B.huge};
     for (auto pp : n_arrays) *pp = ralloc_t<int32_t>(c, (int64_t)n + 1);
     int32_t **k_arrays[] = {&B.pstart, &B.pend, &B.und, &B.ev_end, &B.es, &B.ee};
     for (auto pp : k_arrays) *pp = ralloc_t<int32_t>(c, k);
     B.lock = ralloc_t<int8_t>(c, n);
     B.pw = ralloc_t<unsigned long long>(c, k);
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
+    // at most m / (HUGED + 1) rows are longer than HUGED
+    const int64_t nhub_cap = std::min<int64_t>((int64_t)n, g.m / (HUGED + 1)) + 1;
+    B.ab_acc = ralloc_t<unsigned long long>(c, nhub_cap);
+    B.plan_v = ralloc_t<int32_t>(c, nhub_cap);
+    B.plan_item = ralloc_t<int32_t>(c, nhub_cap);
+    B.plan_off = ralloc_t<int32_t>(c, nhub_cap);
+    B.plan_cnt = ralloc_t<int32_t>(c, 2);
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 2), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
-    HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, d_bigcnt);
+    HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt);
+    if (ls.maxdeg > HUGED)
+        HP_CUDA(cudaMemsetAsync(B.ab_acc, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
     // the gain rows take G = sum min(deg, k) <= m entries: allocated for m, so
     // that no count is read back (the profiler reads G for its byte count)
@@ -1680,7 +1780,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
         log_r0 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
     }
-    PassCfg P{k, finest, any_big, recording, ctl, best_pw};
+    PassCfg P{k, finest, any_big, recording, B.huge_rows, ctl, best_pw};
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     const bool use_graph = graph_loop(c);
     RefineCtl h{};

@@ -113,3 +113,11 @@ def test_mtx_errors(tmp_path):
         graphs.read_mtx(str(p))
     with pytest.raises(ValueError):
         graphs.read_mtx(str(tmp_path / "missing.mtx"))
+
+
+def test_cli_argument_errors(capsys):
+    from hunyuansc25_b200.__main__ import main
+    with pytest.raises(SystemExit):
+        main([])
+    with pytest.raises(SystemExit):
+        main(["only_a_graph.graph"])
