@@ -392,7 +392,7 @@ def main():
     est = ctx.stats()
     source = {}
     for i in range(8):
-        if PROF_NAMES[i] in ("lp", "rebuild"):
+        if PROF_NAMES[i] in ("lp", "rebuild", "rebalance"):
             prof_ms[i] = est.prof_ms[i]
             prof_bytes[i] = est.prof_bytes[i]
             prof_launch[i] = est.prof_launches[i]

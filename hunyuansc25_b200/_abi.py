@@ -113,7 +113,7 @@ HP_PROF_GAIN = 2
 HP_PROF_LP = 3
 HP_PROF_REBUILD = 4
 HP_PROF_INIT = 5
-PROF_NAMES = ["match", "contract", "gain_build", "lp", "rebuild", "init_trials", "", ""]
+PROF_NAMES = ["match", "contract", "gain_build", "lp", "rebuild", "init_trials", "match_more", "rebalance"]
 
 
 I32P = C.POINTER(C.c_int32)

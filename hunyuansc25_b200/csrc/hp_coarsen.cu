@@ -42,19 +42,41 @@ constexpr int HUGE_DEG = 4096;   // rows longer than this use a CTA per vertex
 // unmatched it is still the best, and an empty set stays empty.  Only vertices
 // whose choice was matched away rescan their row (same result as a full rescan).
 __device__ __forceinline__ bool keep_proposal(bool later_round, int32_t v, const int32_t *__restrict__ pref,
-                                              const int32_t *__restrict__ match)
+                                              const int32_t *__restrict__ elig)
 {
     if (!later_round) return false;
     const int32_t pu = pref[v];
-    return pu < 0 || match[pu] == -1;
+    return pu < 0 || elig[pu] != INT_MAX;
 }
+
+// Running best candidate with a lazily computed tie key: a strictly heavier
+// edge wins without hashing, and the seeded tie key is computed only when
+// weights tie (and for the final best, before reductions compare it).  The
+// order is exactly hp::better's.
+struct BestCand {
+    int32_t u = -1, w = 0;
+    uint32_t h = 0;
+    bool hv = false;
+    __device__ __forceinline__ void offer(uint64_t lkey, int32_t v, int32_t cu, int32_t cw)
+    {
+        if (u < 0 || cw > w) { u = cu; w = cw; hv = false; return; }
+        if (cw < w) return;
+        if (!hv) { h = hp::edge_tie(lkey, v, u); hv = true; }
+        const uint32_t ch = hp::edge_tie(lkey, v, cu);
+        if (ch < h || (ch == h && cu < u)) { u = cu; h = ch; }
+    }
+    __device__ __forceinline__ void finish(uint64_t lkey, int32_t v)
+    {
+        if (u >= 0 && !hv) { h = hp::edge_tie(lkey, v, u); hv = true; }
+    }
+};
 
 template <bool ELIG>
 __global__ void __launch_bounds__(256)
 pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
-                  const int32_t *__restrict__ match, int32_t *__restrict__ pref, uint64_t lkey,
-                  int64_t maxvwgt, const unsigned long long *made_prev)
+                  const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
+                  uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
 {
     if (made_prev && *made_prev == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -62,14 +84,13 @@ pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__
     const int32_t b = xadj[v], e = xadj[v + 1];
     if (e - b > BIG_DEG) return;
     if (match[v] != -1) { pref[v] = -1; return; }
-    if (ELIG && keep_proposal(made_prev != nullptr, v, pref, match)) return;
+    if (ELIG && keep_proposal(made_prev != nullptr, v, pref, elig)) return;
     const int32_t wv = vwgt[v];
-    int32_t bu = -1, bw = 0;
-    uint32_t bh = 0;
+    BestCand best;
     // four entries at a time: the row loads, then the neighbour gathers, are
     // issued together so each thread keeps several misses in flight
     for (int32_t j0 = b; j0 < e; j0 += 4) {
-        int32_t u[4], w[4], mu[4], vu[4];
+        int32_t u[4], w[4], eu[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const bool in = j0 + q < e;
@@ -77,22 +98,18 @@ pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__
             w[q] = in ? adjwgt[j0 + q] : 0;
         }
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            mu[q] = (ELIG && u[q] != v) ? match[u[q]] : -1;
-            vu[q] = (ELIG && u[q] != v) ? vwgt[u[q]] : 0;
-        }
+        for (int q = 0; q < 4; q++) eu[q] = (ELIG && u[q] != v) ? elig[u[q]] : 0;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             if (u[q] == v) continue;
             if (ELIG) {
-                if (mu[q] != -1) continue;
-                if ((int64_t)wv + vu[q] > maxvwgt) continue;
+                if (eu[q] == INT_MAX) continue;                     // matched
+                if ((int64_t)wv + eu[q] > maxvwgt) continue;        // weight cap
             }
-            uint32_t h = hp::edge_tie(lkey, v, u[q]);
-            if (bu < 0 || hp::better(w[q], h, u[q], bw, bh, bu)) { bu = u[q]; bw = w[q]; bh = h; }
+            best.offer(lkey, v, u[q], w[q]);
         }
     }
-    pref[v] = bu;
+    pref[v] = best.u;
 }
 
 template <bool ELIG>
@@ -100,8 +117,8 @@ __global__ void __launch_bounds__(256)
 pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                 const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                 const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
-                const int32_t *__restrict__ match, int32_t *__restrict__ pref, uint64_t lkey,
-                int64_t maxvwgt, const unsigned long long *made_prev)
+                const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
+                uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
 {
     if (made_prev && *made_prev == 0ull) return;
     const int lane = threadIdx.x & 31;
@@ -110,21 +127,22 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = list[i];
         if (match[v] != -1) { if (lane == 0) pref[v] = -1; continue; }
-        if (ELIG && keep_proposal(made_prev != nullptr, v, pref, match)) continue;
+        if (ELIG && keep_proposal(made_prev != nullptr, v, pref, elig)) continue;
         const int32_t wv = vwgt[v];
-        int32_t bu = -1, bw = 0;
-        uint32_t bh = 0;
+        BestCand best;
         for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32) {
             int32_t u = adjncy[j];
             if (u == v) continue;
             if (ELIG) {
-                if (match[u] != -1) continue;
-                if ((int64_t)wv + vwgt[u] > maxvwgt) continue;
+                const int32_t eu = elig[u];
+                if (eu == INT_MAX) continue;                     // matched
+                if ((int64_t)wv + eu > maxvwgt) continue;        // weight cap
             }
-            int32_t w = adjwgt[j];
-            uint32_t h = hp::edge_tie(lkey, v, u);
-            if (bu < 0 || hp::better(w, h, u, bw, bh, bu)) { bu = u; bw = w; bh = h; }
+            best.offer(lkey, v, u, adjwgt[j]);
         }
+        best.finish(lkey, v);
+        int32_t bu = best.u, bw = best.w;
+        uint32_t bh = best.h;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
@@ -136,26 +154,215 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
     }
 }
 
+// ---- handshake proposals of long rows with a top-4 candidate cache ---------------
+// A full scan of a long row keeps the TOPK best eligible candidates (in
+// hp::better order).  Between rounds the eligible set only shrinks, so in a
+// later round the first cached candidate that is still unmatched is exactly the
+// best eligible neighbour; if the cache held fewer than TOPK candidates its
+// exhaustion means none is left.  Only a vertex whose full cache was matched
+// away rescans its row.  Results equal a full rescan every round.
+constexpr int TOPK = 4;
+
+struct TopList {
+    int32_t u[TOPK], w[TOPK];
+    uint32_t h[TOPK];
+    __device__ __forceinline__ void init()
+    {
+#pragma unroll
+        for (int q = 0; q < TOPK; q++) { u[q] = -1; w[q] = 0; h[q] = 0u; }
+    }
+    // the tie key is computed only when the candidate can enter the list
+    __device__ __forceinline__ void offer(uint64_t lkey, int32_t v, int32_t cu, int32_t cw)
+    {
+        if (u[TOPK - 1] >= 0 && cw < w[TOPK - 1]) return;
+        uint32_t ch = hp::edge_tie(lkey, v, cu);
+        if (u[TOPK - 1] >= 0 && !hp::better(cw, ch, cu, w[TOPK - 1], h[TOPK - 1], u[TOPK - 1])) return;
+        int32_t iu = cu, iw = cw;
+#pragma unroll
+        for (int q = 0; q < TOPK; q++) {
+            if (iu >= 0 && (u[q] < 0 || hp::better(iw, ch, iu, w[q], h[q], u[q]))) {
+                const int32_t tu = u[q], tw = w[q];
+                const uint32_t th = h[q];
+                u[q] = iu; w[q] = iw; h[q] = ch;
+                iu = tu; iw = tw; ch = th;
+            }
+        }
+    }
+    __device__ __forceinline__ void head(int ptr, int32_t &hu, int32_t &hw, uint32_t &hh) const
+    {
+        hu = -1; hw = 0; hh = 0u;
+#pragma unroll
+        for (int q = 0; q < TOPK; q++)
+            if (ptr == q) { hu = u[q]; hw = w[q]; hh = h[q]; }
+    }
+};
+
+// The TOPK best of the 32 lanes' lists, best first, in every lane (out[q] = -1
+// when fewer exist).  Neighbours of a row are distinct, so the maxima agree.
+__device__ __forceinline__ void warp_topk(const TopList &t, int32_t (&out)[TOPK])
+{
+    const int lane = threadIdx.x & 31;
+    int ptr = 0;
+#pragma unroll
+    for (int r = 0; r < TOPK; r++) {
+        int32_t bu, bw;
+        uint32_t bh;
+        t.head(ptr, bu, bw, bh);
+        int bl = lane;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
+            const int32_t ow = __shfl_xor_sync(HP_FULL_MASK, bw, o);
+            const uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
+            const int ol = __shfl_xor_sync(HP_FULL_MASK, bl, o);
+            if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; bl = ol; }
+        }
+        out[r] = bu;
+        if (bu >= 0 && lane == bl) ptr++;
+    }
+}
+
+// Later rounds: the proposal from the cache, or -2 when the row must be rescanned.
+__device__ __forceinline__ int32_t cached_proposal(const int32_t *__restrict__ cand, int32_t v,
+                                                  const int32_t *__restrict__ elig)
+{
+#pragma unroll
+    for (int q = 0; q < TOPK; q++) {
+        const int32_t cu = cand[(int64_t)v * TOPK + q];
+        if (cu < 0) return -1;                  // the cache held every eligible candidate
+        if (elig[cu] != INT_MAX) return cu;     // still unmatched: the best now
+    }
+    return -2;
+}
+
+__global__ void __launch_bounds__(256)
+pref_big_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                     const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                     const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
+                     const int32_t *__restrict__ match, const int32_t *__restrict__ elig,
+                     int32_t *__restrict__ pref, int32_t *__restrict__ cand, uint64_t lkey, int64_t maxvwgt,
+                     const unsigned long long *made_prev)
+{
+    if (made_prev && *made_prev == 0ull) return;
+    const int lane = threadIdx.x & 31;
+    const int32_t cnt = *d_count;
+    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
+         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+        const int32_t v = list[i];
+        if (match[v] != -1) { if (lane == 0) pref[v] = -1; continue; }
+        if (made_prev) {
+            const int32_t cp = cached_proposal(cand, v, elig);
+            if (cp != -2) { if (lane == 0) pref[v] = cp; continue; }
+        }
+        const int32_t wv = vwgt[v];
+        TopList t;
+        t.init();
+        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32) {
+            const int32_t u = adjncy[j];
+            if (u == v) continue;
+            const int32_t eu = elig[u];
+            if (eu == INT_MAX) continue;                     // matched
+            if ((int64_t)wv + eu > maxvwgt) continue;        // weight cap
+            t.offer(lkey, v, u, adjwgt[j]);
+        }
+        int32_t top[TOPK];
+        warp_topk(t, top);
+        if (lane < TOPK) cand[(int64_t)v * TOPK + lane] = top[lane];
+        if (lane == 0) pref[v] = top[0];
+    }
+}
+
+__global__ void __launch_bounds__(512)
+pref_huge_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                      const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                      const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
+                      const int32_t *__restrict__ match, const int32_t *__restrict__ elig,
+                      int32_t *__restrict__ pref, int32_t *__restrict__ cand, uint64_t lkey, int64_t maxvwgt,
+                      const unsigned long long *made_prev)
+{
+    if (made_prev && *made_prev == 0ull) return;
+    __shared__ int32_t su[16][TOPK], sw[16][TOPK];
+    __shared__ uint32_t sh[16][TOPK];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int32_t cnt = *d_count;
+    for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
+        const int32_t v = list[li];
+        if (match[v] != -1) { if (threadIdx.x == 0) pref[v] = -1; continue; }
+        if (made_prev) {
+            const int32_t cp = cached_proposal(cand, v, elig);
+            if (cp != -2) { if (threadIdx.x == 0) pref[v] = cp; continue; }
+        }
+        const int32_t wv = vwgt[v];
+        TopList t;
+        t.init();
+        for (int32_t j = xadj[v] + threadIdx.x; j < xadj[v + 1]; j += blockDim.x) {
+            const int32_t u = adjncy[j];
+            if (u == v) continue;
+            const int32_t eu = elig[u];
+            if (eu == INT_MAX) continue;
+            if ((int64_t)wv + eu > maxvwgt) continue;
+            t.offer(lkey, v, u, adjwgt[j]);
+        }
+        // per warp: its TOPK best, with their weights and keys (taken from the lists)
+        {
+            int32_t top[TOPK];
+            warp_topk(t, top);
+            // the owner lane of each winner publishes its (w, h); a winner is in
+            // exactly one lane's list
+#pragma unroll
+            for (int q = 0; q < TOPK; q++) {
+#pragma unroll
+                for (int s2 = 0; s2 < TOPK; s2++)
+                    if (top[q] >= 0 && t.u[s2] == top[q]) { sw[wid][q] = t.w[s2]; sh[wid][q] = t.h[s2]; }
+                if (lane == 0) su[wid][q] = top[q];
+            }
+        }
+        __syncthreads();
+        if (wid == 0) {
+            TopList m;
+            m.init();
+            if (lane < (int)(blockDim.x >> 5)) {
+#pragma unroll
+                for (int q = 0; q < TOPK; q++) {
+                    m.u[q] = su[lane][q];
+                    m.w[q] = m.u[q] >= 0 ? sw[lane][q] : 0;
+                    m.h[q] = m.u[q] >= 0 ? sh[lane][q] : 0u;
+                }
+            }
+            int32_t top[TOPK];
+            warp_topk(m, top);
+            if (lane < TOPK) cand[(int64_t)v * TOPK + lane] = top[lane];
+            if (lane == 0) pref[v] = top[0];
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void __launch_bounds__(256)
 commit_kernel(int32_t n, int32_t *__restrict__ match, const int32_t *__restrict__ pref,
-              unsigned long long *made_cur, const unsigned long long *made_prev)
+              int32_t *__restrict__ elig, unsigned long long *made_cur, const unsigned long long *made_prev)
 {
     if (made_prev && *made_prev == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int made = 0;
     if (v < n && match[v] == -1) {
         int32_t u = pref[v];
-        if (u >= 0 && pref[u] == v) { match[v] = u; made = 1; }
+        if (u >= 0 && pref[u] == v) {
+            match[v] = u;
+            elig[v] = INT_MAX;   // no longer a candidate of anyone
+            made = 1;
+        }
     }
     hp::block_add_to<256>(made, made_cur);
 }
 
 __global__ void __launch_bounds__(256)
 big_list_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t *list, int32_t *d_count,
-                int32_t *huge, int32_t *d_huge)
+                int32_t *huge, int32_t *d_huge, const int32_t *__restrict__ vwgt, int32_t *__restrict__ elig)
 {
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
+    elig[v] = vwgt[v];   // every vertex starts unmatched
     const int32_t d = xadj[v + 1] - xadj[v];
     if (d > HUGE_DEG) huge[atomicAdd(d_huge, 1)] = v;
     else if (d > BIG_DEG) list[atomicAdd(d_count, 1)] = v;
@@ -167,8 +374,8 @@ __global__ void __launch_bounds__(512)
 pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                  const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                  const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
-                 const int32_t *__restrict__ match, int32_t *__restrict__ pref, uint64_t lkey,
-                 int64_t maxvwgt, const unsigned long long *made_prev)
+                 const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
+                 uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
 {
     if (made_prev && *made_prev == 0ull) return;
     __shared__ int32_t su[16], sw[16];
@@ -178,21 +385,22 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t v = list[li];
         if (match[v] != -1) { if (threadIdx.x == 0) pref[v] = -1; continue; }
-        if (ELIG && keep_proposal(made_prev != nullptr, v, pref, match)) continue;
+        if (ELIG && keep_proposal(made_prev != nullptr, v, pref, elig)) continue;
         const int32_t wv = vwgt[v];
-        int32_t bu = -1, bw = 0;
-        uint32_t bh = 0;
+        BestCand best;
         for (int32_t j = xadj[v] + threadIdx.x; j < xadj[v + 1]; j += blockDim.x) {
             int32_t u = adjncy[j];
             if (u == v) continue;
             if (ELIG) {
-                if (match[u] != -1) continue;
-                if ((int64_t)wv + vwgt[u] > maxvwgt) continue;
+                const int32_t eu = elig[u];
+                if (eu == INT_MAX) continue;                     // matched
+                if ((int64_t)wv + eu > maxvwgt) continue;        // weight cap
             }
-            int32_t w = adjwgt[j];
-            uint32_t h = hp::edge_tie(lkey, v, u);
-            if (bu < 0 || hp::better(w, h, u, bw, bh, bu)) { bu = u; bw = w; bh = h; }
+            best.offer(lkey, v, u, adjwgt[j]);
         }
+        best.finish(lkey, v);
+        int32_t bu = best.u, bw = best.w;
+        uint32_t bh = best.h;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
@@ -740,11 +948,26 @@ __device__ int group_gather_row(const ContractSrc &src, int32_t c, const RowInfo
 {
     const int t = threadIdx.x % G;
     int self = 0;
-    for (int i = t; i < len; i += G) {
-        int32_t k, w;
-        src.get(c, r, i, k, w);
-        self += k == hp::KEY_NONE;
-        A[i] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)w;
+    // four entries per thread at a time: the row loads, then the coarse-id
+    // gathers, are issued together
+    for (int i0 = t; i0 < len; i0 += 4 * G) {
+        int32_t j[4], a[4], w[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = i0 + q * G;
+            j[q] = i < len ? (i < r.l0 ? r.s0 + i : r.s1 + (i - r.l0)) : -1;
+            a[q] = j[q] >= 0 ? src.adjncy[j[q]] : 0;
+            w[q] = j[q] >= 0 ? src.adjwgt[j[q]] : 0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (j[q] < 0) continue;
+            int32_t k = src.cmap[a[q]];
+            int32_t ww = w[q];
+            if (k == c) { k = hp::KEY_NONE; ww = 0; }
+            self += k == hp::KEY_NONE;
+            A[i0 + q * G] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)ww;
+        }
     }
     int tot;
     group_excl_scan<G>(self, &tot, s_scan);
@@ -781,32 +1004,42 @@ contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__re
 }
 
 // CTA class: 256 threads per row.
+// CTA class: one CTA of NT threads per row of at most CAP entries.  Two
+// instances: <256, 4096> for the rows of 257..4096 entries (list 1) and
+// <1024, 12288> for the rows of 4097..12288 entries taken from list 2, whose
+// longer rows stay with the dense kernel; 2 CAP packed entries plus NT/32
+// digit histograms fit the 227 KB of shared memory of one CTA.
 constexpr int CROW_THREADS = 256;
-__global__ void __launch_bounds__(CROW_THREADS)
+constexpr int XROW_THREADS = 1024, XROW_MAX = 12288;
+
+template <int NT, int CAP>
+__global__ void __launch_bounds__(NT)
 contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, ContractSrc src,
                           const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
                           int32_t *__restrict__ ucnt, int kbits)
 {
     extern __shared__ unsigned long long dsm[];
-    unsigned long long *A = dsm, *B = dsm + CROW_MAX;
-    int32_t *hist = (int32_t *)(dsm + 2 * CROW_MAX);
-    __shared__ int32_t s_scan[2 * (CROW_THREADS / 32) + 2];
+    unsigned long long *A = dsm, *B = dsm + CAP;
+    int32_t *hist = (int32_t *)(dsm + 2 * CAP);
+    __shared__ int32_t s_scan[2 * (NT / 32) + 2];
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t c = list[li];
         RowInfo r;
         int32_t len;
         src.row(c, r, len);
-        const int N = group_gather_row<CROW_THREADS>(src, c, r, len, A, s_scan);
-        group_radix_sort<CROW_THREADS>(A, B, len, kbits, hist, s_scan);
+        if (len > CAP) continue;   // the dense kernel's row
+        const int N = group_gather_row<NT>(src, c, r, len, A, s_scan);
+        group_radix_sort<NT>(A, B, len, kbits, hist, s_scan);
         const int32_t off = toff[c];
-        const int U = group_merge_emit<CROW_THREADS>(A, N, tk + off, tw + off, (uint32_t *)B, s_scan);
+        const int U = group_merge_emit<NT>(A, N, tk + off, tw + off, (uint32_t *)B, s_scan);
         if (threadIdx.x == 0) ucnt[c] = U;
         __syncthreads();
     }
 }
 
-constexpr size_t cta_radix_smem() { return sizeof(unsigned long long) * 2 * CROW_MAX + sizeof(int32_t) * 256 * (CROW_THREADS / 32); }
+template <int NT, int CAP>
+constexpr size_t cta_radix_smem() { return sizeof(unsigned long long) * 2 * CAP + sizeof(int32_t) * 256 * (NT / 32); }
 
 
 // Rows longer than 4096 entries: dense accumulator over the coarse id space in
@@ -828,18 +1061,32 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
         RowInfo r;
         int32_t len;
         src.row(c, r, len);
+        if (len <= XROW_MAX) continue;   // contract_cta_radix_kernel<1024, XROW_MAX>'s row
         // a row much shorter than the bitmap walks the occupied words through
         // the second level; a denser row scans the bitmap directly
         const bool two_level = (int64_t)len * 4 < ((int64_t)cn + 31) / 32;
-        for (int32_t i = threadIdx.x; i < len; i += NT) {
-            int32_t k, w;
-            src.get(c, r, i, k, w);
-            if (k == hp::KEY_NONE) continue;
-            if (two_level) {
-                hp::dense_mark2(dw, bm, bm2, k, w);
-            } else {
-                atomicAdd(&dw[k], w);
-                atomicOr(&bm[k >> 5], 1u << (k & 31));
+        for (int32_t i0 = threadIdx.x; i0 < len; i0 += 4 * NT) {
+            int32_t a[4], wq[4];
+            bool in[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int32_t i = i0 + q * NT;
+                in[q] = i < len;
+                const int32_t j = in[q] ? (i < r.l0 ? r.s0 + i : r.s1 + (i - r.l0)) : 0;
+                a[q] = in[q] ? src.adjncy[j] : 0;
+                wq[q] = in[q] ? src.adjwgt[j] : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (!in[q]) continue;
+                const int32_t k = src.cmap[a[q]];
+                if (k == c) continue;   // the coarse self key
+                if (two_level) {
+                    hp::dense_mark2(dw, bm, bm2, k, wq[q]);
+                } else {
+                    atomicAdd(&dw[k], wq[q]);
+                    atomicOr(&bm[k >> 5], 1u << (k & 31));
+                }
             }
         }
         __syncthreads();
@@ -876,6 +1123,10 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     int32_t *huge = ralloc_t<int32_t>(c, n);
     int32_t *flags = ralloc_t<int32_t>(c, n + 1);
     int32_t *list = ralloc_t<int32_t>(c, n + 1);
+    // candidate state: vwgt while unmatched, INT_MAX once matched (one gather
+    // per neighbour in the proposal kernels)
+    int32_t *elig = ralloc_t<int32_t>(c, n);
+    int32_t *cand = ralloc_t<int32_t>(c, (int64_t)n * TOPK);   // candidate caches of the long rows
     HP_CHECK_OOM(c);
     // scalar slots: [0] big count, [1] list count, [2..2+R) made per round, [40..43] matched counts
     unsigned long long *sc = c->d_scal;
@@ -885,7 +1136,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     int32_t *d_hugecnt = (int32_t *)&sc[38];
 
     HP_TRY(hp_fill_i32(c, g.match, n, -1));
-    HP_LAUNCH(c, big_list_kernel, blocks_for(n), 256, 0, n, g.xadj, big, d_bigcnt, huge, d_hugecnt);
+    HP_LAUNCH(c, big_list_kernel, blocks_for(n), 256, 0, n, g.xadj, big, d_bigcnt, huge, d_hugecnt, g.vwgt, elig);
 
     const int rounds = o.match_rounds < 1 ? 1 : (o.match_rounds > 30 ? 30 : o.match_rounds);
     // algorithmic bytes of one full handshake round: xadj, adjncy, adjwgt,
@@ -895,13 +1146,13 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
         const int tok = hp_prof_begin(c);
         const unsigned long long *prev = r == 0 ? nullptr : &sc[2 + r - 1];
         HP_LAUNCH(c, pref_small_kernel<true>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
-                  g.vwgt, g.match, pref, lkey, maxvwgt, prev);
-        HP_LAUNCH(c, pref_big_kernel<true>, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj,
-                  g.adjncy, g.adjwgt, g.vwgt, g.match, pref, lkey, maxvwgt, prev);
-        HP_LAUNCH(c, pref_huge_kernel<true>, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
-                  g.adjncy, g.adjwgt, g.vwgt, g.match, pref, lkey, maxvwgt, prev);
-        HP_LAUNCH(c, commit_kernel, blocks_for(n), 256, 0, n, g.match, pref, &sc[2 + r], prev);
-        hp_prof_end(c, tok, r == 0 ? HP_PROF_MATCH : 6, r == 0 ? round_bytes : 0);
+                  g.vwgt, g.match, elig, pref, lkey, maxvwgt, prev);
+        HP_LAUNCH(c, pref_big_topk_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
+                  g.vwgt, g.match, elig, pref, cand, lkey, maxvwgt, prev);
+        HP_LAUNCH(c, pref_huge_topk_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
+                  g.adjncy, g.adjwgt, g.vwgt, g.match, elig, pref, cand, lkey, maxvwgt, prev);
+        HP_LAUNCH(c, commit_kernel, blocks_for(n), 256, 0, n, g.match, pref, elig, &sc[2 + r], prev);
+        hp_prof_end(c, tok, r == 0 ? HP_PROF_MATCH : HP_PROF_MATCH_MORE, r == 0 ? round_bytes : 0);
     }
 
     auto matched = [&](int slot, int64_t *out) -> int {
@@ -913,16 +1164,17 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     };
     int64_t nm = 0;
     HP_TRY(matched(40, &nm));
+    const int ftok = hp_prof_begin(c);
     if (4 * nm < 3 * (int64_t)n) {
         // two-hop through a shared heaviest neighbour
         int32_t *hub = pref;
         HP_LAUNCH(c, pref_small_kernel<false>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
-                  g.vwgt, g.match, hub, lkey, maxvwgt, (const unsigned long long *)nullptr);
+                  g.vwgt, g.match, elig, hub, lkey, maxvwgt, (const unsigned long long *)nullptr);
         HP_LAUNCH(c, pref_big_kernel<false>, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj,
-                  g.adjncy, g.adjwgt, g.vwgt, g.match, hub, lkey, maxvwgt,
+                  g.adjncy, g.adjwgt, g.vwgt, g.match, elig, hub, lkey, maxvwgt,
                   (const unsigned long long *)nullptr);
         HP_LAUNCH(c, pref_huge_kernel<false>, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
-                  g.adjncy, g.adjwgt, g.vwgt, g.match, hub, lkey, maxvwgt,
+                  g.adjncy, g.adjwgt, g.vwgt, g.match, elig, hub, lkey, maxvwgt,
                   (const unsigned long long *)nullptr);
         HP_LAUNCH(c, pair_hub_small_kernel, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.vwgt, hub,
                   g.match, maxvwgt);
@@ -930,6 +1182,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
                   g.vwgt, hub, g.match, maxvwgt);
         HP_LAUNCH(c, pair_hub_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
                   g.adjncy, g.vwgt, hub, g.match, maxvwgt);
+        hp_prof_end(c, ftok, HP_PROF_MATCH_MORE, 0);
         HP_TRY(matched(41, &nm));
     }
     for (int pass = 0; pass < 2; pass++) {
@@ -1004,9 +1257,15 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
                       (unsigned)std::min<int64_t>((h.cnt[0] + WROW_WARPS - 1) / WROW_WARPS, c->sm_count * 6),
                       32 * WROW_WARPS, 0, lists, &counts[0], src, toff, tk, tw, ucnt, kbits);
         if (h.cnt[1] > 0)
-            HP_LAUNCH(c, contract_cta_radix_kernel, (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 3),
-                      CROW_THREADS, cta_radix_smem(), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits);
-        if (h.cnt[2] > 0) {
+            HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
+                      (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 3), CROW_THREADS,
+                      (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits);
+        if (h.cnt[2] > 0)
+            HP_LAUNCH(c, (contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>),
+                      (unsigned)std::min<int64_t>(h.cnt[2], c->sm_count), XROW_THREADS,
+                      (cta_radix_smem<XROW_THREADS, XROW_MAX>()), lists + 2 * (int64_t)cn, &counts[2], src, toff, tk,
+                      tw, ucnt, kbits);
+        if (h.maxlen > XROW_MAX) {
             // slab per CTA: cn ints + cn/32 + cn/1024 words; bounded to ~512 MB
             const int64_t nw = ((int64_t)cn + 31) / 32, nw2 = ((int64_t)cn + 1023) / 1024;
             int64_t slab = (int64_t)cn * 4 + nw * 4 + nw2 * 4;
@@ -1058,8 +1317,12 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
 
 int hp_coarsen_init()
 {
-    HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)cta_radix_smem()));
+    HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_radix_smem<CROW_THREADS, CROW_MAX>()));
+    HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_radix_smem<XROW_THREADS, XROW_MAX>()));
     return HP_OK;
 }
 

@@ -192,6 +192,26 @@ __device__ __forceinline__ void lb_begin(LbCtl *ctl, int64_t *tile, unsigned *ep
     *epoch = s_e;
 }
 
+// Persistent form: a CTA reads the launch's epoch once (lb_epoch), then takes
+// tiles in launch order with lb_next until it passes its last tile; a CTA only
+// waits on tiles taken before its own, by running CTAs.
+__device__ __forceinline__ unsigned lb_epoch(LbCtl *ctl)
+{
+    __shared__ unsigned s_e;
+    if (threadIdx.x == 0) s_e = *(volatile unsigned *)&ctl->epoch;
+    __syncthreads();
+    return s_e;
+}
+
+__device__ __forceinline__ int64_t lb_next(LbCtl *ctl)
+{
+    __shared__ unsigned s_t;
+    __syncthreads();   // every thread is done with the previous tile's shared data
+    if (threadIdx.x == 0) s_t = atomicAdd(&ctl->tile_counter, 1u);
+    __syncthreads();
+    return s_t;
+}
+
 // All threads of the CTA, after its last write: the last CTA to finish resets
 // the counters and advances the epoch.
 __device__ __forceinline__ void lb_end(LbCtl *ctl)

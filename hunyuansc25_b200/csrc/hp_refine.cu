@@ -960,8 +960,9 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
 // Over the sorted candidates: pre[i] = weight of the candidates before i in
 // the sorted order (pre[cnt] = total), and the part bounds pstart/pend (first
 // index, one past the last) from the sorted keys.  Tiles of RK_TILE items in
-// launch order with an epoch look-back; tiles beyond the count only take part
-// in the tile accounting.
+// launch order with an epoch look-back, taken by a fixed grid of persistent
+// CTAs until the tile holding index cnt, so the work follows the count on
+// the device, not n.
 constexpr int RK_THREADS = 256, RK_ITEMS = 4, RK_TILE = RK_THREADS * RK_ITEMS;
 
 __global__ void __launch_bounds__(RK_THREADS)
@@ -971,12 +972,12 @@ rb_rank_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, con
 {
     __shared__ int32_t s_scan[RK_THREADS / 32 + 2];
     __shared__ int32_t s_excl;
-    int64_t tile;
-    unsigned epoch;
-    hp::lb_begin(lb, &tile, &epoch);
+    const unsigned epoch = hp::lb_epoch(lb);
     const int32_t cnt = *d_cnt;
-    const int64_t base = tile * RK_TILE;
-    if (base <= cnt) {
+    for (;;) {
+        const int64_t tile = hp::lb_next(lb);
+        const int64_t base = tile * RK_TILE;
+        if (base > cnt) break;   // the tile holding index cnt was the last one
         const int64_t i0 = base + (int64_t)threadIdx.x * RK_ITEMS;
         int32_t w[RK_ITEMS];
         int32_t sum = 0;
@@ -1048,7 +1049,7 @@ __global__ void evict_end_kernel(int32_t k, const int32_t *__restrict__ pstart,
 // i < ev_end[part]) compacted in sorted order -- P[j] = i and sp[j] = weight of
 // the evicted candidates before j (sp[np] = total), *d_np = np -- in one pass
 // with two epoch look-back chains (count: tile words [0, half); weight: words
-// [half, 2 half)).
+// [half, 2 half)); persistent CTAs as in rb_rank_kernel.
 __global__ void __launch_bounds__(RK_THREADS)
 rs_evict_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, const int32_t *__restrict__ d_cnt,
                 const int32_t *__restrict__ ev_end, const int32_t *__restrict__ vwgt, int32_t *__restrict__ P,
@@ -1057,12 +1058,12 @@ rs_evict_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, co
 {
     __shared__ int32_t s_scan[RK_THREADS / 32 + 2];
     __shared__ int32_t s_excl[2];
-    int64_t tile;
-    unsigned epoch;
-    hp::lb_begin(lb, &tile, &epoch);
+    const unsigned epoch = hp::lb_epoch(lb);
     const int32_t cnt = *d_cnt;
-    const int64_t base = tile * RK_TILE;
-    if (base <= cnt) {
+    for (;;) {
+        const int64_t tile = hp::lb_next(lb);
+        const int64_t base = tile * RK_TILE;
+        if (base > cnt) break;   // the tile holding index cnt was the last one
         const int64_t i0 = base + (int64_t)threadIdx.x * RK_ITEMS;
         int32_t w[RK_ITEMS];
         bool f[RK_ITEMS];
@@ -1111,13 +1112,25 @@ rs_evict_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, co
 // Rooms are read 32 parts at a time; a part without room keeps an empty range
 // (the rule gives end = start there); otherwise the end is searched first among
 // the 32 entries after the start (one coalesced read), then 32-ary over the rest.
-__global__ void cookie_cutter_kernel(int32_t k, const unsigned long long *__restrict__ pw,
-                                     const int64_t *__restrict__ maxp, const int32_t *__restrict__ sp,
-                                     const int32_t *__restrict__ d_np, int32_t *__restrict__ es,
-                                     int32_t *__restrict__ ee)
+// The whole CTA first stages sp[0..np] in shared memory when it fits
+// (COOKIE_SMEM_INTS entries), then warp 0 walks the parts; every search then
+// waits on shared memory instead of L2.
+constexpr int COOKIE_SMEM_INTS = 50 * 1024;
+
+__global__ void __launch_bounds__(1024)
+cookie_cutter_kernel(int32_t k, const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
+                     const int32_t *__restrict__ sp_g, const int32_t *__restrict__ d_np, int32_t *__restrict__ es,
+                     int32_t *__restrict__ ee)
 {
-    const int lane = threadIdx.x & 31;
+    extern __shared__ int32_t sp_s[];
     const int32_t np = *d_np;
+    const bool staged = np + 1 <= COOKIE_SMEM_INTS;
+    if (staged)
+        for (int32_t i = threadIdx.x; i <= np; i += blockDim.x) sp_s[i] = sp_g[i];
+    __syncthreads();
+    if (threadIdx.x >= 32) return;
+    const int32_t *sp = staged ? sp_s : sp_g;
+    const int lane = threadIdx.x & 31;
     int32_t st = 0;
     for (int32_t p0 = 0; p0 < k; p0 += 32) {
         const int32_t pl = p0 + lane;
@@ -1274,6 +1287,13 @@ int key_bits_for(int32_t k)
     return (bits + 7) / 8 * 8;
 }
 
+// Persistent grid of the rank/evict kernels: at most the tiles a count of n
+// can need, at most 8 CTAs per SM (they take tiles until the device count).
+unsigned rank_grid(const hp_context *c, int64_t tiles)
+{
+    return (unsigned)std::min<int64_t>(tiles, (int64_t)c->sm_count * 8);
+}
+
 // Candidates of the pass (rb_candidates_kernel, K/V in vertex order) -> stable
 // radix sort by key -> prefix weights and part bounds (rb_rank_kernel).
 // Returns the arrays holding the sorted pairs.
@@ -1293,7 +1313,7 @@ int rank_candidates(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, int32_t
     HP_TRY(hp_sort_pairs(c, B.K, B.V, B.K2, B.V2, n, d_cnt, key_bits_for(k), &in_tmp));
     *Ks = in_tmp ? B.K2 : B.K;
     *Vs = in_tmp ? B.V2 : B.V;
-    HP_LAUNCH(c, rb_rank_kernel, (unsigned)rt, RK_THREADS, 0, *Ks, *Vs, d_cnt, g.vwgt, B.pre, B.pstart, B.pend,
+    HP_LAUNCH(c, rb_rank_kernel, rank_grid(c, rt), RK_THREADS, 0, *Ks, *Vs, d_cnt, g.vwgt, B.pre, B.pstart, B.pend,
               c->lb_status, c->lb_ctl, c->d_status);
     return HP_OK;
 }
@@ -1320,9 +1340,10 @@ int strong_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
     int32_t *d_np = (int32_t *)&sc[S_NP];
     HP_LAUNCH(c, evict_end_kernel, nblk(k), 256, 0, k, B.pstart, B.pend, B.pre, B.pw, B.maxp, B.ev_end);
     const int64_t rt = ((int64_t)n + RK_TILE) / RK_TILE;
-    HP_LAUNCH(c, rs_evict_kernel, (unsigned)rt, RK_THREADS, 0, Ks, Vs, d_cnt, B.ev_end, g.vwgt, B.P, B.sp, d_np,
+    HP_LAUNCH(c, rs_evict_kernel, rank_grid(c, rt), RK_THREADS, 0, Ks, Vs, d_cnt, B.ev_end, g.vwgt, B.P, B.sp, d_np,
               c->lb_status, c->lb_cap / 2, c->lb_ctl, c->d_status);
-    HP_LAUNCH(c, cookie_cutter_kernel, 1, 32, 0, k, B.pw, B.maxp, B.sp, d_np, B.es, B.ee);
+    HP_LAUNCH(c, cookie_cutter_kernel, 1, 1024, sizeof(int32_t) * COOKIE_SMEM_INTS, k, B.pw, B.maxp, B.sp, d_np,
+              B.es, B.ee);
     HP_LAUNCH(c, rs_assign_kernel, pg, 256, 0, k, B.P, d_np, Vs, B.es, B.ee, g.where, B.dest,
               B.moves, &sc[S_NMOVES]);
     return HP_OK;
@@ -1526,10 +1547,11 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
         // select: goff, rows, where, lock in; dest, pregain out.  afterburner:
         // xadj, adjncy, adjwgt, own pregain/dest/where in, lock out
         hp_prof_end(c, ltok, HP_PROF_LP, 8 * ((int64_t)n + 1) + 8 * (int64_t)(B.G) + 8 * g.m + 26 * (int64_t)n);
-    } else if (mode == 1) {
-        HP_TRY(weak_rebalance(c, g, B, k));
     } else {
-        HP_TRY(strong_rebalance(c, g, B, k));
+        const int btok = hp_prof_begin(c);
+        if (mode == 1) HP_TRY(weak_rebalance(c, g, B, k));
+        else HP_TRY(strong_rebalance(c, g, B, k));
+        hp_prof_end(c, btok, HP_PROF_REBALANCE, 0);
     }
     return HP_OK;
 }
@@ -1820,6 +1842,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
 
 int hp_refine_init()
 {
+    HP_CUDA(cudaFuncSetAttribute(cookie_cutter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(int32_t) * COOKIE_SMEM_INTS)));
     const int bytes = HP_MAX_PARTS * 4 + (HP_MAX_PARTS / 32) * 4;
     HP_CUDA(cudaFuncSetAttribute(gain_dense_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     return HP_OK;

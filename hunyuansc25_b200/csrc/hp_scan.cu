@@ -255,15 +255,26 @@ int hp_edgecut_launch(hp_context *c, int32_t n, const int32_t *xadj, const int32
 }
 
 // ---------------------------------------------------------------------------
-// Stable LSD radix sort of (key, value) int32 pairs, 8-bit digits.
-// Pass: per-tile digit histograms stored digit-major, one exclusive scan over
-// them, then a stable scatter in which every tile ranks its items per digit
-// (warp __match_any_sync + per-warp digit counters in shared memory).
+// Stable LSD radix sort of (key, value) int32 pairs, 8-bit digits, on a fixed
+// grid (at most 4 blocks per SM) whatever the count on the device: block b
+// owns a contiguous chunk.  Pass: per-block digit histograms stored
+// digit-major, one exclusive scan over them, then a stable scatter in which
+// every block walks its chunk in order and ranks its items per digit (warp
+// __match_any_sync + per-warp digit counters in shared memory).
 namespace {
 
 constexpr int RS_BLOCK = 256;
 constexpr int RS_ITEMS = 4;
 constexpr int RS_TILE = RS_BLOCK * RS_ITEMS;
+
+// Items of each block: the count split over the fixed grid in whole rounds of
+// RS_BLOCK, block b taking [b chunk, (b+1) chunk) -- the blocks' chunks are in
+// order, so a block-major digit scan keeps the sort stable.
+__device__ __forceinline__ int64_t chunk_of(int32_t cnt, int32_t nblocks)
+{
+    int64_t ch = ((int64_t)cnt + nblocks - 1) / nblocks;
+    return (ch + RS_BLOCK - 1) / RS_BLOCK * RS_BLOCK;
+}
 
 __global__ void __launch_bounds__(RS_BLOCK)
 radix_hist_kernel(const int32_t *__restrict__ keys, const int32_t *__restrict__ d_count,
@@ -273,11 +284,10 @@ radix_hist_kernel(const int32_t *__restrict__ keys, const int32_t *__restrict__ 
     const int32_t cnt = *d_count;
     h[threadIdx.x] = 0;
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
-    for (int r = 0; r < RS_ITEMS; r++) {
-        int64_t i = base + r * RS_BLOCK + threadIdx.x;
-        if (i < cnt) atomicAdd(&h[((unsigned)keys[i] >> shift) & 255u], 1);
-    }
+    const int64_t chunk = chunk_of(cnt, nblocks);
+    const int64_t beg = (int64_t)blockIdx.x * chunk, end = min((int64_t)cnt, beg + chunk);
+    for (int64_t i = beg + threadIdx.x; i < end; i += RS_BLOCK)
+        atomicAdd(&h[((unsigned)keys[i] >> shift) & 255u], 1);
     __syncthreads();
     hist[(int64_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
@@ -288,17 +298,18 @@ radix_scatter_kernel(const int32_t *__restrict__ kin, const int32_t *__restrict_
                      const int32_t *__restrict__ hscan, int32_t *__restrict__ kout,
                      int32_t *__restrict__ vout)
 {
-    __shared__ int32_t run[256];                       // running per-digit offset of this tile
+    __shared__ int32_t run[256];                       // running per-digit offset of this block
     __shared__ int32_t wc[RS_BLOCK / 32][256];         // per-warp digit counts / offsets
     const int32_t cnt = *d_count;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     run[threadIdx.x] = hscan[(int64_t)threadIdx.x * nblocks + blockIdx.x];
-    const int64_t base = (int64_t)blockIdx.x * RS_TILE;
-    for (int r = 0; r < RS_ITEMS; r++) {
+    const int64_t chunk = chunk_of(cnt, nblocks);
+    const int64_t beg = (int64_t)blockIdx.x * chunk, end = min((int64_t)cnt, beg + chunk);
+    for (int64_t r0 = beg; r0 < end; r0 += RS_BLOCK) {   // the chunk in order, RS_BLOCK items a round
         for (int w = 0; w < RS_BLOCK / 32; w++) wc[w][threadIdx.x] = 0;
         __syncthreads();
-        int64_t i = base + r * RS_BLOCK + threadIdx.x;
-        bool valid = i < cnt;
+        int64_t i = r0 + threadIdx.x;
+        bool valid = i < end;
         int32_t k = valid ? kin[i] : 0, v = valid ? vin[i] : 0;
         unsigned d = valid ? (((unsigned)k >> shift) & 255u) : 256u + lane;  // invalid: unique
         unsigned peers = __match_any_sync(HP_FULL_MASK, d);
@@ -331,7 +342,8 @@ int hp_sort_pairs(hp_context *c, int32_t *keys, int32_t *vals, int32_t *tkeys, i
 {
     *in_tmp = false;
     if (bound <= 0) return HP_OK;
-    const int32_t nblocks = (int32_t)((bound + RS_TILE - 1) / RS_TILE);
+    // a fixed grid whatever the count on the device: each block sorts its chunk
+    const int32_t nblocks = (int32_t)std::min<int64_t>((bound + RS_TILE - 1) / RS_TILE, 4 * (int64_t)c->sm_count);
     const size_t mark = c->hi;
     int32_t *hist = ralloc_t<int32_t>(c, (int64_t)nblocks * 256 + 1);
     HP_CHECK_OOM(c);

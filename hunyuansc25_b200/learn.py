@@ -158,8 +158,24 @@ def main(argv=None):
     ap.add_argument("--out", default=DEFAULT_WEIGHTS)
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--sweep-only", action="store_true",
+                    help="keep the weights of --out, re-choose only the threshold on the validation graphs")
+    ap.add_argument("--max-cut-ratio", type=float, default=1.0,
+                    help="accept thresholds whose mean cut (learned / plain) is at most this")
     args = ap.parse_args(argv)
     ctx = hp.Context(0)
+    if args.sweep_only:
+        params, thr_old, meta = load_params(args.out)
+        cands = [-2.0, -1.5, -1.25, -1.0, -0.75, -0.5, -0.25, 0.0, 0.25]
+        thr, report = sweep_threshold(ctx, params, cands, validation_graphs(), args.max_cut_ratio)
+        for t, r, sp in report:
+            print(f"threshold {t:+.3f}: cut ratio {r:.4f}, speed-up {sp:.3f}")
+        if thr is None:
+            thr = thr_old
+        print(f"threshold {thr_old:+.3f} -> {thr:+.3f}")
+        save_params(args.out, params, thr, meta + f" | threshold re-swept (max cut ratio {args.max_cut_ratio})")
+        ctx.close()
+        return 0
     x, y = collect(ctx, training_graphs())
     n = x.shape[0]
     rng = np.random.default_rng(args.seed)

@@ -77,6 +77,8 @@ typedef struct hp_options {
 #define HP_PROF_LP        3   /* LP destination selection + afterburner        */
 #define HP_PROF_REBUILD   4   /* gain rows of moved vertices' neighbourhoods   */
 #define HP_PROF_INIT      5   /* bisection trials                              */
+#define HP_PROF_MATCH_MORE 6  /* handshake rounds after the first + fallbacks  */
+#define HP_PROF_REBALANCE 7   /* weak/strong rebalance proposals (eager passes) */
 #define HP_PROF_NCLASS    8
 
 /* Timing and quality of the last call on a context. */
