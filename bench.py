@@ -172,7 +172,21 @@ def config_of(args, spec, g, m_und):
             "nparts": spec["k"], "ubfactor": spec["ub"],
             "coarsen_to": spec["coarsen_to"] or "reference rule (8k, or max(1024,2k) when 8k > 1024)",
             "parallelism": f"replicas x{args.gpus} (a single graph does not shard)",
-            "l2": "flushed before every timed step (256 MiB write)"}
+            "l2": "flushed before every timed step (256 MiB write)",
+            "tuning": tuning_name(args)}
+
+
+def tuning_name(args):
+    from hunyuansc25_b200 import tune
+    p = tune.resolve_tuning(args.tuning, args.workload)
+    return os.path.relpath(p, ROOT) if p else "defaults"
+
+
+def apply_tuning(ctx, args):
+    from hunyuansc25_b200 import tune
+    p = tune.resolve_tuning(args.tuning, args.workload)
+    if p:
+        ctx.load_tuning(p)
 
 
 def run_batch(args, spec):
@@ -207,6 +221,7 @@ def run_batch(args, spec):
         dist.all_reduce(m_tot)
     m_und = int(m_tot.item())
     ctx = hp.Context(local)
+    apply_tuning(ctx, args)
     for _ in range(max(1, args.warmup)):
         ctx.partition_batch(gs, ks, spec["ub"])
     stream = torch.cuda.current_stream(dev)
@@ -248,7 +263,7 @@ def run_batch(args, spec):
                        "nedges_undirected": m_und,
                        "parallelism": (f"{world} GPUs, graphs sharded by greedy LPT on m+n; 16 worker streams per GPU"
                                        if world > 1 else "one GPU, 16 worker streams"),
-                       "l2": "inputs (host) re-copied every step"},
+                       "l2": "inputs (host) re-copied every step", "tuning": tuning_name(args)},
             "e2e": {"value": m_und / tb, "unit": "edges/s", "h2d_bytes_per_step": int(h2d[0].item()),
                     "d2h_bytes_per_step": int(h2d[1].item())},
             "timing": "host-buffer batch call (H2D and D2H inside); CUDA events on the caller's stream around "
@@ -283,6 +298,9 @@ def main():
     ap.add_argument("--compare-learned", action="store_true",
                     help="also time the learned refiner and report learned vs plain")
     ap.add_argument("--learned-threshold", type=float, default=None)
+    ap.add_argument("--tuning", default="auto",
+                    help="kernel tuning file; 'auto' loads hunyuansc25_b200/tuning/<workload>.json when "
+                         "present, 'none' keeps the library defaults")
     ap.add_argument("--kernel-only", action="store_true",
                     help="skip the e2e and CPU-baseline legs (profiling runs)")
     args = ap.parse_args()
@@ -312,6 +330,7 @@ def main():
         dist.init_process_group("nccl", device_id=dev, timeout=timedelta(seconds=300))
 
     ctx = hp.Context(local)
+    apply_tuning(ctx, args)
     from hunyuansc25_b200 import learn
     if args.learned or args.compare_learned:
         mparams, mthr, _ = learn.load_params()

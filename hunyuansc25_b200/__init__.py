@@ -15,7 +15,7 @@ import numpy as np
 
 from ._abi import (ERROR_NAMES, HP_MLP_NPARAM, HP_OK, HP_TRACE_ADJNCY, HP_TRACE_ADJWGT, HP_TRACE_CMAP,
                    HP_TRACE_MATCH, HP_TRACE_VWGT, HP_TRACE_WHERE_FINAL, HP_TRACE_WHERE_START,
-                   HP_TRACE_XADJ, PROTOTYPES, HpOptions, HpStats, default_options)
+                   HP_TRACE_XADJ, PROTOTYPES, HpOptions, HpStats, HpTuning, default_options)
 
 __all__ = [
     "HpError", "Context", "partition_graph", "PartitionGraph", "default_options", "HpOptions",
@@ -196,6 +196,28 @@ class Context:
         if rc != HP_OK:
             return None
         return out[:size]
+
+    # ---- kernel tuning ---------------------------------------------------------------
+    def set_tuning(self, tuning=None, **fields):
+        """Installs a kernel tuning (speed only; the partition does not change).
+        ``tuning`` is a dict of hp_tuning fields (missing ones take their
+        defaults) or None for the defaults; keyword fields override it."""
+        d = dict(tuning or {})
+        d.update(fields)
+        t = HpTuning.from_dict(d)
+        _check(self.lib.hp_context_set_tuning(self.h, C.byref(t)), "hp_context_set_tuning")
+
+    def get_tuning(self) -> dict:
+        t = HpTuning()
+        _check(self.lib.hp_context_get_tuning(self.h, C.byref(t)), "hp_context_get_tuning")
+        return t.as_dict()
+
+    def load_tuning(self, path: str) -> dict:
+        """Installs the tuning stored in a tuning file (hunyuansc25_b200.tune)."""
+        from . import tune
+        t = tune.read_tuning_file(path)
+        self.set_tuning(t)
+        return t
 
     # ---- learned move proposals -------------------------------------------------------
     def mlp_set_params(self, params, threshold: float = 0.0):

@@ -19,15 +19,10 @@ import sys
 
 import numpy as np
 
-from . import Context, graphs
+from . import Context, graphs, tune
 from ._abi import default_options
 
-WORKLOADS = {
-    "grid2d": (lambda: graphs.config_grid2d(), 8, 1.03),
-    "grid3d": (lambda: graphs.config_grid3d(), 64, 1.03),
-    "rmat22": (lambda: graphs.config_rmat(22), 256, 1.03),
-    "rgg24": (lambda: graphs.config_rgg(1 << 24), 1024, 1.05),
-}
+WORKLOADS = graphs.WORKLOADS
 
 
 def imbalance(g, part, nparts: int) -> float:
@@ -48,6 +43,9 @@ def main(argv=None) -> int:
     ap.add_argument("--learned", action="store_true", help="learned move proposals (default weights)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--write-part", action="store_true", help="write <graph>.part.<nparts>")
+    ap.add_argument("--tuning", default=None,
+                    help="kernel tuning file (hunyuansc25_b200.tune); with --workload, 'auto' (default) "
+                         "loads the committed file of that workload if there is one, 'none' keeps the defaults")
     a = ap.parse_args(argv)
 
     graphs.set_threads(os.cpu_count() or 1)
@@ -69,6 +67,10 @@ def main(argv=None) -> int:
     print(f"graph:{name} {g.nvtxs} {g.nedges // 2} {nparts} 0", flush=True)
 
     ctx = Context(a.device)
+    tpath = tune.resolve_tuning(a.tuning, a.workload)
+    if tpath:
+        ctx.load_tuning(tpath)
+        print(f"tuning: {tpath}")
     opt = default_options(eager=1 if a.eager else 0, learned=1 if a.learned else 0, seed=a.seed)
     if a.learned:
         from . import learn

@@ -78,6 +78,73 @@ def default_options(**overrides) -> HpOptions:
     return o
 
 
+TUNING_FIELDS = [
+    "match_warp_deg",
+    "match_cta_deg",
+    "contract_thread_row",
+    "contract_warp_row",
+    "contract_cta_row",
+    "gain_thread_deg",
+    "gain_hub_deg",
+    "warp_dense_k",
+    "grid_ctas_per_sm",
+    "dense_sparse_ratio",
+]
+
+TUNING_DEFAULTS = {
+    "match_warp_deg": 32,
+    "match_cta_deg": 4096,
+    "contract_thread_row": 32,
+    "contract_warp_row": 256,
+    "contract_cta_row": 4096,
+    "gain_thread_deg": 32,
+    "gain_hub_deg": 4096,
+    "warp_dense_k": 1024,
+    "grid_ctas_per_sm": 8,
+    "dense_sparse_ratio": 4,
+}
+
+TUNE_DEG_MAX = 1 << 24
+
+
+def tuning_violation(t: dict):
+    """First field of a tuning out of range, else None (the ranges that
+    hp_context_set_tuning checks)."""
+    lim = [
+        ("match_warp_deg", 4, 256),
+        ("match_cta_deg", t["match_warp_deg"], TUNE_DEG_MAX),
+        ("contract_thread_row", 8, 32),
+        ("contract_warp_row", t["contract_thread_row"], 256),
+        ("contract_cta_row", t["contract_warp_row"], 4096),
+        ("gain_thread_deg", 8, 32),
+        ("gain_hub_deg", t["gain_thread_deg"], TUNE_DEG_MAX),
+        ("warp_dense_k", 0, 1024),
+        ("grid_ctas_per_sm", 1, 32),
+        ("dense_sparse_ratio", 1, 4096),
+    ]
+    for name, lo, hi in lim:
+        if not lo <= int(t[name]) <= hi:
+            return name
+    return None
+
+
+class HpTuning(C.Structure):
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 6)]
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "HpTuning":
+        unknown = set(d) - set(TUNING_FIELDS)
+        if unknown:
+            raise ValueError(f"unknown tuning fields: {sorted(unknown)}")
+        t = cls()
+        for name in TUNING_FIELDS:
+            setattr(t, name, int(d.get(name, TUNING_DEFAULTS[name])))
+        return t
+
+    def as_dict(self) -> dict:
+        return {name: int(getattr(self, name)) for name in TUNING_FIELDS}
+
+
 class HpStats(C.Structure):
     _fields_ = [
         ("edgecut", C.c_int64),
@@ -124,6 +191,9 @@ F32P = C.POINTER(C.c_float)
 PROTOTYPES = {
     "hp_options_default": (None, [C.POINTER(HpOptions)]),
     "hp_strerror": (C.c_char_p, [C.c_int]),
+    "hp_tuning_default": (None, [C.POINTER(HpTuning)]),
+    "hp_context_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(HpTuning)]),
+    "hp_context_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(HpTuning)]),
     "hp_context_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "hp_context_destroy": (None, [C.c_void_p]),
     "hp_partition": (C.c_int, [C.c_void_p, C.c_int32, I32P, I32P, I32P, I32P, C.c_int32, F32P,

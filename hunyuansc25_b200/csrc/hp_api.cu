@@ -446,6 +446,61 @@ HP_API void hp_options_default(hp_options *o)
     o->seed = 1;
 }
 
+HP_API void hp_tuning_default(hp_tuning *t)
+{
+    if (!t) return;
+    memset(t, 0, sizeof(*t));
+    t->match_warp_deg = 32;
+    t->match_cta_deg = 4096;
+    t->contract_thread_row = HP_TUNE_THREAD_ROW_MAX;
+    t->contract_warp_row = HP_TUNE_WARP_ROW_MAX;
+    t->contract_cta_row = HP_TUNE_CTA_ROW_MAX;
+    t->gain_thread_deg = HP_TUNE_THREAD_ROW_MAX;
+    t->gain_hub_deg = 4096;
+    t->warp_dense_k = HP_TUNE_WARP_DENSE_K_MAX;
+    t->grid_ctas_per_sm = 8;
+    t->dense_sparse_ratio = 4;
+}
+
+namespace {
+// The first field out of its range, or nullptr.
+const char *tuning_violation(const hp_tuning &t)
+{
+    auto in = [](int32_t v, int64_t lo, int64_t hi) { return v >= lo && v <= hi; };
+    if (!in(t.match_warp_deg, 4, 256)) return "match_warp_deg";
+    if (!in(t.match_cta_deg, t.match_warp_deg, HP_TUNE_DEG_MAX)) return "match_cta_deg";
+    if (!in(t.contract_thread_row, 8, HP_TUNE_THREAD_ROW_MAX)) return "contract_thread_row";
+    if (!in(t.contract_warp_row, t.contract_thread_row, HP_TUNE_WARP_ROW_MAX)) return "contract_warp_row";
+    if (!in(t.contract_cta_row, t.contract_warp_row, HP_TUNE_CTA_ROW_MAX)) return "contract_cta_row";
+    if (!in(t.gain_thread_deg, 8, HP_TUNE_THREAD_ROW_MAX)) return "gain_thread_deg";
+    if (!in(t.gain_hub_deg, t.gain_thread_deg, HP_TUNE_DEG_MAX)) return "gain_hub_deg";
+    if (!in(t.warp_dense_k, 0, HP_TUNE_WARP_DENSE_K_MAX)) return "warp_dense_k";
+    if (!in(t.grid_ctas_per_sm, 1, 32)) return "grid_ctas_per_sm";
+    if (!in(t.dense_sparse_ratio, 1, 4096)) return "dense_sparse_ratio";
+    for (int32_t r : t.reserved)
+        if (r != 0) return "reserved";
+    return nullptr;
+}
+}  // namespace
+
+HP_API int hp_context_set_tuning(hp_context *ctx, const hp_tuning *t)
+{
+    if (!ctx || !t) return HP_ERR_INVALID_ARG;
+    if (const char *bad = tuning_violation(*t)) {
+        fprintf(stderr, "hp: tuning field %s out of range\n", bad);
+        return HP_ERR_INVALID_ARG;
+    }
+    ctx->tune = *t;
+    return HP_OK;
+}
+
+HP_API int hp_context_get_tuning(const hp_context *ctx, hp_tuning *t)
+{
+    if (!ctx || !t) return HP_ERR_INVALID_ARG;
+    *t = ctx->tune;
+    return HP_OK;
+}
+
 HP_API const char *hp_strerror(int code)
 {
     switch (code) {
@@ -474,6 +529,7 @@ HP_API int hp_context_create(int device, hp_context **out)
     if (device < 0 || device >= ndev) return HP_ERR_INVALID_ARG;
     hp_context *c = new hp_context();
     c->device = device;
+    hp_tuning_default(&c->tune);
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return HP_ERR_NO_DEVICE; }
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
     bool ok = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) == cudaSuccess;
@@ -712,6 +768,7 @@ HP_API int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *v
         HP_TRY(hp_context_create(ctx->device, &w));
         ctx->workers.push_back(w);
     }
+    for (hp_context *w : ctx->workers) w->tune = ctx->tune;
     std::vector<int32_t> order(ngraphs);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {

@@ -27,8 +27,8 @@
 
 namespace {
 
-constexpr int BIG_DEG = 32;      // rows longer than this use a warp per vertex
-constexpr int HUGE_DEG = 4096;   // rows longer than this use a CTA per vertex
+// Row classes of matching (hp_tuning): rows of at most match_warp_deg entries
+// take a thread, longer rows a warp, rows above match_cta_deg a CTA.
 
 // ---------------------------------------------------------------------------
 // matching
@@ -76,13 +76,13 @@ __global__ void __launch_bounds__(256)
 pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
                   const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
-                  uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
+                  uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev, int32_t warp_deg)
 {
     if (made_prev && *made_prev == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     const int32_t b = xadj[v], e = xadj[v + 1];
-    if (e - b > BIG_DEG) return;
+    if (e - b > warp_deg) return;
     if (match[v] != -1) { pref[v] = -1; return; }
     if (ELIG && keep_proposal(made_prev != nullptr, v, pref, elig)) return;
     const int32_t wv = vwgt[v];
@@ -358,17 +358,18 @@ commit_kernel(int32_t n, int32_t *__restrict__ match, const int32_t *__restrict_
 
 __global__ void __launch_bounds__(256)
 big_list_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t *list, int32_t *d_count,
-                int32_t *huge, int32_t *d_huge, const int32_t *__restrict__ vwgt, int32_t *__restrict__ elig)
+                int32_t *huge, int32_t *d_huge, const int32_t *__restrict__ vwgt, int32_t *__restrict__ elig,
+                int32_t warp_deg, int32_t cta_deg)
 {
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     elig[v] = vwgt[v];   // every vertex starts unmatched
     const int32_t d = xadj[v + 1] - xadj[v];
-    if (d > HUGE_DEG) huge[atomicAdd(d_huge, 1)] = v;
-    else if (d > BIG_DEG) list[atomicAdd(d_count, 1)] = v;
+    if (d > cta_deg) huge[atomicAdd(d_huge, 1)] = v;
+    else if (d > warp_deg) list[atomicAdd(d_count, 1)] = v;
 }
 
-// CTA per vertex for rows longer than HUGE_DEG (R-MAT hubs).
+// CTA per vertex for rows longer than match_cta_deg (R-MAT hubs).
 template <bool ELIG>
 __global__ void __launch_bounds__(512)
 pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
@@ -421,7 +422,7 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
     }
 }
 
-// Hub pairing for rows longer than HUGE_DEG: clients ranked by a CTA scan.
+// Hub pairing for rows longer than match_cta_deg: clients ranked by a CTA scan.
 __global__ void __launch_bounds__(512)
 pair_hub_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                      const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
@@ -466,12 +467,13 @@ count_matched_kernel(int32_t n, const int32_t *__restrict__ match, unsigned long
 __global__ void __launch_bounds__(256)
 pair_hub_small_kernel(int32_t n, const int32_t *__restrict__ xadj,
                       const int32_t *__restrict__ adjncy, const int32_t *__restrict__ vwgt,
-                      const int32_t *__restrict__ hub, int32_t *__restrict__ match, int64_t maxvwgt)
+                      const int32_t *__restrict__ hub, int32_t *__restrict__ match, int64_t maxvwgt,
+                      int32_t warp_deg)
 {
     int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= n) return;
     const int32_t b = xadj[h], e = xadj[h + 1];
-    if (e - b > BIG_DEG) return;
+    if (e - b > warp_deg) return;
     int32_t first = -1, t = 0;
     for (int32_t j = b; j < e; j++) {
         int32_t c = adjncy[j];
@@ -559,9 +561,9 @@ finalize_match_kernel(int32_t n, int32_t *__restrict__ match, int32_t *__restric
 
 // Followers copy the leader's coarse id; leaders describe the coarse row: the
 // fine rows it merges (start and length of the leader's and the mate's row)
-// and its vertex weight.  Rows longer than SMALL_ROW entries are appended to
-// their class list and their length is counted for the temporary row buffer.
-constexpr int32_t SMALL_ROW = 32;
+// and its vertex weight.  Rows longer than thread_row entries are appended to
+// their class list (warp radix up to warp_row, CTA radix up to cta_row, then
+// the long class) and their length is counted for the temporary row buffer.
 
 struct RowInfo {
     int32_t s0, l0, s1, l1;   // leader row start/length, mate row start/length (l1 = 0 if unmatched)
@@ -573,7 +575,7 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
                     int4 *__restrict__ rinfo, int32_t *__restrict__ cvwgt, int32_t *__restrict__ ltlen,
                     int32_t *__restrict__ lists, int32_t *__restrict__ counts, int32_t cn,
                     int32_t *__restrict__ maxlen, unsigned long long *__restrict__ long_total,
-                    int32_t *__restrict__ small_max)
+                    int32_t *__restrict__ small_max, int32_t thread_row, int32_t warp_row, int32_t cta_row)
 {
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
@@ -591,10 +593,10 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
     rinfo[c] = make_int4(s0, l0, s1, l1);
     cvwgt[c] = w;
     const int32_t len = l0 + l1;
-    ltlen[c] = len > SMALL_ROW ? len : 0;
-    if (len <= SMALL_ROW && len > 8) atomicMax(small_max, len);   // picks the assembly kernel's network
-    if (len > SMALL_ROW) {
-        int cls = len <= 256 ? 0 : (len <= 4096 ? 1 : 2);   // warp radix, CTA radix, dense
+    ltlen[c] = len > thread_row ? len : 0;
+    if (len <= thread_row && len > 8) atomicMax(small_max, len);   // picks the assembly kernel's network
+    if (len > thread_row) {
+        int cls = len <= warp_row ? 0 : (len <= cta_row ? 1 : 2);   // warp radix, CTA radix, long
         int32_t pos = atomicAdd(&counts[cls], 1);
         lists[(int64_t)cls * cn + pos] = c;
         if (cls == 2) atomicMax(maxlen, len);
@@ -689,7 +691,7 @@ __global__ void __launch_bounds__(ASM_TILE)
 contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict__ ucnt,
                          int32_t *__restrict__ cxadj, int32_t *__restrict__ cadjncy,
                          int32_t *__restrict__ cadjwgt, unsigned long long *tile_status, hp::LbCtl *lb,
-                         unsigned *status)
+                         unsigned *status, int32_t thread_row)
 {
     __shared__ int32_t s_scan[ASM_TILE / 32 + 2];
     __shared__ int32_t s_excl;
@@ -700,7 +702,7 @@ contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict_
     RowInfo r{0, 0, 0, 0};
     int32_t len = 0;
     if (c < cn) src.row(c, r, len);
-    const bool small = c < cn && len <= SMALL_ROW;
+    const bool small = c < cn && len <= thread_row;
     const unsigned wmax = __reduce_max_sync(HP_FULL_MASK, small ? (unsigned)len : 0u);
     unsigned long long x[XN];
     int u = 0;
@@ -975,8 +977,8 @@ __device__ int group_gather_row(const ContractSrc &src, int32_t c, const RowInfo
     return len - tot;
 }
 
-constexpr int WROW_MAX = 256;    // warp class: 33..256 entries
-constexpr int CROW_MAX = 4096;   // CTA class: 257..4096 entries
+constexpr int WROW_MAX = HP_TUNE_WARP_ROW_MAX;   // warp class: up to 256 entries
+constexpr int CROW_MAX = HP_TUNE_CTA_ROW_MAX;    // CTA class: up to 4096 entries
 constexpr int WROW_WARPS = 8;
 
 // Warp class: 8 warps per CTA, one row per warp at a time.
@@ -1042,14 +1044,16 @@ template <int NT, int CAP>
 constexpr size_t cta_radix_smem() { return sizeof(unsigned long long) * 2 * CAP + sizeof(int32_t) * 256 * (NT / 32); }
 
 
-// Rows longer than 4096 entries: dense accumulator over the coarse id space in
-// a per-CTA global slab (dw: cn ints, bm: cn/32 words; zero on entry/exit).
+// Rows longer than XROW_MAX entries: dense accumulator over the coarse id space
+// in a per-CTA global slab (dw: cn ints, bm: cn/32 words, bm2: cn/1024 words;
+// zero on entry/exit).  A row with len * ratio < cn/32 words walks the occupied
+// words through the second-level bitmap; a denser row scans the bitmap.
 template <int NT>
 __global__ void __launch_bounds__(NT)
 contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                       ContractSrc src, const int32_t *__restrict__ toff, int32_t *__restrict__ tk,
                       int32_t *__restrict__ tw, int32_t *__restrict__ ucnt, int32_t cn,
-                      int32_t *slab_w, unsigned *slab_bm, unsigned *slab_bm2)
+                      int32_t *slab_w, unsigned *slab_bm, unsigned *slab_bm2, int32_t ratio)
 {
     __shared__ int32_t s_scan[NT / 32 + 2];
     int32_t *dw = slab_w + (int64_t)blockIdx.x * cn;
@@ -1062,9 +1066,7 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
         int32_t len;
         src.row(c, r, len);
         if (len <= XROW_MAX) continue;   // contract_cta_radix_kernel<1024, XROW_MAX>'s row
-        // a row much shorter than the bitmap walks the occupied words through
-        // the second level; a denser row scans the bitmap directly
-        const bool two_level = (int64_t)len * 4 < ((int64_t)cn + 31) / 32;
+        const bool two_level = (int64_t)len * ratio < ((int64_t)cn + 31) / 32;
         for (int32_t i0 = threadIdx.x; i0 < len; i0 += 4 * NT) {
             int32_t a[4], wq[4];
             bool in[4];
@@ -1103,9 +1105,9 @@ inline unsigned blocks_for(int64_t threads, int block = 256)
     return (unsigned)(g > 0 ? g : 1);
 }
 
-inline unsigned persistent_grid(hp_context *c, int per_sm = 8)
+inline unsigned persistent_grid(hp_context *c)
 {
-    return (unsigned)(c->sm_count * per_sm);
+    return (unsigned)(c->sm_count * c->tune.grid_ctas_per_sm);
 }
 
 // One matching level.  On return match[] is final (self when unmatched),
@@ -1136,7 +1138,9 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     int32_t *d_hugecnt = (int32_t *)&sc[38];
 
     HP_TRY(hp_fill_i32(c, g.match, n, -1));
-    HP_LAUNCH(c, big_list_kernel, blocks_for(n), 256, 0, n, g.xadj, big, d_bigcnt, huge, d_hugecnt, g.vwgt, elig);
+    const hp_tuning &tn = c->tune;
+    HP_LAUNCH(c, big_list_kernel, blocks_for(n), 256, 0, n, g.xadj, big, d_bigcnt, huge, d_hugecnt, g.vwgt, elig,
+              tn.match_warp_deg, tn.match_cta_deg);
 
     const int rounds = o.match_rounds < 1 ? 1 : (o.match_rounds > 30 ? 30 : o.match_rounds);
     // algorithmic bytes of one full handshake round: xadj, adjncy, adjwgt,
@@ -1146,7 +1150,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
         const int tok = hp_prof_begin(c);
         const unsigned long long *prev = r == 0 ? nullptr : &sc[2 + r - 1];
         HP_LAUNCH(c, pref_small_kernel<true>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
-                  g.vwgt, g.match, elig, pref, lkey, maxvwgt, prev);
+                  g.vwgt, g.match, elig, pref, lkey, maxvwgt, prev, tn.match_warp_deg);
         HP_LAUNCH(c, pref_big_topk_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
                   g.vwgt, g.match, elig, pref, cand, lkey, maxvwgt, prev);
         HP_LAUNCH(c, pref_huge_topk_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
@@ -1169,7 +1173,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
         // two-hop through a shared heaviest neighbour
         int32_t *hub = pref;
         HP_LAUNCH(c, pref_small_kernel<false>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
-                  g.vwgt, g.match, elig, hub, lkey, maxvwgt, (const unsigned long long *)nullptr);
+                  g.vwgt, g.match, elig, hub, lkey, maxvwgt, (const unsigned long long *)nullptr, tn.match_warp_deg);
         HP_LAUNCH(c, pref_big_kernel<false>, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, elig, hub, lkey, maxvwgt,
                   (const unsigned long long *)nullptr);
@@ -1177,7 +1181,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
                   g.adjncy, g.adjwgt, g.vwgt, g.match, elig, hub, lkey, maxvwgt,
                   (const unsigned long long *)nullptr);
         HP_LAUNCH(c, pair_hub_small_kernel, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.vwgt, hub,
-                  g.match, maxvwgt);
+                  g.match, maxvwgt, tn.match_warp_deg);
         HP_LAUNCH(c, pair_hub_big_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy,
                   g.vwgt, hub, g.match, maxvwgt);
         HP_LAUNCH(c, pair_hub_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
@@ -1233,7 +1237,8 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
 
     int tok = hp_prof_begin(c);
     HP_LAUNCH(c, coarse_setup_kernel, blocks_for(n), 256, 0, n, g.match, g.cmap, g.xadj, g.vwgt, rinfo, cg.vwgt,
-              toff, lists, counts, cn, maxlen, long_total, small_max);
+              toff, lists, counts, cn, maxlen, long_total, small_max, c->tune.contract_thread_row,
+              c->tune.contract_warp_row, c->tune.contract_cta_row);
     hp_prof_end(c, tok, HP_PROF_CONTRACT, 0);
     struct { int32_t cnt[3]; int32_t maxlen; unsigned long long total; int32_t small_max, pad; } h;
     HP_TRY(hp_read_scalars(c, sc, sizeof(h), &h));
@@ -1279,19 +1284,19 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
             HP_CUDA(cudaMemsetAsync(sbm, 0, sizeof(unsigned) * (size_t)(nb * nw), c->stream));
             HP_CUDA(cudaMemsetAsync(sbm2, 0, sizeof(unsigned) * (size_t)(nb * nw2), c->stream));
             HP_LAUNCH(c, contract_dense_kernel<1024>, (unsigned)nb, 1024, 0, lists + 2 * (int64_t)cn,
-                      &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm, sbm2);
+                      &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm, sbm2, c->tune.dense_sparse_ratio);
         }
     }
     // short rows + coarse xadj in one ordered pass, then the long rows' copies
     if (h.small_max <= 8)
         HP_LAUNCH(c, contract_assemble_kernel<8>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status);
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
     else if (h.small_max <= 16)
         HP_LAUNCH(c, contract_assemble_kernel<16>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status);
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
     else
         HP_LAUNCH(c, contract_assemble_kernel<32>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status);
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
     if (h.cnt[0] > 0)
         HP_LAUNCH(c, copy_long_rows_kernel<false>, std::min<unsigned>(blocks_for((int64_t)h.cnt[0] * 32),
                                                                      c->sm_count * 16),

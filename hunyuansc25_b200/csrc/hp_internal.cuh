@@ -82,11 +82,19 @@ struct hp_context {
     std::deque<Retired> reaper_q;
     bool reaper_stop = false;
 
+    hp_tuning tune = {};                 // kernel tuning (speed only), hp_context_set_tuning
     std::vector<hp_context *> workers;   // batch worker contexts (own streams and arenas)
     std::vector<HpLevel> levels;
     bool trace_valid = false;
     hp_options opt = {};
 };
+
+// Upper bounds of the kernel tuning: the capacities the kernels are compiled for.
+constexpr int HP_TUNE_THREAD_ROW_MAX = 32;       // register sorting networks (rows per thread)
+constexpr int HP_TUNE_WARP_ROW_MAX = 256;        // contract_warp_radix_kernel's shared buffers
+constexpr int HP_TUNE_CTA_ROW_MAX = 4096;        // contract_cta_radix_kernel<256, 4096>
+constexpr int HP_TUNE_WARP_DENSE_K_MAX = 1024;   // gain_bigwarp_kernel's shared accumulators
+constexpr int HP_TUNE_DEG_MAX = 1 << 24;
 
 #define HP_NSCAL 64
 #define HP_ALIGN 256

@@ -24,8 +24,10 @@
 
 namespace {
 
-constexpr int BIGD = 32;
-constexpr int HUGED = 4096;   // afterburner rows longer than this use a CTA per vertex
+// Row classes of refinement (hp_tuning): rows of at most `bigd` entries take a
+// thread (or a lane segment), longer rows a warp, and hub rows (more than
+// `huged` entries) a CTA or grid-wide chunks.  bigd <= 32, the register
+// networks' width.
 constexpr int32_t NEG = INT_MIN;
 
 inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)std::max<int64_t>(1, (n + b - 1) / b); }
@@ -37,20 +39,21 @@ __global__ void project_kernel(int32_t n, const int32_t *__restrict__ cmap,
     if (v < n) where[v] = cwhere[cmap[v]];
 }
 
-// Row capacities min(deg, k); rows longer than BIGD go on the big list, rows
-// longer than HUGED also on the hub list (count d_bigcnt[3]); d_bigcnt[1]
+// Row capacities min(deg, k); rows longer than bigd go on the big list, rows
+// longer than huged also on the hub list (count d_bigcnt[3]); d_bigcnt[1]
 // records the longest short row above 8 entries, d_bigcnt[2] the longest row
-// above HUGED.
+// above huged.
 __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t k,
-                                int32_t *__restrict__ cap, int32_t *big, int32_t *huge, int32_t *d_bigcnt)
+                                int32_t *__restrict__ cap, int32_t *big, int32_t *huge, int32_t *d_bigcnt,
+                                int32_t bigd, int32_t huged)
 {
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     int32_t d = xadj[v + 1] - xadj[v];
     cap[v] = d < k ? d : k;
-    if (d > BIGD) {
+    if (d > bigd) {
         big[atomicAdd(d_bigcnt, 1)] = v;
-        if (d > HUGED) {
+        if (d > huged) {
             atomicMax(d_bigcnt + 2, d);
             huge[atomicAdd(d_bigcnt + 3, 1)] = v;
         }
@@ -61,19 +64,19 @@ __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int
 
 // Degree statistics of a level, computed for every level at the start of
 // uncoarsening so that the host chooses each level's kernels without reading
-// anything back per level: rows longer than BIGD, the longest row of 9..BIGD
+// anything back per level: rows longer than bigd, the longest row of 9..bigd
 // entries, the longest row overall.
 struct LevelStat {
     int32_t nbig, small_max, maxdeg, pad;
 };
 
 __global__ void __launch_bounds__(256)
-level_stats_kernel(int32_t n, const int32_t *__restrict__ xadj, LevelStat *st)
+level_stats_kernel(int32_t n, const int32_t *__restrict__ xadj, LevelStat *st, int32_t bigd)
 {
     int32_t nbig = 0, smax = 0, dmax = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t d = xadj[v + 1] - xadj[v];
-        if (d > BIGD) nbig++;
+        if (d > bigd) nbig++;
         else if (d > 8) smax = d > smax ? d : smax;
         dmax = d > dmax ? d : dmax;
     }
@@ -87,7 +90,7 @@ level_stats_kernel(int32_t n, const int32_t *__restrict__ xadj, LevelStat *st)
     }
 }
 
-// Gain row of a vertex with at most BIGD neighbours, one thread per row: the
+// Gain row of a vertex with at most bigd neighbours, one thread per row: the
 // (part, weight) pairs are sorted by a register network and merged, then
 // written as the sparse row (ascending parts, part -1 padding up to the
 // capacity) or, when deg >= k, as the dense row (entry q = part q).
@@ -140,7 +143,7 @@ __device__ __forceinline__ void gain_row_thread(int32_t b, int32_t d, const int3
     }
 }
 
-// list == nullptr: every vertex (rows longer than BIGD are skipped: the big-row
+// list == nullptr: every vertex (rows longer than bigd are skipped: the big-row
 // kernel builds them); else the listed vertices, whose dirty flags are cleared.
 template <int XN>
 __global__ void __launch_bounds__(256)
@@ -148,7 +151,7 @@ gain_thread_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__
                    const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                    const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                    const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
-                   int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty)
+                   int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty, int32_t bigd)
 {
     const int32_t cnt = list ? *d_count : n;
     for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < cnt; i0 += (int64_t)gridDim.x * blockDim.x) {
@@ -160,7 +163,7 @@ gain_thread_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__
             d = xadj[v + 1] - b;
             if (dirty) dirty[v] = 0;
         }
-        const bool mine = v >= 0 && d <= BIGD;
+        const bool mine = v >= 0 && d <= bigd;
         const unsigned wmax = __reduce_max_sync(HP_FULL_MASK, mine ? (unsigned)d : 0u);
         if (!mine) continue;
         const int32_t o = goff[v], cap = goff[v + 1] - o;
@@ -220,20 +223,20 @@ gain_seg_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
     }
 }
 
-// Gain rows of BIGD+1 .. HUGED entries when k <= WARP_DENSE_K: one warp per
+// Gain rows of bigd+1 .. huged entries when k <= warp_dense_k: one warp per
 // row with its own dense accumulator and presence bitmap over the k parts in
 // shared memory (k + k/32 words per warp), extracted in part order; only warp
 // synchronisation.  Longer rows (and any row when k is larger) use
 // gain_dense_kernel.
-constexpr int WARP_DENSE_K = 1024;
-constexpr int GW_WARPS = 8;
+constexpr int GW_WARPS = 8;   // k + k/32 words per warp: 33 KB at k = HP_TUNE_WARP_DENSE_K_MAX
 
 __global__ void __launch_bounds__(32 * GW_WARPS)
 gain_bigwarp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                     const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                     const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                     const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
-                    int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty)
+                    int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty, int32_t bigd,
+                    int32_t huged)
 {
     extern __shared__ int32_t gsm[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -247,7 +250,7 @@ gain_bigwarp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict_
     for (int64_t li = (int64_t)blockIdx.x * GW_WARPS + wid; li < cnt; li += (int64_t)gridDim.x * GW_WARPS) {
         const int32_t v = list[li];
         const int32_t b = xadj[v], e = xadj[v + 1];
-        if (e - b <= BIGD || e - b > HUGED) continue;
+        if (e - b <= bigd || e - b > huged) continue;
         if (dirty && lane == 0) dirty[v] = 0;
         for (int32_t j = b + lane; j < e; j += 32) {
             const int32_t q = where[adjncy[j]];
@@ -296,7 +299,8 @@ gain_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ 
                   const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                   const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
-                  int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty)
+                  int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty, int32_t bigd,
+                  int32_t huged, int32_t warp_dense_k)
 {
     extern __shared__ int32_t dsm[];
     __shared__ int32_t s_scan[NT / 32 + 2];
@@ -310,8 +314,8 @@ gain_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ 
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t v = list[li];
         const int32_t b = xadj[v], e = xadj[v + 1];
-        if (e - b <= BIGD) continue;
-        if (k <= WARP_DENSE_K && e - b <= HUGED) continue;   // gain_bigwarp_kernel's rows
+        if (e - b <= bigd) continue;
+        if (k <= warp_dense_k && e - b <= huged) continue;   // gain_bigwarp_kernel's rows
         if (dirty && threadIdx.x == 0) dirty[v] = 0;
         for (int32_t j = b + threadIdx.x; j < e; j += NT) {
             int32_t q = where[adjncy[j]];
@@ -571,13 +575,13 @@ afterburner_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int3
                          const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                          const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
                          int8_t *__restrict__ lock, const unsigned long long *d_ncand,
-                         int32_t *__restrict__ moves, unsigned long long *d_nmoves)
+                         int32_t *__restrict__ moves, unsigned long long *d_nmoves, int32_t bigd)
 {
     if (*d_ncand == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     const int32_t b0 = xadj[v], e0 = xadj[v + 1];
-    if (e0 - b0 > BIGD) return;
+    if (e0 - b0 > bigd) return;
     const int32_t g = pregain[v];
     int8_t sel = 0;
     if (g != NEG) {
@@ -596,7 +600,7 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
                        const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                        const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
                        int8_t *__restrict__ lock, const unsigned long long *d_ncand,
-                       int32_t *__restrict__ moves, unsigned long long *d_nmoves)
+                       int32_t *__restrict__ moves, unsigned long long *d_nmoves, int32_t huged)
 {
     if (*d_ncand == 0ull) return;
     const int lane = threadIdx.x & 31;
@@ -604,7 +608,7 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = big[i];
-        if (xadj[v + 1] - xadj[v] > HUGED) continue;
+        if (xadj[v + 1] - xadj[v] > huged) continue;
         const int32_t g = pregain[v];
         int8_t sel = 0;
         if (g != NEG) {
@@ -622,7 +626,7 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
     }
 }
 
-// ---- hub rows (longer than HUGED): chunk plans ----------------------------------
+// ---- hub rows (longer than huged): chunk plans ----------------------------------
 // The work on hub rows is cut into chunks of HUB_CHUNK entries dealt over the
 // whole grid.  A one-CTA kernel plans it per pass: it selects the hubs that have
 // work (afterburner: candidates; moves: moved hubs), writes each one's vertex,
@@ -752,7 +756,7 @@ __device__ __forceinline__ void touch_neighbour(bool valid, int32_t u, int32_t w
                                                 const int32_t *__restrict__ goff,
                                                 int32_t *__restrict__ gconn, int32_t *__restrict__ dirty,
                                                 int32_t *__restrict__ small_l, int32_t *__restrict__ big_l,
-                                                int32_t *counts, int32_t k)
+                                                int32_t *counts, int32_t k, int32_t bigd)
 {
     // all 32 lanes call (valid marks the lanes with a neighbour); list appends
     // take one counter atomic per warp and list (ballot ranks inside the warp)
@@ -763,7 +767,7 @@ __device__ __forceinline__ void touch_neighbour(bool valid, int32_t u, int32_t w
             atomicAdd(&gconn[o + p], -w);
             atomicAdd(&gconn[o + d], w);
         } else if (atomicExch(&dirty[u], 1) == 0) {
-            if (xadj[u + 1] - xadj[u] > BIGD) bg = true;
+            if (xadj[u + 1] - xadj[u] > bigd) bg = true;
             else sm = true;
         }
     }
@@ -789,7 +793,7 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
                    const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
                    int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
                    int32_t *__restrict__ big_l, int32_t *counts, int32_t k, int32_t *__restrict__ huge_mv,
-                   int32_t *__restrict__ d_nhuge)
+                   int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t huged)
 {
     const int64_t nm = (int64_t)*d_nmoves;
     const int lane = threadIdx.x & 31;
@@ -804,7 +808,7 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
             atomicAdd(&pw[p], (unsigned long long)(-(long long)w));
         }
         const int32_t b = xadj[v], e = xadj[v + 1];
-        if (e - b > HUGED) {
+        if (e - b > huged) {
             // neighbours of a hub are touched by apply_moves_huge_kernel, spread
             // over the whole grid (it reads the old part from oldp)
             if (lane == 0) {
@@ -817,7 +821,7 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
             const int32_t j = j0 + lane;
             const bool valid = j < e;
             touch_neighbour(valid, valid ? adjncy[j] : 0, valid ? adjwgt[j] : 0, p, d, xadj, goff, gconn, dirty,
-                            small_l, big_l, counts, k);
+                            small_l, big_l, counts, k, bigd);
         }
         if (lane == 0) where[v] = d;   // the move itself (every lane has read where[v])
     }
@@ -833,7 +837,7 @@ apply_moves_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__res
                         const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                         const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
                         int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
-                        int32_t *__restrict__ big_l, int32_t *counts, int32_t k)
+                        int32_t *__restrict__ big_l, int32_t *counts, int32_t k, int32_t bigd)
 {
     const int32_t nsel = d_plan[0], nch = d_plan[1];
     for (int64_t gc = blockIdx.x; gc < nch; gc += gridDim.x) {
@@ -844,7 +848,7 @@ apply_moves_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__res
         const int32_t j = xadj[v] + (int32_t)(gc - plan_off[jp]) * HUB_CHUNK + threadIdx.x;
         const bool valid = j < e;
         touch_neighbour(valid, valid ? adjncy[j] : 0, valid ? adjwgt[j] : 0, p, d, xadj, goff, gconn, dirty, small_l,
-                        big_l, counts, k);
+                        big_l, counts, k, bigd);
     }
 }
 
@@ -1222,15 +1226,15 @@ struct RefineBufs {
     unsigned long long *pw;
     const int64_t *opt, *maxp;
     int32_t G;          // gain-row entries of the level
-    int32_t small_max;  // longest row of at most BIGD entries (picks the gain kernel's network)
-    bool huge_rows;     // the level has rows longer than HUGED
+    int32_t small_max;  // longest row of at most bigd entries (picks the gain kernel's network)
+    bool huge_rows;     // the level has rows longer than huged
 };
 
 // scalar slots used by refinement
 // Slots below S_PASS_END are reset at the start of every pass; S_BIGCNT (the
 // level's list of rows longer than 32) lives above it and persists.
 // S_BIGCNT (slots 16-17) holds the big-row count, the longest short row and the
-// longest row above HUGED.
+// longest row above huged.
 enum { S_NMOVES = 0, S_C1 = 1, S_C2 = 2, S_EXCESS = 3, S_NCAND = 4, S_CUT2 = 5, S_DIRTY = 6,
        S_HUGEMV = 7, S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_PASS_END = 12, S_BIGCNT = 16 };
 
@@ -1238,10 +1242,11 @@ int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_
                const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt,
                bool any_big, int32_t *dirty)
 {
+    const hp_tuning &tn = c->tune;
     if (small_list) {
         // rebuild of dirty rows: segments of S lanes per row (latency of a warp
         // per row, 32/S rows per warp)
-        const unsigned grid = (unsigned)(c->sm_count * 8);
+        const unsigned grid = (unsigned)(c->sm_count * tn.grid_ctas_per_sm);
         if (B.small_max <= 8)
             HP_LAUNCH(c, gain_seg_kernel<8>, grid, 256, 0, small_list, d_small_cnt, g.xadj, g.adjncy, g.adjwgt,
                       g.where, B.goff, B.gpart, B.gconn, k, dirty);
@@ -1256,25 +1261,27 @@ int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_
         const unsigned grid = nblk(g.n);
         if (B.small_max <= 8)
             HP_LAUNCH(c, gain_thread_kernel<8>, grid, 256, 0, nullptr, nullptr, g.n, g.xadj, g.adjncy, g.adjwgt,
-                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty, tn.gain_thread_deg);
         else if (B.small_max <= 16)
             HP_LAUNCH(c, gain_thread_kernel<16>, grid, 256, 0, nullptr, nullptr, g.n, g.xadj, g.adjncy, g.adjwgt,
-                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty, tn.gain_thread_deg);
         else
             HP_LAUNCH(c, gain_thread_kernel<32>, grid, 256, 0, nullptr, nullptr, g.n, g.xadj, g.adjncy, g.adjwgt,
-                      g.where, B.goff, B.gpart, B.gconn, k, dirty);
+                      g.where, B.goff, B.gpart, B.gconn, k, dirty, tn.gain_thread_deg);
     }
     if (any_big) {
         const size_t smem = sizeof(int32_t) * (size_t)k + sizeof(unsigned) * (size_t)((k + 31) / 32);
-        if (k <= WARP_DENSE_K)
+        if (k <= tn.warp_dense_k)
             HP_LAUNCH(c, gain_bigwarp_kernel, (unsigned)(c->sm_count * 4), 32 * GW_WARPS, GW_WARPS * smem, big_list,
-                      d_big_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
-        // rows longer than HUGED: every such row in a full build; in a rebuild only
-        // sparse ones (deg < k), which exist only when k > HUGED
-        const bool dense_rows = dirty ? (B.huge_rows && k > HUGED) : B.huge_rows;
-        if (k > WARP_DENSE_K || dense_rows)
+                      d_big_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty,
+                      tn.gain_thread_deg, tn.gain_hub_deg);
+        // hub rows: every such row in a full build; in a rebuild only sparse
+        // ones (deg < k), which exist only when k > gain_hub_deg
+        const bool dense_rows = dirty ? (B.huge_rows && k > tn.gain_hub_deg) : B.huge_rows;
+        if (k > tn.warp_dense_k || dense_rows)
             HP_LAUNCH(c, gain_dense_kernel<256>, (unsigned)(c->sm_count * 2), 256, smem, big_list, d_big_cnt,
-                      g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty);
+                      g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty, tn.gain_thread_deg,
+                      tn.gain_hub_deg, tn.warp_dense_k);
     }
     return HP_OK;
 }
@@ -1288,10 +1295,11 @@ int key_bits_for(int32_t k)
 }
 
 // Persistent grid of the rank/evict kernels: at most the tiles a count of n
-// can need, at most 8 CTAs per SM (they take tiles until the device count).
+// can need, at most grid_ctas_per_sm CTAs per SM (they take tiles until the
+// device count).
 unsigned rank_grid(const hp_context *c, int64_t tiles)
 {
-    return (unsigned)std::min<int64_t>(tiles, (int64_t)c->sm_count * 8);
+    return (unsigned)std::min<int64_t>(tiles, (int64_t)c->sm_count * c->tune.grid_ctas_per_sm);
 }
 
 // Candidates of the pass (rb_candidates_kernel, K/V in vertex order) -> stable
@@ -1512,7 +1520,7 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
     const int32_t n = g.n, k = P.k;
     unsigned long long *sc = c->d_scal;
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
-    const unsigned pg = (unsigned)(c->sm_count * 8);
+    const unsigned pg = (unsigned)(c->sm_count * c->tune.grid_ctas_per_sm);
     const int32_t *gate = both_lp ? &P.ctl->learned_pass : nullptr;
     if (mode == 0) {
         const int ltok = hp_prof_begin(c);
@@ -1528,10 +1536,10 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
                       P.finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.oldp, c->log_x, c->log_v,
                       c->log_d, c->log_acc, c->log_count, c->log_cap);
         HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest,
-                  B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
+                  B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES], c->tune.gain_thread_deg);
         if (P.any_big)
             HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt, g.where,
-                      B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES]);
+                      B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES], c->tune.gain_hub_deg);
         if (P.huge_rows) {
             const int32_t *d_nhuge = d_bigcnt + 3;
             HP_LAUNCH(c, hub_plan_kernel<false>, 1, 1024, 0, B.huge, d_nhuge, B.moves, B.pregain, g.xadj, B.plan_v,
@@ -1563,19 +1571,19 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
 {
     const int32_t n = g.n, k = P.k;
     unsigned long long *sc = c->d_scal;
-    const unsigned pg = (unsigned)(c->sm_count * 8);
+    const unsigned pg = (unsigned)(c->sm_count * c->tune.grid_ctas_per_sm);
     const unsigned mg = nblk(n);
     HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
               B.oldp, 1, &sc[S_C1], k);
     HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw, g.xadj,
               g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k,
-              B.huge_mv, (int32_t *)&sc[S_HUGEMV]);
+              B.huge_mv, (int32_t *)&sc[S_HUGEMV], c->tune.gain_thread_deg, c->tune.gain_hub_deg);
     if (P.huge_rows) {
         HP_LAUNCH(c, hub_plan_kernel<true>, 1, 1024, 0, B.huge_mv, (const int32_t *)&sc[S_HUGEMV], B.moves,
                   B.pregain, g.xadj, B.plan_v, B.plan_item, B.plan_off, B.plan_cnt);
         HP_LAUNCH(c, apply_moves_huge_kernel, (unsigned)(4 * c->sm_count), HUB_CHUNK, 0, B.plan_v, B.plan_item,
                   B.plan_off, B.plan_cnt, B.oldp, B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty,
-                  B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k);
+                  B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k, c->tune.gain_thread_deg);
     }
     const int rtok = hp_prof_begin(c);
     HP_TRY(build_rows(c, g, B, k, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
@@ -1744,8 +1752,9 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.lock = ralloc_t<int8_t>(c, n);
     B.pw = ralloc_t<unsigned long long>(c, k);
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
-    // at most m / (HUGED + 1) rows are longer than HUGED
-    const int64_t nhub_cap = std::min<int64_t>((int64_t)n, g.m / (HUGED + 1)) + 1;
+    // at most m / (huged + 1) rows are longer than huged
+    const int32_t huged = c->tune.gain_hub_deg;
+    const int64_t nhub_cap = std::min<int64_t>((int64_t)n, g.m / ((int64_t)huged + 1)) + 1;
     B.ab_acc = ralloc_t<unsigned long long>(c, nhub_cap);
     B.plan_v = ralloc_t<int32_t>(c, nhub_cap);
     B.plan_item = ralloc_t<int32_t>(c, nhub_cap);
@@ -1755,8 +1764,9 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     unsigned long long *sc = c->d_scal;
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 2), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
-    HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt);
-    if (ls.maxdeg > HUGED)
+    HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt,
+              c->tune.gain_thread_deg, huged);
+    if (ls.maxdeg > huged)
         HP_CUDA(cudaMemsetAsync(B.ab_acc, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
     // the gain rows take G = sum min(deg, k) <= m entries: allocated for m, so
@@ -1769,7 +1779,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     if (c->opt.profile && eager_loop) HP_TRY(hp_read_scalars(c, B.goff + n, sizeof(int32_t), &G));
     B.G = G;
     B.small_max = ls.small_max;
-    B.huge_rows = ls.maxdeg > HUGED;
+    B.huge_rows = ls.maxdeg > huged;
     B.gpart = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
     B.gconn = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
     HP_CHECK_OOM(c);
@@ -1867,7 +1877,7 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
     for (int l = 0; l <= L; l++)
         if (c->levels[l].n > 0)
             HP_LAUNCH(c, level_stats_kernel, std::min<unsigned>(nblk(c->levels[l].n), (unsigned)(c->sm_count * 8)),
-                      256, 0, c->levels[l].n, c->levels[l].xadj, d_ls + l);
+                      256, 0, c->levels[l].n, c->levels[l].xadj, d_ls + l, c->tune.gain_thread_deg);
     std::vector<LevelStat> ls(L + 1);
     HP_CUDA(cudaMemcpyAsync(ls.data(), d_ls, sizeof(LevelStat) * (size_t)(L + 1), cudaMemcpyDeviceToHost,
                             c->stream));

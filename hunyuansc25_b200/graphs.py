@@ -226,3 +226,12 @@ def config_rmat(scale: int = 22) -> Graph:
 
 def config_rgg(n: int = 1 << 24) -> Graph:
     return rgg(n, 12.0, seed=4)
+
+
+# name -> (graph constructor, nparts, imbalance factor)
+WORKLOADS = {
+    "grid2d": (config_grid2d, 8, 1.03),
+    "grid3d": (config_grid3d, 64, 1.03),
+    "rmat22": (config_rmat, 256, 1.03),
+    "rgg24": (config_rgg, 1024, 1.05),
+}

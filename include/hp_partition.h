@@ -136,6 +136,41 @@ int hp_partition_device(hp_context *ctx, int32_t nvtxs, int64_t nedges,
 /* Statistics of the last hp_partition*() call on ctx. */
 int hp_last_stats(const hp_context *ctx, hp_stats *out);
 
+/* ---- kernel tuning ---------------------------------------------------------------
+ * Speed-only parameters of the kernels: degree-class bounds (which kernel
+ * aggregates a row), grid sizes and the accumulator layout.  Every setting in
+ * range gives the same partition and cut bit for bit -- each class produces
+ * the same canonical rows and proposals -- so a tuning changes time only.
+ * The project's autotuner (hunyuansc25_b200/tune.py) searches them per
+ * workload and stores the result in a tuning file.  No counterpart in the
+ * reference, whose class bounds and block sizes are compile-time constants
+ * (hunyuangraph_GPU_match.h, hunyuangraph_GPU_contraction.h). */
+typedef struct hp_tuning {
+    int32_t match_warp_deg;      /* matching: rows longer than this take a warp  [4, 256]      32 */
+    int32_t match_cta_deg;       /* matching: rows longer than this take a CTA   [match_warp_deg, 2^24] 4096 */
+    int32_t contract_thread_row; /* contraction: coarse rows up to this many
+                                    entries merge in one thread's registers      [8, 32]       32 */
+    int32_t contract_warp_row;   /* ... up to this by a warp radix sort           [contract_thread_row, 256] 256 */
+    int32_t contract_cta_row;    /* ... up to this by a 256-thread CTA radix sort [contract_warp_row, 4096] 4096;
+                                    longer rows: 1024-thread radix up to 12288, dense above */
+    int32_t gain_thread_deg;     /* refinement: gain rows of up to this many entries by a
+                                    thread or lane segment                        [8, 32]       32 */
+    int32_t gain_hub_deg;        /* refinement: rows longer than this are hubs (CTA gain
+                                    rows, grid-wide chunked moves and afterburner) [gain_thread_deg, 2^24] 4096 */
+    int32_t warp_dense_k;        /* refinement: warp gain rows with shared-memory
+                                    accumulators when nparts <= this              [0, 1024]     1024 */
+    int32_t grid_ctas_per_sm;    /* grid-stride kernels: CTAs per SM              [1, 32]       8 */
+    int32_t dense_sparse_ratio;  /* dense contraction rows: the two-level bitmap when
+                                    entries * ratio < bitmap words                [1, 4096]     4 */
+    int32_t reserved[6];         /* zero */
+} hp_tuning;
+
+void hp_tuning_default(hp_tuning *t);
+/* Validates and installs a tuning on ctx (batch workers inherit it); returns
+ * HP_ERR_INVALID_ARG, with a message on stderr, for a value out of range. */
+int hp_context_set_tuning(hp_context *ctx, const hp_tuning *t);
+int hp_context_get_tuning(const hp_context *ctx, hp_tuning *t);
+
 /* ---- level trace (opt.trace = 1), for parity checks of every level ----------- */
 #define HP_TRACE_XADJ         0   /* int32[n+1]  CSR of level l                      */
 #define HP_TRACE_ADJNCY       1   /* int32[m]                                        */
