@@ -24,9 +24,11 @@
 namespace {
 
 // Structural validation: vertex checks per thread, adjacency checks in
-// edge-parallel tiles of 256 x 32 entries (the owner of an entry is found by a
-// binary search over xadj, then a forward walk), so hub rows cost no more than
-// their share of the array.
+// edge-parallel tiles of VE_TILE entries, so hub rows cost no more than their
+// share of the array.  The owner row of every entry of a tile comes from a
+// shared-memory max-scan over row-start markers: the rows starting inside the
+// tile mark their first entry, the row overlapping the tile's start (one
+// binary search) marks entry 0, and the running maximum is the owner.
 __global__ void validate_vertices_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
                                          const int32_t *__restrict__ vwgt, unsigned *status)
 {
@@ -40,29 +42,74 @@ __global__ void validate_vertices_kernel(int32_t n, int64_t m, const int32_t *__
     if (bad) atomicOr(status, HP_STATUS_BAD_GRAPH);
 }
 
-// Runs after validate_vertices_kernel succeeded (xadj monotone, in range).
-__global__ void __launch_bounds__(256)
+constexpr int VE_THREADS = 256, VE_ITEMS = 16, VE_TILE = VE_THREADS * VE_ITEMS;
+
+// Runs after validate_vertices_kernel succeeded (xadj monotone, xadj[0] = 0,
+// xadj[n] = m, so every entry has exactly one owner row).
+__global__ void __launch_bounds__(VE_THREADS)
 validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
                       const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt, unsigned *status)
 {
-    if (*status & HP_STATUS_BAD_GRAPH) return;
-    const int64_t tile = 256 * 32;
+    __shared__ int32_t owner[VE_TILE];
+    __shared__ int32_t s_warp[VE_THREADS / 32];
+    __shared__ int32_t s_v0;
+    if (*status & HP_STATUS_BAD_GRAPH) return;   // uniform over the grid
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     bool bad = false;
-    for (int64_t tb = blockIdx.x * tile; tb < m; tb += (int64_t)gridDim.x * tile) {
-        int64_t j = tb + threadIdx.x;
-        if (j >= m) continue;
-        int32_t lo = 0, hi = n - 1;
-        while (lo < hi) {
-            int32_t mid = (int32_t)(((int64_t)lo + hi + 1) / 2);
-            if (xadj[mid] <= j) lo = mid; else hi = mid - 1;
+    for (int64_t tb = (int64_t)blockIdx.x * VE_TILE; tb < m; tb += (int64_t)gridDim.x * VE_TILE) {
+        const int64_t te = tb + VE_TILE < m ? tb + VE_TILE : m;
+        if (threadIdx.x == 0) {
+            // the last row starting at or before tb (xadj[0] = 0 <= tb < m = xadj[n])
+            int32_t lo = 0, hi = n - 1;
+            while (lo < hi) {
+                const int32_t mid = (int32_t)(((int64_t)lo + hi + 1) / 2);
+                if (xadj[mid] <= tb) lo = mid; else hi = mid - 1;
+            }
+            s_v0 = lo;
         }
-        int32_t v = lo;
-        for (int k = 0; k < 32 && j < m; k++, j += 256) {
-            while (xadj[v + 1] <= j) v++;
+        for (int i = threadIdx.x; i < VE_TILE; i += VE_THREADS) owner[i] = -1;
+        __syncthreads();
+        const int32_t v0 = s_v0;
+        if (threadIdx.x == 0) owner[0] = v0;
+        // rows v > v0 start after tb; those starting before te mark their start
+        // (an empty row shares its start with a later row, which wins the max)
+        for (int64_t v = (int64_t)v0 + 1 + threadIdx.x; v < n; v += VE_THREADS) {
+            const int32_t b = xadj[v];
+            if (b >= te) break;
+            atomicMax(&owner[b - tb], (int32_t)v);
+        }
+        __syncthreads();
+        // inclusive max-scan: VE_ITEMS consecutive markers per thread
+        int32_t run = -1;
+#pragma unroll
+        for (int q = 0; q < VE_ITEMS; q++) run = max(run, owner[threadIdx.x * VE_ITEMS + q]);
+        int32_t x = run;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t y = __shfl_up_sync(HP_FULL_MASK, x, o);
+            if (lane >= o) x = max(x, y);
+        }
+        if (lane == 31) s_warp[wid] = x;
+        int32_t ex = __shfl_up_sync(HP_FULL_MASK, x, 1);
+        if (lane == 0) ex = -1;
+        __syncthreads();
+        for (int w = 0; w < wid; w++) ex = max(ex, s_warp[w]);
+        __syncthreads();   // every thread has read the markers it scans
+#pragma unroll
+        for (int q = 0; q < VE_ITEMS; q++) {
+            const int i = threadIdx.x * VE_ITEMS + q;
+            ex = max(ex, owner[i]);
+            owner[i] = ex;
+        }
+        __syncthreads();
+        // checks, coalesced over the tile
+        for (int64_t j = tb + threadIdx.x; j < te; j += VE_THREADS) {
+            const int32_t v = owner[j - tb];
             const int32_t u = adjncy[j];
             if (u < 0 || u >= n || u == v) bad = true;
             if (adjwgt && adjwgt[j] <= 0) bad = true;
         }
+        __syncthreads();   // owner[] is rebuilt for the next tile
     }
     if (bad) atomicOr(status, HP_STATUS_BAD_GRAPH);
 }
@@ -159,7 +206,10 @@ int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, i
 
     if (c->opt.validate) {
         HP_LAUNCH(c, validate_vertices_kernel, gsz(c, n), 256, 0, n, g0.m, g0.xadj, g0.vwgt, c->d_status);
-        HP_LAUNCH(c, validate_edges_kernel, gsz(c, (g0.m + 31) / 32), 256, 0, n, g0.m, g0.xadj, g0.adjncy,
+        HP_LAUNCH(c, validate_edges_kernel,
+                  (unsigned)std::max<int64_t>(1, std::min<int64_t>((g0.m + VE_TILE - 1) / VE_TILE,
+                                                                   (int64_t)c->sm_count * 8)),
+                  VE_THREADS, 0, n, g0.m, g0.xadj, g0.adjncy,
                   g0.adjwgt, c->d_status);
     }
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 2, c->stream));

@@ -76,7 +76,8 @@ __global__ void __launch_bounds__(256)
 pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
                   const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
-                  uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev, int32_t warp_deg)
+                  uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev, int32_t warp_deg,
+                  int32_t *__restrict__ hubflag)
 {
     if (made_prev && *made_prev == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -110,6 +111,7 @@ pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__
         }
     }
     pref[v] = best.u;
+    if (!ELIG && best.u >= 0) hubflag[best.u] = 1;   // the hub has a client to pair
 }
 
 template <bool ELIG>
@@ -118,7 +120,8 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
                 const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                 const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
                 const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
-                uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
+                uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev,
+                int32_t *__restrict__ hubflag)
 {
     if (made_prev && *made_prev == 0ull) return;
     const int lane = threadIdx.x & 31;
@@ -150,7 +153,10 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
             uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
             if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; }
         }
-        if (lane == 0) pref[v] = bu;
+        if (lane == 0) {
+            pref[v] = bu;
+            if (!ELIG && bu >= 0) hubflag[bu] = 1;
+        }
     }
 }
 
@@ -376,7 +382,8 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
                  const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                  const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
                  const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
-                 uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
+                 uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev,
+                 int32_t *__restrict__ hubflag)
 {
     if (made_prev && *made_prev == 0ull) return;
     __shared__ int32_t su[16], sw[16];
@@ -417,6 +424,7 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
                     bu = su[w2]; bw = sw[w2]; bh = sh[w2];
                 }
             pref[v] = bu;
+            if (!ELIG && bu >= 0) hubflag[bu] = 1;
         }
         __syncthreads();
     }
@@ -427,13 +435,14 @@ __global__ void __launch_bounds__(512)
 pair_hub_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                      const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                      const int32_t *__restrict__ vwgt, const int32_t *__restrict__ hub,
-                     int32_t *__restrict__ match, int64_t maxvwgt)
+                     int32_t *__restrict__ match, int64_t maxvwgt, const int32_t *__restrict__ hubflag)
 {
     __shared__ int32_t s_scan[512 / 32 + 2];
     __shared__ int32_t s_cl[512];
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t h = list[li];
+        if (!hubflag[h]) continue;   // nobody chose h: no client in its row
         int32_t t = 0, carry = -1;
         for (int32_t base = xadj[h]; base < xadj[h + 1]; base += 512) {
             const int32_t j = base + threadIdx.x;
@@ -468,10 +477,10 @@ __global__ void __launch_bounds__(256)
 pair_hub_small_kernel(int32_t n, const int32_t *__restrict__ xadj,
                       const int32_t *__restrict__ adjncy, const int32_t *__restrict__ vwgt,
                       const int32_t *__restrict__ hub, int32_t *__restrict__ match, int64_t maxvwgt,
-                      int32_t warp_deg)
+                      int32_t warp_deg, const int32_t *__restrict__ hubflag)
 {
     int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= n) return;
+    if (h >= n || !hubflag[h]) return;
     const int32_t b = xadj[h], e = xadj[h + 1];
     if (e - b > warp_deg) return;
     int32_t first = -1, t = 0;
@@ -488,13 +497,14 @@ __global__ void __launch_bounds__(256)
 pair_hub_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                     const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                     const int32_t *__restrict__ vwgt, const int32_t *__restrict__ hub,
-                    int32_t *__restrict__ match, int64_t maxvwgt)
+                    int32_t *__restrict__ match, int64_t maxvwgt, const int32_t *__restrict__ hubflag)
 {
     const int lane = threadIdx.x & 31;
     const int32_t cnt = *d_count;
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t h = list[i];
+        if (!hubflag[h]) continue;   // nobody chose h: no client in its row
         int32_t t = 0;          // clients seen so far
         int32_t carry = -1;     // unpaired client from the previous chunk (t odd)
         for (int32_t base = xadj[h]; base < xadj[h + 1]; base += 32) {
@@ -1150,7 +1160,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
         const int tok = hp_prof_begin(c);
         const unsigned long long *prev = r == 0 ? nullptr : &sc[2 + r - 1];
         HP_LAUNCH(c, pref_small_kernel<true>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
-                  g.vwgt, g.match, elig, pref, lkey, maxvwgt, prev, tn.match_warp_deg);
+                  g.vwgt, g.match, elig, pref, lkey, maxvwgt, prev, tn.match_warp_deg, (int32_t *)nullptr);
         HP_LAUNCH(c, pref_big_topk_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
                   g.vwgt, g.match, elig, pref, cand, lkey, maxvwgt, prev);
         HP_LAUNCH(c, pref_huge_topk_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
@@ -1170,22 +1180,26 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     HP_TRY(matched(40, &nm));
     const int ftok = hp_prof_begin(c);
     if (4 * nm < 3 * (int64_t)n) {
-        // two-hop through a shared heaviest neighbour
+        // two-hop through a shared heaviest neighbour; hubflag marks the chosen
+        // hubs, so that only their rows are walked for clients
         int32_t *hub = pref;
+        int32_t *hubflag = flags;
+        HP_CUDA(cudaMemsetAsync(hubflag, 0, sizeof(int32_t) * (size_t)n, c->stream));
         HP_LAUNCH(c, pref_small_kernel<false>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
-                  g.vwgt, g.match, elig, hub, lkey, maxvwgt, (const unsigned long long *)nullptr, tn.match_warp_deg);
+                  g.vwgt, g.match, elig, hub, lkey, maxvwgt, (const unsigned long long *)nullptr, tn.match_warp_deg,
+                  hubflag);
         HP_LAUNCH(c, pref_big_kernel<false>, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, elig, hub, lkey, maxvwgt,
-                  (const unsigned long long *)nullptr);
+                  (const unsigned long long *)nullptr, hubflag);
         HP_LAUNCH(c, pref_huge_kernel<false>, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, elig, hub, lkey, maxvwgt,
-                  (const unsigned long long *)nullptr);
+                  (const unsigned long long *)nullptr, hubflag);
         HP_LAUNCH(c, pair_hub_small_kernel, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.vwgt, hub,
-                  g.match, maxvwgt, tn.match_warp_deg);
+                  g.match, maxvwgt, tn.match_warp_deg, hubflag);
         HP_LAUNCH(c, pair_hub_big_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy,
-                  g.vwgt, hub, g.match, maxvwgt);
+                  g.vwgt, hub, g.match, maxvwgt, hubflag);
         HP_LAUNCH(c, pair_hub_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
-                  g.adjncy, g.vwgt, hub, g.match, maxvwgt);
+                  g.adjncy, g.vwgt, hub, g.match, maxvwgt, hubflag);
         hp_prof_end(c, ftok, HP_PROF_MATCH_MORE, 0);
         HP_TRY(matched(41, &nm));
     }

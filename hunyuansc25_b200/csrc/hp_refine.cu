@@ -344,10 +344,20 @@ __device__ __forceinline__ int32_t row_conn(const int32_t *gp, const int32_t *gc
                                             int32_t k)
 {
     if (len == k) return gc[q];   // dense row
-    for (int32_t j = 0; j < len; j++) {
-        int32_t p = gp[j];
+    // rows are ascending by part and padded with -1: bisect to a short window
+    // (entries before lo are parts below q; entries from hi on are padding or
+    // parts >= q), then walk to the first entry that is padding or >= q
+    int32_t lo = 0, hi = len;
+    while (hi - lo > 8) {
+        const int32_t mid = (lo + hi) >> 1;
+        const int32_t p = gp[mid];
+        if (p >= 0 && p < q) lo = mid + 1;
+        else hi = mid;
+    }
+    for (int32_t j = lo; j < len; j++) {
+        const int32_t p = gp[j];
         if (p == q) return gc[j];
-        if (p < 0 || p > q) break;   // rows are ascending by part
+        if (p < 0 || p > q) break;
     }
     return 0;
 }
@@ -380,14 +390,33 @@ rowcut_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__rest
               const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
               unsigned long long *cut2)
 {
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
     long long acc = 0;
+    int32_t p = 0, o = 0, len = 0;
     if (v < n) {
-        const int32_t p = where[v];
-        for (int32_t j = goff[v]; j < goff[v + 1]; j++) {
-            int32_t q = gpart[j];
+        p = where[v];
+        o = goff[v];
+        len = goff[v + 1] - o;
+    }
+    // rows longer than 32 entries are summed by the whole warp, one at a time
+    const bool coop = len > 32;
+    if (!coop)
+        for (int32_t j = o; j < o + len; j++) {
+            const int32_t q = gpart[j];
             if (q < 0) break;
             if (q != p) acc += gconn[j];
+        }
+    unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
+    while (cm) {
+        const int src = __ffs(cm) - 1;
+        cm &= cm - 1;
+        const int32_t so = __shfl_sync(HP_FULL_MASK, o, src), sl = __shfl_sync(HP_FULL_MASK, len, src);
+        const int32_t sp = __shfl_sync(HP_FULL_MASK, p, src);
+        for (int32_t j = lane; j < sl; j += 32) {
+            const int32_t q = gpart[so + j];
+            if (q < 0) break;
+            if (q != sp) acc += gconn[so + j];
         }
     }
     hp::block_add_to<256>(acc, cut2);
@@ -413,6 +442,65 @@ __global__ void excess_kernel(int32_t k, const unsigned long long *__restrict__ 
     }
 }
 
+// One gain row against the own part p: connectivity to p (pc), the best other
+// part b (largest connectivity, the first -- lowest -- part among equals; -1
+// when no other part has positive connectivity) and bc, the row's total
+// connectivity wd and its count np of parts with positive connectivity.
+struct RowBest {
+    int64_t pc, bc, wd;
+    int32_t b, np;
+};
+
+// Called by every lane of the warp, each with its own row (len 0 for none).
+// Rows of at most 32 entries are walked by their lane; longer rows by the
+// whole warp, one row at a time, reduced in the serial walk's order.
+__device__ __forceinline__ RowBest row_best(const int32_t *__restrict__ gpart, const int32_t *__restrict__ gconn,
+                                            int32_t o, int32_t len, int32_t p)
+{
+    const int lane = threadIdx.x & 31;
+    RowBest r{0, 0, 0, -1, 0};
+    const bool coop = len > 32;
+    if (!coop)
+        for (int32_t j = o; j < o + len; j++) {
+            const int32_t q = gpart[j];
+            if (q < 0) break;
+            const int32_t cq = gconn[j];
+            r.wd += cq;
+            r.np += cq > 0;
+            if (q == p) { r.pc = cq; continue; }
+            if (cq > r.bc) { r.bc = cq; r.b = q; }   // ascending parts: first max = lowest part
+        }
+    unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
+    while (cm) {
+        const int src = __ffs(cm) - 1;
+        cm &= cm - 1;
+        const int32_t so = __shfl_sync(HP_FULL_MASK, o, src), sl = __shfl_sync(HP_FULL_MASK, len, src);
+        const int32_t sp = __shfl_sync(HP_FULL_MASK, p, src);
+        int32_t lpc = 0, lbc = 0, lb = -1, lnp = 0;
+        long long lwd = 0;
+        for (int32_t j = lane; j < sl; j += 32) {
+            const int32_t q = gpart[so + j];
+            if (q < 0) break;   // padding runs to the end of the row
+            const int32_t cq = gconn[so + j];
+            lwd += cq;
+            lnp += cq > 0;
+            if (q == sp) { lpc = cq; continue; }
+            if (cq > lbc) { lbc = cq; lb = q; }
+        }
+        lpc = hp::warp_sum(lpc);
+        lnp = hp::warp_sum(lnp);
+        lwd = hp::warp_sum64(lwd);
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) {
+            const int32_t ob = __shfl_xor_sync(HP_FULL_MASK, lb, sh);
+            const int32_t oc = __shfl_xor_sync(HP_FULL_MASK, lbc, sh);
+            if (ob >= 0 && (lb < 0 || oc > lbc || (oc == lbc && ob < lb))) { lb = ob; lbc = oc; }
+        }
+        if (lane == src) { r.pc = lpc; r.bc = lbc; r.b = lb; r.wd = lwd; r.np = lnp; }
+    }
+    return r;
+}
+
 // ---- LP ------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
@@ -421,19 +509,18 @@ lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__r
                  int32_t *__restrict__ pregain, unsigned long long *d_ncand, const int32_t *gate)
 {
     if (gate && *gate != 0) return;   // graph mode: the learned kernel runs this pass
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int cand = 0;
+    int32_t p = 0, o = 0, len = 0;
     if (v < n) {
-        const int32_t p = where[v];
-        int64_t pc = 0, bc = 0;
-        int32_t b = -1;
-        for (int32_t j = goff[v]; j < goff[v + 1]; j++) {
-            int32_t q = gpart[j];
-            if (q < 0) break;
-            int32_t cq = gconn[j];
-            if (q == p) { pc = cq; continue; }
-            if (cq > bc) { bc = cq; b = q; }   // ascending parts: first max = lowest part
-        }
+        p = where[v];
+        o = goff[v];
+        len = goff[v + 1] - o;
+    }
+    const RowBest rb = row_best(gpart, gconn, o, len, p);
+    const int64_t pc = rb.pc, bc = rb.bc;
+    const int32_t b = rb.b;
+    if (v < n) {
         int32_t g = NEG, d = p;
         if (b >= 0) {
             int64_t thr = finest ? pc / 4 : (3 * pc) / 4;
@@ -462,23 +549,20 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
     __shared__ hp::MlpSmem sm;
     hp::mlp_load_smem(sm, params);
     __syncthreads();
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int cand = 0;
     float f[HP_MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int32_t g = NEG, d = 0;
+    int32_t p = 0, o = 0, len = 0;
     if (v < n) {
-        const int32_t p = where[v];
-        int64_t pc = 0, bc = 0, wd = 0;
-        int32_t b = -1, np = 0;
-        for (int32_t j = goff[v]; j < goff[v + 1]; j++) {
-            int32_t q = gpart[j];
-            if (q < 0) break;
-            int32_t cq = gconn[j];
-            wd += cq;
-            np += cq > 0;
-            if (q == p) { pc = cq; continue; }
-            if (cq > bc) { bc = cq; b = q; }
-        }
+        p = where[v];
+        o = goff[v];
+        len = goff[v + 1] - o;
+    }
+    const RowBest rb = row_best(gpart, gconn, o, len, p);
+    if (v < n) {
+        const int64_t pc = rb.pc, bc = rb.bc, wd = rb.wd;
+        const int32_t b = rb.b, np = rb.np;
         d = p;
         if (b >= 0) {
             int64_t thr = finest ? pc / 4 : (3 * pc) / 4;
@@ -734,15 +818,15 @@ c_delta_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nm
                unsigned long long *d_c, int32_t k)
 {
     const int64_t nm = (int64_t)*d_nmoves;
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if ((int64_t)blockIdx.x * blockDim.x >= nm) return;   // whole CTA idle (uniform)
     long long acc = 0;
-    if (i < nm) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm; i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t v = moves[i];
         const int32_t o = goff[v], len = goff[v + 1] - o;
         int32_t from, to;
         if (before) { from = where[v]; to = dest[v]; oldp[i] = from; }
         else { from = oldp[i]; to = where[v]; }
-        acc = (long long)row_conn(gpart + o, gconn + o, len, to, k) - row_conn(gpart + o, gconn + o, len, from, k);
+        acc += (long long)row_conn(gpart + o, gconn + o, len, to, k) - row_conn(gpart + o, gconn + o, len, from, k);
     }
     hp::block_add_to<256>(acc, d_c);
 }
@@ -766,7 +850,9 @@ __device__ __forceinline__ void touch_neighbour(bool valid, int32_t u, int32_t w
         if (goff[u + 1] - o == k) {
             atomicAdd(&gconn[o + p], -w);
             atomicAdd(&gconn[o + d], w);
-        } else if (atomicExch(&dirty[u], 1) == 0) {
+        } else if (__ldcg(&dirty[u]) == 0 && atomicExch(&dirty[u], 1) == 0) {
+            // (a row already queued in this pass is skipped without an atomic;
+            // flags only go from 0 to 1 inside the kernel)
             if (xadj[u + 1] - xadj[u] > bigd) bg = true;
             else sm = true;
         }
@@ -887,6 +973,7 @@ __device__ __forceinline__ void undersized_block(int32_t k, const unsigned long 
 //         loss = -conn(own)
 // The part bounds pstart/pend are reset to -1 here for the rank kernel.
 constexpr int RB_TILE = 256;
+constexpr int RB_COOP = 32;   // weak rebalance: longer gain rows are walked by a warp
 
 template <bool STRONG>
 __global__ void __launch_bounds__(RB_TILE)
@@ -909,42 +996,75 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
         pend[q] = -1;
     }
     const int64_t v64 = tile * RB_TILE + threadIdx.x;
+    const int lane = threadIdx.x & 31;
     int32_t kk = -1;
-    if (v64 < n) {
-        const int32_t v = (int32_t)v64;
-        const int32_t p = where[v];
-        int32_t d = p;
+    const bool in = v64 < n;
+    const int32_t v = in ? (int32_t)v64 : 0;
+    int32_t p = 0;
+    bool cand = false;   // in an overweight part and light enough to leave it
+    if (in) {
+        p = where[v];
         const int64_t pwp = (int64_t)pw[p];
-        if (!STRONG) {
-            if (pwp > maxp[p] && 2 * (int64_t)vwgt[v] < 3 * (pwp - opt[p])) {
-                int64_t pc = 0, bc = 0;
-                int32_t b = -1;
-                for (int32_t j = goff[v]; j < goff[v + 1]; j++) {
-                    int32_t q = gpart[j];
-                    if (q < 0) break;
-                    int32_t cq = gconn[j];
-                    if (q == p) pc = cq;
-                    if ((int64_t)pw[q] < maxp[q] && cq > bc) { bc = cq; b = q; }
-                }
-                int64_t g = 0;
-                bool ok = true;
-                if (b >= 0) g = bc - pc;
-                else {
-                    const int32_t nu = *d_nu;
-                    if (nu == 0) ok = false;
-                    else { b = und[v % nu]; g = -pc; }
-                }
-                if (ok) { d = b; kk = p * 64 + hp::gain_bucket((int32_t)g, vwgt[v]); }
-            }
-        } else {
-            if (pwp > maxp[p] && (int64_t)vwgt[v] < 2 * (pwp - opt[p])) {
-                int32_t o = goff[v];
-                int32_t pc = row_conn(gpart + o, gconn + o, goff[v + 1] - o, p, k);
-                kk = p * 64 + hp::gain_bucket(-pc, vwgt[v]);
+        cand = STRONG ? (pwp > maxp[p] && (int64_t)vwgt[v] < 2 * (pwp - opt[p]))
+                      : (pwp > maxp[p] && 2 * (int64_t)vwgt[v] < 3 * (pwp - opt[p]));
+    }
+    const int32_t o = cand ? goff[v] : 0, len = cand ? goff[v + 1] - o : 0;
+    int32_t d = p;
+    if (!STRONG) {
+        // best underweight part by connectivity (first, i.e. lowest part, among
+        // equals) and the connectivity to the own part; rows of more than
+        // RB_COOP entries are walked by the whole warp, one row at a time
+        int64_t pc = 0, bc = 0;
+        int32_t b = -1;
+        const bool coop = cand && len > RB_COOP;
+        if (cand && !coop) {
+            for (int32_t j = o; j < o + len; j++) {
+                const int32_t q = gpart[j];
+                if (q < 0) break;
+                const int32_t cq = gconn[j];
+                if (q == p) pc = cq;
+                if ((int64_t)pw[q] < maxp[q] && cq > bc) { bc = cq; b = q; }
             }
         }
-        dest[v] = d;
+        unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
+        while (cm) {
+            const int src = __ffs(cm) - 1;
+            cm &= cm - 1;
+            const int32_t so = __shfl_sync(HP_FULL_MASK, o, src), sl = __shfl_sync(HP_FULL_MASK, len, src);
+            const int32_t sp = __shfl_sync(HP_FULL_MASK, p, src);
+            int32_t lpc = 0, lbc = 0, lb = -1;
+            for (int32_t j = lane; j < sl; j += 32) {
+                const int32_t q = gpart[so + j];
+                if (q < 0) break;   // padding runs to the end of the row
+                const int32_t cq = gconn[so + j];
+                if (q == sp) lpc = cq;
+                if ((int64_t)pw[q] < maxp[q] && cq > lbc) { lbc = cq; lb = q; }
+            }
+            lpc = hp::warp_sum(lpc);
+#pragma unroll
+            for (int sh = 16; sh > 0; sh >>= 1) {
+                const int32_t ob = __shfl_xor_sync(HP_FULL_MASK, lb, sh);
+                const int32_t oc = __shfl_xor_sync(HP_FULL_MASK, lbc, sh);
+                if (ob >= 0 && (lb < 0 || oc > lbc || (oc == lbc && ob < lb))) { lb = ob; lbc = oc; }
+            }
+            if (lane == src) { pc = lpc; bc = lbc; b = lb; }
+        }
+        if (cand) {
+            int64_t g = 0;
+            bool ok = true;
+            if (b >= 0) g = bc - pc;
+            else {
+                const int32_t nu = *d_nu;
+                if (nu == 0) ok = false;
+                else { b = und[v % nu]; g = -pc; }
+            }
+            if (ok) { d = b; kk = p * 64 + hp::gain_bucket((int32_t)g, vwgt[v]); }
+        }
+    } else if (cand) {
+        const int32_t pc = row_conn(gpart + o, gconn + o, len, p, k);
+        kk = p * 64 + hp::gain_bucket(-pc, vwgt[v]);
     }
+    if (in) dest[v] = d;
     int tot;
     const int local = hp::block_excl_scan<RB_TILE>(kk >= 0 ? 1 : 0, &tot, s_scan);
     if (threadIdx.x < 32) {
@@ -1572,7 +1692,7 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
     const int32_t n = g.n, k = P.k;
     unsigned long long *sc = c->d_scal;
     const unsigned pg = (unsigned)(c->sm_count * c->tune.grid_ctas_per_sm);
-    const unsigned mg = nblk(n);
+    const unsigned mg = std::min(nblk(n), pg);   // grid-stride over the device move count
     HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
               B.oldp, 1, &sc[S_C1], k);
     HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw, g.xadj,

@@ -233,5 +233,6 @@ WORKLOADS = {
     "grid2d": (config_grid2d, 8, 1.03),
     "grid3d": (config_grid3d, 64, 1.03),
     "rmat22": (config_rmat, 256, 1.03),
+    "rmat20": (lambda: config_rmat(20), 256, 1.03),   # a quarter-size R-MAT for profiler captures
     "rgg24": (config_rgg, 1024, 1.05),
 }
