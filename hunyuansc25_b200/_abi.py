@@ -89,6 +89,7 @@ TUNING_FIELDS = [
     "warp_dense_k",
     "grid_ctas_per_sm",
     "dense_sparse_ratio",
+    "small_level_n",
 ]
 
 TUNING_DEFAULTS = {
@@ -102,6 +103,7 @@ TUNING_DEFAULTS = {
     "warp_dense_k": 1024,
     "grid_ctas_per_sm": 8,
     "dense_sparse_ratio": 4,
+    "small_level_n": 4096,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -121,6 +123,7 @@ def tuning_violation(t: dict):
         ("warp_dense_k", 0, 1024),
         ("grid_ctas_per_sm", 1, 32),
         ("dense_sparse_ratio", 1, 4096),
+        ("small_level_n", 0, 32768),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -129,7 +132,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 6)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 5)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

@@ -95,6 +95,7 @@ constexpr int HP_TUNE_WARP_ROW_MAX = 256;        // contract_warp_radix_kernel's
 constexpr int HP_TUNE_CTA_ROW_MAX = 4096;        // contract_cta_radix_kernel<256, 4096>
 constexpr int HP_TUNE_WARP_DENSE_K_MAX = 1024;   // gain_bigwarp_kernel's shared accumulators
 constexpr int HP_TUNE_DEG_MAX = 1 << 24;
+constexpr int HP_TUNE_SMALL_LEVEL_MAX = 32768;   // refine_small_kernel's staged prefix weights
 
 #define HP_NSCAL 64
 #define HP_ALIGN 256

@@ -184,19 +184,17 @@ gain_thread_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__
 // longest short row): 32/S rows per warp, one segment of S lanes per row,
 // sorted and merged by seg_aggregate; dirty flags are cleared.  Rows with
 // deg >= k (k <= S here) are written dense.
+// (warp, nwarps: this warp's index among the nwarps warps sharing the list)
 template <int S>
-__global__ void __launch_bounds__(256)
-gain_seg_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
-                const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
-                const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
-                const int32_t *__restrict__ goff, int32_t *__restrict__ gpart, int32_t *__restrict__ gconn,
-                int32_t k, int32_t *__restrict__ dirty)
+__device__ __forceinline__ void gain_seg_rows(int64_t warp, int64_t nwarps, const int32_t *__restrict__ list,
+                                              int32_t cnt, const int32_t *__restrict__ xadj,
+                                              const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt,
+                                              const int32_t *__restrict__ where, const int32_t *__restrict__ goff,
+                                              int32_t *__restrict__ gpart, int32_t *__restrict__ gconn, int32_t k,
+                                              int32_t *__restrict__ dirty)
 {
     constexpr int R = 32 / S;
     const int lane = threadIdx.x & 31, sl = lane & (S - 1);
-    const int32_t cnt = *d_count;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i0 = warp * R; i0 < cnt; i0 += nwarps * R) {
         const int64_t i = i0 + lane / S;
         int32_t v = -1, b = 0, d = 0;
@@ -223,6 +221,18 @@ gain_seg_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
     }
 }
 
+template <int S>
+__global__ void __launch_bounds__(256)
+gain_seg_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
+                const int32_t *__restrict__ goff, int32_t *__restrict__ gpart, int32_t *__restrict__ gconn,
+                int32_t k, int32_t *__restrict__ dirty)
+{
+    gain_seg_rows<S>((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, ((int64_t)gridDim.x * blockDim.x) >> 5,
+                     list, *d_count, xadj, adjncy, adjwgt, where, goff, gpart, gconn, k, dirty);
+}
+
 // Gain rows of bigd+1 .. huged entries when k <= warp_dense_k: one warp per
 // row with its own dense accumulator and presence bitmap over the k parts in
 // shared memory (k + k/32 words per warp), extracted in part order; only warp
@@ -230,24 +240,19 @@ gain_seg_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
 // gain_dense_kernel.
 constexpr int GW_WARPS = 8;   // k + k/32 words per warp: 33 KB at k = HP_TUNE_WARP_DENSE_K_MAX
 
-__global__ void __launch_bounds__(32 * GW_WARPS)
-gain_bigwarp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
-                    const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
-                    const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
-                    const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
-                    int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty, int32_t bigd,
-                    int32_t huged)
+// The rows of one warp: dw (k words) and bm (ceil(k/32) words) are the warp's
+// own accumulators, zero on entry and left zero.
+__device__ __forceinline__ void gain_bigwarp_rows(int64_t warp, int64_t nwarps, int32_t *dw, unsigned *bm,
+                                                  const int32_t *__restrict__ list, int32_t cnt,
+                                                  const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                                                  const int32_t *__restrict__ adjwgt,
+                                                  const int32_t *__restrict__ where, const int32_t *__restrict__ goff,
+                                                  int32_t *__restrict__ gpart, int32_t *__restrict__ gconn, int32_t k,
+                                                  int32_t *__restrict__ dirty, int32_t bigd, int32_t huged)
 {
-    extern __shared__ int32_t gsm[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
     const int nwords = (k + 31) >> 5;
-    int32_t *dw = gsm + wid * (k + nwords);
-    unsigned *bm = (unsigned *)(dw + k);
-    for (int i = lane; i < k; i += 32) dw[i] = 0;
-    for (int i = lane; i < nwords; i += 32) bm[i] = 0u;
-    __syncwarp();
-    const int32_t cnt = *d_count;
-    for (int64_t li = (int64_t)blockIdx.x * GW_WARPS + wid; li < cnt; li += (int64_t)gridDim.x * GW_WARPS) {
+    for (int64_t li = warp; li < cnt; li += nwarps) {
         const int32_t v = list[li];
         const int32_t b = xadj[v], e = xadj[v + 1];
         if (e - b <= bigd || e - b > huged) continue;
@@ -291,6 +296,26 @@ gain_bigwarp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict_
         for (int32_t t = run + lane; t < cap; t += 32) { gpart[o + t] = -1; gconn[o + t] = 0; }
         __syncwarp();
     }
+}
+
+__global__ void __launch_bounds__(32 * GW_WARPS)
+gain_bigwarp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                    const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                    const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
+                    const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
+                    int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty, int32_t bigd,
+                    int32_t huged)
+{
+    extern __shared__ int32_t gsm[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nwords = (k + 31) >> 5;
+    int32_t *dw = gsm + wid * (k + nwords);
+    unsigned *bm = (unsigned *)(dw + k);
+    for (int i = lane; i < k; i += 32) dw[i] = 0;
+    for (int i = lane; i < nwords; i += 32) bm[i] = 0u;
+    __syncwarp();
+    gain_bigwarp_rows((int64_t)blockIdx.x * GW_WARPS + wid, (int64_t)gridDim.x * GW_WARPS, dw, bm, list, *d_count,
+                      xadj, adjncy, adjwgt, where, goff, gpart, gconn, k, dirty, bigd, huged);
 }
 
 template <int NT>
@@ -871,20 +896,20 @@ __device__ __forceinline__ void touch_neighbour(bool valid, int32_t u, int32_t w
     if (bg) big_l[bb + __popc(mb & lt)] = u;
 }
 
-__global__ void __launch_bounds__(256)
-apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
-                   int32_t *__restrict__ where, const int32_t *__restrict__ dest,
-                   const int32_t *__restrict__ vwgt, unsigned long long *__restrict__ pw,
-                   const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
-                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
-                   int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
-                   int32_t *__restrict__ big_l, int32_t *counts, int32_t k, int32_t *__restrict__ huge_mv,
-                   int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t huged)
+// One warp per move (warp, nwarps: this warp among those sharing the moves).
+__device__ __forceinline__ void apply_moves_rows(int64_t warp, int64_t nwarps, const int32_t *__restrict__ moves,
+                                                 int64_t nm, int32_t *__restrict__ where,
+                                                 const int32_t *__restrict__ dest, const int32_t *__restrict__ vwgt,
+                                                 unsigned long long *__restrict__ pw, const int32_t *__restrict__ xadj,
+                                                 const int32_t *__restrict__ adjncy,
+                                                 const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
+                                                 int32_t *__restrict__ gconn, int32_t *__restrict__ dirty,
+                                                 int32_t *__restrict__ small_l, int32_t *__restrict__ big_l,
+                                                 int32_t *counts, int32_t k, int32_t *__restrict__ huge_mv,
+                                                 int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t huged)
 {
-    const int64_t nm = (int64_t)*d_nmoves;
     const int lane = threadIdx.x & 31;
-    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < nm;
-         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
+    for (int64_t i = warp; i < nm; i += nwarps) {
         const int32_t v = moves[i];
         const int32_t p = where[v], d = dest[v];
         __syncwarp();
@@ -911,6 +936,21 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
         }
         if (lane == 0) where[v] = d;   // the move itself (every lane has read where[v])
     }
+}
+
+__global__ void __launch_bounds__(256)
+apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
+                   int32_t *__restrict__ where, const int32_t *__restrict__ dest,
+                   const int32_t *__restrict__ vwgt, unsigned long long *__restrict__ pw,
+                   const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
+                   int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
+                   int32_t *__restrict__ big_l, int32_t *counts, int32_t k, int32_t *__restrict__ huge_mv,
+                   int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t huged)
+{
+    apply_moves_rows((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, ((int64_t)gridDim.x * blockDim.x) >> 5,
+                     moves, (int64_t)*d_nmoves, where, dest, vwgt, pw, xadj, adjncy, adjwgt, goff, gconn, dirty,
+                     small_l, big_l, counts, k, huge_mv, d_nhuge, bigd, huged);
 }
 
 // Neighbours of the moved hubs (queued by apply_moves_kernel, planned by
@@ -1241,6 +1281,10 @@ rs_evict_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, co
 // waits on shared memory instead of L2.
 constexpr int COOKIE_SMEM_INTS = 50 * 1024;
 
+__device__ void cookie_cut_warp(int32_t k, const unsigned long long *__restrict__ pw,
+                                const int64_t *__restrict__ maxp, const int32_t *sp, int32_t np,
+                                int32_t *__restrict__ es, int32_t *__restrict__ ee);
+
 __global__ void __launch_bounds__(1024)
 cookie_cutter_kernel(int32_t k, const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
                      const int32_t *__restrict__ sp_g, const int32_t *__restrict__ d_np, int32_t *__restrict__ es,
@@ -1253,7 +1297,14 @@ cookie_cutter_kernel(int32_t k, const unsigned long long *__restrict__ pw, const
         for (int32_t i = threadIdx.x; i <= np; i += blockDim.x) sp_s[i] = sp_g[i];
     __syncthreads();
     if (threadIdx.x >= 32) return;
-    const int32_t *sp = staged ? sp_s : sp_g;
+    cookie_cut_warp(k, pw, maxp, staged ? sp_s : sp_g, np, es, ee);
+}
+
+// The walk itself, by one full warp.
+__device__ void cookie_cut_warp(int32_t k, const unsigned long long *__restrict__ pw,
+                                const int64_t *__restrict__ maxp, const int32_t *sp, int32_t np,
+                                int32_t *__restrict__ es, int32_t *__restrict__ ee)
+{
     const int lane = threadIdx.x & 31;
     int32_t st = 0;
     for (int32_t p0 = 0; p0 < k; p0 += 32) {
@@ -1504,6 +1555,8 @@ __device__ void ctl_prepare(RefineCtl *s)
     s->mode_passes[s->mode]++;
 }
 
+__device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2, long long nmoves, long long ncand);
+
 __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned,
                                 const int32_t *gain_total)
 {
@@ -1552,8 +1605,15 @@ ctl_end_kernel(RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle 
     if (threadIdx.x != 0) return;
     for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = s_max[w] > m ? s_max[w] : m;
     sc[S_EXCESS] = (unsigned long long)m;
-    const long long c1 = (long long)sc[S_C1], c2 = (long long)sc[S_C2];
-    const long long nmoves = (long long)sc[S_NMOVES], ncand = (long long)sc[S_NCAND];
+    const int cont = ctl_advance(s, m, (long long)sc[S_C1], (long long)sc[S_C2], (long long)sc[S_NMOVES],
+                                 (long long)sc[S_NCAND]);
+    if (graph) cudaGraphSetConditional(hloop, cont ? 1u : 0u);
+}
+
+// The control step of a pass end (one thread): new excess m, the cut-change
+// sums c1 and c2, the pass's moves and LP candidates.  Returns the loop condition.
+__device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2, long long nmoves, long long ncand)
+{
     s->excess = m;
     s->cut -= (c1 + c2) / 2;
     s->last_moves = nmoves;
@@ -1587,7 +1647,7 @@ ctl_end_kernel(RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle 
     if (s->passes >= HP_MAX_REFINE_PASSES) cont = 0;
     s->cont = cont;
     if (cont) ctl_prepare(s);
-    if (graph) cudaGraphSetConditional(hloop, cont ? 1u : 0u);
+    return cont;
 }
 
 // Start of a pass (one CTA of 1024 threads): clear the per-pass scalar slots,
@@ -1715,6 +1775,472 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
     HP_LAUNCH(c, save_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, P.ctl, n,
               g.where, B.best_where, k, B.pw, P.best_pw);
     return HP_OK;
+}
+
+// ---- small levels: every pass of the level in one CTA --------------------------------
+// A level with few vertices runs its whole pass loop inside one CTA of
+// SL_THREADS threads.  The phases are those of the multi-kernel pass, in the
+// same order and through the same device functions -- LP selection and
+// afterburner, weak or strong rebalance (candidates, stable radix sort, ranks,
+// selection or eviction and cookie cutter), simultaneous moves, gain-row
+// maintenance, the exact cut change, the control step and the best partition --
+// separated by __syncthreads instead of kernel boundaries.  Gain rows,
+// candidates and moves equal the multi-kernel pass's, so the level's result is
+// identical; what goes away is about fifteen launches per pass, which on small
+// levels cost more than the work.
+constexpr int SL_THREADS = 1024;
+constexpr int SL_WARPS = SL_THREADS / 32;
+constexpr int SL_SORT_INTS = 256 + SL_WARPS * 256;   // digit bases + per-warp digit counts
+
+struct SmallLevel {
+    int32_t n, k, finest, bigd, small_max, key_bits, learned_mlp;
+    float mlp_threshold;
+    const int32_t *xadj, *adjncy, *adjwgt, *vwgt;
+    int32_t *where;
+    const int32_t *goff;
+    int32_t *gpart, *gconn;
+    int32_t *dest, *pregain, *moves, *oldp, *dirty, *small_l, *big_l, *best_where;
+    int32_t *K, *V, *K2, *V2, *pre, *P, *sp;
+    int32_t *pstart, *pend, *und, *ev_end, *es, *ee;
+    int8_t *lock;
+    unsigned long long *pw, *best_pw;
+    const int64_t *opt, *maxp;
+    const float *mlp_params;
+    RefineCtl *ctl;
+};
+
+// Dynamic shared memory of the small-level kernel: the largest of the phases'
+// needs (sort tables; the staged prefix weights of the cookie cutter, at most
+// n + 1; the warps' dense gain-row accumulators).
+size_t small_level_smem(int32_t n, int32_t k)
+{
+    const size_t sort = sizeof(int32_t) * SL_SORT_INTS;
+    const size_t cookie = sizeof(int32_t) * ((size_t)n + 1);
+    const size_t rows = sizeof(int32_t) * SL_WARPS * ((size_t)k + (k + 31) / 32);
+    return std::max(sort, std::max(cookie, rows));
+}
+
+// Block-wide sum / max of a long long; every thread gets the result.
+__device__ __forceinline__ long long sl_sum64(long long v, long long *s_red)
+{
+    v = hp::warp_sum64(v);
+    __syncthreads();   // the previous reduction has been read
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    long long t = 0;
+#pragma unroll 8
+    for (int w = 0; w < SL_WARPS; w++) t += s_red[w];
+    return t;
+}
+
+__device__ __forceinline__ long long sl_max64(long long v, long long *s_red)
+{
+    v = hp::warp_max64(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    long long t = LLONG_MIN;
+#pragma unroll 8
+    for (int w = 0; w < SL_WARPS; w++) t = s_red[w] > t ? s_red[w] : t;
+    return t;
+}
+
+// Stable LSD radix sort of cnt (key, value) pairs by the low key_bits bits of
+// the keys (non-negative), one CTA of SL_THREADS.  Ping-pongs between (K, V)
+// and (K2, V2); returns true when the result is in (K2, V2).  Per 8-bit digit:
+// a histogram, the digit bases, then chunks of SL_THREADS items in order, each
+// item placed at its digit's base + the same digit's count in earlier warps of
+// the chunk + its rank inside its warp (__match_any_sync).  tab: SL_SORT_INTS.
+__device__ bool sl_sort_pairs(int32_t *K, int32_t *V, int32_t *K2, int32_t *V2, int32_t cnt, int key_bits,
+                              int32_t *tab, int32_t *s_scan)
+{
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    int32_t *base = tab, *wc = tab + 256;
+    bool flip = false;
+    for (int shift = 0; shift < key_bits; shift += 8) {
+        const int32_t *ks = flip ? K2 : K, *vs = flip ? V2 : V;
+        int32_t *kd = flip ? K : K2, *vd = flip ? V : V2;
+        if (tid < 256) base[tid] = 0;
+        __syncthreads();
+        for (int32_t i = tid; i < cnt; i += SL_THREADS) atomicAdd(&base[((unsigned)ks[i] >> shift) & 255u], 1);
+        __syncthreads();
+        const int h = tid < 256 ? base[tid] : 0;
+        int tot;
+        const int ex = hp::block_excl_scan<SL_THREADS>(h, &tot, s_scan);   // ends with a barrier
+        if (tid < 256) base[tid] = ex;
+        for (int32_t c0 = 0; c0 < cnt; c0 += SL_THREADS) {
+            const int32_t i = c0 + tid;
+            const bool valid = i < cnt;
+            const int32_t key = valid ? ks[i] : 0;
+            const unsigned d = valid ? (((unsigned)key >> shift) & 255u) : 256u + lane;
+            const unsigned peers = __match_any_sync(HP_FULL_MASK, d);
+            const int rank = __popc(peers & hp::lanemask_lt());
+            for (int q = tid; q < SL_WARPS * 256; q += SL_THREADS) wc[q] = 0;
+            __syncthreads();
+            if (valid && rank == 0) wc[wid * 256 + d] = __popc(peers);
+            __syncthreads();
+            if (valid) {
+                int32_t off = base[d] + rank;
+                for (int w = 0; w < wid; w++) off += wc[w * 256 + d];
+                kd[off] = key;
+                vd[off] = vs[i];
+            }
+            __syncthreads();
+            if (tid < 256) {   // the digit bases move past this chunk
+                int32_t c = 0;
+                for (int w = 0; w < SL_WARPS; w++) c += wc[w * 256 + tid];
+                base[tid] += c;
+            }
+            __syncthreads();
+        }
+        flip = !flip;
+    }
+    __syncthreads();
+    return flip;
+}
+
+__global__ void __launch_bounds__(SL_THREADS, 1)
+refine_small_kernel(SmallLevel a)
+{
+    extern __shared__ __align__(16) int32_t sl_dyn[];
+    __shared__ hp::MlpSmem s_mlp;
+    __shared__ int32_t s_scan[SL_THREADS / 32 + 2];
+    __shared__ long long s_red[SL_WARPS];
+    __shared__ int32_t s_lists[2];   // dirty rows queued this pass: short, long
+    __shared__ int32_t s_nu;         // undersized parts of a weak pass
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int32_t n = a.n, k = a.k;
+    RefineCtl *s = a.ctl;
+    if (a.learned_mlp) hp::mlp_load_smem(s_mlp, a.mlp_params);
+    __syncthreads();
+    // the control step ends the loop; the pass cap bounds it as well
+    for (int32_t guard = 0; guard <= HP_MAX_REFINE_PASSES; guard++) {
+        if (!*(volatile const int32_t *)&s->cont) break;   // written by thread 0 before a barrier
+        const int mode = *(volatile const int32_t *)&s->mode;
+        if (tid < 2) s_lists[tid] = 0;
+        long long ncand = 0;
+        int32_t nmoves = 0;
+        if (mode == 0) {
+            // ---- LP selection (plain or learned), as lp_select[_learned]_kernel
+            const bool lrn = a.learned_mlp && *(volatile const int32_t *)&s->learned_pass;
+            int32_t my_cand = 0;
+            for (int32_t b0 = 0; b0 < n; b0 += SL_THREADS) {
+                const int32_t v = b0 + tid;
+                const bool in = v < n;
+                int32_t p = 0, o = 0, len = 0;
+                if (in) {
+                    p = a.where[v];
+                    o = a.goff[v];
+                    len = a.goff[v + 1] - o;
+                }
+                const RowBest rb = row_best(a.gpart, a.gconn, o, len, p);
+                int cand = 0;
+                int32_t g = NEG, d = p;
+                float f[HP_MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (in && rb.b >= 0) {
+                    const int64_t thr = a.finest ? rb.pc / 4 : (3 * rb.pc) / 4;
+                    if ((rb.bc >= rb.pc || (rb.pc - rb.bc) < thr) && !a.lock[v]) {
+                        g = (int32_t)(rb.bc - rb.pc);
+                        d = rb.b;
+                        cand = 1;
+                        if (lrn)
+                            hp::mlp_features(rb.pc, rb.bc, rb.wd, rb.np, a.xadj[v + 1] - a.xadj[v],
+                                             a.maxp[d] - (int64_t)a.pw[d], a.opt[d], a.maxp[p] - (int64_t)a.pw[p],
+                                             a.opt[p], a.finest, f);
+                    }
+                }
+                if (lrn) {
+                    const float logit = hp::mlp_warp_logit(s_mlp, f);
+                    if (cand && logit < a.mlp_threshold) { cand = 0; g = NEG; d = p; }
+                }
+                if (in) {
+                    a.pregain[v] = g;
+                    a.dest[v] = d;
+                }
+                my_cand += cand;
+            }
+            ncand = sl_sum64(my_cand, s_red);   // (barrier: every selection is visible)
+            if (ncand > 0) {
+                // ---- afterburner: every candidate re-scored against the
+                // higher-priority neighbours; locks and moves (in vertex order)
+                int32_t run = 0;
+                for (int32_t b0 = 0; b0 < n; b0 += SL_THREADS) {
+                    const int32_t v = b0 + tid;
+                    const bool in = v < n;
+                    const int32_t g = in ? a.pregain[v] : NEG;
+                    const bool act = g != NEG;
+                    const int32_t ro = act ? a.xadj[v] : 0, rl = act ? a.xadj[v + 1] - ro : 0;
+                    const int32_t pp = act ? a.where[v] : 0, bb = act ? a.dest[v] : 0;
+                    long long ch = 0;
+                    const bool coop = rl > 32;
+                    if (act && !coop)
+                        for (int32_t j = ro; j < ro + rl; j++)
+                            ch += ab_change(v, g, pp, bb, a.adjncy[j], a.adjwgt[j], a.pregain, a.dest, a.where);
+                    unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
+                    while (cm) {
+                        const int src = __ffs(cm) - 1;
+                        cm &= cm - 1;
+                        const int32_t sv = __shfl_sync(HP_FULL_MASK, v, src), sg = __shfl_sync(HP_FULL_MASK, g, src);
+                        const int32_t sp_ = __shfl_sync(HP_FULL_MASK, pp, src), sb = __shfl_sync(HP_FULL_MASK, bb, src);
+                        const int32_t so = __shfl_sync(HP_FULL_MASK, ro, src), sl = __shfl_sync(HP_FULL_MASK, rl, src);
+                        long long c = 0;
+                        for (int32_t j = lane; j < sl; j += 32)
+                            c += ab_change(sv, sg, sp_, sb, a.adjncy[so + j], a.adjwgt[so + j], a.pregain, a.dest,
+                                           a.where);
+                        c = hp::warp_sum64(c);
+                        if (lane == src) ch = c;
+                    }
+                    const int sel = act && ((long long)g + ch >= 0);
+                    if (in) a.lock[v] = (int8_t)sel;
+                    int tot;
+                    const int ex = hp::block_excl_scan<SL_THREADS>(sel, &tot, s_scan);
+                    if (sel) a.moves[run + ex] = v;
+                    run += tot;
+                }
+                nmoves = run;
+            }
+        } else {
+            // ---- rebalance, as rb_candidates / sort / rb_rank / rw_select or
+            // evict_end / rs_evict / cookie_cutter / rs_assign
+            const bool strong = mode == 2;
+            if (!strong) undersized_block(k, a.pw, a.maxp, a.und, &s_nu, s_scan);
+            for (int32_t p = tid; p < k; p += SL_THREADS) {
+                a.pstart[p] = -1;
+                a.pend[p] = -1;
+            }
+            __syncthreads();
+            const int32_t nu = s_nu;
+            int32_t cnt = 0;
+            for (int32_t b0 = 0; b0 < n; b0 += SL_THREADS) {
+                const int32_t v = b0 + tid;
+                const bool in = v < n;
+                int32_t p = 0;
+                bool cand = false;
+                if (in) {
+                    p = a.where[v];
+                    const int64_t pwp = (int64_t)a.pw[p];
+                    cand = strong ? (pwp > a.maxp[p] && (int64_t)a.vwgt[v] < 2 * (pwp - a.opt[p]))
+                                  : (pwp > a.maxp[p] && 2 * (int64_t)a.vwgt[v] < 3 * (pwp - a.opt[p]));
+                }
+                const int32_t o = cand ? a.goff[v] : 0, len = cand ? a.goff[v + 1] - o : 0;
+                int32_t d = p, kk = -1;
+                if (!strong) {
+                    int64_t pc = 0, bc = 0;
+                    int32_t b = -1;
+                    const bool coop = cand && len > RB_COOP;
+                    if (cand && !coop)
+                        for (int32_t j = o; j < o + len; j++) {
+                            const int32_t q = a.gpart[j];
+                            if (q < 0) break;
+                            const int32_t cq = a.gconn[j];
+                            if (q == p) pc = cq;
+                            if ((int64_t)a.pw[q] < a.maxp[q] && cq > bc) { bc = cq; b = q; }
+                        }
+                    unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
+                    while (cm) {
+                        const int src = __ffs(cm) - 1;
+                        cm &= cm - 1;
+                        const int32_t so = __shfl_sync(HP_FULL_MASK, o, src), sl = __shfl_sync(HP_FULL_MASK, len, src);
+                        const int32_t sp_ = __shfl_sync(HP_FULL_MASK, p, src);
+                        int32_t lpc = 0, lbc = 0, lb = -1;
+                        for (int32_t j = lane; j < sl; j += 32) {
+                            const int32_t q = a.gpart[so + j];
+                            if (q < 0) break;
+                            const int32_t cq = a.gconn[so + j];
+                            if (q == sp_) lpc = cq;
+                            if ((int64_t)a.pw[q] < a.maxp[q] && cq > lbc) { lbc = cq; lb = q; }
+                        }
+                        lpc = hp::warp_sum(lpc);
+#pragma unroll
+                        for (int sh = 16; sh > 0; sh >>= 1) {
+                            const int32_t ob = __shfl_xor_sync(HP_FULL_MASK, lb, sh);
+                            const int32_t oc = __shfl_xor_sync(HP_FULL_MASK, lbc, sh);
+                            if (ob >= 0 && (lb < 0 || oc > lbc || (oc == lbc && ob < lb))) { lb = ob; lbc = oc; }
+                        }
+                        if (lane == src) { pc = lpc; bc = lbc; b = lb; }
+                    }
+                    if (cand) {
+                        int64_t g = 0;
+                        bool ok = true;
+                        if (b >= 0) g = bc - pc;
+                        else if (nu == 0) ok = false;
+                        else { b = a.und[v % nu]; g = -pc; }
+                        if (ok) { d = b; kk = p * 64 + hp::gain_bucket((int32_t)g, a.vwgt[v]); }
+                    }
+                } else if (cand) {
+                    const int32_t pc = row_conn(a.gpart + o, a.gconn + o, len, p, k);
+                    kk = p * 64 + hp::gain_bucket(-pc, a.vwgt[v]);
+                }
+                if (in) a.dest[v] = d;
+                int tot;
+                const int ex = hp::block_excl_scan<SL_THREADS>(kk >= 0 ? 1 : 0, &tot, s_scan);
+                if (kk >= 0) {
+                    a.K[cnt + ex] = kk;
+                    a.V[cnt + ex] = v;
+                }
+                cnt += tot;
+            }
+            const bool flip = sl_sort_pairs(a.K, a.V, a.K2, a.V2, cnt, a.key_bits, sl_dyn, s_scan);
+            const int32_t *Ks = flip ? a.K2 : a.K, *Vs = flip ? a.V2 : a.V;
+            // prefix weights in sorted order and the part bounds
+            int32_t run = 0;
+            for (int32_t b0 = 0; b0 < cnt; b0 += SL_THREADS) {
+                const int32_t i = b0 + tid;
+                const bool valid = i < cnt;
+                const int32_t w = valid ? a.vwgt[Vs[i]] : 0;
+                int tot;
+                const int ex = hp::block_excl_scan<SL_THREADS>(w, &tot, s_scan);
+                if (valid) {
+                    a.pre[i] = run + ex;
+                    const int32_t p = Ks[i] >> 6;
+                    if (i == 0 || (Ks[i - 1] >> 6) != p) a.pstart[p] = i;
+                    if (i == cnt - 1 || (Ks[i + 1] >> 6) != p) a.pend[p] = i + 1;
+                }
+                run += tot;
+            }
+            if (tid == 0) a.pre[cnt] = run;
+            __syncthreads();
+            if (!strong) {
+                int32_t mv = 0;
+                for (int32_t b0 = 0; b0 < cnt; b0 += SL_THREADS) {
+                    const int32_t i = b0 + tid;
+                    int sel = 0;
+                    if (i < cnt) {
+                        const int32_t p = Ks[i] >> 6;
+                        const int64_t before = (int64_t)a.pre[i] - a.pre[a.pstart[p]];
+                        sel = before < (int64_t)a.pw[p] - a.maxp[p];
+                    }
+                    int tot;
+                    const int ex = hp::block_excl_scan<SL_THREADS>(sel, &tot, s_scan);
+                    if (sel) a.moves[mv + ex] = Vs[i];
+                    mv += tot;
+                }
+                nmoves = mv;
+            } else {
+                for (int32_t p = tid; p < k; p += SL_THREADS) {   // evict_end_kernel
+                    const int32_t st = a.pstart[p], en = a.pend[p];
+                    if (st < 0) { a.ev_end[p] = -1; continue; }
+                    const int64_t need = (int64_t)a.pw[p] - a.maxp[p];
+                    int32_t lo = st, hi = en;
+                    while (lo + 1 < hi) {
+                        const int32_t mid = (lo + hi) / 2;
+                        if ((int64_t)a.pre[mid] - a.pre[st] >= need) hi = mid; else lo = mid;
+                    }
+                    a.ev_end[p] = hi;
+                }
+                __syncthreads();
+                int32_t np = 0, wrun = 0;   // rs_evict_kernel
+                for (int32_t b0 = 0; b0 < cnt; b0 += SL_THREADS) {
+                    const int32_t i = b0 + tid;
+                    const int f = i < cnt && i < a.ev_end[Ks[i] >> 6];
+                    const int32_t w = f ? a.vwgt[Vs[i]] : 0;
+                    int tc, tw;
+                    const int ec = hp::block_excl_scan<SL_THREADS>(f, &tc, s_scan);
+                    const int ew = hp::block_excl_scan<SL_THREADS>(w, &tw, s_scan);
+                    if (f) {
+                        a.P[np + ec] = i;
+                        a.sp[np + ec] = wrun + ew;
+                    }
+                    np += tc;
+                    wrun += tw;
+                }
+                // cookie cutter on the prefix weights staged in shared memory
+                for (int32_t i = tid; i < np; i += SL_THREADS) sl_dyn[i] = a.sp[i];
+                if (tid == 0) {
+                    sl_dyn[np] = wrun;
+                    a.sp[np] = wrun;
+                }
+                __syncthreads();
+                if (wid == 0) cookie_cut_warp(k, a.pw, a.maxp, sl_dyn, np, a.es, a.ee);
+                __syncthreads();
+                int32_t mv = 0;   // rs_assign_kernel
+                for (int32_t b0 = 0; b0 < np; b0 += SL_THREADS) {
+                    const int32_t j = b0 + tid;
+                    int sel = 0;
+                    int32_t v = 0;
+                    if (j < np) {
+                        int32_t lo = 0, hi = k - 1;   // last part with es[p] <= j
+                        while (lo < hi) {
+                            const int32_t mid = (lo + hi + 1) / 2;
+                            if (a.es[mid] <= j) lo = mid; else hi = mid - 1;
+                        }
+                        v = Vs[a.P[j]];
+                        if (j < a.ee[lo] && lo != a.where[v]) {
+                            a.dest[v] = lo;
+                            sel = 1;
+                        }
+                    }
+                    int tot;
+                    const int ex = hp::block_excl_scan<SL_THREADS>(sel, &tot, s_scan);
+                    if (sel) a.moves[mv + ex] = v;
+                    mv += tot;
+                }
+                nmoves = mv;
+            }
+        }
+        __syncthreads();
+        // ---- apply: cut change before, moves, gain-row maintenance, cut change after
+        long long acc = 0;
+        for (int32_t i = tid; i < nmoves; i += SL_THREADS) {
+            const int32_t v = a.moves[i];
+            const int32_t o = a.goff[v], len = a.goff[v + 1] - o;
+            const int32_t from = a.where[v], to = a.dest[v];
+            a.oldp[i] = from;
+            acc += (long long)row_conn(a.gpart + o, a.gconn + o, len, to, k) -
+                   row_conn(a.gpart + o, a.gconn + o, len, from, k);
+        }
+        const long long c1 = sl_sum64(acc, s_red);
+        apply_moves_rows(wid, SL_WARPS, a.moves, nmoves, a.where, a.dest, a.vwgt, a.pw, a.xadj, a.adjncy, a.adjwgt,
+                         a.goff, a.gconn, a.dirty, a.small_l, a.big_l, s_lists, k, nullptr, nullptr, a.bigd, INT_MAX);
+        __syncthreads();
+        const int32_t ns = s_lists[0], nb = s_lists[1];
+        if (ns > 0) {
+            if (a.small_max <= 8)
+                gain_seg_rows<8>(wid, SL_WARPS, a.small_l, ns, a.xadj, a.adjncy, a.adjwgt, a.where, a.goff, a.gpart,
+                                 a.gconn, k, a.dirty);
+            else if (a.small_max <= 16)
+                gain_seg_rows<16>(wid, SL_WARPS, a.small_l, ns, a.xadj, a.adjncy, a.adjwgt, a.where, a.goff, a.gpart,
+                                  a.gconn, k, a.dirty);
+            else
+                gain_seg_rows<32>(wid, SL_WARPS, a.small_l, ns, a.xadj, a.adjncy, a.adjwgt, a.where, a.goff, a.gpart,
+                                  a.gconn, k, a.dirty);
+        }
+        if (nb > 0) {
+            const int nw = (k + 31) >> 5;
+            int32_t *dw = sl_dyn + (size_t)wid * (k + nw);
+            unsigned *bm = (unsigned *)(dw + k);
+            for (int i = lane; i < k; i += 32) dw[i] = 0;
+            for (int i = lane; i < nw; i += 32) bm[i] = 0u;
+            __syncwarp();
+            gain_bigwarp_rows(wid, SL_WARPS, dw, bm, a.big_l, nb, a.xadj, a.adjncy, a.adjwgt, a.where, a.goff,
+                              a.gpart, a.gconn, k, a.dirty, a.bigd, INT_MAX);
+        }
+        __syncthreads();
+        acc = 0;
+        for (int32_t i = tid; i < nmoves; i += SL_THREADS) {
+            const int32_t v = a.moves[i];
+            const int32_t o = a.goff[v], len = a.goff[v + 1] - o;
+            const int32_t from = a.oldp[i], to = a.where[v];
+            acc += (long long)row_conn(a.gpart + o, a.gconn + o, len, to, k) -
+                   row_conn(a.gpart + o, a.gconn + o, len, from, k);
+        }
+        const long long c2 = sl_sum64(acc, s_red);
+        long long m = LLONG_MIN;
+        for (int32_t p = tid; p < k; p += SL_THREADS) {
+            const long long e = (long long)a.pw[p] - a.maxp[p];
+            m = e > m ? e : m;
+        }
+        m = sl_max64(m, s_red);
+        if (tid == 0) ctl_advance(s, m, c1, c2, nmoves, ncand);
+        __syncthreads();
+        if (*(volatile const int32_t *)&s->take) {
+            for (int32_t i = tid; i < n; i += SL_THREADS) a.best_where[i] = a.where[i];
+            for (int32_t i = tid; i < k; i += SL_THREADS) a.best_pw[i] = a.pw[i];
+        }
+        __syncthreads();
+    }
+    if (!*(volatile const int32_t *)&s->best_current)
+        for (int32_t i = tid; i < n; i += SL_THREADS) a.where[i] = a.best_where[i];
 }
 
 // Graph-capture helper: records the launches of body() into `graph`.  The capture
@@ -1936,7 +2462,58 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     const bool use_graph = graph_loop(c);
     RefineCtl h{};
-    if (use_graph) {
+    // small levels: the whole pass loop in one CTA (same rule, same result)
+    const int32_t small_n = c->tune.small_level_n;
+    const bool small_level = use_graph && n <= small_n && k <= HP_TUNE_WARP_DENSE_K_MAX &&
+                             g.m <= 16 * (int64_t)small_n;
+    if (small_level) {
+        SmallLevel a{};
+        a.n = n;
+        a.k = k;
+        a.finest = finest ? 1 : 0;
+        a.bigd = c->tune.gain_thread_deg;
+        a.small_max = B.small_max;
+        a.key_bits = key_bits_for(k);
+        a.learned_mlp = learned ? 1 : 0;
+        a.mlp_threshold = c->mlp_threshold;
+        a.xadj = g.xadj;
+        a.adjncy = g.adjncy;
+        a.adjwgt = g.adjwgt;
+        a.vwgt = g.vwgt;
+        a.where = g.where;
+        a.goff = B.goff;
+        a.gpart = B.gpart;
+        a.gconn = B.gconn;
+        a.dest = B.dest;
+        a.pregain = B.pregain;
+        a.moves = B.moves;
+        a.oldp = B.oldp;
+        a.dirty = B.dirty;
+        a.small_l = B.small_l;
+        a.big_l = B.big_l;
+        a.best_where = B.best_where;
+        a.K = B.K;
+        a.V = B.V;
+        a.K2 = B.K2;
+        a.V2 = B.V2;
+        a.pre = B.pre;
+        a.P = B.P;
+        a.sp = B.sp;
+        a.pstart = B.pstart;
+        a.pend = B.pend;
+        a.und = B.und;
+        a.ev_end = B.ev_end;
+        a.es = B.es;
+        a.ee = B.ee;
+        a.lock = B.lock;
+        a.pw = B.pw;
+        a.best_pw = best_pw;
+        a.opt = B.opt;
+        a.maxp = B.maxp;
+        a.mlp_params = c->mlp_params;
+        a.ctl = ctl;
+        HP_LAUNCH(c, refine_small_kernel, 1, SL_THREADS, small_level_smem(n, k), a);
+    } else if (use_graph) {
         ll->graph = true;
         HP_TRY(run_passes_graph(c, g, B, P, learned, &ll->n_common, ll->n_mode, keep));
         HP_LAUNCH(c, restore_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, ctl, n,
@@ -1976,6 +2553,8 @@ int hp_refine_init()
                                  (int)(sizeof(int32_t) * COOKIE_SMEM_INTS)));
     const int bytes = HP_MAX_PARTS * 4 + (HP_MAX_PARTS / 32) * 4;
     HP_CUDA(cudaFuncSetAttribute(gain_dense_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    HP_CUDA(cudaFuncSetAttribute(refine_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)small_level_smem(HP_TUNE_SMALL_LEVEL_MAX, HP_TUNE_WARP_DENSE_K_MAX)));
     return HP_OK;
 }
 

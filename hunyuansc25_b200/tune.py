@@ -55,6 +55,7 @@ SPACE = {
     "warp_dense_k": [0, 256, 512, 1024],
     "grid_ctas_per_sm": [2, 4, 8, 12, 16],
     "dense_sparse_ratio": [1, 2, 4, 8, 32],
+    "small_level_n": [0, 2048, 4096, 8192, 16384, 32768],
 }
 
 

@@ -162,7 +162,10 @@ typedef struct hp_tuning {
     int32_t grid_ctas_per_sm;    /* grid-stride kernels: CTAs per SM              [1, 32]       8 */
     int32_t dense_sparse_ratio;  /* dense contraction rows: the two-level bitmap when
                                     entries * ratio < bitmap words                [1, 4096]     4 */
-    int32_t reserved[6];         /* zero */
+    int32_t small_level_n;       /* refinement: levels of at most this many vertices
+                                    (and 16x as many adjacency entries, nparts <= 1024)
+                                    run all their passes in one CTA; 0 = never    [0, 32768]    4096 */
+    int32_t reserved[5];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);
