@@ -228,6 +228,35 @@ __device__ __forceinline__ void warp_topk(const TopList &t, int32_t (&out)[TOPK]
     }
 }
 
+// One thread's share of a row (entries j0, j0 + stride, ... below e) offered to
+// its top list: four entries at a time, so that the row loads and then the
+// eligibility gathers of the four are in flight together.  The list keeps the
+// best TOPK by hp::better whatever the order of the offers.
+__device__ __forceinline__ void scan_row_topk(TopList &t, int32_t v, int32_t j0, int32_t e, int32_t stride,
+                                              const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt,
+                                              const int32_t *__restrict__ elig, int32_t wv, uint64_t lkey,
+                                              int64_t maxvwgt)
+{
+    for (int32_t j = j0; j < e; j += 4 * stride) {
+        int32_t u[4], w[4], eu[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int32_t jj = j + q * stride;
+            const bool in = jj < e;
+            u[q] = in ? adjncy[jj] : v;
+            w[q] = in ? adjwgt[jj] : 0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) eu[q] = u[q] != v ? elig[u[q]] : INT_MAX;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (eu[q] == INT_MAX) continue;                     // matched, or no entry
+            if ((int64_t)wv + eu[q] > maxvwgt) continue;        // weight cap
+            t.offer(lkey, v, u[q], w[q]);
+        }
+    }
+}
+
 // Later rounds: the proposal from the cache, or -2 when the row must be rescanned.
 __device__ __forceinline__ int32_t cached_proposal(const int32_t *__restrict__ cand, int32_t v,
                                                   const int32_t *__restrict__ elig)
@@ -263,14 +292,7 @@ pref_big_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restrict
         const int32_t wv = vwgt[v];
         TopList t;
         t.init();
-        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32) {
-            const int32_t u = adjncy[j];
-            if (u == v) continue;
-            const int32_t eu = elig[u];
-            if (eu == INT_MAX) continue;                     // matched
-            if ((int64_t)wv + eu > maxvwgt) continue;        // weight cap
-            t.offer(lkey, v, u, adjwgt[j]);
-        }
+        scan_row_topk(t, v, xadj[v] + lane, xadj[v + 1], 32, adjncy, adjwgt, elig, wv, lkey, maxvwgt);
         int32_t top[TOPK];
         warp_topk(t, top);
         if (lane < TOPK) cand[(int64_t)v * TOPK + lane] = top[lane];
@@ -301,14 +323,7 @@ pref_huge_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restric
         const int32_t wv = vwgt[v];
         TopList t;
         t.init();
-        for (int32_t j = xadj[v] + threadIdx.x; j < xadj[v + 1]; j += blockDim.x) {
-            const int32_t u = adjncy[j];
-            if (u == v) continue;
-            const int32_t eu = elig[u];
-            if (eu == INT_MAX) continue;
-            if ((int64_t)wv + eu > maxvwgt) continue;
-            t.offer(lkey, v, u, adjwgt[j]);
-        }
+        scan_row_topk(t, v, xadj[v] + threadIdx.x, xadj[v + 1], blockDim.x, adjncy, adjwgt, elig, wv, lkey, maxvwgt);
         // per warp: its TOPK best, with their weights and keys (taken from the lists)
         {
             int32_t top[TOPK];
@@ -1015,20 +1030,21 @@ contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__re
     }
 }
 
-// CTA class: 256 threads per row.
-// CTA class: one CTA of NT threads per row of at most CAP entries.  Two
-// instances: <256, 4096> for the rows of 257..4096 entries (list 1) and
-// <1024, 12288> for the rows of 4097..12288 entries taken from list 2, whose
-// longer rows stay with the dense kernel; 2 CAP packed entries plus NT/32
-// digit histograms fit the 227 KB of shared memory of one CTA.
+// CTA class: one CTA of NT threads per row of min_len+1 .. CAP entries.  Three
+// instances: <256, 1024> and <256, 4096> split list 1 (rows up to 1024 entries
+// take 24 KB of shared memory, so 8 CTAs share an SM instead of 3), and
+// <1024, 12288> takes the rows of list 2 up to 12288 entries, whose longer
+// rows stay with the dense kernel; 2 CAP packed entries plus NT/32 digit
+// histograms fit the 227 KB of shared memory of one CTA.
 constexpr int CROW_THREADS = 256;
 constexpr int XROW_THREADS = 1024, XROW_MAX = 12288;
+constexpr int MROW_MAX = 1024;   // the smaller CTA instance of list 1
 
 template <int NT, int CAP>
 __global__ void __launch_bounds__(NT)
 contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, ContractSrc src,
                           const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
-                          int32_t *__restrict__ ucnt, int kbits)
+                          int32_t *__restrict__ ucnt, int kbits, int32_t min_len)
 {
     extern __shared__ unsigned long long dsm[];
     unsigned long long *A = dsm, *B = dsm + CAP;
@@ -1040,7 +1056,7 @@ contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__res
         RowInfo r;
         int32_t len;
         src.row(c, r, len);
-        if (len > CAP) continue;   // the dense kernel's row
+        if (len > CAP || len <= min_len) continue;   // another instance's row
         const int N = group_gather_row<NT>(src, c, r, len, A, s_scan);
         group_radix_sort<NT>(A, B, len, kbits, hist, s_scan);
         const int32_t off = toff[c];
@@ -1275,15 +1291,22 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
             HP_LAUNCH(c, contract_warp_radix_kernel,
                       (unsigned)std::min<int64_t>((h.cnt[0] + WROW_WARPS - 1) / WROW_WARPS, c->sm_count * 6),
                       32 * WROW_WARPS, 0, lists, &counts[0], src, toff, tk, tw, ucnt, kbits);
-        if (h.cnt[1] > 0)
-            HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
-                      (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 3), CROW_THREADS,
-                      (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits);
+        if (h.cnt[1] > 0) {
+            HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>),
+                      (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 8), CROW_THREADS,
+                      (cta_radix_smem<CROW_THREADS, MROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits,
+                      0);
+            if (c->tune.contract_cta_row > MROW_MAX)
+                HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
+                          (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 3), CROW_THREADS,
+                          (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt,
+                          kbits, MROW_MAX);
+        }
         if (h.cnt[2] > 0)
             HP_LAUNCH(c, (contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>),
                       (unsigned)std::min<int64_t>(h.cnt[2], c->sm_count), XROW_THREADS,
                       (cta_radix_smem<XROW_THREADS, XROW_MAX>()), lists + 2 * (int64_t)cn, &counts[2], src, toff, tk,
-                      tw, ucnt, kbits);
+                      tw, ucnt, kbits, 0);
         if (h.maxlen > XROW_MAX) {
             // slab per CTA: cn ints + cn/32 + cn/1024 words; bounded to ~512 MB
             const int64_t nw = ((int64_t)cn + 31) / 32, nw2 = ((int64_t)cn + 1023) / 1024;
@@ -1336,6 +1359,9 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
 
 int hp_coarsen_init()
 {
+    HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_radix_smem<CROW_THREADS, MROW_MAX>()));
     HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_radix_smem<CROW_THREADS, CROW_MAX>()));

@@ -257,10 +257,21 @@ __device__ __forceinline__ void gain_bigwarp_rows(int64_t warp, int64_t nwarps, 
         const int32_t b = xadj[v], e = xadj[v + 1];
         if (e - b <= bigd || e - b > huged) continue;
         if (dirty && lane == 0) dirty[v] = 0;
-        for (int32_t j = b + lane; j < e; j += 32) {
-            const int32_t q = where[adjncy[j]];
-            atomicAdd(&dw[q], adjwgt[j]);
-            atomicOr(&bm[q >> 5], 1u << (q & 31));
+        for (int32_t j = b + lane; j < e; j += 128) {   // four chunks in flight
+            int32_t u[4], w[4];
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int32_t jj = j + 32 * t;
+                u[t] = jj < e ? adjncy[jj] : -1;
+                w[t] = jj < e ? adjwgt[jj] : 0;
+            }
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                if (u[t] < 0) continue;
+                const int32_t q = where[u[t]];
+                atomicAdd(&dw[q], w[t]);
+                atomicOr(&bm[q >> 5], 1u << (q & 31));
+            }
         }
         __syncwarp();
         const int32_t o = goff[v], cap = goff[v + 1] - o;
@@ -679,6 +690,44 @@ __device__ __forceinline__ long long ab_change(int32_t v, int32_t g, int32_t p, 
     return ch;
 }
 
+// Sum of ab_change over the entries j0, j0 + stride, ... below e of v's row,
+// four at a time: the row loads, then the neighbour gathers of the four, are in
+// flight together.
+__device__ __forceinline__ long long ab_row_sum(int32_t v, int32_t g, int32_t p, int32_t b, int32_t j0, int32_t e,
+                                                int32_t stride, const int32_t *__restrict__ adjncy,
+                                                const int32_t *__restrict__ adjwgt, const int32_t *pregain,
+                                                const int32_t *dest, const int32_t *where)
+{
+    long long ch = 0;
+    for (int32_t j = j0; j < e; j += 4 * stride) {
+        int32_t u[4], w[4], gu[4], du[4], wu[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int32_t jj = j + q * stride;
+            const bool in = jj < e;
+            u[q] = in ? adjncy[jj] : v;
+            w[q] = in ? adjwgt[jj] : 0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            gu[q] = pregain[u[q]];
+            du[q] = dest[u[q]];
+            wu[q] = where[u[q]];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (u[q] == v) continue;   // no entry (rows have no self loops)
+            if (gu[q] > g || (gu[q] == g && u[q] < v)) {
+                if (du[q] == p) ch -= w[q];
+                else if (du[q] == b) ch += w[q];
+                if (wu[q] == p) ch += w[q];
+                else if (wu[q] == b) ch -= w[q];
+            }
+        }
+    }
+    return ch;
+}
+
 __global__ void __launch_bounds__(256)
 afterburner_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                          const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
@@ -722,9 +771,7 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
         int8_t sel = 0;
         if (g != NEG) {
             const int32_t p = where[v], b = dest[v];
-            long long ch = 0;
-            for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32)
-                ch += ab_change(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where);
+            long long ch = ab_row_sum(v, g, p, b, xadj[v] + lane, xadj[v + 1], 32, adjncy, adjwgt, pregain, dest, where);
             ch = hp::warp_sum64(ch);
             sel = ((long long)g + ch >= 0);
         }
@@ -860,9 +907,10 @@ c_delta_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nm
 // not depend on its own part: only neighbours' rows change.  Dense neighbour
 // rows (deg >= k) take the change in place; a sparse neighbour is queued once
 // (atomicExch on its dirty flag) on the small or big rebuild list.
-__device__ __forceinline__ void touch_neighbour(bool valid, int32_t u, int32_t w, int32_t p, int32_t d,
-                                                const int32_t *__restrict__ xadj,
-                                                const int32_t *__restrict__ goff,
+// o and cap: the neighbour's gain-row offset and capacity (goff[u], goff[u+1] - o),
+// loaded by the caller.
+__device__ __forceinline__ void touch_neighbour(bool valid, int32_t u, int32_t w, int32_t o, int32_t cap, int32_t p,
+                                                int32_t d, const int32_t *__restrict__ xadj,
                                                 int32_t *__restrict__ gconn, int32_t *__restrict__ dirty,
                                                 int32_t *__restrict__ small_l, int32_t *__restrict__ big_l,
                                                 int32_t *counts, int32_t k, int32_t bigd)
@@ -871,8 +919,7 @@ __device__ __forceinline__ void touch_neighbour(bool valid, int32_t u, int32_t w
     // take one counter atomic per warp and list (ballot ranks inside the warp)
     bool sm = false, bg = false;
     if (valid) {
-        const int32_t o = goff[u];
-        if (goff[u + 1] - o == k) {
+        if (cap == k) {
             atomicAdd(&gconn[o + p], -w);
             atomicAdd(&gconn[o + d], w);
         } else if (__ldcg(&dirty[u]) == 0 && atomicExch(&dirty[u], 1) == 0) {
@@ -928,11 +975,26 @@ __device__ __forceinline__ void apply_moves_rows(int64_t warp, int64_t nwarps, c
             }
             continue;
         }
-        for (int32_t j0 = b; j0 < e; j0 += 32) {
-            const int32_t j = j0 + lane;
-            const bool valid = j < e;
-            touch_neighbour(valid, valid ? adjncy[j] : 0, valid ? adjwgt[j] : 0, p, d, xadj, goff, gconn, dirty,
-                            small_l, big_l, counts, k, bigd);
+        // four chunks of 32 entries at a time: row loads, then the neighbours'
+        // gain-row offsets, are in flight together
+        for (int32_t j0 = b; j0 < e; j0 += 128) {
+            int32_t u[4], w[4], o[4], cap[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int32_t j = j0 + 32 * q + lane;
+                const bool valid = j < e;
+                u[q] = valid ? adjncy[j] : -1;
+                w[q] = valid ? adjwgt[j] : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                o[q] = u[q] >= 0 ? goff[u[q]] : 0;
+                cap[q] = u[q] >= 0 ? goff[u[q] + 1] - o[q] : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                touch_neighbour(u[q] >= 0, u[q], w[q], o[q], cap[q], p, d, xadj, gconn, dirty, small_l, big_l, counts,
+                                k, bigd);
         }
         if (lane == 0) where[v] = d;   // the move itself (every lane has read where[v])
     }
@@ -973,8 +1035,10 @@ apply_moves_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__res
         const int32_t e = xadj[v + 1];
         const int32_t j = xadj[v] + (int32_t)(gc - plan_off[jp]) * HUB_CHUNK + threadIdx.x;
         const bool valid = j < e;
-        touch_neighbour(valid, valid ? adjncy[j] : 0, valid ? adjwgt[j] : 0, p, d, xadj, goff, gconn, dirty, small_l,
-                        big_l, counts, k, bigd);
+        const int32_t u = valid ? adjncy[j] : 0;
+        const int32_t o = valid ? goff[u] : 0, cap = valid ? goff[u + 1] - o : 0;
+        touch_neighbour(valid, u, valid ? adjwgt[j] : 0, o, cap, p, d, xadj, gconn, dirty, small_l, big_l, counts, k,
+                        bigd);
     }
 }
 
@@ -1983,10 +2047,8 @@ refine_small_kernel(SmallLevel a)
                         const int32_t sv = __shfl_sync(HP_FULL_MASK, v, src), sg = __shfl_sync(HP_FULL_MASK, g, src);
                         const int32_t sp_ = __shfl_sync(HP_FULL_MASK, pp, src), sb = __shfl_sync(HP_FULL_MASK, bb, src);
                         const int32_t so = __shfl_sync(HP_FULL_MASK, ro, src), sl = __shfl_sync(HP_FULL_MASK, rl, src);
-                        long long c = 0;
-                        for (int32_t j = lane; j < sl; j += 32)
-                            c += ab_change(sv, sg, sp_, sb, a.adjncy[so + j], a.adjwgt[so + j], a.pregain, a.dest,
-                                           a.where);
+                        long long c = ab_row_sum(sv, sg, sp_, sb, so + lane, so + sl, 32, a.adjncy, a.adjwgt,
+                                                 a.pregain, a.dest, a.where);
                         c = hp::warp_sum64(c);
                         if (lane == src) ch = c;
                     }
