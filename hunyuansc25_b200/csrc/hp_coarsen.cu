@@ -76,8 +76,7 @@ __global__ void __launch_bounds__(256)
 pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
                   const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
-                  uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev, int32_t warp_deg,
-                  int32_t *__restrict__ hubflag)
+                  uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev, int32_t warp_deg)
 {
     if (made_prev && *made_prev == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -111,7 +110,6 @@ pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__
         }
     }
     pref[v] = best.u;
-    if (!ELIG && best.u >= 0) hubflag[best.u] = 1;   // the hub has a client to pair
 }
 
 template <bool ELIG>
@@ -120,8 +118,7 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
                 const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                 const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
                 const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
-                uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev,
-                int32_t *__restrict__ hubflag)
+                uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
 {
     if (made_prev && *made_prev == 0ull) return;
     const int lane = threadIdx.x & 31;
@@ -153,10 +150,7 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
             uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
             if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; }
         }
-        if (lane == 0) {
-            pref[v] = bu;
-            if (!ELIG && bu >= 0) hubflag[bu] = 1;
-        }
+        if (lane == 0) pref[v] = bu;
     }
 }
 
@@ -397,8 +391,7 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
                  const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                  const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
                  const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
-                 uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev,
-                 int32_t *__restrict__ hubflag)
+                 uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
 {
     if (made_prev && *made_prev == 0ull) return;
     __shared__ int32_t su[16], sw[16];
@@ -439,43 +432,8 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
                     bu = su[w2]; bw = sw[w2]; bh = sh[w2];
                 }
             pref[v] = bu;
-            if (!ELIG && bu >= 0) hubflag[bu] = 1;
         }
         __syncthreads();
-    }
-}
-
-// Hub pairing for rows longer than match_cta_deg: clients ranked by a CTA scan.
-__global__ void __launch_bounds__(512)
-pair_hub_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
-                     const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
-                     const int32_t *__restrict__ vwgt, const int32_t *__restrict__ hub,
-                     int32_t *__restrict__ match, int64_t maxvwgt, const int32_t *__restrict__ hubflag)
-{
-    __shared__ int32_t s_scan[512 / 32 + 2];
-    __shared__ int32_t s_cl[512];
-    const int32_t cnt = *d_count;
-    for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
-        const int32_t h = list[li];
-        if (!hubflag[h]) continue;   // nobody chose h: no client in its row
-        int32_t t = 0, carry = -1;
-        for (int32_t base = xadj[h]; base < xadj[h + 1]; base += 512) {
-            const int32_t j = base + threadIdx.x;
-            int32_t c = -1;
-            int isc = 0;
-            if (j < xadj[h + 1]) { c = adjncy[j]; isc = hub[c] == h; }
-            int tot;
-            const int ex = hp::block_excl_scan<512>(isc, &tot, s_scan);
-            if (isc) s_cl[ex] = c;
-            __syncthreads();
-            if (isc && ((t + ex) & 1)) {
-                const int32_t first = ex > 0 ? s_cl[ex - 1] : carry;
-                if ((int64_t)vwgt[first] + vwgt[c] <= maxvwgt) { match[first] = c; match[c] = first; }
-            }
-            if (tot > 0 && ((t + tot - 1) & 1) == 0) carry = s_cl[tot - 1];
-            t += tot;
-            __syncthreads();
-        }
     }
 }
 
@@ -486,67 +444,45 @@ count_matched_kernel(int32_t n, const int32_t *__restrict__ match, unsigned long
     hp::block_add_to<256>((v < n && match[v] != -1) ? 1 : 0, out);
 }
 
-// Pair the clients of hub h (unmatched vertices whose hub is h) in h's row
-// order: (c0,c1), (c2,c3), ... when the weight sum fits.
+// Two-hop pairing.  The clients of hub h (unmatched vertices whose hub is h)
+// are paired in h's row order -- (c0,c1), (c2,c3), ... when the weight sum
+// fits.  Rows are sorted by neighbour id, so h's row order is ascending client
+// id, and the pairs follow from the clients sorted stably by hub: a client at
+// an odd offset in its hub's run pairs with the one before it.  The work is
+// proportional to the number of clients, not to the length of the hubs' rows.
 __global__ void __launch_bounds__(256)
-pair_hub_small_kernel(int32_t n, const int32_t *__restrict__ xadj,
-                      const int32_t *__restrict__ adjncy, const int32_t *__restrict__ vwgt,
-                      const int32_t *__restrict__ hub, int32_t *__restrict__ match, int64_t maxvwgt,
-                      int32_t warp_deg, const int32_t *__restrict__ hubflag)
+client_flag_kernel(int32_t n, const int32_t *__restrict__ match, const int32_t *__restrict__ hub,
+                   int32_t *__restrict__ flags)
 {
-    int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= n || !hubflag[h]) return;
-    const int32_t b = xadj[h], e = xadj[h + 1];
-    if (e - b > warp_deg) return;
-    int32_t first = -1, t = 0;
-    for (int32_t j = b; j < e; j++) {
-        int32_t c = adjncy[j];
-        if (hub[c] != h) continue;
-        if ((t & 1) == 0) first = c;
-        else if ((int64_t)vwgt[first] + vwgt[c] <= maxvwgt) { match[first] = c; match[c] = first; }
-        t++;
-    }
+    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < n) flags[v] = match[v] == -1 && hub[v] >= 0;
 }
 
 __global__ void __launch_bounds__(256)
-pair_hub_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
-                    const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
-                    const int32_t *__restrict__ vwgt, const int32_t *__restrict__ hub,
-                    int32_t *__restrict__ match, int64_t maxvwgt, const int32_t *__restrict__ hubflag)
+client_keys_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
+                   const int32_t *__restrict__ hub, int32_t *__restrict__ keys)
 {
-    const int lane = threadIdx.x & 31;
     const int32_t cnt = *d_count;
-    for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
-         i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
-        const int32_t h = list[i];
-        if (!hubflag[h]) continue;   // nobody chose h: no client in its row
-        int32_t t = 0;          // clients seen so far
-        int32_t carry = -1;     // unpaired client from the previous chunk (t odd)
-        for (int32_t base = xadj[h]; base < xadj[h + 1]; base += 32) {
-            int32_t j = base + lane;
-            int32_t c = -1;
-            bool isc = false;
-            if (j < xadj[h + 1]) { c = adjncy[j]; isc = hub[c] == h; }
-            unsigned m = __ballot_sync(HP_FULL_MASK, isc);
-            // partner of an odd-ranked client is the previous client: either
-            // the nearest lower lane in this chunk or the carried one
-            unsigned below_all = m & hp::lanemask_lt();
-            int src = below_all ? 31 - __clz(below_all) : lane;
-            int32_t prevc = __shfl_sync(HP_FULL_MASK, c, src);
-            if (isc) {
-                int32_t r = t + __popc(below_all);
-                if (r & 1) {
-                    int32_t first = below_all ? prevc : carry;
-                    if ((int64_t)vwgt[first] + vwgt[c] <= maxvwgt) { match[first] = c; match[c] = first; }
-                }
-            }
-            int tot = __popc(m);
-            if (tot) {
-                int lastlane = 31 - __clz(m);
-                int32_t lastc = __shfl_sync(HP_FULL_MASK, c, lastlane);
-                if (((t + tot - 1) & 1) == 0) carry = lastc;  // last client has even rank
-            }
-            t += tot;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x)
+        keys[i] = hub[list[i]];
+}
+
+__global__ void __launch_bounds__(256)
+pair_clients_kernel(const int32_t *__restrict__ keys, const int32_t *__restrict__ vals,
+                    const int32_t *__restrict__ d_count, const int32_t *__restrict__ vwgt,
+                    int32_t *__restrict__ match, int64_t maxvwgt)
+{
+    const int32_t cnt = *d_count;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t h = keys[i];
+        int32_t lo = 0, hi = (int32_t)i;   // first index of the run of h
+        while (lo < hi) {
+            const int32_t mid = (lo + hi) >> 1;
+            if (keys[mid] < h) lo = mid + 1; else hi = mid;
+        }
+        if (((int32_t)i - lo) & 1) {
+            const int32_t a = vals[i - 1], b = vals[i];
+            if ((int64_t)vwgt[a] + vwgt[b] <= maxvwgt) { match[a] = b; match[b] = a; }
         }
     }
 }
@@ -1176,7 +1112,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
         const int tok = hp_prof_begin(c);
         const unsigned long long *prev = r == 0 ? nullptr : &sc[2 + r - 1];
         HP_LAUNCH(c, pref_small_kernel<true>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
-                  g.vwgt, g.match, elig, pref, lkey, maxvwgt, prev, tn.match_warp_deg, (int32_t *)nullptr);
+                  g.vwgt, g.match, elig, pref, lkey, maxvwgt, prev, tn.match_warp_deg);
         HP_LAUNCH(c, pref_big_topk_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
                   g.vwgt, g.match, elig, pref, cand, lkey, maxvwgt, prev);
         HP_LAUNCH(c, pref_huge_topk_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
@@ -1196,26 +1132,29 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     HP_TRY(matched(40, &nm));
     const int ftok = hp_prof_begin(c);
     if (4 * nm < 3 * (int64_t)n) {
-        // two-hop through a shared heaviest neighbour; hubflag marks the chosen
-        // hubs, so that only their rows are walked for clients
+        // two-hop through a shared heaviest neighbour: every unmatched vertex
+        // names its heaviest neighbour (any neighbour) as its hub; the clients,
+        // sorted stably by hub, are paired inside each hub's run
         int32_t *hub = pref;
-        int32_t *hubflag = flags;
-        HP_CUDA(cudaMemsetAsync(hubflag, 0, sizeof(int32_t) * (size_t)n, c->stream));
         HP_LAUNCH(c, pref_small_kernel<false>, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt,
-                  g.vwgt, g.match, elig, hub, lkey, maxvwgt, (const unsigned long long *)nullptr, tn.match_warp_deg,
-                  hubflag);
+                  g.vwgt, g.match, elig, hub, lkey, maxvwgt, (const unsigned long long *)nullptr, tn.match_warp_deg);
         HP_LAUNCH(c, pref_big_kernel<false>, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, elig, hub, lkey, maxvwgt,
-                  (const unsigned long long *)nullptr, hubflag);
+                  (const unsigned long long *)nullptr);
         HP_LAUNCH(c, pref_huge_kernel<false>, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, elig, hub, lkey, maxvwgt,
-                  (const unsigned long long *)nullptr, hubflag);
-        HP_LAUNCH(c, pair_hub_small_kernel, blocks_for(n), 256, 0, n, g.xadj, g.adjncy, g.vwgt, hub,
-                  g.match, maxvwgt, tn.match_warp_deg, hubflag);
-        HP_LAUNCH(c, pair_hub_big_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy,
-                  g.vwgt, hub, g.match, maxvwgt, hubflag);
-        HP_LAUNCH(c, pair_hub_huge_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
-                  g.adjncy, g.vwgt, hub, g.match, maxvwgt, hubflag);
+                  (const unsigned long long *)nullptr);
+        HP_LAUNCH(c, client_flag_kernel, blocks_for(n), 256, 0, n, g.match, hub, flags);
+        HP_TRY(hp_compact_flags(c, flags, n, list, d_listcnt));
+        // sort scratch: the candidate caches are not needed any more
+        int32_t *ck = cand, *ck2 = cand + n, *cv2 = cand + 2 * (int64_t)n;
+        HP_LAUNCH(c, client_keys_kernel, persistent_grid(c), 256, 0, list, d_listcnt, hub, ck);
+        int kbits = 0;
+        while ((1ll << kbits) < (int64_t)n) kbits++;
+        bool in_tmp = false;
+        HP_TRY(hp_sort_pairs(c, ck, list, ck2, cv2, n, d_listcnt, kbits, &in_tmp));
+        HP_LAUNCH(c, pair_clients_kernel, persistent_grid(c), 256, 0, in_tmp ? ck2 : ck, in_tmp ? cv2 : list,
+                  d_listcnt, g.vwgt, g.match, maxvwgt);
         hp_prof_end(c, ftok, HP_PROF_MATCH_MORE, 0);
         HP_TRY(matched(41, &nm));
     }

@@ -162,7 +162,9 @@ int32_t ora_match(int32_t n, const int32_t *xadj, const int32_t *adjncy,
     /* Fallbacks, each gated at 75 % matched. */
     if (4 * (int64_t)count_matched(n, match) < 3 * (int64_t)n) {
         /* two-hop: unmatched vertices that share their heaviest neighbour (the
-         * hub) are paired in the hub's row order */
+         * hub) are paired in ascending id -- the hub's row order, rows being
+         * sorted (hunyuangraph_GPU_match.h:1374-1716 pairs its leaf/relative
+         * classes through a shared neighbour as well) */
         int32_t *hub = pref;
 #pragma omp parallel for schedule(dynamic, 2048)
         for (int32_t v = 0; v < n; v++) {
@@ -179,26 +181,23 @@ int32_t ora_match(int32_t n, const int32_t *xadj, const int32_t *adjncy,
             }
             hub[v] = bu;
         }
-#pragma omp parallel
+        /* clients bucketed by hub in ascending id (a counting sort), then paired
+         * per hub: (c0,c1), (c2,c3), ... */
+        int32_t *start = (int32_t *)calloc((size_t)n + 1, sizeof(int32_t));
+        int32_t *ord = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+        for (int32_t c = 0; c < n; c++)
+            if (match[c] == -1 && hub[c] >= 0) start[hub[c] + 1]++;
+        for (int32_t h = 0; h < n; h++) start[h + 1] += start[h];
         {
-            int32_t *buf = NULL;
-            int32_t cap = 0;
-#pragma omp for schedule(dynamic, 1024)
-            for (int32_t h = 0; h < n; h++) {
-                int32_t len = 0;
-                for (int32_t j = xadj[h]; j < xadj[h + 1]; j++) {
-                    int32_t c = adjncy[j];
-                    if (hub[c] != h) continue;
-                    if (len == cap) {
-                        cap = cap ? 2 * cap : 64;
-                        buf = (int32_t *)realloc(buf, sizeof(int32_t) * (size_t)cap);
-                    }
-                    buf[len++] = c;
-                }
-                pair_list(buf, len, vwgt, maxvwgt, match);
-            }
-            free(buf);
+            int32_t *fill = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+            for (int32_t h = 0; h < n; h++) fill[h] = start[h];
+            for (int32_t c = 0; c < n; c++)
+                if (match[c] == -1 && hub[c] >= 0) ord[fill[hub[c]]++] = c;
+            free(fill);
         }
+        for (int32_t h = 0; h < n; h++) pair_list(ord + start[h], start[h + 1] - start[h], vwgt, maxvwgt, match);
+        free(start);
+        free(ord);
     }
     if (4 * (int64_t)count_matched(n, match) < 3 * (int64_t)n) {
         /* isolated vertices, paired in id order */
