@@ -90,6 +90,7 @@ TUNING_FIELDS = [
     "grid_ctas_per_sm",
     "dense_sparse_ratio",
     "small_level_n",
+    "chunk_deg",
 ]
 
 TUNING_DEFAULTS = {
@@ -104,6 +105,7 @@ TUNING_DEFAULTS = {
     "grid_ctas_per_sm": 8,
     "dense_sparse_ratio": 4,
     "small_level_n": 4096,
+    "chunk_deg": 4096,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -124,6 +126,7 @@ def tuning_violation(t: dict):
         ("grid_ctas_per_sm", 1, 32),
         ("dense_sparse_ratio", 1, 4096),
         ("small_level_n", 0, 32768),
+        ("chunk_deg", t["gain_thread_deg"], TUNE_DEG_MAX),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -132,7 +135,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 5)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 4)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

@@ -511,6 +511,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->grid_ctas_per_sm = 8;
     t->dense_sparse_ratio = 4;
     t->small_level_n = 4096;
+    t->chunk_deg = 4096;
 }
 
 namespace {
@@ -529,6 +530,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.grid_ctas_per_sm, 1, 32)) return "grid_ctas_per_sm";
     if (!in(t.dense_sparse_ratio, 1, 4096)) return "dense_sparse_ratio";
     if (!in(t.small_level_n, 0, HP_TUNE_SMALL_LEVEL_MAX)) return "small_level_n";
+    if (!in(t.chunk_deg, t.gain_thread_deg, HP_TUNE_DEG_MAX)) return "chunk_deg";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;

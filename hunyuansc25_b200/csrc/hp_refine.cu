@@ -40,9 +40,9 @@ __global__ void project_kernel(int32_t n, const int32_t *__restrict__ cmap,
 }
 
 // Row capacities min(deg, k); rows longer than bigd go on the big list, rows
-// longer than huged also on the hub list (count d_bigcnt[3]); d_bigcnt[1]
-// records the longest short row above 8 entries, d_bigcnt[2] the longest row
-// above huged.
+// longer than huged (the caller's chunk_deg) also on the long-row list (count
+// d_bigcnt[3]); d_bigcnt[1] records the longest short row above 8 entries,
+// d_bigcnt[2] the longest row above huged.
 __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t k,
                                 int32_t *__restrict__ cap, int32_t *big, int32_t *huge, int32_t *d_bigcnt,
                                 int32_t bigd, int32_t huged)
@@ -758,7 +758,7 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
                        const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                        const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
                        int8_t *__restrict__ lock, const unsigned long long *d_ncand,
-                       int32_t *__restrict__ moves, unsigned long long *d_nmoves, int32_t huged)
+                       int32_t *__restrict__ moves, unsigned long long *d_nmoves, int32_t chunkd)
 {
     if (*d_ncand == 0ull) return;
     const int lane = threadIdx.x & 31;
@@ -766,7 +766,7 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = big[i];
-        if (xadj[v + 1] - xadj[v] > huged) continue;
+        if (xadj[v + 1] - xadj[v] > chunkd) continue;   // chunked over the grid
         const int32_t g = pregain[v];
         int8_t sel = 0;
         if (g != NEG) {
@@ -782,48 +782,81 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
     }
 }
 
-// ---- hub rows (longer than huged): chunk plans ----------------------------------
-// The work on hub rows is cut into chunks of HUB_CHUNK entries dealt over the
-// whole grid.  A one-CTA kernel plans it per pass: it selects the hubs that have
-// work (afterburner: candidates; moves: moved hubs), writes each one's vertex,
-// its item (hub-list position or move index) and the exclusive prefix of the
-// chunk counts, so that a chunk finds its hub by a binary search.
+// ---- long rows (longer than chunk_deg): chunk plans ------------------------------
+// The afterburner and move application of rows longer than the tuning's
+// chunk_deg are cut into chunks of HUB_CHUNK entries dealt over the whole grid,
+// so that no warp walks a long row alone.  A plan per pass selects the rows that
+// have work (afterburner: candidates; moves: moved rows) and writes each one's
+// vertex, its item (list position or move index) and the exclusive prefix of
+// the chunk counts, so that a chunk finds its row by a binary search.  The plan
+// is one pass of persistent CTAs over tiles of PLAN_TILE items with two epoch
+// look-back chains (selected rows: tile words [0, half); chunks: [half, 2 half)).
 constexpr int HUB_CHUNK = 512;
+constexpr int PLAN_THREADS = 256, PLAN_ITEMS = 4, PLAN_TILE = PLAN_THREADS * PLAN_ITEMS;
 
 template <bool MOVES>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(PLAN_THREADS)
 hub_plan_kernel(const int32_t *__restrict__ items, const int32_t *__restrict__ d_nitems,
                 const int32_t *__restrict__ moves, const int32_t *__restrict__ pregain,
                 const int32_t *__restrict__ xadj, int32_t *__restrict__ plan_v, int32_t *__restrict__ plan_item,
-                int32_t *__restrict__ plan_off, int32_t *__restrict__ d_plan)
+                int32_t *__restrict__ plan_off, int32_t *__restrict__ d_plan, unsigned long long *tile_status,
+                int64_t half, hp::LbCtl *lb, unsigned *status)
 {
-    __shared__ int32_t s_scan[1024 / 32 + 2];
+    __shared__ int32_t s_scan[PLAN_THREADS / 32 + 2];
+    __shared__ int32_t s_excl[2];
+    const unsigned epoch = hp::lb_epoch(lb);
     const int32_t ni = *d_nitems;
-    int32_t nsel = 0, nch = 0;
-    for (int32_t base = 0; base < ni; base += 1024) {
-        const int32_t t = base + threadIdx.x;
-        int32_t v = -1, c = 0;
-        if (t < ni) {
-            v = MOVES ? moves[items[t]] : items[t];
-            const bool take = MOVES || pregain[v] != NEG;
-            if (take) c = (xadj[v + 1] - xadj[v] + HUB_CHUNK - 1) / HUB_CHUNK;
-            else v = -1;
+    for (;;) {
+        const int64_t tile = hp::lb_next(lb);
+        const int64_t base = tile * PLAN_TILE;
+        if (base > ni) break;   // the tile holding index ni (it writes the totals) was the last
+        const int64_t t0 = base + (int64_t)threadIdx.x * PLAN_ITEMS;
+        int32_t v[PLAN_ITEMS], c[PLAN_ITEMS];
+        int32_t ns = 0, nc = 0;
+#pragma unroll
+        for (int q = 0; q < PLAN_ITEMS; q++) {
+            const int64_t t = t0 + q;
+            v[q] = -1;
+            c[q] = 0;
+            if (t < ni) {
+                const int32_t vv = MOVES ? moves[items[t]] : items[t];
+                if (MOVES || pregain[vv] != NEG) {
+                    v[q] = vv;
+                    c[q] = (xadj[vv + 1] - xadj[vv] + HUB_CHUNK - 1) / HUB_CHUNK;
+                }
+            }
+            ns += v[q] >= 0;
+            nc += c[q];
         }
-        int tsel, tch;
-        const int psel = nsel + hp::block_excl_scan<1024>(v >= 0 ? 1 : 0, &tsel, s_scan);
-        const int pch = nch + hp::block_excl_scan<1024>(c, &tch, s_scan);
-        if (v >= 0) {
-            plan_v[psel] = v;
-            plan_item[psel] = MOVES ? items[t] : t;
-            plan_off[psel] = pch;
+        int ts, tc;
+        int32_t ps = hp::block_excl_scan<PLAN_THREADS>(ns, &ts, s_scan);
+        int32_t pc = hp::block_excl_scan<PLAN_THREADS>(nc, &tc, s_scan);
+        if (threadIdx.x < 32) {
+            const int32_t ex = hp::lookback_epoch(tile_status, tile, ts, epoch, status);
+            if (threadIdx.x == 0) s_excl[0] = ex;
+        } else if (threadIdx.x < 64) {
+            const int32_t ex = hp::lookback_epoch(tile_status + half, tile, tc, epoch, status);
+            if (threadIdx.x == 32) s_excl[1] = ex;
         }
-        nsel += tsel;
-        nch += tch;
+        __syncthreads();
+        ps += s_excl[0];
+        pc += s_excl[1];
+#pragma unroll
+        for (int q = 0; q < PLAN_ITEMS; q++) {
+            if (v[q] >= 0) {
+                plan_v[ps] = v[q];
+                plan_item[ps] = MOVES ? items[t0 + q] : (int32_t)(t0 + q);
+                plan_off[ps] = pc;
+                ps++;
+            }
+            pc += c[q];
+        }
+        if (ni >= base && ni < base + PLAN_TILE && threadIdx.x == 0) {
+            d_plan[0] = s_excl[0] + ts;
+            d_plan[1] = s_excl[1] + tc;
+        }
     }
-    if (threadIdx.x == 0) {
-        d_plan[0] = nsel;
-        d_plan[1] = nch;
-    }
+    hp::lb_end(lb);
 }
 
 // chunk gc -> selected hub j (the last j with plan_off[j] <= gc)
@@ -953,7 +986,7 @@ __device__ __forceinline__ void apply_moves_rows(int64_t warp, int64_t nwarps, c
                                                  int32_t *__restrict__ gconn, int32_t *__restrict__ dirty,
                                                  int32_t *__restrict__ small_l, int32_t *__restrict__ big_l,
                                                  int32_t *counts, int32_t k, int32_t *__restrict__ huge_mv,
-                                                 int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t huged)
+                                                 int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t chunkd)
 {
     const int lane = threadIdx.x & 31;
     for (int64_t i = warp; i < nm; i += nwarps) {
@@ -966,7 +999,7 @@ __device__ __forceinline__ void apply_moves_rows(int64_t warp, int64_t nwarps, c
             atomicAdd(&pw[p], (unsigned long long)(-(long long)w));
         }
         const int32_t b = xadj[v], e = xadj[v + 1];
-        if (e - b > huged) {
+        if (e - b > chunkd) {
             // neighbours of a hub are touched by apply_moves_huge_kernel, spread
             // over the whole grid (it reads the old part from oldp)
             if (lane == 0) {
@@ -1008,11 +1041,11 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
                    const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ goff,
                    int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
                    int32_t *__restrict__ big_l, int32_t *counts, int32_t k, int32_t *__restrict__ huge_mv,
-                   int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t huged)
+                   int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t chunkd)
 {
     apply_moves_rows((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, ((int64_t)gridDim.x * blockDim.x) >> 5,
                      moves, (int64_t)*d_nmoves, where, dest, vwgt, pw, xadj, adjncy, adjwgt, goff, gconn, dirty,
-                     small_l, big_l, counts, k, huge_mv, d_nhuge, bigd, huged);
+                     small_l, big_l, counts, k, huge_mv, d_nhuge, bigd, chunkd);
 }
 
 // Neighbours of the moved hubs (queued by apply_moves_kernel, planned by
@@ -1453,7 +1486,8 @@ __global__ void rs_assign_kernel(int32_t k, const int32_t *__restrict__ P, const
 struct RefineBufs {
     int32_t *goff, *gpart, *gconn, *big, *dest, *pregain, *moves, *oldp, *dirty;
     int32_t *small_l, *big_l, *best_where, *huge_mv, *huge;
-    int32_t *plan_v, *plan_item, *plan_off, *plan_cnt;   // hub chunk plan of the current step
+    int32_t *plan_v, *plan_item, *plan_off, *plan_cnt;   // chunk plan of the current step
+    int64_t nhub_cap;   // capacity of the long-row list and the plan (rows longer than chunk_deg)
     unsigned long long *ab_acc;   // afterburner sums of the hub rows (zero between passes)
     int8_t *lock;
     int32_t *K, *V, *K2, *V2, *pre, *P, *sp;
@@ -1535,6 +1569,13 @@ int key_bits_for(int32_t k)
 unsigned rank_grid(const hp_context *c, int64_t tiles)
 {
     return (unsigned)std::min<int64_t>(tiles, (int64_t)c->sm_count * c->tune.grid_ctas_per_sm);
+}
+
+// Persistent grid of a chunk plan over at most cap items (the tile holding
+// index cap included).
+unsigned plan_grid(const hp_context *c, int64_t cap)
+{
+    return rank_grid(c, cap / PLAN_TILE + 1);
 }
 
 // Candidates of the pass (rb_candidates_kernel, K/V in vertex order) -> stable
@@ -1750,7 +1791,7 @@ __global__ void restore_best_kernel(const RefineCtl *s, int32_t n, const int32_t
 
 struct PassCfg {
     int32_t k;
-    bool finest, any_big, recording, huge_rows;
+    bool finest, any_big, recording, huge_rows;   // huge_rows: rows longer than chunk_deg exist
     RefineCtl *ctl;
     unsigned long long *best_pw;
 };
@@ -1783,11 +1824,12 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
                   B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES], c->tune.gain_thread_deg);
         if (P.any_big)
             HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt, g.where,
-                      B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES], c->tune.gain_hub_deg);
+                      B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES], c->tune.chunk_deg);
         if (P.huge_rows) {
             const int32_t *d_nhuge = d_bigcnt + 3;
-            HP_LAUNCH(c, hub_plan_kernel<false>, 1, 1024, 0, B.huge, d_nhuge, B.moves, B.pregain, g.xadj, B.plan_v,
-                      B.plan_item, B.plan_off, B.plan_cnt);
+            HP_LAUNCH(c, hub_plan_kernel<false>, plan_grid(c, B.nhub_cap), PLAN_THREADS, 0, B.huge, d_nhuge, B.moves,
+                      B.pregain, g.xadj, B.plan_v, B.plan_item, B.plan_off, B.plan_cnt, c->lb_status, c->lb_cap / 2,
+                      c->lb_ctl, c->d_status);
             HP_LAUNCH(c, afterburner_huge_kernel, (unsigned)(4 * c->sm_count), HUB_CHUNK, 0, B.plan_v, B.plan_item,
                       B.plan_off, B.plan_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, &sc[S_NCAND],
                       B.ab_acc);
@@ -1821,10 +1863,11 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
               B.oldp, 1, &sc[S_C1], k);
     HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw, g.xadj,
               g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k,
-              B.huge_mv, (int32_t *)&sc[S_HUGEMV], c->tune.gain_thread_deg, c->tune.gain_hub_deg);
+              B.huge_mv, (int32_t *)&sc[S_HUGEMV], c->tune.gain_thread_deg, c->tune.chunk_deg);
     if (P.huge_rows) {
-        HP_LAUNCH(c, hub_plan_kernel<true>, 1, 1024, 0, B.huge_mv, (const int32_t *)&sc[S_HUGEMV], B.moves,
-                  B.pregain, g.xadj, B.plan_v, B.plan_item, B.plan_off, B.plan_cnt);
+        HP_LAUNCH(c, hub_plan_kernel<true>, plan_grid(c, B.nhub_cap), PLAN_THREADS, 0, B.huge_mv,
+                  (const int32_t *)&sc[S_HUGEMV], B.moves, B.pregain, g.xadj, B.plan_v, B.plan_item, B.plan_off,
+                  B.plan_cnt, c->lb_status, c->lb_cap / 2, c->lb_ctl, c->d_status);
         HP_LAUNCH(c, apply_moves_huge_kernel, (unsigned)(4 * c->sm_count), HUB_CHUNK, 0, B.plan_v, B.plan_item,
                   B.plan_off, B.plan_cnt, B.oldp, B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty,
                   B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k, c->tune.gain_thread_deg);
@@ -2460,9 +2503,12 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.lock = ralloc_t<int8_t>(c, n);
     B.pw = ralloc_t<unsigned long long>(c, k);
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
-    // at most m / (huged + 1) rows are longer than huged
-    const int32_t huged = c->tune.gain_hub_deg;
-    const int64_t nhub_cap = std::min<int64_t>((int64_t)n, g.m / ((int64_t)huged + 1)) + 1;
+    // at most m / (chunk_deg + 1) rows are longer than chunk_deg (the long-row
+    // list of the afterburner and of the moves)
+    const int32_t huged = c->tune.gain_hub_deg, chunkd = c->tune.chunk_deg;
+    const int64_t nhub_cap = std::min<int64_t>((int64_t)n, g.m / ((int64_t)chunkd + 1)) + 1;
+    if (2 * (nhub_cap / PLAN_TILE + 1) > c->lb_cap) return HP_ERR_INTERNAL;
+    B.nhub_cap = nhub_cap;
     B.ab_acc = ralloc_t<unsigned long long>(c, nhub_cap);
     B.plan_v = ralloc_t<int32_t>(c, nhub_cap);
     B.plan_item = ralloc_t<int32_t>(c, nhub_cap);
@@ -2473,8 +2519,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 2), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
     HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt,
-              c->tune.gain_thread_deg, huged);
-    if (ls.maxdeg > huged)
+              c->tune.gain_thread_deg, chunkd);
+    if (ls.maxdeg > chunkd)
         HP_CUDA(cudaMemsetAsync(B.ab_acc, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
     // the gain rows take G = sum min(deg, k) <= m entries: allocated for m, so
@@ -2520,7 +2566,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
         log_r0 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
     }
-    PassCfg P{k, finest, any_big, recording, B.huge_rows, ctl, best_pw};
+    PassCfg P{k, finest, any_big, recording, ls.maxdeg > chunkd, ctl, best_pw};
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     const bool use_graph = graph_loop(c);
     RefineCtl h{};

@@ -56,6 +56,7 @@ SPACE = {
     "grid_ctas_per_sm": [2, 4, 8, 12, 16],
     "dense_sparse_ratio": [1, 2, 4, 8, 32],
     "small_level_n": [0, 2048, 4096, 8192, 16384, 32768],
+    "chunk_deg": [512, 1024, 2048, 4096, 8192],
 }
 
 

@@ -165,7 +165,10 @@ typedef struct hp_tuning {
     int32_t small_level_n;       /* refinement: levels of at most this many vertices
                                     (and 16x as many adjacency entries, nparts <= 1024)
                                     run all their passes in one CTA; 0 = never    [0, 32768]    4096 */
-    int32_t reserved[5];         /* zero */
+    int32_t chunk_deg;           /* refinement: the afterburner and move application
+                                    split rows longer than this into chunks of 512
+                                    entries over the whole grid                  [gain_thread_deg, 2^24] 4096 */
+    int32_t reserved[4];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);
