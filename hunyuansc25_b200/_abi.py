@@ -91,6 +91,7 @@ TUNING_FIELDS = [
     "dense_sparse_ratio",
     "small_level_n",
     "chunk_deg",
+    "trial_cta_n",
 ]
 
 TUNING_DEFAULTS = {
@@ -106,6 +107,7 @@ TUNING_DEFAULTS = {
     "dense_sparse_ratio": 4,
     "small_level_n": 4096,
     "chunk_deg": 4096,
+    "trial_cta_n": 512,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -127,6 +129,7 @@ def tuning_violation(t: dict):
         ("dense_sparse_ratio", 1, 4096),
         ("small_level_n", 0, 32768),
         ("chunk_deg", t["gain_thread_deg"], TUNE_DEG_MAX),
+        ("trial_cta_n", 1, TUNE_DEG_MAX),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -135,7 +138,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 4)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 3)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

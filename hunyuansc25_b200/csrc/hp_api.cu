@@ -512,6 +512,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->dense_sparse_ratio = 4;
     t->small_level_n = 4096;
     t->chunk_deg = 4096;
+    t->trial_cta_n = 512;
 }
 
 namespace {
@@ -531,6 +532,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.dense_sparse_ratio, 1, 4096)) return "dense_sparse_ratio";
     if (!in(t.small_level_n, 0, HP_TUNE_SMALL_LEVEL_MAX)) return "small_level_n";
     if (!in(t.chunk_deg, t.gain_thread_deg, HP_TUNE_DEG_MAX)) return "chunk_deg";
+    if (!in(t.trial_cta_n, 1, HP_TUNE_DEG_MAX)) return "trial_cta_n";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;

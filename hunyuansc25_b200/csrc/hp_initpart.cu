@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "hp_internal.cuh"
+#include "hp_rowagg.cuh"
 
 // Shared memory for the trial states of one CTA (<= 227 KB per CTA on B200).
 #define HP_TRIAL_SMEM (200 * 1024)
@@ -246,6 +247,221 @@ trial_warp_kernel(const SubInfo *__restrict__ subs, const int32_t *__restrict__ 
     if (lane == 0) { tr_cut[t] = cut; tr_viol[t] = viol; }
 }
 
+// The same trial with one CTA of TC_THREADS threads per trial, for the large
+// subgraphs of the first recursion depths: the FM pop is an argmax of n/256
+// candidates per thread reduced across the warps, the BFS appends a row chunk's
+// unvisited neighbours in row order through a block scan, and every decision
+// is taken by all threads alike from shared values, so the trial's moves, cut
+// and sides are those of trial_warp_kernel.
+constexpr int TC_THREADS = 256;
+constexpr int TC_WARPS = TC_THREADS / 32;
+
+__device__ __forceinline__ int32_t tc_block_min(int32_t v, int32_t *s_red)
+{
+    v = __reduce_min_sync(HP_FULL_MASK, v);
+    __syncthreads();   // earlier readers of s_red are done
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int32_t r = INT_MAX;
+#pragma unroll
+    for (int w = 0; w < TC_WARPS; w++) r = min(r, s_red[w]);
+    return r;
+}
+
+__global__ void __launch_bounds__(TC_THREADS)
+trial_cta_kernel(const SubInfo *__restrict__ subs, const int32_t *__restrict__ trial_sub,
+                 int32_t ntrials, const int32_t *__restrict__ fxadj, const int32_t *__restrict__ fadj,
+                 const int32_t *__restrict__ fwgt, const int32_t *__restrict__ fvwgt, char *slab_base,
+                 int32_t starts, int32_t fm_passes, int64_t *tr_cut, int64_t *tr_viol, int use_smem)
+{
+    extern __shared__ __align__(16) char tsm[];
+    __shared__ int32_t s_red[TC_WARPS], s_key[TC_WARPS];
+    __shared__ int32_t s_scan[TC_WARPS + 2];
+    __shared__ long long s_cut[TC_WARPS];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int32_t t = blockIdx.x;
+    if (t >= ntrials) return;   // whole CTA
+    const SubInfo S = subs[trial_sub[t]];
+    const int32_t lt = t - S.tbeg;
+    const int32_t n = S.n;
+    const int32_t *xadj = fxadj + S.vbeg;
+    const int32_t *vwgt = fvwgt + S.vbeg;
+    char *base = use_smem ? tsm : slab_base + S.slab_off + (int64_t)lt * state_bytes(n);
+    TrialState T = carve(base, n);
+    const int32_t start = (n <= starts) ? lt : (int32_t)(((int64_t)lt * n) / starts);
+    const int64_t tv = S.tv, want1 = S.want1, onemin = S.onemin, onemax = S.onemax;
+    int64_t pw0 = 0, pw1 = tv;
+
+    // ---- BFS growth of side 0
+    for (int32_t v = tid; v < n; v += TC_THREADS) { T.where[v] = 1; T.vis[v] = 0; }
+    __syncthreads();
+    int32_t first = 0, last = 1, nleft = n - 1, next_unvis = 0;
+    bool drain = false;
+    if (tid == 0) { T.swaps[0] = start; T.vis[start] = 1; }
+    __syncthreads();
+    for (;;) {
+        if (first == last) {
+            if (nleft == 0 || drain) break;
+            for (;;) {   // lowest unvisited vertex
+                const int32_t v = next_unvis + tid;
+                const int32_t mv = tc_block_min(v < n && !T.vis[v] ? v : INT_MAX, s_red);
+                if (mv != INT_MAX) { next_unvis = mv; break; }
+                next_unvis += TC_THREADS;
+            }
+            __syncthreads();
+            if (tid == 0) { T.swaps[0] = next_unvis; T.vis[next_unvis] = 1; }
+            __syncthreads();
+            first = 0; last = 1; nleft--;
+        }
+        const int32_t i = T.swaps[first++];
+        const int32_t wi = vwgt[i];
+        if (pw0 > 0 && pw1 - wi < onemin) { drain = true; continue; }
+        __syncthreads();   // every thread has read swaps[first - 1]
+        if (tid == 0) T.where[i] = 0;
+        pw0 += wi; pw1 -= wi;
+        if (pw1 <= onemax) break;
+        drain = false;
+        for (int32_t base_j = xadj[i]; base_j < xadj[i + 1]; base_j += TC_THREADS) {
+            const int32_t j = base_j + tid;
+            int32_t k = -1;
+            bool un = false;
+            if (j < xadj[i + 1]) { k = fadj[j]; un = !T.vis[k]; }
+            int tot;
+            const int ex = hp::block_excl_scan<TC_THREADS>(un ? 1 : 0, &tot, s_scan);
+            if (un) { T.swaps[last + ex] = k; T.vis[k] = 1; }
+            last += tot;
+            nleft -= tot;
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+
+    // ---- 2-way FM
+    long long cut2 = 0;
+    for (int32_t v = tid; v < n; v += TC_THREADS) {
+        int32_t tid_ = 0, ted = 0;
+        const int8_t wv = T.where[v];
+        for (int32_t j = xadj[v]; j < xadj[v + 1]; j++) {
+            if (T.where[fadj[j]] == wv) tid_ += fwgt[j];
+            else ted += fwgt[j];
+        }
+        T.id[v] = tid_; T.ed[v] = ted;
+        T.bnd[v] = (ted > 0 || xadj[v] == xadj[v + 1]);
+        cut2 += ted;
+        T.moved[v] = -1;
+    }
+    cut2 = hp::warp_sum64(cut2);
+    if (lane == 0) s_cut[wid] = cut2;
+    __syncthreads();
+    long long call = 0;
+#pragma unroll
+    for (int w = 0; w < TC_WARPS; w++) call += s_cut[w];
+    int64_t cut = call / 2;
+    const int64_t tpw0 = tv - want1, tpw1 = want1;
+    int64_t limit = n / 100;
+    if (limit < 15) limit = 15;
+    if (limit > 100) limit = 100;
+    int64_t avgvwgt = (pw0 + pw1) / 20;
+    if (n > 0 && 2 * (pw0 + pw1) / n < avgvwgt) avgvwgt = 2 * (pw0 + pw1) / n;
+    const int64_t origdiff = hp::iabs64(tpw0 - pw0);
+
+    auto relax = [&](int32_t h, int to) {
+        for (int32_t j = xadj[h] + tid; j < xadj[h + 1]; j += TC_THREADS) {
+            const int32_t k = fadj[j];
+            const int32_t kw = (to == T.where[k]) ? fwgt[j] : -fwgt[j];
+            const int32_t nid = T.id[k] + kw, ned = T.ed[k] - kw;
+            T.id[k] = nid; T.ed[k] = ned;
+            if (T.bnd[k]) { if (ned == 0) T.bnd[k] = 0; }
+            else if (ned > 0) T.bnd[k] = 1;
+        }
+        __syncthreads();
+    };
+
+    for (int32_t pass = 0; pass < fm_passes; pass++) {
+        int64_t mincutorder = -1;
+        int64_t newcut = cut, mincut = cut, initcut = cut;
+        int64_t mindiff = hp::iabs64(tpw0 - pw0);
+        int32_t nswaps;
+        for (nswaps = 0; nswaps < n; nswaps++) {
+            const int from = (tpw0 - pw0 < tpw1 - pw1) ? 0 : 1;
+            const int to = 1 - from;
+            int32_t bh = -1, bk = 0;
+            for (int32_t v = tid; v < n; v += TC_THREADS) {
+                if (T.bnd[v] && T.moved[v] == -1 && T.where[v] == from) {
+                    const int32_t key = T.ed[v] - T.id[v];
+                    if (bh < 0 || key > bk) { bh = v; bk = key; }   // ascending v per thread
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const int32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
+                const int32_t ok = __shfl_xor_sync(HP_FULL_MASK, bk, o);
+                if (oh >= 0 && (bh < 0 || ok > bk || (ok == bk && oh < bh))) { bh = oh; bk = ok; }
+            }
+            __syncthreads();   // earlier readers of s_red / s_key are done
+            if (lane == 0) { s_red[wid] = bh; s_key[wid] = bk; }
+            __syncthreads();
+            bh = -1; bk = 0;
+#pragma unroll
+            for (int w = 0; w < TC_WARPS; w++) {
+                const int32_t oh = s_red[w], ok = s_key[w];
+                if (oh >= 0 && (bh < 0 || ok > bk || (ok == bk && oh < bh))) { bh = oh; bk = ok; }
+            }
+            const int32_t h = bh;
+            if (h < 0) break;
+            const int32_t gain = bk, wh = vwgt[h];
+            newcut -= gain;
+            if (to == 0) { pw0 += wh; pw1 -= wh; } else { pw1 += wh; pw0 -= wh; }
+            if ((newcut < mincut && hp::iabs64(tpw0 - pw0) <= origdiff + avgvwgt) ||
+                (newcut == mincut && hp::iabs64(tpw0 - pw0) < mindiff)) {
+                mincut = newcut;
+                mindiff = hp::iabs64(tpw0 - pw0);
+                mincutorder = nswaps;
+            } else if (nswaps - mincutorder > limit) {
+                newcut += gain;
+                if (to == 0) { pw0 -= wh; pw1 += wh; } else { pw1 -= wh; pw0 += wh; }
+                break;
+            }
+            if (tid == 0) {
+                T.where[h] = (int8_t)to;
+                T.moved[h] = nswaps;
+                T.swaps[nswaps] = h;
+                int32_t tt = T.id[h]; T.id[h] = T.ed[h]; T.ed[h] = tt;
+                if (T.ed[h] == 0 && xadj[h] < xadj[h + 1]) T.bnd[h] = 0;
+            }
+            __syncthreads();
+            relax(h, to);
+        }
+        __syncthreads();
+        for (int32_t i = tid; i < nswaps; i += TC_THREADS) T.moved[T.swaps[i]] = -1;
+        __syncthreads();
+        for (nswaps--; nswaps > mincutorder; nswaps--) {
+            const int32_t h = T.swaps[nswaps];
+            const int to = 1 - T.where[h];
+            __syncthreads();   // every thread has read where[h]
+            if (tid == 0) {
+                T.where[h] = (int8_t)to;
+                int32_t tt = T.id[h]; T.id[h] = T.ed[h]; T.ed[h] = tt;
+                if (T.ed[h] == 0 && T.bnd[h] && xadj[h] < xadj[h + 1]) T.bnd[h] = 0;
+                else if (T.ed[h] > 0 && !T.bnd[h]) T.bnd[h] = 1;
+            }
+            const int32_t wh = vwgt[h];
+            if (to == 0) { pw0 += wh; pw1 -= wh; } else { pw1 += wh; pw0 -= wh; }
+            __syncthreads();
+            relax(h, to);
+        }
+        cut = mincut;
+        if (mincutorder <= 0 || mincut == initcut) break;
+    }
+    int64_t viol = 0;
+    if (pw1 > onemax) viol += pw1 - onemax;
+    if (pw1 < onemin) viol += onemin - pw1;
+    int8_t *wout = (int8_t *)(slab_base + S.slab_off + (int64_t)lt * state_bytes(n));
+    if (use_smem)
+        for (int32_t v = tid; v < n; v += TC_THREADS) wout[v] = T.where[v];
+    if (tid == 0) { tr_cut[t] = cut; tr_viol[t] = viol; }
+}
+
 // Best trial of every subgraph: min (violation, cut, trial index); copies its
 // sides into side[] and reports the side-0 vertex count and weight.
 __global__ void __launch_bounds__(256)
@@ -401,6 +617,8 @@ int hp_initpart_init()
 {
     HP_CUDA(cudaFuncSetAttribute(trial_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)HP_TRIAL_SMEM));
+    HP_CUDA(cudaFuncSetAttribute(trial_cta_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)HP_TRIAL_SMEM));
     return HP_OK;
 }
 
@@ -487,9 +705,13 @@ int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_
         const int use_smem = per <= HP_TRIAL_SMEM ? 1 : 0;
         const int wpb_eff = use_smem ? wpb : 4;
         const int tok = hp_prof_begin(c);
-        HP_LAUNCH(c, trial_warp_kernel, nblk(tcount, wpb_eff), 32 * wpb_eff,
-                  use_smem ? (size_t)(per * wpb_eff) : 0, d_info, d_tsub, tcount, fxadj, fadj, fwgt, fvwgt,
-                  slab, starts, fm_passes, d_cut, d_viol, use_smem, per);
+        if (maxn >= c->tune.trial_cta_n)   // a CTA per trial (same trial, same result)
+            HP_LAUNCH(c, trial_cta_kernel, (unsigned)tcount, TC_THREADS, use_smem ? (size_t)per : 0, d_info, d_tsub,
+                      tcount, fxadj, fadj, fwgt, fvwgt, slab, starts, fm_passes, d_cut, d_viol, use_smem);
+        else
+            HP_LAUNCH(c, trial_warp_kernel, nblk(tcount, wpb_eff), 32 * wpb_eff,
+                      use_smem ? (size_t)(per * wpb_eff) : 0, d_info, d_tsub, tcount, fxadj, fadj, fwgt, fvwgt,
+                      slab, starts, fm_passes, d_cut, d_viol, use_smem, per);
         hp_prof_end(c, tok, HP_PROF_INIT, 0);
         HP_LAUNCH(c, select_kernel, (unsigned)ns, 256, 0, d_info, d_cut, d_viol, slab, fvwgt, side, d_res);
         std::vector<int64_t> res(2 * ns);

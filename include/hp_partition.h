@@ -168,7 +168,10 @@ typedef struct hp_tuning {
     int32_t chunk_deg;           /* refinement: the afterburner and move application
                                     split rows longer than this into chunks of 512
                                     entries over the whole grid                  [gain_thread_deg, 2^24] 4096 */
-    int32_t reserved[4];         /* zero */
+    int32_t trial_cta_n;         /* initial bisection: a recursion depth whose largest
+                                    subgraph has at least this many vertices runs
+                                    a CTA per trial instead of a warp             [1, 2^24]     512 */
+    int32_t reserved[3];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);
