@@ -1373,6 +1373,7 @@ rs_evict_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, co
 // Rooms are read 32 parts at a time; a part without room keeps an empty range
 // (the rule gives end = start there); otherwise the end is searched first among
 // the 32 entries after the start (one coalesced read), then 32-ary over the rest.
+// Once the start reaches np the remaining parts all get the empty range [np, np).
 // The whole CTA first stages sp[0..np] in shared memory when it fits
 // (COOKIE_SMEM_INTS entries), then warp 0 walks the parts; every search then
 // waits on shared memory instead of L2.
@@ -1453,6 +1454,13 @@ __device__ void cookie_cut_warp(int32_t k, const unsigned long long *__restrict_
             }
             if (lane == 0) { es[p] = lo0; ee[p] = end; }
             st = end;
+            if (st == np) {
+                // the evicted list is used up: every later part starts at np and,
+                // room or not, ends there (nothing lies beyond np), so the rest is
+                // written in parallel
+                for (int32_t r = p + 1 + lane; r < k; r += 32) { es[r] = np; ee[r] = np; }
+                return;
+            }
         }
     }
 }
