@@ -491,7 +491,7 @@ struct RowBest {
 // Rows of at most 32 entries are walked by their lane; longer rows by the
 // whole warp, one row at a time, reduced in the serial walk's order.
 __device__ __forceinline__ RowBest row_best(const int32_t *__restrict__ gpart, const int32_t *__restrict__ gconn,
-                                            int32_t o, int32_t len, int32_t p)
+                                            int32_t o, int32_t len, int32_t p, int32_t k)
 {
     const int lane = threadIdx.x & 31;
     RowBest r{0, 0, 0, -1, 0};
@@ -514,8 +514,9 @@ __device__ __forceinline__ RowBest row_best(const int32_t *__restrict__ gpart, c
         const int32_t sp = __shfl_sync(HP_FULL_MASK, p, src);
         int32_t lpc = 0, lbc = 0, lb = -1, lnp = 0;
         long long lwd = 0;
+        const bool dense = sl == k;   // entry j is part j
         for (int32_t j = lane; j < sl; j += 32) {
-            const int32_t q = gpart[so + j];
+            const int32_t q = dense ? j : gpart[so + j];
             if (q < 0) break;   // padding runs to the end of the row
             const int32_t cq = gconn[so + j];
             lwd += cq;
@@ -542,7 +543,7 @@ __global__ void __launch_bounds__(256)
 lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
                  const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
                  const int8_t *__restrict__ lock, int finest, int32_t *__restrict__ dest,
-                 int32_t *__restrict__ pregain, unsigned long long *d_ncand, const int32_t *gate)
+                 int32_t *__restrict__ pregain, unsigned long long *d_ncand, const int32_t *gate, int32_t k)
 {
     if (gate && *gate != 0) return;   // graph mode: the learned kernel runs this pass
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -553,7 +554,7 @@ lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__r
         o = goff[v];
         len = goff[v + 1] - o;
     }
-    const RowBest rb = row_best(gpart, gconn, o, len, p);
+    const RowBest rb = row_best(gpart, gconn, o, len, p, k);
     const int64_t pc = rb.pc, bc = rb.bc;
     const int32_t b = rb.b;
     if (v < n) {
@@ -579,7 +580,7 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
                          const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
                          const int64_t *__restrict__ opt, const float *__restrict__ params, float threshold,
                          int32_t *__restrict__ dest, int32_t *__restrict__ pregain, unsigned long long *d_ncand,
-                         const int32_t *gate)
+                         const int32_t *gate, int32_t k)
 {
     if (gate && *gate != 1) return;   // graph mode: the plain kernel runs this pass
     __shared__ hp::MlpSmem sm;
@@ -595,7 +596,7 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
         o = goff[v];
         len = goff[v + 1] - o;
     }
-    const RowBest rb = row_best(gpart, gconn, o, len, p);
+    const RowBest rb = row_best(gpart, gconn, o, len, p, k);
     if (v < n) {
         const int64_t pc = rb.pc, bc = rb.bc, wd = rb.wd;
         const int32_t b = rb.b, np = rb.np;
@@ -1121,7 +1122,8 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
                      const int32_t *__restrict__ und, const int32_t *__restrict__ d_nu, int32_t k,
                      int32_t *__restrict__ K, int32_t *__restrict__ V, int32_t *__restrict__ dest,
                      int32_t *__restrict__ d_cnt, int32_t *__restrict__ pstart, int32_t *__restrict__ pend,
-                     unsigned long long *tile_status, hp::LbCtl *lb, unsigned *status)
+                     unsigned long long *tile_status, hp::LbCtl *lb, unsigned *status,
+                     const int8_t *__restrict__ ufl)
 {
     __shared__ int32_t s_scan[RB_TILE / 32 + 2];
     __shared__ int32_t s_excl;
@@ -1160,7 +1162,7 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
                 if (q < 0) break;
                 const int32_t cq = gconn[j];
                 if (q == p) pc = cq;
-                if ((int64_t)pw[q] < maxp[q] && cq > bc) { bc = cq; b = q; }
+                if (ufl[q] && cq > bc) { bc = cq; b = q; }
             }
         }
         unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
@@ -1170,12 +1172,13 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
             const int32_t so = __shfl_sync(HP_FULL_MASK, o, src), sl = __shfl_sync(HP_FULL_MASK, len, src);
             const int32_t sp = __shfl_sync(HP_FULL_MASK, p, src);
             int32_t lpc = 0, lbc = 0, lb = -1;
+            const bool dense = sl == k;   // entry j is part j
             for (int32_t j = lane; j < sl; j += 32) {
-                const int32_t q = gpart[so + j];
+                const int32_t q = dense ? j : gpart[so + j];
                 if (q < 0) break;   // padding runs to the end of the row
                 const int32_t cq = gconn[so + j];
                 if (q == sp) lpc = cq;
-                if ((int64_t)pw[q] < maxp[q] && cq > lbc) { lbc = cq; lb = q; }
+                if (ufl[q] && cq > lbc) { lbc = cq; lb = q; }
             }
             lpc = hp::warp_sum(lpc);
 #pragma unroll
@@ -1500,6 +1503,7 @@ struct RefineBufs {
     int8_t *lock;
     int32_t *K, *V, *K2, *V2, *pre, *P, *sp;
     int32_t *pstart, *pend, *und, *ev_end, *es, *ee;
+    int8_t *ufl;   // per part: pw < maxp (a weak pass's destination rule), set by ctl_begin
     unsigned long long *pw;
     const int64_t *opt, *maxp;
     int32_t G;          // gain-row entries of the level
@@ -1600,7 +1604,7 @@ int rank_candidates(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, int32_t
     if (ct > c->lb_cap || 2 * rt > c->lb_cap) return HP_ERR_INTERNAL;
     HP_LAUNCH(c, rb_candidates_kernel<STRONG>, (unsigned)ct, RB_TILE, 0, n, g.where, g.vwgt, B.pw, B.maxp, B.opt,
               B.goff, B.gpart, B.gconn, B.und, (const int32_t *)&sc[S_NU], k, B.K, B.V, B.dest, d_cnt, B.pstart,
-              B.pend, c->lb_status, c->lb_ctl, c->d_status);
+              B.pend, c->lb_status, c->lb_ctl, c->d_status, B.ufl);
     bool in_tmp = false;
     HP_TRY(hp_sort_pairs(c, B.K, B.V, B.K2, B.V2, n, d_cnt, key_bits_for(k), &in_tmp));
     *Ks = in_tmp ? B.K2 : B.K;
@@ -1769,14 +1773,17 @@ __device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2
 __global__ void __launch_bounds__(1024)
 ctl_begin_kernel(const RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle hmode, int graph, int32_t k,
                  const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
-                 int32_t *__restrict__ und)
+                 int32_t *__restrict__ und, int8_t *__restrict__ ufl)
 {
     __shared__ int32_t s_scan[1024 / 32 + 2];
     if (threadIdx.x < S_PASS_END) sc[threadIdx.x] = 0;
     const int mode = s->mode;
     if (graph && threadIdx.x == 0) cudaGraphSetConditional(hmode, (unsigned)mode);
     __syncthreads();
-    if (mode == 1) undersized_block(k, pw, maxp, und, (int32_t *)&sc[S_NU], s_scan);
+    if (mode == 1) {
+        undersized_block(k, pw, maxp, und, (int32_t *)&sc[S_NU], s_scan);
+        for (int32_t q = threadIdx.x; q < k; q += blockDim.x) ufl[q] = (int64_t)pw[q] < maxp[q];
+    }
 }
 
 __global__ void save_best_kernel(const RefineCtl *s, int32_t n, const int32_t *__restrict__ where,
@@ -1820,10 +1827,10 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
         if (both_lp || learned_pass)
             HP_LAUNCH(c, lp_select_learned_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, g.xadj,
                       B.lock, P.finest ? 1 : 0, B.pw, B.maxp, B.opt, c->mlp_params, c->mlp_threshold, B.dest,
-                      B.pregain, &sc[S_NCAND], gate);
+                      B.pregain, &sc[S_NCAND], gate, k);
         if (both_lp || !learned_pass)
             HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
-                      P.finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND], gate);
+                      P.finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND], gate, k);
         if (P.recording)
             HP_LAUNCH(c, log_candidates_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, g.xadj,
                       P.finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.oldp, c->log_x, c->log_v,
@@ -2048,7 +2055,7 @@ refine_small_kernel(SmallLevel a)
                     o = a.goff[v];
                     len = a.goff[v + 1] - o;
                 }
-                const RowBest rb = row_best(a.gpart, a.gconn, o, len, p);
+                const RowBest rb = row_best(a.gpart, a.gconn, o, len, p, k);
                 int cand = 0;
                 int32_t g = NEG, d = p;
                 float f[HP_MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -2436,7 +2443,7 @@ int run_passes_graph(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P,
     tick(t, 0);
     const int l0 = c->launches;
     HP_TRY(capture_into(c, body, [&]() -> int {
-        HP_LAUNCH(c, ctl_begin_kernel, 1, 1024, 0, P.ctl, c->d_scal, hmode, 1, P.k, B.pw, B.maxp, B.und);
+        HP_LAUNCH(c, ctl_begin_kernel, 1, 1024, 0, P.ctl, c->d_scal, hmode, 1, P.k, B.pw, B.maxp, B.und, B.ufl);
         cudaStreamCaptureStatus cs;
         cudaGraph_t capg = nullptr;
         const cudaGraphNode_t *deps = nullptr;
@@ -2509,6 +2516,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     int32_t **k_arrays[] = {&B.pstart, &B.pend, &B.und, &B.ev_end, &B.es, &B.ee};
     for (auto pp : k_arrays) *pp = ralloc_t<int32_t>(c, k);
     B.lock = ralloc_t<int8_t>(c, n);
+    B.ufl = ralloc_t<int8_t>(c, k);
     B.pw = ralloc_t<unsigned long long>(c, k);
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
     // at most m / (chunk_deg + 1) rows are longer than chunk_deg (the long-row
@@ -2638,7 +2646,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));
         while (h.cont) {
             HP_LAUNCH(c, ctl_begin_kernel, 1, 1024, 0, ctl, sc, cudaGraphConditionalHandle{}, 0, k, B.pw, B.maxp,
-                      B.und);
+                      B.und, B.ufl);
             HP_TRY(pass_propose(c, g, B, P, h.mode, h.learned_pass != 0, false));
             HP_TRY(pass_apply(c, g, B, P, 0, 0));
             HP_TRY(hp_read_scalars(c, ctl, sizeof(h), &h));
