@@ -92,6 +92,7 @@ TUNING_FIELDS = [
     "small_level_n",
     "chunk_deg",
     "trial_cta_n",
+    "contract_smem_cn",
 ]
 
 TUNING_DEFAULTS = {
@@ -108,6 +109,7 @@ TUNING_DEFAULTS = {
     "small_level_n": 4096,
     "chunk_deg": 4096,
     "trial_cta_n": 512,
+    "contract_smem_cn": 49152,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -130,6 +132,7 @@ def tuning_violation(t: dict):
         ("small_level_n", 0, 32768),
         ("chunk_deg", t["gain_thread_deg"], TUNE_DEG_MAX),
         ("trial_cta_n", 1, TUNE_DEG_MAX),
+        ("contract_smem_cn", 0, 49152),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -138,7 +141,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 3)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 2)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

@@ -513,6 +513,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->small_level_n = 4096;
     t->chunk_deg = 4096;
     t->trial_cta_n = 512;
+    t->contract_smem_cn = HP_TUNE_SMEM_CN_MAX;
 }
 
 namespace {
@@ -533,6 +534,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.small_level_n, 0, HP_TUNE_SMALL_LEVEL_MAX)) return "small_level_n";
     if (!in(t.chunk_deg, t.gain_thread_deg, HP_TUNE_DEG_MAX)) return "chunk_deg";
     if (!in(t.trial_cta_n, 1, HP_TUNE_DEG_MAX)) return "trial_cta_n";
+    if (!in(t.contract_smem_cn, 0, HP_TUNE_SMEM_CN_MAX)) return "contract_smem_cn";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;

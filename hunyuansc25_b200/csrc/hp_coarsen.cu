@@ -1010,24 +1010,40 @@ constexpr size_t cta_radix_smem() { return sizeof(unsigned long long) * 2 * CAP 
 // in a per-CTA global slab (dw: cn ints, bm: cn/32 words, bm2: cn/1024 words;
 // zero on entry/exit).  A row with len * ratio < cn/32 words walks the occupied
 // words through the second-level bitmap; a denser row scans the bitmap.
-template <int NT>
+// SMEM: the accumulators live in the CTA's shared memory (cn + cn/32 + cn/1024
+// words, zeroed here), for levels whose coarse vertex count fits; every row of
+// the list longer than min_len is taken.  Otherwise they are the CTA's global
+// slab and only the rows above XROW_MAX are taken (min_len).
+template <int NT, bool SMEM>
 __global__ void __launch_bounds__(NT)
 contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                       ContractSrc src, const int32_t *__restrict__ toff, int32_t *__restrict__ tk,
                       int32_t *__restrict__ tw, int32_t *__restrict__ ucnt, int32_t cn,
-                      int32_t *slab_w, unsigned *slab_bm, unsigned *slab_bm2, int32_t ratio)
+                      int32_t *slab_w, unsigned *slab_bm, unsigned *slab_bm2, int32_t ratio, int32_t min_len)
 {
+    extern __shared__ int32_t dsm_acc[];
     __shared__ int32_t s_scan[NT / 32 + 2];
-    int32_t *dw = slab_w + (int64_t)blockIdx.x * cn;
-    unsigned *bm = slab_bm + (int64_t)blockIdx.x * ((cn + 31) / 32);
-    unsigned *bm2 = slab_bm2 + (int64_t)blockIdx.x * ((cn + 1023) / 1024);
+    const int32_t nw = (cn + 31) / 32, nw2 = (cn + 1023) / 1024;
+    int32_t *dw;
+    unsigned *bm, *bm2;
+    if (SMEM) {
+        dw = dsm_acc;
+        bm = (unsigned *)(dsm_acc + cn);
+        bm2 = bm + nw;
+        for (int32_t i = threadIdx.x; i < cn + nw + nw2; i += NT) dsm_acc[i] = 0;
+        __syncthreads();
+    } else {
+        dw = slab_w + (int64_t)blockIdx.x * cn;
+        bm = slab_bm + (int64_t)blockIdx.x * nw;
+        bm2 = slab_bm2 + (int64_t)blockIdx.x * nw2;
+    }
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t c = list[li];
         RowInfo r;
         int32_t len;
         src.row(c, r, len);
-        if (len <= XROW_MAX) continue;   // contract_cta_radix_kernel<1024, XROW_MAX>'s row
+        if (len <= min_len) continue;   // another kernel's row
         const bool two_level = (int64_t)len * ratio < ((int64_t)cn + 31) / 32;
         for (int32_t i0 = threadIdx.x; i0 < len; i0 += 4 * NT) {
             int32_t a[4], wq[4];
@@ -1230,7 +1246,20 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
             HP_LAUNCH(c, contract_warp_radix_kernel,
                       (unsigned)std::min<int64_t>((h.cnt[0] + WROW_WARPS - 1) / WROW_WARPS, c->sm_count * 6),
                       32 * WROW_WARPS, 0, lists, &counts[0], src, toff, tk, tw, ucnt, kbits);
-        if (h.cnt[1] > 0) {
+        // a level whose coarse ids fit a shared-memory dense accumulator merges
+        // every long row there (one atomic per entry, ordered extraction)
+        const bool smem_dense = cn <= c->tune.contract_smem_cn;
+        if (smem_dense) {
+            const size_t acc = sizeof(int32_t) * ((size_t)cn + (cn + 31) / 32 + (cn + 1023) / 1024);
+            for (int cls = 1; cls <= 2; cls++)
+                if (h.cnt[cls] > 0)
+                    HP_LAUNCH(c, (contract_dense_kernel<1024, true>),
+                              (unsigned)std::min<int64_t>(h.cnt[cls], c->sm_count), 1024, acc,
+                              lists + cls * (int64_t)cn, &counts[cls], src, toff, tk, tw, ucnt, cn,
+                              (int32_t *)nullptr, (unsigned *)nullptr, (unsigned *)nullptr,
+                              c->tune.dense_sparse_ratio, 0);
+        }
+        if (!smem_dense && h.cnt[1] > 0) {
             HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>),
                       (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 8), CROW_THREADS,
                       (cta_radix_smem<CROW_THREADS, MROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits,
@@ -1241,12 +1270,12 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
                           (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt,
                           kbits, MROW_MAX);
         }
-        if (h.cnt[2] > 0)
+        if (!smem_dense && h.cnt[2] > 0)
             HP_LAUNCH(c, (contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>),
                       (unsigned)std::min<int64_t>(h.cnt[2], c->sm_count), XROW_THREADS,
                       (cta_radix_smem<XROW_THREADS, XROW_MAX>()), lists + 2 * (int64_t)cn, &counts[2], src, toff, tk,
                       tw, ucnt, kbits, 0);
-        if (h.maxlen > XROW_MAX) {
+        if (!smem_dense && h.maxlen > XROW_MAX) {
             // slab per CTA: cn ints + cn/32 + cn/1024 words; bounded to ~512 MB
             const int64_t nw = ((int64_t)cn + 31) / 32, nw2 = ((int64_t)cn + 1023) / 1024;
             int64_t slab = (int64_t)cn * 4 + nw * 4 + nw2 * 4;
@@ -1259,8 +1288,8 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
             HP_CUDA(cudaMemsetAsync(sw, 0, sizeof(int32_t) * (size_t)(nb * cn), c->stream));
             HP_CUDA(cudaMemsetAsync(sbm, 0, sizeof(unsigned) * (size_t)(nb * nw), c->stream));
             HP_CUDA(cudaMemsetAsync(sbm2, 0, sizeof(unsigned) * (size_t)(nb * nw2), c->stream));
-            HP_LAUNCH(c, contract_dense_kernel<1024>, (unsigned)nb, 1024, 0, lists + 2 * (int64_t)cn,
-                      &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm, sbm2, c->tune.dense_sparse_ratio);
+            HP_LAUNCH(c, (contract_dense_kernel<1024, false>), (unsigned)nb, 1024, 0, lists + 2 * (int64_t)cn,
+                      &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm, sbm2, c->tune.dense_sparse_ratio, XROW_MAX);
         }
     }
     // short rows + coarse xadj in one ordered pass, then the long rows' copies
@@ -1298,6 +1327,9 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
 
 int hp_coarsen_init()
 {
+    HP_CUDA(cudaFuncSetAttribute(contract_dense_kernel<1024, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(int32_t) * (HP_TUNE_SMEM_CN_MAX + (HP_TUNE_SMEM_CN_MAX + 31) / 32 +
+                                                          (HP_TUNE_SMEM_CN_MAX + 1023) / 1024))));
     HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_radix_smem<CROW_THREADS, MROW_MAX>()));

@@ -171,7 +171,10 @@ typedef struct hp_tuning {
     int32_t trial_cta_n;         /* initial bisection: a recursion depth whose largest
                                     subgraph has at least this many vertices runs
                                     a CTA per trial instead of a warp             [1, 2^24]     512 */
-    int32_t reserved[3];         /* zero */
+    int32_t contract_smem_cn;    /* contraction: a level with at most this many coarse
+                                    vertices merges its long rows in a shared-memory
+                                    dense accumulator instead of radix sorts      [0, 49152]    49152 */
+    int32_t reserved[2];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);

@@ -35,7 +35,7 @@ def test_library_defaults_match_python():
     t = HpTuning()
     lib.hp_tuning_default(C.byref(t))
     assert t.as_dict() == TUNING_DEFAULTS
-    assert list(t.reserved) == [0] * 3
+    assert list(t.reserved) == [0] * 2
     assert tuning_violation(TUNING_DEFAULTS) is None
 
 
@@ -44,7 +44,7 @@ def test_library_defaults_match_python():
     ("contract_thread_row", 7), ("contract_warp_row", 257), ("contract_cta_row", 4097), ("contract_cta_row", 100),
     ("gain_thread_deg", 33), ("gain_hub_deg", 31), ("warp_dense_k", 1025), ("warp_dense_k", -1),
     ("grid_ctas_per_sm", 0), ("grid_ctas_per_sm", 33), ("dense_sparse_ratio", 0),
-    ("small_level_n", -1), ("small_level_n", 32769), ("chunk_deg", 31), ("trial_cta_n", 0),
+    ("small_level_n", -1), ("small_level_n", 32769), ("chunk_deg", 31), ("trial_cta_n", 0), ("contract_smem_cn", 49153),
 ])
 def test_violations(field, value):
     t = dict(TUNING_DEFAULTS)
