@@ -335,7 +335,9 @@ def main():
     if args.learned or args.compare_learned:
         mparams, mthr, _ = learn.load_params()
         ctx.mlp_set_params(mparams, mthr if args.learned_threshold is None else args.learned_threshold)
-    opt = default_options(coarsen_to=spec["coarsen_to"], profile=1, learned=1 if args.learned else 0)
+    # the timed steps run without the kernel-class profiler; one extra step
+    # after the timed region records the classes
+    opt = default_options(coarsen_to=spec["coarsen_to"], profile=0, learned=1 if args.learned else 0)
     xadj, adj, vw, ew = (torch.from_numpy(a).to(dev) for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt))
     part = torch.empty(g.nvtxs, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
@@ -381,34 +383,32 @@ def main():
     job_ms = float(t.item())
     value = world * args.steps * m_und / (job_ms / 1000.0)
 
-    # Kernel classes from the library's CUDA-event profile.  Coarsening, gain-table
-    # builds and bisection are timed live in the timed steps; the LP and gain-row
-    # rebuild launches of the refinement passes run inside CUDA graphs there, so
-    # they come from one extra step with eager passes (which also gives the
-    # graph-vs-eager time of the whole partition).
-    prof_ms = np.zeros(8)
-    prof_bytes = np.zeros(8)
-    prof_launch = np.zeros(8)
-    launches = 0
-    for s in stats:
-        prof_ms += np.array(list(s.prof_ms))
-        prof_bytes += np.array(list(s.prof_bytes), dtype=np.float64)
-        prof_launch += np.array(list(s.prof_launches))
-        launches += s.kernel_launches
-    prof_ms /= args.steps
-    prof_bytes /= args.steps
-    prof_launch /= args.steps
-    eopt = default_options(coarsen_to=spec["coarsen_to"], profile=1, eager=1, learned=opt.learned)
-    with torch.cuda.stream(stream):
-        flush.zero_()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    _, ecut = step(eopt)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    eager_ms = e0.elapsed_time(e1)
-    est = ctx.stats()
+    launches = sum(s.kernel_launches for s in stats)
+
+    def one_step(o):
+        """One untimed-region step on the library's stream: (device ms, cut, stats)."""
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        _, c = step(o)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), c, ctx.stats()
+
+    # Kernel classes from the library's CUDA-event profile, recorded after the
+    # timed region.  Coarsening, gain-table builds and bisection come from one
+    # profiled step with graphed passes; the LP, gain-row rebuild and rebalance
+    # launches run inside the pass graphs there, so they come from one profiled
+    # step with eager passes.  The graph-vs-eager comparison times one eager step
+    # without the profiler.
+    _, _, pst = one_step(default_options(coarsen_to=spec["coarsen_to"], profile=1, learned=opt.learned))
+    eager_ms, ecut, _ = one_step(default_options(coarsen_to=spec["coarsen_to"], eager=1, learned=opt.learned))
+    _, _, est = one_step(default_options(coarsen_to=spec["coarsen_to"], profile=1, eager=1, learned=opt.learned))
+    prof_ms = np.array(list(pst.prof_ms), dtype=np.float64)
+    prof_bytes = np.array(list(pst.prof_bytes), dtype=np.float64)
+    prof_launch = np.array(list(pst.prof_launches), dtype=np.float64)
     source = {}
     for i in range(8):
         if PROF_NAMES[i] in ("lp", "rebuild", "rebalance"):
@@ -417,7 +417,7 @@ def main():
             prof_launch[i] = est.prof_launches[i]
             source[i] = "eager profiled step"
         else:
-            source[i] = "timed steps"
+            source[i] = "profiled step"
     with_bytes = [i for i in range(8) if prof_bytes[i] > 0]
     dom = max(with_bytes, key=lambda i: prof_ms[i]) if with_bytes else 0
     peak, peak_kind = load_peaks()
@@ -442,20 +442,23 @@ def main():
 
     learned_cmp = None
     if args.compare_learned:
+        # the learned steps are timed exactly as the plain timed steps above
         lopt = default_options(coarsen_to=spec["coarsen_to"], learned=1)
-        lms, lcut = [], None
-        for i in range(args.warmup + args.steps):
+        for _ in range(args.warmup):
+            step(lopt)
+        torch.cuda.synchronize()
+        levs, lcut = [], None
+        for _ in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            _, lcut = ctx.partition_device(xadj, adj, spec["k"], vw, ew, spec["ub"], options=lopt, stream=stream,
-                                           part=part)
+            _, lcut = step(lopt)
             e1.record(stream)
-            torch.cuda.synchronize()
-            if i >= args.warmup:
-                lms.append(e0.elapsed_time(e1))
+            levs.append((e0, e1))
+        torch.cuda.synchronize()
+        lms = [a.elapsed_time(b) for a, b in levs]
         plain_ms = job_ms / args.steps
         learned_ms = sum(lms) / len(lms)
         learned_cmp = {"plain_ms": round(plain_ms, 3), "learned_ms": round(learned_ms, 3),
