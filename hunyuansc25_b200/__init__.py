@@ -74,6 +74,11 @@ def _p32(a):
     return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int32))
 
 
+class BatchInput:
+    """Concatenated host arrays of many graphs in hp_partition_batch's layout
+    (Context.prepare_batch), with the output buffers."""
+
+
 class Context:
     """One device arena + per-call state (reentrant replacement of the
     reference's file-scope globals, hunyuangraph_GPU_memory.h:18-32)."""
@@ -144,30 +149,44 @@ class Context:
         _check(rc, "hp_partition_device")
         return part[:n], cut.value
 
-    def partition_batch(self, graphs, nparts, ubfactor=1.03, options=None):
-        """Partition many independent graphs; returns (list of part arrays, cuts)."""
+    def prepare_batch(self, graphs, nparts, ubfactor=1.03) -> "BatchInput":
+        """The concatenated host arrays of hp_partition_batch for these graphs
+        (built once; partition_prepared() can run them many times)."""
         G = len(graphs)
-        nparts = np.ascontiguousarray(np.broadcast_to(np.asarray(nparts, np.int32), (G,)))
-        ub = np.ascontiguousarray(np.broadcast_to(np.asarray(ubfactor, np.float32), (G,)))
-        vtx = np.zeros(G + 1, np.int64)
-        edg = np.zeros(G + 1, np.int64)
+        b = BatchInput()
+        b.G = G
+        b.nparts = np.ascontiguousarray(np.broadcast_to(np.asarray(nparts, np.int32), (G,)))
+        b.ub = np.ascontiguousarray(np.broadcast_to(np.asarray(ubfactor, np.float32), (G,)))
+        b.vtx = np.zeros(G + 1, np.int64)
+        b.edg = np.zeros(G + 1, np.int64)
         for i, g in enumerate(graphs):
-            vtx[i + 1] = vtx[i] + g.nvtxs
-            edg[i + 1] = edg[i] + g.nedges
-        xadj = np.concatenate([g.xadj for g in graphs]).astype(np.int32)
-        adj = np.concatenate([g.adjncy for g in graphs]).astype(np.int32)
-        vw = np.concatenate([g.vwgt for g in graphs]).astype(np.int32)
-        ew = np.concatenate([g.adjwgt for g in graphs]).astype(np.int32)
-        part = np.empty(max(int(vtx[-1]), 1), np.int32)
-        cuts = np.zeros(G, np.int64)
+            b.vtx[i + 1] = b.vtx[i] + g.nvtxs
+            b.edg[i + 1] = b.edg[i] + g.nedges
+        b.xadj = np.concatenate([g.xadj for g in graphs]).astype(np.int32)
+        b.adj = np.concatenate([g.adjncy for g in graphs]).astype(np.int32)
+        b.vw = np.concatenate([g.vwgt for g in graphs]).astype(np.int32)
+        b.ew = np.concatenate([g.adjwgt for g in graphs]).astype(np.int32)
+        b.part = np.empty(max(int(b.vtx[-1]), 1), np.int32)
+        b.cuts = np.zeros(G, np.int64)
+        return b
+
+    def partition_prepared(self, b: "BatchInput", options=None):
+        """One hp_partition_batch call on prepared arrays; returns (list of part
+        arrays, cuts) -- views of the BatchInput's output arrays."""
         opt = options if options is not None else default_options()
         I64 = C.POINTER(C.c_int64)
-        rc = self.lib.hp_partition_batch(self.h, G, vtx.ctypes.data_as(I64), edg.ctypes.data_as(I64),
-                                         _p32(xadj), _p32(adj), _p32(vw), _p32(ew), _p32(nparts),
-                                         ub.ctypes.data_as(C.POINTER(C.c_float)), C.byref(opt),
-                                         _p32(part), cuts.ctypes.data_as(I64))
+        rc = self.lib.hp_partition_batch(self.h, b.G, b.vtx.ctypes.data_as(I64), b.edg.ctypes.data_as(I64),
+                                         _p32(b.xadj), _p32(b.adj), _p32(b.vw), _p32(b.ew), _p32(b.nparts),
+                                         b.ub.ctypes.data_as(C.POINTER(C.c_float)), C.byref(opt),
+                                         _p32(b.part), b.cuts.ctypes.data_as(I64))
         _check(rc, "hp_partition_batch")
-        return [part[vtx[i]:vtx[i + 1]] for i in range(G)], cuts
+        return [b.part[b.vtx[i]:b.vtx[i + 1]] for i in range(b.G)], b.cuts
+
+    def partition_batch(self, graphs, nparts, ubfactor=1.03, options=None):
+        """Partition many independent graphs; returns (list of part arrays, cuts)."""
+        b = self.prepare_batch(graphs, nparts, ubfactor)
+        parts, cuts = self.partition_prepared(b, options)
+        return [p.copy() for p in parts], cuts.copy()
 
     def stats(self) -> HpStats:
         st = HpStats()

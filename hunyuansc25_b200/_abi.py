@@ -93,6 +93,7 @@ TUNING_FIELDS = [
     "chunk_deg",
     "trial_cta_n",
     "contract_smem_cn",
+    "batch_workers",
 ]
 
 TUNING_DEFAULTS = {
@@ -110,6 +111,7 @@ TUNING_DEFAULTS = {
     "chunk_deg": 4096,
     "trial_cta_n": 512,
     "contract_smem_cn": 49152,
+    "batch_workers": 16,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -133,6 +135,7 @@ def tuning_violation(t: dict):
         ("chunk_deg", t["gain_thread_deg"], TUNE_DEG_MAX),
         ("trial_cta_n", 1, TUNE_DEG_MAX),
         ("contract_smem_cn", 0, 49152),
+        ("batch_workers", 1, 64),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -141,7 +144,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 2)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 1)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

@@ -514,6 +514,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->chunk_deg = 4096;
     t->trial_cta_n = 512;
     t->contract_smem_cn = HP_TUNE_SMEM_CN_MAX;
+    t->batch_workers = 16;
 }
 
 namespace {
@@ -535,6 +536,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.chunk_deg, t.gain_thread_deg, HP_TUNE_DEG_MAX)) return "chunk_deg";
     if (!in(t.trial_cta_n, 1, HP_TUNE_DEG_MAX)) return "trial_cta_n";
     if (!in(t.contract_smem_cn, 0, HP_TUNE_SMEM_CN_MAX)) return "contract_smem_cn";
+    if (!in(t.batch_workers, 1, 64)) return "batch_workers";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;
@@ -819,7 +821,7 @@ HP_API int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *v
         if (vtxdist[gi + 1] < vtxdist[gi] || edgedist[gi + 1] < edgedist[gi]) return HP_ERR_INVALID_ARG;
         if (vtxdist[gi + 1] - vtxdist[gi] > INT32_MAX - 1) return HP_ERR_UNSUPPORTED;
     }
-    const int nworkers = (int)std::min<int64_t>(ngraphs, 16);
+    const int nworkers = (int)std::min<int64_t>(ngraphs, ctx->tune.batch_workers);
     HP_CUDA(cudaSetDevice(ctx->device));
     while ((int)ctx->workers.size() < nworkers) {
         hp_context *w = nullptr;
@@ -827,6 +829,14 @@ HP_API int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *v
         ctx->workers.push_back(w);
     }
     for (hp_context *w : ctx->workers) w->tune = ctx->tune;
+    // The workers run their levels' pass loops eagerly: sixteen host threads that
+    // capture and instantiate a CUDA graph per level contend for the driver, and
+    // the graphs of small graphs' levels never amortise (the small-level kernel
+    // still takes the small levels).  Results are the same in both loop modes.
+    hp_options wopt;
+    if (opt) wopt = *opt;
+    else hp_options_default(&wopt);
+    wopt.eager = 1;
     std::vector<int32_t> order(ngraphs);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
@@ -846,7 +856,7 @@ HP_API int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *v
             const int64_t v0 = vtxdist[gi], n = vtxdist[gi + 1] - v0, e0 = edgedist[gi];
             int64_t cut = 0;
             int rc = hp_partition(w, (int32_t)n, xadj + v0 + gi, adjncy + e0, vwgt ? vwgt + v0 : nullptr,
-                                  adjwgt ? adjwgt + e0 : nullptr, nparts[gi], nullptr, ubfactor[gi], opt,
+                                  adjwgt ? adjwgt + e0 : nullptr, nparts[gi], nullptr, ubfactor[gi], &wopt,
                                   part + v0, &cut);
             if (rc != HP_OK) {
                 int expected = HP_OK;

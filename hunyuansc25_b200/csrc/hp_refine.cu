@@ -2586,9 +2586,10 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     const bool use_graph = graph_loop(c);
     RefineCtl h{};
-    // small levels: the whole pass loop in one CTA (same rule, same result)
+    // small levels: the whole pass loop in one CTA (same rule, same result), in
+    // either loop mode unless the per-pass move log or pass log is on
     const int32_t small_n = c->tune.small_level_n;
-    const bool small_level = use_graph && n <= small_n && k <= HP_TUNE_WARP_DENSE_K_MAX &&
+    const bool small_level = !recording && !dbg && n <= small_n && k <= HP_TUNE_WARP_DENSE_K_MAX &&
                              g.m <= 16 * (int64_t)small_n;
     if (small_level) {
         SmallLevel a{};

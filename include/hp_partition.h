@@ -174,7 +174,9 @@ typedef struct hp_tuning {
     int32_t contract_smem_cn;    /* contraction: a level with at most this many coarse
                                     vertices merges its long rows in a shared-memory
                                     dense accumulator instead of radix sorts      [0, 49152]    49152 */
-    int32_t reserved[2];         /* zero */
+    int32_t batch_workers;       /* hp_partition_batch: worker contexts (streams) that
+                                    partition graphs concurrently                 [1, 64]       16 */
+    int32_t reserved[1];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);

@@ -41,3 +41,15 @@ def test_batch_error_reported(ctx):
         ctx.partition_batch([good, bad], [2, 2], 1.03)
     parts, cuts = ctx.partition_batch([good], [2], 1.03)
     assert cuts[0] == oracle.edgecut(good, parts[0])
+
+
+def test_prepared_batch_matches_batch_call(ctx):
+    gs = [graphs.batch_graph("rmat" if i % 2 else "grid2d", 2000 + 500 * i, seed=300 + i) for i in range(5)]
+    ks = [2, 4, 8, 16, 32]
+    parts, cuts = ctx.partition_batch(gs, ks, 1.03)
+    b = ctx.prepare_batch(gs, ks, 1.03)
+    for _ in range(2):   # the prepared arrays serve repeated calls
+        p2, c2 = ctx.partition_prepared(b)
+        assert [int(x) for x in c2] == [int(x) for x in cuts]
+        for a, q in zip(parts, p2):
+            assert np.array_equal(a, q)

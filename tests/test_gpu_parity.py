@@ -108,15 +108,21 @@ def test_full_grid3d_128_k64(ctx):
 
 def test_eager_passes_match_oracle(ctx):
     """The eager pass loop (one launch per kernel, a host read per pass) against
-    the oracle, on the graphs the graph-mode tests above use."""
-    compare_runs(ctx, graphs.config_grid2d(), 8, coarsen_to=160, eager=1)
-    compare_runs(ctx, graphs.rmat(14, 16, seed=3, wmin=1, wmax=100), 256, eager=1)
+    the oracle, on the graphs the graph-mode tests above use; every level on the
+    multi-kernel passes (the one-CTA small-level loop off)."""
+    ctx.set_tuning(small_level_n=0)
+    try:
+        compare_runs(ctx, graphs.config_grid2d(), 8, coarsen_to=160, eager=1)
+        compare_runs(ctx, graphs.rmat(14, 16, seed=3, wmin=1, wmax=100), 256, eager=1)
+    finally:
+        ctx.set_tuning(None)
 
 
 @pytest.mark.parametrize("name", ["grid3d_48", "rmat13_hubs", "rgg17", "star"])
 def test_graph_loop_equals_eager_loop(ctx, name):
-    """CUDA-graph pass loop (device-side WHILE/SWITCH control) and the eager loop
-    give the same partition, cut and pass count."""
+    """CUDA-graph pass loop (device-side WHILE/SWITCH control, the one-CTA loop
+    on the small levels) and the eager multi-kernel loop on every level give the
+    same partition, cut and pass count."""
     if name == "grid3d_48":
         g, k = graphs.grid3d(48, 48, 48, seed=2, wmin=1, wmax=10), 64
     elif name == "rmat13_hubs":
@@ -131,7 +137,11 @@ def test_graph_loop_equals_eager_loop(ctx, name):
         adj = np.concatenate([np.arange(1, n), np.zeros(n - 1)]).astype(np.int32)
         g = graphs.Graph(xadj, adj, np.ones(n, np.int32), np.ones(2 * (n - 1), np.int32), "star")
         k = 16
-    pe, ce = ctx.partition_graph(g, k, options=default_options(eager=1))
+    ctx.set_tuning(small_level_n=0)
+    try:
+        pe, ce = ctx.partition_graph(g, k, options=default_options(eager=1))
+    finally:
+        ctx.set_tuning(None)
     se = ctx.stats()
     pg, cg = ctx.partition_graph(g, k, options=default_options(eager=0))
     sg = ctx.stats()
