@@ -675,6 +675,32 @@ __global__ void log_label_kernel(int64_t r0, int64_t r1, const int32_t *__restri
     if (r < r1) ly[r] = (lacc[r] && where[lv[r]] == ld[r]) ? 1.f : 0.f;
 }
 
+// Where a pass's moves go: the move list and count, the old part per move, and
+// the cut-change sum c1 (conn(to) - conn(from) of every move, read from the mover's
+// own gain row before any move applies).  The kernels that decide the moves append
+// them through move_append and add the c1 terms per block, so no separate pass
+// over the moves precedes their application.
+struct MoveSink {
+    int32_t *moves, *oldp;
+    unsigned long long *d_nmoves, *d_c1;
+    const int32_t *goff, *gpart, *gconn;
+    int32_t k;
+};
+
+__device__ __forceinline__ int32_t row_conn(const int32_t *gp, const int32_t *gc, int32_t len, int32_t q,
+                                            int32_t k);
+
+// Appends the move of v from p to d; returns its c1 term.
+__device__ __forceinline__ long long move_append(const MoveSink &ms, int32_t v, int32_t p, int32_t d)
+{
+    const unsigned long long i = atomicAdd(ms.d_nmoves, 1ull);
+    ms.moves[i] = v;
+    ms.oldp[i] = p;
+    const int32_t o = ms.goff[v], len = ms.goff[v + 1] - o;
+    return (long long)row_conn(ms.gpart + o, ms.gconn + o, len, d, ms.k) -
+           row_conn(ms.gpart + o, ms.gconn + o, len, p, ms.k);
+}
+
 __device__ __forceinline__ long long ab_change(int32_t v, int32_t g, int32_t p, int32_t b,
                                                int32_t u, int32_t w, const int32_t *pregain,
                                                const int32_t *dest, const int32_t *where)
@@ -733,24 +759,30 @@ __global__ void __launch_bounds__(256)
 afterburner_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                          const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                          const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
-                         int8_t *__restrict__ lock, const unsigned long long *d_ncand,
-                         int32_t *__restrict__ moves, unsigned long long *d_nmoves, int32_t bigd)
+                         int8_t *__restrict__ lock, const unsigned long long *d_ncand, MoveSink ms, int32_t bigd)
 {
     if (*d_ncand == 0ull) return;
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    const int32_t b0 = xadj[v], e0 = xadj[v + 1];
-    if (e0 - b0 > bigd) return;
-    const int32_t g = pregain[v];
-    int8_t sel = 0;
-    if (g != NEG) {
-        const int32_t p = where[v], b = dest[v];
-        long long ch = 0;
-        for (int32_t j = b0; j < e0; j++) ch += ab_change(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where);
-        sel = ((long long)g + ch >= 0);
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    long long c1 = 0;
+    if (v < n) {
+        const int32_t b0 = xadj[v], e0 = xadj[v + 1];
+        if (e0 - b0 <= bigd) {
+            const int32_t g = pregain[v];
+            int8_t sel = 0;
+            int32_t p = 0, b = 0;
+            if (g != NEG) {
+                p = where[v];
+                b = dest[v];
+                long long ch = 0;
+                for (int32_t j = b0; j < e0; j++)
+                    ch += ab_change(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where);
+                sel = ((long long)g + ch >= 0);
+            }
+            lock[v] = sel;
+            if (sel) c1 = move_append(ms, v, p, b);
+        }
     }
-    lock[v] = sel;
-    if (sel) moves[atomicAdd(d_nmoves, 1ull)] = v;
+    hp::block_add_to<256>(c1, ms.d_c1);
 }
 
 __global__ void __launch_bounds__(256)
@@ -758,29 +790,33 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
                        const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                        const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                        const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
-                       int8_t *__restrict__ lock, const unsigned long long *d_ncand,
-                       int32_t *__restrict__ moves, unsigned long long *d_nmoves, int32_t chunkd)
+                       int8_t *__restrict__ lock, const unsigned long long *d_ncand, MoveSink ms,
+                       int32_t chunkd)
 {
     if (*d_ncand == 0ull) return;
     const int lane = threadIdx.x & 31;
     const int32_t cnt = *d_bigcnt;
+    long long c1 = 0;
     for (int64_t i = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; i < cnt;
          i += ((int64_t)gridDim.x * blockDim.x) >> 5) {
         const int32_t v = big[i];
         if (xadj[v + 1] - xadj[v] > chunkd) continue;   // chunked over the grid
         const int32_t g = pregain[v];
         int8_t sel = 0;
+        int32_t p = 0, b = 0;
         if (g != NEG) {
-            const int32_t p = where[v], b = dest[v];
+            p = where[v];
+            b = dest[v];
             long long ch = ab_row_sum(v, g, p, b, xadj[v] + lane, xadj[v + 1], 32, adjncy, adjwgt, pregain, dest, where);
             ch = hp::warp_sum64(ch);
             sel = ((long long)g + ch >= 0);
         }
         if (lane == 0) {
             lock[v] = sel;
-            if (sel) moves[atomicAdd(d_nmoves, 1ull)] = v;
+            if (sel) c1 += move_append(ms, v, p, b);
         }
     }
+    hp::block_add_to<256>(c1, ms.d_c1);
 }
 
 // ---- long rows (longer than chunk_deg): chunk plans ------------------------------
@@ -900,10 +936,12 @@ afterburner_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__res
 __global__ void afterburner_huge_final_kernel(const int32_t *__restrict__ huge, const int32_t *__restrict__ d_nhuge,
                                               const int32_t *__restrict__ pregain, const unsigned long long *d_ncand,
                                               unsigned long long *__restrict__ ab_acc, int8_t *__restrict__ lock,
-                                              int32_t *__restrict__ moves, unsigned long long *d_nmoves)
+                                              const int32_t *__restrict__ where, const int32_t *__restrict__ dest,
+                                              MoveSink ms)
 {
     if (*d_ncand == 0ull) return;
     const int32_t nh = *d_nhuge;
+    long long c1 = 0;
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += gridDim.x * blockDim.x) {
         const int32_t v = huge[i];
         const int32_t g = pregain[v];
@@ -911,8 +949,9 @@ __global__ void afterburner_huge_final_kernel(const int32_t *__restrict__ huge, 
         ab_acc[i] = 0ull;
         const int8_t sel = (g != NEG) && ((long long)g + tot >= 0);
         lock[v] = sel;
-        if (sel) moves[atomicAdd(d_nmoves, 1ull)] = v;
+        if (sel) c1 += move_append(ms, v, where[v], dest[v]);
     }
+    hp::block_add_to<256>(c1, ms.d_c1);
 }
 
 // ---- applying moves -------------------------------------------------------------
@@ -1277,16 +1316,20 @@ __global__ void rw_select_kernel(const int32_t *__restrict__ K, const int32_t *_
                                  const int32_t *__restrict__ d_cnt, const int32_t *__restrict__ pre,
                                  const int32_t *__restrict__ pstart,
                                  const unsigned long long *__restrict__ pw,
-                                 const int64_t *__restrict__ maxp, int32_t *__restrict__ moves,
-                                 unsigned long long *d_nmoves)
+                                 const int64_t *__restrict__ maxp, const int32_t *__restrict__ dest, MoveSink ms)
 {
     const int32_t cnt = *d_cnt;
+    long long c1 = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt;
          i += (int64_t)gridDim.x * blockDim.x) {
         int32_t p = K[i] >> 6;
         int64_t before = (int64_t)pre[i] - pre[pstart[p]];
-        if (before < (int64_t)pw[p] - maxp[p]) moves[atomicAdd(d_nmoves, 1ull)] = V[i];
+        if (before < (int64_t)pw[p] - maxp[p]) {
+            const int32_t v = V[i];
+            c1 += move_append(ms, v, p, dest[v]);
+        }
     }
+    hp::block_add_to<256>(c1, ms.d_c1);
 }
 
 // Evicted prefix of every overweight part: smallest e in (s, end] with
@@ -1471,10 +1514,10 @@ __device__ void cookie_cut_warp(int32_t k, const unsigned long long *__restrict_
 __global__ void rs_assign_kernel(int32_t k, const int32_t *__restrict__ P, const int32_t *__restrict__ d_np,
                                  const int32_t *__restrict__ V, const int32_t *__restrict__ es,
                                  const int32_t *__restrict__ ee, const int32_t *__restrict__ where,
-                                 int32_t *__restrict__ dest, int32_t *__restrict__ moves,
-                                 unsigned long long *d_nmoves)
+                                 int32_t *__restrict__ dest, MoveSink ms)
 {
     const int32_t np = *d_np;
+    long long c1 = 0;
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < np;
          j += (int64_t)gridDim.x * blockDim.x) {
         // last part with es[p] <= j
@@ -1485,11 +1528,13 @@ __global__ void rs_assign_kernel(int32_t k, const int32_t *__restrict__ P, const
         }
         const int32_t p = lo;
         const int32_t v = V[P[j]];
-        if (j < ee[p] && p != where[v]) {
+        const int32_t from = where[v];
+        if (j < ee[p] && p != from) {
             dest[v] = p;
-            moves[atomicAdd(d_nmoves, 1ull)] = v;
+            c1 += move_append(ms, v, from, p);
         }
     }
+    hp::block_add_to<256>(c1, ms.d_c1);
 }
 
 
@@ -1497,6 +1542,7 @@ __global__ void rs_assign_kernel(int32_t k, const int32_t *__restrict__ P, const
 struct RefineBufs {
     int32_t *goff, *gpart, *gconn, *big, *dest, *pregain, *moves, *oldp, *dirty;
     int32_t *small_l, *big_l, *best_where, *huge_mv, *huge;
+    int32_t *recof;   // move log: a vertex's record (record mode)
     int32_t *plan_v, *plan_item, *plan_off, *plan_cnt;   // chunk plan of the current step
     int64_t nhub_cap;   // capacity of the long-row list and the plan (rows longer than chunk_deg)
     unsigned long long *ab_acc;   // afterburner sums of the hub rows (zero between passes)
@@ -1614,6 +1660,12 @@ int rank_candidates(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, int32_t
     return HP_OK;
 }
 
+MoveSink move_sink(hp_context *c, const RefineBufs &B, int32_t k)
+{
+    unsigned long long *sc = c->d_scal;
+    return MoveSink{B.moves, B.oldp, &sc[S_NMOVES], &sc[S_C1], B.goff, B.gpart, B.gconn, k};
+}
+
 // The undersized-part list of a weak pass is built by ctl_begin_kernel.
 int weak_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
 {
@@ -1621,7 +1673,7 @@ int weak_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
     int32_t *Ks, *Vs;
     HP_TRY(rank_candidates<false>(c, g, B, k, &Ks, &Vs));
     HP_LAUNCH(c, rw_select_kernel, (unsigned)(c->sm_count * 8), 256, 0, Ks, Vs,
-              (const int32_t *)&sc[S_LISTCNT], B.pre, B.pstart, B.pw, B.maxp, B.moves, &sc[S_NMOVES]);
+              (const int32_t *)&sc[S_LISTCNT], B.pre, B.pstart, B.pw, B.maxp, B.dest, move_sink(c, B, k));
     return HP_OK;
 }
 
@@ -1641,7 +1693,7 @@ int strong_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
     HP_LAUNCH(c, cookie_cutter_kernel, 1, 1024, sizeof(int32_t) * COOKIE_SMEM_INTS, k, B.pw, B.maxp, B.sp, d_np,
               B.es, B.ee);
     HP_LAUNCH(c, rs_assign_kernel, pg, 256, 0, k, B.P, d_np, Vs, B.es, B.ee, g.where, B.dest,
-              B.moves, &sc[S_NMOVES]);
+              move_sink(c, B, k));
     return HP_OK;
 }
 
@@ -1833,13 +1885,13 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
                       P.finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND], gate, k);
         if (P.recording)
             HP_LAUNCH(c, log_candidates_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, g.xadj,
-                      P.finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.oldp, c->log_x, c->log_v,
+                      P.finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.recof, c->log_x, c->log_v,
                       c->log_d, c->log_acc, c->log_count, c->log_cap);
         HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest,
-                  B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES], c->tune.gain_thread_deg);
+                  B.pregain, B.lock, &sc[S_NCAND], move_sink(c, B, k), c->tune.gain_thread_deg);
         if (P.any_big)
             HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt, g.where,
-                      B.dest, B.pregain, B.lock, &sc[S_NCAND], B.moves, &sc[S_NMOVES], c->tune.chunk_deg);
+                      B.dest, B.pregain, B.lock, &sc[S_NCAND], move_sink(c, B, k), c->tune.chunk_deg);
         if (P.huge_rows) {
             const int32_t *d_nhuge = d_bigcnt + 3;
             HP_LAUNCH(c, hub_plan_kernel<false>, plan_grid(c, B.nhub_cap), PLAN_THREADS, 0, B.huge, d_nhuge, B.moves,
@@ -1849,10 +1901,10 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
                       B.plan_off, B.plan_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, &sc[S_NCAND],
                       B.ab_acc);
             HP_LAUNCH(c, afterburner_huge_final_kernel, (unsigned)c->sm_count, 256, 0, B.huge, d_nhuge, B.pregain,
-                      &sc[S_NCAND], B.ab_acc, B.lock, B.moves, &sc[S_NMOVES]);
+                      &sc[S_NCAND], B.ab_acc, B.lock, g.where, B.dest, move_sink(c, B, k));
         }
         if (P.recording)
-            HP_LAUNCH(c, log_accept_kernel, nblk(n), 256, 0, n, B.oldp, B.lock, &sc[S_NCAND], c->log_acc);
+            HP_LAUNCH(c, log_accept_kernel, nblk(n), 256, 0, n, B.recof, B.lock, &sc[S_NCAND], c->log_acc);
         // select: goff, rows, where, lock in; dest, pregain out.  afterburner:
         // xadj, adjncy, adjwgt, own pregain/dest/where in, lock out
         hp_prof_end(c, ltok, HP_PROF_LP, 8 * ((int64_t)n + 1) + 8 * (int64_t)(B.G) + 8 * g.m + 26 * (int64_t)n);
@@ -1874,8 +1926,7 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
     unsigned long long *sc = c->d_scal;
     const unsigned pg = (unsigned)(c->sm_count * c->tune.grid_ctas_per_sm);
     const unsigned mg = std::min(nblk(n), pg);   // grid-stride over the device move count
-    HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
-              B.oldp, 1, &sc[S_C1], k);
+    // (the proposal kernels appended the moves with their old parts and c1)
     HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw, g.xadj,
               g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k,
               B.huge_mv, (int32_t *)&sc[S_HUGEMV], c->tune.gain_thread_deg, c->tune.chunk_deg);
@@ -2511,7 +2562,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.maxp = d_maxp;
     int32_t **n_arrays[] = {&B.goff, &B.big, &B.dest, &B.pregain, &B.moves, &B.oldp, &B.dirty,
                             &B.small_l, &B.big_l, &B.best_where, &B.K, &B.V, &B.K2, &B.V2, &B.pre,
-                            &B.P, &B.sp, &B.huge_mv, &B.huge};
+                            &B.P, &B.sp, &B.huge_mv, &B.huge, &B.recof};
     for (auto pp : n_arrays) *pp = ralloc_t<int32_t>(c, (int64_t)n + 1);
     int32_t **k_arrays[] = {&B.pstart, &B.pend, &B.und, &B.ev_end, &B.es, &B.ee};
     for (auto pp : k_arrays) *pp = ralloc_t<int32_t>(c, k);
