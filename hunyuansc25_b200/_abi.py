@@ -94,6 +94,7 @@ TUNING_FIELDS = [
     "trial_cta_n",
     "contract_smem_cn",
     "batch_workers",
+    "small_match_n",
 ]
 
 TUNING_DEFAULTS = {
@@ -112,6 +113,7 @@ TUNING_DEFAULTS = {
     "trial_cta_n": 512,
     "contract_smem_cn": 49152,
     "batch_workers": 16,
+    "small_match_n": 4096,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -136,6 +138,7 @@ def tuning_violation(t: dict):
         ("trial_cta_n", 1, TUNE_DEG_MAX),
         ("contract_smem_cn", 0, 49152),
         ("batch_workers", 1, 64),
+        ("small_match_n", 0, 8192),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -144,7 +147,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 1)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 8)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

@@ -515,6 +515,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->trial_cta_n = 512;
     t->contract_smem_cn = HP_TUNE_SMEM_CN_MAX;
     t->batch_workers = 16;
+    t->small_match_n = 4096;
 }
 
 namespace {
@@ -537,6 +538,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.trial_cta_n, 1, HP_TUNE_DEG_MAX)) return "trial_cta_n";
     if (!in(t.contract_smem_cn, 0, HP_TUNE_SMEM_CN_MAX)) return "contract_smem_cn";
     if (!in(t.batch_workers, 1, 64)) return "batch_workers";
+    if (!in(t.small_match_n, 0, HP_TUNE_SMALL_MATCH_MAX)) return "small_match_n";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;

@@ -22,6 +22,8 @@
 // The reference's matching is an atomicCAS race (nondeterministic); every
 // decision here is a pure function of the level's CSR and the seed, so the
 // CPU oracle reproduces each level bit for bit.
+#include <cstdlib>
+
 #include "hp_internal.cuh"
 #include "hp_rowagg.cuh"
 
@@ -1077,6 +1079,247 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
     }
 }
 
+// ---- small levels: the whole matching in one CTA -------------------------------------
+// A level with few vertices is matched by one CTA of MS_THREADS threads: the
+// handshake rounds (a proposal that is still valid is kept, as in the cached
+// kernels), the two-hop pairing (clients sorted stably by hub with a block
+// radix sort), the isolated and forced pairings, each gated at 75 % matched,
+// the self matches of the rest and the exclusive scan of the leader flags into
+// cmap -- the rules of match_level, separated by __syncthreads instead of
+// kernel boundaries and host reads.  The match, eligibility and proposal
+// arrays live in shared memory (at most HP_TUNE_SMALL_MATCH_MAX vertices), so a
+// row scan's only global loads are the row's own entries; cmap[n], the coarse
+// vertex count, is all the host reads back.
+constexpr int MS_THREADS = 1024;
+
+inline size_t ms_smem_bytes(int32_t n)
+{
+    return sizeof(int32_t) * ((size_t)hp::block_sort_ints(MS_THREADS) + 3 * (size_t)n);
+}
+
+// v's best candidate over its row: a thread walks rows of up to 32 entries
+// (eight loads in flight), the whole warp longer ones, one at a time, reduced
+// in hp::better's order -- a total order, so the split does not change the
+// winner.  ELIG: unmatched neighbours within the weight cap only (s_elig:
+// vertex weight, INT_MAX once matched); else any neighbour.  All lanes of the
+// warp call; act marks the lanes with a row to scan.
+template <bool ELIG>
+__device__ int32_t ms_best(bool act, int32_t v, const int32_t *__restrict__ xadj,
+                           const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt,
+                           const int32_t *s_elig, int32_t wv, uint64_t lkey, int64_t maxvwgt)
+{
+    const int lane = threadIdx.x & 31;
+    const int32_t b = act ? xadj[v] : 0, e = act ? xadj[v + 1] : 0;
+    const bool coop = act && e - b > 32;
+    int32_t res = -1;
+    if (act && !coop) {
+        BestCand best;
+        for (int32_t j0 = b; j0 < e; j0 += 8) {
+            int32_t u[8], w[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                const bool in = j0 + q < e;
+                u[q] = in ? adjncy[j0 + q] : v;
+                w[q] = in ? adjwgt[j0 + q] : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (u[q] == v) continue;
+                if (ELIG) {
+                    const int32_t eu = s_elig[u[q]];
+                    if (eu == INT_MAX) continue;                     // matched
+                    if ((int64_t)wv + eu > maxvwgt) continue;        // weight cap
+                }
+                best.offer(lkey, v, u[q], w[q]);
+            }
+        }
+        res = best.u;
+    }
+    unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
+    while (cm) {
+        const int src = __ffs(cm) - 1;
+        cm &= cm - 1;
+        const int32_t sv = __shfl_sync(HP_FULL_MASK, v, src), sb = __shfl_sync(HP_FULL_MASK, b, src);
+        const int32_t se = __shfl_sync(HP_FULL_MASK, e, src), swv = __shfl_sync(HP_FULL_MASK, wv, src);
+        BestCand best;
+        for (int32_t j = sb + lane; j < se; j += 32) {
+            const int32_t u = adjncy[j];
+            if (u == sv) continue;
+            if (ELIG) {
+                const int32_t eu = s_elig[u];
+                if (eu == INT_MAX) continue;
+                if ((int64_t)swv + eu > maxvwgt) continue;
+            }
+            best.offer(lkey, sv, u, adjwgt[j]);
+        }
+        best.finish(lkey, sv);
+        int32_t bu = best.u, bw = best.w;
+        uint32_t bh = best.h;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
+            const int32_t ow = __shfl_xor_sync(HP_FULL_MASK, bw, o);
+            const uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
+            if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; }
+        }
+        if (lane == src) res = bu;
+    }
+    return res;
+}
+
+// Number of v < n with s_match[v] != -1 (every thread gets it).
+__device__ __forceinline__ int32_t ms_matched(int32_t n, const int32_t *s_match, int32_t *s_scan)
+{
+    int c = 0;
+    for (int32_t v = threadIdx.x; v < n; v += MS_THREADS) c += s_match[v] != -1;
+    int tot;
+    hp::block_excl_scan<MS_THREADS>(c, &tot, s_scan);
+    return tot;
+}
+
+// Pairs (list[2i], list[2i+1]) of the unmatched vertices (ISOLATED_ONLY: the
+// unmatched vertices without neighbours) in id order, when the weight sum fits
+// (pair_list_kernel's rule).  list: n ints.
+template <bool ISOLATED_ONLY>
+__device__ void ms_pair_unmatched(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ vwgt,
+                                  int32_t *s_match, int32_t *__restrict__ list, int64_t maxvwgt, int32_t *s_scan)
+{
+    int32_t cnt = 0;
+    for (int32_t b0 = 0; b0 < n; b0 += MS_THREADS) {
+        const int32_t v = b0 + threadIdx.x;
+        int f = v < n && s_match[v] == -1;
+        if (ISOLATED_ONLY && f) f = xadj[v] == xadj[v + 1];
+        int tot;
+        const int ex = hp::block_excl_scan<MS_THREADS>(f, &tot, s_scan);
+        if (f) list[cnt + ex] = v;
+        cnt += tot;
+    }
+    __syncthreads();
+    for (int32_t i = threadIdx.x; 2 * i + 1 < cnt; i += MS_THREADS) {
+        const int32_t a = list[2 * i], b = list[2 * i + 1];
+        if ((int64_t)vwgt[a] + vwgt[b] <= maxvwgt) { s_match[a] = b; s_match[b] = a; }
+    }
+    __syncthreads();
+}
+
+// Dynamic shared memory: ms_smem_bytes(n).  K, V, K2, V2: n ints each (the
+// two-hop sort and the pairing lists).
+__global__ void __launch_bounds__(MS_THREADS, 1)
+match_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                   const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt, int32_t *__restrict__ match,
+                   int32_t *__restrict__ cmap, int32_t *K, int32_t *V, int32_t *K2, int32_t *V2, uint64_t lkey,
+                   int64_t maxvwgt, int rounds, int key_bits)
+{
+    extern __shared__ int32_t ms_sh[];
+    int32_t *tab = ms_sh;                                        // block radix sort
+    int32_t *s_match = tab + hp::block_sort_ints(MS_THREADS);
+    int32_t *s_elig = s_match + n;
+    int32_t *s_pref = s_elig + n;
+    __shared__ int32_t s_scan[MS_THREADS / 32 + 2];
+    const int tid = threadIdx.x;
+    for (int32_t v = tid; v < n; v += MS_THREADS) {
+        s_match[v] = -1;
+        s_elig[v] = vwgt[v];
+        s_pref[v] = -1;
+    }
+    __syncthreads();
+    // handshake rounds; a round that matched nothing ends them (the next would
+    // repeat it)
+    for (int r = 0; r < rounds; r++) {
+        for (int32_t b0 = 0; b0 < n; b0 += MS_THREADS) {
+            const int32_t v = b0 + tid;
+            const bool in = v < n;
+            const bool unmatched = in && s_match[v] == -1;
+            bool act = unmatched;
+            if (act && r > 0) {   // keep a proposal that is still valid (keep_proposal)
+                const int32_t pu = s_pref[v];
+                act = pu >= 0 && s_elig[pu] == INT_MAX;
+            }
+            const int32_t u = ms_best<true>(act, v, xadj, adjncy, adjwgt, s_elig, act ? vwgt[v] : 0, lkey, maxvwgt);
+            if (act) s_pref[v] = u;
+            else if (in && !unmatched) s_pref[v] = -1;
+        }
+        __syncthreads();
+        int made = 0;
+        for (int32_t v = tid; v < n; v += MS_THREADS) {
+            if (s_match[v] != -1) continue;
+            const int32_t u = s_pref[v];
+            if (u >= 0 && s_pref[u] == v) {
+                s_match[v] = u;
+                s_elig[v] = INT_MAX;
+                made++;
+            }
+        }
+        int tot;
+        hp::block_excl_scan<MS_THREADS>(made, &tot, s_scan);   // (ends with a barrier)
+        if (tot == 0) break;
+    }
+    int32_t nm = ms_matched(n, s_match, s_scan);
+    if (4 * (int64_t)nm < 3 * (int64_t)n) {
+        // two-hop: the hub of every unmatched vertex (any neighbour), the clients
+        // sorted stably by hub, odd offsets in a hub's run paired with the one before
+        for (int32_t b0 = 0; b0 < n; b0 += MS_THREADS) {
+            const int32_t v = b0 + tid;
+            const bool in = v < n;
+            const bool act = in && s_match[v] == -1;
+            const int32_t u = ms_best<false>(act, v, xadj, adjncy, adjwgt, nullptr, 0, lkey, maxvwgt);
+            if (in) s_pref[v] = act ? u : -1;
+        }
+        __syncthreads();
+        int32_t cnt = 0;
+        for (int32_t b0 = 0; b0 < n; b0 += MS_THREADS) {
+            const int32_t c = b0 + tid;
+            const int f = c < n && s_match[c] == -1 && s_pref[c] >= 0;
+            int tot;
+            const int ex = hp::block_excl_scan<MS_THREADS>(f, &tot, s_scan);
+            if (f) {
+                K[cnt + ex] = s_pref[c];
+                V[cnt + ex] = c;
+            }
+            cnt += tot;
+        }
+        const bool flip = hp::block_sort_pairs<MS_THREADS>(K, V, K2, V2, cnt, key_bits, tab, s_scan);
+        const int32_t *Ks = flip ? K2 : K, *Vs = flip ? V2 : V;
+        for (int32_t i = tid; i < cnt; i += MS_THREADS) {
+            const int32_t h = Ks[i];
+            int32_t lo = 0, hi = i;   // first index of the run of h
+            while (lo < hi) {
+                const int32_t mid = (lo + hi) >> 1;
+                if (Ks[mid] < h) lo = mid + 1; else hi = mid;
+            }
+            if ((i - lo) & 1) {
+                const int32_t a = Vs[i - 1], b = Vs[i];
+                if ((int64_t)vwgt[a] + vwgt[b] <= maxvwgt) { s_match[a] = b; s_match[b] = a; }
+            }
+        }
+        __syncthreads();
+        nm = ms_matched(n, s_match, s_scan);
+    }
+    if (4 * (int64_t)nm < 3 * (int64_t)n) {   // isolated vertices, in id order
+        ms_pair_unmatched<true>(n, xadj, vwgt, s_match, K, maxvwgt, s_scan);
+        nm = ms_matched(n, s_match, s_scan);
+    }
+    if (4 * (int64_t)nm < 3 * (int64_t)n)     // forced: every remaining vertex, in id order
+        ms_pair_unmatched<false>(n, xadj, vwgt, s_match, K, maxvwgt, s_scan);
+    // self matches of the rest; cmap = exclusive scan of the leader flags
+    int32_t run = 0;
+    for (int32_t b0 = 0; b0 < n; b0 += MS_THREADS) {
+        const int32_t v = b0 + tid;
+        int lead = 0;
+        if (v < n) {
+            int32_t u = s_match[v];
+            if (u == -1) u = v;
+            match[v] = u;
+            lead = v <= u;
+        }
+        int tot;
+        const int ex = hp::block_excl_scan<MS_THREADS>(lead, &tot, s_scan);
+        if (v < n) cmap[v] = run + ex;
+        run += tot;
+    }
+    if (tid == 0) cmap[n] = run;
+}
+
 inline unsigned blocks_for(int64_t threads, int block = 256)
 {
     int64_t g = (threads + block - 1) / block;
@@ -1098,6 +1341,29 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     const uint64_t lkey = hp::level_key(o.seed, level);
     const size_t mark = c->hi;
 
+    const hp_tuning &tn = c->tune;
+    const int rounds = o.match_rounds < 1 ? 1 : (o.match_rounds > 30 ? 30 : o.match_rounds);
+    // algorithmic bytes of one full handshake round: xadj, adjncy, adjwgt,
+    // vwgt, match read and write (neighbour gathers not counted)
+    const int64_t round_bytes = 4 * ((int64_t)n + 1) + 8 * g.m + 12 * (int64_t)n;
+    if (n <= tn.small_match_n && g.m <= 64 * (int64_t)n) {
+        // a small level: the whole matching in one CTA, one read back (cn)
+        int32_t *sb = ralloc_t<int32_t>(c, 4 * ((int64_t)n + 1));
+        HP_CHECK_OOM(c);
+        int32_t *sk = sb, *sv = sb + (n + 1), *sk2 = sb + 2 * (n + 1), *sv2 = sb + 3 * (n + 1);
+        int kbits = 0;
+        while ((1ll << kbits) < (int64_t)n) kbits++;
+        const int tok = hp_prof_begin(c);
+        HP_LAUNCH(c, match_small_kernel, 1, MS_THREADS, ms_smem_bytes(n), n, g.xadj, g.adjncy, g.adjwgt, g.vwgt,
+                  g.match, g.cmap, sk, sv, sk2, sv2, lkey, maxvwgt, rounds, kbits);
+        hp_prof_end(c, tok, HP_PROF_MATCH, round_bytes);
+        int32_t cn = 0;
+        HP_TRY(hp_read_scalars(c, g.cmap + n, sizeof(int32_t), &cn));
+        *cn_out = cn;
+        c->hi = mark;
+        return HP_OK;
+    }
+
     int32_t *pref = ralloc_t<int32_t>(c, n);
     int32_t *big = ralloc_t<int32_t>(c, n);
     int32_t *huge = ralloc_t<int32_t>(c, n);
@@ -1116,14 +1382,9 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     int32_t *d_hugecnt = (int32_t *)&sc[38];
 
     HP_TRY(hp_fill_i32(c, g.match, n, -1));
-    const hp_tuning &tn = c->tune;
     HP_LAUNCH(c, big_list_kernel, blocks_for(n), 256, 0, n, g.xadj, big, d_bigcnt, huge, d_hugecnt, g.vwgt, elig,
               tn.match_warp_deg, tn.match_cta_deg);
 
-    const int rounds = o.match_rounds < 1 ? 1 : (o.match_rounds > 30 ? 30 : o.match_rounds);
-    // algorithmic bytes of one full handshake round: xadj, adjncy, adjwgt,
-    // vwgt, match read and write (neighbour gathers not counted)
-    const int64_t round_bytes = 4 * ((int64_t)n + 1) + 8 * g.m + 12 * (int64_t)n;
     for (int r = 0; r < rounds; r++) {
         const int tok = hp_prof_begin(c);
         const unsigned long long *prev = r == 0 ? nullptr : &sc[2 + r - 1];
@@ -1327,6 +1588,8 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
 
 int hp_coarsen_init()
 {
+    HP_CUDA(cudaFuncSetAttribute(match_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)ms_smem_bytes(HP_TUNE_SMALL_MATCH_MAX)));
     HP_CUDA(cudaFuncSetAttribute(contract_dense_kernel<1024, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(int32_t) * (HP_TUNE_SMEM_CN_MAX + (HP_TUNE_SMEM_CN_MAX + 31) / 32 +
                                                           (HP_TUNE_SMEM_CN_MAX + 1023) / 1024))));
@@ -1344,21 +1607,40 @@ int hp_coarsen_init()
 
 int hp_coarsen(hp_context *c, int32_t coarsen_to, int64_t maxvwgt)
 {
+    // HP_DEBUG_LEVELS: device time of every level's matching and contraction on stderr
+    const bool dbg = getenv("HP_DEBUG_LEVELS") != nullptr;
+    cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+    if (dbg)
+        for (auto &x : e) HP_CUDA(cudaEventCreate(&x));
     int level = 0;
+    int rc = HP_OK;
     while (level < c->opt.max_levels && c->levels[level].n > coarsen_to) {
         HpLevel &g = c->levels[level];
         g.match = lalloc_t<int32_t>(c, g.n);
         g.cmap = lalloc_t<int32_t>(c, (int64_t)g.n + 1);
-        HP_CHECK_OOM(c);
+        if (c->oom) { rc = HP_ERR_NOMEM; break; }
         int32_t cn = 0;
-        HP_TRY(match_level(c, g, level, maxvwgt, &cn));
+        if (dbg) cudaEventRecord(e[0], c->stream);
+        if ((rc = match_level(c, g, level, maxvwgt, &cn)) != HP_OK) break;
+        if (dbg) cudaEventRecord(e[1], c->stream);
         c->levels.emplace_back();
         HpLevel &f = c->levels[level];
         HpLevel &cg = c->levels[level + 1];
-        HP_TRY(contract_level(c, f, cn, cg));
-        HP_TRY(hp_check_status(c));
+        if ((rc = contract_level(c, f, cn, cg)) != HP_OK) break;
+        if ((rc = hp_check_status(c)) != HP_OK) break;
+        if (dbg) {
+            cudaEventRecord(e[2], c->stream);
+            cudaEventSynchronize(e[2]);
+            float ms_m = 0.f, ms_c = 0.f;
+            cudaEventElapsedTime(&ms_m, e[0], e[1]);
+            cudaEventElapsedTime(&ms_c, e[1], e[2]);
+            fprintf(stderr, "gpu coarsen level %d n=%d m=%lld match_ms=%.3f contract_ms=%.3f\n", level, f.n,
+                    (long long)f.m, ms_m, ms_c);
+        }
         level++;
         if (!(100 * (int64_t)cg.n < 85 * (int64_t)f.n && cg.m > cg.n / 2)) break;
     }
-    return HP_OK;
+    if (dbg)
+        for (auto &x : e) cudaEventDestroy(x);
+    return rc;
 }

@@ -96,6 +96,7 @@ constexpr int HP_TUNE_CTA_ROW_MAX = 4096;        // contract_cta_radix_kernel<25
 constexpr int HP_TUNE_WARP_DENSE_K_MAX = 1024;   // gain_bigwarp_kernel's shared accumulators
 constexpr int HP_TUNE_DEG_MAX = 1 << 24;
 constexpr int HP_TUNE_SMALL_LEVEL_MAX = 32768;   // refine_small_kernel's staged prefix weights
+constexpr int HP_TUNE_SMALL_MATCH_MAX = 8192;    // match_small_kernel's shared-memory state
 constexpr int HP_TUNE_SMEM_CN_MAX = 49152;       // shared-memory dense accumulator of the contraction
 
 #define HP_NSCAL 64

@@ -1963,7 +1963,7 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
 // levels cost more than the work.
 constexpr int SL_THREADS = 1024;
 constexpr int SL_WARPS = SL_THREADS / 32;
-constexpr int SL_SORT_INTS = 256 + SL_WARPS * 256;   // digit bases + per-warp digit counts
+constexpr int SL_SORT_INTS = hp::block_sort_ints(SL_THREADS);
 
 struct SmallLevel {
     int32_t n, k, finest, bigd, small_max, key_bits, learned_mlp;
@@ -2016,60 +2016,6 @@ __device__ __forceinline__ long long sl_max64(long long v, long long *s_red)
 #pragma unroll 8
     for (int w = 0; w < SL_WARPS; w++) t = s_red[w] > t ? s_red[w] : t;
     return t;
-}
-
-// Stable LSD radix sort of cnt (key, value) pairs by the low key_bits bits of
-// the keys (non-negative), one CTA of SL_THREADS.  Ping-pongs between (K, V)
-// and (K2, V2); returns true when the result is in (K2, V2).  Per 8-bit digit:
-// a histogram, the digit bases, then chunks of SL_THREADS items in order, each
-// item placed at its digit's base + the same digit's count in earlier warps of
-// the chunk + its rank inside its warp (__match_any_sync).  tab: SL_SORT_INTS.
-__device__ bool sl_sort_pairs(int32_t *K, int32_t *V, int32_t *K2, int32_t *V2, int32_t cnt, int key_bits,
-                              int32_t *tab, int32_t *s_scan)
-{
-    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    int32_t *base = tab, *wc = tab + 256;
-    bool flip = false;
-    for (int shift = 0; shift < key_bits; shift += 8) {
-        const int32_t *ks = flip ? K2 : K, *vs = flip ? V2 : V;
-        int32_t *kd = flip ? K : K2, *vd = flip ? V : V2;
-        if (tid < 256) base[tid] = 0;
-        __syncthreads();
-        for (int32_t i = tid; i < cnt; i += SL_THREADS) atomicAdd(&base[((unsigned)ks[i] >> shift) & 255u], 1);
-        __syncthreads();
-        const int h = tid < 256 ? base[tid] : 0;
-        int tot;
-        const int ex = hp::block_excl_scan<SL_THREADS>(h, &tot, s_scan);   // ends with a barrier
-        if (tid < 256) base[tid] = ex;
-        for (int32_t c0 = 0; c0 < cnt; c0 += SL_THREADS) {
-            const int32_t i = c0 + tid;
-            const bool valid = i < cnt;
-            const int32_t key = valid ? ks[i] : 0;
-            const unsigned d = valid ? (((unsigned)key >> shift) & 255u) : 256u + lane;
-            const unsigned peers = __match_any_sync(HP_FULL_MASK, d);
-            const int rank = __popc(peers & hp::lanemask_lt());
-            for (int q = tid; q < SL_WARPS * 256; q += SL_THREADS) wc[q] = 0;
-            __syncthreads();
-            if (valid && rank == 0) wc[wid * 256 + d] = __popc(peers);
-            __syncthreads();
-            if (valid) {
-                int32_t off = base[d] + rank;
-                for (int w = 0; w < wid; w++) off += wc[w * 256 + d];
-                kd[off] = key;
-                vd[off] = vs[i];
-            }
-            __syncthreads();
-            if (tid < 256) {   // the digit bases move past this chunk
-                int32_t c = 0;
-                for (int w = 0; w < SL_WARPS; w++) c += wc[w * 256 + tid];
-                base[tid] += c;
-            }
-            __syncthreads();
-        }
-        flip = !flip;
-    }
-    __syncthreads();
-    return flip;
 }
 
 __global__ void __launch_bounds__(SL_THREADS, 1)
@@ -2251,7 +2197,7 @@ refine_small_kernel(SmallLevel a)
                 }
                 cnt += tot;
             }
-            const bool flip = sl_sort_pairs(a.K, a.V, a.K2, a.V2, cnt, a.key_bits, sl_dyn, s_scan);
+            const bool flip = hp::block_sort_pairs<SL_THREADS>(a.K, a.V, a.K2, a.V2, cnt, a.key_bits, sl_dyn, s_scan);
             const int32_t *Ks = flip ? a.K2 : a.K, *Vs = flip ? a.V2 : a.V;
             // prefix weights in sorted order and the part bounds
             int32_t run = 0;

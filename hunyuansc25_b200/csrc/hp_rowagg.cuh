@@ -296,4 +296,64 @@ __device__ __forceinline__ int dense_extract2(int32_t *dw, unsigned *bm, unsigne
     return running;
 }
 
+
+// Stable LSD radix sort of cnt (key, value) pairs by the low key_bits bits of
+// the keys (non-negative), by one CTA of NT threads.  Ping-pongs between (K, V)
+// and (K2, V2); returns true when the result is in (K2, V2).  Per 8-bit digit: a
+// histogram, the digit bases, then chunks of NT items in order, each item placed
+// at its digit's base + the same digit's count in earlier warps of the chunk +
+// its rank inside its warp (__match_any_sync).  tab: block_sort_ints(NT) ints of
+// shared memory; s_scan: NT/32 + 2 ints.
+constexpr int block_sort_ints(int nt) { return 256 + (nt / 32) * 256; }
+
+template <int NT>
+__device__ bool block_sort_pairs(int32_t *K, int32_t *V, int32_t *K2, int32_t *V2, int32_t cnt, int key_bits,
+                                 int32_t *tab, int32_t *s_scan)
+{
+    constexpr int W = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    int32_t *base = tab, *wc = tab + 256;
+    bool flip = false;
+    for (int shift = 0; shift < key_bits; shift += 8) {
+        const int32_t *ks = flip ? K2 : K, *vs = flip ? V2 : V;
+        int32_t *kd = flip ? K : K2, *vd = flip ? V : V2;
+        for (int q = tid; q < 256; q += NT) base[q] = 0;
+        __syncthreads();
+        for (int32_t i = tid; i < cnt; i += NT) atomicAdd(&base[((unsigned)ks[i] >> shift) & 255u], 1);
+        __syncthreads();
+        const int h = tid < 256 ? base[tid] : 0;
+        int tot;
+        const int ex = block_excl_scan<NT>(h, &tot, s_scan);   // ends with a barrier
+        if (tid < 256) base[tid] = ex;
+        for (int32_t c0 = 0; c0 < cnt; c0 += NT) {
+            const int32_t i = c0 + tid;
+            const bool valid = i < cnt;
+            const int32_t key = valid ? ks[i] : 0;
+            const unsigned d = valid ? (((unsigned)key >> shift) & 255u) : 256u + lane;
+            const unsigned peers = __match_any_sync(HP_FULL_MASK, d);
+            const int rank = __popc(peers & lanemask_lt());
+            for (int q = tid; q < W * 256; q += NT) wc[q] = 0;
+            __syncthreads();
+            if (valid && rank == 0) wc[wid * 256 + d] = __popc(peers);
+            __syncthreads();
+            if (valid) {
+                int32_t off = base[d] + rank;
+                for (int w = 0; w < wid; w++) off += wc[w * 256 + d];
+                kd[off] = key;
+                vd[off] = vs[i];
+            }
+            __syncthreads();
+            if (tid < 256) {   // the digit bases move past this chunk
+                int32_t c = 0;
+                for (int w = 0; w < W; w++) c += wc[w * 256 + tid];
+                base[tid] += c;
+            }
+            __syncthreads();
+        }
+        flip = !flip;
+    }
+    __syncthreads();
+    return flip;
+}
+
 }  // namespace hp

@@ -176,7 +176,10 @@ typedef struct hp_tuning {
                                     dense accumulator instead of radix sorts      [0, 49152]    49152 */
     int32_t batch_workers;       /* hp_partition_batch: worker contexts (streams) that
                                     partition graphs concurrently                 [1, 64]       16 */
-    int32_t reserved[1];         /* zero */
+    int32_t small_match_n;       /* coarsening: levels of at most this many vertices (and
+                                    64x as many adjacency entries) are matched by one
+                                    CTA; 0 = never                               [0, 8192]     4096 */
+    int32_t reserved[8];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);

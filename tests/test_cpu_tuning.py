@@ -26,7 +26,7 @@ def test_tuning_struct_matches_header(tmp_path):
     got = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
     want = [getattr(HpTuning, f).offset for f in TUNING_FIELDS] + [HpTuning.reserved.offset, C.sizeof(HpTuning)]
     assert got == want
-    assert C.sizeof(HpTuning) == 64
+    assert C.sizeof(HpTuning) == 96
 
 
 def test_library_defaults_match_python():
@@ -35,7 +35,7 @@ def test_library_defaults_match_python():
     t = HpTuning()
     lib.hp_tuning_default(C.byref(t))
     assert t.as_dict() == TUNING_DEFAULTS
-    assert list(t.reserved) == [0] * 1
+    assert list(t.reserved) == [0] * 8
     assert tuning_violation(TUNING_DEFAULTS) is None
 
 
@@ -45,7 +45,7 @@ def test_library_defaults_match_python():
     ("gain_thread_deg", 33), ("gain_hub_deg", 31), ("warp_dense_k", 1025), ("warp_dense_k", -1),
     ("grid_ctas_per_sm", 0), ("grid_ctas_per_sm", 33), ("dense_sparse_ratio", 0),
     ("small_level_n", -1), ("small_level_n", 32769), ("chunk_deg", 31), ("trial_cta_n", 0), ("contract_smem_cn", 49153),
-    ("batch_workers", 0), ("batch_workers", 65),
+    ("batch_workers", 0), ("batch_workers", 65), ("small_match_n", -1), ("small_match_n", 8193),
 ])
 def test_violations(field, value):
     t = dict(TUNING_DEFAULTS)

@@ -177,6 +177,58 @@ def test_edge_cases(ctx):
     compare_runs(ctx, gg, 3)
 
 
+def mixed_matching_graph(leaves=400, isolated=200, tri=1000):
+    """A star, isolated vertices and triangles weighted 3/2/1: the handshake
+    rounds match the hub with one leaf and two vertices of each triangle; the
+    other leaves pair through the hub (two-hop); the isolated vertices pair in
+    id order; the third vertices of the triangles are forced into pairs."""
+    n = 1 + leaves + isolated + 3 * tri
+    rows = [[] for _ in range(n)]
+
+    def edge(a, b, w):
+        rows[a].append((b, w))
+        rows[b].append((a, w))
+    for i in range(1, leaves + 1):
+        edge(0, i, 1)
+    base = 1 + leaves + isolated
+    for t in range(tri):
+        a = base + 3 * t
+        edge(a, a + 1, 3)
+        edge(a + 1, a + 2, 2)
+        edge(a, a + 2, 1)
+    xadj = np.zeros(n + 1, np.int32)
+    adj, w = [], []
+    for v in range(n):
+        r = sorted(rows[v])
+        xadj[v + 1] = xadj[v] + len(r)
+        adj += [u for u, _ in r]
+        w += [x for _, x in r]
+    return graphs.Graph(xadj, np.array(adj, np.int32), np.ones(n, np.int32), np.array(w, np.int32), "mixed")
+
+
+@pytest.mark.parametrize("small_match_n", [4096, 0], ids=["one_cta", "multi_kernel"])
+def test_matching_fallbacks(ctx, small_match_n):
+    g = mixed_matching_graph()
+    n = len(g.xadj) - 1
+    _, _, tr = oracle.partition(g, 4, 1.03, opt=default_options(trace=1), trace=True)
+    m = tr.array(0, 4)
+    v = np.arange(n)
+    pair = m > v
+    leaf = (v >= 1) & (v <= 400)
+    iso = (v >= 401) & (v <= 600)
+    # the level-0 matching of this graph takes every fallback
+    assert np.sum(pair & leaf & leaf[m]) == 199
+    assert np.sum(pair & iso & iso[m]) == 100
+    assert np.sum(pair & (v >= 601) & (m - v >= 3)) == 499   # forced: third vertices
+    assert np.sum(pair & leaf & (m >= 601)) == 1             # forced: the last leaf
+    ctx.set_tuning(small_match_n=small_match_n)
+    try:
+        compare_runs(ctx, g, 4)
+        compare_runs(ctx, g, 64)
+    finally:
+        ctx.set_tuning()
+
+
 def test_invalid_inputs(ctx):
     bad = np.array([0, 1, 2], np.int32)
     with pytest.raises(hp.HpError) as e:
