@@ -588,20 +588,15 @@ struct ContractSrc {
 };
 
 // ---- short rows: one thread per coarse row, aggregation in registers ------------
+// The row's entries come from the tile's staging buffer (packed key << 32 |
+// weight, the self key already PACK_NONE); a bitonic network of NET sorts them
+// and the unique keys are counted.
 template <int NET, int XN>
-__device__ __forceinline__ int gather_sort_row(const ContractSrc &src, int32_t c, const RowInfo &r, int32_t len,
+__device__ __forceinline__ int sort_staged_row(const unsigned long long *stage, int32_t len,
                                                unsigned long long (&x)[XN])
 {
 #pragma unroll
-    for (int i = 0; i < NET; i++) {
-        unsigned long long e = hp::PACK_NONE;
-        if (i < len) {
-            int32_t k, w;
-            src.get(c, r, i, k, w);
-            if (k != hp::KEY_NONE) e = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)w;
-        }
-        x[i] = e;
-    }
+    for (int i = 0; i < NET; i++) x[i] = i < len ? stage[i] : hp::PACK_NONE;
     hp::sort_regs<NET, XN>(x);
     int u = 0;
 #pragma unroll
@@ -613,9 +608,11 @@ __device__ __forceinline__ int gather_sort_row(const ContractSrc &src, int32_t c
     return u;
 }
 
+// The sorted row merged (weights of equal keys summed) into out[0..u), each
+// entry tagged with the tile row t.
 template <int NET, int XN>
-__device__ __forceinline__ void emit_row(const unsigned long long (&x)[XN], int32_t *__restrict__ out_k,
-                                         int32_t *__restrict__ out_w)
+__device__ __forceinline__ void emit_staged_row(const unsigned long long (&x)[XN], unsigned long long *out,
+                                                uint8_t *orow, uint8_t t)
 {
     int r = -1;
     uint32_t prev = 0xffffffffu;
@@ -626,29 +623,40 @@ __device__ __forceinline__ void emit_row(const unsigned long long (&x)[XN], int3
         const int32_t w = (int32_t)(uint32_t)x[i];
         if (k == (uint32_t)hp::KEY_NONE) continue;
         if (k != prev) {
-            if (r >= 0) out_w[r] = acc;
+            if (r >= 0) out[r] = ((unsigned long long)prev << 32) | (uint32_t)acc;
             r++;
-            out_k[r] = (int32_t)k;
+            orow[r] = t;
             acc = w;
             prev = k;
         } else {
             acc += w;
         }
     }
-    if (r >= 0) out_w[r] = acc;
+    if (r >= 0) out[r] = ((unsigned long long)prev << 32) | (uint32_t)acc;
 }
 
 // Coarse CSR assembly in one ordered pass: tiles of ASM_TILE coarse rows are
-// taken in order (dynamic tile counter); each thread aggregates its short row in
-// registers (network of 8, 16 or 32 by the longest short row in the warp) or
-// reads the unique count of a long row aggregated before; a block scan plus a
-// decoupled look-back across tiles gives every row its final offset, so cxadj
-// and the short rows' entries are written directly, with no second scan and no
-// compaction copy.  Long rows are placed afterwards by copy_long_rows_kernel.
+// taken in order (dynamic tile counter).  The tile's short rows are staged in
+// shared memory: consecutive threads load consecutive entries of the rows (the
+// row reads coalesce, the cmap gathers of one row hit neighbouring ids), each
+// thread then sorts its row in registers (network of 8, 16 or 32 by the
+// longest short row in the warp) or takes the unique count of a long row
+// aggregated before; a block scan plus a decoupled look-back across tiles gives
+// every row its final offset; the merged short rows go back through shared
+// memory and are written with consecutive threads on consecutive entries.
+// cxadj is written directly, with no second scan and no compaction copy; long
+// rows are placed afterwards by copy_long_rows_kernel.
 constexpr int ASM_TILE = 256;
 
+// Dynamic shared memory: ASM_TILE * XN staged entries and their tile rows.
+template <int XN>
+constexpr size_t asm_smem_bytes()
+{
+    return (sizeof(unsigned long long) + sizeof(uint8_t)) * (size_t)ASM_TILE * XN;
+}
+
 // XN: the longest network the level needs (8, 16 or 32; the host reads the
-// longest short row) -- the register array, and so the occupancy, follow it.
+// longest short row) -- every short row has at most XN entries.
 template <int XN>
 __global__ void __launch_bounds__(ASM_TILE)
 contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict__ ucnt,
@@ -656,43 +664,96 @@ contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict_
                          int32_t *__restrict__ cadjwgt, unsigned long long *tile_status, hp::LbCtl *lb,
                          unsigned *status, int32_t thread_row)
 {
+    extern __shared__ unsigned long long asm_stage[];                      // ASM_TILE * XN
+    uint8_t *s_row = reinterpret_cast<uint8_t *>(asm_stage + ASM_TILE * XN);   // tile row of each entry
+    __shared__ int4 s_ri[ASM_TILE];
+    __shared__ int32_t s_off[ASM_TILE];     // staged offset of the row's input, then of its output
+    __shared__ int32_t s_goff[ASM_TILE];    // the row's final offset
     __shared__ int32_t s_scan[ASM_TILE / 32 + 2];
     __shared__ int32_t s_excl;
     int64_t tile;
     unsigned epoch;
     hp::lb_begin(lb, &tile, &epoch);
-    const int32_t c = (int32_t)(tile * ASM_TILE + threadIdx.x);
+    const int t = threadIdx.x;
+    const int32_t c0 = (int32_t)(tile * ASM_TILE);
+    const int32_t c = c0 + t;
     RowInfo r{0, 0, 0, 0};
     int32_t len = 0;
     if (c < cn) src.row(c, r, len);
     const bool small = c < cn && len <= thread_row;
+    int tin;
+    const int ioff = hp::block_excl_scan<ASM_TILE>(small ? len : 0, &tin, s_scan);
+    s_ri[t] = make_int4(r.s0, r.l0, r.s1, r.l1);
+    s_off[t] = ioff;
+    if (small)
+        for (int i = 0; i < len; i++) s_row[ioff + i] = (uint8_t)t;
+    __syncthreads();
+    // stage: four entries per thread in flight (row reads, then the cmap gathers)
+    for (int f0 = t; f0 < tin; f0 += 4 * ASM_TILE) {
+        int32_t a[4], w[4], rt[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int f = f0 + q * ASM_TILE;
+            rt[q] = -1;
+            a[q] = 0;
+            w[q] = 0;
+            if (f < tin) {
+                rt[q] = s_row[f];
+                const int4 ri = s_ri[rt[q]];
+                const int i = f - s_off[rt[q]];
+                const int32_t j = i < ri.y ? ri.x + i : ri.z + (i - ri.y);
+                a[q] = src.adjncy[j];
+                w[q] = src.adjwgt[j];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (rt[q] < 0) continue;
+            const int32_t k = src.cmap[a[q]];
+            asm_stage[f0 + q * ASM_TILE] =
+                k == c0 + rt[q] ? hp::PACK_NONE : (((unsigned long long)(uint32_t)k << 32) | (uint32_t)w[q]);
+        }
+    }
+    __syncthreads();
     const unsigned wmax = __reduce_max_sync(HP_FULL_MASK, small ? (unsigned)len : 0u);
     unsigned long long x[XN];
     int u = 0;
     if (c < cn && !small) u = ucnt[c];
     if (XN == 8 || wmax <= 8) {
-        if (small) u = gather_sort_row<8, XN>(src, c, r, len, x);
+        if (small) u = sort_staged_row<8, XN>(asm_stage + ioff, len, x);
     } else if (XN == 16 || wmax <= 16) {
-        if (small) u = gather_sort_row<(XN < 16 ? XN : 16), XN>(src, c, r, len, x);
+        if (small) u = sort_staged_row<(XN < 16 ? XN : 16), XN>(asm_stage + ioff, len, x);
     } else {
-        if (small) u = gather_sort_row<XN, XN>(src, c, r, len, x);
+        if (small) u = sort_staged_row<XN, XN>(asm_stage + ioff, len, x);
     }
-    int agg;
-    const int local = hp::block_excl_scan<ASM_TILE>(u, &agg, s_scan);
-    if (threadIdx.x < 32) {
+    int agg, tout;
+    const int local = hp::block_excl_scan<ASM_TILE>(u, &agg, s_scan);   // (the staged input is read)
+    const int ooff = hp::block_excl_scan<ASM_TILE>(small ? u : 0, &tout, s_scan);
+    if (t < 32) {
         const int32_t excl = hp::lookback_epoch(tile_status, tile, agg, epoch, status);
-        if (threadIdx.x == 0) s_excl = excl;
+        if (t == 0) s_excl = excl;
     }
+    if (small) {
+        if (XN == 8 || wmax <= 8) emit_staged_row<8, XN>(x, asm_stage + ooff, s_row + ooff, (uint8_t)t);
+        else if (XN == 16 || wmax <= 16)
+            emit_staged_row<(XN < 16 ? XN : 16), XN>(x, asm_stage + ooff, s_row + ooff, (uint8_t)t);
+        else emit_staged_row<XN, XN>(x, asm_stage + ooff, s_row + ooff, (uint8_t)t);
+    }
+    s_off[t] = ooff;
     __syncthreads();
     const int32_t off = s_excl + local;
+    s_goff[t] = off;
     if (c < cn) {
         cxadj[c] = off;
         if (c == cn - 1) cxadj[cn] = off + u;
     }
-    if (small) {
-        if (XN == 8 || wmax <= 8) emit_row<8, XN>(x, cadjncy + off, cadjwgt + off);
-        else if (XN == 16 || wmax <= 16) emit_row<(XN < 16 ? XN : 16), XN>(x, cadjncy + off, cadjwgt + off);
-        else emit_row<XN, XN>(x, cadjncy + off, cadjwgt + off);
+    __syncthreads();
+    for (int f = t; f < tout; f += ASM_TILE) {
+        const int rt = s_row[f];
+        const int32_t pos = s_goff[rt] + (f - s_off[rt]);
+        const unsigned long long e = asm_stage[f];
+        cadjncy[pos] = (int32_t)(e >> 32);
+        cadjwgt[pos] = (int32_t)(uint32_t)e;
     }
     hp::lb_end(lb);
 }
@@ -1555,13 +1616,13 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     }
     // short rows + coarse xadj in one ordered pass, then the long rows' copies
     if (h.small_max <= 8)
-        HP_LAUNCH(c, contract_assemble_kernel<8>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
+        HP_LAUNCH(c, contract_assemble_kernel<8>, (unsigned)ntiles, ASM_TILE, asm_smem_bytes<8>(), cn, src, ucnt, cg.xadj,
                   cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
     else if (h.small_max <= 16)
-        HP_LAUNCH(c, contract_assemble_kernel<16>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
+        HP_LAUNCH(c, contract_assemble_kernel<16>, (unsigned)ntiles, ASM_TILE, asm_smem_bytes<16>(), cn, src, ucnt, cg.xadj,
                   cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
     else
-        HP_LAUNCH(c, contract_assemble_kernel<32>, (unsigned)ntiles, ASM_TILE, 0, cn, src, ucnt, cg.xadj,
+        HP_LAUNCH(c, contract_assemble_kernel<32>, (unsigned)ntiles, ASM_TILE, asm_smem_bytes<32>(), cn, src, ucnt, cg.xadj,
                   cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
     if (h.cnt[0] > 0)
         HP_LAUNCH(c, copy_long_rows_kernel<false>, std::min<unsigned>(blocks_for((int64_t)h.cnt[0] * 32),
@@ -1588,6 +1649,8 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
 
 int hp_coarsen_init()
 {
+    HP_CUDA(cudaFuncSetAttribute(contract_assemble_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)asm_smem_bytes<32>()));
     HP_CUDA(cudaFuncSetAttribute(match_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)ms_smem_bytes(HP_TUNE_SMALL_MATCH_MAX)));
     HP_CUDA(cudaFuncSetAttribute(contract_dense_kernel<1024, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
