@@ -73,6 +73,8 @@ struct BestCand {
     }
 };
 
+constexpr int PREF_BATCH = 4;
+
 template <bool ELIG>
 __global__ void __launch_bounds__(256)
 pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
@@ -89,20 +91,20 @@ pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__
     if (ELIG && keep_proposal(made_prev != nullptr, v, pref, elig)) return;
     const int32_t wv = vwgt[v];
     BestCand best;
-    // four entries at a time: the row loads, then the neighbour gathers, are
-    // issued together so each thread keeps several misses in flight
-    for (int32_t j0 = b; j0 < e; j0 += 4) {
-        int32_t u[4], w[4], eu[4];
+    // PREF_BATCH entries at a time: the row loads, then the neighbour gathers,
+    // are issued together so each thread keeps several misses in flight
+    for (int32_t j0 = b; j0 < e; j0 += PREF_BATCH) {
+        int32_t u[PREF_BATCH], w[PREF_BATCH], eu[PREF_BATCH];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < PREF_BATCH; q++) {
             const bool in = j0 + q < e;
             u[q] = in ? adjncy[j0 + q] : v;
             w[q] = in ? adjwgt[j0 + q] : 0;
         }
 #pragma unroll
-        for (int q = 0; q < 4; q++) eu[q] = (ELIG && u[q] != v) ? elig[u[q]] : 0;
+        for (int q = 0; q < PREF_BATCH; q++) eu[q] = (ELIG && u[q] != v) ? elig[u[q]] : 0;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < PREF_BATCH; q++) {
             if (u[q] == v) continue;
             if (ELIG) {
                 if (eu[q] == INT_MAX) continue;                     // matched
@@ -567,8 +569,9 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
     }
 }
 
-// Entry i of coarse vertex c: the i-th entry of the leader's row, then of the
-// mate's row, mapped through cmap; the coarse self key is dropped.
+// The fine rows merged into coarse row c: entry i is the i-th entry of the
+// leader's row, then of the mate's row, mapped through cmap (the coarse self key
+// is dropped).
 struct ContractSrc {
     const int4 *rinfo;
     const int32_t *adjncy, *adjwgt, *cmap;
@@ -577,13 +580,6 @@ struct ContractSrc {
         const int4 q = rinfo[c];
         r = RowInfo{q.x, q.y, q.z, q.w};
         len = r.l0 + r.l1;
-    }
-    __device__ __forceinline__ void get(int32_t c, const RowInfo &r, int32_t i, int32_t &k, int32_t &w) const
-    {
-        int32_t j = i < r.l0 ? r.s0 + i : r.s1 + (i - r.l0);
-        k = cmap[adjncy[j]];
-        w = adjwgt[j];
-        if (k == c) { k = hp::KEY_NONE; w = 0; }
     }
 };
 
