@@ -8,7 +8,7 @@
  *
  * Pins: the contraction and edge-cut semantics are checked against the
  * reference's own CPU code (hunyuangraph_cpu_create_cgraph,
- * hunyuangraph_computecut_cpu) built from /root/reference by
+ * hunyuangraph_computecut_cpu) compiled from the reference's sources by
  * oracle/build_ref.sh, and against committed fixtures in tests/golden/.
  * The reference publishes no golden vectors for matching, bisection or
  * refinement (it ships no tests); those rules are pinned only by this
