@@ -925,6 +925,38 @@ HP_API int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xa
     return HP_OK;
 }
 
+// ---- failure path of the bounded device waits ----------------------------------------
+// One warp runs the scans' look-back wait (hp::lookback_exclusive) as tile 1,
+// against a tile 0 whose status word nothing ever sets.  Lane 0 polls it
+// HP_SPIN_LIMIT times, then sets HP_STATUS_SPIN_TIMEOUT and counts the
+// predecessor as zero, so the kernel ends by itself.
+__global__ void wait_expiry_kernel(unsigned long long *tile_status, unsigned *status, int32_t *excl)
+{
+    const int32_t e = hp::lookback_exclusive(tile_status, 1, 5, status);
+    if (threadIdx.x == 0) *excl = e;
+}
+
+HP_API int hp_test_wait_expiry(hp_context *ctx)
+{
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    HP_CUDA(cudaSetDevice(ctx->device));
+    ctx->stream = ctx->own_stream;
+    unsigned long long *tiles = ctx->d_scal;                    // tile 0 (never set), tile 1
+    int32_t *excl = reinterpret_cast<int32_t *>(ctx->d_scal + 2);
+    HP_CUDA(cudaMemsetAsync(tiles, 0, 3 * sizeof(unsigned long long), ctx->stream));
+    const unsigned zero = 0;
+    HP_CUDA(cudaMemcpyAsync(ctx->d_status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    HP_LAUNCH(ctx, wait_expiry_kernel, 1, 32, 0, tiles, ctx->d_status, excl);
+    const int rc = hp_check_status(ctx);
+    int32_t e = -1;
+    HP_TRY(hp_read_scalars(ctx, excl, sizeof(int32_t), &e));
+    // the status is cleared: the context is usable for the next call
+    HP_CUDA(cudaMemcpyAsync(ctx->d_status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    HP_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (rc == HP_ERR_TIMEOUT && e != 0) return HP_ERR_INTERNAL;   // the expired predecessor counts as 0
+    return rc;
+}
+
 // ---- legacy drop-in ------------------------------------------------------------------
 static std::mutex g_legacy_mu;
 static hp_context *g_legacy = nullptr;

@@ -284,6 +284,14 @@ int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xadj,
                       const int32_t *d_adjncy, const int32_t *d_adjwgt,
                       const int32_t *d_where, void *stream, int64_t *cut);
 
+/* Test of the failure path of the bounded device waits: runs the scans'
+ * look-back wait against a predecessor flag that nothing sets.  The wait gives
+ * up after its spin limit (about a second) and the call returns what a
+ * partition would: HP_ERR_TIMEOUT.  The status word is cleared afterwards, so
+ * the context stays usable.  No counterpart in the reference (its one device
+ * spin-wait, hunyuangraph_GPU_match.h:350-358, is unbounded). */
+int hp_test_wait_expiry(hp_context *ctx);
+
 /* ---- legacy drop-in ------------------------------------------------------------
  * Identical signature to the reference (hunyuangraph_partitiongraph.h:284).
  * Uses a process-wide context on device 0 and hp_options_default(); ubvec[0]

@@ -2,6 +2,7 @@
 (coarse CSR, vertex/edge weights, matching, cmap, initial and projected
 partitions, refined partitions, cuts) must be bit-identical."""
 import ctypes as C
+import time
 
 import numpy as np
 import pytest
@@ -9,8 +10,8 @@ import pytest
 import hunyuansc25_b200 as hp
 import oracle
 from hunyuansc25_b200 import graphs
-from hunyuansc25_b200._abi import (HP_ERR_INVALID_ARG, HP_ERR_INVALID_GRAPH, HP_ERR_UNSUPPORTED,
-                                   default_options)
+from hunyuansc25_b200._abi import (HP_ERR_INVALID_ARG, HP_ERR_INVALID_GRAPH, HP_ERR_TIMEOUT,
+                                   HP_ERR_UNSUPPORTED, default_options)
 
 pytestmark = pytest.mark.gpu
 
@@ -227,6 +228,18 @@ def test_matching_fallbacks(ctx, small_match_n):
         compare_runs(ctx, g, 64)
     finally:
         ctx.set_tuning()
+
+
+def test_bounded_wait_expiry(ctx):
+    """The failure path of the device waits: the scans' look-back wait on a flag
+    that nothing sets gives up after its spin limit, the call reports
+    HP_ERR_TIMEOUT, and the same context then partitions bit-exactly."""
+    t0 = time.perf_counter()
+    rc = ctx.lib.hp_test_wait_expiry(ctx.h)
+    elapsed = time.perf_counter() - t0
+    assert rc == HP_ERR_TIMEOUT
+    assert elapsed < 60
+    compare_runs(ctx, graphs.grid2d(40, 30, seed=6, wmin=1, wmax=5), 8)
 
 
 def test_invalid_inputs(ctx):
