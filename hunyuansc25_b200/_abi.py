@@ -113,7 +113,7 @@ TUNING_DEFAULTS = {
     "trial_cta_n": 512,
     "contract_smem_cn": 49152,
     "batch_workers": 16,
-    "small_match_n": 4096,
+    "small_match_n": 8192,
 }
 
 TUNE_DEG_MAX = 1 << 24

@@ -515,7 +515,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->trial_cta_n = 512;
     t->contract_smem_cn = HP_TUNE_SMEM_CN_MAX;
     t->batch_workers = 16;
-    t->small_match_n = 4096;
+    t->small_match_n = 8192;
 }
 
 namespace {

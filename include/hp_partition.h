@@ -178,7 +178,7 @@ typedef struct hp_tuning {
                                     partition graphs concurrently                 [1, 64]       16 */
     int32_t small_match_n;       /* coarsening: levels of at most this many vertices (and
                                     64x as many adjacency entries) are matched by one
-                                    CTA; 0 = never                               [0, 8192]     4096 */
+                                    CTA; 0 = never                               [0, 8192]     8192 */
     int32_t reserved[8];         /* zero */
 } hp_tuning;
 
