@@ -10,15 +10,21 @@
 //   contraction                        hunyuangraph_GPU_contraction.h:715-1247
 //     (scatter -> segmented sort -> mark -> scan -> write; here each coarse
 //      row gathers both fine rows, merges equal coarse neighbours and is
-//      written sorted, by size class:
-//        <= 32 entries    one thread, bitonic network in registers, written in
+//      written sorted, by size class (default bounds; hp_tuning fields):
+//        <= 32 entries    staged per tile of 256 rows in shared memory, one
+//                         thread's bitonic network in registers, written in
 //                         place by one ordered pass with a decoupled look-back
 //                         that also produces the coarse xadj
 //        33..256          one warp, LSD radix sort in shared memory
-//        257..4096        one CTA, LSD radix sort in shared memory
+//        257..4096        one CTA of 256, LSD radix sort in shared memory
+//        4097..12288      one CTA of 1024, LSD radix sort in shared memory
 //        larger           one CTA, dense accumulator + presence bitmap
+//        (a level whose coarse ids fit contract_smem_cn merges every long row
+//         in a shared-memory dense accumulator instead)
 //      the long classes go through a temporary buffer and are copied to their
 //      final offsets)
+//   small levels (at most small_match_n vertices): one CTA runs the whole
+//   matching of the level in one launch (match_small_kernel)
 // The reference's matching is an atomicCAS race (nondeterministic); every
 // decision here is a pure function of the level's CSR and the seed, so the
 // CPU oracle reproduces each level bit for bit.
