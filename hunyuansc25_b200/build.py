@@ -89,8 +89,10 @@ def build_cuda(force=False, verbose_ptxas=False):
     for s in srcs:
         o = os.path.join(objdir, os.path.basename(s) + ".o")
         if force or not _newer(o, [s] + [d for d in deps if not d.endswith(".cu")]):
-            _run([nvcc, *ARCH, *flags, "-I", INCLUDE, "-I", CSRC, "-ccbin", _cc().replace("gcc", "g++"),
-                  "-c", s, "-o", o])
+            log = _run([nvcc, *ARCH, *flags, "-I", INCLUDE, "-I", CSRC, "-ccbin", _cc().replace("gcc", "g++"),
+                        "-c", s, "-o", o])
+            if verbose_ptxas:
+                sys.stderr.write(log)
         objs.append(o)
     _run([nvcc, *ARCH, "-shared", "-Xcompiler", "-fopenmp", "-ccbin", _cc().replace("gcc", "g++"),
           "-o", out, *objs, "-cudart", "static", "-lgomp"])
@@ -102,5 +104,8 @@ def build_all(force=False):
 
 
 if __name__ == "__main__":
-    for p in build_all(force="--force" in sys.argv):
-        print(p)
+    # --ptxas: rebuild the CUDA library with ptxas's per-kernel resource report
+    # (registers, shared memory, spills) on stderr
+    ptxas = "--ptxas" in sys.argv
+    print(build_gen(force="--force" in sys.argv))
+    print(build_cuda(force="--force" in sys.argv or ptxas, verbose_ptxas=ptxas))
