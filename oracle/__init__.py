@@ -63,6 +63,9 @@ def lib():
         L.ora_contract.argtypes = [C.c_int32, I32P, I32P, I32P, I32P, I32P, I32P, C.c_int32,
                                    C.POINTER(I32P), C.POINTER(I32P), C.POINTER(I32P), C.POINTER(I32P)]
         L.ora_contract.restype = C.c_int64
+        L.ora_split.argtypes = [C.c_int32, I32P, I32P, I32P, I32P, I32P, C.c_int32, I32P, I32P, I32P, I32P,
+                                I32P, I32P]
+        L.ora_split.restype = C.c_int64
         L.ora_free.argtypes = [C.c_void_p]
         L.ora_part_targets.argtypes = [C.c_int64, C.c_int32, C.POINTER(C.c_float), C.c_float, I64P, I64P]
         L.ora_bisect_ub_fx.argtypes = [C.c_float, C.c_int32]
@@ -173,6 +176,24 @@ def contract(g, match_, cmap, cn):
     for p in (px, pa, pw, pv):
         lib().ora_free(C.cast(p, C.c_void_p))
     return out
+
+
+def split(g, where, side):
+    """One side of the 2-way split the recursive bisection makes:
+    (xadj, adjncy, adjwgt, vwgt, label) of the induced subgraph."""
+    n, m = g.nvtxs, g.nedges
+    sn = C.c_int32()
+    sx = np.empty(n + 1, np.int32)
+    sa = np.empty(max(m, 1), np.int32)
+    sw = np.empty(max(m, 1), np.int32)
+    sv = np.empty(max(n, 1), np.int32)
+    sl = np.empty(max(n, 1), np.int32)
+    mm = lib().ora_split(n, _p(i32(g.xadj)), _p(i32(g.adjncy)), _p(i32(g.vwgt)), _p(i32(g.adjwgt)),
+                         _p(i32(where)), side, C.byref(sn), _p(sx), _p(sa), _p(sw), _p(sv), _p(sl))
+    if mm < 0:
+        raise ValueError("where[] must hold 0 or 1")
+    k = sn.value
+    return sx[:k + 1], sa[:mm], sw[:mm], sv[:k], sl[:k]
 
 
 def part_targets(tvwgt, nparts, ubfactor, tpwgts=None):

@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libhp_ref.so: the reference's own CPU contraction, edge
-# cut and CPU coarsening, compiled from the reference sources in place
+# cut, graph split and CPU coarsening, compiled from the reference sources in place
 # (REF_DIR, default /root/reference) through oracle/ref_harness.cu.
 # TEST INFRASTRUCTURE ONLY; output stays in oracle/_ref/ (git-ignored).
 set -euo pipefail

@@ -572,6 +572,48 @@ typedef struct {
     int32_t *xadj, *adjncy, *adjwgt, *vwgt, *label;
 } sub_t;
 
+/* The two induced subgraphs of a 2-way split (hunyuangraph_splitgraph,
+ * hunyuangraph_CPU_splitgraph.h:8-167): each side's vertices renumbered in id
+ * order, rows in their original order with the other side's neighbours
+ * dropped, vertex weights and labels carried over. */
+static void split2(const sub_t *g, const int32_t *side_of, sub_t s[2])
+{
+    const int32_t n = g->n;
+    int32_t *lid = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t cnt[2] = {0, 0};
+    for (int32_t v = 0; v < n; v++) lid[v] = cnt[side_of[v]]++;
+    for (int side = 0; side < 2; side++) {
+        s[side].n = cnt[side];
+        s[side].xadj = (int32_t *)xmalloc(sizeof(int32_t) * ((size_t)cnt[side] + 1));
+        s[side].vwgt = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(cnt[side] > 0 ? cnt[side] : 1));
+        s[side].label = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(cnt[side] > 0 ? cnt[side] : 1));
+        int64_t m = 0;
+        for (int32_t v = 0; v < n; v++) {
+            if (side_of[v] != side) continue;
+            for (int32_t j = g->xadj[v]; j < g->xadj[v + 1]; j++) m += (side_of[g->adjncy[j]] == side);
+        }
+        s[side].adjncy = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+        s[side].adjwgt = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+        int64_t e = 0;
+        for (int32_t v = 0; v < n; v++) {
+            if (side_of[v] != side) continue;
+            int32_t lv = lid[v];
+            s[side].xadj[lv] = (int32_t)e;
+            s[side].vwgt[lv] = g->vwgt[v];
+            s[side].label[lv] = g->label[v];
+            for (int32_t j = g->xadj[v]; j < g->xadj[v + 1]; j++) {
+                int32_t u = g->adjncy[j];
+                if (side_of[u] != side) continue;
+                s[side].adjncy[e] = lid[u];
+                s[side].adjwgt[e] = g->adjwgt[j];
+                e++;
+            }
+        }
+        s[side].xadj[cnt[side]] = (int32_t)e;
+    }
+    free(lid);
+}
+
 static void rb(const sub_t *g, int32_t nparts, int32_t fpart, const int64_t *tw, int64_t ub2_fx,
                int32_t starts, int32_t fm_passes, int32_t *out_where)
 {
@@ -632,39 +674,7 @@ static void rb(const sub_t *g, int32_t nparts, int32_t fpart, const int64_t *tw,
 
     /* split into the two induced subgraphs, vertex order preserved */
     sub_t s[2];
-    int32_t *lid = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)n);
-    int32_t cnt[2] = {0, 0};
-    for (int32_t v = 0; v < n; v++) lid[v] = cnt[best[v]]++;
-    for (int side = 0; side < 2; side++) {
-        s[side].n = cnt[side];
-        s[side].xadj = (int32_t *)xmalloc(sizeof(int32_t) * ((size_t)cnt[side] + 1));
-        s[side].vwgt = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)cnt[side]);
-        s[side].label = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)cnt[side]);
-        int64_t m = 0;
-        for (int32_t v = 0; v < n; v++) {
-            if (best[v] != side) continue;
-            for (int32_t j = g->xadj[v]; j < g->xadj[v + 1]; j++) m += (best[g->adjncy[j]] == side);
-        }
-        s[side].adjncy = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)m);
-        s[side].adjwgt = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)m);
-        int64_t e = 0;
-        for (int32_t v = 0; v < n; v++) {
-            if (best[v] != side) continue;
-            int32_t lv = lid[v];
-            s[side].xadj[lv] = (int32_t)e;
-            s[side].vwgt[lv] = g->vwgt[v];
-            s[side].label[lv] = g->label[v];
-            for (int32_t j = g->xadj[v]; j < g->xadj[v + 1]; j++) {
-                int32_t u = g->adjncy[j];
-                if (best[u] != side) continue;
-                s[side].adjncy[e] = lid[u];
-                s[side].adjwgt[e] = g->adjwgt[j];
-                e++;
-            }
-        }
-        s[side].xadj[cnt[side]] = (int32_t)e;
-    }
-    free(lid);
+    split2(g, best, s);
     free(best);
     rb(&s[0], kl, fpart, tw, ub2_fx, starts, fm_passes, out_where);
     rb(&s[1], nparts - kl, fpart + kl, tw, ub2_fx, starts, fm_passes, out_where);
@@ -672,6 +682,33 @@ static void rb(const sub_t *g, int32_t nparts, int32_t fpart, const int64_t *tw,
         free(s[side].xadj); free(s[side].adjncy); free(s[side].adjwgt);
         free(s[side].vwgt); free(s[side].label);
     }
+}
+
+int64_t ora_split(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int32_t *vwgt,
+                  const int32_t *adjwgt, const int32_t *where, int32_t side, int32_t *sn,
+                  int32_t *sxadj, int32_t *sadjncy, int32_t *sadjwgt, int32_t *svwgt, int32_t *slabel)
+{
+    if (n < 0 || side < 0 || side > 1 || !sn) return -1;
+    for (int32_t v = 0; v < n; v++)
+        if (where[v] != 0 && where[v] != 1) return -1;
+    int32_t *label = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    for (int32_t v = 0; v < n; v++) label[v] = v;
+    sub_t g = {n, (int32_t *)xadj, (int32_t *)adjncy, (int32_t *)adjwgt, (int32_t *)vwgt, label};
+    sub_t s[2];
+    split2(&g, where, s);
+    const sub_t *o = &s[side];
+    const int64_t m = o->xadj[o->n];
+    *sn = o->n;
+    memcpy(sxadj, o->xadj, sizeof(int32_t) * ((size_t)o->n + 1));
+    memcpy(sadjncy, o->adjncy, sizeof(int32_t) * (size_t)m);
+    memcpy(sadjwgt, o->adjwgt, sizeof(int32_t) * (size_t)m);
+    memcpy(svwgt, o->vwgt, sizeof(int32_t) * (size_t)o->n);
+    memcpy(slabel, o->label, sizeof(int32_t) * (size_t)o->n);
+    for (int k = 0; k < 2; k++) {
+        free(s[k].xadj); free(s[k].adjncy); free(s[k].adjwgt); free(s[k].vwgt); free(s[k].label);
+    }
+    free(label);
+    return m;
 }
 
 int ora_initpart(int32_t n, const int32_t *xadj, const int32_t *adjncy,

@@ -66,6 +66,15 @@ void ora_part_targets(int64_t tvwgt, int32_t nparts, const float *tpwgts, float 
                       int64_t *opt, int64_t *maxp);
 int64_t ora_bisect_ub_fx(float ubfactor, int32_t nparts);
 
+/* One side (0 or 1) of a 2-way split into induced subgraphs, as the recursive
+ * bisection splits: vertices renumbered in id order, rows in their original
+ * order without the other side's neighbours, labels = original ids.  Buffers:
+ * n + 1 (sxadj), m (sadjncy, sadjwgt), n (svwgt, slabel).  Returns the side's
+ * adjacency count, or -1 for a where[] entry outside {0, 1}. */
+int64_t ora_split(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int32_t *vwgt,
+                  const int32_t *adjwgt, const int32_t *where, int32_t side, int32_t *sn,
+                  int32_t *sxadj, int32_t *sadjncy, int32_t *sadjwgt, int32_t *svwgt, int32_t *slabel);
+
 /* Recursive-bisection initial partition of a (small) graph. */
 int ora_initpart(int32_t n, const int32_t *xadj, const int32_t *adjncy,
                  const int32_t *vwgt, const int32_t *adjwgt, int32_t nparts,

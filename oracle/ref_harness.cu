@@ -1,9 +1,9 @@
 // ref_harness.cu — TEST INFRASTRUCTURE ONLY.  C wrappers around the
 // reference's own CPU routines, compiled from the reference sources where they
 // lie (see build_ref.sh; nothing of the reference is copied into this
-// repository).  Used by tests/ to pin the oracle's contraction and edge-cut
-// semantics against the reference implementation, and by bench.py's CPU
-// baseline to time the reference's CPU coarsening.
+// repository).  Used by tests/ to pin the oracle's contraction, edge-cut and
+// graph-split semantics against the reference implementation, and by
+// bench.py's CPU baseline to time the reference's CPU coarsening.
 #include "HunyuanGRAPH.h"
 
 extern "C" {
@@ -61,6 +61,46 @@ int ref_cpu_coarsen(int n, const int *xadj, const int *adjncy, const int *vwgt, 
     for (hunyuangraph_graph_t *t = c; t->finer; t = t->finer) levels++;
     *coarsest_n = c->nvtxs;
     return levels;
+}
+
+// hunyuangraph_splitgraph (hunyuangraph_CPU_splitgraph.h:8-167): the two
+// induced subgraphs of a 2-way partition; side 0 or 1 is copied out.  The
+// function copies the rows of vertices whose bndptr is -1 whole and filters
+// the others, so bndptr is set here to -1 exactly for the vertices with no
+// neighbour on the other side.  Labels start as the vertex ids.
+int ref_cpu_split(int n, const int *xadj, const int *adjncy, const int *vwgt, const int *adjwgt,
+                  const int *where, int side, int *sn, int *sxadj, int *sadjncy, int *sadjwgt, int *svwgt,
+                  int *slabel)
+{
+    hunyuangraph_admin_t admin;
+    memset(&admin, 0, sizeof(admin));
+    admin.mcore = hunyuangraph_create_mcore(0);
+    hunyuangraph_graph_t *g = hunyuangraph_set_first_level_graph(
+        n, (int *)xadj, (int *)adjncy, (int *)vwgt, (int *)adjwgt);
+    const size_t cap = (size_t)(n > 0 ? n : 1);
+    int *label = (int *)malloc(sizeof(int) * cap);
+    int *wh = (int *)malloc(sizeof(int) * cap);
+    int *bnd = (int *)malloc(sizeof(int) * cap);
+    for (int i = 0; i < n; i++) {
+        label[i] = i;
+        wh[i] = where[i];
+        bnd[i] = -1;
+        for (int j = xadj[i]; j < xadj[i + 1]; j++)
+            if (where[adjncy[j]] != where[i]) bnd[i] = 0;
+    }
+    g->label = label;
+    g->where = wh;
+    g->bndptr = bnd;
+    hunyuangraph_graph_t *l = nullptr, *r = nullptr;
+    hunyuangraph_splitgraph(&admin, g, &l, &r);
+    hunyuangraph_graph_t *o = side ? r : l;
+    *sn = o->nvtxs;
+    memcpy(sxadj, o->xadj, sizeof(int) * (o->nvtxs + 1));
+    memcpy(sadjncy, o->adjncy, sizeof(int) * o->nedges);
+    memcpy(sadjwgt, o->adjwgt, sizeof(int) * o->nedges);
+    memcpy(svwgt, o->vwgt, sizeof(int) * o->nvtxs);
+    memcpy(slabel, o->label, sizeof(int) * o->nvtxs);
+    return o->nedges;
 }
 
 }

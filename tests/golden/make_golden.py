@@ -5,6 +5,9 @@
   edge cut (hunyuangraph_computecut_cpu, hunyuangraph_graph.h:144-155), run
   through oracle/_ref/libhp_ref.so (built from the reference sources by
   oracle/build_ref.sh), on small seeded graphs with a seeded matching.
+* ref_split_*.npz — the reference's own CPU graph split (hunyuangraph_splitgraph,
+  hunyuangraph_CPU_splitgraph.h:8-167), both sides, on the same graphs with a
+  seeded 2-way partition.
 * oracle_vcycle.json — per-level sizes, cuts and array digests of the oracle's
   V-cycle on the 256x256 grid workload (k = 8) and a 3-D grid, so that any
   change of the oracle's rules is visible in review.
@@ -67,15 +70,40 @@ def digest(a):
     return hashlib.sha256(np.ascontiguousarray(a, dtype=np.int32).tobytes()).hexdigest()[:16]
 
 
-def main():
-    ref = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libhp_ref.so"))
-    cases = {
+def cases():
+    return {
         "grid2d_16x16_w": graphs.grid2d(16, 16, seed=9, wmin=1, wmax=20),
         "grid3d_6": graphs.grid3d(6, 6, 6, seed=2, wmin=1, wmax=10),
         "rmat_s8": graphs.rmat(8, 8, seed=3, wmin=1, wmax=100),
         "rgg_600": graphs.rgg(600, 10.0, seed=4),
     }
-    for name, g in cases.items():
+
+
+def make_split_fixtures(ref):
+    """Both sides of the reference's split under a seeded 2-way partition."""
+    for name, g in cases().items():
+        n, m = g.nvtxs, g.nedges
+        where = (np.random.default_rng(77).random(n) < 0.4).astype(np.int32)
+        out = {"xadj": g.xadj, "adjncy": g.adjncy, "vwgt": g.vwgt, "adjwgt": g.adjwgt, "where": where}
+        for side in (0, 1):
+            sn = C.c_int32()
+            sx = np.empty(n + 1, np.int32)
+            sa = np.empty(max(m, 1), np.int32)
+            sw = np.empty(max(m, 1), np.int32)
+            sv = np.empty(max(n, 1), np.int32)
+            sl = np.empty(max(n, 1), np.int32)
+            mm = ref.ref_cpu_split(n, p(g.xadj), p(g.adjncy), p(g.vwgt), p(g.adjwgt), p(where), side,
+                                   C.byref(sn), p(sx), p(sa), p(sw), p(sv), p(sl))
+            k = sn.value
+            out.update({f"s{side}_xadj": sx[:k + 1], f"s{side}_adjncy": sa[:mm], f"s{side}_adjwgt": sw[:mm],
+                        f"s{side}_vwgt": sv[:k], f"s{side}_label": sl[:k]})
+            print(name, "side", side, k, mm)
+        np.savez_compressed(os.path.join(HERE, f"ref_split_{name}.npz"), **out)
+
+
+def main():
+    ref = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libhp_ref.so"))
+    for name, g in cases().items():
         match, cmap, cn = seeded_matching(g, 1234)
         rx = np.empty(cn + 1, np.int32)
         ra = np.empty(g.nedges, np.int32)
@@ -90,6 +118,7 @@ def main():
                             match=match, cmap=cmap, cn=np.int32(cn), cxadj=rx, cadjncy=ra[:mc],
                             cadjwgt=rw[:mc], cvwgt=rv, part=part, cut=np.int64(cut))
         print(name, g.nvtxs, g.nedges, "->", cn, mc, "cut", cut)
+    make_split_fixtures(ref)
 
     oracle.set_threads(4)
     snap = {}

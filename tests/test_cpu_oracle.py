@@ -55,6 +55,46 @@ def test_contract_matches_reference_golden(path):
 
 def test_golden_fixtures_present():
     assert len(glob.glob(os.path.join(GOLDEN, "ref_contract_*.npz"))) >= 4
+    assert len(glob.glob(os.path.join(GOLDEN, "ref_split_*.npz"))) >= 4
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "ref_split_*.npz"))))
+def test_split_matches_reference_golden(path):
+    """The recursive bisection's split into induced subgraphs equals the
+    reference's hunyuangraph_splitgraph on both sides, arrays and order."""
+    d = np.load(path)
+    g = G(d["xadj"], d["adjncy"], d["vwgt"], d["adjwgt"])
+    for side in (0, 1):
+        got = oracle.split(g, d["where"], side)
+        for arr, name in zip(got, ("xadj", "adjncy", "adjwgt", "vwgt", "label")):
+            assert np.array_equal(arr, d[f"s{side}_{name}"]), (side, name)
+
+
+def test_split_rejects_non_binary_where():
+    g = graphs.grid2d(4, 4)
+    with pytest.raises(ValueError):
+        oracle.split(g, np.full(g.nvtxs, 2, np.int32), 0)
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.REFLIB), reason="reference CPU harness not built")
+def test_split_matches_reference_live():
+    ref = C.CDLL(oracle.REFLIB)
+    I = C.POINTER(C.c_int32)
+    p = lambda a: a.ctypes.data_as(I)  # noqa: E731
+    for gi, g in enumerate((graphs.grid3d(12, 11, 10, seed=8, wmin=1, wmax=10), graphs.rmat(11, 8, seed=21))):
+        n, m = g.nvtxs, g.nedges
+        for s in range(3):
+            where = (np.random.default_rng(100 * gi + s).random(n) < 0.3 + 0.2 * s).astype(np.int32)
+            for side in (0, 1):
+                sn = C.c_int32()
+                rx, rv, rl = (np.empty(n + 1, np.int32), np.empty(n, np.int32), np.empty(n, np.int32))
+                ra, rw = np.empty(m, np.int32), np.empty(m, np.int32)
+                mm = ref.ref_cpu_split(n, p(g.xadj), p(g.adjncy), p(g.vwgt), p(g.adjwgt), p(where), side,
+                                       C.byref(sn), p(rx), p(ra), p(rw), p(rv), p(rl))
+                k = sn.value
+                ox, oa, ow, ov, ol = oracle.split(g, where, side)
+                assert np.array_equal(ox, rx[:k + 1]) and np.array_equal(oa, ra[:mm])
+                assert np.array_equal(ow, rw[:mm]) and np.array_equal(ov, rv[:k]) and np.array_equal(ol, rl[:k])
 
 
 @pytest.mark.skipif(not os.path.exists(oracle.REFLIB), reason="reference CPU harness not built")

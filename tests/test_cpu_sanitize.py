@@ -85,6 +85,24 @@ static void components(const hp_graph *g)
     const int64_t cm = ora_contract(n, g->xadj, g->adjncy, g->vwgt, g->adjwgt, match, cmap, cn, &cx, &ca, &cw, &cv);
     CHECK(cm >= 0 && cm <= g->nedges && cx[cn] == cm);
     ora_free(cx); ora_free(ca); ora_free(cw); ora_free(cv);
+    /* both sides of a 2-way split, and a where[] outside {0, 1} refused */
+    int32_t *where = malloc(sizeof(int32_t) * (size_t)n);
+    for (int32_t i = 0; i < n; i++) where[i] = (int32_t)((i * 2654435761u) % 3u == 0);
+    int32_t *sx = malloc(sizeof(int32_t) * (size_t)(n + 1)), *sv = malloc(sizeof(int32_t) * (size_t)n);
+    int32_t *sl = malloc(sizeof(int32_t) * (size_t)n);
+    int32_t *sa = malloc(sizeof(int32_t) * (size_t)g->nedges), *sw = malloc(sizeof(int32_t) * (size_t)g->nedges);
+    int64_t total = 0;
+    for (int side = 0; side < 2; side++) {
+        int32_t sn = -1;
+        const int64_t sm = ora_split(n, g->xadj, g->adjncy, g->vwgt, g->adjwgt, where, side, &sn, sx, sa, sw, sv, sl);
+        CHECK(sm >= 0 && sn >= 0 && sx[sn] == sm);
+        total += sn;
+    }
+    CHECK(total == n);
+    where[0] = 5;
+    int32_t sn = 0;
+    CHECK(ora_split(n, g->xadj, g->adjncy, g->vwgt, g->adjwgt, where, 0, &sn, sx, sa, sw, sv, sl) == -1);
+    free(where); free(sx); free(sv); free(sl); free(sa); free(sw);
     free(match); free(cmap);
 }
 
