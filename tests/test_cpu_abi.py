@@ -3,6 +3,8 @@ the Python mirror matches the header.  No compute call is made here."""
 import ctypes as C
 import os
 import re
+import shutil
+import subprocess
 
 import pytest
 
@@ -32,6 +34,46 @@ def test_partition_header_symbols_exported(lib):
     assert "hp_partition" in names and "hunyuangraph_PartitionGraph" in names
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
+
+
+def test_c_program_links_every_entry_point(lib, tmp_path):
+    """A C caller compiled against include/hp_partition.h links libhp_b200.so:
+    every declared function resolves at link time (the legacy
+    hunyuangraph_PartitionGraph among them), and the entry points that need
+    no device run."""
+    cc = shutil.which("gcc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    names = declared_functions("hp_partition.h")
+    refs = "\n".join(f"    (void *)&{n}," for n in names)
+    src = tmp_path / "caller.c"
+    src.write_text(f"""#include <stdio.h>
+#include <string.h>
+#include "hp_partition.h"
+static void *const entry_points[] = {{
+{refs}
+}};
+int main(void)
+{{
+    for (size_t i = 0; i < sizeof entry_points / sizeof entry_points[0]; i++)
+        if (!entry_points[i]) return 2;
+    hp_options o;
+    hp_options_default(&o);
+    hp_tuning t;
+    hp_tuning_default(&t);
+    if (o.version != HP_OPTIONS_VERSION || o.match_rounds != 6 || t.small_match_n != 8192) return 3;
+    if (strcmp(hp_strerror(HP_ERR_TIMEOUT), hp_strerror(HP_OK)) == 0) return 4;
+    printf("linked %zu entry points\\n", sizeof entry_points / sizeof entry_points[0]);
+    return 0;
+}}
+""")
+    libdir = os.path.dirname(hp.library_path())
+    exe = tmp_path / "caller"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe),
+                    "-L", libdir, "-lhp_b200", f"-Wl,-rpath,{libdir}"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert f"linked {len(names)} entry points" in r.stdout
 
 
 def test_gen_header_symbols_exported():
