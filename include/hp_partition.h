@@ -286,7 +286,7 @@ int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xadj,
 
 /* Test of the failure path of the bounded device waits: runs the scans'
  * look-back wait against a predecessor flag that nothing sets.  The wait gives
- * up after its spin limit (about a second) and the call returns what a
+ * up after its spin limit (2^22 polls) and the call returns what a
  * partition would: HP_ERR_TIMEOUT.  The status word is cleared afterwards, so
  * the context stays usable.  No counterpart in the reference (its one device
  * spin-wait, hunyuangraph_GPU_match.h:350-358, is unbounded). */
