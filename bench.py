@@ -11,8 +11,15 @@ ranks.  e2e repeats the metric through the host-buffer C-ABI entry point
 (hp_partition) with pinned inputs, the H2D copies and the D2H of the partition
 inside the timed call.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload grid3d|grid2d|rmat22|rgg24]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload rmat22|grid3d|grid2d|rgg24|batch]
+                  [--refiner learned|plain] [--no-compare]
   python bench.py --impl reference ...   # the CPU path on the host cores
+
+Default: R-MAT scale 22, k = 256, the metric's own configuration.  The timed
+refiner (value, e2e) is the learned move proposals there; the plain refiner is
+timed the same way right after it and learned_vs_plain reports both times,
+both cuts and their ratio.  cpu_baseline checks the plain cut against the CPU
+port of the path.
 """
 from __future__ import annotations
 
@@ -41,7 +48,7 @@ WORKLOADS = {
     "grid2d": dict(desc="grid2d 256x256 5-point, unit weights, k=8, imbalance 1.03, coarsen to k*20",
                    k=8, ub=1.03, coarsen_to=160, make=lambda: graphs.config_grid2d()),
     "rmat22": dict(desc="R-MAT scale 22 edge factor 16 (a,b,c=.57,.19,.19, seed 3), weights U{1..100}, "
-                        "k=256, imbalance 1.03", k=256, ub=1.03, coarsen_to=0,
+                        "k=256, imbalance 1.03", k=256, ub=1.03, coarsen_to=0, refiner="learned",
                    make=lambda: graphs.config_rmat(22)),
     "rgg24": dict(desc="RGG 2^24 points (seed 4), mean degree 12, w=int(1000(1-d/r))+1, k=1024, "
                        "imbalance 1.05", k=1024, ub=1.05, coarsen_to=0,
@@ -52,6 +59,8 @@ WORKLOADS["batch"] = dict(desc="1,024 graphs, n log-uniform in [1e3, 2e5] (seed 
                           k=0, ub=1.03, coarsen_to=0, make=None)
 METRIC = "partition ms & edges/s at equal edge cut (±1%), learned vs plain, 1 B200"
 L2_FLUSH_BYTES = 256 << 20
+# kernel classes that run inside the pass graphs (timed from an eager profiled step)
+PASS_CLASSES = ("lp", "rebuild", "rebalance", "apply")
 
 
 def load_peaks():
@@ -295,13 +304,14 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="grid3d", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="rmat22", choices=sorted(WORKLOADS))
+    ap.add_argument("--refiner", default=None, choices=["learned", "plain"],
+                    help="the refiner of the timed steps (value, e2e); default: the workload's "
+                         "(learned on rmat22, the metric's configuration; plain elsewhere)")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="do not time the other refiner (no learned_vs_plain)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--learned", action="store_true",
-                    help="time the learned move proposals (MLP) instead of the plain refiner")
-    ap.add_argument("--compare-learned", action="store_true",
-                    help="also time the learned refiner and report learned vs plain")
     ap.add_argument("--learned-threshold", type=float, default=None)
     ap.add_argument("--tuning", default="auto",
                     help="kernel tuning file; 'auto' loads hunyuansc25_b200/tuning/<workload>.json when "
@@ -334,64 +344,74 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", device_id=dev, timeout=timedelta(seconds=300))
 
+    refiner = args.refiner or spec.get("refiner", "plain")
+    learned_main = refiner == "learned"
+    compare = not args.no_compare
     ctx = hp.Context(local)
     apply_tuning(ctx, args)
     from hunyuansc25_b200 import learn
-    if args.learned or args.compare_learned:
+    if learned_main or compare:
         mparams, mthr, _ = learn.load_params()
         ctx.mlp_set_params(mparams, mthr if args.learned_threshold is None else args.learned_threshold)
-    # the timed steps run without the kernel-class profiler; one extra step
-    # after the timed region records the classes
-    opt = default_options(coarsen_to=spec["coarsen_to"], profile=0, learned=1 if args.learned else 0)
+
+    def opts(learned, **kw):
+        return default_options(coarsen_to=spec["coarsen_to"], learned=1 if learned else 0, **kw)
+
+    # the timed steps run without the kernel-class profiler; profiled steps
+    # after the timed region record the classes
+    opt_main = opts(learned_main)
+    opt_other = opts(not learned_main)
     xadj, adj, vw, ew = (torch.from_numpy(a).to(dev) for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt))
     part = torch.empty(g.nvtxs, dtype=torch.int32, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
     # one stream for the L2 flush, the events and the library's launches
     stream = torch.cuda.Stream(dev)
 
-    def step(o=None):
-        return ctx.partition_device(xadj, adj, spec["k"], vw, ew, spec["ub"], options=o or opt, stream=stream,
-                                    part=part)
+    def step(o):
+        return ctx.partition_device(xadj, adj, spec["k"], vw, ew, spec["ub"], options=o, stream=stream, part=part)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
+    def timed_arm(o):
+        """W untimed warm-up steps, then K steps, each timed with CUDA events on
+        the library's stream after an L2 flush: (per-step ms, cut, stats)."""
+        for _ in range(args.warmup):
+            step(o)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        evs, sts, c = [], [], None
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _, c = step(o)
+            e1.record(stream)
+            evs.append((e0, e1))
+            sts.append(ctx.stats())
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        return [a.elapsed_time(b) for a, b in evs], c, sts
 
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    evs = []
-    stats = []
-    cut = None
-    for _ in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        _, cut = step()
-        e1.record(stream)
-        evs.append((e0, e1))
-        stats.append(ctx.stats())
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
+    step_ms, cut, stats = timed_arm(opt_main)
+    other = timed_arm(opt_other) if compare else None
     clocks = sampler.stop()
-    step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = sum(step_ms)
     t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     job_ms = float(t.item())
     value = world * args.steps * m_und / (job_ms / 1000.0)
-
     launches = sum(s.kernel_launches for s in stats)
+    last = stats[-1]
 
     def one_step(o):
-        """One untimed-region step on the library's stream: (device ms, cut, stats)."""
+        """One step outside the timed region on the library's stream: (device ms, cut, stats)."""
         with torch.cuda.stream(stream):
             flush.zero_()
         a = torch.cuda.Event(enable_timing=True)
@@ -402,84 +422,77 @@ def main():
         torch.cuda.synchronize()
         return a.elapsed_time(b), c, ctx.stats()
 
-    # Kernel classes from the library's CUDA-event profile, recorded after the
-    # timed region.  Coarsening, gain-table builds and bisection come from one
-    # profiled step with graphed passes; the LP, gain-row rebuild and rebalance
-    # launches run inside the pass graphs there, so they come from one profiled
-    # step with eager passes.  The graph-vs-eager comparison times one eager step
-    # without the profiler.
-    _, _, pst = one_step(default_options(coarsen_to=spec["coarsen_to"], profile=1, learned=opt.learned))
-    eager_ms, ecut, _ = one_step(default_options(coarsen_to=spec["coarsen_to"], eager=1, learned=opt.learned))
-    _, _, est = one_step(default_options(coarsen_to=spec["coarsen_to"], profile=1, eager=1, learned=opt.learned))
+    # Kernel classes of the timed refiner from the library's CUDA-event
+    # profile, recorded after the timed region.  Coarsening, gain-table builds
+    # and bisection come from one profiled step with graphed passes; the pass
+    # classes (LP, gain-row rebuild, rebalance, move application) run inside
+    # the pass graphs there, so they come from one profiled step with eager
+    # passes.  The graph-vs-eager comparison times one eager step without the
+    # profiler.
+    _, _, pst = one_step(opts(learned_main, profile=1))
+    eager_ms, ecut, _ = one_step(opts(learned_main, eager=1))
+    _, _, est = one_step(opts(learned_main, profile=1, eager=1))
+    ncls = len(PROF_NAMES)
     prof_ms = np.array(list(pst.prof_ms), dtype=np.float64)
     prof_bytes = np.array(list(pst.prof_bytes), dtype=np.float64)
     prof_launch = np.array(list(pst.prof_launches), dtype=np.float64)
     source = {}
-    for i in range(8):
-        if PROF_NAMES[i] in ("lp", "rebuild", "rebalance"):
+    for i in range(ncls):
+        if PROF_NAMES[i] in PASS_CLASSES:
             prof_ms[i] = est.prof_ms[i]
             prof_bytes[i] = est.prof_bytes[i]
             prof_launch[i] = est.prof_launches[i]
             source[i] = "eager profiled step"
         else:
             source[i] = "profiled step"
-    with_bytes = [i for i in range(8) if prof_bytes[i] > 0]
-    dom = max(with_bytes, key=lambda i: prof_ms[i]) if with_bytes else 0
+    timed = [i for i in range(ncls) if PROF_NAMES[i] and prof_ms[i] > 0]
+    dom = max(timed, key=lambda i: prof_ms[i]) if timed else 0   # the class with the most device time
     peak, peak_kind = load_peaks()
-    achieved = prof_bytes[dom] / (prof_ms[dom] / 1000.0) / 1e9 if prof_ms[dom] > 0 else 0.0
+    achieved = prof_bytes[dom] / (prof_ms[dom] / 1000.0) / 1e9 if prof_ms[dom] > 0 and prof_bytes[dom] > 0 else None
     traffic_ratio = load_traffic(args.workload, PROF_NAMES[dom])
     per_launch_alg = prof_bytes[dom] / max(prof_launch[dom], 1)
     roofline = {
-        "bound": "hbm", "kernel": PROF_NAMES[dom], "achieved": round(achieved, 1), "peak": peak,
-        "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+        "bound": "hbm", "kernel": PROF_NAMES[dom], "achieved": round(achieved, 1) if achieved else None,
+        "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4) if achieved else None,
+        "peak_kind": peak_kind,
         "traffic": (round(traffic_ratio * per_launch_alg) if traffic_ratio else None),
+        "traffic_source": ("DRAM bytes per algorithmic byte of this class from the committed ncu capture "
+                           "(profiles/traffic.json) x its algorithmic bytes per launch" if traffic_ratio else None),
         "algorithmic_bytes_per_launch": int(per_launch_alg),
-        "classes": {PROF_NAMES[i]: {"ms_per_step": round(prof_ms[i], 3),
+        "class_ms_per_step": round(prof_ms[dom], 3), "class_bytes_per_step": int(prof_bytes[dom]),
+        "launches_per_step": int(prof_launch[dom]),
+        "classes": {PROF_NAMES[i]: {"ms_per_step": round(prof_ms[i], 3), "bytes_per_step": int(prof_bytes[i]),
                                     "GB/s": (round(prof_bytes[i] / (prof_ms[i] / 1e3) / 1e9, 1)
                                              if prof_bytes[i] > 0 and prof_ms[i] > 0 else None),
                                     "launches": int(prof_launch[i]), "source": source[i]}
-                    for i in range(8) if PROF_NAMES[i] and prof_ms[i] > 0},
+                    for i in timed},
     }
     graph_vs_eager = {"graph_ms": round(job_ms / args.steps, 3), "eager_ms": round(eager_ms, 3),
                       "speedup": round(eager_ms / (job_ms / args.steps), 4), "identical_cut": int(ecut) == int(cut),
                       "eager_launches": int(est.kernel_launches)}
-    last = stats[-1]
 
     learned_cmp = None
-    if args.compare_learned:
-        # the learned steps are timed exactly as the plain timed steps above
-        lopt = default_options(coarsen_to=spec["coarsen_to"], learned=1)
-        for _ in range(args.warmup):
-            step(lopt)
-        torch.cuda.synchronize()
-        levs, lcut = [], None
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            _, lcut = step(lopt)
-            e1.record(stream)
-            levs.append((e0, e1))
-        torch.cuda.synchronize()
-        lms = [a.elapsed_time(b) for a, b in levs]
-        plain_ms = job_ms / args.steps
-        learned_ms = sum(lms) / len(lms)
-        learned_cmp = {"plain_ms": round(plain_ms, 3), "learned_ms": round(learned_ms, 3),
-                       "speedup": round(plain_ms / learned_ms, 4), "plain_cut": int(cut), "learned_cut": int(lcut),
-                       "cut_ratio": round(int(lcut) / max(1, int(cut)), 5),
-                       "learned_balanced": ctx.stats().max_excess <= 0}
+    plain_cut = None if learned_main else int(cut)
+    if other is not None:
+        oms, ocut, osts = other
+        lms, lcut, lst = (step_ms, cut, stats) if learned_main else (oms, ocut, osts)
+        pms, pcut, pst_ = (oms, ocut, osts) if learned_main else (step_ms, cut, stats)
+        plain_cut = int(pcut)
+        learned_cmp = {"plain_ms": round(sum(pms) / len(pms), 3), "learned_ms": round(sum(lms) / len(lms), 3),
+                       "speedup": round(sum(pms) / sum(lms), 4), "plain_cut": int(pcut), "learned_cut": int(lcut),
+                       "cut_ratio": round(int(lcut) / max(1, int(pcut)), 5),
+                       "plain_balanced": pst_[-1].max_excess <= 0, "learned_balanced": lst[-1].max_excess <= 0,
+                       "timing": "both arms: the same warm-up and step counts, L2 flush, stream, events and tuning"}
 
-    # end-to-end through the host-buffer entry point with pinned inputs
+    # end-to-end through the host-buffer entry point with pinned inputs, the
+    # timed refiner's options
     pin = [torch.from_numpy(a).pin_memory() for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt)]
     hn = [p.numpy() for p in pin]
-    e2e_opt = default_options(coarsen_to=spec["coarsen_to"])
     e2e_t = []
     for i in range(0 if args.kernel_only else args.e2e_steps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        hpart, hcut = ctx.partition(hn[0], hn[1], spec["k"], hn[2], hn[3], spec["ub"], options=e2e_opt)
+        hpart, hcut = ctx.partition(hn[0], hn[1], spec["k"], hn[2], hn[3], spec["ub"], options=opt_main)
         dt = time.perf_counter() - t0
         if i > 0:
             e2e_t.append(dt)
@@ -492,11 +505,15 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.kernel_only:
+        if plain_cut is None:   # the learned arm alone was timed: the plain cut for the parity check
+            plain_cut = int(one_step(opts(False))[1])
         threads = os.cpu_count() or 1
         dt, ocut = cpu_port_run(g, spec, threads)
         cpu = {"value": m_und / dt, "unit": "edges/s", "cores": threads, "kind": "port",
-               "sample": "one full partition of the workload graph by the CPU port (all host threads)",
-               "edgecut": int(ocut), "parity_cut_equal": int(ocut) == int(cut)}
+               "sample": "one full partition of the workload graph by the CPU port of the plain path "
+                         "(all host threads)",
+               "edgecut": int(ocut), "parity_cut_equal": int(ocut) == plain_cut,
+               "parity_against": "the GPU plain refiner's cut (the learned refiner has no CPU counterpart)"}
 
     if rank == 0:
         line = {
@@ -504,15 +521,15 @@ def main():
             "warmup": args.warmup, "ms_per_step": job_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": config_of(args, spec, g, m_und),
+            "refiner": refiner,
             "e2e": {"value": e2e_value, "unit": "edges/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "ms_per_step": 1000 * sum(e2e_t) / len(e2e_t) if e2e_t else None},
+                    "ms_per_step": 1000 * sum(e2e_t) / len(e2e_t) if e2e_t else None, "refiner": refiner},
             "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "quality": {"edgecut": int(cut), "max_excess": int(last.max_excess), "balanced": last.max_excess <= 0,
                         "levels": last.nlevels, "coarsest_nvtxs": last.coarsest_nvtxs,
                         "phase_ms": {"coarsen": round(last.ms_coarsen, 3), "init": round(last.ms_init, 3),
                                      "uncoarsen": round(last.ms_uncoarsen, 3)}},
             "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
-            "refiner": "learned" if args.learned else "plain",
             "refine_passes": int(last.refine_passes),
             "graph_vs_eager": graph_vs_eager,
         }

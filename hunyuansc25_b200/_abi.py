@@ -16,6 +16,7 @@ HP_MAX_PARTS = 16384
 HP_OPTIONS_VERSION = 1
 HP_SCAN_NOALLOC_MAX_N = 1 << 26
 HP_MLP_NPARAM = 1377
+HP_PROF_NCLASS = 12
 
 HP_TRACE_XADJ = 0
 HP_TRACE_ADJNCY = 1
@@ -179,9 +180,9 @@ class HpStats(C.Structure):
         ("ms_uncoarsen", C.c_float),
         ("ms_h2d", C.c_float),
         ("ms_d2h", C.c_float),
-        ("prof_ms", C.c_float * 8),
-        ("prof_bytes", C.c_int64 * 8),
-        ("prof_launches", C.c_int32 * 8),
+        ("prof_ms", C.c_float * HP_PROF_NCLASS),
+        ("prof_bytes", C.c_int64 * HP_PROF_NCLASS),
+        ("prof_launches", C.c_int32 * HP_PROF_NCLASS),
     ]
 
     def as_dict(self):
@@ -198,7 +199,12 @@ HP_PROF_GAIN = 2
 HP_PROF_LP = 3
 HP_PROF_REBUILD = 4
 HP_PROF_INIT = 5
-PROF_NAMES = ["match", "contract", "gain_build", "lp", "rebuild", "init_trials", "match_more", "rebalance"]
+HP_PROF_MATCH_MORE = 6
+HP_PROF_REBALANCE = 7
+HP_PROF_APPLY = 8
+# class names by index; "" for the unused slots of the stats arrays
+PROF_NAMES = ["match", "contract", "gain_build", "lp", "rebuild", "init_trials", "match_more", "rebalance",
+              "apply", "", "", ""]
 
 
 I32P = C.POINTER(C.c_int32)

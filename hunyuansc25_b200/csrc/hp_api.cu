@@ -44,11 +44,33 @@ __global__ void validate_vertices_kernel(int32_t n, int64_t m, const int32_t *__
 
 constexpr int VE_THREADS = 256, VE_ITEMS = 16, VE_TILE = VE_THREADS * VE_ITEMS;
 
+// Antisymmetric fingerprint of a directed weighted entry (row v, neighbour u,
+// weight w): +h for v < u, -h for v > u, with h a hash of the undirected edge
+// (min, max, w).  Over a symmetric multiset of entries (every (v, u, w) with
+// its (u, v, w)) the terms cancel and the sum is 0 mod 2^64; a missing reverse
+// entry, or a weight that differs between the two directions, leaves a
+// non-zero sum except with probability about 2^-64.
+__device__ __forceinline__ unsigned long long sym_term(int32_t v, int32_t u, int32_t w)
+{
+    const uint32_t lo = (uint32_t)min(v, u), hi = (uint32_t)max(v, u);
+    const unsigned long long h =
+        hp::mix64((((uint64_t)lo << 32) | hi) + (uint64_t)(uint32_t)w * 0x9E3779B97F4A7C15ull);
+    return v < u ? h : 0ull - h;
+}
+
 // Runs after validate_vertices_kernel succeeded (xadj monotone, xadj[0] = 0,
-// xadj[n] = m, so every entry has exactly one owner row).
+// xadj[n] = m, so every entry has exactly one owner row).  Besides the range,
+// self-loop and weight checks of every entry it accumulates:
+//   sums[0]           the symmetry fingerprint (0 for a symmetric adjacency);
+//   sums[1]           unused (zero);
+//   sums[2]           the total edge weight (int64);
+//   sums[3]           the entries of the rows that are not strictly increasing
+//                     (unsorted[v] = 1 for those rows), the only rows that
+//                     can hold a duplicate neighbour.
 __global__ void __launch_bounds__(VE_THREADS)
 validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
-                      const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt, unsigned *status)
+                      const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt, unsigned *status,
+                      int32_t *__restrict__ unsorted, unsigned long long *sums)
 {
     __shared__ int32_t owner[VE_TILE];
     __shared__ int32_t s_warp[VE_THREADS / 32];
@@ -56,6 +78,8 @@ validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
     if (*status & HP_STATUS_BAD_GRAPH) return;   // uniform over the grid
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     bool bad = false;
+    unsigned long long fp = 0;
+    long long wsum = 0, uent = 0;
     for (int64_t tb = (int64_t)blockIdx.x * VE_TILE; tb < m; tb += (int64_t)gridDim.x * VE_TILE) {
         const int64_t te = tb + VE_TILE < m ? tb + VE_TILE : m;
         if (threadIdx.x == 0) {
@@ -106,12 +130,50 @@ validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
         for (int64_t j = tb + threadIdx.x; j < te; j += VE_THREADS) {
             const int32_t v = owner[j - tb];
             const int32_t u = adjncy[j];
+            const int32_t w = adjwgt ? adjwgt[j] : 1;
             if (u < 0 || u >= n || u == v) bad = true;
-            if (adjwgt && adjwgt[j] <= 0) bad = true;
+            if (w <= 0) bad = true;
+            wsum += w;
+            fp += sym_term(v, u, w);
+            // the next entry of the same row (within the tile, or across its end)
+            const int64_t jn = j + 1;
+            const bool same = jn < te ? owner[jn - tb] == v : (jn < m && xadj[v + 1] > jn);
+            if (same && adjncy[jn] <= u && atomicExch(&unsorted[v], 1) == 0) uent += xadj[v + 1] - xadj[v];
         }
         __syncthreads();   // owner[] is rebuilt for the next tile
     }
     if (bad) atomicOr(status, HP_STATUS_BAD_GRAPH);
+    hp::block_add_to<VE_THREADS>((long long)fp, &sums[0]);
+    hp::block_add_to<VE_THREADS>(wsum, &sums[2]);
+    hp::block_add_to<VE_THREADS>(uent, &sums[3]);
+}
+
+// Duplicate neighbours in the rows validate_edges_kernel found unsorted: every
+// (row, neighbour) key of those rows goes into an open-addressing hash table
+// (linear probing, 64-bit keys, at most half full, all ones = empty); a key
+// that is already present is a duplicate edge.  One warp per row.
+__global__ void __launch_bounds__(256)
+dup_check_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+                 const int32_t *__restrict__ unsorted, unsigned long long *table, uint64_t mask, unsigned *status)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    bool dup = false;
+    for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+        if (!unsorted[v]) continue;
+        const int32_t e = xadj[v + 1];
+        for (int32_t j = xadj[v] + lane; j < e; j += 32) {
+            const unsigned long long key = ((unsigned long long)(uint32_t)v << 32) | (uint32_t)adjncy[j];
+            uint64_t h = hp::mix64(key) & mask;
+            for (uint64_t probe = 0; probe <= mask; probe++) {
+                const unsigned long long prev = atomicCAS(&table[h], ~0ull, key);
+                if (prev == ~0ull) break;
+                if (prev == key) { dup = true; break; }
+                h = (h + 1) & mask;
+            }
+        }
+    }
+    if (dup) atomicOr(status, HP_STATUS_BAD_GRAPH);
 }
 
 __global__ void sum_kernel(int64_t n, const int32_t *__restrict__ a, unsigned long long *out)
@@ -204,21 +266,61 @@ int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, i
     hp_stats &st = c->stats;
     unsigned long long *sc = c->d_scal;
 
+    // scalar slots: [0] total vertex weight, [1] symmetry fingerprint, [2]
+    // unused, [3] total edge weight, [4] entries of unsorted rows
+    const size_t vmark = c->hi;
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 5, c->stream));
+    int32_t *unsorted = nullptr;
     if (c->opt.validate) {
+        unsorted = ralloc_t<int32_t>(c, n);
+        HP_CHECK_OOM(c);
+        HP_CUDA(cudaMemsetAsync(unsorted, 0, sizeof(int32_t) * (size_t)n, c->stream));
         HP_LAUNCH(c, validate_vertices_kernel, gsz(c, n), 256, 0, n, g0.m, g0.xadj, g0.vwgt, c->d_status);
         HP_LAUNCH(c, validate_edges_kernel,
                   (unsigned)std::max<int64_t>(1, std::min<int64_t>((g0.m + VE_TILE - 1) / VE_TILE,
                                                                    (int64_t)c->sm_count * 8)),
                   VE_THREADS, 0, n, g0.m, g0.xadj, g0.adjncy,
-                  g0.adjwgt, c->d_status);
+                  g0.adjwgt, c->d_status, unsorted, &sc[1]);
+    } else {
+        HP_LAUNCH(c, sum_kernel, gsz(c, g0.m), 256, 0, g0.m, g0.adjwgt, &sc[3]);
     }
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 2, c->stream));
     HP_LAUNCH(c, sum_kernel, gsz(c, n), 256, 0, (int64_t)n, g0.vwgt, &sc[0]);
-    long long tv = 0;
-    HP_TRY(hp_read_scalars(c, &sc[0], sizeof(long long), &tv));
+    long long vs[5] = {};
+    HP_TRY(hp_read_scalars(c, &sc[0], sizeof(vs), vs));
     HP_TRY(hp_check_status(c));
+    if (c->opt.validate) {
+        if (vs[1] != 0) {
+            fprintf(stderr, "hp: invalid graph: the adjacency is not symmetric (an entry (v, u, w) without its "
+                            "reverse (u, v, w))\n");
+            return HP_ERR_INVALID_GRAPH;
+        }
+        if (vs[4] > 0) {
+            // some rows are not strictly increasing: look for duplicate neighbours in them
+            uint64_t cap = 1024;
+            while (cap < 2 * (uint64_t)vs[4]) cap <<= 1;
+            unsigned long long *table = ralloc_t<unsigned long long>(c, (int64_t)cap);
+            HP_CHECK_OOM(c);
+            HP_CUDA(cudaMemsetAsync(table, 0xff, sizeof(unsigned long long) * cap, c->stream));
+            HP_LAUNCH(c, dup_check_kernel, gsz(c, (int64_t)n * 32), 256, 0, n, g0.xadj, g0.adjncy, unsorted, table,
+                      cap - 1, c->d_status);
+            if (hp_check_status(c) == HP_ERR_INVALID_GRAPH) {
+                fprintf(stderr, "hp: invalid graph: a row lists the same neighbour twice\n");
+                return HP_ERR_INVALID_GRAPH;
+            }
+        }
+    }
+    c->hi = vmark;
+    const long long tv = vs[0];
     if (tv >= INT32_MAX) return HP_ERR_UNSUPPORTED;
     st.tvwgt = tv;
+    // Coarse edge weights, gain-row connectivities and bisection gains are
+    // int32.  Each is a sum of level-0 edge weights, so when the total edge
+    // weight is below 2^31 none can wrap; otherwise every contraction checks
+    // that each matched pair's weighted degrees sum below 2^31 (a bound on
+    // every coarse edge weight and connectivity it creates) and the call fails
+    // with HP_ERR_UNSUPPORTED if one does not.
+    c->weight_check = vs[3] >= (long long)INT32_MAX;
+    if (c->weight_check) HP_TRY(hp_check_weight_range(c, g0));   // read with the first level's status check
 
     const int32_t thr = c->opt.coarsen_to > 0 ? c->opt.coarsen_to : default_coarsen_to(nparts);
     const int64_t maxvwgt = (3 * (int64_t)tv) / (2 * (int64_t)thr);
@@ -291,6 +393,8 @@ int begin_call(hp_context *c, const hp_options *opt, void *stream)
     memset(&c->stats, 0, sizeof(c->stats));
     unsigned zero = 0;
     HP_CUDA(cudaMemcpyAsync(c->d_status, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
+    if (c->opt.profile)
+        HP_CUDA(cudaMemsetAsync(c->d_profb, 0, sizeof(unsigned long long) * HP_PROF_NCLASS, c->stream));
     return HP_OK;
 }
 
@@ -352,10 +456,25 @@ void hp_prof_add_bytes(hp_context *c, int token, int64_t bytes)
     c->prof_recs[token].bytes += bytes;
 }
 
+unsigned long long *hp_prof_counter(hp_context *c, int cls)
+{
+    if (!c->opt.profile || c->prof_suspended || cls < 0 || cls >= HP_PROF_NCLASS) return nullptr;
+    return c->d_profb + cls;
+}
+
 void hp_prof_resolve(hp_context *c)
 {
+    if (c->opt.profile) {
+        // the stream is idle here (finish_stats synchronised it)
+        unsigned long long dev[HP_PROF_NCLASS] = {};
+        if (cudaMemcpy(dev, c->d_profb, sizeof(dev), cudaMemcpyDeviceToHost) == cudaSuccess) {
+            for (int i = 0; i < HP_PROF_NCLASS; i++) c->stats.prof_bytes[i] += (int64_t)dev[i];
+        } else {
+            cudaGetLastError();
+        }
+    }
     for (const auto &r : c->prof_recs) {
-        if (r.cls < 0 || r.cls >= 8 || r.ev1 < 0) continue;
+        if (r.cls < 0 || r.cls >= HP_PROF_NCLASS || r.ev1 < 0) continue;
         float ms = 0;
         if (cudaEventElapsedTime(&ms, c->prof_events[r.ev0], c->prof_events[r.ev1]) != cudaSuccess) {
             cudaGetLastError();
@@ -451,6 +570,11 @@ int hp_check_status(hp_context *c)
     if (s & HP_STATUS_SPIN_TIMEOUT) return HP_ERR_TIMEOUT;
     if (s & HP_STATUS_BAD_GRAPH) return HP_ERR_INVALID_GRAPH;
     if (s & HP_STATUS_OVERFLOW) return HP_ERR_INTERNAL;
+    if (s & HP_STATUS_WEIGHT_RANGE) {
+        fprintf(stderr, "hp: the edge weights of a matched pair sum to 2^31 or more: coarse edge weights "
+                        "would not fit int32\n");
+        return HP_ERR_UNSUPPORTED;
+    }
     return HP_OK;
 }
 
@@ -596,10 +720,11 @@ HP_API int hp_context_create(int device, hp_context **out)
     cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
     bool ok = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) == cudaSuccess;
     void *blk = nullptr;
-    ok = ok && cudaMalloc(&blk, 256 + sizeof(unsigned long long) * HP_NSCAL) == cudaSuccess;
+    ok = ok && cudaMalloc(&blk, 256 + sizeof(unsigned long long) * (HP_NSCAL + HP_PROF_NCLASS)) == cudaSuccess;
     if (ok) {
         c->d_status = (unsigned *)blk;
         c->d_scal = (unsigned long long *)((char *)blk + 256);
+        c->d_profb = c->d_scal + HP_NSCAL;
     }
     ok = ok && cudaMallocHost((void **)&c->h_pin, sizeof(long long) * HP_NSCAL) == cudaSuccess;
     for (int i = 0; ok && i < 8; i++) ok = cudaEventCreate(&c->ev[i]) == cudaSuccess;

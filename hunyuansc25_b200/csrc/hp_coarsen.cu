@@ -386,12 +386,17 @@ big_list_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t *list, int3
                 int32_t *huge, int32_t *d_huge, const int32_t *__restrict__ vwgt, int32_t *__restrict__ elig,
                 int32_t warp_deg, int32_t cta_deg)
 {
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    elig[v] = vwgt[v];   // every vertex starts unmatched
-    const int32_t d = xadj[v + 1] - xadj[v];
-    if (d > cta_deg) huge[atomicAdd(d_huge, 1)] = v;
-    else if (d > warp_deg) list[atomicAdd(d_count, 1)] = v;
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t d = 0;
+    if (v < n) {
+        elig[v] = vwgt[v];   // every vertex starts unmatched
+        d = xadj[v + 1] - xadj[v];
+    }
+    const bool is_huge = v < n && d > cta_deg, is_big = v < n && !is_huge && d > warp_deg;
+    const int32_t ph = hp::warp_append(d_huge, is_huge);
+    const int32_t pb = hp::warp_append(d_count, is_big);
+    if (is_huge) huge[ph] = v;
+    if (is_big) list[pb] = v;
 }
 
 // CTA per vertex for rows longer than match_cta_deg (R-MAT hubs).
@@ -548,31 +553,74 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
                     int32_t *__restrict__ maxlen, unsigned long long *__restrict__ long_total,
                     int32_t *__restrict__ small_max, int32_t thread_row, int32_t warp_row, int32_t cta_row)
 {
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    int32_t u = match[v];
-    if (v > u) { cmap[v] = cmap[u]; return; }
-    int32_t c = cmap[v];
-    const int32_t s0 = xadj[v], l0 = xadj[v + 1] - s0;
-    int32_t s1 = 0, l1 = 0;
-    int32_t w = vwgt[v];
-    if (u != v) {
-        s1 = xadj[u];
-        l1 = xadj[u + 1] - s1;
-        w += vwgt[u];
+    // no early exit: the list appends and maxima are aggregated per warp
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    bool lead = false;
+    int32_t c = 0, len = 0;
+    if (v < n) {
+        const int32_t u = match[v];
+        if (v > u) {
+            cmap[v] = cmap[u];
+        } else {
+            lead = true;
+            c = cmap[v];
+            const int32_t s0 = xadj[v], l0 = xadj[v + 1] - s0;
+            int32_t s1 = 0, l1 = 0;
+            int32_t w = vwgt[v];
+            if (u != v) {
+                s1 = xadj[u];
+                l1 = xadj[u + 1] - s1;
+                w += vwgt[u];
+            }
+            rinfo[c] = make_int4(s0, l0, s1, l1);
+            cvwgt[c] = w;
+            len = l0 + l1;
+            ltlen[c] = len > thread_row ? len : 0;
+        }
     }
-    rinfo[c] = make_int4(s0, l0, s1, l1);
-    cvwgt[c] = w;
-    const int32_t len = l0 + l1;
-    ltlen[c] = len > thread_row ? len : 0;
-    if (len <= thread_row && len > 8) atomicMax(small_max, len);   // picks the assembly kernel's network
-    if (len > thread_row) {
-        int cls = len <= warp_row ? 0 : (len <= cta_row ? 1 : 2);   // warp radix, CTA radix, long
-        int32_t pos = atomicAdd(&counts[cls], 1);
-        lists[(int64_t)cls * cn + pos] = c;
-        if (cls == 2) atomicMax(maxlen, len);
-        atomicAdd(long_total, (unsigned long long)len);
+    const bool is_long = lead && len > thread_row;
+    const int cls = !is_long ? -1 : (len <= warp_row ? 0 : (len <= cta_row ? 1 : 2));   // warp radix, CTA radix, long
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        const int32_t pos = hp::warp_append(&counts[q], cls == q);
+        if (cls == q) lists[(int64_t)q * cn + pos] = c;
     }
+    // the longest short row above 8 entries picks the assembly kernel's network
+    const int32_t sm = hp::warp_max(lead && !is_long && len > 8 ? len : 0);
+    const int32_t lm = hp::warp_max(cls == 2 ? len : 0);
+    const long long tot = hp::warp_sum64(is_long ? len : 0);
+    if ((threadIdx.x & 31) == 0) {
+        if (sm > 0) atomicMax(small_max, sm);
+        if (lm > 0) atomicMax(maxlen, lm);
+        if (tot > 0) atomicAdd(long_total, (unsigned long long)tot);
+    }
+}
+
+// Weight range of a contraction (run when the level-0 total edge weight is
+// 2^31 or more): every coarse edge weight and every connectivity of a coarse
+// vertex is at most the sum of its pair's fine weighted degrees, so a pair
+// whose sum reaches 2^31 sets HP_STATUS_WEIGHT_RANGE (the int32 coarse weights
+// could wrap; the call then fails) and no other pair can wrap.  One warp per
+// vertex; leaders sum both rows in int64.  match = nullptr checks every
+// vertex's own weighted degree (the input level).
+__global__ void __launch_bounds__(256)
+pair_weight_bound_kernel(int32_t n, const int32_t *__restrict__ match, const int32_t *__restrict__ xadj,
+                         const int32_t *__restrict__ adjwgt, unsigned *status)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    bool over = false;
+    for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+        const int32_t u = match ? match[v] : (int32_t)v;   // no match: every vertex alone
+        if (u < v) continue;   // a follower: its leader sums the pair
+        long long s = 0;
+        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32) s += adjwgt[j];
+        if (u != v)
+            for (int32_t j = xadj[u] + lane; j < xadj[u + 1]; j += 32) s += adjwgt[j];
+        s = hp::warp_sum64(s);
+        over |= s >= (long long)INT32_MAX;
+    }
+    if (over && lane == 0) atomicOr(status, HP_STATUS_WEIGHT_RANGE);
 }
 
 // The fine rows merged into coarse row c: entry i is the i-th entry of the
@@ -1409,6 +1457,10 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
     // algorithmic bytes of one full handshake round: xadj, adjncy, adjwgt,
     // vwgt, match read and write (neighbour gathers not counted)
     const int64_t round_bytes = 4 * ((int64_t)n + 1) + 8 * g.m + 12 * (int64_t)n;
+    // a later round (a vertex whose previous proposal is still unmatched keeps
+    // it without a rescan): xadj, match, eligibility, previous proposal in,
+    // proposal out; the rows rescanned are not counted (a lower bound)
+    const int64_t later_round_bytes = 4 * ((int64_t)n + 1) + 16 * (int64_t)n;
     if (n <= tn.small_match_n && g.m <= 64 * (int64_t)n) {
         // a small level: the whole matching in one CTA, one read back (cn)
         int32_t *sb = ralloc_t<int32_t>(c, 4 * ((int64_t)n + 1));
@@ -1458,7 +1510,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
         HP_LAUNCH(c, pref_huge_topk_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, elig, pref, cand, lkey, maxvwgt, prev);
         HP_LAUNCH(c, commit_kernel, blocks_for(n), 256, 0, n, g.match, pref, elig, &sc[2 + r], prev);
-        hp_prof_end(c, tok, r == 0 ? HP_PROF_MATCH : HP_PROF_MATCH_MORE, r == 0 ? round_bytes : 0);
+        hp_prof_end(c, tok, r == 0 ? HP_PROF_MATCH : HP_PROF_MATCH_MORE, r == 0 ? round_bytes : later_round_bytes);
     }
 
     auto matched = [&](int slot, int64_t *out) -> int {
@@ -1544,6 +1596,9 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     unsigned long long *long_total = &sc[2];  // entries of the long rows
     int32_t *small_max = (int32_t *)&sc[3];   // longest short row above 8 entries (0: none)
 
+    if (c->weight_check)
+        HP_LAUNCH(c, pair_weight_bound_kernel, std::min<unsigned>(blocks_for((int64_t)n * 32), c->sm_count * 16),
+                  256, 0, n, g.match, g.xadj, g.adjwgt, c->d_status);
     int tok = hp_prof_begin(c);
     HP_LAUNCH(c, coarse_setup_kernel, blocks_for(n), 256, 0, n, g.match, g.cmap, g.xadj, g.vwgt, rinfo, cg.vwgt,
               toff, lists, counts, cn, maxlen, long_total, small_max, c->tune.contract_thread_row,
@@ -1667,6 +1722,13 @@ int hp_coarsen_init()
     HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_radix_smem<XROW_THREADS, XROW_MAX>()));
+    return HP_OK;
+}
+
+int hp_check_weight_range(hp_context *c, const HpLevel &g)
+{
+    HP_LAUNCH(c, pair_weight_bound_kernel, std::min<unsigned>(blocks_for((int64_t)g.n * 32), c->sm_count * 16), 256,
+              0, g.n, (const int32_t *)nullptr, g.xadj, g.adjwgt, c->d_status);
     return HP_OK;
 }
 

@@ -15,6 +15,7 @@
 #define HP_STATUS_SPIN_TIMEOUT 1u   // a bounded look-back / flag wait gave up
 #define HP_STATUS_BAD_GRAPH    2u   // structural validation failed
 #define HP_STATUS_OVERFLOW     4u   // a capacity bound was exceeded (never expected)
+#define HP_STATUS_WEIGHT_RANGE 8u   // a matched pair's weighted degrees reach 2^31 (int32 coarse weights)
 
 // Spin limit of every device-side wait (iterations with __nanosleep back-off).
 #define HP_SPIN_LIMIT (1u << 22)
@@ -79,6 +80,28 @@ __device__ __forceinline__ long long warp_max64(long long v)
         v = t > v ? t : v;
     }
     return v;
+}
+
+__device__ __forceinline__ int warp_max(int v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(HP_FULL_MASK, v, o));
+    return v;
+}
+
+// Warp-aggregated append: every lane with pred set gets its own slot of the
+// list counted by *counter, with one atomic per warp instead of one per lane
+// (same-address atomics serialise in L2).  Lanes without pred get -1.  All 32
+// lanes must call it.
+__device__ __forceinline__ int32_t warp_append(int32_t *counter, bool pred)
+{
+    const unsigned m = __ballot_sync(HP_FULL_MASK, pred);
+    if (m == 0u) return -1;
+    const int leader = __ffs(m) - 1;
+    int32_t base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(counter, __popc(m));
+    base = __shfl_sync(HP_FULL_MASK, base, leader);
+    return pred ? base + __popc(m & lanemask_lt()) : -1;
 }
 
 // Inclusive warp scan.

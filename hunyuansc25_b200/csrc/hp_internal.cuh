@@ -56,6 +56,10 @@ struct hp_context {
     std::vector<ProfRec> prof_recs;
     int prof_next = 0;
     bool prof_suspended = false;   // set while launches are captured into a CUDA graph
+    // Device-side byte counts of the data-dependent terms of the class byte
+    // models (HP_PROF_NCLASS slots after the scalar slots), added by the
+    // profile-only counting kernels and folded into stats.prof_bytes.
+    unsigned long long *d_profb = nullptr;
 
     hp_stats stats = {};
 
@@ -86,6 +90,7 @@ struct hp_context {
     std::vector<hp_context *> workers;   // batch worker contexts (own streams and arenas)
     std::vector<HpLevel> levels;
     bool trace_valid = false;
+    bool weight_check = false;           // total edge weight >= 2^31: contractions check pair bounds
     hp_options opt = {};
 };
 
@@ -147,6 +152,11 @@ int hp_prof_begin(hp_context *c);
 void hp_prof_end(hp_context *c, int token, int cls, int64_t bytes);
 // Algorithmic bytes of an interval that are known only after it was closed.
 void hp_prof_add_bytes(hp_context *c, int token, int64_t bytes);
+// The device byte counter of class cls while the profiler records launches
+// (opt.profile and not capturing), else nullptr: callers launch their counting
+// kernels only when it is set, after the class's hp_prof_end, so that the
+// counting is not part of the class's time.
+unsigned long long *hp_prof_counter(hp_context *c, int cls);
 void hp_prof_resolve(hp_context *c);
 
 // Hands graphs whose last launch is enqueued on c->stream to the reaper thread
@@ -182,6 +192,9 @@ int hp_edgecut_launch(hp_context *c, int32_t n, const int32_t *xadj, const int32
 // ---- coarsening (hp_coarsen.cu) -----------------------------------------------
 // Builds levels[1..] from levels[0]; returns HP_OK and fills c->levels.
 int hp_coarsen(hp_context *c, int32_t coarsen_to, int64_t maxvwgt);
+// Sets HP_STATUS_WEIGHT_RANGE when a vertex of g has a weighted degree of 2^31
+// or more (the input level's check when its total edge weight reaches 2^31).
+int hp_check_weight_range(hp_context *c, const HpLevel &g);
 
 // ---- initial partition (hp_initpart.cu) ------------------------------------------
 int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_t *h_tw,

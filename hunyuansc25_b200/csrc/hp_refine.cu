@@ -47,18 +47,23 @@ __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int
                                 int32_t *__restrict__ cap, int32_t *big, int32_t *huge, int32_t *d_bigcnt,
                                 int32_t bigd, int32_t huged)
 {
-    int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= n) return;
-    int32_t d = xadj[v + 1] - xadj[v];
-    cap[v] = d < k ? d : k;
-    if (d > bigd) {
-        big[atomicAdd(d_bigcnt, 1)] = v;
-        if (d > huged) {
-            atomicMax(d_bigcnt + 2, d);
-            huge[atomicAdd(d_bigcnt + 3, 1)] = v;
-        }
-    } else if (d > 8) {
-        atomicMax(d_bigcnt + 1, d);
+    // no early exit: the list appends and maxima are aggregated per warp
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    int32_t d = 0;
+    if (v < n) {
+        d = xadj[v + 1] - xadj[v];
+        cap[v] = d < k ? d : k;
+    }
+    const bool is_big = v < n && d > bigd, is_huge = is_big && d > huged;
+    const int32_t pb = hp::warp_append(d_bigcnt, is_big);
+    const int32_t ph = hp::warp_append(d_bigcnt + 3, is_huge);
+    if (is_big) big[pb] = v;
+    if (is_huge) huge[ph] = v;
+    const int32_t hm = hp::warp_max(is_huge ? d : 0);
+    const int32_t sm = hp::warp_max(v < n && !is_big && d > 8 ? d : 0);
+    if ((threadIdx.x & 31) == 0) {
+        if (hm > 0) atomicMax(d_bigcnt + 2, hm);
+        if (sm > 0) atomicMax(d_bigcnt + 1, sm);
     }
 }
 
@@ -1552,7 +1557,6 @@ struct RefineBufs {
     int8_t *ufl;   // per part: pw < maxp (a weak pass's destination rule), set by ctl_begin
     unsigned long long *pw;
     const int64_t *opt, *maxp;
-    int32_t G;          // gain-row entries of the level
     int32_t small_max;  // longest row of at most bigd entries (picks the gain kernel's network)
     bool huge_rows;     // the level has rows longer than huged
 };
@@ -1856,6 +1860,99 @@ __global__ void restore_best_kernel(const RefineCtl *s, int32_t n, const int32_t
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) where[i] = best_where[i];
 }
 
+// ---- profile-only byte counts -------------------------------------------------------
+// The data-dependent terms of the refinement classes' algorithmic byte models
+// (rows walked, candidates, moves, dirty rows), counted on the device in
+// profiled eager passes into the class counters (hp_prof_counter) after the
+// class's launches, so that the counting is not timed with them.  Neighbour
+// gathers are not counted (compulsory-traffic model, as for every class).
+
+// Bytes a gain-row walk reads: a dense row (k entries, longer than 32 and so
+// walked by a warp with the part ids implied) reads k connectivities; any
+// other row its (part, conn) pairs up to and including the first padding slot.
+__device__ __forceinline__ long long row_walk_bytes(const int32_t *__restrict__ gpart, int32_t o, int32_t len,
+                                                    int32_t k)
+{
+    if (len > 32 && len == k) return 4ll * k;
+    int32_t f = 0;
+    while (f < len && gpart[o + f] >= 0) f++;
+    return 8ll * (f < len ? f + 1 : f);
+}
+
+// LP: every row's walk by the selection, and each candidate's adjacency row
+// (adjncy + adjwgt) and destination read by the afterburner.
+__global__ void __launch_bounds__(256)
+lp_bytes_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
+                const int32_t *__restrict__ xadj, const int32_t *__restrict__ pregain, int32_t k,
+                unsigned long long *acc)
+{
+    long long b = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        b += row_walk_bytes(gpart, goff[v], goff[v + 1] - goff[v], k);
+        if (pregain[v] != NEG) b += 8ll * (xadj[v + 1] - xadj[v]) + 4;
+    }
+    hp::block_add_to<256>(b, acc);
+}
+
+// Rebuild of the dirty rows: xadj, goff and the list entry, the adjacency row,
+// the rewritten gain row (8 bytes per slot) and the dirty flag's reset.
+__global__ void __launch_bounds__(256)
+rebuild_bytes_kernel(const int32_t *__restrict__ small_l, const int32_t *__restrict__ d_nsmall,
+                     const int32_t *__restrict__ big_l, const int32_t *__restrict__ d_nbig,
+                     const int32_t *__restrict__ xadj, const int32_t *__restrict__ goff, unsigned long long *acc)
+{
+    const int32_t ns = *d_nsmall, nb = *d_nbig;
+    long long b = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)ns + nb;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = i < ns ? small_l[i] : big_l[i - ns];
+        b += 24 + 8ll * (xadj[v + 1] - xadj[v]) + 8ll * (goff[v + 1] - goff[v]);
+    }
+    hp::block_add_to<256>(b, acc);
+}
+
+// Rebalance proposals (counted before the moves apply, with the part weights
+// the proposal saw): where and dest of every vertex; vertex weight, goff and
+// the gain-row walk of every vertex of an overweight part; per candidate its
+// key/value write, 20 bytes per radix pass (digit histogram read, pair
+// scatter) and the rank/select (or evict) reads of the sorted pairs.
+__global__ void __launch_bounds__(256)
+rebalance_bytes_kernel(int32_t n, const int32_t *__restrict__ where, const unsigned long long *__restrict__ pw,
+                       const int64_t *__restrict__ maxp, const int32_t *__restrict__ goff,
+                       const int32_t *__restrict__ gpart, int32_t k, const int32_t *__restrict__ d_cnt,
+                       int32_t radix_passes, unsigned long long *acc)
+{
+    long long b = 0;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t p = where[v];
+        b += 8;
+        if ((int64_t)pw[p] > maxp[p]) b += 12 + row_walk_bytes(gpart, goff[v], goff[v + 1] - goff[v], k);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) b += (long long)(*d_cnt) * (32 + 20ll * radix_passes);
+    hp::block_add_to<256>(b, acc);
+}
+
+// Move application: per move its list entries (vertex, old part), destination,
+// vertex weight, xadj, adjacency row and where write, then the exact cut
+// change's goff read and walk of the mover's gain row; once per pass the
+// control step's part weights and bounds, and the best-partition copy when
+// the pass was the best so far.
+__global__ void __launch_bounds__(256)
+apply_bytes_kernel(const int32_t *__restrict__ moves, const unsigned long long *__restrict__ d_nmoves,
+                   const int32_t *__restrict__ xadj, const int32_t *__restrict__ goff,
+                   const int32_t *__restrict__ gpart, int32_t k, int32_t n, const RefineCtl *ctl,
+                   unsigned long long *acc)
+{
+    const int64_t nm = (int64_t)*d_nmoves;
+    long long b = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = moves[i];
+        b += 36 + 8ll * (xadj[v + 1] - xadj[v]) + row_walk_bytes(gpart, goff[v], goff[v + 1] - goff[v], k);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) b += 16ll * k + (ctl->take ? 8ll * n + 16ll * k : 0);
+    hp::block_add_to<256>(b, acc);
+}
+
 struct PassCfg {
     int32_t k;
     bool finest, any_big, recording, huge_rows;   // huge_rows: rows longer than chunk_deg exist
@@ -1905,14 +2002,21 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
         }
         if (P.recording)
             HP_LAUNCH(c, log_accept_kernel, nblk(n), 256, 0, n, B.recof, B.lock, &sc[S_NCAND], c->log_acc);
-        // select: goff, rows, where, lock in; dest, pregain out.  afterburner:
-        // xadj, adjncy, adjwgt, own pregain/dest/where in, lock out
-        hp_prof_end(c, ltok, HP_PROF_LP, 8 * ((int64_t)n + 1) + 8 * (int64_t)(B.G) + 8 * g.m + 26 * (int64_t)n);
+        // fixed terms -- selection: goff, where, lock in, dest and pregain out;
+        // afterburner: xadj, pregain in, lock out.  The rows walked and the
+        // candidates' adjacency rows are counted on the device.
+        hp_prof_end(c, ltok, HP_PROF_LP, 8 * ((int64_t)n + 1) + 18 * (int64_t)n);
+        if (unsigned long long *cnt = hp_prof_counter(c, HP_PROF_LP))
+            HP_LAUNCH(c, lp_bytes_kernel, std::min(nblk(n), pg), 256, 0, n, B.goff, B.gpart, g.xadj, B.pregain, k,
+                      cnt);
     } else {
         const int btok = hp_prof_begin(c);
         if (mode == 1) HP_TRY(weak_rebalance(c, g, B, k));
         else HP_TRY(strong_rebalance(c, g, B, k));
         hp_prof_end(c, btok, HP_PROF_REBALANCE, 0);
+        if (unsigned long long *cnt = hp_prof_counter(c, HP_PROF_REBALANCE))
+            HP_LAUNCH(c, rebalance_bytes_kernel, std::min(nblk(n), pg), 256, 0, n, g.where, B.pw, B.maxp, B.goff,
+                      B.gpart, k, (const int32_t *)&sc[S_LISTCNT], key_bits_for(k) / 8, cnt);
     }
     return HP_OK;
 }
@@ -1927,6 +2031,7 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
     const unsigned pg = (unsigned)(c->sm_count * c->tune.grid_ctas_per_sm);
     const unsigned mg = std::min(nblk(n), pg);   // grid-stride over the device move count
     // (the proposal kernels appended the moves with their old parts and c1)
+    int atok = hp_prof_begin(c);
     HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw, g.xadj,
               g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k,
               B.huge_mv, (int32_t *)&sc[S_HUGEMV], c->tune.gain_thread_deg, c->tune.chunk_deg);
@@ -1938,15 +2043,24 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
                   B.plan_off, B.plan_cnt, B.oldp, B.dest, g.xadj, g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty,
                   B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k, c->tune.gain_thread_deg);
     }
+    hp_prof_end(c, atok, HP_PROF_APPLY, 0);
     const int rtok = hp_prof_begin(c);
     HP_TRY(build_rows(c, g, B, k, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
                       ((const int32_t *)&sc[S_DIRTY]) + 1, P.any_big, B.dirty));
     hp_prof_end(c, rtok, HP_PROF_REBUILD, 0);
+    if (unsigned long long *cnt = hp_prof_counter(c, HP_PROF_REBUILD))
+        HP_LAUNCH(c, rebuild_bytes_kernel, pg, 256, 0, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
+                  ((const int32_t *)&sc[S_DIRTY]) + 1, g.xadj, B.goff, cnt);
+    atok = hp_prof_begin(c);
     HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
               B.oldp, 0, &sc[S_C2], k);
     HP_LAUNCH(c, ctl_end_kernel, 1, 1024, 0, P.ctl, sc, hloop, graph, k, B.pw, B.maxp);
     HP_LAUNCH(c, save_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, P.ctl, n,
               g.where, B.best_where, k, B.pw, P.best_pw);
+    hp_prof_end(c, atok, HP_PROF_APPLY, 0);
+    if (unsigned long long *cnt = hp_prof_counter(c, HP_PROF_APPLY))
+        HP_LAUNCH(c, apply_bytes_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], g.xadj, B.goff, B.gpart, k, n, P.ctl,
+                  cnt);
     return HP_OK;
 }
 
@@ -2537,14 +2651,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         HP_CUDA(cudaMemsetAsync(B.ab_acc, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
     // the gain rows take G = sum min(deg, k) <= m entries: allocated for m, so
-    // that no count is read back (the profiler reads G for its byte count)
-    // (the eager loop, which reads back every pass anyway, reads G for the LP
-    // class's byte count; the graphed levels complete their gain-build bytes
-    // from the control block at the end of uncoarsening)
-    const bool eager_loop = !graph_loop(c);
-    int32_t G = (int32_t)std::max<int64_t>(g.m, 1);
-    if (c->opt.profile && eager_loop) HP_TRY(hp_read_scalars(c, B.goff + n, sizeof(int32_t), &G));
-    B.G = G;
+    // that no count is read back (the gain-build class completes its byte
+    // count with G from the control block at the end of uncoarsening)
     B.small_max = ls.small_max;
     B.huge_rows = ls.maxdeg > huged;
     B.gpart = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));

@@ -9,7 +9,6 @@
 // (HP_SPIN_LIMIT); on expiry the CTA sets HP_STATUS_SPIN_TIMEOUT and continues,
 // so a stalled predecessor can never hang the device.
 #include <cstring>
-#include <mutex>
 
 #include "hp_internal.cuh"
 
@@ -163,11 +162,6 @@ int hp_scan_excl(hp_context *c, const int32_t *in, int32_t *out, int64_t n)
 #define HP_NOALLOC_TILES ((HP_SCAN_NOALLOC_MAX_N + 1 + SCAN_TILE - 1) / SCAN_TILE)
 static __device__ __align__(256) unsigned long long g_scan_noalloc_scratch[HP_NOALLOC_TILES + 3];
 
-namespace {
-std::mutex g_noalloc_mu;
-unsigned long long *g_noalloc_ptr[64] = {};   // device address per CUDA ordinal
-}
-
 extern "C" __attribute__((visibility("default")))
 int hp_scan_exclusive_i32_noalloc(const int32_t *d_in, int32_t *d_out, int64_t n, void *stream)
 {
@@ -178,25 +172,33 @@ int hp_scan_exclusive_i32_noalloc(const int32_t *d_in, int32_t *d_out, int64_t n
                 (long long)n, (long long)HP_SCAN_NOALLOC_MAX_N);
         return HP_ERR_UNSUPPORTED;
     }
-    int dev = 0;
-    HP_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return HP_ERR_UNSUPPORTED;
+    // An error left pending by the caller's earlier work would otherwise be
+    // reported as this call's launch failure after the scan was enqueued:
+    // refuse up front and leave the error for its owner to read.
+    cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        fprintf(stderr, "hp_scan_exclusive_i32_noalloc: a CUDA error from earlier work is pending (%s); "
+                        "nothing was launched\n", cudaGetErrorString(pending));
+        return HP_ERR_CUDA;
+    }
+    // The host-side name of a __device__ array is not a device address: look
+    // the address up with the caller's device and context current.  This is
+    // done on every call, not cached per device number, so that a
+    // cudaDeviceReset or a different (non-primary) context on the same device
+    // cannot leave a stale address behind.  Once the library's device code is
+    // loaded in the context the lookup allocates nothing; the first call in a
+    // context loads it, which is why that first call belongs before any
+    // stream capture.
     unsigned long long *scratch = nullptr;
     {
-        // set-up, once per device, with that device current: the host-side
-        // name of a __device__ array is not a device address, so look it up
-        std::lock_guard<std::mutex> lk(g_noalloc_mu);
-        if (!g_noalloc_ptr[dev]) {
-            void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_scan_noalloc_scratch);
-            if (e != cudaSuccess || !p) {
-                fprintf(stderr, "hp_scan_exclusive_i32_noalloc: cudaGetSymbolAddress failed: %s\n",
-                        cudaGetErrorString(e));
-                return HP_ERR_CUDA;
-            }
-            g_noalloc_ptr[dev] = (unsigned long long *)p;
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_scan_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            fprintf(stderr, "hp_scan_exclusive_i32_noalloc: cudaGetSymbolAddress failed: %s\n",
+                    cudaGetErrorString(e));
+            return HP_ERR_CUDA;
         }
-        scratch = g_noalloc_ptr[dev];
+        scratch = (unsigned long long *)p;
     }
     cudaStream_t s = (cudaStream_t)stream;
     const int64_t ntiles = (n + 1 + SCAN_TILE - 1) / SCAN_TILE;

@@ -79,7 +79,9 @@ typedef struct hp_options {
 #define HP_PROF_INIT      5   /* bisection trials                              */
 #define HP_PROF_MATCH_MORE 6  /* handshake rounds after the first + fallbacks  */
 #define HP_PROF_REBALANCE 7   /* weak/strong rebalance proposals (eager passes) */
-#define HP_PROF_NCLASS    8
+#define HP_PROF_APPLY     8   /* move application, exact cut change, pass control
+                                 and best-partition copy (eager passes)         */
+#define HP_PROF_NCLASS   12   /* array size; classes 9-11 are unused (zero)    */
 
 /* Timing and quality of the last call on a context. */
 typedef struct hp_stats {
@@ -97,9 +99,12 @@ typedef struct hp_stats {
     float   ms_uncoarsen;
     float   ms_h2d;            /* host<->device copies inside hp_partition() (0 for _device) */
     float   ms_d2h;
-    float   prof_ms[8];        /* device time per kernel class (HP_PROF_*)                    */
-    int64_t prof_bytes[8];     /* algorithmic HBM bytes per kernel class                      */
-    int32_t prof_launches[8];  /* kernel launches per class                                   */
+    float   prof_ms[HP_PROF_NCLASS];       /* device time per kernel class (HP_PROF_*)        */
+    int64_t prof_bytes[HP_PROF_NCLASS];    /* algorithmic HBM bytes per kernel class: fixed
+                                              per-launch terms plus the data-dependent terms
+                                              (rows walked, candidates, moves, dirty rows)
+                                              counted on the device in profiled calls     */
+    int32_t prof_launches[HP_PROF_NCLASS]; /* kernel launches per class                       */
 } hp_stats;
 
 typedef struct hp_context hp_context;
@@ -269,8 +274,13 @@ int hp_scan_exclusive_i32(hp_context *ctx, const int32_t *d_in, int32_t *d_out,
  * library until the process exits), so n is limited to
  * HP_SCAN_NOALLOC_MAX_N; larger n returns HP_ERR_UNSUPPORTED with a message
  * on stderr.  The caller still passes d_in and d_out (n + 1 entries).
- *   - The first call on a device looks up the array's device address with that
- *     device current; make that first call before any stream capture.
+ *   - Every call looks up the array's device address with the caller's device
+ *     and context current (so a cudaDeviceReset or a non-primary context is
+ *     handled); the lookup allocates nothing once the library's device code is
+ *     loaded, which the first call in a context does: make that first call
+ *     before any stream capture.
+ *   - A CUDA error already pending from the caller's earlier work is not
+ *     cleared: the call returns HP_ERR_CUDA without launching anything.
  *   - Runs on the calling thread's current device and `stream`, and returns
  *     after the scan completed (it reads the status word back).
  *   - All calls share the one array: calls that overlap on the GPU (other

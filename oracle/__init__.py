@@ -51,6 +51,8 @@ def lib():
         L.ora_partition.argtypes = [C.c_int32, I32P, I32P, I32P, I32P, C.c_int32, C.POINTER(C.c_float),
                                     C.c_float, C.POINTER(HpOptions), I32P, I64P, C.POINTER(C.c_void_p)]
         L.ora_partition.restype = C.c_int
+        L.ora_weight_range_ok.argtypes = [C.c_int32, I32P, I32P, I32P]
+        L.ora_weight_range_ok.restype = C.c_int
         L.ora_trace_nlevels.argtypes = [C.c_void_p]
         L.ora_trace_level.argtypes = [C.c_void_p, C.c_int, I32P, I64P, I64P, I64P]
         L.ora_trace_copy.argtypes = [C.c_void_p, C.c_int, C.c_int, I32P, C.c_int64]
@@ -136,6 +138,14 @@ class Trace:
         return out[:size]
 
 
+class OracleError(RuntimeError):
+    """A non-zero return of ora_partition; .code is the HP_ERR_* value."""
+
+    def __init__(self, code: int):
+        self.code = code
+        super().__init__(f"ora_partition failed: {code}")
+
+
 def partition(g, nparts, ubfactor=1.03, tpwgts=None, opt: HpOptions | None = None, trace=False):
     """Full oracle V-cycle. Returns (part, cut, Trace|None)."""
     if opt is None:
@@ -151,8 +161,15 @@ def partition(g, nparts, ubfactor=1.03, tpwgts=None, opt: HpOptions | None = Non
                              C.c_float(ubfactor), C.byref(opt), _p(part), C.byref(cut),
                              C.byref(th) if trace else None)
     if rc != 0:
-        raise RuntimeError(f"ora_partition failed: {rc}")
+        raise OracleError(rc)
     return part[:g.nvtxs], cut.value, (Trace(th.value) if trace else None)
+
+
+def weight_range_ok(g, match_=None) -> bool:
+    """The weight-range rule: every matched pair's (match_ None: every
+    vertex's) weighted degrees sum below 2^31."""
+    return bool(lib().ora_weight_range_ok(g.nvtxs, _p(i32(g.xadj)), _p(i32(g.adjwgt)),
+                                          None if match_ is None else _p(i32(match_))))
 
 
 def match(g, level, seed, maxvwgt, rounds):

@@ -229,7 +229,9 @@ int32_t ora_match(int32_t n, const int32_t *xadj, const int32_t *adjncy,
 /* ------------------------------------------------------------------------- */
 /* Contraction.                                                               */
 
-typedef struct { int32_t k, w; } kw_t;
+/* Coarse weights accumulate in int64 (they are stored as int32 once merged;
+ * ora_weight_range_ok below guarantees that every merged weight fits). */
+typedef struct { int32_t k; int64_t w; } kw_t;
 
 static int cmp_kw(const void *a, const void *b)
 {
@@ -249,6 +251,28 @@ static void sort_kw(kw_t *r, int64_t len)
     } else {
         qsort(r, (size_t)len, sizeof(kw_t), cmp_kw);
     }
+}
+
+/* Weight range of a contraction (the library's pair_weight_bound_kernel,
+ * checked when the input's total edge weight reaches 2^31): every coarse edge
+ * weight and connectivity is at most the sum of its pair's fine weighted
+ * degrees, so the contraction is accepted when every pair's sum stays below
+ * 2^31.  match = NULL checks every vertex alone (the input level).  Returns 1
+ * when the range holds. */
+int ora_weight_range_ok(int32_t n, const int32_t *xadj, const int32_t *adjwgt, const int32_t *match)
+{
+    int ok = 1;
+#pragma omp parallel for schedule(dynamic, 4096) reduction(&& : ok)
+    for (int32_t v = 0; v < n; v++) {
+        const int32_t u = match ? match[v] : v;
+        if (u < v) continue;
+        int64_t s = 0;
+        for (int32_t j = xadj[v]; j < xadj[v + 1]; j++) s += adjwgt[j];
+        if (u != v)
+            for (int32_t j = xadj[u]; j < xadj[u + 1]; j++) s += adjwgt[j];
+        ok = ok && s < (int64_t)INT32_MAX;
+    }
+    return ok;
 }
 
 int64_t ora_contract(int32_t n, const int32_t *xadj, const int32_t *adjncy,
@@ -306,7 +330,7 @@ int64_t ora_contract(int32_t n, const int32_t *xadj, const int32_t *adjncy,
         const kw_t *r = tmp + toff[c];
         for (int32_t j = 0; j < ucnt[c]; j++) {
             cadj[cxadj[c] + j] = r[j].k;
-            cwgt[cxadj[c] + j] = r[j].w;
+            cwgt[cxadj[c] + j] = (int32_t)r[j].w;
         }
     }
     free(leader); free(toff); free(tmp); free(ucnt);
@@ -1197,6 +1221,14 @@ int ora_partition(int32_t n, const int32_t *xadj, const int32_t *adjncy,
     for (int64_t j = 0; j < m0; j++) ew[j] = adjwgt_in ? adjwgt_in[j] : 1;
     int64_t tv = 0;
     for (int32_t v = 0; v < n; v++) tv += vw[v];
+    if (tv >= INT32_MAX) { free(vw); free(ew); return HP_ERR_UNSUPPORTED; }
+    int64_t tw = 0;
+    for (int64_t j = 0; j < m0; j++) tw += ew[j];
+    const int weight_check = tw >= (int64_t)INT32_MAX;
+    if (weight_check && !ora_weight_range_ok(n, xadj, ew, NULL)) {
+        free(vw); free(ew);
+        return HP_ERR_UNSUPPORTED;
+    }
 
     int cap = 16;
     olevel *lv = (olevel *)calloc((size_t)cap, sizeof(olevel));
@@ -1218,6 +1250,16 @@ int ora_partition(int32_t n, const int32_t *xadj, const int32_t *adjncy,
             lv = (olevel *)realloc(lv, sizeof(olevel) * (size_t)cap);
             memset(lv + L + 1, 0, sizeof(olevel) * (size_t)(cap - L - 1));
             f = &lv[L];
+        }
+        if (weight_check && !ora_weight_range_ok(f->n, f->xadj, f->adjwgt, f->match)) {
+            /* a coarse weight could exceed int32: the call fails as the library's does */
+            for (int32_t l = 0; l <= L; l++) {
+                olevel *g = &lv[l];
+                if (g->owns_graph) { free(g->xadj); free(g->adjncy); free(g->adjwgt); free(g->vwgt); }
+                free(g->match); free(g->cmap);
+            }
+            free(lv); free(vw); free(ew);
+            return HP_ERR_UNSUPPORTED;
         }
         olevel *c = &lv[L + 1];
         c->n = cn;

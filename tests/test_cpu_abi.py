@@ -101,7 +101,9 @@ def test_options_struct_layout():
     assert C.sizeof(_abi.HpOptions) == 56
     assert _abi.HpOptions.eager.offset == 44
     assert _abi.HpOptions.seed.offset == 48
-    assert C.sizeof(_abi.HpStats) == 8 * 3 + 4 * 2 + 8 + 4 * 2 + 4 * 6 + 4 * 8 + 8 * 8 + 4 * 8
+    # the per-class arrays hold HP_PROF_NCLASS (12) entries
+    assert _abi.HP_PROF_NCLASS == 12
+    assert C.sizeof(_abi.HpStats) == 8 * 3 + 4 * 2 + 8 + 4 * 2 + 4 * 6 + 4 * 12 + 8 * 12 + 4 * 12
 
 
 def test_options_default_matches_library(lib):

@@ -235,3 +235,25 @@ def test_oracle_edge_cases():
     part, cut, _ = oracle.partition(g, 40, 1.03)
     assert part.min() >= 0 and part.max() < 40
     assert cut == oracle.edgecut(g, part)
+
+
+def test_weight_range_rule():
+    """The weight-range rule shared with the library: when the total edge
+    weight reaches 2^31, a matched pair whose weighted degrees sum to 2^31 or
+    more fails the call (HP_ERR_UNSUPPORTED), since the int32 coarse weights
+    could wrap; below that the partition is the ordinary one."""
+    from hunyuansc25_b200._abi import HP_ERR_UNSUPPORTED
+    n = 4096
+    xadj = np.zeros(n + 1, np.int32)
+    xadj[1:] = np.cumsum([1 if v in (0, n - 1) else 2 for v in range(n)])
+    adj = np.array([u for v in range(n) for u in (v - 1, v + 1) if 0 <= u < n], np.int32)
+    path = G(xadj, adj, np.ones(n, np.int32), np.full(adj.size, 1 << 29, np.int32))
+    assert oracle.weight_range_ok(path)                            # every vertex alone: 2^30
+    match = np.arange(n, dtype=np.int32) ^ 1                       # pairs (0,1), (2,3), ...
+    assert not oracle.weight_range_ok(path, match)                 # a pair: 2^31
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.partition(path, 2, 1.03)
+    assert e.value.code == HP_ERR_UNSUPPORTED
+    light = G(xadj, adj, np.ones(n, np.int32), np.full(adj.size, 1 << 20, np.int32))
+    part, cut, _ = oracle.partition(light, 2, 1.03)
+    assert cut == oracle.edgecut(light, part)

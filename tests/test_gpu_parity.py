@@ -268,6 +268,87 @@ def test_invalid_inputs(ctx):
     assert cut == oracle.edgecut(g, part)
 
 
+def _csr(n, rows, weights=None):
+    xadj = np.zeros(n + 1, np.int32)
+    for v, r in enumerate(rows):
+        xadj[v + 1] = xadj[v] + len(r)
+    adj = np.array([u for r in rows for u in r], np.int32)
+    w = None if weights is None else np.array([x for r in weights for x in r], np.int32)
+    return xadj, adj, w
+
+
+def test_invalid_asymmetric_and_duplicate(ctx):
+    """Asymmetric adjacency (a missing reverse entry, or a weight that differs
+    between the two directions) and duplicate neighbours (in a sorted row and
+    in an unsorted one) are rejected with HP_ERR_INVALID_GRAPH; the reference's
+    own checker is check_graph (hunyuangraph_GPU_match.h:1718-1800)."""
+    # 0-1, 1-2, 2-3 path; vertex 3 lacks its entry for 2
+    xadj, adj, _ = _csr(4, [[1], [0, 2], [1, 3], []])
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition(xadj, adj, 2)
+    assert e.value.code == HP_ERR_INVALID_GRAPH
+    # symmetric structure, weight 5 one way and 6 the other
+    xadj, adj, w = _csr(3, [[1], [0, 2], [1]], [[4], [4, 5], [6]])
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition(xadj, adj, 2, adjwgt=w)
+    assert e.value.code == HP_ERR_INVALID_GRAPH
+    # duplicate neighbour in a sorted row (the pair 0-1 listed twice both ways)
+    xadj, adj, _ = _csr(3, [[1, 1, 2], [0, 0], [0]])
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition(xadj, adj, 2)
+    assert e.value.code == HP_ERR_INVALID_GRAPH
+    # the same in unsorted rows of a larger graph (the hash-table path)
+    g = graphs.rmat(12, 8, seed=5)
+    rows = [list(g.adjncy[g.xadj[v]:g.xadj[v + 1]][::-1]) for v in range(g.nvtxs)]
+    v = int(np.argmax(np.diff(g.xadj)))
+    u = rows[v][0]
+    rows[v].append(u)
+    rows[u].append(v)
+    xadj, adj, _ = _csr(g.nvtxs, rows)
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition(xadj, adj, 8)
+    assert e.value.code == HP_ERR_INVALID_GRAPH
+    # unsorted rows without duplicates are accepted and give the sorted graph's partition
+    rows = [list(g.adjncy[g.xadj[v]:g.xadj[v + 1]][::-1]) for v in range(g.nvtxs)]
+    xadj, adj, _ = _csr(g.nvtxs, rows)
+    p_unsorted, c_unsorted = ctx.partition(xadj, adj, 8)
+    assert c_unsorted == oracle.edgecut(graphs.Graph(xadj, adj, g.vwgt, np.ones_like(adj)), p_unsorted)
+    # the context stays usable
+    part, cut = ctx.partition_graph(graphs.grid2d(8, 8), 4)
+    assert cut == oracle.edgecut(graphs.grid2d(8, 8), part)
+
+
+def test_weight_range(ctx):
+    """Edge weights whose sums could wrap the int32 coarse weights: a matched
+    pair whose weighted degrees reach 2^31 fails with HP_ERR_UNSUPPORTED, as in
+    the oracle; a graph whose total weight exceeds 2^31 but whose pairs stay
+    below it partitions exactly as the oracle does."""
+    n = 4096
+    rows = [[v - 1] if v == n - 1 else ([v + 1] if v == 0 else [v - 1, v + 1]) for v in range(n)]
+    xadj, adj, _ = _csr(n, rows)
+    path = graphs.Graph(xadj, adj, np.ones(n, np.int32), np.full(adj.size, 1 << 29, np.int32))
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition_graph(path, 2)
+    assert e.value.code == HP_ERR_UNSUPPORTED
+    with pytest.raises(oracle.OracleError) as oe:
+        oracle.partition(path, 2, 1.03)
+    assert oe.value.code == HP_ERR_UNSUPPORTED
+    # grid weights 2^21: total about 5.5e11, every pair far below 2^31
+    g = graphs.grid2d(256, 256)
+    heavy = graphs.Graph(g.xadj, g.adjncy, g.vwgt, np.full(g.nedges, 1 << 21, np.int32))
+    compare_runs(ctx, heavy, 8)
+    # grid weights 2^26: level 0 fits, a coarser level's pairs reach 2^31
+    heavier = graphs.Graph(g.xadj, g.adjncy, g.vwgt, np.full(g.nedges, 1 << 26, np.int32))
+    with pytest.raises(hp.HpError) as e:
+        ctx.partition_graph(heavier, 8)
+    assert e.value.code == HP_ERR_UNSUPPORTED
+    with pytest.raises(oracle.OracleError) as oe:
+        oracle.partition(heavier, 8, 1.03)
+    assert oe.value.code == HP_ERR_UNSUPPORTED
+    part, cut = ctx.partition_graph(g, 4)
+    assert cut == oracle.edgecut(g, part)
+
+
 def test_legacy_entry_point(ctx):
     g = graphs.grid2d(40, 30, seed=3, wmin=1, wmax=9)
     lib = hp.load_library()
