@@ -96,6 +96,7 @@ TUNING_FIELDS = [
     "contract_smem_cn",
     "batch_workers",
     "small_match_n",
+    "contract_hybrid",
 ]
 
 TUNING_DEFAULTS = {
@@ -115,6 +116,7 @@ TUNING_DEFAULTS = {
     "contract_smem_cn": 49152,
     "batch_workers": 16,
     "small_match_n": 8192,
+    "contract_hybrid": 1,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -140,6 +142,7 @@ def tuning_violation(t: dict):
         ("contract_smem_cn", 0, 49152),
         ("batch_workers", 1, 64),
         ("small_match_n", 0, 8192),
+        ("contract_hybrid", 0, 1),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -148,7 +151,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 8)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 7)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

@@ -25,21 +25,25 @@ namespace {
 
 // Structural validation: vertex checks per thread, adjacency checks in
 // edge-parallel tiles of VE_TILE entries, so hub rows cost no more than their
-// share of the array.  The owner row of every entry of a tile comes from a
-// shared-memory max-scan over row-start markers: the rows starting inside the
-// tile mark their first entry, the row overlapping the tile's start (one
-// binary search) marks entry 0, and the running maximum is the owner.
+// share of the array.  The owner row of every entry of a tile comes from
+// hp::tile_owners (row-start markers and a shared-memory max-scan).
+// Also records the largest degree (*maxdeg, for the weight-range gate).
 __global__ void validate_vertices_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
-                                         const int32_t *__restrict__ vwgt, unsigned *status)
+                                         const int32_t *__restrict__ vwgt, unsigned *status,
+                                         unsigned long long *maxdeg)
 {
     bool bad = false;
+    int32_t dmax = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         int32_t b = xadj[v], e = xadj[v + 1];
         if (b > e || b < 0 || e > m) bad = true;
         if (vwgt && vwgt[v] < 0) bad = true;
+        dmax = max(dmax, e - b);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && (xadj[0] != 0 || xadj[n] != m)) bad = true;
     if (bad) atomicOr(status, HP_STATUS_BAD_GRAPH);
+    dmax = hp::warp_max(dmax);
+    if ((threadIdx.x & 31) == 0 && dmax > 0) atomicMax(maxdeg, (unsigned long long)dmax);
 }
 
 constexpr int VE_THREADS = 256, VE_ITEMS = 16, VE_TILE = VE_THREADS * VE_ITEMS;
@@ -62,7 +66,7 @@ __device__ __forceinline__ unsigned long long sym_term(int32_t v, int32_t u, int
 // xadj[n] = m, so every entry has exactly one owner row).  Besides the range,
 // self-loop and weight checks of every entry it accumulates:
 //   sums[0]           the symmetry fingerprint (0 for a symmetric adjacency);
-//   sums[1]           unused (zero);
+//   sums[1]           the largest edge weight (atomic max);
 //   sums[2]           the total edge weight (int64);
 //   sums[3]           the entries of the rows that are not strictly increasing
 //                     (unsorted[v] = 1 for those rows), the only rows that
@@ -76,56 +80,13 @@ validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
     __shared__ int32_t s_warp[VE_THREADS / 32];
     __shared__ int32_t s_v0;
     if (*status & HP_STATUS_BAD_GRAPH) return;   // uniform over the grid
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     bool bad = false;
     unsigned long long fp = 0;
     long long wsum = 0, uent = 0;
+    int32_t wmax = 0;
     for (int64_t tb = (int64_t)blockIdx.x * VE_TILE; tb < m; tb += (int64_t)gridDim.x * VE_TILE) {
         const int64_t te = tb + VE_TILE < m ? tb + VE_TILE : m;
-        if (threadIdx.x == 0) {
-            // the last row starting at or before tb (xadj[0] = 0 <= tb < m = xadj[n])
-            int32_t lo = 0, hi = n - 1;
-            while (lo < hi) {
-                const int32_t mid = (int32_t)(((int64_t)lo + hi + 1) / 2);
-                if (xadj[mid] <= tb) lo = mid; else hi = mid - 1;
-            }
-            s_v0 = lo;
-        }
-        for (int i = threadIdx.x; i < VE_TILE; i += VE_THREADS) owner[i] = -1;
-        __syncthreads();
-        const int32_t v0 = s_v0;
-        if (threadIdx.x == 0) owner[0] = v0;
-        // rows v > v0 start after tb; those starting before te mark their start
-        // (an empty row shares its start with a later row, which wins the max)
-        for (int64_t v = (int64_t)v0 + 1 + threadIdx.x; v < n; v += VE_THREADS) {
-            const int32_t b = xadj[v];
-            if (b >= te) break;
-            atomicMax(&owner[b - tb], (int32_t)v);
-        }
-        __syncthreads();
-        // inclusive max-scan: VE_ITEMS consecutive markers per thread
-        int32_t run = -1;
-#pragma unroll
-        for (int q = 0; q < VE_ITEMS; q++) run = max(run, owner[threadIdx.x * VE_ITEMS + q]);
-        int32_t x = run;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int32_t y = __shfl_up_sync(HP_FULL_MASK, x, o);
-            if (lane >= o) x = max(x, y);
-        }
-        if (lane == 31) s_warp[wid] = x;
-        int32_t ex = __shfl_up_sync(HP_FULL_MASK, x, 1);
-        if (lane == 0) ex = -1;
-        __syncthreads();
-        for (int w = 0; w < wid; w++) ex = max(ex, s_warp[w]);
-        __syncthreads();   // every thread has read the markers it scans
-#pragma unroll
-        for (int q = 0; q < VE_ITEMS; q++) {
-            const int i = threadIdx.x * VE_ITEMS + q;
-            ex = max(ex, owner[i]);
-            owner[i] = ex;
-        }
-        __syncthreads();
+        hp::tile_owners<VE_THREADS, VE_ITEMS>(xadj, n, tb, te, owner, s_warp, &s_v0);
         // checks, coalesced over the tile
         for (int64_t j = tb + threadIdx.x; j < te; j += VE_THREADS) {
             const int32_t v = owner[j - tb];
@@ -134,6 +95,7 @@ validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
             if (u < 0 || u >= n || u == v) bad = true;
             if (w <= 0) bad = true;
             wsum += w;
+            wmax = max(wmax, w);
             fp += sym_term(v, u, w);
             // the next entry of the same row (within the tile, or across its end)
             const int64_t jn = j + 1;
@@ -145,6 +107,8 @@ validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
     if (bad) atomicOr(status, HP_STATUS_BAD_GRAPH);
     hp::block_add_to<VE_THREADS>((long long)fp, &sums[0]);
     hp::block_add_to<VE_THREADS>(wsum, &sums[2]);
+    wmax = hp::warp_max(wmax);
+    if ((threadIdx.x & 31) == 0 && wmax > 0) atomicMax(&sums[1], (unsigned long long)wmax);
     hp::block_add_to<VE_THREADS>(uent, &sums[3]);
 }
 
@@ -246,9 +210,14 @@ void reset_arena(hp_context *c)
     c->trace_valid = false;
 }
 
+// The level chain holds sum_l (8 m_l + ~20 n_l) bytes.  On power-law graphs the
+// adjacency barely shrinks for the first levels (R-MAT: sum_l m_l is about
+// 7-9 m_0, against 3 m_0 on a 3-D grid and 1.7 m_0 on a geometric graph), so
+// the estimate covers 8 bytes x 8 m_0 plus the uncoarsening's gain rows and
+// work arrays; an arena that still runs out is doubled and the call restarts.
 size_t estimate_arena(int64_t n, int64_t m)
 {
-    return (size_t)(160 * n + 40 * m) + ((size_t)256 << 20);
+    return (size_t)(160 * n + 80 * m) + ((size_t)256 << 20);
 }
 
 int32_t default_coarsen_to(int32_t nparts)
@@ -267,15 +236,16 @@ int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, i
     unsigned long long *sc = c->d_scal;
 
     // scalar slots: [0] total vertex weight, [1] symmetry fingerprint, [2]
-    // unused, [3] total edge weight, [4] entries of unsorted rows
+    // largest edge weight, [3] total edge weight, [4] entries of unsorted rows,
+    // [5] largest degree
     const size_t vmark = c->hi;
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 5, c->stream));
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 6, c->stream));
     int32_t *unsorted = nullptr;
     if (c->opt.validate) {
         unsorted = ralloc_t<int32_t>(c, n);
         HP_CHECK_OOM(c);
         HP_CUDA(cudaMemsetAsync(unsorted, 0, sizeof(int32_t) * (size_t)n, c->stream));
-        HP_LAUNCH(c, validate_vertices_kernel, gsz(c, n), 256, 0, n, g0.m, g0.xadj, g0.vwgt, c->d_status);
+        HP_LAUNCH(c, validate_vertices_kernel, gsz(c, n), 256, 0, n, g0.m, g0.xadj, g0.vwgt, c->d_status, &sc[5]);
         HP_LAUNCH(c, validate_edges_kernel,
                   (unsigned)std::max<int64_t>(1, std::min<int64_t>((g0.m + VE_TILE - 1) / VE_TILE,
                                                                    (int64_t)c->sm_count * 8)),
@@ -285,7 +255,7 @@ int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, i
         HP_LAUNCH(c, sum_kernel, gsz(c, g0.m), 256, 0, g0.m, g0.adjwgt, &sc[3]);
     }
     HP_LAUNCH(c, sum_kernel, gsz(c, n), 256, 0, (int64_t)n, g0.vwgt, &sc[0]);
-    long long vs[5] = {};
+    long long vs[6] = {};
     HP_TRY(hp_read_scalars(c, &sc[0], sizeof(vs), vs));
     HP_TRY(hp_check_status(c));
     if (c->opt.validate) {
@@ -314,13 +284,19 @@ int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, i
     if (tv >= INT32_MAX) return HP_ERR_UNSUPPORTED;
     st.tvwgt = tv;
     // Coarse edge weights, gain-row connectivities and bisection gains are
-    // int32.  Each is a sum of level-0 edge weights, so when the total edge
-    // weight is below 2^31 none can wrap; otherwise every contraction checks
-    // that each matched pair's weighted degrees sum below 2^31 (a bound on
-    // every coarse edge weight and connectivity it creates) and the call fails
-    // with HP_ERR_UNSUPPORTED if one does not.
+    // int32.  Each is a sum of input edge weights, so when the total edge
+    // weight is below 2^31 none can wrap; otherwise the input's rows and every
+    // coarse row the contraction builds must have a weighted degree below 2^31
+    // (each weight or connectivity of a vertex is at most that), and the call
+    // fails with HP_ERR_UNSUPPORTED if one does not.
     c->weight_check = vs[3] >= (long long)INT32_MAX;
-    if (c->weight_check) HP_TRY(hp_check_weight_range(c, g0));   // read with the first level's status check
+    // the input level's rows, before any kernel sums them in int32; not needed
+    // when the validation's largest degree times largest weight is below 2^31
+    const bool row_bound = c->opt.validate && vs[5] * vs[2] < (long long)INT32_MAX;
+    if (c->weight_check && !row_bound) {
+        HP_TRY(hp_check_weight_range(c, g0));
+        HP_TRY(hp_check_status(c));
+    }
 
     const int32_t thr = c->opt.coarsen_to > 0 ? c->opt.coarsen_to : default_coarsen_to(nparts);
     const int64_t maxvwgt = (3 * (int64_t)tv) / (2 * (int64_t)thr);
@@ -350,7 +326,7 @@ int vcycle(hp_context *c, int32_t nparts, const float *tpwgts, float ubfactor, i
     HP_CUDA(cudaMemsetAsync(pw, 0, sizeof(unsigned long long) * nparts, c->stream));
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 2, c->stream));
     HpLevel &f = c->levels[0];
-    HP_TRY(hp_edgecut_launch(c, n, f.xadj, f.adjncy, f.adjwgt, f.where, &sc[0]));
+    HP_TRY(hp_edgecut_launch(c, n, f.m, f.xadj, f.adjncy, f.adjwgt, f.where, &sc[0]));
     HP_LAUNCH(c, final_pw_kernel, gsz(c, n), 256, nparts <= 2048 ? sizeof(unsigned long long) * nparts : 0, n,
               f.where, f.vwgt, pw, nparts, c->d_status);
     std::vector<unsigned long long> hpw(nparts);
@@ -640,6 +616,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->contract_smem_cn = HP_TUNE_SMEM_CN_MAX;
     t->batch_workers = 16;
     t->small_match_n = 8192;
+    t->contract_hybrid = 1;
 }
 
 namespace {
@@ -663,6 +640,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.contract_smem_cn, 0, HP_TUNE_SMEM_CN_MAX)) return "contract_smem_cn";
     if (!in(t.batch_workers, 1, 64)) return "batch_workers";
     if (!in(t.small_match_n, 0, HP_TUNE_SMALL_MATCH_MAX)) return "small_match_n";
+    if (!in(t.contract_hybrid, 0, 1)) return "contract_hybrid";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;
@@ -1029,7 +1007,7 @@ HP_API int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xa
     ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
     HP_CUDA(cudaMemsetAsync(ctx->d_scal, 0, sizeof(unsigned long long), ctx->stream));
     if (d_adjwgt) {
-        HP_TRY(hp_edgecut_launch(ctx, nvtxs, d_xadj, d_adjncy, d_adjwgt, d_where, ctx->d_scal));
+        HP_TRY(hp_edgecut_launch(ctx, nvtxs, -1, d_xadj, d_adjncy, d_adjwgt, d_where, ctx->d_scal));
     } else {
         // unit weights: count cut entries through a ones array in the arena
         int64_t m = 0;
@@ -1042,7 +1020,7 @@ HP_API int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xa
         int32_t *ones = ralloc_t<int32_t>(ctx, m);
         HP_CHECK_OOM(ctx);
         HP_LAUNCH(ctx, fill_ones_kernel, gsz(ctx, m), 256, 0, m, ones);
-        HP_TRY(hp_edgecut_launch(ctx, nvtxs, d_xadj, d_adjncy, ones, d_where, ctx->d_scal));
+        HP_TRY(hp_edgecut_launch(ctx, nvtxs, -1, d_xadj, d_adjncy, ones, d_where, ctx->d_scal));
     }
     long long c2 = 0;
     HP_TRY(hp_read_scalars(ctx, ctx->d_scal, sizeof(long long), &c2));

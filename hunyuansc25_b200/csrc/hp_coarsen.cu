@@ -596,31 +596,39 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
     }
 }
 
-// Weight range of a contraction (run when the level-0 total edge weight is
-// 2^31 or more): every coarse edge weight and every connectivity of a coarse
-// vertex is at most the sum of its pair's fine weighted degrees, so a pair
-// whose sum reaches 2^31 sets HP_STATUS_WEIGHT_RANGE (the int32 coarse weights
-// could wrap; the call then fails) and no other pair can wrap.  One warp per
-// vertex; leaders sum both rows in int64.  match = nullptr checks every
-// vertex's own weighted degree (the input level).
+// Weight range (checked when the input's total edge weight is 2^31 or more):
+// every coarse edge weight and every gain-row connectivity of a vertex is at
+// most the vertex's weighted degree, so the int32 weights and connectivities
+// cannot wrap while every vertex of every level has a weighted degree below
+// 2^31.  The contraction kernels check each coarse row's sum of kept weights
+// (int64) as they gather it; this kernel checks the input level's rows (a
+// thread per row, rows longer than 32 entries by the whole warp).  A row at or
+// above 2^31 sets HP_STATUS_WEIGHT_RANGE, and the call fails.
 __global__ void __launch_bounds__(256)
-pair_weight_bound_kernel(int32_t n, const int32_t *__restrict__ match, const int32_t *__restrict__ xadj,
-                         const int32_t *__restrict__ adjwgt, unsigned *status)
+row_weight_range_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjwgt,
+                        unsigned *status)
 {
     const int lane = threadIdx.x & 31;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const int32_t b = v < n ? xadj[v] : 0, e = v < n ? xadj[v + 1] : 0;
+    const bool coop = e - b > 32;
     bool over = false;
-    for (int64_t v = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
-        const int32_t u = match ? match[v] : (int32_t)v;   // no match: every vertex alone
-        if (u < v) continue;   // a follower: its leader sums the pair
+    if (!coop) {
         long long s = 0;
-        for (int32_t j = xadj[v] + lane; j < xadj[v + 1]; j += 32) s += adjwgt[j];
-        if (u != v)
-            for (int32_t j = xadj[u] + lane; j < xadj[u + 1]; j += 32) s += adjwgt[j];
+        for (int32_t j = b; j < e; j++) s += adjwgt[j];
+        over = s >= (long long)INT32_MAX;
+    }
+    unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
+    while (cm) {
+        const int src = __ffs(cm) - 1;
+        cm &= cm - 1;
+        const int32_t sb = __shfl_sync(HP_FULL_MASK, b, src), se = __shfl_sync(HP_FULL_MASK, e, src);
+        long long s = 0;
+        for (int32_t j = sb + lane; j < se; j += 32) s += adjwgt[j];
         s = hp::warp_sum64(s);
         over |= s >= (long long)INT32_MAX;
     }
-    if (over && lane == 0) atomicOr(status, HP_STATUS_WEIGHT_RANGE);
+    if (over) atomicOr(status, HP_STATUS_WEIGHT_RANGE);
 }
 
 // The fine rows merged into coarse row c: entry i is the i-th entry of the
@@ -712,7 +720,7 @@ __global__ void __launch_bounds__(ASM_TILE)
 contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict__ ucnt,
                          int32_t *__restrict__ cxadj, int32_t *__restrict__ cadjncy,
                          int32_t *__restrict__ cadjwgt, unsigned long long *tile_status, hp::LbCtl *lb,
-                         unsigned *status, int32_t thread_row)
+                         unsigned *status, int32_t thread_row, int wcheck)
 {
     extern __shared__ unsigned long long asm_stage[];                      // ASM_TILE * XN
     uint8_t *s_row = reinterpret_cast<uint8_t *>(asm_stage + ASM_TILE * XN);   // tile row of each entry
@@ -765,6 +773,15 @@ contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict_
         }
     }
     __syncthreads();
+    if (wcheck && small) {
+        // the coarse row's weighted degree (weight range, row_weight_range_kernel)
+        long long ws = 0;
+        for (int i = 0; i < len; i++) {
+            const unsigned long long e = asm_stage[ioff + i];
+            if (e != hp::PACK_NONE) ws += (uint32_t)e;
+        }
+        if (ws >= (long long)INT32_MAX) atomicOr(status, HP_STATUS_WEIGHT_RANGE);
+    }
     const unsigned wmax = __reduce_max_sync(HP_FULL_MASK, small ? (unsigned)len : 0u);
     unsigned long long x[XN];
     int u = 0;
@@ -1020,10 +1037,11 @@ __device__ int group_merge_emit(const unsigned long long *A, int N, int32_t *out
 // the count of real entries is returned.
 template <int G>
 __device__ int group_gather_row(const ContractSrc &src, int32_t c, const RowInfo &r, int32_t len,
-                                unsigned long long *A, int32_t *s_scan)
+                                unsigned long long *A, int32_t *s_scan, long long *wpart)
 {
     const int t = threadIdx.x % G;
     int self = 0;
+    long long ws = 0;   // this thread's share of the row's kept weights
     // four entries per thread at a time: the row loads, then the coarse-id
     // gathers, are issued together
     for (int i0 = t; i0 < len; i0 += 4 * G) {
@@ -1042,13 +1060,36 @@ __device__ int group_gather_row(const ContractSrc &src, int32_t c, const RowInfo
             int32_t ww = w[q];
             if (k == c) { k = hp::KEY_NONE; ww = 0; }
             self += k == hp::KEY_NONE;
+            ws += ww;
             A[i0 + q * G] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)ww;
         }
     }
+    *wpart = ws;
     int tot;
     group_excl_scan<G>(self, &tot, s_scan);
     group_sync<G>();
     return len - tot;
+}
+
+// Weight range of a coarse row gathered by a group (row_weight_range_kernel's
+// rule): the group's int64 total of the kept weights; s64 holds G/32 slots.
+template <int G>
+__device__ void group_weight_range(long long wpart, long long *s64, unsigned *status)
+{
+    const long long w = hp::warp_sum64(wpart);
+    if (G == 32) {
+        if ((threadIdx.x & 31) == 0 && w >= (long long)INT32_MAX) atomicOr(status, HP_STATUS_WEIGHT_RANGE);
+        return;
+    }
+    const int t = threadIdx.x % G;
+    if ((t & 31) == 0) s64[t >> 5] = w;
+    group_sync<G>();
+    if (t == 0) {
+        long long tot = 0;
+        for (int i = 0; i < G / 32; i++) tot += s64[i];
+        if (tot >= (long long)INT32_MAX) atomicOr(status, HP_STATUS_WEIGHT_RANGE);
+    }
+    group_sync<G>();
 }
 
 constexpr int WROW_MAX = HP_TUNE_WARP_ROW_MAX;   // warp class: up to 256 entries
@@ -1059,7 +1100,7 @@ constexpr int WROW_WARPS = 8;
 __global__ void __launch_bounds__(32 * WROW_WARPS)
 contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, ContractSrc src,
                            const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
-                           int32_t *__restrict__ ucnt, int kbits)
+                           int32_t *__restrict__ ucnt, int kbits, int wcheck, unsigned *status)
 {
     __shared__ unsigned long long sA[WROW_WARPS][WROW_MAX], sB[WROW_WARPS][WROW_MAX];
     __shared__ int32_t sH[WROW_WARPS][256];
@@ -1070,7 +1111,9 @@ contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__re
         RowInfo r;
         int32_t len;
         src.row(c, r, len);
-        const int N = group_gather_row<32>(src, c, r, len, sA[wid], nullptr);
+        long long wpart;
+        const int N = group_gather_row<32>(src, c, r, len, sA[wid], nullptr, &wpart);
+        if (wcheck) group_weight_range<32>(wpart, nullptr, status);
         group_radix_sort<32>(sA[wid], sB[wid], len, kbits, sH[wid], nullptr);
         const int32_t off = toff[c];
         const int U = group_merge_emit<32>(sA[wid], N, tk + off, tw + off, (uint32_t *)sB[wid], nullptr);
@@ -1093,12 +1136,13 @@ template <int NT, int CAP>
 __global__ void __launch_bounds__(NT)
 contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, ContractSrc src,
                           const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
-                          int32_t *__restrict__ ucnt, int kbits, int32_t min_len)
+                          int32_t *__restrict__ ucnt, int kbits, int32_t min_len, int wcheck, unsigned *status)
 {
     extern __shared__ unsigned long long dsm[];
     unsigned long long *A = dsm, *B = dsm + CAP;
     int32_t *hist = (int32_t *)(dsm + 2 * CAP);
     __shared__ int32_t s_scan[2 * (NT / 32) + 2];
+    __shared__ long long s64[NT / 32];
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
         const int32_t c = list[li];
@@ -1106,7 +1150,9 @@ contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__res
         int32_t len;
         src.row(c, r, len);
         if (len > CAP || len <= min_len) continue;   // another instance's row
-        const int N = group_gather_row<NT>(src, c, r, len, A, s_scan);
+        long long wpart;
+        const int N = group_gather_row<NT>(src, c, r, len, A, s_scan, &wpart);
+        if (wcheck) group_weight_range<NT>(wpart, s64, status);
         group_radix_sort<NT>(A, B, len, kbits, hist, s_scan);
         const int32_t off = toff[c];
         const int U = group_merge_emit<NT>(A, N, tk + off, tw + off, (uint32_t *)B, s_scan);
@@ -1118,6 +1164,151 @@ contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__res
 template <int NT, int CAP>
 constexpr size_t cta_radix_smem() { return sizeof(unsigned long long) * 2 * CAP + sizeof(int32_t) * 256 * (NT / 32); }
 
+
+// ---- long rows, hybrid: dense accumulation of the low ids, radix sort of the rest --
+// On power-law graphs a long coarse row points mostly at hubs, and hubs have
+// low coarse ids (coarse ids follow the leaders' fine ids, and the R-MAT hubs
+// have low ids): on R-MAT levels of 90K-160K coarse vertices 78-98 % of the
+// long rows' entries have an id below 48K, 57 % at 300K.  The shared-memory
+// dense accumulator is several times faster per entry than a radix sort, but
+// one accumulator over all coarse ids fits only up to 48K ids.  So each CTA
+// keeps a dense accumulator for the ids below HY_HOT and a buffer for the rest:
+//   - gather: an entry with a low id is added to acc[id] and marked in the
+//     bitmap; any other entry is appended to the cold buffer (its order does
+//     not matter: equal ids are merged by summing, and the sort orders the rest);
+//   - the low ids come out in ascending order from the bitmap (two words per
+//     thread, a block scan for the offsets), clearing acc and the bitmap;
+//   - the cold entries are radix-sorted and merged after them, so the row is
+//     sorted as a whole and equals what the pure radix path writes.
+// A row whose cold part exceeds HY_COLD entries is cleared and appended to the
+// spill list, which the radix / dense kernels then take.  The kernel runs one
+// CTA per SM (its shared memory), so it pays on levels where most entries are
+// low ids: levels of at most HY_MAX_CN coarse vertices (measured on R-MAT
+// scale 22: 2x faster than the radix classes at 74K coarse ids, slower from
+// about 200K, where half of the entries are cold).
+constexpr int HY_THREADS = 1024;
+constexpr int HY_HOT = 32768;                 // ids below this accumulate densely
+constexpr int HY_WORDS = HY_HOT / 32;         // bitmap words
+constexpr int HY_WPT = HY_WORDS / HY_THREADS; // bitmap words per thread in the extraction
+constexpr int HY_COLD = 2048;                 // cold entries a row may have
+constexpr int32_t HY_MAX_CN = 4 * HY_HOT;     // levels the hybrid kernel takes
+static_assert(HY_WORDS % HY_THREADS == 0 && HY_WPT >= 1, "extraction: whole words per thread");
+
+constexpr size_t hybrid_smem()
+{
+    return sizeof(unsigned long long) * 2 * HY_COLD + sizeof(int32_t) * HY_HOT + sizeof(unsigned) * HY_WORDS +
+           sizeof(int32_t) * 256 * (HY_THREADS / 32);
+}
+
+__global__ void __launch_bounds__(HY_THREADS, 1)
+contract_hybrid_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count, ContractSrc src,
+                       const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
+                       int32_t *__restrict__ ucnt, int kbits, int32_t min_len, int32_t *__restrict__ spill,
+                       int32_t *d_nspill, int wcheck, unsigned *status)
+{
+    extern __shared__ unsigned long long hy_smem[];
+    unsigned long long *A = hy_smem, *B = hy_smem + HY_COLD;
+    int32_t *acc = reinterpret_cast<int32_t *>(hy_smem + 2 * HY_COLD);
+    unsigned *bm = reinterpret_cast<unsigned *>(acc + HY_HOT);
+    int32_t *hist = reinterpret_cast<int32_t *>(bm + HY_WORDS);
+    __shared__ int32_t s_scan[2 * (HY_THREADS / 32) + 2];
+    __shared__ long long s64[HY_THREADS / 32];
+    __shared__ int32_t s_ncold;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < HY_HOT; i += HY_THREADS) acc[i] = 0;   // every row leaves them zero
+    for (int i = tid; i < HY_WORDS; i += HY_THREADS) bm[i] = 0u;
+    if (tid == 0) s_ncold = 0;
+    __syncthreads();
+    const int32_t cnt = *d_count;
+    for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
+        const int32_t c = list[li];
+        RowInfo r;
+        int32_t len;
+        src.row(c, r, len);
+        if (len <= min_len) continue;   // (uniform over the CTA)
+        long long ws = 0;
+        // four entries per thread in flight: the row loads, then the cmap gathers
+        for (int32_t i0 = tid; i0 < len; i0 += 4 * HY_THREADS) {
+            int32_t a[4], w[4];
+            bool in[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int32_t i = i0 + q * HY_THREADS;
+                in[q] = i < len;
+                const int32_t j = in[q] ? (i < r.l0 ? r.s0 + i : r.s1 + (i - r.l0)) : 0;
+                a[q] = in[q] ? src.adjncy[j] : 0;
+                w[q] = in[q] ? src.adjwgt[j] : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (!in[q]) continue;
+                const int32_t k = src.cmap[a[q]];
+                if (k == c) continue;   // the coarse self key
+                ws += w[q];
+                if (k < HY_HOT) {
+                    atomicAdd(&acc[k], w[q]);
+                    atomicOr(&bm[k >> 5], 1u << (k & 31));
+                } else {
+                    const int32_t pos = atomicAdd(&s_ncold, 1);
+                    if (pos < HY_COLD) A[pos] = ((unsigned long long)(uint32_t)k << 32) | (uint32_t)w[q];
+                }
+            }
+        }
+        __syncthreads();
+        if (wcheck) group_weight_range<HY_THREADS>(ws, s64, status);
+        const int32_t ncold = s_ncold;
+        if (ncold > HY_COLD) {
+            // the cold part does not fit: clear the dense part and leave the row to the spill kernels
+            for (int wi = tid; wi < HY_WORDS; wi += HY_THREADS) {
+                unsigned word = bm[wi];
+                if (!word) continue;
+                bm[wi] = 0u;
+                for (; word; word &= word - 1) acc[(wi << 5) + __ffs(word) - 1] = 0;
+            }
+            if (tid == 0) {
+                spill[atomicAdd(d_nspill, 1)] = c;
+                s_ncold = 0;
+            }
+            __syncthreads();
+            continue;
+        }
+        const int32_t off = toff[c];
+        // the low ids in ascending order: HY_WPT consecutive bitmap words per thread
+        unsigned wd[HY_WPT];
+        int hc = 0;
+#pragma unroll
+        for (int q = 0; q < HY_WPT; q++) {
+            wd[q] = bm[tid * HY_WPT + q];
+            hc += __popc(wd[q]);
+        }
+        int uh;
+        int p = hp::block_excl_scan<HY_THREADS>(hc, &uh, s_scan);
+#pragma unroll
+        for (int q = 0; q < HY_WPT; q++) {
+            const int wi = tid * HY_WPT + q;
+            unsigned word = wd[q];
+            if (word) bm[wi] = 0u;
+            for (; word; word &= word - 1) {
+                const int32_t k = (wi << 5) + __ffs(word) - 1;
+                tk[off + p] = k;
+                tw[off + p] = acc[k];
+                acc[k] = 0;
+                p++;
+            }
+        }
+        // the rest, sorted and merged after them
+        int uc = 0;
+        if (ncold > 0) {
+            group_radix_sort<HY_THREADS>(A, B, ncold, kbits, hist, s_scan);
+            uc = group_merge_emit<HY_THREADS>(A, ncold, tk + off + uh, tw + off + uh, (uint32_t *)B, s_scan);
+        }
+        if (tid == 0) {
+            ucnt[c] = uh + uc;
+            s_ncold = 0;
+        }
+        __syncthreads();
+    }
+}
 
 // Rows longer than XROW_MAX entries: dense accumulator over the coarse id space
 // in a per-CTA global slab (dw: cn ints, bm: cn/32 words, bm2: cn/1024 words;
@@ -1132,10 +1323,12 @@ __global__ void __launch_bounds__(NT)
 contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                       ContractSrc src, const int32_t *__restrict__ toff, int32_t *__restrict__ tk,
                       int32_t *__restrict__ tw, int32_t *__restrict__ ucnt, int32_t cn,
-                      int32_t *slab_w, unsigned *slab_bm, unsigned *slab_bm2, int32_t ratio, int32_t min_len)
+                      int32_t *slab_w, unsigned *slab_bm, unsigned *slab_bm2, int32_t ratio, int32_t min_len,
+                      int wcheck, unsigned *status)
 {
     extern __shared__ int32_t dsm_acc[];
     __shared__ int32_t s_scan[NT / 32 + 2];
+    __shared__ long long s64[NT / 32];
     const int32_t nw = (cn + 31) / 32, nw2 = (cn + 1023) / 1024;
     int32_t *dw;
     unsigned *bm, *bm2;
@@ -1158,6 +1351,7 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
         src.row(c, r, len);
         if (len <= min_len) continue;   // another kernel's row
         const bool two_level = (int64_t)len * ratio < ((int64_t)cn + 31) / 32;
+        long long ws = 0;   // this thread's share of the row's kept weights (weight range)
         for (int32_t i0 = threadIdx.x; i0 < len; i0 += 4 * NT) {
             int32_t a[4], wq[4];
             bool in[4];
@@ -1174,6 +1368,7 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
                 if (!in[q]) continue;
                 const int32_t k = src.cmap[a[q]];
                 if (k == c) continue;   // the coarse self key
+                ws += wq[q];
                 if (two_level) {
                     hp::dense_mark2(dw, bm, bm2, k, wq[q]);
                 } else {
@@ -1183,6 +1378,7 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
             }
         }
         __syncthreads();
+        if (wcheck) group_weight_range<NT>(ws, s64, status);
         int32_t off = toff[c];
         int tot = two_level ? hp::dense_extract2<NT>(dw, bm, bm2, cn, tk + off, tw + off, s_scan)
                             : hp::dense_extract<NT>(dw, bm, cn, tk + off, tw + off, s_scan);
@@ -1590,15 +1786,12 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     if (ntiles > c->lb_cap) return HP_ERR_INTERNAL;   // reserved at the start of every call
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 4, c->stream));
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 5, c->stream));
     int32_t *counts = (int32_t *)sc;          // 3 long-row class counts + max length in slots 0-1
     int32_t *maxlen = counts + 3;
     unsigned long long *long_total = &sc[2];  // entries of the long rows
     int32_t *small_max = (int32_t *)&sc[3];   // longest short row above 8 entries (0: none)
 
-    if (c->weight_check)
-        HP_LAUNCH(c, pair_weight_bound_kernel, std::min<unsigned>(blocks_for((int64_t)n * 32), c->sm_count * 16),
-                  256, 0, n, g.match, g.xadj, g.adjwgt, c->d_status);
     int tok = hp_prof_begin(c);
     HP_LAUNCH(c, coarse_setup_kernel, blocks_for(n), 256, 0, n, g.match, g.cmap, g.xadj, g.vwgt, rinfo, cg.vwgt,
               toff, lists, counts, cn, maxlen, long_total, small_max, c->tune.contract_thread_row,
@@ -1608,6 +1801,7 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     HP_TRY(hp_read_scalars(c, sc, sizeof(h), &h));
     const bool any_long = h.cnt[0] + h.cnt[1] + h.cnt[2] > 0;
     ContractSrc src{rinfo, g.adjncy, g.adjwgt, g.cmap};
+    const int wchk = c->weight_check ? 1 : 0;   // coarse rows' weighted degrees below 2^31
     int32_t *tk = nullptr, *tw = nullptr;
     tok = hp_prof_begin(c);
     if (any_long) {
@@ -1624,7 +1818,7 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
         if (h.cnt[0] > 0)
             HP_LAUNCH(c, contract_warp_radix_kernel,
                       (unsigned)std::min<int64_t>((h.cnt[0] + WROW_WARPS - 1) / WROW_WARPS, c->sm_count * 6),
-                      32 * WROW_WARPS, 0, lists, &counts[0], src, toff, tk, tw, ucnt, kbits);
+                      32 * WROW_WARPS, 0, lists, &counts[0], src, toff, tk, tw, ucnt, kbits, wchk, c->d_status);
         // a level whose coarse ids fit a shared-memory dense accumulator merges
         // every long row there (one atomic per entry, ordered extraction)
         const bool smem_dense = cn <= c->tune.contract_smem_cn;
@@ -1636,24 +1830,43 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
                               (unsigned)std::min<int64_t>(h.cnt[cls], c->sm_count), 1024, acc,
                               lists + cls * (int64_t)cn, &counts[cls], src, toff, tk, tw, ucnt, cn,
                               (int32_t *)nullptr, (unsigned *)nullptr, (unsigned *)nullptr,
-                              c->tune.dense_sparse_ratio, 0);
+                              c->tune.dense_sparse_ratio, 0, wchk, c->d_status);
         }
-        if (!smem_dense && h.cnt[1] > 0) {
+        // hybrid: the rows of lists 1 and 2 accumulate their low ids densely and
+        // radix-sort the rest; rows whose rest does not fit go to the spill list,
+        // which the CTA radix (up to XROW_MAX) and dense slab kernels then take
+        const bool hybrid = !smem_dense && cn <= HY_MAX_CN && c->tune.contract_hybrid && h.cnt[1] + h.cnt[2] > 0;
+        int32_t *spill = nullptr;
+        int32_t *d_nspill = (int32_t *)&sc[4];
+        if (hybrid) {
+            spill = ralloc_t<int32_t>(c, (int64_t)h.cnt[1] + h.cnt[2]);
+            HP_CHECK_OOM(c);
+            for (int cls = 1; cls <= 2; cls++)
+                if (h.cnt[cls] > 0)
+                    HP_LAUNCH(c, contract_hybrid_kernel, (unsigned)std::min<int64_t>(h.cnt[cls], c->sm_count),
+                              HY_THREADS, hybrid_smem(), lists + cls * (int64_t)cn, &counts[cls], src, toff, tk, tw,
+                              ucnt, kbits, 0, spill, d_nspill, wchk, c->d_status);
+            HP_LAUNCH(c, (contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>),
+                      (unsigned)std::min<int64_t>((int64_t)h.cnt[1] + h.cnt[2], c->sm_count), XROW_THREADS,
+                      (cta_radix_smem<XROW_THREADS, XROW_MAX>()), spill, d_nspill, src, toff, tk, tw, ucnt, kbits, 0,
+                      wchk, c->d_status);
+        }
+        if (!smem_dense && !hybrid && h.cnt[1] > 0) {
             HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>),
                       (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 8), CROW_THREADS,
                       (cta_radix_smem<CROW_THREADS, MROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits,
-                      0);
+                      0, wchk, c->d_status);
             if (c->tune.contract_cta_row > MROW_MAX)
                 HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
                           (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 3), CROW_THREADS,
                           (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt,
-                          kbits, MROW_MAX);
+                          kbits, MROW_MAX, wchk, c->d_status);
         }
-        if (!smem_dense && h.cnt[2] > 0)
+        if (!smem_dense && !hybrid && h.cnt[2] > 0)
             HP_LAUNCH(c, (contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>),
                       (unsigned)std::min<int64_t>(h.cnt[2], c->sm_count), XROW_THREADS,
                       (cta_radix_smem<XROW_THREADS, XROW_MAX>()), lists + 2 * (int64_t)cn, &counts[2], src, toff, tk,
-                      tw, ucnt, kbits, 0);
+                      tw, ucnt, kbits, 0, wchk, c->d_status);
         if (!smem_dense && h.maxlen > XROW_MAX) {
             // slab per CTA: cn ints + cn/32 + cn/1024 words; bounded to ~512 MB
             const int64_t nw = ((int64_t)cn + 31) / 32, nw2 = ((int64_t)cn + 1023) / 1024;
@@ -1667,20 +1880,21 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
             HP_CUDA(cudaMemsetAsync(sw, 0, sizeof(int32_t) * (size_t)(nb * cn), c->stream));
             HP_CUDA(cudaMemsetAsync(sbm, 0, sizeof(unsigned) * (size_t)(nb * nw), c->stream));
             HP_CUDA(cudaMemsetAsync(sbm2, 0, sizeof(unsigned) * (size_t)(nb * nw2), c->stream));
-            HP_LAUNCH(c, (contract_dense_kernel<1024, false>), (unsigned)nb, 1024, 0, lists + 2 * (int64_t)cn,
-                      &counts[2], src, toff, tk, tw, ucnt, cn, sw, sbm, sbm2, c->tune.dense_sparse_ratio, XROW_MAX);
+            HP_LAUNCH(c, (contract_dense_kernel<1024, false>), (unsigned)nb, 1024, 0,
+                      hybrid ? spill : lists + 2 * (int64_t)cn, hybrid ? d_nspill : &counts[2], src, toff, tk, tw,
+                      ucnt, cn, sw, sbm, sbm2, c->tune.dense_sparse_ratio, XROW_MAX, wchk, c->d_status);
         }
     }
     // short rows + coarse xadj in one ordered pass, then the long rows' copies
     if (h.small_max <= 8)
         HP_LAUNCH(c, contract_assemble_kernel<8>, (unsigned)ntiles, ASM_TILE, asm_smem_bytes<8>(), cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row, wchk);
     else if (h.small_max <= 16)
         HP_LAUNCH(c, contract_assemble_kernel<16>, (unsigned)ntiles, ASM_TILE, asm_smem_bytes<16>(), cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row, wchk);
     else
         HP_LAUNCH(c, contract_assemble_kernel<32>, (unsigned)ntiles, ASM_TILE, asm_smem_bytes<32>(), cn, src, ucnt, cg.xadj,
-                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row);
+                  cg.adjncy, cg.adjwgt, c->lb_status, c->lb_ctl, c->d_status, c->tune.contract_thread_row, wchk);
     if (h.cnt[0] > 0)
         HP_LAUNCH(c, copy_long_rows_kernel<false>, std::min<unsigned>(blocks_for((int64_t)h.cnt[0] * 32),
                                                                      c->sm_count * 16),
@@ -1713,6 +1927,8 @@ int hp_coarsen_init()
     HP_CUDA(cudaFuncSetAttribute(contract_dense_kernel<1024, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(int32_t) * (HP_TUNE_SMEM_CN_MAX + (HP_TUNE_SMEM_CN_MAX + 31) / 32 +
                                                           (HP_TUNE_SMEM_CN_MAX + 1023) / 1024))));
+    HP_CUDA(cudaFuncSetAttribute(contract_hybrid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)hybrid_smem()));
     HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_radix_smem<CROW_THREADS, MROW_MAX>()));
@@ -1727,8 +1943,7 @@ int hp_coarsen_init()
 
 int hp_check_weight_range(hp_context *c, const HpLevel &g)
 {
-    HP_LAUNCH(c, pair_weight_bound_kernel, std::min<unsigned>(blocks_for((int64_t)g.n * 32), c->sm_count * 16), 256,
-              0, g.n, (const int32_t *)nullptr, g.xadj, g.adjwgt, c->d_status);
+    HP_LAUNCH(c, row_weight_range_kernel, blocks_for(g.n), 256, 0, g.n, g.xadj, g.adjwgt, c->d_status);
     return HP_OK;
 }
 

@@ -104,6 +104,83 @@ __device__ __forceinline__ int32_t warp_append(int32_t *counter, bool pred)
     return pred ? base + __popc(m & lanemask_lt()) : -1;
 }
 
+// The row owning entry j of a CSR: the last v with xadj[v] <= j, for
+// xadj[0] = 0 <= j < xadj[n].  A 32-ary search by one warp (one load per lane
+// per round, about log32(n) rounds) instead of a serial binary search's
+// log2(n) dependent loads.  All 32 lanes call it and get the result.
+__device__ __forceinline__ int32_t warp_find_row(const int32_t *__restrict__ xadj, int32_t n, int64_t j)
+{
+    const int lane = threadIdx.x & 31;
+    int32_t lo = 0, hi = n - 1;   // xadj[lo] <= j; the answer lies in [lo, hi]
+    while (hi - lo >= 32) {
+        // 32 probes covering (lo, hi]: p(0) = lo + 1, p(31) = hi
+        const int64_t span = (int64_t)hi - lo;
+        const int32_t p = lo + 1 + (int32_t)((span - 1) * lane / 31);
+        const unsigned m = __ballot_sync(HP_FULL_MASK, xadj[p] <= j);   // a prefix of the lanes
+        if (m == 0u) return lo;
+        const int L = 31 - __clz(m);
+        const int32_t nlo = __shfl_sync(HP_FULL_MASK, p, L);
+        const int32_t nxt = __shfl_sync(HP_FULL_MASK, p, L < 31 ? L + 1 : 31);
+        hi = L < 31 ? nxt - 1 : hi;
+        lo = nlo;
+    }
+    const int32_t p = lo + 1 + lane;
+    const unsigned m = __ballot_sync(HP_FULL_MASK, p <= hi && xadj[p] <= j);
+    return m ? lo + 1 + (31 - __clz(m)) : lo;
+}
+
+// Owner rows of a tile of CSR entries: owner[i] = the row of entry tb + i for
+// i < te - tb <= NT * ITEMS (xadj monotone, xadj[0] = 0, xadj[n] = m > tb).
+// The row holding entry tb comes from warp_find_row; every later row that
+// starts inside the tile marks its first entry (an empty row shares its start
+// with a later row, which wins the max), and an inclusive max-scan over the
+// markers gives every entry its row.  s_warp: NT/32 ints; s_v0: one int.  All
+// NT threads call it; it ends with a barrier.
+template <int NT, int ITEMS>
+__device__ void tile_owners(const int32_t *__restrict__ xadj, int32_t n, int64_t tb, int64_t te,
+                            int32_t *owner, int32_t *s_warp, int32_t *s_v0)
+{
+    constexpr int TILE = NT * ITEMS;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (wid == 0) {
+        const int32_t v0 = warp_find_row(xadj, n, tb);
+        if (lane == 0) *s_v0 = v0;
+    }
+    for (int i = threadIdx.x; i < TILE; i += NT) owner[i] = -1;
+    __syncthreads();
+    const int32_t v0 = *s_v0;
+    if (threadIdx.x == 0) owner[0] = v0;
+    for (int64_t v = (int64_t)v0 + 1 + threadIdx.x; v < n; v += NT) {
+        const int32_t b = xadj[v];
+        if (b >= te) break;
+        atomicMax(&owner[b - tb], (int32_t)v);
+    }
+    __syncthreads();
+    // inclusive max-scan: ITEMS consecutive markers per thread
+    int32_t run = -1;
+#pragma unroll
+    for (int q = 0; q < ITEMS; q++) run = max(run, owner[threadIdx.x * ITEMS + q]);
+    int32_t x = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(HP_FULL_MASK, x, o);
+        if (lane >= o) x = max(x, y);
+    }
+    if (lane == 31) s_warp[wid] = x;
+    int32_t ex = __shfl_up_sync(HP_FULL_MASK, x, 1);
+    if (lane == 0) ex = -1;
+    __syncthreads();
+    for (int w = 0; w < wid; w++) ex = max(ex, s_warp[w]);
+    __syncthreads();   // every thread has read the markers it scans
+#pragma unroll
+    for (int q = 0; q < ITEMS; q++) {
+        const int i = threadIdx.x * ITEMS + q;
+        ex = max(ex, owner[i]);
+        owner[i] = ex;
+    }
+    __syncthreads();
+}
+
 // Inclusive warp scan.
 __device__ __forceinline__ int warp_incl_scan(int v)
 {

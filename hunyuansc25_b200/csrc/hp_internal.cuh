@@ -186,7 +186,7 @@ int hp_compact_flags(hp_context *c, const int32_t *flags, int64_t n, int32_t *ou
 int hp_sort_pairs(hp_context *c, int32_t *keys, int32_t *vals, int32_t *tkeys, int32_t *tvals,
                   int64_t bound, const int32_t *d_count, int key_bits, bool *in_tmp);
 // Exact edge cut (int64) into *d_cut (device, accumulated; caller zeroes).
-int hp_edgecut_launch(hp_context *c, int32_t n, const int32_t *xadj, const int32_t *adjncy,
+int hp_edgecut_launch(hp_context *c, int32_t n, int64_t m, const int32_t *xadj, const int32_t *adjncy,
                       const int32_t *adjwgt, const int32_t *where, unsigned long long *d_cut);
 
 // ---- coarsening (hp_coarsen.cu) -----------------------------------------------

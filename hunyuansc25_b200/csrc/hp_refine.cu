@@ -1730,11 +1730,15 @@ __device__ void ctl_prepare(RefineCtl *s)
 
 __device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2, long long nmoves, long long ncand);
 
+// The level's starting cut: the coarser level's best cut when there is one (a
+// projection keeps the cut exactly: every coarse edge weight is the sum of
+// the fine edges between its two clusters, and edges inside a cluster are
+// never cut), else the cut summed from the gain rows (rowcut_kernel).
 __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned,
-                                const int32_t *gain_total)
+                                const int32_t *gain_total, const RefineCtl *coarser)
 {
     s->gain_entries = *gain_total;
-    s->cut = (long long)sc[S_CUT2] / 2;
+    s->cut = coarser ? coarser->best_cut : (long long)sc[S_CUT2] / 2;
     s->excess = (long long)sc[S_EXCESS];
     s->cut_start = s->cut;
     s->best_cut = s->cut;
@@ -2612,7 +2616,8 @@ struct LevelLaunches {
 };
 
 int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_t *d_opt,
-                 const int64_t *d_maxp, const LevelStat &ls, RefineCtl *ctl, LevelLaunches *ll, GraphKeep *keep)
+                 const int64_t *d_maxp, const LevelStat &ls, RefineCtl *ctl, const RefineCtl *coarser,
+                 LevelLaunches *ll, GraphKeep *keep)
 {
     const int32_t n = g.n;
     if (n == 0) return HP_OK;
@@ -2669,7 +2674,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     HP_CUDA(cudaMemsetAsync(B.dirty, 0, sizeof(int32_t) * (size_t)n, c->stream));
     HP_LAUNCH(c, pw_kernel, (unsigned)std::min<int64_t>(nblk(n), c->sm_count * 8), 256,
               k <= 2048 ? sizeof(unsigned long long) * k : 0, n, g.where, g.vwgt, B.pw, k);
-    HP_LAUNCH(c, rowcut_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, &sc[S_CUT2]);
+    if (!coarser)   // the coarsest level; the others start from the coarser level's best cut
+        HP_LAUNCH(c, rowcut_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, &sc[S_CUT2]);
     HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);
     HP_CUDA(cudaMemcpyAsync(B.best_where, g.where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
     HP_CUDA(cudaMemcpyAsync(best_pw, B.pw, sizeof(unsigned long long) * k, cudaMemcpyDeviceToDevice, c->stream));
@@ -2680,7 +2686,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
     const int patience = c->opt.refine_patience;
     HP_LAUNCH(c, ctl_init_kernel, 1, 1, 0, ctl, (const unsigned long long *)sc, patience, learned ? 1 : 0,
-              (const int32_t *)(B.goff + n));
+              (const int32_t *)(B.goff + n), coarser);
     int64_t log_r0 = 0;
     if (recording) {
         unsigned long long lc = 0;
@@ -2841,7 +2847,8 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
             HP_CHECK_OOM(c);
             HP_CUDA(cudaMemcpyAsync(g.where_start, g.where, sizeof(int32_t) * g.n, cudaMemcpyDeviceToDevice, c->stream));
         }
-        HP_TRY(refine_level(c, g, nparts, l == 0, d_opt, d_maxp, ls[l], d_ctl + l, &ll[l], &keep));
+        HP_TRY(refine_level(c, g, nparts, l == 0, d_opt, d_maxp, ls[l], d_ctl + l,
+                            l < L && c->levels[l + 1].n > 0 ? d_ctl + l + 1 : nullptr, &ll[l], &keep));
         if (dbg_levels) {
             HP_CUDA(cudaEventRecord(lev[2 * l + 1], c->stream));
             host_ms[l] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

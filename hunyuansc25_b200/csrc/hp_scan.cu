@@ -104,34 +104,27 @@ __global__ void scatter_flags_kernel(const int32_t *flags, const int32_t *pos, i
     if (blockIdx.x == 0 && threadIdx.x == 0) *d_count = pos[n];
 }
 
-// Edge-parallel over the adjacency array in tiles of 256 x 32 entries
-// (coalesced reads of adjncy/adjwgt); each thread finds the owner of its first
-// entry by binary search over xadj and walks forward 256 entries at a time.
-// int64 block partial sums of 2 x cut.
-constexpr int CUT_ITEMS = 32;
-__global__ void __launch_bounds__(256)
-edgecut_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
-               const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
-               unsigned long long *cut2)
+// Exact cut, edge-parallel over the adjacency in tiles of CUT_THREADS x
+// CUT_ITEMS entries (coalesced reads of adjncy and adjwgt; hub rows cost their
+// share of the array): each entry's row comes from hp::tile_owners.  int64
+// block partial sums of 2 x cut.
+constexpr int CUT_THREADS = 256, CUT_ITEMS = 16, CUT_TILE = CUT_THREADS * CUT_ITEMS;
+__global__ void __launch_bounds__(CUT_THREADS)
+edgecut_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
+               const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where, unsigned long long *cut2)
 {
-    const int64_t m = xadj[n];
-    const int64_t tile = 256 * CUT_ITEMS;
+    __shared__ int32_t owner[CUT_TILE];
+    __shared__ int32_t s_warp[CUT_THREADS / 32];
+    __shared__ int32_t s_v0;
     long long acc = 0;
-    for (int64_t tb = blockIdx.x * tile; tb < m; tb += (int64_t)gridDim.x * tile) {
-        int64_t j = tb + threadIdx.x;
-        if (j >= m) continue;
-        int32_t lo = 0, hi = n - 1;
-        while (lo < hi) {
-            int32_t mid = (int32_t)(((int64_t)lo + hi + 1) / 2);
-            if (xadj[mid] <= j) lo = mid; else hi = mid - 1;
-        }
-        int32_t v = lo;
-        for (int k = 0; k < CUT_ITEMS && j < m; k++, j += 256) {
-            while (xadj[v + 1] <= j) v++;
-            if (where[adjncy[j]] != where[v]) acc += adjwgt[j];
-        }
+    for (int64_t tb = (int64_t)blockIdx.x * CUT_TILE; tb < m; tb += (int64_t)gridDim.x * CUT_TILE) {
+        const int64_t te = tb + CUT_TILE < m ? tb + CUT_TILE : m;
+        hp::tile_owners<CUT_THREADS, CUT_ITEMS>(xadj, n, tb, te, owner, s_warp, &s_v0);
+        for (int64_t j = tb + threadIdx.x; j < te; j += CUT_THREADS)
+            if (where[adjncy[j]] != where[owner[j - tb]]) acc += adjwgt ? adjwgt[j] : 1;
+        __syncthreads();   // owner[] is rebuilt for the next tile
     }
-    hp::block_add_to<256>(acc, cut2);
+    hp::block_add_to<CUT_THREADS>(acc, cut2);
 }
 
 inline unsigned grid_for(hp_context *c, int64_t n, int block)
@@ -243,16 +236,21 @@ int hp_compact_flags(hp_context *c, const int32_t *flags, int64_t n, int32_t *ou
     return HP_OK;
 }
 
-int hp_edgecut_launch(hp_context *c, int32_t n, const int32_t *xadj, const int32_t *adjncy,
+int hp_edgecut_launch(hp_context *c, int32_t n, int64_t m, const int32_t *xadj, const int32_t *adjncy,
                       const int32_t *adjwgt, const int32_t *where, unsigned long long *d_cut2)
 {
     if (n <= 0) return HP_OK;
-    int32_t m = 0;
-    HP_CUDA(cudaMemcpyAsync(c->h_pin, xadj + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-    HP_CUDA(cudaStreamSynchronize(c->stream));
-    memcpy(&m, c->h_pin, sizeof(int32_t));
-    HP_LAUNCH(c, edgecut_kernel, grid_for(c, ((int64_t)m + CUT_ITEMS - 1) / CUT_ITEMS, 256), 256, 0, n, xadj,
-              adjncy, adjwgt, where, d_cut2);
+    if (m < 0) {   // not known to the caller: read xadj[n]
+        int32_t mm = 0;
+        HP_CUDA(cudaMemcpyAsync(c->h_pin, xadj + n, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        HP_CUDA(cudaStreamSynchronize(c->stream));
+        memcpy(&mm, c->h_pin, sizeof(int32_t));
+        m = mm;
+    }
+    if (m <= 0) return HP_OK;
+    const int64_t tiles = (m + CUT_TILE - 1) / CUT_TILE;
+    HP_LAUNCH(c, edgecut_kernel, (unsigned)std::min<int64_t>(tiles, (int64_t)c->sm_count * 8), CUT_THREADS, 0, n, m,
+              xadj, adjncy, adjwgt, where, d_cut2);
     return HP_OK;
 }
 

@@ -60,6 +60,7 @@ SPACE = {
     "trial_cta_n": [128, 256, 512, 1024, 4096, 1 << 24],
     "contract_smem_cn": [0, 8192, 16384, 32768, 49152],
     "small_match_n": [0, 1024, 2048, 4096, 8192],
+    "contract_hybrid": [0, 1],
 }
 
 

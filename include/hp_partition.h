@@ -184,7 +184,12 @@ typedef struct hp_tuning {
     int32_t small_match_n;       /* coarsening: levels of at most this many vertices (and
                                     64x as many adjacency entries) are matched by one
                                     CTA; 0 = never                               [0, 8192]     8192 */
-    int32_t reserved[8];         /* zero */
+    int32_t contract_hybrid;     /* contraction: on levels with more coarse vertices than
+                                    contract_smem_cn and at most 131072, rows longer than
+                                    contract_warp_row accumulate their ids below 32768 in
+                                    a shared-memory dense accumulator and radix-sort the
+                                    rest (1), or radix-sort every entry (0)      [0, 1]        1 */
+    int32_t reserved[7];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);

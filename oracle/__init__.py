@@ -51,7 +51,7 @@ def lib():
         L.ora_partition.argtypes = [C.c_int32, I32P, I32P, I32P, I32P, C.c_int32, C.POINTER(C.c_float),
                                     C.c_float, C.POINTER(HpOptions), I32P, I64P, C.POINTER(C.c_void_p)]
         L.ora_partition.restype = C.c_int
-        L.ora_weight_range_ok.argtypes = [C.c_int32, I32P, I32P, I32P]
+        L.ora_weight_range_ok.argtypes = [C.c_int32, I32P, I32P]
         L.ora_weight_range_ok.restype = C.c_int
         L.ora_trace_nlevels.argtypes = [C.c_void_p]
         L.ora_trace_level.argtypes = [C.c_void_p, C.c_int, I32P, I64P, I64P, I64P]
@@ -165,11 +165,9 @@ def partition(g, nparts, ubfactor=1.03, tpwgts=None, opt: HpOptions | None = Non
     return part[:g.nvtxs], cut.value, (Trace(th.value) if trace else None)
 
 
-def weight_range_ok(g, match_=None) -> bool:
-    """The weight-range rule: every matched pair's (match_ None: every
-    vertex's) weighted degrees sum below 2^31."""
-    return bool(lib().ora_weight_range_ok(g.nvtxs, _p(i32(g.xadj)), _p(i32(g.adjwgt)),
-                                          None if match_ is None else _p(i32(match_))))
+def weight_range_ok(g) -> bool:
+    """The weight-range rule: every vertex's weighted degree is below 2^31."""
+    return bool(lib().ora_weight_range_ok(g.nvtxs, _p(i32(g.xadj)), _p(i32(g.adjwgt))))
 
 
 def match(g, level, seed, maxvwgt, rounds):

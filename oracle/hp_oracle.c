@@ -253,23 +253,18 @@ static void sort_kw(kw_t *r, int64_t len)
     }
 }
 
-/* Weight range of a contraction (the library's pair_weight_bound_kernel,
- * checked when the input's total edge weight reaches 2^31): every coarse edge
- * weight and connectivity is at most the sum of its pair's fine weighted
- * degrees, so the contraction is accepted when every pair's sum stays below
- * 2^31.  match = NULL checks every vertex alone (the input level).  Returns 1
- * when the range holds. */
-int ora_weight_range_ok(int32_t n, const int32_t *xadj, const int32_t *adjwgt, const int32_t *match)
+/* Weight range (the library's rule, checked when the input's total edge
+ * weight reaches 2^31): every coarse edge weight and every connectivity of a
+ * vertex is at most the vertex's weighted degree, so the int32 weights cannot
+ * wrap while every vertex of every level has a weighted degree below 2^31.
+ * Returns 1 when every row of the graph sums below 2^31. */
+int ora_weight_range_ok(int32_t n, const int32_t *xadj, const int32_t *adjwgt)
 {
     int ok = 1;
 #pragma omp parallel for schedule(dynamic, 4096) reduction(&& : ok)
     for (int32_t v = 0; v < n; v++) {
-        const int32_t u = match ? match[v] : v;
-        if (u < v) continue;
         int64_t s = 0;
         for (int32_t j = xadj[v]; j < xadj[v + 1]; j++) s += adjwgt[j];
-        if (u != v)
-            for (int32_t j = xadj[u]; j < xadj[u + 1]; j++) s += adjwgt[j];
         ok = ok && s < (int64_t)INT32_MAX;
     }
     return ok;
@@ -330,7 +325,9 @@ int64_t ora_contract(int32_t n, const int32_t *xadj, const int32_t *adjncy,
         const kw_t *r = tmp + toff[c];
         for (int32_t j = 0; j < ucnt[c]; j++) {
             cadj[cxadj[c] + j] = r[j].k;
-            cwgt[cxadj[c] + j] = (int32_t)r[j].w;
+            /* saturated: a merged weight beyond int32 makes its row fail the
+             * weight-range check, as the row's sum is at least as large */
+            cwgt[cxadj[c] + j] = r[j].w > INT32_MAX ? INT32_MAX : (int32_t)r[j].w;
         }
     }
     free(leader); free(toff); free(tmp); free(ucnt);
@@ -1225,7 +1222,7 @@ int ora_partition(int32_t n, const int32_t *xadj, const int32_t *adjncy,
     int64_t tw = 0;
     for (int64_t j = 0; j < m0; j++) tw += ew[j];
     const int weight_check = tw >= (int64_t)INT32_MAX;
-    if (weight_check && !ora_weight_range_ok(n, xadj, ew, NULL)) {
+    if (weight_check && !ora_weight_range_ok(n, xadj, ew)) {
         free(vw); free(ew);
         return HP_ERR_UNSUPPORTED;
     }
@@ -1251,8 +1248,14 @@ int ora_partition(int32_t n, const int32_t *xadj, const int32_t *adjncy,
             memset(lv + L + 1, 0, sizeof(olevel) * (size_t)(cap - L - 1));
             f = &lv[L];
         }
-        if (weight_check && !ora_weight_range_ok(f->n, f->xadj, f->adjwgt, f->match)) {
-            /* a coarse weight could exceed int32: the call fails as the library's does */
+        olevel *c = &lv[L + 1];
+        c->n = cn;
+        c->m = ora_contract(f->n, f->xadj, f->adjncy, f->vwgt, f->adjwgt, f->match, f->cmap, cn,
+                            &c->xadj, &c->adjncy, &c->adjwgt, &c->vwgt);
+        c->owns_graph = 1;
+        L++;
+        if (weight_check && !ora_weight_range_ok(c->n, c->xadj, c->adjwgt)) {
+            /* a coarse vertex's weighted degree reaches 2^31: the call fails as the library's does */
             for (int32_t l = 0; l <= L; l++) {
                 olevel *g = &lv[l];
                 if (g->owns_graph) { free(g->xadj); free(g->adjncy); free(g->adjwgt); free(g->vwgt); }
@@ -1261,12 +1264,6 @@ int ora_partition(int32_t n, const int32_t *xadj, const int32_t *adjncy,
             free(lv); free(vw); free(ew);
             return HP_ERR_UNSUPPORTED;
         }
-        olevel *c = &lv[L + 1];
-        c->n = cn;
-        c->m = ora_contract(f->n, f->xadj, f->adjncy, f->vwgt, f->adjwgt, f->match, f->cmap, cn,
-                            &c->xadj, &c->adjncy, &c->adjwgt, &c->vwgt);
-        c->owns_graph = 1;
-        L++;
         if (!(100 * (int64_t)c->n < 85 * (int64_t)f->n && c->m > c->n / 2)) break;
     }
 

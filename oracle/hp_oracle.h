@@ -42,9 +42,9 @@ int  ora_trace_copy(const ora_trace *t, int level, int what, int32_t *dst, int64
 void ora_trace_free(ora_trace *t);
 
 /* ---- components (each follows the same rule as the CUDA path) ------------- */
-/* 1 when every matched pair's (match = NULL: every vertex's) weighted
- * degrees sum below 2^31 (the library's weight-range rule). */
-int ora_weight_range_ok(int32_t n, const int32_t *xadj, const int32_t *adjwgt, const int32_t *match);
+/* 1 when every vertex's weighted degree is below 2^31 (the library's
+ * weight-range rule, applied to the input and to every coarse level). */
+int ora_weight_range_ok(int32_t n, const int32_t *xadj, const int32_t *adjwgt);
 int64_t ora_edgecut(int32_t n, const int32_t *xadj, const int32_t *adjncy,
                     const int32_t *adjwgt, const int32_t *where);
 

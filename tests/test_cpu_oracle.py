@@ -239,21 +239,29 @@ def test_oracle_edge_cases():
 
 def test_weight_range_rule():
     """The weight-range rule shared with the library: when the total edge
-    weight reaches 2^31, a matched pair whose weighted degrees sum to 2^31 or
-    more fails the call (HP_ERR_UNSUPPORTED), since the int32 coarse weights
-    could wrap; below that the partition is the ordinary one."""
+    weight reaches 2^31, a vertex of any level whose weighted degree reaches
+    2^31 fails the call (HP_ERR_UNSUPPORTED), since the int32 coarse weights
+    and connectivities could wrap; below that the partition is the ordinary
+    one."""
     from hunyuansc25_b200._abi import HP_ERR_UNSUPPORTED
-    n = 4096
-    xadj = np.zeros(n + 1, np.int32)
-    xadj[1:] = np.cumsum([1 if v in (0, n - 1) else 2 for v in range(n)])
-    adj = np.array([u for v in range(n) for u in (v - 1, v + 1) if 0 <= u < n], np.int32)
-    path = G(xadj, adj, np.ones(n, np.int32), np.full(adj.size, 1 << 29, np.int32))
-    assert oracle.weight_range_ok(path)                            # every vertex alone: 2^30
-    match = np.arange(n, dtype=np.int32) ^ 1                       # pairs (0,1), (2,3), ...
-    assert not oracle.weight_range_ok(path, match)                 # a pair: 2^31
+    # a star: the centre's weighted degree is 8 * 2^29 = 2^32 on the input level
+    n = 9
+    xadj = np.array([0, 8] + list(range(9, 17)), np.int32)
+    adj = np.array(list(range(1, 9)) + [0] * 8, np.int32)
+    star = G(xadj, adj, np.ones(n, np.int32), np.full(16, 1 << 29, np.int32))
+    assert not oracle.weight_range_ok(star)
     with pytest.raises(oracle.OracleError) as e:
-        oracle.partition(path, 2, 1.03)
+        oracle.partition(star, 2, 1.03)
     assert e.value.code == HP_ERR_UNSUPPORTED
-    light = G(xadj, adj, np.ones(n, np.int32), np.full(adj.size, 1 << 20, np.int32))
-    part, cut, _ = oracle.partition(light, 2, 1.03)
+    # a 2-D grid of weight 2^26: the input fits (4 * 2^26), coarse vertices with
+    # a perimeter of 32 fine edges or more do not
+    g = graphs.grid2d(256, 256)
+    heavy = G(g.xadj, g.adjncy, g.vwgt, np.full(g.nedges, 1 << 26, np.int32))
+    assert oracle.weight_range_ok(heavy)
+    with pytest.raises(oracle.OracleError) as e:
+        oracle.partition(heavy, 8, 1.03)
+    assert e.value.code == HP_ERR_UNSUPPORTED
+    # weight 2^21: total about 5.5e11, every coarse vertex below 2^31
+    light = G(g.xadj, g.adjncy, g.vwgt, np.full(g.nedges, 1 << 21, np.int32))
+    part, cut, _ = oracle.partition(light, 8, 1.03)
     assert cut == oracle.edgecut(light, part)

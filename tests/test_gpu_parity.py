@@ -319,35 +319,32 @@ def test_invalid_asymmetric_and_duplicate(ctx):
 
 
 def test_weight_range(ctx):
-    """Edge weights whose sums could wrap the int32 coarse weights: a matched
-    pair whose weighted degrees reach 2^31 fails with HP_ERR_UNSUPPORTED, as in
-    the oracle; a graph whose total weight exceeds 2^31 but whose pairs stay
-    below it partitions exactly as the oracle does."""
-    n = 4096
-    rows = [[v - 1] if v == n - 1 else ([v + 1] if v == 0 else [v - 1, v + 1]) for v in range(n)]
-    xadj, adj, _ = _csr(n, rows)
-    path = graphs.Graph(xadj, adj, np.ones(n, np.int32), np.full(adj.size, 1 << 29, np.int32))
+    """Edge weights whose sums could wrap the int32 coarse weights and
+    connectivities: a vertex of any level with a weighted degree of 2^31 or
+    more fails with HP_ERR_UNSUPPORTED, as in the oracle (on the input level,
+    a star; on a coarse level, a heavy grid); a graph whose total weight
+    exceeds 2^31 but whose vertices stay below it partitions exactly as the
+    oracle does."""
+    n = 9
+    xadj = np.array([0, 8] + list(range(9, 17)), np.int32)
+    adj = np.array(list(range(1, 9)) + [0] * 8, np.int32)
+    star = graphs.Graph(xadj, adj, np.ones(n, np.int32), np.full(16, 1 << 29, np.int32))
     with pytest.raises(hp.HpError) as e:
-        ctx.partition_graph(path, 2)
+        ctx.partition_graph(star, 2)
     assert e.value.code == HP_ERR_UNSUPPORTED
-    with pytest.raises(oracle.OracleError) as oe:
-        oracle.partition(path, 2, 1.03)
-    assert oe.value.code == HP_ERR_UNSUPPORTED
-    # grid weights 2^21: total about 5.5e11, every pair far below 2^31
     g = graphs.grid2d(256, 256)
-    heavy = graphs.Graph(g.xadj, g.adjncy, g.vwgt, np.full(g.nedges, 1 << 21, np.int32))
-    compare_runs(ctx, heavy, 8)
-    # grid weights 2^26: level 0 fits, a coarser level's pairs reach 2^31
-    heavier = graphs.Graph(g.xadj, g.adjncy, g.vwgt, np.full(g.nedges, 1 << 26, np.int32))
+    heavy = graphs.Graph(g.xadj, g.adjncy, g.vwgt, np.full(g.nedges, 1 << 26, np.int32))
     with pytest.raises(hp.HpError) as e:
-        ctx.partition_graph(heavier, 8)
+        ctx.partition_graph(heavy, 8)
     assert e.value.code == HP_ERR_UNSUPPORTED
     with pytest.raises(oracle.OracleError) as oe:
-        oracle.partition(heavier, 8, 1.03)
+        oracle.partition(heavy, 8, 1.03)
     assert oe.value.code == HP_ERR_UNSUPPORTED
+    # weight 2^21: total about 5.5e11, every vertex of every level below 2^31
+    light = graphs.Graph(g.xadj, g.adjncy, g.vwgt, np.full(g.nedges, 1 << 21, np.int32))
+    compare_runs(ctx, light, 8)
     part, cut = ctx.partition_graph(g, 4)
     assert cut == oracle.edgecut(g, part)
-
 
 def test_legacy_entry_point(ctx):
     g = graphs.grid2d(40, 30, seed=3, wmin=1, wmax=9)
@@ -379,3 +376,47 @@ def test_partition_device_torch(ctx):
     assert cut == ref_cut
     assert np.array_equal(part.cpu().numpy(), ref_part)
     assert ctx.edgecut_device(t[0], t[1], t[3], part) == ref_cut
+
+
+def hybrid_test_graph():
+    """R-MAT scale 17 plus two hubs joined to 11,000 and 20,000 vertices with
+    high ids: on level 0 (about 70K coarse ids) the long rows have entries on
+    both sides of the hybrid contraction's dense range (ids below 32768), and
+    the hubs' rows have more high ids than its 4096-entry buffer, so they spill
+    to the CTA radix kernel (up to 12288 entries) and to the dense slab kernel
+    (longer)."""
+    g = graphs.rmat(17, 16, seed=11, wmin=1, wmax=100)
+    n = g.nvtxs
+    rng = np.random.default_rng(5)
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(g.xadj))
+    dst = g.adjncy.astype(np.int64)
+    extra = []
+    for hub, cnt in ((3, 11000), (5, 20000)):
+        nb = rng.choice(np.arange(n // 2, n), size=cnt, replace=False)
+        extra.append((np.full(cnt, hub), nb))
+    es = np.concatenate([src] + [a for a, b in extra] + [b for a, b in extra])
+    ed = np.concatenate([dst] + [b for a, b in extra] + [a for a, b in extra])
+    key = np.unique(es * n + ed)                      # sorted, duplicates dropped
+    s, d = key // n, key % n
+    keep = s != d
+    s, d = s[keep], d[keep]
+    xadj = np.zeros(n + 1, np.int64)
+    np.add.at(xadj, s + 1, 1)
+    xadj = np.cumsum(xadj).astype(np.int32)
+    lo, hi = np.minimum(s, d).astype(np.uint64), np.maximum(s, d).astype(np.uint64)
+    w = ((lo * np.uint64(2654435761) + hi * np.uint64(40503)) % np.uint64(100) + np.uint64(1)).astype(np.int32)
+    return graphs.Graph(xadj, d.astype(np.int32), np.ones(n, np.int32), w)
+
+
+@pytest.mark.parametrize("hybrid", [1, 0])
+def test_hybrid_contraction(ctx, hybrid):
+    """The hybrid long-row contraction (dense shared-memory accumulation of the
+    low coarse ids, radix sort of the rest, spills of rows whose rest does not
+    fit) writes the same coarse rows as the radix path: every level equal to
+    the oracle, with both settings, every level off the 48K shared-memory path."""
+    g = hybrid_test_graph()
+    ctx.set_tuning(contract_smem_cn=0, contract_hybrid=hybrid)
+    try:
+        compare_runs(ctx, g, 64)
+    finally:
+        ctx.set_tuning(None)
