@@ -742,6 +742,7 @@ HP_API void hp_context_destroy(hp_context *c)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (auto e : c->prof_events) cudaEventDestroy(e);
     if (c->mlp_params) cudaFree(c->mlp_params);
+    if (c->mlp_scratch) cudaFree(c->mlp_scratch);
     if (c->log_x) cudaFree(c->log_x);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;

@@ -65,6 +65,7 @@ struct hp_context {
 
     // move-scoring MLP (hp_mlp.cu): params, gradient, Adam moments
     float *mlp_params = nullptr, *mlp_grad = nullptr, *mlp_m = nullptr, *mlp_v = nullptr;
+    float *mlp_scratch = nullptr;   // per-sample gradient rows of a training chunk
     float mlp_threshold = 0.0f;
     bool mlp_ready = false;
     // move log recorded by the plain refiner (opt.learned = 2)

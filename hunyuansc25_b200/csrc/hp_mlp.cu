@@ -3,7 +3,7 @@
 //
 // No counterpart in the reference (its refinement has no learned component).
 // Training is plain FP32 on CUDA cores (mini-batch Adam; the network has 1,377
-// parameters), inference inside refinement is BF16 tensor-core MMA with FP32
+// parameters; gradients summed in a fixed order, so training is reproducible), inference inside refinement is BF16 tensor-core MMA with FP32
 // accumulation (hp_mlp.cuh).  The network only proposes: an LP candidate it
 // scores below the threshold is dropped before the exact integer afterburner,
 // and every accepted move is still checked and applied in integers.
@@ -35,55 +35,91 @@ __device__ __forceinline__ float mlp_fwd(const float *__restrict__ P, const floa
     return y;
 }
 
-// Mean binary cross-entropy (with logits) and its gradient over samples
-// [b0, b0+nb) of the (possibly permuted) index list.  Per-thread gradients
-// are reduced in shared memory and added to g[] once per block.
+// Gradient of the mean binary cross-entropy (with logits), deterministic: no
+// float atomics, so the same samples and parameters give the same gradient bit
+// for bit on every run.  Two kernels per chunk of at most MLP_CHUNK samples:
+//   mlp_sample_grad_kernel  one thread per sample writes that sample's scaled
+//                           gradient (HP_MLP_NPARAM values) and loss term
+//                           parameter-major into G[(p) * nb + s] (coalesced:
+//                           consecutive threads, consecutive samples);
+//   mlp_reduce_kernel       one block per parameter (and one for the loss) sums
+//                           its row in a fixed order -- strided per thread, then
+//                           a fixed shuffle tree -- and adds it to g[p].
+// Chunks are reduced one after another, so the order of every sum is fixed.
+constexpr int64_t MLP_CHUNK = 8192;
+constexpr int MLP_RED = 256;
+constexpr int MLP_ROWS = HP_MLP_NPARAM + 1;   // the parameters, then the loss
+
 __global__ void __launch_bounds__(MLP_BLOCK)
-mlp_grad_kernel(const float *__restrict__ P, const float *__restrict__ X, const float *__restrict__ Y,
-                const int32_t *__restrict__ idx, int64_t b0, int64_t nb, float scale, float *__restrict__ g,
-                float *__restrict__ loss)
+mlp_sample_grad_kernel(const float *__restrict__ P, const float *__restrict__ X, const float *__restrict__ Y,
+                       const int32_t *__restrict__ idx, int64_t b0, int64_t nb, float scale,
+                       float *__restrict__ G)
 {
-    __shared__ float sg[HP_MLP_NPARAM];
-    __shared__ float sl;
-    for (int i = threadIdx.x; i < HP_MLP_NPARAM; i += blockDim.x) sg[i] = 0.f;
-    if (threadIdx.x == 0) sl = 0.f;
-    __syncthreads();
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < nb; s += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t r = idx ? idx[b0 + s] : b0 + s;
-        float x[HP_MLP_IN], z1[HP_MLP_H], z2[HP_MLP_H];
-        for (int i = 0; i < HP_MLP_IN; i++) x[i] = X[r * HP_MLP_IN + i];
-        const float y = mlp_fwd(P, x, z1, z2);
-        const float t = Y[r];
-        // loss = softplus(y) - t*y ; dL/dy = sigmoid(y) - t
-        const float sp = y > 0 ? y + log1pf(__expf(-y)) : log1pf(__expf(y));
-        atomicAdd(&sl, (sp - t * y) * scale);
-        const float dy = (1.f / (1.f + __expf(-y)) - t) * scale;
-        atomicAdd(&sg[HP_MLP_OFF_B3], dy);
-        float da1[HP_MLP_H];
-        for (int i = 0; i < HP_MLP_H; i++) da1[i] = 0.f;
-        for (int j = 0; j < HP_MLP_H; j++) {
-            const float a2 = fmaxf(z2[j], 0.f);
-            atomicAdd(&sg[HP_MLP_OFF_W3 + j], dy * a2);
-            const float dz2 = z2[j] > 0.f ? dy * P[HP_MLP_OFF_W3 + j] : 0.f;
-            if (dz2 != 0.f) {
-                atomicAdd(&sg[HP_MLP_OFF_B2 + j], dz2);
-                for (int i = 0; i < HP_MLP_H; i++) {
-                    atomicAdd(&sg[HP_MLP_OFF_W2 + j * HP_MLP_H + i], dz2 * fmaxf(z1[i], 0.f));
-                    da1[i] += dz2 * P[HP_MLP_OFF_W2 + j * HP_MLP_H + i];
-                }
-            }
-        }
+    const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (s >= nb) return;
+    const int64_t r = idx ? idx[b0 + s] : b0 + s;
+    float x[HP_MLP_IN], z1[HP_MLP_H], z2[HP_MLP_H];
+    for (int i = 0; i < HP_MLP_IN; i++) x[i] = X[r * HP_MLP_IN + i];
+    const float y = mlp_fwd(P, x, z1, z2);
+    const float t = Y[r];
+    // loss = softplus(y) - t*y ; dL/dy = sigmoid(y) - t
+    const float sp = y > 0 ? y + log1pf(__expf(-y)) : log1pf(__expf(y));
+    G[(int64_t)HP_MLP_NPARAM * nb + s] = (sp - t * y) * scale;
+    const float dy = (1.f / (1.f + __expf(-y)) - t) * scale;
+    G[(int64_t)HP_MLP_OFF_B3 * nb + s] = dy;
+    float da1[HP_MLP_H];
+    for (int i = 0; i < HP_MLP_H; i++) da1[i] = 0.f;
+    for (int j = 0; j < HP_MLP_H; j++) {
+        G[(int64_t)(HP_MLP_OFF_W3 + j) * nb + s] = dy * fmaxf(z2[j], 0.f);
+        const float dz2 = z2[j] > 0.f ? dy * P[HP_MLP_OFF_W3 + j] : 0.f;
+        G[(int64_t)(HP_MLP_OFF_B2 + j) * nb + s] = dz2;
         for (int i = 0; i < HP_MLP_H; i++) {
-            const float dz1 = z1[i] > 0.f ? da1[i] : 0.f;
-            if (dz1 == 0.f) continue;
-            atomicAdd(&sg[HP_MLP_OFF_B1 + i], dz1);
-            for (int c = 0; c < HP_MLP_IN; c++) atomicAdd(&sg[HP_MLP_OFF_W1 + i * HP_MLP_IN + c], dz1 * x[c]);
+            G[(int64_t)(HP_MLP_OFF_W2 + j * HP_MLP_H + i) * nb + s] = dz2 * fmaxf(z1[i], 0.f);
+            da1[i] += dz2 * P[HP_MLP_OFF_W2 + j * HP_MLP_H + i];
         }
     }
+    for (int i = 0; i < HP_MLP_H; i++) {
+        const float dz1 = z1[i] > 0.f ? da1[i] : 0.f;
+        G[(int64_t)(HP_MLP_OFF_B1 + i) * nb + s] = dz1;
+        for (int c = 0; c < HP_MLP_IN; c++) G[(int64_t)(HP_MLP_OFF_W1 + i * HP_MLP_IN + c) * nb + s] = dz1 * x[c];
+    }
+}
+
+// Row p of G (nb samples) summed in a fixed order and added to out[p] (p <
+// HP_MLP_NPARAM) or to *loss (p = HP_MLP_NPARAM, when loss is set).
+__global__ void __launch_bounds__(MLP_RED)
+mlp_reduce_kernel(const float *__restrict__ G, int64_t nb, float *__restrict__ out, float *__restrict__ loss)
+{
+    __shared__ float sw[MLP_RED / 32];
+    const int p = blockIdx.x;
+    const float *row = G + (int64_t)p * nb;
+    float acc = 0.f;
+    for (int64_t s = threadIdx.x; s < nb; s += MLP_RED) acc += row[s];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(HP_FULL_MASK, acc, o);
+    if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = acc;
     __syncthreads();
-    for (int i = threadIdx.x; i < HP_MLP_NPARAM; i += blockDim.x)
-        if (sg[i] != 0.f) atomicAdd(&g[i], sg[i]);
-    if (threadIdx.x == 0 && loss) atomicAdd(loss, sl);
+    if (threadIdx.x == 0) {
+        float t = 0.f;
+        for (int w = 0; w < MLP_RED / 32; w++) t += sw[w];
+        if (p < HP_MLP_NPARAM) out[p] += t;
+        else if (loss) *loss += t;
+    }
+}
+
+// Gradient (and loss) of samples [b0, b0 + nb) of the index list, scaled by
+// `scale`, added to g (and *loss) in a fixed order; G: MLP_ROWS * MLP_CHUNK floats.
+int mlp_grad_det(cudaStream_t st, const float *P, const float *X, const float *Y, const int32_t *idx, int64_t b0,
+                 int64_t nb, float scale, float *G, float *g, float *loss)
+{
+    for (int64_t c0 = 0; c0 < nb; c0 += MLP_CHUNK) {
+        const int64_t cn = std::min<int64_t>(MLP_CHUNK, nb - c0);
+        mlp_sample_grad_kernel<<<(unsigned)((cn + MLP_BLOCK - 1) / MLP_BLOCK), MLP_BLOCK, 0, st>>>(
+            P, X, Y, idx, b0 + c0, cn, scale, G);
+        mlp_reduce_kernel<<<loss ? MLP_ROWS : HP_MLP_NPARAM, MLP_RED, 0, st>>>(G, cn, g, loss);
+        HP_CUDA(cudaGetLastError());
+    }
+    return HP_OK;
 }
 
 __global__ void adam_kernel(float *__restrict__ P, const float *__restrict__ g, float *__restrict__ m,
@@ -140,6 +176,20 @@ int hp_mlp_ensure(hp_context *c)
     return HP_OK;
 }
 
+// Per-sample gradient rows of one chunk (MLP_ROWS x MLP_CHUNK floats, 45 MB),
+// allocated on the first training or gradient call of a context.
+int hp_mlp_ensure_scratch(hp_context *c)
+{
+    if (c->mlp_scratch) return HP_OK;
+    void *p = nullptr;
+    if (cudaMalloc(&p, sizeof(float) * (size_t)MLP_ROWS * MLP_CHUNK) != cudaSuccess) {
+        cudaGetLastError();
+        return HP_ERR_NOMEM;
+    }
+    c->mlp_scratch = (float *)p;
+    return HP_OK;
+}
+
 #define HP_API extern "C" __attribute__((visibility("default")))
 
 HP_API int hp_mlp_set_params(hp_context *c, const float *params, int32_t count, float threshold)
@@ -168,12 +218,11 @@ HP_API int hp_mlp_loss_grad(hp_context *c, const float *d_x, const float *d_y, i
     if (!c || !d_x || !d_y || n <= 0 || !grad || !c->mlp_params) return HP_ERR_INVALID_ARG;
     HP_CUDA(cudaSetDevice(c->device));
     cudaStream_t s = c->own_stream;
+    HP_TRY(hp_mlp_ensure_scratch(c));
     HP_CUDA(cudaMemsetAsync(c->mlp_grad, 0, sizeof(float) * HP_MLP_NPARAM, s));
     HP_CUDA(cudaMemsetAsync(c->d_scal, 0, sizeof(float), s));
-    const unsigned grid = (unsigned)std::min<int64_t>((n + MLP_BLOCK - 1) / MLP_BLOCK, c->sm_count * 4);
-    mlp_grad_kernel<<<grid, MLP_BLOCK, 0, s>>>(c->mlp_params, d_x, d_y, nullptr, 0, n, 1.0f / (float)n,
-                                               c->mlp_grad, (float *)c->d_scal);
-    HP_CUDA(cudaGetLastError());
+    HP_TRY(mlp_grad_det(s, c->mlp_params, d_x, d_y, nullptr, 0, n, 1.0f / (float)n, c->mlp_scratch, c->mlp_grad,
+                        (float *)c->d_scal));
     HP_CUDA(cudaMemcpyAsync(grad, c->mlp_grad, sizeof(float) * HP_MLP_NPARAM, cudaMemcpyDeviceToHost, s));
     float l = 0;
     HP_CUDA(cudaMemcpyAsync(&l, c->d_scal, sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -188,6 +237,7 @@ HP_API int hp_mlp_train(hp_context *c, const float *d_x, const float *d_y, const
     if (!c || !d_x || !d_y || n <= 0 || epochs <= 0 || batch <= 0 || !c->mlp_params) return HP_ERR_INVALID_ARG;
     HP_CUDA(cudaSetDevice(c->device));
     cudaStream_t s = c->own_stream;
+    HP_TRY(hp_mlp_ensure_scratch(c));
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     float p1 = 1.f, p2 = 1.f;
     for (int e = 0; e < epochs; e++) {
@@ -196,10 +246,8 @@ HP_API int hp_mlp_train(hp_context *c, const float *d_x, const float *d_y, const
         for (int64_t b0 = 0; b0 < n; b0 += batch) {
             const int64_t nb = std::min<int64_t>(batch, n - b0);
             HP_CUDA(cudaMemsetAsync(c->mlp_grad, 0, sizeof(float) * HP_MLP_NPARAM, s));
-            const unsigned grid = (unsigned)std::min<int64_t>((nb + MLP_BLOCK - 1) / MLP_BLOCK, c->sm_count * 2);
-            mlp_grad_kernel<<<grid, MLP_BLOCK, 0, s>>>(c->mlp_params, d_x, d_y, d_perm, b0, nb, 1.0f / (float)nb,
-                                                       c->mlp_grad,
-                                                       last_epoch ? (float *)c->d_scal : (float *)nullptr);
+            HP_TRY(mlp_grad_det(s, c->mlp_params, d_x, d_y, d_perm, b0, nb, 1.0f / (float)nb, c->mlp_scratch,
+                                c->mlp_grad, last_epoch ? (float *)c->d_scal : (float *)nullptr));
             p1 *= b1;
             p2 *= b2;
             adam_kernel<<<(HP_MLP_NPARAM + 255) / 256, 256, 0, s>>>(c->mlp_params, c->mlp_grad, c->mlp_m, c->mlp_v,

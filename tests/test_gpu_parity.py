@@ -2,6 +2,7 @@
 (coarse CSR, vertex/edge weights, matching, cmap, initial and projected
 partitions, refined partitions, cuts) must be bit-identical."""
 import ctypes as C
+import os
 import time
 
 import numpy as np
@@ -20,7 +21,7 @@ NAMES = ["xadj", "adjncy", "adjwgt", "vwgt", "match", "cmap", "where_start", "wh
 
 def compare_runs(ctx, g, k, ub=1.03, tpwgts=None, **optkw):
     opt = default_options(trace=1, **optkw)
-    oracle.set_threads(8)
+    oracle.set_threads(os.cpu_count() or 1)
     part_o, cut_o, tr = oracle.partition(g, k, ub, tpwgts=tpwgts, opt=opt, trace=True)
     part_g, cut_g = ctx.partition_graph(g, k, ub, tpwgts=tpwgts, options=opt)
     L = tr.nlevels
