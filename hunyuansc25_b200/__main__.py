@@ -67,7 +67,7 @@ def main(argv=None) -> int:
     print(f"graph:{name} {g.nvtxs} {g.nedges // 2} {nparts} 0", flush=True)
 
     ctx = Context(a.device)
-    tpath = tune.resolve_tuning(a.tuning, a.workload)
+    tpath = tune.resolve_tuning(a.tuning, a.workload, a.learned)
     if tpath:
         ctx.load_tuning(tpath)
         print(f"tuning: {tpath}")

@@ -97,6 +97,7 @@ TUNING_FIELDS = [
     "batch_workers",
     "small_match_n",
     "contract_hybrid",
+    "apply_chunk_deg",
 ]
 
 TUNING_DEFAULTS = {
@@ -117,6 +118,7 @@ TUNING_DEFAULTS = {
     "batch_workers": 16,
     "small_match_n": 8192,
     "contract_hybrid": 1,
+    "apply_chunk_deg": 4096,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -143,6 +145,7 @@ def tuning_violation(t: dict):
         ("batch_workers", 1, 64),
         ("small_match_n", 0, 8192),
         ("contract_hybrid", 0, 1),
+        ("apply_chunk_deg", t["gain_thread_deg"], TUNE_DEG_MAX),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -151,7 +154,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 7)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 6)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

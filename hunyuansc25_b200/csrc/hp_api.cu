@@ -617,6 +617,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->batch_workers = 16;
     t->small_match_n = 8192;
     t->contract_hybrid = 1;
+    t->apply_chunk_deg = 4096;
 }
 
 namespace {
@@ -641,6 +642,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.batch_workers, 1, 64)) return "batch_workers";
     if (!in(t.small_match_n, 0, HP_TUNE_SMALL_MATCH_MAX)) return "small_match_n";
     if (!in(t.contract_hybrid, 0, 1)) return "contract_hybrid";
+    if (!in(t.apply_chunk_deg, t.gain_thread_deg, HP_TUNE_DEG_MAX)) return "apply_chunk_deg";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;

@@ -206,6 +206,9 @@ __device__ __forceinline__ void block_add_to(long long v, unsigned long long *ou
         t = warp_sum64(t);
         if (threadIdx.x == 0 && t != 0) atomicAdd(out, (unsigned long long)t);
     }
+    // s_part is one array for every call site of this BLOCK size: a following
+    // call may write it only after the first warp has read it
+    __syncthreads();
 }
 
 // Decoupled look-back (single-pass scan across CTAs).  tile_status[t] holds

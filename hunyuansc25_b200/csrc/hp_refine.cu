@@ -1960,6 +1960,7 @@ apply_bytes_kernel(const int32_t *__restrict__ moves, const unsigned long long *
 struct PassCfg {
     int32_t k;
     bool finest, any_big, recording, huge_rows;   // huge_rows: rows longer than chunk_deg exist
+    bool huge_moves;                              // rows longer than apply_chunk_deg exist
     RefineCtl *ctl;
     unsigned long long *best_pw;
 };
@@ -2038,8 +2039,8 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
     int atok = hp_prof_begin(c);
     HP_LAUNCH(c, apply_moves_kernel, pg, 256, 0, B.moves, &sc[S_NMOVES], g.where, B.dest, g.vwgt, B.pw, g.xadj,
               g.adjncy, g.adjwgt, B.goff, B.gconn, B.dirty, B.small_l, B.big_l, (int32_t *)&sc[S_DIRTY], k,
-              B.huge_mv, (int32_t *)&sc[S_HUGEMV], c->tune.gain_thread_deg, c->tune.chunk_deg);
-    if (P.huge_rows) {
+              B.huge_mv, (int32_t *)&sc[S_HUGEMV], c->tune.gain_thread_deg, c->tune.apply_chunk_deg);
+    if (P.huge_moves) {
         HP_LAUNCH(c, hub_plan_kernel<true>, plan_grid(c, B.nhub_cap), PLAN_THREADS, 0, B.huge_mv,
                   (const int32_t *)&sc[S_HUGEMV], B.moves, B.pregain, g.xadj, B.plan_v, B.plan_item, B.plan_off,
                   B.plan_cnt, c->lb_status, c->lb_cap / 2, c->lb_ctl, c->d_status);
@@ -2635,10 +2636,12 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.ufl = ralloc_t<int8_t>(c, k);
     B.pw = ralloc_t<unsigned long long>(c, k);
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
-    // at most m / (chunk_deg + 1) rows are longer than chunk_deg (the long-row
-    // list of the afterburner and of the moves)
-    const int32_t huged = c->tune.gain_hub_deg, chunkd = c->tune.chunk_deg;
-    const int64_t nhub_cap = std::min<int64_t>((int64_t)n, g.m / ((int64_t)chunkd + 1)) + 1;
+    // at most m / (t + 1) rows are longer than t: the long-row lists of the
+    // afterburner (t = chunk_deg) and of the moves (t = apply_chunk_deg) share
+    // the chunk-plan buffers
+    const int32_t huged = c->tune.gain_hub_deg, chunkd = c->tune.chunk_deg, mchunkd = c->tune.apply_chunk_deg;
+    const int64_t nhub_cap =
+        std::min<int64_t>((int64_t)n, g.m / ((int64_t)std::min(chunkd, mchunkd) + 1)) + 1;
     if (2 * (nhub_cap / PLAN_TILE + 1) > c->lb_cap) return HP_ERR_INTERNAL;
     B.nhub_cap = nhub_cap;
     B.ab_acc = ralloc_t<unsigned long long>(c, nhub_cap);
@@ -2693,7 +2696,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
         log_r0 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
     }
-    PassCfg P{k, finest, any_big, recording, ls.maxdeg > chunkd, ctl, best_pw};
+    PassCfg P{k, finest, any_big, recording, ls.maxdeg > chunkd, ls.maxdeg > mchunkd, ctl, best_pw};
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     const bool use_graph = graph_loop(c);
     RefineCtl h{};

@@ -61,6 +61,7 @@ SPACE = {
     "contract_smem_cn": [0, 8192, 16384, 32768, 49152],
     "small_match_n": [0, 1024, 2048, 4096, 8192],
     "contract_hybrid": [0, 1],
+    "apply_chunk_deg": [256, 512, 1024, 2048, 4096, 8192],
 }
 
 
@@ -100,18 +101,27 @@ def write_tuning_file(path: str, tuning: dict, **meta) -> None:
         f.write("\n")
 
 
-def workload_tuning_path(workload: str | None) -> str | None:
+def workload_tuning_path(workload: str | None, learned: bool = False) -> str | None:
+    """The committed tuning file of a workload: tuning/<workload>.json for the
+    plain refiner, tuning/<workload>_learned.json (when present, else the plain
+    file) for the learned move proposals, whose passes move far fewer vertices
+    and so favour other row-class bounds."""
     if not workload:
         return None
+    if learned:
+        p = os.path.join(TUNING_DIR, f"{workload}_learned.json")
+        if os.path.exists(p):
+            return p
     p = os.path.join(TUNING_DIR, f"{workload}.json")
     return p if os.path.exists(p) else None
 
 
-def resolve_tuning(arg: str | None, workload: str | None) -> str | None:
+def resolve_tuning(arg: str | None, workload: str | None, learned: bool = False) -> str | None:
     """Tuning file for a --tuning argument: None/'auto' -> the workload's
-    committed file if there is one, 'none' -> no file, else the path given."""
+    committed file for that refiner if there is one, 'none' -> no file, else
+    the path given."""
     if arg in (None, "auto"):
-        return workload_tuning_path(workload)
+        return workload_tuning_path(workload, learned)
     if arg == "none":
         return None
     if not os.path.exists(arg):
@@ -232,6 +242,9 @@ def main(argv=None) -> int:
     ap.add_argument("--sweeps", type=int, default=2)
     ap.add_argument("--min-gain", type=float, default=0.01)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--learned", action="store_true",
+                    help="tune the learned move proposals (committed weights); the file is "
+                         "tuning/<workload>_learned.json")
     a = ap.parse_args(argv)
     graphs.set_threads(os.cpu_count() or 1)
     if a.workload:
@@ -240,7 +253,7 @@ def main(argv=None) -> int:
         name = a.workload
         nparts = a.nparts or nparts
         ub = a.ub or ub
-        out = a.out or os.path.join(TUNING_DIR, f"{a.workload}.json")
+        out = a.out or os.path.join(TUNING_DIR, f"{a.workload}{'_learned' if a.learned else ''}.json")
     else:
         if not a.graph or a.nparts is None:
             ap.error("give <graph> <nparts>, or --workload")
@@ -249,12 +262,19 @@ def main(argv=None) -> int:
         out = a.out or f"{a.graph}.tuning.json"
     import torch
     ctx = Context(a.device)
-    best, rep = autotune(ctx, g, nparts, ub, reps=a.reps, sweeps=a.sweeps, min_gain=a.min_gain,
-                         log=lambda s: print(s, flush=True), device=a.device)
+    options = None
+    if a.learned:
+        from . import learn
+        params, thr, _ = learn.load_params()
+        ctx.mlp_set_params(params, thr)
+        options = default_options(learned=1)
+    best, rep = autotune(ctx, g, nparts, ub, options=options, reps=a.reps, sweeps=a.sweeps,
+                         min_gain=a.min_gain, log=lambda s: print(s, flush=True), device=a.device)
     write_tuning_file(out, best, device=torch.cuda.get_device_name(a.device),
                       sm_count=torch.cuda.get_device_properties(a.device).multi_processor_count,
                       workload={"name": name, "nvtxs": g.nvtxs, "nedges_undirected": g.nedges // 2,
                                 "nparts": nparts, "ubfactor": ub},
+                      refiner="learned" if a.learned else "plain",
                       **rep)
     print(json.dumps({"out": out, "tuning": best, **{k: v for k, v in rep.items() if k != "changes"}}))
     ctx.close()

@@ -189,7 +189,10 @@ typedef struct hp_tuning {
                                     contract_warp_row accumulate their ids below 32768 in
                                     a shared-memory dense accumulator and radix-sort the
                                     rest (1), or radix-sort every entry (0)      [0, 1]        1 */
-    int32_t reserved[7];         /* zero */
+    int32_t apply_chunk_deg;     /* refinement: move application splits rows longer than
+                                    this into chunks of 512 entries over the whole grid
+                                    (chunk_deg is the afterburner's)     [gain_thread_deg, 2^24] 4096 */
+    int32_t reserved[6];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);

@@ -35,7 +35,7 @@ def test_library_defaults_match_python():
     t = HpTuning()
     lib.hp_tuning_default(C.byref(t))
     assert t.as_dict() == TUNING_DEFAULTS
-    assert list(t.reserved) == [0] * 7
+    assert list(t.reserved) == [0] * 6
     assert tuning_violation(TUNING_DEFAULTS) is None
 
 
@@ -46,7 +46,7 @@ def test_library_defaults_match_python():
     ("grid_ctas_per_sm", 0), ("grid_ctas_per_sm", 33), ("dense_sparse_ratio", 0),
     ("small_level_n", -1), ("small_level_n", 32769), ("chunk_deg", 31), ("trial_cta_n", 0), ("contract_smem_cn", 49153),
     ("batch_workers", 0), ("batch_workers", 65), ("small_match_n", -1), ("small_match_n", 8193),
-    ("contract_hybrid", -1), ("contract_hybrid", 2),
+    ("contract_hybrid", -1), ("contract_hybrid", 2), ("apply_chunk_deg", 31),
 ])
 def test_violations(field, value):
     t = dict(TUNING_DEFAULTS)
