@@ -193,6 +193,24 @@ class Context:
         _check(self.lib.hp_last_stats(self.h, C.byref(st)), "hp_last_stats")
         return st
 
+    # ---- nested-dissection ordering ---------------------------------------------------
+    def node_nd(self, xadj, adjncy, vwgt=None, options: HpOptions | None = None):
+        """Fill-reducing nested-dissection ordering of a host CSR (hp_node_nd):
+        (perm, iperm) with perm[new] = old and iperm[old] = new."""
+        xadj = _i32(xadj)
+        adjncy = _i32(adjncy)
+        vwgt = None if vwgt is None else _i32(vwgt)
+        n = xadj.shape[0] - 1
+        perm = np.empty(max(n, 1), np.int32)
+        iperm = np.empty(max(n, 1), np.int32)
+        opt = options if options is not None else default_options()
+        _check(self.lib.hp_node_nd(self.h, n, _p32(xadj), _p32(adjncy), _p32(vwgt), C.byref(opt), _p32(perm),
+                                   _p32(iperm)), "hp_node_nd")
+        return perm[:n], iperm[:n]
+
+    def node_nd_graph(self, g, options=None):
+        return self.node_nd(g.xadj, g.adjncy, g.vwgt, options)
+
     # ---- trace ----------------------------------------------------------------------
     @property
     def trace_nlevels(self) -> int:

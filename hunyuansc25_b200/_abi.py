@@ -247,6 +247,7 @@ PROTOTYPES = {
     "hp_movelog_count": (C.c_int64, [C.c_void_p]),
     "hp_movelog_copy": (C.c_int, [C.c_void_p, F32P, F32P, C.c_int64]),
     "hp_movelog_reset": (C.c_int, [C.c_void_p]),
+    "hp_node_nd": (C.c_int, [C.c_void_p, C.c_int32, I32P, I32P, I32P, C.POINTER(HpOptions), I32P, I32P]),
     "hp_scan_exclusive_i32": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
                                         C.c_void_p]),
     "hp_scan_exclusive_i32_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),

@@ -34,6 +34,7 @@ CU_SOURCES = [
     "hp_initpart.cu",
     "hp_refine.cu",
     "hp_mlp.cu",
+    "hp_nd.cu",
 ]
 
 

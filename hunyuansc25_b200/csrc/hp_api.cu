@@ -911,6 +911,18 @@ HP_API int hp_trace_copy(const hp_context *ctx, int level, int what, int32_t *ds
     return HP_OK;
 }
 
+int hp_ensure_workers(hp_context *ctx, int nworkers)
+{
+    HP_CUDA(cudaSetDevice(ctx->device));
+    while ((int)ctx->workers.size() < nworkers) {
+        hp_context *w = nullptr;
+        HP_TRY(hp_context_create(ctx->device, &w));
+        ctx->workers.push_back(w);
+    }
+    for (hp_context *w : ctx->workers) w->tune = ctx->tune;
+    return HP_OK;
+}
+
 HP_API int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *vtxdist,
                               const int64_t *edgedist, const int32_t *xadj, const int32_t *adjncy,
                               const int32_t *vwgt, const int32_t *adjwgt, const int32_t *nparts,
@@ -930,13 +942,7 @@ HP_API int hp_partition_batch(hp_context *ctx, int32_t ngraphs, const int64_t *v
         if (vtxdist[gi + 1] - vtxdist[gi] > INT32_MAX - 1) return HP_ERR_UNSUPPORTED;
     }
     const int nworkers = (int)std::min<int64_t>(ngraphs, ctx->tune.batch_workers);
-    HP_CUDA(cudaSetDevice(ctx->device));
-    while ((int)ctx->workers.size() < nworkers) {
-        hp_context *w = nullptr;
-        HP_TRY(hp_context_create(ctx->device, &w));
-        ctx->workers.push_back(w);
-    }
-    for (hp_context *w : ctx->workers) w->tune = ctx->tune;
+    HP_TRY(hp_ensure_workers(ctx, nworkers));
     // The workers run their levels' pass loops eagerly: sixteen host threads that
     // capture and instantiate a CUDA graph per level contend for the driver, and
     // the graphs of small graphs' levels never amortise (the small-level kernel

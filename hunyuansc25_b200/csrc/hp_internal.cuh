@@ -204,6 +204,11 @@ int hp_initial_partition(hp_context *c, HpLevel &g, int32_t nparts, const int64_
 // ---- refinement (hp_refine.cu) --------------------------------------------------
 int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int64_t *h_maxp);
 // One-time kernel attributes (dynamic shared memory above 48 KB).
+// Worker contexts of a context (own streams and arenas) for independent
+// partitions run concurrently (hp_partition_batch, hp_node_nd): at least
+// nworkers of them, with the context's tuning.
+int hp_ensure_workers(hp_context *ctx, int nworkers);
+
 int hp_refine_init();
 int hp_initpart_init();
 int hp_coarsen_init();

@@ -263,6 +263,23 @@ int64_t hp_movelog_count(hp_context *ctx);
 int     hp_movelog_copy(hp_context *ctx, float *features, float *labels, int64_t count);
 int     hp_movelog_reset(hp_context *ctx);
 
+/* ---- nested-dissection ordering -------------------------------------------------
+ * Fill-reducing ordering of a symmetric sparsity pattern (host CSR as for
+ * hp_partition; vwgt may be NULL; edge weights are not used).  Replaces the
+ * reference's ReorderGraph / NestedBisection
+ * (mygp_0.9.9_test_initpartition/reordergraph.h:177-306): a vertex separator
+ * of every subgraph takes the highest numbers of the subgraph's range, the
+ * two sides are ordered recursively (left side first) and subgraphs of at
+ * most 120 vertices, or without edges, are ordered by an exact minimum-degree
+ * elimination (the reference's MMD_Order, whose source is not in its tree).
+ * Separators come from 2-way partitions by this library (imbalance 1.05, the
+ * options in opt, NULL = defaults), so the ordering is deterministic.  Output:
+ * iperm[old] = new and, when perm is not NULL, perm[new] = old (METIS_NodeND's
+ * convention; the reference's reflect array is iperm).  hp_last_stats reports
+ * the recursion depths in nlevels and the 2-way partitions in refine_passes. */
+int hp_node_nd(hp_context *ctx, int32_t nvtxs, const int32_t *xadj, const int32_t *adjncy,
+               const int32_t *vwgt, const hp_options *opt, int32_t *perm, int32_t *iperm);
+
 /* ---- device primitives (device pointers, issued on `stream`) ------------------- */
 /* Exclusive int32 prefix sum, single-pass decoupled look-back.  Writes n+1
  * outputs (out[n] = total); in == out is allowed.  Replaces prefixsum()

@@ -53,6 +53,12 @@ def lib():
         L.ora_partition.restype = C.c_int
         L.ora_weight_range_ok.argtypes = [C.c_int32, I32P, I32P]
         L.ora_weight_range_ok.restype = C.c_int
+        L.ora_node_nd.argtypes = [C.c_int32, I32P, I32P, I32P, C.POINTER(HpOptions), I32P, I32P]
+        L.ora_node_nd.restype = C.c_int
+        L.ora_nd_separator.argtypes = [C.c_int32, I32P, I32P, I32P, I32P]
+        L.ora_nd_separator.restype = None
+        L.ora_cholesky_nnz.argtypes = [C.c_int32, I32P, I32P, I32P]
+        L.ora_cholesky_nnz.restype = C.c_int64
         L.ora_trace_nlevels.argtypes = [C.c_void_p]
         L.ora_trace_level.argtypes = [C.c_void_p, C.c_int, I32P, I64P, I64P, I64P]
         L.ora_trace_copy.argtypes = [C.c_void_p, C.c_int, C.c_int, I32P, C.c_int64]
@@ -163,6 +169,31 @@ def partition(g, nparts, ubfactor=1.03, tpwgts=None, opt: HpOptions | None = Non
     if rc != 0:
         raise OracleError(rc)
     return part[:g.nvtxs], cut.value, (Trace(th.value) if trace else None)
+
+
+def node_nd(g, opt: HpOptions | None = None):
+    """Nested-dissection ordering (the library's hp_node_nd rules):
+    (perm, iperm) with perm[new] = old and iperm[old] = new."""
+    n = g.nvtxs
+    perm = np.empty(max(n, 1), np.int32)
+    iperm = np.empty(max(n, 1), np.int32)
+    rc = lib().ora_node_nd(n, _p(i32(g.xadj)), _p(i32(g.adjncy)), _p(i32(g.vwgt)),
+                           C.byref(opt if opt is not None else default_options()), _p(perm), _p(iperm))
+    if rc != 0:
+        raise OracleError(rc)
+    return perm[:n], iperm[:n]
+
+
+def nd_separator(g, where):
+    """side_of in {0, 1, 2 = separator} from a 2-way partition (ND's rule)."""
+    out = np.empty(max(g.nvtxs, 1), np.int32)
+    lib().ora_nd_separator(g.nvtxs, _p(i32(g.xadj)), _p(i32(g.adjncy)), _p(i32(where)), _p(out))
+    return out[:g.nvtxs]
+
+
+def cholesky_nnz(g, iperm) -> int:
+    """Entries of the Cholesky factor (diagonal included) under iperm."""
+    return int(lib().ora_cholesky_nnz(g.nvtxs, _p(i32(g.xadj)), _p(i32(g.adjncy)), _p(i32(iperm))))
 
 
 def weight_range_ok(g) -> bool:

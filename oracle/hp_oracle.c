@@ -1399,3 +1399,248 @@ float ora_mlp_loss_grad(const float *P, const float *X, const float *Y, int64_t 
     for (int i = 0; i < OMLP_N; i++) grad[i] = (float)(g[i] / (double)n);
     return (float)(loss / (double)n);
 }
+
+/* ------------------------------------------------------------------------- */
+/* Nested-dissection ordering (the library's hp_node_nd).                     */
+/*
+ * Follows the structure of the reference's NestedBisection / ReorderGraph
+ * (mygp_0.9.9_test_initpartition/reordergraph.h:177-306): a vertex separator
+ * of the graph is numbered last, the two sides are split off as induced
+ * subgraphs and ordered recursively (left side first, then right), and a
+ * subgraph of at most ND_LEAF vertices or without edges is ordered directly
+ * (the reference calls MMD_Order from mmdorder.h, which the reference tree
+ * does not contain; here an exact minimum-degree elimination).  The rules
+ * that the reference leaves to randomised code are fixed:
+ *   - the 2-way partition is this library's multilevel partition (k = 2,
+ *     imbalance ND_UB, unit edge weights, the caller's vertex weights and
+ *     options), where the reference runs its own randomised bisection with
+ *     node refinement (reordergraph.h:17-135, refine.h:1398-1856);
+ *   - separator: the boundary vertices of the side with fewer of them (side
+ *     0 on a tie), then thinning: a separator vertex without a neighbour in
+ *     the rest of its own side joins the other side (decided for every
+ *     separator vertex at once, which keeps a separator);
+ *   - numbering: separator vertices in increasing local id take the highest
+ *     numbers of the subgraph's range; the left side the lowest block, the
+ *     right side the block before the separator;
+ *   - a split that leaves the whole subgraph on one side (no separator, an
+ *     empty side) orders the subgraph by increasing vertex id;
+ *   - leaves: repeatedly the live vertex of least degree in the elimination
+ *     graph (ties: lowest id) takes the next number and its live neighbours
+ *     become a clique.
+ */
+#define ND_LEAF 120
+#define ND_UB 1.05f
+
+typedef struct {
+    int32_t n;
+    int32_t *xadj, *adjncy, *vwgt, *label;
+} nd_sub;
+
+static void nd_free(nd_sub *s)
+{
+    free(s->xadj); free(s->adjncy); free(s->vwgt); free(s->label);
+    memset(s, 0, sizeof(*s));
+}
+
+/* Exact minimum-degree elimination of a leaf (n <= ND_LEAF), numbers lo.. */
+static void nd_leaf(const nd_sub *g, int32_t lo, int32_t *iperm)
+{
+    const int32_t n = g->n;
+    if (n == 0) return;
+    if (n > ND_LEAF || g->xadj[n] == 0) {   /* no edges: every degree stays 0 */
+        for (int32_t v = 0; v < n; v++) iperm[g->label[v]] = lo + v;
+        return;
+    }
+    enum { W = (ND_LEAF + 63) / 64 };
+    uint64_t adj[ND_LEAF][W];
+    memset(adj, 0, sizeof(adj));
+    for (int32_t v = 0; v < n; v++)
+        for (int32_t j = g->xadj[v]; j < g->xadj[v + 1]; j++) {
+            const int32_t u = g->adjncy[j];
+            adj[v][u >> 6] |= 1ull << (u & 63);
+        }
+    uint64_t alive[W];
+    memset(alive, 0, sizeof(alive));
+    for (int32_t v = 0; v < n; v++) alive[v >> 6] |= 1ull << (v & 63);
+    for (int32_t step = 0; step < n; step++) {
+        int32_t best = -1, bdeg = 0;
+        for (int32_t v = 0; v < n; v++) {
+            if (!(alive[v >> 6] >> (v & 63) & 1)) continue;
+            int32_t d = 0;
+            for (int w = 0; w < W; w++) d += __builtin_popcountll(adj[v][w] & alive[w]);
+            if (best < 0 || d < bdeg) { best = v; bdeg = d; }
+        }
+        iperm[g->label[best]] = lo + step;
+        alive[best >> 6] &= ~(1ull << (best & 63));
+        uint64_t nb[W];
+        for (int w = 0; w < W; w++) nb[w] = adj[best][w] & alive[w];
+        for (int32_t u = 0; u < n; u++) {
+            if (!(nb[u >> 6] >> (u & 63) & 1)) continue;
+            for (int w = 0; w < W; w++) adj[u][w] |= nb[w];
+            adj[u][u >> 6] &= ~(1ull << (u & 63));
+        }
+    }
+}
+
+/* One side (0 or 1) of a 3-way side_of (2 = separator) as an induced subgraph,
+ * vertex order and row order kept. */
+static void nd_split(const nd_sub *g, const int32_t *side_of, int32_t side, nd_sub *out)
+{
+    const int32_t n = g->n;
+    int32_t *lid = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    int32_t cnt = 0;
+    for (int32_t v = 0; v < n; v++) lid[v] = side_of[v] == side ? cnt++ : -1;
+    out->n = cnt;
+    out->xadj = (int32_t *)xmalloc(sizeof(int32_t) * ((size_t)cnt + 1));
+    out->vwgt = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(cnt > 0 ? cnt : 1));
+    out->label = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(cnt > 0 ? cnt : 1));
+    int64_t m = 0;
+    for (int32_t v = 0; v < n; v++)
+        if (side_of[v] == side)
+            for (int32_t j = g->xadj[v]; j < g->xadj[v + 1]; j++) m += side_of[g->adjncy[j]] == side;
+    out->adjncy = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    int64_t e = 0;
+    for (int32_t v = 0; v < n; v++) {
+        if (side_of[v] != side) continue;
+        out->xadj[lid[v]] = (int32_t)e;
+        out->vwgt[lid[v]] = g->vwgt[v];
+        out->label[lid[v]] = g->label[v];
+        for (int32_t j = g->xadj[v]; j < g->xadj[v + 1]; j++)
+            if (side_of[g->adjncy[j]] == side) out->adjncy[e++] = lid[g->adjncy[j]];
+    }
+    out->xadj[cnt] = (int32_t)e;
+    free(lid);
+}
+
+/* The separator rule: side_of[v] in {0, 1, 2 (separator)} from a 2-way where. */
+void ora_nd_separator(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int32_t *where,
+                      int32_t *side_of)
+{
+    int32_t bnd[2] = {0, 0};
+    uint8_t *b = (uint8_t *)xmalloc((size_t)(n > 0 ? n : 1));
+    for (int32_t v = 0; v < n; v++) {
+        b[v] = 0;
+        for (int32_t j = xadj[v]; j < xadj[v + 1]; j++)
+            if (where[adjncy[j]] != where[v]) { b[v] = 1; break; }
+        bnd[where[v]] += b[v];
+    }
+    const int32_t a = bnd[0] <= bnd[1] ? 0 : 1;
+    for (int32_t v = 0; v < n; v++) {
+        side_of[v] = where[v];
+        if (where[v] != a || !b[v]) continue;
+        int keep = 0;   /* a neighbour in the rest of side a keeps v in the separator */
+        for (int32_t j = xadj[v]; j < xadj[v + 1]; j++) {
+            const int32_t u = adjncy[j];
+            if (where[u] == a && !b[u]) { keep = 1; break; }
+        }
+        side_of[v] = keep ? 2 : 1 - a;
+    }
+    free(b);
+}
+
+static int nd_rec(nd_sub *g, int32_t hi, const hp_options *opt, int32_t *iperm)
+{
+    const int32_t n = g->n;
+    if (n == 0) return HP_OK;
+    const int32_t lo = hi - n;
+    if (n <= ND_LEAF || g->xadj[n] == 0) {
+        nd_leaf(g, lo, iperm);
+        return HP_OK;
+    }
+    int32_t *where = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)n);
+    int64_t cut = 0;
+    int rc = ora_partition(n, g->xadj, g->adjncy, g->vwgt, NULL, 2, NULL, ND_UB, opt, where, &cut, NULL);
+    if (rc != HP_OK) { free(where); return rc; }
+    int32_t *side_of = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)n);
+    ora_nd_separator(n, g->xadj, g->adjncy, where, side_of);
+    free(where);
+    int32_t cnt[3] = {0, 0, 0};
+    for (int32_t v = 0; v < n; v++) cnt[side_of[v]]++;
+    if (cnt[0] == n || cnt[1] == n) {   /* no progress: vertex order */
+        for (int32_t v = 0; v < n; v++) iperm[g->label[v]] = lo + v;
+        free(side_of);
+        return HP_OK;
+    }
+    int32_t r = 0;
+    for (int32_t v = 0; v < n; v++)
+        if (side_of[v] == 2) iperm[g->label[v]] = hi - cnt[2] + r++;
+    nd_sub L, R;
+    nd_split(g, side_of, 0, &L);
+    nd_split(g, side_of, 1, &R);
+    free(side_of);
+    nd_free(g);   /* the parent is not needed below */
+    rc = nd_rec(&L, hi - cnt[2] - cnt[1], opt, iperm);
+    if (rc == HP_OK) rc = nd_rec(&R, hi - cnt[2], opt, iperm);
+    nd_free(&L);
+    nd_free(&R);
+    return rc;
+}
+
+int ora_node_nd(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int32_t *vwgt,
+                const hp_options *opt_in, int32_t *perm, int32_t *iperm)
+{
+    if (n < 0 || !xadj || (n > 0 && !adjncy) || !iperm) return HP_ERR_INVALID_ARG;
+    hp_options opt;
+    if (opt_in) opt = *opt_in; else ora_options_default(&opt);
+    opt.trace = 0;
+    nd_sub g;
+    g.n = n;
+    const int64_t m = xadj[n];
+    g.xadj = (int32_t *)xmalloc(sizeof(int32_t) * ((size_t)n + 1));
+    g.adjncy = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(m > 0 ? m : 1));
+    g.vwgt = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    g.label = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)(n > 0 ? n : 1));
+    memcpy(g.xadj, xadj, sizeof(int32_t) * ((size_t)n + 1));
+    if (m > 0) memcpy(g.adjncy, adjncy, sizeof(int32_t) * (size_t)m);
+    for (int32_t v = 0; v < n; v++) { g.vwgt[v] = vwgt ? vwgt[v] : 1; g.label[v] = v; }
+    const int rc = nd_rec(&g, n, &opt, iperm);
+    nd_free(&g);
+    if (rc == HP_OK && perm)
+        for (int32_t v = 0; v < n; v++) perm[iperm[v]] = v;
+    return rc;
+}
+
+/* Entries of the Cholesky factor L (diagonal included) of the symmetric
+ * matrix with this sparsity under the ordering iperm (old -> new): the
+ * elimination tree (Liu's algorithm with path compression), then each row's
+ * subtree walked from its below-diagonal entries up to the marked nodes. */
+int64_t ora_cholesky_nnz(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int32_t *iperm)
+{
+    if (n <= 0) return 0;
+    int32_t *perm = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)n);
+    for (int32_t v = 0; v < n; v++) perm[iperm[v]] = v;
+    int32_t *parent = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)n);
+    int32_t *anc = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)n);
+    for (int32_t i = 0; i < n; i++) {
+        parent[i] = -1;
+        anc[i] = -1;
+        const int32_t v = perm[i];
+        for (int32_t j = xadj[v]; j < xadj[v + 1]; j++) {
+            int32_t k = iperm[adjncy[j]];
+            while (k >= 0 && k < i) {
+                const int32_t next = anc[k];
+                anc[k] = i;
+                if (next < 0) { parent[k] = i; break; }
+                k = next;
+            }
+        }
+    }
+    int32_t *mark = (int32_t *)xmalloc(sizeof(int32_t) * (size_t)n);
+    for (int32_t i = 0; i < n; i++) mark[i] = -1;
+    int64_t nnz = 0;
+    for (int32_t i = 0; i < n; i++) {
+        nnz++;   /* diagonal */
+        mark[i] = i;
+        const int32_t v = perm[i];
+        for (int32_t j = xadj[v]; j < xadj[v + 1]; j++) {
+            int32_t k = iperm[adjncy[j]];
+            if (k >= i) continue;
+            for (; mark[k] != i; k = parent[k]) {   /* row i of L has column k */
+                nnz++;
+                mark[k] = i;
+            }
+        }
+    }
+    free(perm); free(parent); free(anc); free(mark);
+    return nnz;
+}

@@ -97,6 +97,16 @@ float ora_mlp_loss_grad(const float *params, const float *x, const float *y, int
 /* Weak-rebalance gain bucket (float semantics of the reference). */
 int32_t ora_gain_bucket(int32_t gain, int32_t vwgt);
 
+/* Nested-dissection ordering (the library's hp_node_nd): perm[new] = old,
+ * iperm[old] = new (perm may be NULL). */
+int ora_node_nd(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int32_t *vwgt,
+                const hp_options *opt, int32_t *perm, int32_t *iperm);
+/* The nested dissection's separator rule: side_of in {0, 1, 2 = separator}. */
+void ora_nd_separator(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int32_t *where,
+                      int32_t *side_of);
+/* Entries of the Cholesky factor (diagonal included) under the ordering iperm. */
+int64_t ora_cholesky_nnz(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int32_t *iperm);
+
 #ifdef __cplusplus
 }
 #endif
