@@ -54,6 +54,8 @@ WORKLOADS = {
                        "imbalance 1.05", k=1024, ub=1.05, coarsen_to=0,
                   make=lambda: graphs.config_rgg(1 << 24)),
 }
+WORKLOADS["nd"] = dict(desc="nested-dissection ordering of the grid3d 128^3 7-point mesh (hp_node_nd), unit weights",
+                       k=0, ub=1.05, coarsen_to=0, make=lambda: graphs.grid3d(128, 128, 128, seed=2, wmin=1, wmax=1))
 WORKLOADS["batch"] = dict(desc="1,024 graphs, n log-uniform in [1e3, 2e5] (seed 5), half 2-D grids, half R-MAT "
                                "(edge factor 8), weights U{1..100}, k from {2,4,8,16,32,64}, imbalance 1.03",
                           k=0, ub=1.03, coarsen_to=0, make=None)
@@ -145,6 +147,32 @@ def cpu_port_run(g, spec, threads):
     part, cut, _ = oracle.partition(g, spec["k"], spec["ub"], opt=opt)
     dt = time.perf_counter() - t0
     return dt, cut
+
+
+def ref_cpu_coarsen(g, spec):
+    """The reference's own CPU coarsening (hunyuangraph_cpu_coarsen,
+    hunyuangraph_CPU_coarsen.h:11-46: HEM matching and hash contraction per
+    level, one host thread), built from the reference sources into
+    oracle/_ref/libhp_ref.so by oracle/build_ref.sh, timed on the workload graph
+    down to the workload's coarsening threshold; None when the harness is not
+    built.  The reference's GPU path is timed by baseline/compare_ref_gpu.py."""
+    import ctypes as C
+    path = os.path.join(ROOT, "oracle", "_ref", "libhp_ref.so")
+    if not os.path.exists(path) or g.adjwgt.min(initial=1) == g.adjwgt.max(initial=1) == 1:
+        return None   # not built, or unit weights (the reference's unit-weight RM path is broken)
+    lib = C.CDLL(path)
+    P = C.POINTER(C.c_int)
+    lib.ref_cpu_coarsen.argtypes = [C.c_int, P, P, P, P, C.c_int, P]
+    lib.ref_cpu_coarsen.restype = C.c_int
+    k = spec["k"]
+    thr = spec["coarsen_to"] or (k * 8 if k * 8 <= 1024 else max(1024, 2 * k))
+    arrs = [np.ascontiguousarray(a, np.int32) for a in (g.xadj, g.adjncy, g.vwgt, g.adjwgt)]
+    cn = C.c_int()
+    t0 = time.perf_counter()
+    levels = lib.ref_cpu_coarsen(g.nvtxs, *(a.ctypes.data_as(P) for a in arrs), thr, C.byref(cn))
+    dt = time.perf_counter() - t0
+    return {"ms": round(1000 * dt, 1), "cores": 1, "levels": int(levels), "coarsest_nvtxs": int(cn.value),
+            "coarsen_to": thr, "what": "the reference's CPU coarsening alone (hunyuangraph_cpu_coarsen)"}
 
 
 def run_reference(args, spec, g, m_und):
@@ -319,6 +347,79 @@ def run_batch(args, spec):
         dist.destroy_process_group()
 
 
+def run_nd(args, spec, g):
+    """Nested-dissection ordering (hp_node_nd, host buffers, synchronous):
+    ms per ordering and edges/s, the Cholesky fill of the ordering against the
+    natural order, and the oracle's ordering of the same graph on all host
+    threads (identical iperm) as the CPU baseline.  Rank 0 only (the ordering
+    of one graph is not sharded)."""
+    import torch
+    import hunyuansc25_b200 as hp
+    import oracle
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    m_und = g.nedges // 2
+    threads = os.cpu_count() or 1
+    if args.impl == "reference":
+        oracle.set_threads(threads)
+        ts = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            oracle.node_nd(g)
+            if i >= args.warmup:
+                ts.append(time.perf_counter() - t0)
+        value = m_und * len(ts) / sum(ts)
+        print(json.dumps({"impl": "reference", "metric": "nested-dissection ordering edges/s", "value": value,
+                          "unit": "edges/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": 1000 * sum(ts) / len(ts), "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+                          "config": {"workload": spec["desc"], "name": "nd", "nvtxs": g.nvtxs,
+                                     "nedges_undirected": m_und},
+                          "cpu_baseline": {"value": value, "unit": "edges/s", "cores": threads, "kind": "port",
+                                           "sample": f"{args.steps} orderings of the mesh by the oracle"},
+                          "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    torch.cuda.set_device(0)
+    ctx = hp.Context(0)
+    for _ in range(args.warmup):
+        ctx.node_nd_graph(g)
+    ts, launches = [], 0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        perm, iperm = ctx.node_nd_graph(g)
+        ts.append(time.perf_counter() - t0)
+        launches += ctx.stats().kernel_launches
+    st = ctx.stats()
+    ms = 1000 * sum(ts) / len(ts)
+    cpu = None
+    fill = None
+    if not args.no_cpu_baseline:
+        oracle.set_threads(threads)
+        t0 = time.perf_counter()
+        _, oip = oracle.node_nd(g)
+        dt = time.perf_counter() - t0
+        cpu = {"value": m_und / dt, "unit": "edges/s", "cores": threads, "kind": "port", "ms": 1000 * dt,
+               "sample": "one ordering of the mesh by the oracle (all host threads)",
+               "parity_iperm_equal": bool(np.array_equal(oip, iperm))}
+        nat = oracle.cholesky_nnz(g, np.arange(g.nvtxs, dtype=np.int32))
+        nd = oracle.cholesky_nnz(g, iperm)
+        fill = {"nnz_L_natural": nat, "nnz_L_nd": nd, "ratio": round(nd / nat, 4)}
+    print(json.dumps({"metric": "nested-dissection ordering edges/s", "value": m_und / (ms / 1000),
+                      "unit": "edges/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                      "dtype": "int32", "data": "synthetic",
+                      "config": {"workload": spec["desc"], "name": "nd", "nvtxs": g.nvtxs, "nedges_undirected": m_und},
+                      "e2e": {"value": m_und / (ms / 1000), "unit": "edges/s",
+                              "h2d_bytes_per_step": (2 * g.nvtxs + 1 + g.nedges) * 4,
+                              "d2h_bytes_per_step": g.nvtxs * 4},
+                      "timing": "wall time of the synchronous host-buffer call (H2D, every partition and kernel, D2H)",
+                      "gpu_launches": launches, "depths": st.nlevels, "partitions": st.refine_passes,
+                      "cpu_baseline": cpu, "fill": fill}), flush=True)
+    ctx.close()
+
+
 def graph_cost_spec(kind, n):
     """Cost estimate (m + n) of a batch graph from its spec, without generating it:
     5-point grids have about 4n directed entries, R-MAT with edge factor 8 about 14n."""
@@ -353,6 +454,9 @@ def main():
         return
     g = spec["make"]()
     m_und = g.nedges // 2
+    if args.workload == "nd":
+        run_nd(args, spec, g)
+        return
 
     if args.impl == "reference":
         run_reference(args, spec, g, m_und)
@@ -543,7 +647,9 @@ def main():
                "sample": "one full partition of the workload graph by the CPU port of the plain path "
                          "(all host threads)",
                "edgecut": int(ocut), "parity_cut_equal": int(ocut) == plain_cut,
-               "parity_against": "the GPU plain refiner's cut (the learned refiner has no CPU counterpart)"}
+               "parity_against": "the GPU plain refiner's cut (the learned refiner has no CPU counterpart)",
+               "reference_cpu_coarsen": ref_cpu_coarsen(g, spec),
+               "coarsen_ms_gpu": round(last.ms_coarsen, 3)}
 
     if rank == 0:
         line = {

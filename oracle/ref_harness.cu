@@ -3,7 +3,8 @@
 // lie (see build_ref.sh; nothing of the reference is copied into this
 // repository).  Used by tests/ to pin the oracle's contraction, edge-cut and
 // graph-split semantics against the reference implementation, and by
-// bench.py's CPU baseline to time the reference's CPU coarsening.
+// bench.py's CPU-baseline leg to time the reference's CPU coarsening
+// (ref_cpu_coarsen).
 #include "HunyuanGRAPH.h"
 
 extern "C" {
