@@ -262,8 +262,11 @@ __device__ __forceinline__ void gain_bigwarp_rows(int64_t warp, int64_t nwarps, 
         const int32_t b = xadj[v], e = xadj[v + 1];
         if (e - b <= bigd || e - b > huged) continue;
         if (dirty && lane == 0) dirty[v] = 0;
+        // a row of at least k entries becomes a dense row (entry q = part q):
+        // its presence bits are never read
+        const bool dense = e - b >= k;
         for (int32_t j = b + lane; j < e; j += 128) {   // four chunks in flight
-            int32_t u[4], w[4];
+            int32_t u[4], w[4], q[4];
 #pragma unroll
             for (int t = 0; t < 4; t++) {
                 const int32_t jj = j + 32 * t;
@@ -271,22 +274,22 @@ __device__ __forceinline__ void gain_bigwarp_rows(int64_t warp, int64_t nwarps, 
                 w[t] = jj < e ? adjwgt[jj] : 0;
             }
 #pragma unroll
+            for (int t = 0; t < 4; t++) q[t] = u[t] >= 0 ? where[u[t]] : -1;   // the four gathers together
+#pragma unroll
             for (int t = 0; t < 4; t++) {
-                if (u[t] < 0) continue;
-                const int32_t q = where[u[t]];
-                atomicAdd(&dw[q], w[t]);
-                atomicOr(&bm[q >> 5], 1u << (q & 31));
+                if (q[t] < 0) continue;
+                atomicAdd(&dw[q[t]], w[t]);
+                if (!dense) atomicOr(&bm[q[t] >> 5], 1u << (q[t] & 31));
             }
         }
         __syncwarp();
         const int32_t o = goff[v], cap = goff[v + 1] - o;
-        if (e - b >= k) {   // dense row
+        if (dense) {   // (no presence bits were set)
             for (int32_t q = lane; q < k; q += 32) {
                 gpart[o + q] = q;
                 gconn[o + q] = dw[q];
                 dw[q] = 0;
             }
-            for (int32_t q = lane; q < nwords; q += 32) bm[q] = 0u;
             __syncwarp();
             continue;
         }
@@ -358,20 +361,34 @@ gain_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ 
         if (e - b <= bigd) continue;
         if (k <= warp_dense_k && e - b <= huged) continue;   // gain_bigwarp_kernel's rows
         if (dirty && threadIdx.x == 0) dirty[v] = 0;
-        for (int32_t j = b + threadIdx.x; j < e; j += NT) {
-            int32_t q = where[adjncy[j]];
-            atomicAdd(&dw[q], adjwgt[j]);
-            atomicOr(&bm[q >> 5], 1u << (q & 31));
+        // a row of at least k entries becomes a dense row (entry q = part q):
+        // its presence bits are never read
+        const bool dense = e - b >= k;
+        for (int32_t j = b + threadIdx.x; j < e; j += 4 * NT) {   // four entries per thread in flight
+            int32_t u[4], w[4], q[4];
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const int32_t jj = j + NT * t;
+                u[t] = jj < e ? adjncy[jj] : -1;
+                w[t] = jj < e ? adjwgt[jj] : 0;
+            }
+#pragma unroll
+            for (int t = 0; t < 4; t++) q[t] = u[t] >= 0 ? where[u[t]] : -1;
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                if (q[t] < 0) continue;
+                atomicAdd(&dw[q[t]], w[t]);
+                if (!dense) atomicOr(&bm[q[t] >> 5], 1u << (q[t] & 31));
+            }
         }
         __syncthreads();
         const int32_t o = goff[v], cap = goff[v + 1] - o;
-        if (e - b >= k) {   // dense row
+        if (dense) {
             for (int32_t q = threadIdx.x; q < k; q += NT) {
                 gpart[o + q] = q;
                 gconn[o + q] = dw[q];
                 dw[q] = 0;
             }
-            for (int32_t q = threadIdx.x; q < nwords; q += NT) bm[q] = 0;
             __syncthreads();
             continue;
         }
@@ -617,7 +634,10 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
             }
         }
     }
-    const float logit = hp::mlp_warp_logit(sm, f);
+    // the warp's tensor-core inference only when one of its vertices is a
+    // candidate (the logit is read for candidates alone; the vote is uniform)
+    float logit = 0.0f;
+    if (__any_sync(HP_FULL_MASK, cand)) logit = hp::mlp_warp_logit(sm, f);
     if (cand && logit < threshold) { cand = 0; g = NEG; d = where[v]; }
     if (v < n) { pregain[v] = g; dest[v] = d; }
     hp::block_add_to<256>(cand, d_ncand);
@@ -2187,7 +2207,7 @@ refine_small_kernel(SmallLevel a)
                                              a.opt[p], a.finest, f);
                     }
                 }
-                if (lrn) {
+                if (lrn && __any_sync(HP_FULL_MASK, cand)) {   // a warp without candidates needs no scores
                     const float logit = hp::mlp_warp_logit(s_mlp, f);
                     if (cand && logit < a.mlp_threshold) { cand = 0; g = NEG; d = p; }
                 }
