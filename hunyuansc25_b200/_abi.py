@@ -252,6 +252,8 @@ PROTOTYPES = {
                                         C.c_void_p]),
     "hp_scan_exclusive_i32_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]),
     "hp_test_wait_expiry": (C.c_int, [C.c_void_p]),
+    "hp_test_arena_first": (C.c_int, [C.c_void_p, C.c_int64]),
+    "hp_test_arena_restarts": (C.c_int, [C.c_void_p]),
     "hp_edgecut_device": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_void_p, I64P]),
     "hunyuangraph_PartitionGraph": (None, [I32P, I32P, I32P, I32P, I32P, I32P, F32P, F32P, I32P]),

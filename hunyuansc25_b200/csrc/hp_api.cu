@@ -798,8 +798,14 @@ static int partition_common(hp_context *c, int32_t n, int64_t m, const int32_t *
     // 256 vertices (the smallest tile), plus the scans' slack
     HP_TRY(hp_lb_reserve(c, ((int64_t)n + 255) / 256 + 1024));
     size_t want = estimate_arena(n, m);
+    if (c->arena_first) {   // hp_test_arena_first freed the arena: this attempt gets exactly that
+        want = c->arena_first;
+        c->arena_first = 0;
+    }
+    c->arena_restarts = 0;
     int rc = HP_ERR_NOMEM;
     for (int attempt = 0; attempt < 4 && rc == HP_ERR_NOMEM; attempt++) {
+        if (attempt > 0) c->arena_restarts++;
         HP_TRY(ensure_arena(c, want));
         reset_arena(c);
         unsigned zero = 0;
@@ -1067,6 +1073,28 @@ HP_API int hp_test_wait_expiry(hp_context *ctx)
     HP_CUDA(cudaStreamSynchronize(ctx->stream));
     if (rc == HP_ERR_TIMEOUT && e != 0) return HP_ERR_INTERNAL;   // the expired predecessor counts as 0
     return rc;
+}
+
+HP_API int hp_test_arena_first(hp_context *ctx, int64_t bytes)
+{
+    if (!ctx || bytes < 0) return HP_ERR_INVALID_ARG;
+    HP_CUDA(cudaSetDevice(ctx->device));
+    if (bytes > 0 && ctx->arena) {
+        HP_CUDA(cudaStreamSynchronize(ctx->own_stream));
+        cudaFree(ctx->arena);   // synchronises the device: no earlier call still reads it
+        ctx->arena = nullptr;
+        ctx->arena_cap = 0;
+        ctx->levels.clear();    // the last call's trace lived in the arena
+        ctx->trace_valid = false;
+    }
+    ctx->arena_first = (size_t)bytes;
+    return HP_OK;
+}
+
+HP_API int hp_test_arena_restarts(hp_context *ctx)
+{
+    if (!ctx) return HP_ERR_INVALID_ARG;
+    return ctx->arena_restarts;
 }
 
 // ---- legacy drop-in ------------------------------------------------------------------

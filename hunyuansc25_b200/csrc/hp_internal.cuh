@@ -34,6 +34,8 @@ struct hp_context {
     char *arena = nullptr;
     size_t arena_cap = 0, lo = 0, hi = 0;
     bool oom = false;
+    size_t arena_first = 0;     // hp_test_arena_first: size of the next call's first attempt
+    int arena_restarts = 0;     // restarts of the last partition call after running out
 
     // Small fixed device block: status word + scalar slots, and a pinned
     // host mirror for blocking scalar reads.
@@ -133,9 +135,12 @@ template <class T> inline T *ralloc_t(hp_context *c, int64_t n) { return (T *)hp
 
 #define HP_CHECK_OOM(c) do { if ((c)->oom) return HP_ERR_NOMEM; } while (0)
 
-// Count and check every kernel launch.
+// Count and check every kernel launch.  Once the arena has run out nothing more is
+// launched (a pointer allocated after that is null): the call unwinds with
+// HP_ERR_NOMEM and partition_common retries with a larger arena.
 #define HP_LAUNCH(ctx, kernel, grid, block, smem, ...)                                      \
     do {                                                                                    \
+        if ((ctx)->oom) return HP_ERR_NOMEM;                                                \
         if ((grid) > 0) {                                                                   \
             kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);                \
             (ctx)->launches++;                                                              \

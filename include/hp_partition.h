@@ -327,6 +327,18 @@ int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xadj,
  * spin-wait, hunyuangraph_GPU_match.h:350-358, is unbounded). */
 int hp_test_wait_expiry(hp_context *ctx);
 
+/* Test of the arena's grow-and-retry path.  bytes > 0 frees the context's
+ * arena and makes the next hp_partition / hp_partition_device call start with
+ * an arena of exactly `bytes` instead of the size estimated from (n, m); an
+ * attempt that runs out launches nothing more, unwinds with HP_ERR_NOMEM and
+ * restarts with twice the arena, at most four attempts in all, after which
+ * the call returns HP_ERR_NOMEM.  bytes == 0 clears a pending override.
+ * hp_test_arena_restarts returns how many restarts the last partition call
+ * made.  The reference prints and calls exit() when its device memory
+ * manager runs out (hunyuangraph_GPU_memory.h:117-121). */
+int hp_test_arena_first(hp_context *ctx, int64_t bytes);
+int hp_test_arena_restarts(hp_context *ctx);
+
 /* ---- legacy drop-in ------------------------------------------------------------
  * Identical signature to the reference (hunyuangraph_partitiongraph.h:284).
  * Uses a process-wide context on device 0 and hp_options_default(); ubvec[0]

@@ -11,7 +11,7 @@ import pytest
 import hunyuansc25_b200 as hp
 import oracle
 from hunyuansc25_b200 import graphs
-from hunyuansc25_b200._abi import (HP_ERR_INVALID_ARG, HP_ERR_INVALID_GRAPH, HP_ERR_TIMEOUT,
+from hunyuansc25_b200._abi import (HP_ERR_INVALID_ARG, HP_ERR_INVALID_GRAPH, HP_ERR_NOMEM, HP_ERR_TIMEOUT,
                                    HP_ERR_UNSUPPORTED, default_options)
 
 pytestmark = pytest.mark.gpu
@@ -241,6 +241,41 @@ def test_bounded_wait_expiry(ctx):
     assert rc == HP_ERR_TIMEOUT
     assert elapsed < 60
     compare_runs(ctx, graphs.grid2d(40, 30, seed=6, wmin=1, wmax=5), 8)
+
+
+def test_arena_exhaustion_retry(ctx):
+    """The arena's grow-and-retry path, driven from the host: the first attempt
+    gets a small arena, runs out, launches nothing more and restarts with twice
+    the arena.  Four attempts that all run out return HP_ERR_NOMEM and leave
+    the context usable; the first start size that succeeds does so after
+    restarts, with the same partition as a call with the estimated arena."""
+    g = graphs.rmat(14, seed=7)
+    ref_part, ref_cut, _ = compare_runs(ctx, g, 16)
+    lib, h = ctx.lib, ctx.h
+    assert lib.hp_test_arena_first(h, -1) == HP_ERR_INVALID_ARG
+    first = 64 << 10
+    seen_nomem = False
+    while True:
+        assert lib.hp_test_arena_first(h, first) == 0
+        try:
+            part, cut = ctx.partition_graph(g, 16)
+        except hp.HpError as e:
+            assert e.code == HP_ERR_NOMEM
+            assert lib.hp_test_arena_restarts(h) == 3
+            seen_nomem = True
+            first *= 2
+            assert first <= 1 << 30
+            continue
+        break
+    assert seen_nomem
+    assert lib.hp_test_arena_restarts(h) >= 1
+    assert np.array_equal(part, ref_part) and cut == ref_cut
+    # an override cleared before use leaves the next call on the estimate
+    assert lib.hp_test_arena_first(h, 1 << 20) == 0
+    assert lib.hp_test_arena_first(h, 0) == 0
+    part, cut = ctx.partition_graph(g, 16)
+    assert lib.hp_test_arena_restarts(h) == 0
+    assert np.array_equal(part, ref_part) and cut == ref_cut
 
 
 def test_invalid_inputs(ctx):
