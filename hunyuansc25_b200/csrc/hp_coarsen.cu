@@ -79,6 +79,25 @@ struct BestCand {
     }
 };
 
+// The best candidate of the warp in hp::better order (heavier edge, then lower
+// tie key, then lower id) among the lanes holding one (bu >= 0), in every lane:
+// three warp reductions (redux.sync) in place of a shuffle butterfly.  Edge
+// weights are positive, so w + 1 > 0 marks a held candidate.
+__device__ __forceinline__ void warp_best(int32_t &bu, int32_t &bw, uint32_t &bh)
+{
+    const unsigned wk = bu >= 0 ? (unsigned)bw + 1u : 0u;
+    const unsigned wm = __reduce_max_sync(HP_FULL_MASK, wk);
+    const bool c1 = wm != 0u && wk == wm;
+    const unsigned hm = __reduce_min_sync(HP_FULL_MASK, c1 ? bh : 0xffffffffu);
+    const bool c2 = c1 && bh == hm;
+    const unsigned um = __reduce_min_sync(HP_FULL_MASK, c2 ? (unsigned)bu : 0xffffffffu);
+    if (wm == 0u) {
+        bu = -1; bw = 0; bh = 0u;
+        return;
+    }
+    bu = (int32_t)um; bw = (int32_t)(wm - 1u); bh = hm;
+}
+
 constexpr int PREF_BATCH = 4;
 
 template <bool ELIG>
@@ -153,13 +172,7 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
         best.finish(lkey, v);
         int32_t bu = best.u, bw = best.w;
         uint32_t bh = best.h;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
-            int32_t ow = __shfl_xor_sync(HP_FULL_MASK, bw, o);
-            uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
-            if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; }
-        }
+        warp_best(bu, bw, bh);
         if (lane == 0) pref[v] = bu;
     }
 }
@@ -173,7 +186,14 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
 // away rescans its row.  Results equal a full rescan every round.
 constexpr int TOPK = 4;
 
-struct TopList {
+// The TOPK best candidates of a row, kept by a whole warp: every lane holds the
+// same list, best first (u = -1 in the unused slots).  Entries are offered one
+// per lane; only those that can enter (weight at least the last held weight once
+// the list is full) are hashed and merged, best first by warp_best, until the
+// best remaining one cannot enter -- so after the first few batches of a row an
+// offer costs one ballot.  The list is the TOPK best of everything offered,
+// whatever the order of the offers (hp::better is a total order on distinct ids).
+struct WarpTop {
     int32_t u[TOPK], w[TOPK];
     uint32_t h[TOPK];
     __device__ __forceinline__ void init()
@@ -181,71 +201,68 @@ struct TopList {
 #pragma unroll
         for (int q = 0; q < TOPK; q++) { u[q] = -1; w[q] = 0; h[q] = 0u; }
     }
-    // the tie key is computed only when the candidate can enter the list
-    __device__ __forceinline__ void offer(uint64_t lkey, int32_t v, int32_t cu, int32_t cw)
+    __device__ __forceinline__ bool full() const { return u[TOPK - 1] >= 0; }
+    // the same candidate in every lane; it is better than the last entry or the list is not full
+    __device__ __forceinline__ void insert(int32_t cu, int32_t cw, uint32_t ch)
     {
-        if (u[TOPK - 1] >= 0 && cw < w[TOPK - 1]) return;
-        uint32_t ch = hp::edge_tie(lkey, v, cu);
-        if (u[TOPK - 1] >= 0 && !hp::better(cw, ch, cu, w[TOPK - 1], h[TOPK - 1], u[TOPK - 1])) return;
-        int32_t iu = cu, iw = cw;
 #pragma unroll
         for (int q = 0; q < TOPK; q++) {
-            if (iu >= 0 && (u[q] < 0 || hp::better(iw, ch, iu, w[q], h[q], u[q]))) {
+            if (cu >= 0 && (u[q] < 0 || hp::better(cw, ch, cu, w[q], h[q], u[q]))) {
                 const int32_t tu = u[q], tw = w[q];
                 const uint32_t th = h[q];
-                u[q] = iu; w[q] = iw; h[q] = ch;
-                iu = tu; iw = tw; ch = th;
+                u[q] = cu; w[q] = cw; h[q] = ch;
+                cu = tu; cw = tw; ch = th;
             }
         }
     }
-    __device__ __forceinline__ void head(int ptr, int32_t &hu, int32_t &hw, uint32_t &hh) const
+    // Merges the lanes' candidates (cu < 0: none) whose tie keys are known; all
+    // lanes call.  At most TOPK insertions and one failed test.
+    __device__ __forceinline__ void merge(int32_t cu, int32_t cw, uint32_t ch)
     {
-        hu = -1; hw = 0; hh = 0u;
+        for (;;) {
+            int32_t bu = cu, bw = cw;
+            uint32_t bh = ch;
+            warp_best(bu, bw, bh);
+            if (bu < 0) return;
+            if (full() && !hp::better(bw, bh, bu, w[TOPK - 1], h[TOPK - 1], u[TOPK - 1])) return;
+            insert(bu, bw, bh);
+            if (cu == bu) cu = -1;
+        }
+    }
+    // Offers one entry of v's row per lane (cu < 0: none); all lanes call.
+    __device__ __forceinline__ void offer(uint64_t lkey, int32_t v, int32_t cu, int32_t cw)
+    {
+        const bool c = cu >= 0 && (!full() || cw >= w[TOPK - 1]);
+        if (!__ballot_sync(HP_FULL_MASK, c)) return;
+        merge(c ? cu : -1, cw, c ? hp::edge_tie(lkey, v, cu) : 0u);
+    }
+    // u[q] of lane q (q < TOPK), -1 elsewhere
+    __device__ __forceinline__ int32_t lane_entry() const
+    {
+        const int lane = threadIdx.x & 31;
+        int32_t r = -1;
 #pragma unroll
         for (int q = 0; q < TOPK; q++)
-            if (ptr == q) { hu = u[q]; hw = w[q]; hh = h[q]; }
+            if (lane == q) r = u[q];
+        return r;
     }
 };
 
-// The TOPK best of the 32 lanes' lists, best first, in every lane (out[q] = -1
-// when fewer exist).  Neighbours of a row are distinct, so the maxima agree.
-__device__ __forceinline__ void warp_topk(const TopList &t, int32_t (&out)[TOPK])
+// The entries [j0, e) of v's row, `step` apart per batch of 4 x 32 (the warp's
+// share: j0 and step are the same in all its lanes), offered to the warp's list.
+// The four row loads of a lane, then their eligibility gathers, are in flight
+// together.
+__device__ __forceinline__ void scan_row_top(WarpTop &t, int32_t v, int32_t j0, int32_t e, int32_t step,
+                                             const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt,
+                                             const int32_t *__restrict__ elig, int32_t wv, uint64_t lkey,
+                                             int64_t maxvwgt)
 {
     const int lane = threadIdx.x & 31;
-    int ptr = 0;
-#pragma unroll
-    for (int r = 0; r < TOPK; r++) {
-        int32_t bu, bw;
-        uint32_t bh;
-        t.head(ptr, bu, bw, bh);
-        int bl = lane;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
-            const int32_t ow = __shfl_xor_sync(HP_FULL_MASK, bw, o);
-            const uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
-            const int ol = __shfl_xor_sync(HP_FULL_MASK, bl, o);
-            if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; bl = ol; }
-        }
-        out[r] = bu;
-        if (bu >= 0 && lane == bl) ptr++;
-    }
-}
-
-// One thread's share of a row (entries j0, j0 + stride, ... below e) offered to
-// its top list: four entries at a time, so that the row loads and then the
-// eligibility gathers of the four are in flight together.  The list keeps the
-// best TOPK by hp::better whatever the order of the offers.
-__device__ __forceinline__ void scan_row_topk(TopList &t, int32_t v, int32_t j0, int32_t e, int32_t stride,
-                                              const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt,
-                                              const int32_t *__restrict__ elig, int32_t wv, uint64_t lkey,
-                                              int64_t maxvwgt)
-{
-    for (int32_t j = j0; j < e; j += 4 * stride) {
+    for (int32_t j = j0; j < e; j += step) {
         int32_t u[4], w[4], eu[4];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const int32_t jj = j + q * stride;
+            const int32_t jj = j + lane + 32 * q;
             const bool in = jj < e;
             u[q] = in ? adjncy[jj] : v;
             w[q] = in ? adjwgt[jj] : 0;
@@ -254,9 +271,9 @@ __device__ __forceinline__ void scan_row_topk(TopList &t, int32_t v, int32_t j0,
         for (int q = 0; q < 4; q++) eu[q] = u[q] != v ? elig[u[q]] : INT_MAX;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            if (eu[q] == INT_MAX) continue;                     // matched, or no entry
-            if ((int64_t)wv + eu[q] > maxvwgt) continue;        // weight cap
-            t.offer(lkey, v, u[q], w[q]);
+            // matched (or no entry), or over the weight cap: not a candidate
+            const bool ok = eu[q] != INT_MAX && (int64_t)wv + eu[q] <= maxvwgt;
+            t.offer(lkey, v, ok ? u[q] : -1, w[q]);
         }
     }
 }
@@ -293,18 +310,20 @@ pref_big_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restrict
             const int32_t cp = cached_proposal(cand, v, elig);
             if (cp != -2) { if (lane == 0) pref[v] = cp; continue; }
         }
-        const int32_t wv = vwgt[v];
-        TopList t;
+        WarpTop t;
         t.init();
-        scan_row_topk(t, v, xadj[v] + lane, xadj[v + 1], 32, adjncy, adjwgt, elig, wv, lkey, maxvwgt);
-        int32_t top[TOPK];
-        warp_topk(t, top);
-        if (lane < TOPK) cand[(int64_t)v * TOPK + lane] = top[lane];
-        if (lane == 0) pref[v] = top[0];
+        scan_row_top(t, v, xadj[v], xadj[v + 1], 4 * 32, adjncy, adjwgt, elig, vwgt[v], lkey, maxvwgt);
+        const int32_t mine = t.lane_entry();
+        if (lane < TOPK) cand[(int64_t)v * TOPK + lane] = mine;
+        if (lane == 0) pref[v] = t.u[0];
     }
 }
 
-__global__ void __launch_bounds__(512)
+// CTA per row for rows above match_cta_deg: each warp keeps the list of its
+// batches of the row, then warp 0 merges the warps' lists.
+constexpr int HUGE_TOPK_THREADS = 512;
+
+__global__ void __launch_bounds__(HUGE_TOPK_THREADS)
 pref_huge_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                       const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                       const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ vwgt,
@@ -313,8 +332,9 @@ pref_huge_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restric
                       const unsigned long long *made_prev)
 {
     if (made_prev && *made_prev == 0ull) return;
-    __shared__ int32_t su[16][TOPK], sw[16][TOPK];
-    __shared__ uint32_t sh[16][TOPK];
+    constexpr int NW = HUGE_TOPK_THREADS / 32;
+    __shared__ int32_t su[TOPK][NW], sw[TOPK][NW];
+    __shared__ uint32_t sh[TOPK][NW];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int32_t cnt = *d_count;
     for (int32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
@@ -324,40 +344,26 @@ pref_huge_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restric
             const int32_t cp = cached_proposal(cand, v, elig);
             if (cp != -2) { if (threadIdx.x == 0) pref[v] = cp; continue; }
         }
-        const int32_t wv = vwgt[v];
-        TopList t;
+        WarpTop t;
         t.init();
-        scan_row_topk(t, v, xadj[v] + threadIdx.x, xadj[v + 1], blockDim.x, adjncy, adjwgt, elig, wv, lkey, maxvwgt);
-        // per warp: its TOPK best, with their weights and keys (taken from the lists)
-        {
-            int32_t top[TOPK];
-            warp_topk(t, top);
-            // the owner lane of each winner publishes its (w, h); a winner is in
-            // exactly one lane's list
+        scan_row_top(t, v, xadj[v] + 4 * 32 * wid, xadj[v + 1], 4 * 32 * NW, adjncy, adjwgt, elig, vwgt[v], lkey,
+                     maxvwgt);
+        if (lane == 0) {
 #pragma unroll
-            for (int q = 0; q < TOPK; q++) {
-#pragma unroll
-                for (int s2 = 0; s2 < TOPK; s2++)
-                    if (top[q] >= 0 && t.u[s2] == top[q]) { sw[wid][q] = t.w[s2]; sh[wid][q] = t.h[s2]; }
-                if (lane == 0) su[wid][q] = top[q];
-            }
+            for (int q = 0; q < TOPK; q++) { su[q][wid] = t.u[q]; sw[q][wid] = t.w[q]; sh[q][wid] = t.h[q]; }
         }
         __syncthreads();
         if (wid == 0) {
-            TopList m;
+            WarpTop m;
             m.init();
-            if (lane < (int)(blockDim.x >> 5)) {
 #pragma unroll
-                for (int q = 0; q < TOPK; q++) {
-                    m.u[q] = su[lane][q];
-                    m.w[q] = m.u[q] >= 0 ? sw[lane][q] : 0;
-                    m.h[q] = m.u[q] >= 0 ? sh[lane][q] : 0u;
-                }
+            for (int q = 0; q < TOPK; q++) {
+                const bool in = lane < NW;
+                m.merge(in ? su[q][lane] : -1, in ? sw[q][lane] : 0, in ? sh[q][lane] : 0u);
             }
-            int32_t top[TOPK];
-            warp_topk(m, top);
-            if (lane < TOPK) cand[(int64_t)v * TOPK + lane] = top[lane];
-            if (lane == 0) pref[v] = top[0];
+            const int32_t mine = m.lane_entry();
+            if (lane < TOPK) cand[(int64_t)v * TOPK + lane] = mine;
+            if (lane == 0) pref[v] = m.u[0];
         }
         __syncthreads();
     }
@@ -432,13 +438,7 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
         best.finish(lkey, v);
         int32_t bu = best.u, bw = best.w;
         uint32_t bh = best.h;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
-            int32_t ow = __shfl_xor_sync(HP_FULL_MASK, bw, o);
-            uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
-            if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; }
-        }
+        warp_best(bu, bw, bh);
         if (lane == 0) { su[wid] = bu; sw[wid] = bw; sh[wid] = bh; }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -1462,13 +1462,7 @@ __device__ int32_t ms_best(bool act, int32_t v, const int32_t *__restrict__ xadj
         best.finish(lkey, sv);
         int32_t bu = best.u, bw = best.w;
         uint32_t bh = best.h;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const int32_t ou = __shfl_xor_sync(HP_FULL_MASK, bu, o);
-            const int32_t ow = __shfl_xor_sync(HP_FULL_MASK, bw, o);
-            const uint32_t oh = __shfl_xor_sync(HP_FULL_MASK, bh, o);
-            if (ou >= 0 && (bu < 0 || hp::better(ow, oh, ou, bw, bh, bu))) { bu = ou; bw = ow; bh = oh; }
-        }
+        warp_best(bu, bw, bh);
         if (lane == src) res = bu;
     }
     return res;
@@ -1703,7 +1697,7 @@ int match_level(hp_context *c, HpLevel &g, int32_t level, int64_t maxvwgt, int32
                   g.vwgt, g.match, elig, pref, lkey, maxvwgt, prev, tn.match_warp_deg);
         HP_LAUNCH(c, pref_big_topk_kernel, persistent_grid(c), 256, 0, big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt,
                   g.vwgt, g.match, elig, pref, cand, lkey, maxvwgt, prev);
-        HP_LAUNCH(c, pref_huge_topk_kernel, (unsigned)(2 * c->sm_count), 512, 0, huge, d_hugecnt, g.xadj,
+        HP_LAUNCH(c, pref_huge_topk_kernel, (unsigned)(2 * c->sm_count), HUGE_TOPK_THREADS, 0, huge, d_hugecnt, g.xadj,
                   g.adjncy, g.adjwgt, g.vwgt, g.match, elig, pref, cand, lkey, maxvwgt, prev);
         HP_LAUNCH(c, commit_kernel, blocks_for(n), 256, 0, n, g.match, pref, elig, &sc[2 + r], prev);
         hp_prof_end(c, tok, r == 0 ? HP_PROF_MATCH : HP_PROF_MATCH_MORE, r == 0 ? round_bytes : later_round_bytes);
