@@ -98,6 +98,7 @@ TUNING_FIELDS = [
     "small_match_n",
     "contract_hybrid",
     "apply_chunk_deg",
+    "pdl",
 ]
 
 TUNING_DEFAULTS = {
@@ -119,6 +120,7 @@ TUNING_DEFAULTS = {
     "small_match_n": 8192,
     "contract_hybrid": 1,
     "apply_chunk_deg": 4096,
+    "pdl": 1,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -146,6 +148,7 @@ def tuning_violation(t: dict):
         ("small_match_n", 0, 8192),
         ("contract_hybrid", 0, 1),
         ("apply_chunk_deg", t["gain_thread_deg"], TUNE_DEG_MAX),
+        ("pdl", 0, 1),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -154,7 +157,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 6)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 5)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

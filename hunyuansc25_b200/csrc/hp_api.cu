@@ -32,6 +32,7 @@ __global__ void validate_vertices_kernel(int32_t n, int64_t m, const int32_t *__
                                          const int32_t *__restrict__ vwgt, unsigned *status,
                                          unsigned long long *maxdeg)
 {
+    hp::pdl_wait();
     bool bad = false;
     int32_t dmax = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
@@ -76,6 +77,7 @@ validate_edges_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj,
                       const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt, unsigned *status,
                       int32_t *__restrict__ unsorted, unsigned long long *sums)
 {
+    hp::pdl_wait();
     __shared__ int32_t owner[VE_TILE];
     __shared__ int32_t s_warp[VE_THREADS / 32];
     __shared__ int32_t s_v0;
@@ -120,6 +122,7 @@ __global__ void __launch_bounds__(256)
 dup_check_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                  const int32_t *__restrict__ unsorted, unsigned long long *table, uint64_t mask, unsigned *status)
 {
+    hp::pdl_wait();
     const int lane = threadIdx.x & 31;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     bool dup = false;
@@ -142,6 +145,7 @@ dup_check_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__r
 
 __global__ void sum_kernel(int64_t n, const int32_t *__restrict__ a, unsigned long long *out)
 {
+    hp::pdl_wait();
     long long acc = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         acc += a[i];
@@ -151,6 +155,7 @@ __global__ void sum_kernel(int64_t n, const int32_t *__restrict__ a, unsigned lo
 __global__ void final_pw_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__restrict__ vwgt,
                                 unsigned long long *pw, int32_t k, unsigned *status)
 {
+    hp::pdl_wait();
     extern __shared__ unsigned long long fpw[];
     const bool use_s = k <= 2048;
     if (use_s) {
@@ -172,6 +177,7 @@ __global__ void final_pw_kernel(int32_t n, const int32_t *__restrict__ where, co
 
 __global__ void fill_ones_kernel(int64_t n, int32_t *p)
 {
+    hp::pdl_wait();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = 1;
 }
@@ -618,6 +624,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->small_match_n = 8192;
     t->contract_hybrid = 1;
     t->apply_chunk_deg = 4096;
+    t->pdl = 1;
 }
 
 namespace {
@@ -643,6 +650,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.small_match_n, 0, HP_TUNE_SMALL_MATCH_MAX)) return "small_match_n";
     if (!in(t.contract_hybrid, 0, 1)) return "contract_hybrid";
     if (!in(t.apply_chunk_deg, t.gain_thread_deg, HP_TUNE_DEG_MAX)) return "apply_chunk_deg";
+    if (!in(t.pdl, 0, 1)) return "pdl";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;
@@ -1050,6 +1058,7 @@ HP_API int hp_edgecut_device(hp_context *ctx, int32_t nvtxs, const int32_t *d_xa
 // predecessor as zero, so the kernel ends by itself.
 __global__ void wait_expiry_kernel(unsigned long long *tile_status, unsigned *status, int32_t *excl)
 {
+    hp::pdl_wait();
     const int32_t e = hp::lookback_exclusive(tile_status, 1, 5, status);
     if (threadIdx.x == 0) *excl = e;
 }

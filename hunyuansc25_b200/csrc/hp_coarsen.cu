@@ -107,6 +107,7 @@ pref_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__
                   const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
                   uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev, int32_t warp_deg)
 {
+    hp::pdl_wait();
     if (made_prev && *made_prev == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
@@ -149,6 +150,7 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
                 const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
                 uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
 {
+    hp::pdl_wait();
     if (made_prev && *made_prev == 0ull) return;
     const int lane = threadIdx.x & 31;
     const int32_t cnt = *d_count;
@@ -299,6 +301,7 @@ pref_big_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restrict
                      int32_t *__restrict__ pref, int32_t *__restrict__ cand, uint64_t lkey, int64_t maxvwgt,
                      const unsigned long long *made_prev)
 {
+    hp::pdl_wait();
     if (made_prev && *made_prev == 0ull) return;
     const int lane = threadIdx.x & 31;
     const int32_t cnt = *d_count;
@@ -331,6 +334,7 @@ pref_huge_topk_kernel(const int32_t *__restrict__ list, const int32_t *__restric
                       int32_t *__restrict__ pref, int32_t *__restrict__ cand, uint64_t lkey, int64_t maxvwgt,
                       const unsigned long long *made_prev)
 {
+    hp::pdl_wait();
     if (made_prev && *made_prev == 0ull) return;
     constexpr int NW = HUGE_TOPK_THREADS / 32;
     __shared__ int32_t su[TOPK][NW], sw[TOPK][NW];
@@ -373,6 +377,7 @@ __global__ void __launch_bounds__(256)
 commit_kernel(int32_t n, int32_t *__restrict__ match, const int32_t *__restrict__ pref,
               int32_t *__restrict__ elig, unsigned long long *made_cur, const unsigned long long *made_prev)
 {
+    hp::pdl_wait();
     if (made_prev && *made_prev == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int made = 0;
@@ -392,6 +397,7 @@ big_list_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t *list, int3
                 int32_t *huge, int32_t *d_huge, const int32_t *__restrict__ vwgt, int32_t *__restrict__ elig,
                 int32_t warp_deg, int32_t cta_deg)
 {
+    hp::pdl_wait();
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int32_t d = 0;
     if (v < n) {
@@ -414,6 +420,7 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
                  const int32_t *__restrict__ match, const int32_t *__restrict__ elig, int32_t *__restrict__ pref,
                  uint64_t lkey, int64_t maxvwgt, const unsigned long long *made_prev)
 {
+    hp::pdl_wait();
     if (made_prev && *made_prev == 0ull) return;
     __shared__ int32_t su[16], sw[16];
     __shared__ uint32_t sh[16];
@@ -455,6 +462,7 @@ pref_huge_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
 __global__ void __launch_bounds__(256)
 count_matched_kernel(int32_t n, const int32_t *__restrict__ match, unsigned long long *out)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     hp::block_add_to<256>((v < n && match[v] != -1) ? 1 : 0, out);
 }
@@ -469,6 +477,7 @@ __global__ void __launch_bounds__(256)
 client_flag_kernel(int32_t n, const int32_t *__restrict__ match, const int32_t *__restrict__ hub,
                    int32_t *__restrict__ flags)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < n) flags[v] = match[v] == -1 && hub[v] >= 0;
 }
@@ -477,6 +486,7 @@ __global__ void __launch_bounds__(256)
 client_keys_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                    const int32_t *__restrict__ hub, int32_t *__restrict__ keys)
 {
+    hp::pdl_wait();
     const int32_t cnt = *d_count;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x)
         keys[i] = hub[list[i]];
@@ -487,6 +497,7 @@ pair_clients_kernel(const int32_t *__restrict__ keys, const int32_t *__restrict_
                     const int32_t *__restrict__ d_count, const int32_t *__restrict__ vwgt,
                     int32_t *__restrict__ match, int64_t maxvwgt)
 {
+    hp::pdl_wait();
     const int32_t cnt = *d_count;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt; i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t h = keys[i];
@@ -506,6 +517,7 @@ __global__ void __launch_bounds__(256)
 flag_unmatched_kernel(int32_t n, const int32_t *__restrict__ xadj,
                       const int32_t *__restrict__ match, int32_t *__restrict__ flags, int isolated_only)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     int f = match[v] == -1;
@@ -517,6 +529,7 @@ __global__ void __launch_bounds__(256)
 pair_list_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_count,
                  const int32_t *__restrict__ vwgt, int32_t *__restrict__ match, int64_t maxvwgt)
 {
+    hp::pdl_wait();
     const int32_t cnt = *d_count;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; 2 * i + 1 < cnt;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -528,6 +541,7 @@ pair_list_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d
 __global__ void __launch_bounds__(256)
 finalize_match_kernel(int32_t n, int32_t *__restrict__ match, int32_t *__restrict__ leader_flag)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     int32_t u = match[v];
@@ -553,6 +567,7 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
                     int32_t *__restrict__ maxlen, unsigned long long *__restrict__ long_total,
                     int32_t *__restrict__ small_max, int32_t thread_row, int32_t warp_row, int32_t cta_row)
 {
+    hp::pdl_wait();
     // no early exit: the list appends and maxima are aggregated per warp
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     bool lead = false;
@@ -608,6 +623,7 @@ __global__ void __launch_bounds__(256)
 row_weight_range_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjwgt,
                         unsigned *status)
 {
+    hp::pdl_wait();
     const int lane = threadIdx.x & 31;
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     const int32_t b = v < n ? xadj[v] : 0, e = v < n ? xadj[v + 1] : 0;
@@ -722,6 +738,7 @@ contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict_
                          int32_t *__restrict__ cadjwgt, unsigned long long *tile_status, hp::LbCtl *lb,
                          unsigned *status, int32_t thread_row, int wcheck)
 {
+    hp::pdl_wait();
     extern __shared__ unsigned long long asm_stage[];                      // ASM_TILE * XN
     uint8_t *s_row = reinterpret_cast<uint8_t *>(asm_stage + ASM_TILE * XN);   // tile row of each entry
     __shared__ int4 s_ri[ASM_TILE];
@@ -835,6 +852,7 @@ copy_long_rows_kernel(const int32_t *__restrict__ lists, const int32_t *__restri
                       const int32_t *__restrict__ cxadj, const int32_t *__restrict__ tk,
                       const int32_t *__restrict__ tw, int32_t *__restrict__ cadjncy, int32_t *__restrict__ cadjwgt)
 {
+    hp::pdl_wait();
     const int lane = CTA ? threadIdx.x : (threadIdx.x & 31);
     const int width = CTA ? blockDim.x : 32;
     const int64_t total = CTA ? (int64_t)counts[1] + counts[2] : (int64_t)counts[0];
@@ -1102,6 +1120,7 @@ contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__re
                            const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
                            int32_t *__restrict__ ucnt, int kbits, int wcheck, unsigned *status)
 {
+    hp::pdl_wait();
     __shared__ unsigned long long sA[WROW_WARPS][WROW_MAX], sB[WROW_WARPS][WROW_MAX];
     __shared__ int32_t sH[WROW_WARPS][256];
     const int wid = threadIdx.x >> 5;
@@ -1138,6 +1157,7 @@ contract_cta_radix_kernel(const int32_t *__restrict__ list, const int32_t *__res
                           const int32_t *__restrict__ toff, int32_t *__restrict__ tk, int32_t *__restrict__ tw,
                           int32_t *__restrict__ ucnt, int kbits, int32_t min_len, int wcheck, unsigned *status)
 {
+    hp::pdl_wait();
     extern __shared__ unsigned long long dsm[];
     unsigned long long *A = dsm, *B = dsm + CAP;
     int32_t *hist = (int32_t *)(dsm + 2 * CAP);
@@ -1206,6 +1226,7 @@ contract_hybrid_kernel(const int32_t *__restrict__ list, const int32_t *__restri
                        int32_t *__restrict__ ucnt, int kbits, int32_t min_len, int32_t *__restrict__ spill,
                        int32_t *d_nspill, int wcheck, unsigned *status)
 {
+    hp::pdl_wait();
     extern __shared__ unsigned long long hy_smem[];
     unsigned long long *A = hy_smem, *B = hy_smem + HY_COLD;
     int32_t *acc = reinterpret_cast<int32_t *>(hy_smem + 2 * HY_COLD);
@@ -1326,6 +1347,7 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
                       int32_t *slab_w, unsigned *slab_bm, unsigned *slab_bm2, int32_t ratio, int32_t min_len,
                       int wcheck, unsigned *status)
 {
+    hp::pdl_wait();
     extern __shared__ int32_t dsm_acc[];
     __shared__ int32_t s_scan[NT / 32 + 2];
     __shared__ long long s64[NT / 32];
@@ -1511,6 +1533,7 @@ match_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *_
                    int32_t *__restrict__ cmap, int32_t *K, int32_t *V, int32_t *K2, int32_t *V2, uint64_t lkey,
                    int64_t maxvwgt, int rounds, int key_bits)
 {
+    hp::pdl_wait();
     extern __shared__ int32_t ms_sh[];
     int32_t *tab = ms_sh;                                        // block radix sort
     int32_t *s_match = tab + hp::block_sort_ints(MS_THREADS);

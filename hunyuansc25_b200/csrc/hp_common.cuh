@@ -22,6 +22,16 @@
 
 namespace hp {
 
+// First statement of every kernel of the library: when the kernel was launched
+// as a programmatic dependent of the previous kernel in its stream (hp_tuning.pdl),
+// it may already be resident while that kernel drains; this waits until the
+// previous kernel has completed and its writes are visible.  Without such a
+// launch it returns at once.
+__device__ __forceinline__ void pdl_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 // splitmix64 finaliser (Vigna): the matching tie-break hash.
 __host__ __device__ __forceinline__ uint64_t mix64(uint64_t z)
 {

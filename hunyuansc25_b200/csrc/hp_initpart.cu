@@ -75,6 +75,7 @@ trial_warp_kernel(const SubInfo *__restrict__ subs, const int32_t *__restrict__ 
                   int32_t starts, int32_t fm_passes, int64_t *tr_cut, int64_t *tr_viol,
                   int use_smem, int64_t smem_per_warp)
 {
+    hp::pdl_wait();
     extern __shared__ __align__(16) char tsm[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int32_t t = blockIdx.x * (blockDim.x >> 5) + wib;
@@ -274,6 +275,7 @@ trial_cta_kernel(const SubInfo *__restrict__ subs, const int32_t *__restrict__ t
                  const int32_t *__restrict__ fwgt, const int32_t *__restrict__ fvwgt, char *slab_base,
                  int32_t starts, int32_t fm_passes, int64_t *tr_cut, int64_t *tr_viol, int use_smem)
 {
+    hp::pdl_wait();
     extern __shared__ __align__(16) char tsm[];
     __shared__ int32_t s_red[TC_WARPS], s_key[TC_WARPS];
     __shared__ int32_t s_scan[TC_WARPS + 2];
@@ -470,6 +472,7 @@ select_kernel(const SubInfo *__restrict__ subs, const int64_t *__restrict__ tr_c
               const int32_t *__restrict__ fvwgt, int32_t *__restrict__ side,
               int64_t *__restrict__ res /* per sub: n0, tv0 */)
 {
+    hp::pdl_wait();
     __shared__ long long s_v[8], s_c[8];
     __shared__ int s_t[8];
     __shared__ int s_best;
@@ -524,6 +527,7 @@ __global__ void __launch_bounds__(256)
 sub_of_kernel(const SubInfo *__restrict__ subs, int32_t *__restrict__ sub_of,
               int32_t *__restrict__ flag0)
 {
+    hp::pdl_wait();
     const SubInfo S = subs[blockIdx.x];
     for (int i = threadIdx.x; i < S.n; i += blockDim.x) sub_of[S.vbeg + i] = blockIdx.x;
     (void)flag0;
@@ -532,6 +536,7 @@ sub_of_kernel(const SubInfo *__restrict__ subs, int32_t *__restrict__ sub_of,
 __global__ void __launch_bounds__(256)
 side_flag_kernel(int32_t nf, const int32_t *__restrict__ side, int32_t *__restrict__ f0)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < nf) f0[v] = side[v] == 0;
 }
@@ -545,6 +550,7 @@ split_count_kernel(int32_t nf, const SubInfo *__restrict__ subs, const int32_t *
                    const int32_t *__restrict__ fadj, const int32_t *__restrict__ label,
                    int32_t *__restrict__ newid, int32_t *__restrict__ ndeg, int32_t *__restrict__ where_out)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nf) return;
     const int32_t s = sub_of[v];
@@ -571,6 +577,7 @@ split_write_kernel(int32_t nf, const SubInfo *__restrict__ subs, const int32_t *
                    const int32_t *__restrict__ nxadj, int32_t *__restrict__ nadj,
                    int32_t *__restrict__ nwgt, int32_t *__restrict__ nvwgt, int32_t *__restrict__ nlabel)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nf) return;
     const int32_t nid = newid[v];
@@ -593,12 +600,14 @@ split_write_kernel(int32_t nf, const SubInfo *__restrict__ subs, const int32_t *
 
 __global__ void assign_all_kernel(int32_t n, int32_t *where, int32_t value)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < n) where[v] = value;
 }
 
 __global__ void copy_kernel(int64_t n, const int32_t *src, int32_t *dst)
 {
+    hp::pdl_wait();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         dst[i] = src[i];
 }

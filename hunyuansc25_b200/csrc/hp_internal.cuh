@@ -135,6 +135,29 @@ template <class T> inline T *ralloc_t(hp_context *c, int64_t n) { return (T *)hp
 
 #define HP_CHECK_OOM(c) do { if ((c)->oom) return HP_ERR_NOMEM; } while (0)
 
+// Launch of a kernel on the context's stream.  With hp_tuning.pdl the launch is a
+// programmatic dependent of the stream's previous kernel: the hardware may start
+// it while that kernel drains (the launch latency overlaps its tail), and every
+// kernel of the library begins with hp::pdl_wait(), so nothing it reads or writes
+// is touched before the previous kernel has completed -- the order of effects is
+// exactly that of a plain launch.
+template <class... P, class... A>
+inline cudaError_t hp_launch_kernel(const hp_context *c, void (*kernel)(P...), unsigned grid, unsigned block,
+                                    size_t smem, A &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = c->tune.pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 // Count and check every kernel launch.  Once the arena has run out nothing more is
 // launched (a pointer allocated after that is null): the call unwinds with
 // HP_ERR_NOMEM and partition_common retries with a larger arena.
@@ -142,9 +165,10 @@ template <class T> inline T *ralloc_t(hp_context *c, int64_t n) { return (T *)hp
     do {                                                                                    \
         if ((ctx)->oom) return HP_ERR_NOMEM;                                                \
         if ((grid) > 0) {                                                                   \
-            kernel<<<(grid), (block), (smem), (ctx)->stream>>>(__VA_ARGS__);                \
+            cudaError_t e__ = hp_launch_kernel((ctx), kernel, (unsigned)(grid), (unsigned)(block), \
+                                               (size_t)(smem), __VA_ARGS__);                \
             (ctx)->launches++;                                                              \
-            cudaError_t e__ = cudaGetLastError();                                           \
+            if (e__ == cudaSuccess) e__ = cudaGetLastError();                               \
             if (e__ != cudaSuccess) {                                                       \
                 fprintf(stderr, "hp: launch %s failed: %s\n", #kernel, cudaGetErrorString(e__)); \
                 return HP_ERR_CUDA;                                                         \

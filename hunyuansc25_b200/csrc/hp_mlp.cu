@@ -55,6 +55,7 @@ mlp_sample_grad_kernel(const float *__restrict__ P, const float *__restrict__ X,
                        const int32_t *__restrict__ idx, int64_t b0, int64_t nb, float scale,
                        float *__restrict__ G)
 {
+    hp::pdl_wait();
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (s >= nb) return;
     const int64_t r = idx ? idx[b0 + s] : b0 + s;
@@ -90,6 +91,7 @@ mlp_sample_grad_kernel(const float *__restrict__ P, const float *__restrict__ X,
 __global__ void __launch_bounds__(MLP_RED)
 mlp_reduce_kernel(const float *__restrict__ G, int64_t nb, float *__restrict__ out, float *__restrict__ loss)
 {
+    hp::pdl_wait();
     __shared__ float sw[MLP_RED / 32];
     const int p = blockIdx.x;
     const float *row = G + (int64_t)p * nb;
@@ -125,6 +127,7 @@ int mlp_grad_det(cudaStream_t st, const float *P, const float *X, const float *Y
 __global__ void adam_kernel(float *__restrict__ P, const float *__restrict__ g, float *__restrict__ m,
                             float *__restrict__ v, float lr, float b1, float b2, float eps, float c1, float c2)
 {
+    hp::pdl_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= HP_MLP_NPARAM) return;
     const float gi = g[i];
@@ -141,6 +144,7 @@ __global__ void __launch_bounds__(128)
 mlp_infer_kernel(const float *__restrict__ P, const float *__restrict__ X, int64_t n, float *__restrict__ out,
                  int tensor)
 {
+    hp::pdl_wait();
     __shared__ hp::MlpSmem sm;
     hp::mlp_load_smem(sm, P);
     __syncthreads();

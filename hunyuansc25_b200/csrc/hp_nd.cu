@@ -61,6 +61,7 @@ nd_boundary_kernel(int64_t N, Tier t, const int64_t *__restrict__ vtx, const int
                    const int32_t *__restrict__ mode, const int32_t *__restrict__ where, int8_t *__restrict__ bnd,
                    int32_t *__restrict__ bcnt)
 {
+    hp::pdl_wait();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     int key = -1;
     if (i < N) {
@@ -90,6 +91,7 @@ nd_separator_kernel(int64_t N, Tier t, const int64_t *__restrict__ vtx, const in
                     const int32_t *__restrict__ mode, const int32_t *__restrict__ where,
                     const int8_t *__restrict__ bnd, const int32_t *__restrict__ bcnt, int32_t *__restrict__ side)
 {
+    hp::pdl_wait();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int32_t g = t.vsub[i];
@@ -117,6 +119,7 @@ nd_count_kernel(int64_t N, Tier t, const int64_t *__restrict__ vtx, const int64_
                 const int32_t *__restrict__ side, int32_t *__restrict__ fl, int32_t *__restrict__ fr,
                 int32_t *__restrict__ fs, int32_t *__restrict__ cl, int32_t *__restrict__ cr)
 {
+    hp::pdl_wait();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int32_t s = side[i];
@@ -143,6 +146,7 @@ __global__ void nd_sizes_kernel(int32_t G, const int64_t *__restrict__ vtx, cons
                                 const int32_t *__restrict__ scl, const int32_t *__restrict__ scr,
                                 int32_t *__restrict__ sizes)
 {
+    hp::pdl_wait();
     const int32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= G) return;
     const int64_t a = vtx[g], b = vtx[g + 1];
@@ -161,6 +165,7 @@ nd_number_kernel(int64_t N, Tier t, const int64_t *__restrict__ vtx, const int32
                  const int32_t *__restrict__ hi, const int32_t *__restrict__ side, const int32_t *__restrict__ ss,
                  const int32_t *__restrict__ sizes, int32_t *__restrict__ iperm)
 {
+    hp::pdl_wait();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int32_t g = t.vsub[i];
@@ -183,6 +188,7 @@ nd_split_kernel(int64_t N, Tier t, const int64_t *__restrict__ vtx, const int64_
                 const int32_t *__restrict__ scl, const int32_t *__restrict__ scr, const int32_t *__restrict__ child,
                 Tier nt, const int64_t *__restrict__ nvtx, const int64_t *__restrict__ nedg)
 {
+    hp::pdl_wait();
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= N) return;
     const int32_t s = side[i];
@@ -216,6 +222,7 @@ nd_split_kernel(int64_t N, Tier t, const int64_t *__restrict__ vtx, const int64_
 __global__ void nd_close_kernel(int32_t G, Tier nt, const int64_t *__restrict__ nvtx,
                                 const int64_t *__restrict__ nedg)
 {
+    hp::pdl_wait();
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= G) return;
     nt.xadj[nvtx[c + 1] + c] = (int32_t)(nedg[c + 1] - nedg[c]);
@@ -229,6 +236,7 @@ __global__ void __launch_bounds__(ND_LEAF_THREADS)
 nd_leaf_kernel(const int32_t *__restrict__ leaves, Tier t, const int64_t *__restrict__ vtx,
                const int64_t *__restrict__ edg, const int32_t *__restrict__ hi, int32_t *__restrict__ iperm)
 {
+    hp::pdl_wait();
     __shared__ unsigned long long adj[ND_LEAF][ND_W];
     __shared__ unsigned long long alive[ND_W];
     __shared__ unsigned long long s_key[ND_LEAF_THREADS / 32];

@@ -35,6 +35,7 @@ inline unsigned nblk(int64_t n, int b = 256) { return (unsigned)std::max<int64_t
 __global__ void project_kernel(int32_t n, const int32_t *__restrict__ cmap,
                                const int32_t *__restrict__ cwhere, int32_t *__restrict__ where)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < n) where[v] = cwhere[cmap[v]];
 }
@@ -47,6 +48,7 @@ __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int
                                 int32_t *__restrict__ cap, int32_t *big, int32_t *huge, int32_t *d_bigcnt,
                                 int32_t bigd, int32_t huged)
 {
+    hp::pdl_wait();
     // no early exit: the list appends and maxima are aggregated per warp
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int32_t d = 0;
@@ -78,6 +80,7 @@ struct LevelStat {
 __global__ void __launch_bounds__(256)
 level_stats_kernel(int32_t n, const int32_t *__restrict__ xadj, LevelStat *st, int32_t bigd)
 {
+    hp::pdl_wait();
     int32_t nbig = 0, smax = 0, dmax = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t d = xadj[v + 1] - xadj[v];
@@ -158,6 +161,7 @@ gain_thread_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__
                    const int32_t *__restrict__ goff, int32_t *__restrict__ gpart,
                    int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty, int32_t bigd)
 {
+    hp::pdl_wait();
     const int32_t cnt = list ? *d_count : n;
     for (int64_t i0 = blockIdx.x * (int64_t)blockDim.x; i0 < cnt; i0 += (int64_t)gridDim.x * blockDim.x) {
         const int64_t i = i0 + threadIdx.x;
@@ -234,6 +238,7 @@ gain_seg_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
                 const int32_t *__restrict__ goff, int32_t *__restrict__ gpart, int32_t *__restrict__ gconn,
                 int32_t k, int32_t *__restrict__ dirty)
 {
+    hp::pdl_wait();
     gain_seg_rows<S>((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, ((int64_t)gridDim.x * blockDim.x) >> 5,
                      list, *d_count, xadj, adjncy, adjwgt, where, goff, gpart, gconn, k, dirty);
 }
@@ -325,6 +330,7 @@ gain_bigwarp_kernel(const int32_t *__restrict__ list, const int32_t *__restrict_
                     int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty, int32_t bigd,
                     int32_t huged)
 {
+    hp::pdl_wait();
     extern __shared__ int32_t gsm[];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int nwords = (k + 31) >> 5;
@@ -346,6 +352,7 @@ gain_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ 
                   int32_t *__restrict__ gconn, int32_t k, int32_t *__restrict__ dirty, int32_t bigd,
                   int32_t huged, int32_t warp_dense_k)
 {
+    hp::pdl_wait();
     extern __shared__ int32_t dsm[];
     __shared__ int32_t s_scan[NT / 32 + 2];
     int32_t *dw = dsm;
@@ -424,6 +431,7 @@ __global__ void __launch_bounds__(256)
 pw_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t *__restrict__ vwgt,
           unsigned long long *__restrict__ pw, int32_t k)
 {
+    hp::pdl_wait();
     extern __shared__ unsigned long long spw[];
     const bool use_s = k <= 2048;
     if (use_s) {
@@ -448,6 +456,7 @@ rowcut_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__rest
               const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
               unsigned long long *cut2)
 {
+    hp::pdl_wait();
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     long long acc = 0;
@@ -485,6 +494,7 @@ rowcut_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__rest
 __global__ void excess_kernel(int32_t k, const unsigned long long *__restrict__ pw,
                               const int64_t *__restrict__ maxp, long long *out)
 {
+    hp::pdl_wait();
     long long m = LLONG_MIN;
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
         long long e = (long long)pw[p] - maxp[p];
@@ -567,6 +577,7 @@ lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__r
                  const int8_t *__restrict__ lock, int finest, int32_t *__restrict__ dest,
                  int32_t *__restrict__ pregain, unsigned long long *d_ncand, const int32_t *gate, int32_t k)
 {
+    hp::pdl_wait();
     if (gate && *gate != 0) return;   // graph mode: the learned kernel runs this pass
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int cand = 0;
@@ -604,6 +615,7 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
                          int32_t *__restrict__ dest, int32_t *__restrict__ pregain, unsigned long long *d_ncand,
                          const int32_t *gate, int32_t k)
 {
+    hp::pdl_wait();
     if (gate && *gate != 1) return;   // graph mode: the plain kernel runs this pass
     __shared__ hp::MlpSmem sm;
     hp::mlp_load_smem(sm, params);
@@ -654,6 +666,7 @@ log_candidates_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t
                       int32_t *__restrict__ rec_of, float *__restrict__ lx, int32_t *__restrict__ lv,
                       int32_t *__restrict__ ld, int32_t *__restrict__ lacc, unsigned long long *lcount, int64_t cap)
 {
+    hp::pdl_wait();
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= n) return;
     rec_of[v] = -1;
@@ -685,6 +698,7 @@ log_candidates_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t
 __global__ void log_accept_kernel(int32_t n, const int32_t *__restrict__ rec_of, const int8_t *__restrict__ lock,
                                   const unsigned long long *d_ncand, int32_t *__restrict__ lacc)
 {
+    hp::pdl_wait();
     if (*d_ncand == 0ull) return;
     int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v < n && rec_of[v] >= 0) lacc[rec_of[v]] = lock[v];
@@ -696,6 +710,7 @@ __global__ void log_label_kernel(int64_t r0, int64_t r1, const int32_t *__restri
                                  const int32_t *__restrict__ lv, const int32_t *__restrict__ ld,
                                  const int32_t *__restrict__ lacc, float *__restrict__ ly)
 {
+    hp::pdl_wait();
     int64_t r = r0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (r < r1) ly[r] = (lacc[r] && where[lv[r]] == ld[r]) ? 1.f : 0.f;
 }
@@ -786,6 +801,7 @@ afterburner_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int3
                          const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
                          int8_t *__restrict__ lock, const unsigned long long *d_ncand, MoveSink ms, int32_t bigd)
 {
+    hp::pdl_wait();
     if (*d_ncand == 0ull) return;
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     long long c1 = 0;
@@ -818,6 +834,7 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
                        int8_t *__restrict__ lock, const unsigned long long *d_ncand, MoveSink ms,
                        int32_t chunkd)
 {
+    hp::pdl_wait();
     if (*d_ncand == 0ull) return;
     const int lane = threadIdx.x & 31;
     const int32_t cnt = *d_bigcnt;
@@ -864,6 +881,7 @@ hub_plan_kernel(const int32_t *__restrict__ items, const int32_t *__restrict__ d
                 int32_t *__restrict__ plan_off, int32_t *__restrict__ d_plan, unsigned long long *tile_status,
                 int64_t half, hp::LbCtl *lb, unsigned *status)
 {
+    hp::pdl_wait();
     __shared__ int32_t s_scan[PLAN_THREADS / 32 + 2];
     __shared__ int32_t s_excl[2];
     const unsigned epoch = hp::lb_epoch(lb);
@@ -943,6 +961,7 @@ afterburner_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__res
                         const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
                         const unsigned long long *d_ncand, unsigned long long *__restrict__ ab_acc)
 {
+    hp::pdl_wait();
     if (*d_ncand == 0ull) return;
     const int lane = threadIdx.x & 31;
     const int32_t nsel = d_plan[0], nch = d_plan[1];
@@ -964,6 +983,7 @@ __global__ void afterburner_huge_final_kernel(const int32_t *__restrict__ huge, 
                                               const int32_t *__restrict__ where, const int32_t *__restrict__ dest,
                                               MoveSink ms)
 {
+    hp::pdl_wait();
     if (*d_ncand == 0ull) return;
     const int32_t nh = *d_nhuge;
     long long c1 = 0;
@@ -987,6 +1007,7 @@ c_delta_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nm
                const int32_t *__restrict__ dest, int32_t *__restrict__ oldp, int before,
                unsigned long long *d_c, int32_t k)
 {
+    hp::pdl_wait();
     const int64_t nm = (int64_t)*d_nmoves;
     if ((int64_t)blockIdx.x * blockDim.x >= nm) return;   // whole CTA idle (uniform)
     long long acc = 0;
@@ -1108,6 +1129,7 @@ apply_moves_kernel(const int32_t *__restrict__ moves, const unsigned long long *
                    int32_t *__restrict__ big_l, int32_t *counts, int32_t k, int32_t *__restrict__ huge_mv,
                    int32_t *__restrict__ d_nhuge, int32_t bigd, int32_t chunkd)
 {
+    hp::pdl_wait();
     apply_moves_rows((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, ((int64_t)gridDim.x * blockDim.x) >> 5,
                      moves, (int64_t)*d_nmoves, where, dest, vwgt, pw, xadj, adjncy, adjwgt, goff, gconn, dirty,
                      small_l, big_l, counts, k, huge_mv, d_nhuge, bigd, chunkd);
@@ -1125,6 +1147,7 @@ apply_moves_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__res
                         int32_t *__restrict__ gconn, int32_t *__restrict__ dirty, int32_t *__restrict__ small_l,
                         int32_t *__restrict__ big_l, int32_t *counts, int32_t k, int32_t bigd)
 {
+    hp::pdl_wait();
     const int32_t nsel = d_plan[0], nch = d_plan[1];
     for (int64_t gc = blockIdx.x; gc < nch; gc += gridDim.x) {
         const int32_t jp = plan_find(plan_off, nsel, gc);
@@ -1189,6 +1212,7 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
                      unsigned long long *tile_status, hp::LbCtl *lb, unsigned *status,
                      const int8_t *__restrict__ ufl)
 {
+    hp::pdl_wait();
     __shared__ int32_t s_scan[RB_TILE / 32 + 2];
     __shared__ int32_t s_excl;
     int64_t tile;
@@ -1298,6 +1322,7 @@ rb_rank_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, con
                const int32_t *__restrict__ vwgt, int32_t *__restrict__ pre, int32_t *__restrict__ pstart,
                int32_t *__restrict__ pend, unsigned long long *tile_status, hp::LbCtl *lb, unsigned *status)
 {
+    hp::pdl_wait();
     __shared__ int32_t s_scan[RK_THREADS / 32 + 2];
     __shared__ int32_t s_excl;
     const unsigned epoch = hp::lb_epoch(lb);
@@ -1343,6 +1368,7 @@ __global__ void rw_select_kernel(const int32_t *__restrict__ K, const int32_t *_
                                  const unsigned long long *__restrict__ pw,
                                  const int64_t *__restrict__ maxp, const int32_t *__restrict__ dest, MoveSink ms)
 {
+    hp::pdl_wait();
     const int32_t cnt = *d_cnt;
     long long c1 = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < cnt;
@@ -1364,6 +1390,7 @@ __global__ void evict_end_kernel(int32_t k, const int32_t *__restrict__ pstart,
                                  const unsigned long long *__restrict__ pw,
                                  const int64_t *__restrict__ maxp, int32_t *__restrict__ ev_end)
 {
+    hp::pdl_wait();
     int32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= k) return;
     int32_t s = pstart[p], e = pend[p];
@@ -1388,6 +1415,7 @@ rs_evict_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, co
                 int32_t *__restrict__ sp, int32_t *__restrict__ d_np, unsigned long long *tile_status,
                 int64_t half, hp::LbCtl *lb, unsigned *status)
 {
+    hp::pdl_wait();
     __shared__ int32_t s_scan[RK_THREADS / 32 + 2];
     __shared__ int32_t s_excl[2];
     const unsigned epoch = hp::lb_epoch(lb);
@@ -1459,6 +1487,7 @@ cookie_cutter_kernel(int32_t k, const unsigned long long *__restrict__ pw, const
                      const int32_t *__restrict__ sp_g, const int32_t *__restrict__ d_np, int32_t *__restrict__ es,
                      int32_t *__restrict__ ee)
 {
+    hp::pdl_wait();
     extern __shared__ int32_t sp_s[];
     const int32_t np = *d_np;
     const bool staged = np + 1 <= COOKIE_SMEM_INTS;
@@ -1541,6 +1570,7 @@ __global__ void rs_assign_kernel(int32_t k, const int32_t *__restrict__ P, const
                                  const int32_t *__restrict__ ee, const int32_t *__restrict__ where,
                                  int32_t *__restrict__ dest, MoveSink ms)
 {
+    hp::pdl_wait();
     const int32_t np = *d_np;
     long long c1 = 0;
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < np;
@@ -1757,6 +1787,7 @@ __device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2
 __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned,
                                 const int32_t *gain_total, const RefineCtl *coarser)
 {
+    hp::pdl_wait();
     s->gain_entries = *gain_total;
     s->cut = coarser ? coarser->best_cut : (long long)sc[S_CUT2] / 2;
     s->excess = (long long)sc[S_EXCESS];
@@ -1790,6 +1821,7 @@ __global__ void __launch_bounds__(1024)
 ctl_end_kernel(RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle hloop, int graph, int32_t k,
                const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp)
 {
+    hp::pdl_wait();
     long long m = LLONG_MIN;
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
         const long long e = (long long)pw[p] - maxp[p];
@@ -1855,6 +1887,7 @@ ctl_begin_kernel(const RefineCtl *s, unsigned long long *sc, cudaGraphConditiona
                  const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
                  int32_t *__restrict__ und, int8_t *__restrict__ ufl)
 {
+    hp::pdl_wait();
     __shared__ int32_t s_scan[1024 / 32 + 2];
     if (threadIdx.x < S_PASS_END) sc[threadIdx.x] = 0;
     const int mode = s->mode;
@@ -1870,6 +1903,7 @@ __global__ void save_best_kernel(const RefineCtl *s, int32_t n, const int32_t *_
                                  int32_t *__restrict__ best_where, int32_t k,
                                  const unsigned long long *__restrict__ pw, unsigned long long *__restrict__ best_pw)
 {
+    hp::pdl_wait();
     if (!s->take) return;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) best_where[i] = where[i];
@@ -1879,6 +1913,7 @@ __global__ void save_best_kernel(const RefineCtl *s, int32_t n, const int32_t *_
 __global__ void restore_best_kernel(const RefineCtl *s, int32_t n, const int32_t *__restrict__ best_where,
                                     int32_t *__restrict__ where)
 {
+    hp::pdl_wait();
     if (s->best_current) return;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) where[i] = best_where[i];
@@ -1910,6 +1945,7 @@ lp_bytes_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__re
                 const int32_t *__restrict__ xadj, const int32_t *__restrict__ pregain, int32_t k,
                 unsigned long long *acc)
 {
+    hp::pdl_wait();
     long long b = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         b += row_walk_bytes(gpart, goff[v], goff[v + 1] - goff[v], k);
@@ -1925,6 +1961,7 @@ rebuild_bytes_kernel(const int32_t *__restrict__ small_l, const int32_t *__restr
                      const int32_t *__restrict__ big_l, const int32_t *__restrict__ d_nbig,
                      const int32_t *__restrict__ xadj, const int32_t *__restrict__ goff, unsigned long long *acc)
 {
+    hp::pdl_wait();
     const int32_t ns = *d_nsmall, nb = *d_nbig;
     long long b = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (int64_t)ns + nb;
@@ -1946,6 +1983,7 @@ rebalance_bytes_kernel(int32_t n, const int32_t *__restrict__ where, const unsig
                        const int32_t *__restrict__ gpart, int32_t k, const int32_t *__restrict__ d_cnt,
                        int32_t radix_passes, unsigned long long *acc)
 {
+    hp::pdl_wait();
     long long b = 0;
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t p = where[v];
@@ -1967,6 +2005,7 @@ apply_bytes_kernel(const int32_t *__restrict__ moves, const unsigned long long *
                    const int32_t *__restrict__ gpart, int32_t k, int32_t n, const RefineCtl *ctl,
                    unsigned long long *acc)
 {
+    hp::pdl_wait();
     const int64_t nm = (int64_t)*d_nmoves;
     long long b = 0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm; i += (int64_t)gridDim.x * blockDim.x) {
@@ -2160,6 +2199,7 @@ __device__ __forceinline__ long long sl_max64(long long v, long long *s_red)
 __global__ void __launch_bounds__(SL_THREADS, 1)
 refine_small_kernel(SmallLevel a)
 {
+    hp::pdl_wait();
     extern __shared__ __align__(16) int32_t sl_dyn[];
     __shared__ hp::MlpSmem s_mlp;
     __shared__ int32_t s_scan[SL_THREADS / 32 + 2];

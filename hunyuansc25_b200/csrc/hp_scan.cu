@@ -28,6 +28,7 @@ __global__ void __launch_bounds__(SCAN_BLOCK)
 scan_excl_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int64_t n,
                  unsigned long long *tile_status, hp::LbCtl *ctl, unsigned *status)
 {
+    hp::pdl_wait();
     __shared__ int32_t s[SCAN_TILE + SCAN_TILE / 32];
     __shared__ int32_t s_warp[SCAN_BLOCK / 32];
     __shared__ int32_t s_excl;
@@ -83,6 +84,7 @@ scan_excl_kernel(const int32_t *__restrict__ in, int32_t *__restrict__ out, int6
 
 __global__ void fill_kernel(int32_t *p, int64_t n, int32_t value)
 {
+    hp::pdl_wait();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
         p[i] = value;
@@ -90,6 +92,7 @@ __global__ void fill_kernel(int32_t *p, int64_t n, int32_t value)
 
 __global__ void iota_kernel(int32_t *p, int64_t n)
 {
+    hp::pdl_wait();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
         p[i] = (int32_t)i;
@@ -98,6 +101,7 @@ __global__ void iota_kernel(int32_t *p, int64_t n)
 __global__ void scatter_flags_kernel(const int32_t *flags, const int32_t *pos, int64_t n,
                                      int32_t *out, int32_t *d_count)
 {
+    hp::pdl_wait();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x)
         if (flags[i]) out[pos[i]] = (int32_t)i;
@@ -113,6 +117,7 @@ __global__ void __launch_bounds__(CUT_THREADS)
 edgecut_kernel(int32_t n, int64_t m, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where, unsigned long long *cut2)
 {
+    hp::pdl_wait();
     __shared__ int32_t owner[CUT_TILE];
     __shared__ int32_t s_warp[CUT_THREADS / 32];
     __shared__ int32_t s_v0;
@@ -280,6 +285,7 @@ __global__ void __launch_bounds__(RS_BLOCK)
 radix_hist_kernel(const int32_t *__restrict__ keys, const int32_t *__restrict__ d_count,
                   int shift, int32_t nblocks, int32_t *__restrict__ hist)
 {
+    hp::pdl_wait();
     __shared__ int32_t h[256];
     const int32_t cnt = *d_count;
     h[threadIdx.x] = 0;
@@ -298,6 +304,7 @@ radix_scatter_kernel(const int32_t *__restrict__ kin, const int32_t *__restrict_
                      const int32_t *__restrict__ hscan, int32_t *__restrict__ kout,
                      int32_t *__restrict__ vout)
 {
+    hp::pdl_wait();
     __shared__ int32_t run[256];                       // running per-digit offset of this block
     __shared__ int32_t wc[RS_BLOCK / 32][256];         // per-warp digit counts / offsets
     const int32_t cnt = *d_count;

@@ -62,6 +62,7 @@ SPACE = {
     "small_match_n": [0, 1024, 2048, 4096, 8192],
     "contract_hybrid": [0, 1],
     "apply_chunk_deg": [256, 512, 1024, 2048, 4096, 8192],
+    "pdl": [0, 1],
 }
 
 

@@ -192,7 +192,11 @@ typedef struct hp_tuning {
     int32_t apply_chunk_deg;     /* refinement: move application splits rows longer than
                                     this into chunks of 512 entries over the whole grid
                                     (chunk_deg is the afterburner's)     [gain_thread_deg, 2^24] 4096 */
-    int32_t reserved[6];         /* zero */
+    int32_t pdl;                 /* launches: each kernel of a call may be launched while the
+                                    previous one drains and waits for it on the device
+                                    (programmatic dependent launch) (1), or after it (0)
+                                                                                  [0, 1]        1 */
+    int32_t reserved[5];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);
