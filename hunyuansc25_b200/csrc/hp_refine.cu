@@ -604,8 +604,11 @@ lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__r
 
 // Learned LP selection: the plain rule first, then the MLP scores every
 // candidate (all lanes of a warp run the tensor-core inference together) and
-// drops candidates scoring below the threshold.  Dropped candidates simply
-// stay; nothing the network says bypasses the exact afterburner.
+// drops candidates scoring below the threshold.  Dropped candidates stay put;
+// under the judge (learned = 3) they keep their plain gain and destination
+// with prune[v] = 1, so that the afterburner leaves them out of the learned
+// move set but keeps them in the plain set it judges the pass by.  Nothing the
+// network says bypasses the exact afterburner.
 __global__ void __launch_bounds__(256)
 lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
                          const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
@@ -613,7 +616,8 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
                          const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp,
                          const int64_t *__restrict__ opt, const float *__restrict__ params, float threshold,
                          int32_t *__restrict__ dest, int32_t *__restrict__ pregain, unsigned long long *d_ncand,
-                         const int32_t *gate, int32_t k)
+                         const int32_t *gate, int32_t k, int8_t *__restrict__ prune,
+                         unsigned long long *d_ncandp, const int32_t *judge_flag)
 {
     hp::pdl_wait();
     if (gate && *gate != 1) return;   // graph mode: the plain kernel runs this pass
@@ -621,7 +625,8 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
     hp::mlp_load_smem(sm, params);
     __syncthreads();
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
-    int cand = 0;
+    int cand = 0, candp = 0;
+    int8_t pr = 0;
     float f[HP_MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     int32_t g = NEG, d = 0;
     int32_t p = 0, o = 0, len = 0;
@@ -641,6 +646,7 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
                 g = (int32_t)(bc - pc);
                 d = b;
                 cand = 1;
+                candp = 1;
                 hp::mlp_features(pc, bc, wd, np, xadj[v + 1] - xadj[v], maxp[b] - (int64_t)pw[b], opt[b],
                                  maxp[p] - (int64_t)pw[p], opt[p], finest, f);
             }
@@ -650,9 +656,20 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
     // candidate (the logit is read for candidates alone; the vote is uniform)
     float logit = 0.0f;
     if (__any_sync(HP_FULL_MASK, cand)) logit = hp::mlp_warp_logit(sm, f);
-    if (cand && logit < threshold) { cand = 0; g = NEG; d = where[v]; }
-    if (v < n) { pregain[v] = g; dest[v] = d; }
+    // under the judge a dropped candidate keeps its plain gain and destination
+    const bool judge = *judge_flag != 0;
+    if (cand && logit < threshold) {
+        cand = 0;
+        if (judge) pr = 1;
+        else { g = NEG; d = where[v]; }
+    }
+    if (v < n) {
+        pregain[v] = g;
+        dest[v] = d;
+        if (judge) prune[v] = pr;
+    }
     hp::block_add_to<256>(cand, d_ncand);
+    if (judge) hp::block_add_to<256>(candp, d_ncandp);
 }
 
 // Move log (record mode): features of every LP candidate, its vertex and
@@ -757,15 +774,41 @@ __device__ __forceinline__ long long ab_change(int32_t v, int32_t g, int32_t p, 
     return ch;
 }
 
-// Sum of ab_change over the entries j0, j0 + stride, ... below e of v's row,
-// four at a time: the row loads, then the neighbour gathers of the four, are in
-// flight together.
-__device__ __forceinline__ long long ab_row_sum(int32_t v, int32_t g, int32_t p, int32_t b, int32_t j0, int32_t e,
-                                                int32_t stride, const int32_t *__restrict__ adjncy,
-                                                const int32_t *__restrict__ adjwgt, const int32_t *pregain,
-                                                const int32_t *dest, const int32_t *where)
+// The plain refiner as the judge of a learned LP pass.  In such a pass the
+// selection keeps the plain rule's candidates and marks the ones the MLP dropped
+// (prune); the afterburner scores every candidate twice in one walk of its row --
+// against the higher-priority plain candidates and against the learned ones only
+// -- applies the learned decision (lock, moves) and keeps the plain one in accp.
+// The vertices that either decision moves are listed (list, *d_n), and
+// judge_off_kernel / judge_delta_kernel add both move sets' exact cut changes
+// over their rows.  flag: the control block's learned_pass, so the plain
+// refiner's passes (and every pass of a plain run) skip all of it.
+struct Judge {
+    const int32_t *flag;
+    const int8_t *prune;
+    int8_t *accp;
+    int32_t *list, *d_n;
+    const unsigned long long *d_ncandp;   // plain candidates of the pass
+};
+
+// ab_change of one entry into the plain sum and, when judging, into the sum
+// over the learned candidates (a neighbour the MLP dropped stays put there).
+__device__ __forceinline__ void ab_change2(int32_t v, int32_t g, int32_t p, int32_t b, int32_t u, int32_t w,
+                                           const int32_t *pregain, const int32_t *dest, const int32_t *where,
+                                           const int8_t *prune, bool judge, long long &chp, long long &chl)
 {
-    long long ch = 0;
+    const long long c = ab_change(v, g, p, b, u, w, pregain, dest, where);
+    chp += c;
+    if (judge && c != 0 && !prune[u]) chl += c;
+}
+
+// ab_row_sum into both sums (chl only when judging).
+__device__ __forceinline__ void ab_row_sum2(int32_t v, int32_t g, int32_t p, int32_t b, int32_t j0, int32_t e,
+                                            int32_t stride, const int32_t *__restrict__ adjncy,
+                                            const int32_t *__restrict__ adjwgt, const int32_t *pregain,
+                                            const int32_t *dest, const int32_t *where, const int8_t *prune,
+                                            bool judge, long long &chp, long long &chl)
+{
     for (int32_t j = j0; j < e; j += 4 * stride) {
         int32_t u[4], w[4], gu[4], du[4], wu[4];
 #pragma unroll
@@ -785,43 +828,57 @@ __device__ __forceinline__ long long ab_row_sum(int32_t v, int32_t g, int32_t p,
         for (int q = 0; q < 4; q++) {
             if (u[q] == v) continue;   // no entry (rows have no self loops)
             if (gu[q] > g || (gu[q] == g && u[q] < v)) {
-                if (du[q] == p) ch -= w[q];
-                else if (du[q] == b) ch += w[q];
-                if (wu[q] == p) ch += w[q];
-                else if (wu[q] == b) ch -= w[q];
+                long long c = 0;
+                if (du[q] == p) c -= w[q];
+                else if (du[q] == b) c += w[q];
+                if (wu[q] == p) c += w[q];
+                else if (wu[q] == b) c -= w[q];
+                chp += c;
+                if (judge && c != 0 && !prune[u[q]]) chl += c;
             }
         }
     }
-    return ch;
 }
 
 __global__ void __launch_bounds__(256)
 afterburner_small_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                          const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                          const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
-                         int8_t *__restrict__ lock, const unsigned long long *d_ncand, MoveSink ms, int32_t bigd)
+                         int8_t *__restrict__ lock, const unsigned long long *d_ncand, MoveSink ms, int32_t bigd,
+                         Judge J)
 {
     hp::pdl_wait();
-    if (*d_ncand == 0ull) return;
+    const bool judge = *J.flag != 0;
+    if (*d_ncand == 0ull && !(judge && *J.d_ncandp != 0ull)) return;
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     long long c1 = 0;
+    bool listed = false;
     if (v < n) {
         const int32_t b0 = xadj[v], e0 = xadj[v + 1];
         if (e0 - b0 <= bigd) {
             const int32_t g = pregain[v];
-            int8_t sel = 0;
+            int8_t sel = 0, selp = 0;
             int32_t p = 0, b = 0;
             if (g != NEG) {
                 p = where[v];
                 b = dest[v];
-                long long ch = 0;
+                long long chp = 0, chl = 0;
                 for (int32_t j = b0; j < e0; j++)
-                    ch += ab_change(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where);
-                sel = ((long long)g + ch >= 0);
+                    ab_change2(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where, J.prune, judge, chp, chl);
+                selp = ((long long)g + chp >= 0);
+                sel = judge ? (int8_t)(!J.prune[v] && (long long)g + chl >= 0) : selp;
             }
             lock[v] = sel;
+            if (judge) {
+                J.accp[v] = selp;
+                listed = sel || selp;
+            }
             if (sel) c1 = move_append(ms, v, p, b);
         }
+    }
+    if (judge) {
+        const int32_t pos = hp::warp_append(J.d_n, listed);
+        if (listed) J.list[pos] = v;
     }
     hp::block_add_to<256>(c1, ms.d_c1);
 }
@@ -832,10 +889,11 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
                        const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                        const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
                        int8_t *__restrict__ lock, const unsigned long long *d_ncand, MoveSink ms,
-                       int32_t chunkd)
+                       int32_t chunkd, Judge J)
 {
     hp::pdl_wait();
-    if (*d_ncand == 0ull) return;
+    const bool judge = *J.flag != 0;
+    if (*d_ncand == 0ull && !(judge && *J.d_ncandp != 0ull)) return;
     const int lane = threadIdx.x & 31;
     const int32_t cnt = *d_bigcnt;
     long long c1 = 0;
@@ -844,17 +902,29 @@ afterburner_big_kernel(const int32_t *__restrict__ big, const int32_t *__restric
         const int32_t v = big[i];
         if (xadj[v + 1] - xadj[v] > chunkd) continue;   // chunked over the grid
         const int32_t g = pregain[v];
-        int8_t sel = 0;
+        int8_t sel = 0, selp = 0;
         int32_t p = 0, b = 0;
         if (g != NEG) {
             p = where[v];
             b = dest[v];
-            long long ch = ab_row_sum(v, g, p, b, xadj[v] + lane, xadj[v + 1], 32, adjncy, adjwgt, pregain, dest, where);
-            ch = hp::warp_sum64(ch);
-            sel = ((long long)g + ch >= 0);
+            long long chp = 0, chl = 0;
+            ab_row_sum2(v, g, p, b, xadj[v] + lane, xadj[v + 1], 32, adjncy, adjwgt, pregain, dest, where, J.prune,
+                        judge, chp, chl);
+            chp = hp::warp_sum64(chp);
+            selp = ((long long)g + chp >= 0);
+            if (judge) {
+                chl = hp::warp_sum64(chl);
+                sel = (int8_t)(!J.prune[v] && (long long)g + chl >= 0);
+            } else {
+                sel = selp;
+            }
         }
         if (lane == 0) {
             lock[v] = sel;
+            if (judge) {
+                J.accp[v] = selp;
+                if (sel || selp) J.list[atomicAdd(J.d_n, 1)] = v;
+            }
             if (sel) c1 += move_append(ms, v, p, b);
         }
     }
@@ -951,7 +1021,8 @@ __device__ __forceinline__ int32_t plan_find(const int32_t *__restrict__ plan_of
 }
 
 // Afterburner of the candidate hubs: every chunk adds its part of the change to
-// the hub's accumulator (ab_acc, indexed by hub-list position, zero on entry);
+// the hub's accumulator (ab_acc, indexed by hub-list position, zero on entry;
+// ab_acc2 the learned candidates' sum when judging);
 // afterburner_huge_final_kernel then decides from the full sums.
 __global__ void __launch_bounds__(HUB_CHUNK)
 afterburner_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__restrict__ plan_item,
@@ -959,10 +1030,12 @@ afterburner_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__res
                         const int32_t *__restrict__ xadj, const int32_t *__restrict__ adjncy,
                         const int32_t *__restrict__ adjwgt, const int32_t *__restrict__ where,
                         const int32_t *__restrict__ dest, const int32_t *__restrict__ pregain,
-                        const unsigned long long *d_ncand, unsigned long long *__restrict__ ab_acc)
+                        const unsigned long long *d_ncand, unsigned long long *__restrict__ ab_acc,
+                        unsigned long long *__restrict__ ab_acc2, Judge J)
 {
     hp::pdl_wait();
-    if (*d_ncand == 0ull) return;
+    const bool judge = *J.flag != 0;
+    if (*d_ncand == 0ull && !(judge && *J.d_ncandp != 0ull)) return;
     const int lane = threadIdx.x & 31;
     const int32_t nsel = d_plan[0], nch = d_plan[1];
     for (int64_t gc = blockIdx.x; gc < nch; gc += gridDim.x) {
@@ -971,32 +1044,99 @@ afterburner_huge_kernel(const int32_t *__restrict__ plan_v, const int32_t *__res
         const int32_t g = pregain[v], p = where[v], b = dest[v];
         const int32_t e0 = xadj[v + 1];
         const int32_t j = xadj[v] + (int32_t)(gc - plan_off[jp]) * HUB_CHUNK + threadIdx.x;
-        long long c = j < e0 ? ab_change(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where) : 0;
-        c = hp::warp_sum64(c);
-        if (lane == 0 && c != 0) atomicAdd(&ab_acc[plan_item[jp]], (unsigned long long)c);
+        long long cp = 0, cl = 0;
+        if (j < e0) ab_change2(v, g, p, b, adjncy[j], adjwgt[j], pregain, dest, where, J.prune, judge, cp, cl);
+        cp = hp::warp_sum64(cp);
+        if (judge) cl = hp::warp_sum64(cl);
+        if (lane == 0 && cp != 0) atomicAdd(&ab_acc[plan_item[jp]], (unsigned long long)cp);
+        if (lane == 0 && cl != 0) atomicAdd(&ab_acc2[plan_item[jp]], (unsigned long long)cl);
     }
 }
 
 __global__ void afterburner_huge_final_kernel(const int32_t *__restrict__ huge, const int32_t *__restrict__ d_nhuge,
                                               const int32_t *__restrict__ pregain, const unsigned long long *d_ncand,
-                                              unsigned long long *__restrict__ ab_acc, int8_t *__restrict__ lock,
+                                              unsigned long long *__restrict__ ab_acc,
+                                              unsigned long long *__restrict__ ab_acc2, int8_t *__restrict__ lock,
                                               const int32_t *__restrict__ where, const int32_t *__restrict__ dest,
-                                              MoveSink ms)
+                                              MoveSink ms, Judge J)
 {
     hp::pdl_wait();
-    if (*d_ncand == 0ull) return;
+    const bool judge = *J.flag != 0;
+    if (*d_ncand == 0ull && !(judge && *J.d_ncandp != 0ull)) return;
     const int32_t nh = *d_nhuge;
     long long c1 = 0;
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += gridDim.x * blockDim.x) {
         const int32_t v = huge[i];
         const int32_t g = pregain[v];
-        const long long tot = (long long)ab_acc[i];
+        const long long totp = (long long)ab_acc[i];
         ab_acc[i] = 0ull;
-        const int8_t sel = (g != NEG) && ((long long)g + tot >= 0);
+        const int8_t selp = (g != NEG) && ((long long)g + totp >= 0);
+        int8_t sel = selp;
+        if (judge) {
+            const long long totl = (long long)ab_acc2[i];
+            ab_acc2[i] = 0ull;
+            sel = (g != NEG) && !J.prune[v] && ((long long)g + totl >= 0);
+            J.accp[v] = selp;
+            if (sel || selp) J.list[atomicAdd(J.d_n, 1)] = v;
+        }
         lock[v] = sel;
         if (sel) c1 += move_append(ms, v, where[v], dest[v]);
     }
     hp::block_add_to<256>(c1, ms.d_c1);
+}
+
+// ---- the judge's exact cut changes ---------------------------------------------------
+// Over the listed vertices' entries (tiles of JD_TILE, owner rows from the
+// prefix): twice the exact cut decrease of the plain move set (accp) into
+// sums[0] and of the learned one (lock) into sums[1].  An entry (v, u, w) of a
+// moved v counts w ([p_v != p_u] - [d_v != new p_u]), twice when u stays put
+// and once when u moves too (then its row counts the edge again).
+constexpr int JD_THREADS = 256, JD_ITEMS = 8, JD_TILE = JD_THREADS * JD_ITEMS;
+
+// One entry (v, u, w) of a listed vertex v (part pv, destination dv; apv / alv:
+// v moves in the plain / learned set) into the two sums.
+__device__ __forceinline__ void judge_entry(int32_t pv, int32_t dv, bool apv, bool alv, int32_t u, int32_t w,
+                                            const int32_t *where, const int32_t *dest, const int8_t *accp,
+                                            const int8_t *lock, long long &sp, long long &sl)
+{
+    const int32_t pu = where[u];
+    const bool apu = accp[u] != 0, alu = lock[u] != 0;
+    const int32_t du = (apu || alu) ? dest[u] : pu;
+    const long long before = pv != pu;
+    if (apv) sp += (long long)w * (before - (dv != (apu ? du : pu))) * (apu ? 1 : 2);
+    if (alv) sl += (long long)w * (before - (dv != (alu ? du : pu))) * (alu ? 1 : 2);
+}
+
+__global__ void __launch_bounds__(JD_THREADS)
+judge_delta_kernel(const int32_t *flag, const int32_t *__restrict__ list, const int32_t *d_n,
+                   const int32_t *__restrict__ off, const int32_t *__restrict__ xadj,
+                   const int32_t *__restrict__ adjncy, const int32_t *__restrict__ adjwgt,
+                   const int32_t *__restrict__ where, const int32_t *__restrict__ dest,
+                   const int8_t *__restrict__ accp, const int8_t *__restrict__ lock, unsigned long long *sums)
+{
+    hp::pdl_wait();
+    __shared__ int32_t owner[JD_TILE];
+    __shared__ int32_t s_warp[JD_THREADS / 32];
+    __shared__ int32_t s_v0;
+    if (*flag == 0) return;
+    const int32_t cnt = *d_n;
+    if (cnt <= 0) return;
+    const int64_t tot = off[cnt];
+    long long sp = 0, sl = 0;
+    for (int64_t tb = (int64_t)blockIdx.x * JD_TILE; tb < tot; tb += (int64_t)gridDim.x * JD_TILE) {
+        const int64_t te = tb + JD_TILE < tot ? tb + JD_TILE : tot;
+        hp::tile_owners<JD_THREADS, JD_ITEMS>(off, cnt, tb, te, owner, s_warp, &s_v0);
+        for (int64_t t = tb + threadIdx.x; t < te; t += JD_THREADS) {
+            const int32_t i = owner[t - tb];
+            const int32_t v = list[i];
+            const int32_t j = xadj[v] + (int32_t)(t - off[i]);
+            judge_entry(where[v], dest[v], accp[v] != 0, lock[v] != 0, adjncy[j], adjwgt[j], where, dest, accp, lock,
+                        sp, sl);
+        }
+        __syncthreads();   // owner[] is rebuilt for the next tile
+    }
+    hp::block_add_to<JD_THREADS>(sp, &sums[0]);
+    hp::block_add_to<JD_THREADS>(sl, &sums[1]);
 }
 
 // ---- applying moves -------------------------------------------------------------
@@ -1362,6 +1502,53 @@ rb_rank_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V, con
     hp::lb_end(lb);
 }
 
+// The judge's list: exclusive prefix of the row lengths of the listed vertices
+// (off[i]; off[cnt] = all their entries), in tiles of RK_TILE with an epoch
+// look-back, by persistent CTAs until the tile holding index cnt.
+__global__ void __launch_bounds__(RK_THREADS)
+judge_off_kernel(const int32_t *flag, const int32_t *__restrict__ list, const int32_t *d_n,
+                 const int32_t *__restrict__ xadj, int32_t *__restrict__ off, unsigned long long *tile_status,
+                 hp::LbCtl *lb, unsigned *status)
+{
+    hp::pdl_wait();
+    __shared__ int32_t s_scan[RK_THREADS / 32 + 2];
+    __shared__ int32_t s_excl;
+    const unsigned epoch = hp::lb_epoch(lb);
+    const int32_t cnt = *flag != 0 ? *d_n : -1;   // -1: not judging, no tile
+    for (;;) {
+        const int64_t tile = hp::lb_next(lb);
+        const int64_t base = tile * RK_TILE;
+        if (base > cnt) break;   // the tile holding index cnt was the last one
+        const int64_t i0 = base + (int64_t)threadIdx.x * RK_ITEMS;
+        int32_t d[RK_ITEMS];
+        int32_t sum = 0;
+#pragma unroll
+        for (int q = 0; q < RK_ITEMS; q++) {
+            const int64_t i = i0 + q;
+            d[q] = 0;
+            if (i < cnt) {
+                const int32_t v = list[i];
+                d[q] = xadj[v + 1] - xadj[v];
+            }
+            sum += d[q];
+        }
+        int tot;
+        int32_t run = hp::block_excl_scan<RK_THREADS>(sum, &tot, s_scan);
+        if (threadIdx.x < 32) {
+            const int32_t ex = hp::lookback_epoch(tile_status, tile, tot, epoch, status);
+            if (threadIdx.x == 0) s_excl = ex;
+        }
+        __syncthreads();
+        run += s_excl;
+#pragma unroll
+        for (int q = 0; q < RK_ITEMS; q++) {
+            if (i0 + q <= cnt) off[i0 + q] = run;
+            run += d[q];
+        }
+    }
+    hp::lb_end(lb);
+}
+
 __global__ void rw_select_kernel(const int32_t *__restrict__ K, const int32_t *__restrict__ V,
                                  const int32_t *__restrict__ d_cnt, const int32_t *__restrict__ pre,
                                  const int32_t *__restrict__ pstart,
@@ -1602,6 +1789,9 @@ struct RefineBufs {
     int64_t nhub_cap;   // capacity of the long-row list and the plan (rows longer than chunk_deg)
     unsigned long long *ab_acc;   // afterburner sums of the hub rows (zero between passes)
     int8_t *lock;
+    int8_t *prune, *accp;                  // the judge of a learned pass (Judge)
+    int32_t *jlist, *joff;                 // its listed vertices and their row prefix
+    unsigned long long *ab_acc2;           // learned-candidate sums of the hub rows
     int32_t *K, *V, *K2, *V2, *pre, *P, *sp;
     int32_t *pstart, *pend, *und, *ev_end, *es, *ee;
     int8_t *ufl;   // per part: pw < maxp (a weak pass's destination rule), set by ctl_begin
@@ -1612,12 +1802,15 @@ struct RefineBufs {
 };
 
 // scalar slots used by refinement
-// Slots below S_PASS_END are reset at the start of every pass; S_BIGCNT (the
+// Slots below S_PASS_END are reset at the start of every pass (S_NCANDP .. S_JL:
+// the judge of a learned pass -- plain candidates, listed vertices, twice the
+// plain and the learned exact cut decrease); S_BIGCNT (the
 // level's list of rows longer than 32) lives above it and persists.
 // S_BIGCNT (slots 16-17) holds the big-row count, the longest short row and the
 // longest row above huged.
 enum { S_NMOVES = 0, S_C1 = 1, S_C2 = 2, S_EXCESS = 3, S_NCAND = 4, S_CUT2 = 5, S_DIRTY = 6,
-       S_HUGEMV = 7, S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_PASS_END = 12, S_BIGCNT = 16 };
+       S_HUGEMV = 7, S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_NCANDP = 11, S_JN = 12, S_JP = 13, S_JL = 14,
+       S_PASS_END = 16, S_BIGCNT = 16 };
 
 int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_t *small_list,
                const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt,
@@ -1766,6 +1959,8 @@ struct RefineCtl {
     int32_t take, cont, patience, last_mode;
     int32_t mode_passes[4];
     int32_t gain_entries, pad;   // G of the level (for the profiler's byte counts)
+    int32_t judge_mode;          // hp_options.learned = 3: the plain refiner judges every learned pass
+    int32_t judge_pass;          // the current pass is a learned LP pass under that judge
 };
 
 __device__ void ctl_prepare(RefineCtl *s)
@@ -1773,19 +1968,21 @@ __device__ void ctl_prepare(RefineCtl *s)
     s->passes++;
     s->mode = s->excess <= 0 ? 0 : (s->bal < 2 ? 1 : 2);
     s->learned_pass = (s->excess <= 0 && s->learned_active) ? 1 : 0;
+    s->judge_pass = s->learned_pass && s->judge_mode;
     s->cut_before = s->cut;
     s->bal = s->mode == 0 ? 0 : s->bal + 1;
     s->mode_passes[s->mode]++;
 }
 
-__device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2, long long nmoves, long long ncand);
+__device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2, long long nmoves, long long ncand,
+                           long long jp2);
 
 // The level's starting cut: the coarser level's best cut when there is one (a
 // projection keeps the cut exactly: every coarse edge weight is the sum of
 // the fine edges between its two clusters, and edges inside a cluster are
 // never cut), else the cut summed from the gain rows (rowcut_kernel).
 __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned,
-                                const int32_t *gain_total, const RefineCtl *coarser)
+                                const int32_t *gain_total, const RefineCtl *coarser, int32_t judge)
 {
     hp::pdl_wait();
     s->gain_entries = *gain_total;
@@ -1801,6 +1998,8 @@ __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int3
     s->lp_idle = 0;
     s->learned_active = learned;
     s->learned_pass = 0;
+    s->judge_mode = learned && judge;
+    s->judge_pass = 0;
     s->take = 0;
     s->last_moves = 0;
     s->last_mode = -1;
@@ -1819,7 +2018,7 @@ __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int3
 // the control block.
 __global__ void __launch_bounds__(1024)
 ctl_end_kernel(RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle hloop, int graph, int32_t k,
-               const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp)
+               const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp, unsigned *status)
 {
     hp::pdl_wait();
     long long m = LLONG_MIN;
@@ -1834,25 +2033,40 @@ ctl_end_kernel(RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle 
     if (threadIdx.x != 0) return;
     for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = s_max[w] > m ? s_max[w] : m;
     sc[S_EXCESS] = (unsigned long long)m;
-    const int cont = ctl_advance(s, m, (long long)sc[S_C1], (long long)sc[S_C2], (long long)sc[S_NMOVES],
-                                 (long long)sc[S_NCAND]);
+    const long long c1 = (long long)sc[S_C1], c2 = (long long)sc[S_C2];
+    // the judge's sum over the learned moves is the applied pass's exact change
+    if (s->judge_pass && (long long)sc[S_JL] != c1 + c2) atomicOr(status, HP_STATUS_OVERFLOW);
+    const int cont = ctl_advance(s, m, c1, c2, (long long)sc[S_NMOVES], (long long)sc[S_NCAND], (long long)sc[S_JP]);
     if (graph) cudaGraphSetConditional(hloop, cont ? 1u : 0u);
 }
 
 // The control step of a pass end (one thread): new excess m, the cut-change
 // sums c1 and c2, the pass's moves and LP candidates.  Returns the loop condition.
-__device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2, long long nmoves, long long ncand)
+__device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2, long long nmoves, long long ncand,
+                           long long jp2)
 {
     s->excess = m;
     s->cut -= (c1 + c2) / 2;
     s->last_moves = nmoves;
     s->last_mode = s->mode;
-    if (s->learned_pass && s->cut >= s->cut_before) s->learned_active = 0;
+    // The plain refiner takes over for the rest of the level as soon as a
+    // learned pass does not lower the cut, and under the judge (learned = 3) as
+    // soon as it lowers the cut less than the plain pass would have on the same
+    // state: c1 + c2 and jp2 are twice the exact cut decrease of the learned and
+    // of the plain moves.
+    bool handed = false;
+    if (s->learned_pass && (c1 + c2 <= 0 || (s->judge_pass && c1 + c2 < jp2))) {
+        s->learned_active = 0;
+        handed = true;
+    }
     const int mode = s->mode;
     // A pass that changed nothing (no moves, no lock change) is repeated
     // identically by every later pass and can never improve the best
-    // partition: stop now; the result is the same as running on.
-    const bool stalled = nmoves == 0 && (mode == 2 || (mode == 0 && (ncand == 0 || s->lp_idle)));
+    // partition: stop now; the result is the same as running on.  Under the
+    // judge a learned pass that handed over is not such a pass: the plain pass
+    // after it differs.
+    const bool stalled = !(handed && s->judge_mode) && nmoves == 0 &&
+                         (mode == 2 || (mode == 0 && (ncand == 0 || s->lp_idle)));
     s->lp_idle = (mode == 0 && nmoves == 0) ? 1 : 0;
     int take = 0;
     if (s->best_excess > 0 && s->excess < s->best_excess) {
@@ -2019,6 +2233,7 @@ apply_bytes_kernel(const int32_t *__restrict__ moves, const unsigned long long *
 struct PassCfg {
     int32_t k;
     bool finest, any_big, recording, huge_rows;   // huge_rows: rows longer than chunk_deg exist
+    bool judged;                                  // learned = 3: learned passes are judged
     bool huge_moves;                              // rows longer than apply_chunk_deg exist
     RefineCtl *ctl;
     unsigned long long *best_pw;
@@ -2037,10 +2252,12 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
     const int32_t *gate = both_lp ? &P.ctl->learned_pass : nullptr;
     if (mode == 0) {
         const int ltok = hp_prof_begin(c);
+        const Judge J{&P.ctl->judge_pass, B.prune, B.accp, B.jlist, (int32_t *)&sc[S_JN], &sc[S_NCANDP]};
+        const bool judging = P.judged && (both_lp || learned_pass);
         if (both_lp || learned_pass)
             HP_LAUNCH(c, lp_select_learned_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, g.xadj,
                       B.lock, P.finest ? 1 : 0, B.pw, B.maxp, B.opt, c->mlp_params, c->mlp_threshold, B.dest,
-                      B.pregain, &sc[S_NCAND], gate, k);
+                      B.pregain, &sc[S_NCAND], gate, k, B.prune, &sc[S_NCANDP], J.flag);
         if (both_lp || !learned_pass)
             HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
                       P.finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND], gate, k);
@@ -2049,10 +2266,10 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
                       P.finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.recof, c->log_x, c->log_v,
                       c->log_d, c->log_acc, c->log_count, c->log_cap);
         HP_LAUNCH(c, afterburner_small_kernel, nblk(n), 256, 0, n, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest,
-                  B.pregain, B.lock, &sc[S_NCAND], move_sink(c, B, k), c->tune.gain_thread_deg);
+                  B.pregain, B.lock, &sc[S_NCAND], move_sink(c, B, k), c->tune.gain_thread_deg, J);
         if (P.any_big)
             HP_LAUNCH(c, afterburner_big_kernel, pg, 256, 0, B.big, d_bigcnt, g.xadj, g.adjncy, g.adjwgt, g.where,
-                      B.dest, B.pregain, B.lock, &sc[S_NCAND], move_sink(c, B, k), c->tune.chunk_deg);
+                      B.dest, B.pregain, B.lock, &sc[S_NCAND], move_sink(c, B, k), c->tune.chunk_deg, J);
         if (P.huge_rows) {
             const int32_t *d_nhuge = d_bigcnt + 3;
             HP_LAUNCH(c, hub_plan_kernel<false>, plan_grid(c, B.nhub_cap), PLAN_THREADS, 0, B.huge, d_nhuge, B.moves,
@@ -2060,9 +2277,17 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
                       c->lb_ctl, c->d_status);
             HP_LAUNCH(c, afterburner_huge_kernel, (unsigned)(4 * c->sm_count), HUB_CHUNK, 0, B.plan_v, B.plan_item,
                       B.plan_off, B.plan_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.dest, B.pregain, &sc[S_NCAND],
-                      B.ab_acc);
+                      B.ab_acc, B.ab_acc2, J);
             HP_LAUNCH(c, afterburner_huge_final_kernel, (unsigned)c->sm_count, 256, 0, B.huge, d_nhuge, B.pregain,
-                      &sc[S_NCAND], B.ab_acc, B.lock, g.where, B.dest, move_sink(c, B, k));
+                      &sc[S_NCAND], B.ab_acc, B.ab_acc2, B.lock, g.where, B.dest, move_sink(c, B, k), J);
+        }
+        if (judging) {   // the plain refiner's exact cut change on the same state (learned passes only)
+            const int64_t rt = ((int64_t)n + RK_TILE) / RK_TILE;   // a tile holds index cnt <= n
+            if (rt > c->lb_cap) return HP_ERR_INTERNAL;
+            HP_LAUNCH(c, judge_off_kernel, rank_grid(c, rt), RK_THREADS, 0, J.flag, B.jlist, J.d_n, g.xadj, B.joff,
+                      c->lb_status, c->lb_ctl, c->d_status);
+            HP_LAUNCH(c, judge_delta_kernel, pg, JD_THREADS, 0, J.flag, B.jlist, J.d_n, B.joff, g.xadj, g.adjncy,
+                      g.adjwgt, g.where, B.dest, B.accp, B.lock, &sc[S_JP]);
         }
         if (P.recording)
             HP_LAUNCH(c, log_accept_kernel, nblk(n), 256, 0, n, B.recof, B.lock, &sc[S_NCAND], c->log_acc);
@@ -2118,7 +2343,7 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
     atok = hp_prof_begin(c);
     HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
               B.oldp, 0, &sc[S_C2], k);
-    HP_LAUNCH(c, ctl_end_kernel, 1, 1024, 0, P.ctl, sc, hloop, graph, k, B.pw, B.maxp);
+    HP_LAUNCH(c, ctl_end_kernel, 1, 1024, 0, P.ctl, sc, hloop, graph, k, B.pw, B.maxp, c->d_status);
     HP_LAUNCH(c, save_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, P.ctl, n,
               g.where, B.best_where, k, B.pw, P.best_pw);
     hp_prof_end(c, atok, HP_PROF_APPLY, 0);
@@ -2154,10 +2379,12 @@ struct SmallLevel {
     int32_t *K, *V, *K2, *V2, *pre, *P, *sp;
     int32_t *pstart, *pend, *und, *ev_end, *es, *ee;
     int8_t *lock;
+    int8_t *prune, *accp;   // the judge of a learned pass
     unsigned long long *pw, *best_pw;
     const int64_t *opt, *maxp;
     const float *mlp_params;
     RefineCtl *ctl;
+    unsigned *status;
 };
 
 // Dynamic shared memory of the small-level kernel: the largest of the phases'
@@ -2216,12 +2443,14 @@ refine_small_kernel(SmallLevel a)
         if (!*(volatile const int32_t *)&s->cont) break;   // written by thread 0 before a barrier
         const int mode = *(volatile const int32_t *)&s->mode;
         if (tid < 2) s_lists[tid] = 0;
-        long long ncand = 0;
+        long long ncand = 0, jp2 = 0, jl2 = 0;
+        bool judged = false;
         int32_t nmoves = 0;
         if (mode == 0) {
             // ---- LP selection (plain or learned), as lp_select[_learned]_kernel
             const bool lrn = a.learned_mlp && *(volatile const int32_t *)&s->learned_pass;
-            int32_t my_cand = 0;
+            const bool jdg = lrn && *(volatile const int32_t *)&s->judge_pass;
+            int32_t my_cand = 0, my_candp = 0;
             for (int32_t b0 = 0; b0 < n; b0 += SL_THREADS) {
                 const int32_t v = b0 + tid;
                 const bool in = v < n;
@@ -2247,18 +2476,27 @@ refine_small_kernel(SmallLevel a)
                                              a.opt[p], a.finest, f);
                     }
                 }
+                int8_t pr = 0;   // dropped by the MLP: keeps the plain gain and destination for the judge
+                my_candp += cand;
                 if (lrn && __any_sync(HP_FULL_MASK, cand)) {   // a warp without candidates needs no scores
                     const float logit = hp::mlp_warp_logit(s_mlp, f);
-                    if (cand && logit < a.mlp_threshold) { cand = 0; g = NEG; d = p; }
+                    if (cand && logit < a.mlp_threshold) {
+                        cand = 0;
+                        if (jdg) pr = 1;
+                        else { g = NEG; d = p; }
+                    }
                 }
                 if (in) {
                     a.pregain[v] = g;
                     a.dest[v] = d;
+                    if (jdg) a.prune[v] = pr;
                 }
                 my_cand += cand;
             }
             ncand = sl_sum64(my_cand, s_red);   // (barrier: every selection is visible)
-            if (ncand > 0) {
+            const long long ncandp = jdg ? sl_sum64(my_candp, s_red) : ncand;
+            judged = jdg;
+            if (ncand > 0 || (jdg && ncandp > 0)) {
                 // ---- afterburner: every candidate re-scored against the
                 // higher-priority neighbours; locks and moves (in vertex order)
                 int32_t run = 0;
@@ -2269,11 +2507,12 @@ refine_small_kernel(SmallLevel a)
                     const bool act = g != NEG;
                     const int32_t ro = act ? a.xadj[v] : 0, rl = act ? a.xadj[v + 1] - ro : 0;
                     const int32_t pp = act ? a.where[v] : 0, bb = act ? a.dest[v] : 0;
-                    long long ch = 0;
+                    long long chp = 0, chl = 0;
                     const bool coop = rl > 32;
                     if (act && !coop)
                         for (int32_t j = ro; j < ro + rl; j++)
-                            ch += ab_change(v, g, pp, bb, a.adjncy[j], a.adjwgt[j], a.pregain, a.dest, a.where);
+                            ab_change2(v, g, pp, bb, a.adjncy[j], a.adjwgt[j], a.pregain, a.dest, a.where, a.prune,
+                                       jdg, chp, chl);
                     unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
                     while (cm) {
                         const int src = __ffs(cm) - 1;
@@ -2281,19 +2520,58 @@ refine_small_kernel(SmallLevel a)
                         const int32_t sv = __shfl_sync(HP_FULL_MASK, v, src), sg = __shfl_sync(HP_FULL_MASK, g, src);
                         const int32_t sp_ = __shfl_sync(HP_FULL_MASK, pp, src), sb = __shfl_sync(HP_FULL_MASK, bb, src);
                         const int32_t so = __shfl_sync(HP_FULL_MASK, ro, src), sl = __shfl_sync(HP_FULL_MASK, rl, src);
-                        long long c = ab_row_sum(sv, sg, sp_, sb, so + lane, so + sl, 32, a.adjncy, a.adjwgt,
-                                                 a.pregain, a.dest, a.where);
-                        c = hp::warp_sum64(c);
-                        if (lane == src) ch = c;
+                        long long cp = 0, cl = 0;
+                        ab_row_sum2(sv, sg, sp_, sb, so + lane, so + sl, 32, a.adjncy, a.adjwgt, a.pregain, a.dest,
+                                    a.where, a.prune, jdg, cp, cl);
+                        cp = hp::warp_sum64(cp);
+                        if (jdg) cl = hp::warp_sum64(cl);
+                        if (lane == src) { chp = cp; chl = cl; }
                     }
-                    const int sel = act && ((long long)g + ch >= 0);
-                    if (in) a.lock[v] = (int8_t)sel;
+                    const int selp = act && ((long long)g + chp >= 0);
+                    const int sel = jdg ? (act && !a.prune[v] && (long long)g + chl >= 0) : selp;
+                    if (in) {
+                        a.lock[v] = (int8_t)sel;
+                        if (jdg) a.accp[v] = (int8_t)selp;
+                    }
                     int tot;
                     const int ex = hp::block_excl_scan<SL_THREADS>(sel, &tot, s_scan);
                     if (sel) a.moves[run + ex] = v;
                     run += tot;
                 }
                 nmoves = run;
+                if (jdg) {
+                    // ---- the judge: exact cut decrease of the plain and the
+                    // learned move sets on this state, as judge_delta_kernel
+                    __syncthreads();   // every lock / accp is visible
+                    long long sp = 0, sl = 0;
+                    for (int32_t b0 = 0; b0 < n; b0 += SL_THREADS) {
+                        const int32_t v = b0 + tid;
+                        const bool in = v < n;
+                        const bool mp = in && a.accp[v] != 0, ml = in && a.lock[v] != 0;
+                        const bool act = mp || ml;
+                        const int32_t ro = act ? a.xadj[v] : 0, rl = act ? a.xadj[v + 1] - ro : 0;
+                        const int32_t pv = act ? a.where[v] : 0, dv = act ? a.dest[v] : 0;
+                        const bool coop = rl > 32;
+                        if (act && !coop)
+                            for (int32_t j = ro; j < ro + rl; j++)
+                                judge_entry(pv, dv, mp, ml, a.adjncy[j], a.adjwgt[j], a.where, a.dest, a.accp, a.lock,
+                                            sp, sl);
+                        unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
+                        while (cm) {
+                            const int src = __ffs(cm) - 1;
+                            cm &= cm - 1;
+                            const int32_t so = __shfl_sync(HP_FULL_MASK, ro, src), sn = __shfl_sync(HP_FULL_MASK, rl, src);
+                            const int32_t spv = __shfl_sync(HP_FULL_MASK, pv, src), sdv = __shfl_sync(HP_FULL_MASK, dv, src);
+                            const bool smp = __shfl_sync(HP_FULL_MASK, (int)mp, src) != 0;
+                            const bool sml = __shfl_sync(HP_FULL_MASK, (int)ml, src) != 0;
+                            for (int32_t j = so + lane; j < so + sn; j += 32)
+                                judge_entry(spv, sdv, smp, sml, a.adjncy[j], a.adjwgt[j], a.where, a.dest, a.accp,
+                                            a.lock, sp, sl);
+                        }
+                    }
+                    jp2 = sl_sum64(sp, s_red);
+                    jl2 = sl_sum64(sl, s_red);
+                }
             }
         } else {
             // ---- rebalance, as rb_candidates / sort / rb_rank / rw_select or
@@ -2527,7 +2805,11 @@ refine_small_kernel(SmallLevel a)
             m = e > m ? e : m;
         }
         m = sl_max64(m, s_red);
-        if (tid == 0) ctl_advance(s, m, c1, c2, nmoves, ncand);
+        if (tid == 0) {
+            // the judge's sum over the learned moves is the applied pass's exact change
+            if (judged && jl2 != c1 + c2) atomicOr(a.status, HP_STATUS_OVERFLOW);
+            ctl_advance(s, m, c1, c2, nmoves, ncand, jp2);
+        }
         __syncthreads();
         if (*(volatile const int32_t *)&s->take) {
             for (int32_t i = tid; i < n; i += SL_THREADS) a.best_where[i] = a.where[i];
@@ -2693,6 +2975,10 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     int32_t **k_arrays[] = {&B.pstart, &B.pend, &B.und, &B.ev_end, &B.es, &B.ee};
     for (auto pp : k_arrays) *pp = ralloc_t<int32_t>(c, k);
     B.lock = ralloc_t<int8_t>(c, n);
+    B.prune = ralloc_t<int8_t>(c, n);
+    B.accp = ralloc_t<int8_t>(c, n);
+    B.jlist = ralloc_t<int32_t>(c, (int64_t)n + 1);
+    B.joff = ralloc_t<int32_t>(c, (int64_t)n + 2);
     B.ufl = ralloc_t<int8_t>(c, k);
     B.pw = ralloc_t<unsigned long long>(c, k);
     unsigned long long *best_pw = ralloc_t<unsigned long long>(c, k);
@@ -2705,6 +2991,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     if (2 * (nhub_cap / PLAN_TILE + 1) > c->lb_cap) return HP_ERR_INTERNAL;
     B.nhub_cap = nhub_cap;
     B.ab_acc = ralloc_t<unsigned long long>(c, nhub_cap);
+    B.ab_acc2 = ralloc_t<unsigned long long>(c, nhub_cap);
     B.plan_v = ralloc_t<int32_t>(c, nhub_cap);
     B.plan_item = ralloc_t<int32_t>(c, nhub_cap);
     B.plan_off = ralloc_t<int32_t>(c, nhub_cap);
@@ -2715,8 +3002,10 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
     HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt,
               c->tune.gain_thread_deg, chunkd);
-    if (ls.maxdeg > chunkd)
+    if (ls.maxdeg > chunkd) {
         HP_CUDA(cudaMemsetAsync(B.ab_acc, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
+        HP_CUDA(cudaMemsetAsync(B.ab_acc2, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
+    }
     HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
     // the gain rows take G = sum min(deg, k) <= m entries: allocated for m, so
     // that no count is read back (the gain-build class completes its byte
@@ -2743,20 +3032,22 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     HP_CUDA(cudaMemcpyAsync(B.best_where, g.where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
     HP_CUDA(cudaMemcpyAsync(best_pw, B.pw, sizeof(unsigned long long) * k, cudaMemcpyDeviceToDevice, c->stream));
 
-    // learned LP proposals (opt.learned = 1) until a learned pass fails to
+    // learned LP proposals (opt.learned = 1, or 3 with the plain refiner as the
+    // judge of every learned pass) until a learned pass fails to
     // improve the exact cut; then the plain rule for the rest of the level
-    const bool learned = c->opt.learned == 1 && c->mlp_ready;
+    const bool learned = (c->opt.learned == 1 || c->opt.learned == 3) && c->mlp_ready;
+    const bool judged = learned && c->opt.learned == 3;
     const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
     const int patience = c->opt.refine_patience;
     HP_LAUNCH(c, ctl_init_kernel, 1, 1, 0, ctl, (const unsigned long long *)sc, patience, learned ? 1 : 0,
-              (const int32_t *)(B.goff + n), coarser);
+              (const int32_t *)(B.goff + n), coarser, judged ? 1 : 0);
     int64_t log_r0 = 0;
     if (recording) {
         unsigned long long lc = 0;
         HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
         log_r0 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
     }
-    PassCfg P{k, finest, any_big, recording, ls.maxdeg > chunkd, ls.maxdeg > mchunkd, ctl, best_pw};
+    PassCfg P{k, finest, any_big, recording, ls.maxdeg > chunkd, judged, ls.maxdeg > mchunkd, ctl, best_pw};
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
     const bool use_graph = graph_loop(c);
     RefineCtl h{};
@@ -2805,6 +3096,9 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         a.es = B.es;
         a.ee = B.ee;
         a.lock = B.lock;
+        a.prune = B.prune;
+        a.accp = B.accp;
+        a.status = c->d_status;
         a.pw = B.pw;
         a.best_pw = best_pw;
         a.opt = B.opt;

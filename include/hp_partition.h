@@ -58,7 +58,12 @@ typedef struct hp_options {
     int32_t  fm_passes;        /* 2-way FM passes per trial (default 10,
                                   hunyuangraph_admin.h:14)                                    */
     int32_t  max_levels;       /* coarsening level cap (default 64)                           */
-    int32_t  learned;          /* 0 plain refinement, 1 MLP move proposals, 2 record move log */
+    int32_t  learned;          /* 0 plain refinement, 1 MLP move proposals, 2 record move log,
+                                  3 MLP move proposals judged pass by pass: the plain refiner
+                                  takes over for the rest of a level as soon as a learned
+                                  pass lowers the exact cut less than the plain pass would
+                                  have on the same state (with 1, as soon as a learned pass
+                                  does not lower it)                                          */
     int32_t  validate;         /* 0 none, 1 structural check on the device (default)          */
     int32_t  trace;            /* 1: keep every level for hp_trace_*() (tests)                */
     int32_t  profile;          /* 1: time kernel classes with CUDA events into hp_stats.prof_* */

@@ -140,3 +140,37 @@ def test_learned_gain_over_plain(ctx):
     assert learned["apply"] <= 0.25 * plain["apply"]
     assert learned["rebuild"] <= 0.5 * plain["rebuild"]
     assert plain["ms"] / learned["ms"] >= 1.05, (plain["ms"], learned["ms"])
+
+
+@pytest.mark.parametrize("name", ["rmat14", "grid3d_32", "rgg16"])
+def test_judged_learned_passes(ctx, name):
+    """learned = 3: every learned LP pass is judged by the plain refiner on the
+    same state (exact cut decrease of both move sets from one afterburner walk
+    and one pass over the moved rows).  The judge's sum over the learned moves
+    is checked on the device against the applied pass's exact cut change (a
+    mismatch fails the call with HP_ERR_INTERNAL); results are deterministic and
+    the same in the CUDA-graph loop, the eager loop and the one-CTA small-level
+    loop, and the partition is balanced with its exact cut."""
+    if name == "rmat14":
+        g, k = graphs.rmat(14, 16, seed=3, wmin=1, wmax=100), 256
+    elif name == "grid3d_32":
+        g, k = graphs.grid3d(32, 32, 32, seed=2, wmin=1, wmax=10), 64
+    else:
+        g, k = graphs.rgg(1 << 16, 12.0, seed=4), 256
+    params, thr, _ = learn.load_params()
+    ctx.mlp_set_params(params, thr)
+    jopt = default_options(learned=3)
+    a_part, a_cut = ctx.partition_graph(g, k, options=jopt)
+    st = ctx.stats()
+    assert st.max_excess <= 0
+    assert a_cut == oracle.edgecut(g, a_part)
+    b_part, b_cut = ctx.partition_graph(g, k, options=jopt)
+    assert b_cut == a_cut and np.array_equal(b_part, a_part)
+    e_part, e_cut = ctx.partition_graph(g, k, options=default_options(learned=3, eager=1))
+    assert e_cut == a_cut and np.array_equal(e_part, a_part)
+    ctx.set_tuning(small_level_n=0)
+    try:
+        m_part, m_cut = ctx.partition_graph(g, k, options=jopt)
+    finally:
+        ctx.set_tuning(None)
+    assert m_cut == a_cut and np.array_equal(m_part, a_part)
