@@ -41,6 +41,8 @@ def main(argv=None) -> int:
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--eager", action="store_true", help="launch refinement passes one by one")
     ap.add_argument("--learned", action="store_true", help="learned move proposals (default weights)")
+    ap.add_argument("--judged", action="store_true",
+                    help="learned move proposals with the plain refiner judging every learned pass (learned = 3)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--write-part", action="store_true", help="write <graph>.part.<nparts>")
     ap.add_argument("--tuning", default=None,
@@ -48,6 +50,8 @@ def main(argv=None) -> int:
                          "loads the committed file of that workload if there is one, 'none' keeps the defaults")
     a = ap.parse_args(argv)
 
+    if a.judged:
+        a.learned = True
     graphs.set_threads(os.cpu_count() or 1)
     if a.workload:
         make, k_default, ub_default = WORKLOADS[a.workload]
@@ -71,7 +75,7 @@ def main(argv=None) -> int:
     if tpath:
         ctx.load_tuning(tpath)
         print(f"tuning: {tpath}")
-    opt = default_options(eager=1 if a.eager else 0, learned=1 if a.learned else 0, seed=a.seed)
+    opt = default_options(eager=1 if a.eager else 0, learned=(3 if a.judged else 1) if a.learned else 0, seed=a.seed)
     if a.learned:
         from . import learn
         params, thr, _ = learn.load_params()
