@@ -570,6 +570,89 @@ __device__ __forceinline__ RowBest row_best(const int32_t *__restrict__ gpart, c
     return r;
 }
 
+// Long gain rows (more than 32 entries) of a CTA, shared by all its warps: the
+// rows are queued in shared memory and the warps take them in turn, so that a
+// warp with many long rows does not hold the whole CTA at its next barrier
+// (the look-back of rb_candidates_kernel, the block sums of the LP selection).
+// A row's result does not depend on the warp that walks it.
+template <int NT>
+struct CoopRows {
+    int32_t o[NT], len[NT], p[NT];
+    long long pc[NT], bc[NT], wd[NT];
+    int32_t b[NT], np[NT];
+    int32_t n;
+};
+
+// Queues the calling thread's row when it is long; returns its queue slot or -1.
+// All NT threads call it; it ends with a barrier.
+template <int NT>
+__device__ __forceinline__ int coop_queue(CoopRows<NT> &S, bool coop, int32_t o, int32_t len, int32_t p)
+{
+    if (threadIdx.x == 0) S.n = 0;
+    __syncthreads();
+    int my = -1;
+    if (coop) {
+        my = atomicAdd(&S.n, 1);
+        S.o[my] = o;
+        S.len[my] = len;
+        S.p[my] = p;
+    }
+    __syncthreads();
+    return my;
+}
+
+// row_best with the CTA's long rows shared by all its warps (CoopRows).  All NT
+// threads call it.
+template <int NT>
+__device__ __forceinline__ RowBest row_best_cta(CoopRows<NT> &S, const int32_t *__restrict__ gpart,
+                                                const int32_t *__restrict__ gconn, int32_t o, int32_t len,
+                                                int32_t p, int32_t k)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    RowBest r{0, 0, 0, -1, 0};
+    const bool coop = len > 32;
+    if (!coop)
+        for (int32_t j = o; j < o + len; j++) {
+            const int32_t q = gpart[j];
+            if (q < 0) break;
+            const int32_t cq = gconn[j];
+            r.wd += cq;
+            r.np += cq > 0;
+            if (q == p) { r.pc = cq; continue; }
+            if (cq > r.bc) { r.bc = cq; r.b = q; }   // ascending parts: first max = lowest part
+        }
+    const int my = coop_queue<NT>(S, coop, o, len, p);
+    const int nc = S.n;
+    for (int i = wid; i < nc; i += NT / 32) {
+        const int32_t so = S.o[i], sl = S.len[i], sp = S.p[i];
+        int32_t lpc = 0, lbc = 0, lb = -1, lnp = 0;
+        long long lwd = 0;
+        const bool dense = sl == k;   // entry j is part j
+        for (int32_t j = lane; j < sl; j += 32) {
+            const int32_t q = dense ? j : gpart[so + j];
+            if (q < 0) break;   // padding runs to the end of the row
+            const int32_t cq = gconn[so + j];
+            lwd += cq;
+            lnp += cq > 0;
+            if (q == sp) { lpc = cq; continue; }
+            if (cq > lbc) { lbc = cq; lb = q; }
+        }
+        lpc = hp::warp_sum(lpc);
+        lnp = hp::warp_sum(lnp);
+        lwd = hp::warp_sum64(lwd);
+#pragma unroll
+        for (int sh = 16; sh > 0; sh >>= 1) {
+            const int32_t ob = __shfl_xor_sync(HP_FULL_MASK, lb, sh);
+            const int32_t oc = __shfl_xor_sync(HP_FULL_MASK, lbc, sh);
+            if (ob >= 0 && (lb < 0 || oc > lbc || (oc == lbc && ob < lb))) { lb = ob; lbc = oc; }
+        }
+        if (lane == 0) { S.pc[i] = lpc; S.bc[i] = lbc; S.b[i] = lb; S.wd[i] = lwd; S.np[i] = lnp; }
+    }
+    __syncthreads();
+    if (my >= 0) { r.pc = S.pc[my]; r.bc = S.bc[my]; r.b = S.b[my]; r.wd = S.wd[my]; r.np = S.np[my]; }
+    return r;
+}
+
 // ---- LP ------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
@@ -579,6 +662,7 @@ lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__r
 {
     hp::pdl_wait();
     if (gate && *gate != 0) return;   // graph mode: the learned kernel runs this pass
+    __shared__ CoopRows<256> S;
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
     int cand = 0;
     int32_t p = 0, o = 0, len = 0;
@@ -587,7 +671,7 @@ lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__r
         o = goff[v];
         len = goff[v + 1] - o;
     }
-    const RowBest rb = row_best(gpart, gconn, o, len, p, k);
+    const RowBest rb = row_best_cta<256>(S, gpart, gconn, o, len, p, k);
     const int64_t pc = rb.pc, bc = rb.bc;
     const int32_t b = rb.b;
     if (v < n) {
@@ -622,6 +706,7 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
     hp::pdl_wait();
     if (gate && *gate != 1) return;   // graph mode: the plain kernel runs this pass
     __shared__ hp::MlpSmem sm;
+    __shared__ CoopRows<256> S;
     hp::mlp_load_smem(sm, params);
     __syncthreads();
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -635,7 +720,7 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
         o = goff[v];
         len = goff[v + 1] - o;
     }
-    const RowBest rb = row_best(gpart, gconn, o, len, p, k);
+    const RowBest rb = row_best_cta<256>(S, gpart, gconn, o, len, p, k);
     if (v < n) {
         const int64_t pc = rb.pc, bc = rb.bc, wd = rb.wd;
         const int32_t b = rb.b, np = rb.np;
@@ -1355,6 +1440,7 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
     hp::pdl_wait();
     __shared__ int32_t s_scan[RB_TILE / 32 + 2];
     __shared__ int32_t s_excl;
+    __shared__ CoopRows<RB_TILE> S;
     int64_t tile;
     unsigned epoch;
     hp::lb_begin(lb, &tile, &epoch);
@@ -1380,7 +1466,7 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
     if (!STRONG) {
         // best underweight part by connectivity (first, i.e. lowest part, among
         // equals) and the connectivity to the own part; rows of more than
-        // RB_COOP entries are walked by the whole warp, one row at a time
+        // RB_COOP entries are walked by a whole warp, any warp of the CTA
         int64_t pc = 0, bc = 0;
         int32_t b = -1;
         const bool coop = cand && len > RB_COOP;
@@ -1393,12 +1479,11 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
                 if (ufl[q] && cq > bc) { bc = cq; b = q; }
             }
         }
-        unsigned cm = __ballot_sync(HP_FULL_MASK, coop);
-        while (cm) {
-            const int src = __ffs(cm) - 1;
-            cm &= cm - 1;
-            const int32_t so = __shfl_sync(HP_FULL_MASK, o, src), sl = __shfl_sync(HP_FULL_MASK, len, src);
-            const int32_t sp = __shfl_sync(HP_FULL_MASK, p, src);
+        // the CTA's long rows, shared by all its warps
+        const int my = coop_queue<RB_TILE>(S, coop, o, len, p);
+        const int nc = S.n;
+        for (int i = threadIdx.x >> 5; i < nc; i += RB_TILE / 32) {
+            const int32_t so = S.o[i], sl = S.len[i], sp = S.p[i];
             int32_t lpc = 0, lbc = 0, lb = -1;
             const bool dense = sl == k;   // entry j is part j
             for (int32_t j = lane; j < sl; j += 32) {
@@ -1415,8 +1500,10 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
                 const int32_t oc = __shfl_xor_sync(HP_FULL_MASK, lbc, sh);
                 if (ob >= 0 && (lb < 0 || oc > lbc || (oc == lbc && ob < lb))) { lb = ob; lbc = oc; }
             }
-            if (lane == src) { pc = lpc; bc = lbc; b = lb; }
+            if (lane == 0) { S.pc[i] = lpc; S.bc[i] = lbc; S.b[i] = lb; }
         }
+        __syncthreads();
+        if (my >= 0) { pc = S.pc[my]; bc = S.bc[my]; b = S.b[my]; }
         if (cand) {
             int64_t g = 0;
             bool ok = true;
