@@ -112,6 +112,19 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def wait_first(self, timeout=10.0):
+        """Blocks until nvidia-smi has written its first sample: its start-up
+        (driver initialisation in the sampling process) then happens before the
+        timed steps, not inside them."""
+        t_end = time.time() + timeout
+        while self.proc is not None and time.time() < t_end:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    return
+            except OSError:
+                return
+            time.sleep(0.05)
+
     def stop(self):
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
         if self.proc is None:
@@ -546,6 +559,7 @@ def main():
 
     sampler = ClockSampler(local)
     sampler.start()
+    sampler.wait_first()
     time.sleep(0.3)
     step_ms, cut, stats = timed_arm(opt_main)
     other = timed_arm(opt_other) if compare else None

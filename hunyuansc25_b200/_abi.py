@@ -99,6 +99,7 @@ TUNING_FIELDS = [
     "contract_hybrid",
     "apply_chunk_deg",
     "pdl",
+    "graph_passes",
 ]
 
 TUNING_DEFAULTS = {
@@ -121,6 +122,7 @@ TUNING_DEFAULTS = {
     "contract_hybrid": 1,
     "apply_chunk_deg": 4096,
     "pdl": 1,
+    "graph_passes": 1,
 }
 
 TUNE_DEG_MAX = 1 << 24
@@ -149,6 +151,7 @@ def tuning_violation(t: dict):
         ("contract_hybrid", 0, 1),
         ("apply_chunk_deg", t["gain_thread_deg"], TUNE_DEG_MAX),
         ("pdl", 0, 1),
+        ("graph_passes", 0, 1),
     ]
     for name, lo, hi in lim:
         if not lo <= int(t[name]) <= hi:
@@ -157,7 +160,7 @@ def tuning_violation(t: dict):
 
 
 class HpTuning(C.Structure):
-    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 5)]
+    _fields_ = [(name, C.c_int32) for name in TUNING_FIELDS] + [("reserved", C.c_int32 * 4)]
 
     @classmethod
     def from_dict(cls, d: dict) -> "HpTuning":

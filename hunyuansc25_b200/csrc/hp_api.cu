@@ -625,6 +625,7 @@ HP_API void hp_tuning_default(hp_tuning *t)
     t->contract_hybrid = 1;
     t->apply_chunk_deg = 4096;
     t->pdl = 1;
+    t->graph_passes = 1;
 }
 
 namespace {
@@ -651,6 +652,7 @@ const char *tuning_violation(const hp_tuning &t)
     if (!in(t.contract_hybrid, 0, 1)) return "contract_hybrid";
     if (!in(t.apply_chunk_deg, t.gain_thread_deg, HP_TUNE_DEG_MAX)) return "apply_chunk_deg";
     if (!in(t.pdl, 0, 1)) return "pdl";
+    if (!in(t.graph_passes, 0, 1)) return "graph_passes";
     for (int32_t r : t.reserved)
         if (r != 0) return "reserved";
     return nullptr;

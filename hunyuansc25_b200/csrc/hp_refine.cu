@@ -3033,7 +3033,8 @@ int run_passes_graph(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P,
 bool graph_loop(const hp_context *c)
 {
     const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
-    return !c->opt.eager && !recording && getenv("HP_DEBUG_PASSES") == nullptr && c->opt.refine_patience >= 0 &&
+    return !c->opt.eager && c->tune.graph_passes && !recording && getenv("HP_DEBUG_PASSES") == nullptr &&
+           c->opt.refine_patience >= 0 &&
            c->stream != nullptr && c->stream != cudaStreamLegacy;
 }
 

@@ -63,6 +63,7 @@ SPACE = {
     "contract_hybrid": [0, 1],
     "apply_chunk_deg": [256, 512, 1024, 2048, 4096, 8192],
     "pdl": [0, 1],
+    "graph_passes": [0, 1],
 }
 
 

@@ -201,7 +201,11 @@ typedef struct hp_tuning {
                                     previous one drains and waits for it on the device
                                     (programmatic dependent launch) (1), or after it (0)
                                                                                   [0, 1]        1 */
-    int32_t reserved[5];         /* zero */
+    int32_t graph_passes;        /* refinement: each level's pass loop as one CUDA graph with
+                                    device-side control (1), or its passes launched one by one
+                                    (0); hp_options.eager = 1 forces the latter.  Results are
+                                    identical                                     [0, 1]        1 */
+    int32_t reserved[4];         /* zero */
 } hp_tuning;
 
 void hp_tuning_default(hp_tuning *t);

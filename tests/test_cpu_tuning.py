@@ -35,7 +35,7 @@ def test_library_defaults_match_python():
     t = HpTuning()
     lib.hp_tuning_default(C.byref(t))
     assert t.as_dict() == TUNING_DEFAULTS
-    assert list(t.reserved) == [0] * 5
+    assert list(t.reserved) == [0] * 4
     assert tuning_violation(TUNING_DEFAULTS) is None
 
 
