@@ -596,6 +596,10 @@ def main():
     _, _, pst = one_step(opts(learned_main, profile=1))
     eager_ms, ecut, _ = one_step(opts(learned_main, eager=1))
     _, _, est = one_step(opts(learned_main, profile=1, eager=1))
+    tuned = ctx.get_tuning()   # the workload's tuning picks the loop the timed steps ran
+    ctx.set_tuning(dict(tuned, graph_passes=1))
+    graph_ms, gcut, _ = one_step(opts(learned_main))
+    ctx.set_tuning(tuned)
     ncls = len(PROF_NAMES)
     prof_ms = np.array(list(pst.prof_ms), dtype=np.float64)
     prof_bytes = np.array(list(pst.prof_bytes), dtype=np.float64)
@@ -631,9 +635,12 @@ def main():
                                     "launches": int(prof_launch[i]), "source": source[i]}
                     for i in timed},
     }
-    graph_vs_eager = {"graph_ms": round(job_ms / args.steps, 3), "eager_ms": round(eager_ms, 3),
-                      "speedup": round(eager_ms / (job_ms / args.steps), 4), "identical_cut": int(ecut) == int(cut),
-                      "eager_launches": int(est.kernel_launches)}
+    graph_vs_eager = {"timed_loop": "CUDA graph per level" if tuned["graph_passes"] else "launched passes",
+                      "graph_ms": round(graph_ms, 3), "eager_ms": round(eager_ms, 3),
+                      "speedup": round(eager_ms / graph_ms, 4),
+                      "identical_cut": int(ecut) == int(cut) == int(gcut),
+                      "eager_launches": int(est.kernel_launches),
+                      "note": "one step each outside the timed region; the tuning field graph_passes picks the loop"}
 
     learned_cmp = None
     plain_cut = None if learned_main else int(cut)
@@ -695,7 +702,8 @@ def main():
                         "levels": last.nlevels, "coarsest_nvtxs": last.coarsest_nvtxs,
                         "phase_ms": {"coarsen": round(last.ms_coarsen, 3), "init": round(last.ms_init, 3),
                                      "uncoarsen": round(last.ms_uncoarsen, 3)}},
-            "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
+            "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms),
+                        "all": [round(x, 2) for x in step_ms]},
             "refine_passes": int(last.refine_passes),
             "graph_vs_eager": graph_vs_eager,
         }
