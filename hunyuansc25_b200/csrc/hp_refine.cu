@@ -570,6 +570,26 @@ __device__ __forceinline__ RowBest row_best(const int32_t *__restrict__ gpart, c
     return r;
 }
 
+// The best partition so far, copied by the first proposal kernel of the next
+// pass: when the previous pass set the control block's take flag, the partition
+// it left is the best so far, and that kernel, which reads where[v] of every
+// vertex anyway, stores it into best_where (and block / tile 0 the part weights
+// into best_pw) before any move of its own pass is applied.  A pass that ends
+// the level needs no copy: where is then either the best (take set) or
+// restored from best_where.
+struct BestCopy {
+    const int32_t *take;
+    int32_t *best_where;
+    const unsigned long long *pw;
+    unsigned long long *best_pw;
+    int32_t k;
+    __device__ __forceinline__ bool on() const { return *take != 0; }
+    __device__ __forceinline__ void parts() const
+    {
+        for (int32_t q = threadIdx.x; q < k; q += blockDim.x) best_pw[q] = pw[q];
+    }
+};
+
 // Long gain rows (more than 32 entries) of a CTA, shared by all its warps: the
 // rows are queued in shared memory and the warps take them in turn, so that a
 // warp with many long rows does not hold the whole CTA at its next barrier
@@ -658,18 +678,22 @@ __global__ void __launch_bounds__(256)
 lp_select_kernel(int32_t n, const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
                  const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
                  const int8_t *__restrict__ lock, int finest, int32_t *__restrict__ dest,
-                 int32_t *__restrict__ pregain, unsigned long long *d_ncand, const int32_t *gate, int32_t k)
+                 int32_t *__restrict__ pregain, unsigned long long *d_ncand, const int32_t *gate, int32_t k,
+                 BestCopy bcp)
 {
     hp::pdl_wait();
     if (gate && *gate != 0) return;   // graph mode: the learned kernel runs this pass
     __shared__ CoopRows<256> S;
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool copy = bcp.on();
+    if (copy && blockIdx.x == 0) bcp.parts();
     int cand = 0;
     int32_t p = 0, o = 0, len = 0;
     if (v < n) {
         p = where[v];
         o = goff[v];
         len = goff[v + 1] - o;
+        if (copy) bcp.best_where[v] = p;
     }
     const RowBest rb = row_best_cta<256>(S, gpart, gconn, o, len, p, k);
     const int64_t pc = rb.pc, bc = rb.bc;
@@ -701,7 +725,7 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
                          const int64_t *__restrict__ opt, const float *__restrict__ params, float threshold,
                          int32_t *__restrict__ dest, int32_t *__restrict__ pregain, unsigned long long *d_ncand,
                          const int32_t *gate, int32_t k, int8_t *__restrict__ prune,
-                         unsigned long long *d_ncandp, const int32_t *judge_flag)
+                         unsigned long long *d_ncandp, const int32_t *judge_flag, BestCopy bcp)
 {
     hp::pdl_wait();
     if (gate && *gate != 1) return;   // graph mode: the plain kernel runs this pass
@@ -710,6 +734,8 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
     hp::mlp_load_smem(sm, params);
     __syncthreads();
     const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool copy = bcp.on();
+    if (copy && blockIdx.x == 0) bcp.parts();
     int cand = 0, candp = 0;
     int8_t pr = 0;
     float f[HP_MLP_IN] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -719,6 +745,7 @@ lp_select_learned_kernel(int32_t n, const int32_t *__restrict__ goff, const int3
         p = where[v];
         o = goff[v];
         len = goff[v + 1] - o;
+        if (copy) bcp.best_where[v] = p;
     }
     const RowBest rb = row_best_cta<256>(S, gpart, gconn, o, len, p, k);
     if (v < n) {
@@ -1225,28 +1252,6 @@ judge_delta_kernel(const int32_t *flag, const int32_t *__restrict__ list, const 
 }
 
 // ---- applying moves -------------------------------------------------------------
-__global__ void __launch_bounds__(256)
-c_delta_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
-               const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
-               const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
-               const int32_t *__restrict__ dest, int32_t *__restrict__ oldp, int before,
-               unsigned long long *d_c, int32_t k)
-{
-    hp::pdl_wait();
-    const int64_t nm = (int64_t)*d_nmoves;
-    if ((int64_t)blockIdx.x * blockDim.x >= nm) return;   // whole CTA idle (uniform)
-    long long acc = 0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm; i += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t v = moves[i];
-        const int32_t o = goff[v], len = goff[v + 1] - o;
-        int32_t from, to;
-        if (before) { from = where[v]; to = dest[v]; oldp[i] = from; }
-        else { from = oldp[i]; to = where[v]; }
-        acc += (long long)row_conn(gpart + o, gconn + o, len, to, k) - row_conn(gpart + o, gconn + o, len, from, k);
-    }
-    hp::block_add_to<256>(acc, d_c);
-}
-
 // Effect of one move on its neighbours' gain rows.  A vertex's own row does
 // not depend on its own part: only neighbours' rows change.  Dense neighbour
 // rows (deg >= k) take the change in place; a sparse neighbour is queued once
@@ -1435,7 +1440,7 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
                      int32_t *__restrict__ K, int32_t *__restrict__ V, int32_t *__restrict__ dest,
                      int32_t *__restrict__ d_cnt, int32_t *__restrict__ pstart, int32_t *__restrict__ pend,
                      unsigned long long *tile_status, hp::LbCtl *lb, unsigned *status,
-                     const int8_t *__restrict__ ufl)
+                     const int8_t *__restrict__ ufl, BestCopy bcp)
 {
     hp::pdl_wait();
     __shared__ int32_t s_scan[RB_TILE / 32 + 2];
@@ -1455,8 +1460,11 @@ rb_candidates_kernel(int32_t n, const int32_t *__restrict__ where, const int32_t
     const int32_t v = in ? (int32_t)v64 : 0;
     int32_t p = 0;
     bool cand = false;   // in an overweight part and light enough to leave it
+    const bool copy = bcp.on();
+    if (copy && tile == 0) bcp.parts();
     if (in) {
         p = where[v];
+        if (copy) bcp.best_where[v] = p;
         const int64_t pwp = (int64_t)pw[p];
         cand = STRONG ? (pwp > maxp[p] && (int64_t)vwgt[v] < 2 * (pwp - opt[p]))
                       : (pwp > maxp[p] && 2 * (int64_t)vwgt[v] < 3 * (pwp - opt[p]));
@@ -1897,7 +1905,7 @@ struct RefineBufs {
 // longest row above huged.
 enum { S_NMOVES = 0, S_C1 = 1, S_C2 = 2, S_EXCESS = 3, S_NCAND = 4, S_CUT2 = 5, S_DIRTY = 6,
        S_HUGEMV = 7, S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_NCANDP = 11, S_JN = 12, S_JP = 13, S_JL = 14,
-       S_PASS_END = 16, S_BIGCNT = 16 };
+       S_PASS_END = 16, S_BIGCNT = 16, S_DONE = 20 };
 
 int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_t *small_list,
                const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt,
@@ -1974,7 +1982,8 @@ unsigned plan_grid(const hp_context *c, int64_t cap)
 // radix sort by key -> prefix weights and part bounds (rb_rank_kernel).
 // Returns the arrays holding the sorted pairs.
 template <bool STRONG>
-int rank_candidates(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, int32_t **Ks, int32_t **Vs)
+int rank_candidates(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, int32_t **Ks, int32_t **Vs,
+                    const BestCopy &bcp)
 {
     const int32_t n = g.n;
     unsigned long long *sc = c->d_scal;
@@ -1984,7 +1993,7 @@ int rank_candidates(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, int32_t
     if (ct > c->lb_cap || 2 * rt > c->lb_cap) return HP_ERR_INTERNAL;
     HP_LAUNCH(c, rb_candidates_kernel<STRONG>, (unsigned)ct, RB_TILE, 0, n, g.where, g.vwgt, B.pw, B.maxp, B.opt,
               B.goff, B.gpart, B.gconn, B.und, (const int32_t *)&sc[S_NU], k, B.K, B.V, B.dest, d_cnt, B.pstart,
-              B.pend, c->lb_status, c->lb_ctl, c->d_status, B.ufl);
+              B.pend, c->lb_status, c->lb_ctl, c->d_status, B.ufl, bcp);
     bool in_tmp = false;
     HP_TRY(hp_sort_pairs(c, B.K, B.V, B.K2, B.V2, n, d_cnt, key_bits_for(k), &in_tmp));
     *Ks = in_tmp ? B.K2 : B.K;
@@ -2001,22 +2010,22 @@ MoveSink move_sink(hp_context *c, const RefineBufs &B, int32_t k)
 }
 
 // The undersized-part list of a weak pass is built by ctl_begin_kernel.
-int weak_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
+int weak_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const BestCopy &bcp)
 {
     unsigned long long *sc = c->d_scal;
     int32_t *Ks, *Vs;
-    HP_TRY(rank_candidates<false>(c, g, B, k, &Ks, &Vs));
+    HP_TRY(rank_candidates<false>(c, g, B, k, &Ks, &Vs, bcp));
     HP_LAUNCH(c, rw_select_kernel, (unsigned)(c->sm_count * 8), 256, 0, Ks, Vs,
               (const int32_t *)&sc[S_LISTCNT], B.pre, B.pstart, B.pw, B.maxp, B.dest, move_sink(c, B, k));
     return HP_OK;
 }
 
-int strong_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k)
+int strong_rebalance(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const BestCopy &bcp)
 {
     const int32_t n = g.n;
     unsigned long long *sc = c->d_scal;
     int32_t *Ks, *Vs;
-    HP_TRY(rank_candidates<true>(c, g, B, k, &Ks, &Vs));
+    HP_TRY(rank_candidates<true>(c, g, B, k, &Ks, &Vs, bcp));
     const unsigned pg = (unsigned)(c->sm_count * 8);
     const int32_t *d_cnt = (const int32_t *)&sc[S_LISTCNT];
     int32_t *d_np = (int32_t *)&sc[S_NP];
@@ -2100,30 +2109,56 @@ __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int3
 
 // End of a pass: the exact cut change, the learned fallback, the stall rule, the
 // best partition and the loop condition, in the order of the host loop they replace.
-// One CTA of 1024 threads: the block first reduces the max excess over the
-// parts (max_p pw[p] - maxp[p]) into the status slot, then thread 0 advances
-// the control block.
-__global__ void __launch_bounds__(1024)
-ctl_end_kernel(RefineCtl *s, unsigned long long *sc, cudaGraphConditionalHandle hloop, int graph, int32_t k,
-               const unsigned long long *__restrict__ pw, const int64_t *__restrict__ maxp, unsigned *status)
+// End of a pass: the after-move half of the exact cut change (c2: the moved
+// vertices' gain rows, rebuilt, at the old and new parts; c1 came with the moves),
+// then the control step, run by the last CTA to finish (a ticket on *done,
+// reset by that CTA): the max excess over the parts (max_p pw[p] - maxp[p]) and,
+// by thread 0, the control block's advance and the graph loop's condition.
+// One launch instead of a cut-change kernel and a one-CTA control kernel.
+__global__ void __launch_bounds__(256)
+pass_end_kernel(const int32_t *__restrict__ moves, const unsigned long long *d_nmoves,
+                const int32_t *__restrict__ goff, const int32_t *__restrict__ gpart,
+                const int32_t *__restrict__ gconn, const int32_t *__restrict__ where,
+                const int32_t *__restrict__ oldp, int32_t k, RefineCtl *s, unsigned long long *sc,
+                cudaGraphConditionalHandle hloop, int graph, const unsigned long long *__restrict__ pw,
+                const int64_t *__restrict__ maxp, unsigned *status, unsigned *done)
 {
     hp::pdl_wait();
+    __shared__ bool s_last;
+    __shared__ long long s_max[256 / 32];
+    const int64_t nm = (int64_t)*d_nmoves;
+    long long acc = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nm; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t v = moves[i];
+        const int32_t o = goff[v], len = goff[v + 1] - o;
+        acc += (long long)row_conn(gpart + o, gconn + o, len, where[v], k) -
+               row_conn(gpart + o, gconn + o, len, oldp[i], k);
+    }
+    hp::block_add_to<256>(acc, &sc[S_C2]);   // ends with a barrier
+    if (threadIdx.x == 0) {
+        __threadfence();   // this CTA's sum is visible before its ticket
+        s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
     long long m = LLONG_MIN;
     for (int p = threadIdx.x; p < k; p += blockDim.x) {
         const long long e = (long long)pw[p] - maxp[p];
         m = e > m ? e : m;
     }
     m = hp::warp_max64(m);
-    __shared__ long long s_max[32];
     if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
     __syncthreads();
     if (threadIdx.x != 0) return;
     for (int w = 1; w < (int)(blockDim.x >> 5); w++) m = s_max[w] > m ? s_max[w] : m;
+    *done = 0u;
+    volatile unsigned long long *vs = sc;
     sc[S_EXCESS] = (unsigned long long)m;
-    const long long c1 = (long long)sc[S_C1], c2 = (long long)sc[S_C2];
+    const long long c1 = (long long)vs[S_C1], c2 = (long long)vs[S_C2];
     // the judge's sum over the learned moves is the applied pass's exact change
-    if (s->judge_pass && (long long)sc[S_JL] != c1 + c2) atomicOr(status, HP_STATUS_OVERFLOW);
-    const int cont = ctl_advance(s, m, c1, c2, (long long)sc[S_NMOVES], (long long)sc[S_NCAND], (long long)sc[S_JP]);
+    if (s->judge_pass && (long long)vs[S_JL] != c1 + c2) atomicOr(status, HP_STATUS_OVERFLOW);
+    const int cont = ctl_advance(s, m, c1, c2, (long long)vs[S_NMOVES], (long long)vs[S_NCAND], (long long)vs[S_JP]);
     if (graph) cudaGraphSetConditional(hloop, cont ? 1u : 0u);
 }
 
@@ -2198,17 +2233,6 @@ ctl_begin_kernel(const RefineCtl *s, unsigned long long *sc, cudaGraphConditiona
         undersized_block(k, pw, maxp, und, (int32_t *)&sc[S_NU], s_scan);
         for (int32_t q = threadIdx.x; q < k; q += blockDim.x) ufl[q] = (int64_t)pw[q] < maxp[q];
     }
-}
-
-__global__ void save_best_kernel(const RefineCtl *s, int32_t n, const int32_t *__restrict__ where,
-                                 int32_t *__restrict__ best_where, int32_t k,
-                                 const unsigned long long *__restrict__ pw, unsigned long long *__restrict__ best_pw)
-{
-    hp::pdl_wait();
-    if (!s->take) return;
-    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) best_where[i] = where[i];
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += stride) best_pw[i] = pw[i];
 }
 
 __global__ void restore_best_kernel(const RefineCtl *s, int32_t n, const int32_t *__restrict__ best_where,
@@ -2326,6 +2350,11 @@ struct PassCfg {
     unsigned long long *best_pw;
 };
 
+BestCopy best_copy(const RefineBufs &B, const PassCfg &P)
+{
+    return BestCopy{&P.ctl->take, B.best_where, B.pw, P.best_pw, P.k};
+}
+
 // Proposal phase of one pass.  Eager mode launches the LP selection kernel the
 // host chose; graph mode launches both when the MLP is loaded, gated by the
 // control block's learned_pass flag.
@@ -2344,10 +2373,10 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
         if (both_lp || learned_pass)
             HP_LAUNCH(c, lp_select_learned_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, g.xadj,
                       B.lock, P.finest ? 1 : 0, B.pw, B.maxp, B.opt, c->mlp_params, c->mlp_threshold, B.dest,
-                      B.pregain, &sc[S_NCAND], gate, k, B.prune, &sc[S_NCANDP], J.flag);
+                      B.pregain, &sc[S_NCAND], gate, k, B.prune, &sc[S_NCANDP], J.flag, best_copy(B, P));
         if (both_lp || !learned_pass)
             HP_LAUNCH(c, lp_select_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, B.lock,
-                      P.finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND], gate, k);
+                      P.finest ? 1 : 0, B.dest, B.pregain, &sc[S_NCAND], gate, k, best_copy(B, P));
         if (P.recording)
             HP_LAUNCH(c, log_candidates_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, g.xadj,
                       P.finest ? 1 : 0, B.pw, B.maxp, B.opt, B.dest, B.pregain, B.recof, c->log_x, c->log_v,
@@ -2387,8 +2416,8 @@ int pass_propose(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, int
                       cnt);
     } else {
         const int btok = hp_prof_begin(c);
-        if (mode == 1) HP_TRY(weak_rebalance(c, g, B, k));
-        else HP_TRY(strong_rebalance(c, g, B, k));
+        if (mode == 1) HP_TRY(weak_rebalance(c, g, B, k, best_copy(B, P)));
+        else HP_TRY(strong_rebalance(c, g, B, k, best_copy(B, P)));
         hp_prof_end(c, btok, HP_PROF_REBALANCE, 0);
         if (unsigned long long *cnt = hp_prof_counter(c, HP_PROF_REBALANCE))
             HP_LAUNCH(c, rebalance_bytes_kernel, std::min(nblk(n), pg), 256, 0, n, g.where, B.pw, B.maxp, B.goff,
@@ -2428,11 +2457,8 @@ int pass_apply(hp_context *c, HpLevel &g, RefineBufs &B, const PassCfg &P, cudaG
         HP_LAUNCH(c, rebuild_bytes_kernel, pg, 256, 0, B.small_l, (const int32_t *)&sc[S_DIRTY], B.big_l,
                   ((const int32_t *)&sc[S_DIRTY]) + 1, g.xadj, B.goff, cnt);
     atok = hp_prof_begin(c);
-    HP_LAUNCH(c, c_delta_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.dest,
-              B.oldp, 0, &sc[S_C2], k);
-    HP_LAUNCH(c, ctl_end_kernel, 1, 1024, 0, P.ctl, sc, hloop, graph, k, B.pw, B.maxp, c->d_status);
-    HP_LAUNCH(c, save_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, P.ctl, n,
-              g.where, B.best_where, k, B.pw, P.best_pw);
+    HP_LAUNCH(c, pass_end_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], B.goff, B.gpart, B.gconn, g.where, B.oldp, k,
+              P.ctl, sc, hloop, graph, B.pw, B.maxp, c->d_status, (unsigned *)&sc[S_DONE]);
     hp_prof_end(c, atok, HP_PROF_APPLY, 0);
     if (unsigned long long *cnt = hp_prof_counter(c, HP_PROF_APPLY))
         HP_LAUNCH(c, apply_bytes_kernel, mg, 256, 0, B.moves, &sc[S_NMOVES], g.xadj, B.goff, B.gpart, k, n, P.ctl,
@@ -2952,8 +2978,8 @@ struct GraphKeep {
 };
 
 // The level's pass loop as one CUDA graph:
-//   WHILE (cont) { ctl_begin; SWITCH (mode) { LP | weak | strong }; apply; ctl_end; save_best }
-// ctl_end sets the WHILE condition, ctl_begin the SWITCH value; nothing returns to
+//   WHILE (cont) { ctl_begin; SWITCH (mode) { LP | weak | strong }; apply; pass_end }
+// pass_end sets the WHILE condition, ctl_begin the SWITCH value; nothing returns to
 // the host between passes.  Launch accounting: kernels per body x passes per mode,
 // read back from the control block.
 // host milliseconds per step of run_passes_graph (HP_DEBUG_LEVELS diagnostics):
@@ -3086,7 +3112,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.plan_cnt = ralloc_t<int32_t>(c, 2);
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_BIGCNT + 2), c->stream));
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_DONE + 1), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
     HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt,
               c->tune.gain_thread_deg, chunkd);
