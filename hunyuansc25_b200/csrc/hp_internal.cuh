@@ -94,6 +94,7 @@ struct hp_context {
     std::vector<HpLevel> levels;
     bool trace_valid = false;
     bool weight_check = false;           // total edge weight >= 2^31: contractions check pair bounds
+    bool learned_skewed = false;         // the input's degrees are skewed enough for the learned proposals
     hp_options opt = {};
 };
 
@@ -106,6 +107,7 @@ constexpr int HP_TUNE_DEG_MAX = 1 << 24;
 constexpr int HP_TUNE_SMALL_LEVEL_MAX = 32768;   // refine_small_kernel's staged prefix weights
 constexpr int HP_TUNE_SMALL_MATCH_MAX = 8192;    // match_small_kernel's shared-memory state
 constexpr int HP_TUNE_SMEM_CN_MAX = 49152;       // shared-memory dense accumulator of the contraction
+constexpr int64_t HP_LEARNED_SKEW = 16;          // learned proposals: max degree / mean degree of the input
 
 #define HP_NSCAL 64
 #define HP_ALIGN 256

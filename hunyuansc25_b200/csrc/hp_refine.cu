@@ -3149,7 +3149,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     // learned LP proposals (opt.learned = 1, or 3 with the plain refiner as the
     // judge of every learned pass) until a learned pass fails to
     // improve the exact cut; then the plain rule for the rest of the level
-    const bool learned = (c->opt.learned == 1 || c->opt.learned == 3) && c->mlp_ready;
+    const bool learned = (c->opt.learned == 1 || c->opt.learned == 3) && c->mlp_ready && c->learned_skewed;
     const bool judged = learned && c->opt.learned == 3;
     const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
     const int patience = c->opt.refine_patience;
@@ -3288,6 +3288,16 @@ int hp_uncoarsen(hp_context *c, int32_t nparts, const int64_t *h_opt, const int6
     HP_CUDA(cudaMemcpyAsync(ls.data(), d_ls, sizeof(LevelStat) * (size_t)(L + 1), cudaMemcpyDeviceToHost,
                             c->stream));
     HP_CUDA(cudaStreamSynchronize(c->stream));
+    // The learned move proposals run on inputs whose degree distribution is as
+    // skewed as the power-law graphs the network was trained for and validated on
+    // (largest degree at least HP_LEARNED_SKEW times the mean degree; R-MAT scale
+    // 22: 10^4; the 3-D grid and the RGG: 1-3); on the others the plain refiner
+    // runs, as it would after a hand-over.
+    {
+        const HpLevel &g0 = c->levels[0];
+        const int64_t mean0 = std::max<int64_t>(1, g0.m / std::max<int64_t>(1, g0.n));
+        c->learned_skewed = (int64_t)ls[0].maxdeg >= HP_LEARNED_SKEW * mean0;
+    }
     std::vector<LevelLaunches> ll(L + 1);
     GraphKeep keep;
     keep.c = c;

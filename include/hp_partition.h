@@ -63,7 +63,10 @@ typedef struct hp_options {
                                   takes over for the rest of a level as soon as a learned
                                   pass lowers the exact cut less than the plain pass would
                                   have on the same state (with 1, as soon as a learned pass
-                                  does not lower it)                                          */
+                                  does not lower it).  1 and 3 apply to inputs whose largest
+                                  degree is at least 16x the mean degree (the power-law
+                                  graphs the network is validated on); other inputs are
+                                  refined by the plain rule                                   */
     int32_t  validate;         /* 0 none, 1 structural check on the device (default)          */
     int32_t  trace;            /* 1: keep every level for hp_trace_*() (tests)                */
     int32_t  profile;          /* 1: time kernel classes with CUDA events into hp_stats.prof_* */
