@@ -20,17 +20,20 @@ pytestmark = pytest.mark.gpu
 SMALL_CLASSES = dict(match_warp_deg=4, match_cta_deg=24, contract_thread_row=8, contract_warp_row=16,
                      contract_cta_row=48, gain_thread_deg=8, gain_hub_deg=24, warp_dense_k=0,
                      grid_ctas_per_sm=1, dense_sparse_ratio=1, small_level_n=32768, chunk_deg=8,
-                     trial_cta_n=1, contract_smem_cn=49152, small_match_n=8192)
+                     trial_cta_n=1, contract_smem_cn=49152, small_match_n=8192, contract_hybrid=1,
+                     apply_chunk_deg=8)
 # the largest per-thread and warp classes, many CTAs, every level on the
-# multi-kernel pass loop
+# multi-kernel pass loop, launched pass by pass without programmatic dependent
+# launch
 LARGE_CLASSES = dict(match_warp_deg=256, match_cta_deg=1 << 24, contract_thread_row=32, contract_warp_row=256,
                      contract_cta_row=4096, gain_thread_deg=32, gain_hub_deg=1 << 24, warp_dense_k=1024,
                      grid_ctas_per_sm=32, dense_sparse_ratio=4096, small_level_n=0, chunk_deg=1 << 24,
-                     trial_cta_n=1 << 24, contract_smem_cn=0, small_match_n=0)
+                     trial_cta_n=1 << 24, contract_smem_cn=0, small_match_n=0, contract_hybrid=0,
+                     apply_chunk_deg=1 << 24, pdl=0, graph_passes=0)
 MIXED = dict(match_warp_deg=16, match_cta_deg=256, contract_thread_row=16, contract_warp_row=64,
              contract_cta_row=512, gain_thread_deg=16, gain_hub_deg=512, warp_dense_k=256, grid_ctas_per_sm=3,
              dense_sparse_ratio=2, small_level_n=4096, chunk_deg=96, trial_cta_n=200,
-             contract_smem_cn=3000, small_match_n=2000)
+             contract_smem_cn=3000, small_match_n=2000, apply_chunk_deg=64, pdl=0)
 
 
 def hub_graph(n=20000):
