@@ -36,6 +36,11 @@ namespace {
 
 constexpr int32_t ND_LEAF = 120;      // subgraphs of at most this many vertices are leaves
 constexpr float ND_UB = 1.05f;        // imbalance of the separator partitions
+// The separator partitions coarsen to graphs of about leaf size when the caller's
+// coarsen_to is 0, not to the 2-way rule's 16 vertices: the levels below that
+// cost every subgraph's partition its launches (the deep tiers are bound by the
+// launch rate of the worker threads) and buy nothing.
+constexpr int32_t ND_COARSEN_TO = 128;
 constexpr int ND_LEAF_THREADS = 128;  // one thread per leaf vertex
 constexpr int ND_W = 2;               // 64-bit words of a leaf adjacency row (128 >= ND_LEAF)
 static_assert(ND_LEAF <= 64 * ND_W && ND_LEAF <= ND_LEAF_THREADS, "leaf rows fit the bitsets and the CTA");
@@ -330,6 +335,7 @@ HP_API int hp_node_nd(hp_context *ctx, int32_t nvtxs, const int32_t *xadj, const
     else hp_options_default(&popt);
     popt.trace = 0;
     popt.profile = 0;
+    if (popt.coarsen_to <= 0) popt.coarsen_to = ND_COARSEN_TO;
 
     // two tier buffers, plus the per-vertex work arrays of the current tier
     const int64_t cap_x = 2 * n + 1;

@@ -289,7 +289,8 @@ int     hp_movelog_reset(hp_context *ctx);
  * most 120 vertices, or without edges, are ordered by an exact minimum-degree
  * elimination (the reference's MMD_Order, whose source is not in its tree).
  * Separators come from 2-way partitions by this library (imbalance 1.05, the
- * options in opt, NULL = defaults), so the ordering is deterministic.  Output:
+ * options in opt, NULL = defaults; coarsening to 128 vertices when
+ * opt->coarsen_to is 0), so the ordering is deterministic.  Output:
  * iperm[old] = new and, when perm is not NULL, perm[new] = old (METIS_NodeND's
  * convention; the reference's reflect array is iperm).  hp_last_stats reports
  * the recursion depths in nlevels and the 2-way partitions in refine_passes. */

@@ -1413,7 +1413,8 @@ float ora_mlp_loss_grad(const float *P, const float *X, const float *Y, int64_t 
  * that the reference leaves to randomised code are fixed:
  *   - the 2-way partition is this library's multilevel partition (k = 2,
  *     imbalance ND_UB, unit edge weights, the caller's vertex weights and
- *     options), where the reference runs its own randomised bisection with
+ *     options, coarsened to ND_COARSEN_TO vertices unless the caller sets
+ *     coarsen_to), where the reference runs its own randomised bisection with
  *     node refinement (reordergraph.h:17-135, refine.h:1398-1856);
  *   - separator: the boundary vertices of the side with fewer of them (side
  *     0 on a tie), then thinning: a separator vertex without a neighbour in
@@ -1430,6 +1431,10 @@ float ora_mlp_loss_grad(const float *P, const float *X, const float *Y, int64_t 
  */
 #define ND_LEAF 120
 #define ND_UB 1.05f
+/* the separator partitions coarsen to graphs of about leaf size (when the
+ * caller's coarsen_to is 0), not to the 2-way rule's 16 vertices: every level
+ * below that costs a subgraph's partition its launches and buys nothing */
+#define ND_COARSEN_TO 128
 
 typedef struct {
     int32_t n;
@@ -1583,6 +1588,7 @@ int ora_node_nd(int32_t n, const int32_t *xadj, const int32_t *adjncy, const int
     hp_options opt;
     if (opt_in) opt = *opt_in; else ora_options_default(&opt);
     opt.trace = 0;
+    if (opt.coarsen_to <= 0) opt.coarsen_to = ND_COARSEN_TO;
     nd_sub g;
     g.n = n;
     const int64_t m = xadj[n];
