@@ -2077,13 +2077,12 @@ __device__ int ctl_advance(RefineCtl *s, long long m, long long c1, long long c2
 // projection keeps the cut exactly: every coarse edge weight is the sum of
 // the fine edges between its two clusters, and edges inside a cluster are
 // never cut), else the cut summed from the gain rows (rowcut_kernel).
-__global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned,
-                                const int32_t *gain_total, const RefineCtl *coarser, int32_t judge)
+__device__ void ctl_init_state(RefineCtl *s, long long cut, long long excess, int32_t patience, int32_t learned,
+                               int32_t gain_total, int32_t judge)
 {
-    hp::pdl_wait();
-    s->gain_entries = *gain_total;
-    s->cut = coarser ? coarser->best_cut : (long long)sc[S_CUT2] / 2;
-    s->excess = (long long)sc[S_EXCESS];
+    s->gain_entries = gain_total;
+    s->cut = cut;
+    s->excess = excess;
     s->cut_start = s->cut;
     s->best_cut = s->cut;
     s->best_excess = s->excess;
@@ -2105,6 +2104,14 @@ __global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int3
     s->cont = s->count <= patience;   // while (count++ <= patience)
     s->count++;
     if (s->cont) ctl_prepare(s);
+}
+
+__global__ void ctl_init_kernel(RefineCtl *s, const unsigned long long *sc, int32_t patience, int32_t learned,
+                                const int32_t *gain_total, const RefineCtl *coarser, int32_t judge)
+{
+    hp::pdl_wait();
+    ctl_init_state(s, coarser ? coarser->best_cut : (long long)sc[S_CUT2] / 2, (long long)sc[S_EXCESS], patience,
+                   learned, *gain_total, judge);
 }
 
 // End of a pass: the exact cut change, the learned fallback, the stall rule, the
@@ -2483,10 +2490,12 @@ constexpr int SL_SORT_INTS = hp::block_sort_ints(SL_THREADS);
 
 struct SmallLevel {
     int32_t n, k, finest, bigd, small_max, key_bits, learned_mlp;
+    int32_t patience, judge;    // the control block's init (the level's setup runs in the kernel)
+    const RefineCtl *coarser;   // the coarser level's control block (its best cut), or nullptr
     float mlp_threshold;
     const int32_t *xadj, *adjncy, *adjwgt, *vwgt;
     int32_t *where;
-    const int32_t *goff;
+    int32_t *goff;
     int32_t *gpart, *gconn;
     int32_t *dest, *pregain, *moves, *oldp, *dirty, *small_l, *big_l, *best_where;
     int32_t *K, *V, *K2, *V2, *pre, *P, *sp;
@@ -2550,6 +2559,89 @@ refine_small_kernel(SmallLevel a)
     const int32_t n = a.n, k = a.k;
     RefineCtl *s = a.ctl;
     if (a.learned_mlp) hp::mlp_load_smem(s_mlp, a.mlp_params);
+    // ---- the level's setup, as the launches of the multi-kernel levels:
+    // gain-row capacities min(deg, k) and offsets, cleared locks and dirty
+    // flags, the rows' lists by length, part weights, the full gain-row build,
+    // the starting cut (the coarser level's best cut, else summed from the
+    // rows), the excess, the best-partition copy and the control block
+    {
+        int32_t run = 0, ns = 0, nb = 0;
+        for (int32_t b0 = 0; b0 < n; b0 += SL_THREADS) {
+            const int32_t v = b0 + tid;
+            int32_t cap = 0, d = 0;
+            if (v < n) {
+                d = a.xadj[v + 1] - a.xadj[v];
+                cap = d < k ? d : k;
+                a.lock[v] = 0;
+                a.dirty[v] = 0;
+                a.best_where[v] = a.where[v];
+            }
+            int tot;
+            const int ex = hp::block_excl_scan<SL_THREADS>(cap, &tot, s_scan);
+            if (v < n) a.goff[v] = run + ex;
+            run += tot;
+            const bool sh = v < n && d <= a.bigd, lg = v < n && d > a.bigd;
+            int ts, tl;
+            const int es = hp::block_excl_scan<SL_THREADS>(sh ? 1 : 0, &ts, s_scan);
+            const int el = hp::block_excl_scan<SL_THREADS>(lg ? 1 : 0, &tl, s_scan);
+            if (sh) a.small_l[ns + es] = v;
+            if (lg) a.big_l[nb + el] = v;
+            ns += ts;
+            nb += tl;
+        }
+        if (tid == 0) a.goff[n] = run;
+        unsigned long long *spw = (unsigned long long *)sl_dyn;   // k <= 1024 part weights
+        for (int32_t q = tid; q < k; q += SL_THREADS) spw[q] = 0ull;
+        __syncthreads();
+        for (int32_t v = tid; v < n; v += SL_THREADS) atomicAdd(&spw[a.where[v]], (unsigned long long)a.vwgt[v]);
+        __syncthreads();
+        for (int32_t q = tid; q < k; q += SL_THREADS) { a.pw[q] = spw[q]; a.best_pw[q] = spw[q]; }
+        __syncthreads();   // the accumulators below reuse the shared memory
+        if (ns > 0) {
+            if (a.small_max <= 8)
+                gain_seg_rows<8>(wid, SL_WARPS, a.small_l, ns, a.xadj, a.adjncy, a.adjwgt, a.where, a.goff, a.gpart,
+                                 a.gconn, k, a.dirty);
+            else if (a.small_max <= 16)
+                gain_seg_rows<16>(wid, SL_WARPS, a.small_l, ns, a.xadj, a.adjncy, a.adjwgt, a.where, a.goff, a.gpart,
+                                  a.gconn, k, a.dirty);
+            else
+                gain_seg_rows<32>(wid, SL_WARPS, a.small_l, ns, a.xadj, a.adjncy, a.adjwgt, a.where, a.goff, a.gpart,
+                                  a.gconn, k, a.dirty);
+        }
+        if (nb > 0) {
+            const int nw = (k + 31) >> 5;
+            int32_t *dw = sl_dyn + (size_t)wid * (k + nw);
+            unsigned *bm = (unsigned *)(dw + k);
+            for (int i = lane; i < k; i += 32) dw[i] = 0;
+            for (int i = lane; i < nw; i += 32) bm[i] = 0u;
+            __syncwarp();
+            gain_bigwarp_rows(wid, SL_WARPS, dw, bm, a.big_l, nb, a.xadj, a.adjncy, a.adjwgt, a.where, a.goff,
+                              a.gpart, a.gconn, k, a.dirty, a.bigd, INT_MAX);
+        }
+        __syncthreads();
+        long long cut = 0;
+        if (!a.coarser) {   // the coarsest level: the cut from the gain rows
+            long long acc = 0;
+            for (int32_t v = tid; v < n; v += SL_THREADS) {
+                const int32_t p = a.where[v], o = a.goff[v], len = a.goff[v + 1] - o;
+                for (int32_t j = o; j < o + len; j++) {
+                    const int32_t q = a.gpart[j];
+                    if (q < 0) break;
+                    if (q != p) acc += a.gconn[j];
+                }
+            }
+            cut = sl_sum64(acc, s_red) / 2;
+        }
+        long long m = LLONG_MIN;
+        for (int32_t q = tid; q < k; q += SL_THREADS) {
+            const long long e = (long long)a.pw[q] - a.maxp[q];
+            m = e > m ? e : m;
+        }
+        m = sl_max64(m, s_red);
+        if (tid == 0)
+            ctl_init_state(s, a.coarser ? a.coarser->best_cut : cut, m, a.patience, a.learned_mlp, a.goff[n],
+                           a.judge);
+    }
     __syncthreads();
     // the control step ends the loop; the pass cap bounds it as well
     for (int32_t guard = 0; guard <= HP_MAX_REFINE_PASSES; guard++) {
@@ -3111,41 +3203,6 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.plan_off = ralloc_t<int32_t>(c, nhub_cap);
     B.plan_cnt = ralloc_t<int32_t>(c, 2);
     HP_CHECK_OOM(c);
-    unsigned long long *sc = c->d_scal;
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_DONE + 1), c->stream));
-    int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
-    HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt,
-              c->tune.gain_thread_deg, chunkd);
-    if (ls.maxdeg > chunkd) {
-        HP_CUDA(cudaMemsetAsync(B.ab_acc, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
-        HP_CUDA(cudaMemsetAsync(B.ab_acc2, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
-    }
-    HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
-    // the gain rows take G = sum min(deg, k) <= m entries: allocated for m, so
-    // that no count is read back (the gain-build class completes its byte
-    // count with G from the control block at the end of uncoarsening)
-    B.small_max = ls.small_max;
-    B.huge_rows = ls.maxdeg > huged;
-    B.gpart = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
-    B.gconn = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
-    HP_CHECK_OOM(c);
-    const bool any_big = ls.nbig > 0;
-    int tok = hp_prof_begin(c);
-    HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt, any_big, nullptr));
-    // xadj, adjncy, adjwgt, where (own), goff in; gain rows (8 G) out
-    hp_prof_end(c, tok, HP_PROF_GAIN, 4 * ((int64_t)n + 1) + 8 * g.m + 4 * (int64_t)n + 4 * ((int64_t)n + 1));
-    ll->gain_tok = tok;
-    HP_CUDA(cudaMemsetAsync(B.pw, 0, sizeof(unsigned long long) * (size_t)k, c->stream));
-    HP_CUDA(cudaMemsetAsync(B.lock, 0, (size_t)n, c->stream));
-    HP_CUDA(cudaMemsetAsync(B.dirty, 0, sizeof(int32_t) * (size_t)n, c->stream));
-    HP_LAUNCH(c, pw_kernel, (unsigned)std::min<int64_t>(nblk(n), c->sm_count * 8), 256,
-              k <= 2048 ? sizeof(unsigned long long) * k : 0, n, g.where, g.vwgt, B.pw, k);
-    if (!coarser)   // the coarsest level; the others start from the coarser level's best cut
-        HP_LAUNCH(c, rowcut_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, &sc[S_CUT2]);
-    HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);
-    HP_CUDA(cudaMemcpyAsync(B.best_where, g.where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
-    HP_CUDA(cudaMemcpyAsync(best_pw, B.pw, sizeof(unsigned long long) * k, cudaMemcpyDeviceToDevice, c->stream));
-
     // learned LP proposals (opt.learned = 1, or 3 with the plain refiner as the
     // judge of every learned pass) until a learned pass fails to
     // improve the exact cut; then the plain rule for the rest of the level
@@ -3153,24 +3210,19 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     const bool judged = learned && c->opt.learned == 3;
     const bool recording = c->opt.learned == 2 && c->log_x != nullptr;
     const int patience = c->opt.refine_patience;
-    HP_LAUNCH(c, ctl_init_kernel, 1, 1, 0, ctl, (const unsigned long long *)sc, patience, learned ? 1 : 0,
-              (const int32_t *)(B.goff + n), coarser, judged ? 1 : 0);
-    int64_t log_r0 = 0;
-    if (recording) {
-        unsigned long long lc = 0;
-        HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
-        log_r0 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
-    }
-    PassCfg P{k, finest, any_big, recording, ls.maxdeg > chunkd, judged, ls.maxdeg > mchunkd, ctl, best_pw};
     const bool dbg = getenv("HP_DEBUG_PASSES") != nullptr;
-    const bool use_graph = graph_loop(c);
-    RefineCtl h{};
     // small levels: the whole pass loop in one CTA (same rule, same result), in
     // either loop mode unless the per-pass move log or pass log is on
     const int32_t small_n = c->tune.small_level_n;
     const bool small_level = !recording && !dbg && n <= small_n && k <= HP_TUNE_WARP_DENSE_K_MAX &&
                              g.m <= 16 * (int64_t)small_n;
     if (small_level) {
+        // the level's setup (gain rows, part weights, cut, control block) runs
+        // inside the kernel: no launch per setup step
+        B.gpart = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
+        B.gconn = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
+        B.small_max = ls.small_max;
+        HP_CHECK_OOM(c);
         SmallLevel a{};
         a.n = n;
         a.k = k;
@@ -3179,6 +3231,9 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         a.small_max = B.small_max;
         a.key_bits = key_bits_for(k);
         a.learned_mlp = learned ? 1 : 0;
+        a.patience = patience;
+        a.judge = judged ? 1 : 0;
+        a.coarser = coarser;
         a.mlp_threshold = c->mlp_threshold;
         a.xadj = g.xadj;
         a.adjncy = g.adjncy;
@@ -3220,7 +3275,56 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
         a.mlp_params = c->mlp_params;
         a.ctl = ctl;
         HP_LAUNCH(c, refine_small_kernel, 1, SL_THREADS, small_level_smem(n, k), a);
-    } else if (use_graph) {
+        c->hi = mark;
+        return HP_OK;
+    }
+    unsigned long long *sc = c->d_scal;
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_DONE + 1), c->stream));
+    int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
+    HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt,
+              c->tune.gain_thread_deg, chunkd);
+    if (ls.maxdeg > chunkd) {
+        HP_CUDA(cudaMemsetAsync(B.ab_acc, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
+        HP_CUDA(cudaMemsetAsync(B.ab_acc2, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
+    }
+    HP_TRY(hp_scan_excl(c, B.goff, B.goff, n));
+    // the gain rows take G = sum min(deg, k) <= m entries: allocated for m, so
+    // that no count is read back (the gain-build class completes its byte
+    // count with G from the control block at the end of uncoarsening)
+    B.small_max = ls.small_max;
+    B.huge_rows = ls.maxdeg > huged;
+    B.gpart = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
+    B.gconn = ralloc_t<int32_t>(c, std::max<int64_t>(g.m, 1));
+    HP_CHECK_OOM(c);
+    const bool any_big = ls.nbig > 0;
+    int tok = hp_prof_begin(c);
+    HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt, any_big, nullptr));
+    // xadj, adjncy, adjwgt, where (own), goff in; gain rows (8 G) out
+    hp_prof_end(c, tok, HP_PROF_GAIN, 4 * ((int64_t)n + 1) + 8 * g.m + 4 * (int64_t)n + 4 * ((int64_t)n + 1));
+    ll->gain_tok = tok;
+    HP_CUDA(cudaMemsetAsync(B.pw, 0, sizeof(unsigned long long) * (size_t)k, c->stream));
+    HP_CUDA(cudaMemsetAsync(B.lock, 0, (size_t)n, c->stream));
+    HP_CUDA(cudaMemsetAsync(B.dirty, 0, sizeof(int32_t) * (size_t)n, c->stream));
+    HP_LAUNCH(c, pw_kernel, (unsigned)std::min<int64_t>(nblk(n), c->sm_count * 8), 256,
+              k <= 2048 ? sizeof(unsigned long long) * k : 0, n, g.where, g.vwgt, B.pw, k);
+    if (!coarser)   // the coarsest level; the others start from the coarser level's best cut
+        HP_LAUNCH(c, rowcut_kernel, nblk(n), 256, 0, n, B.goff, B.gpart, B.gconn, g.where, &sc[S_CUT2]);
+    HP_LAUNCH(c, excess_kernel, 1, 1024, 0, k, B.pw, B.maxp, (long long *)&sc[S_EXCESS]);
+    HP_CUDA(cudaMemcpyAsync(B.best_where, g.where, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, c->stream));
+    HP_CUDA(cudaMemcpyAsync(best_pw, B.pw, sizeof(unsigned long long) * k, cudaMemcpyDeviceToDevice, c->stream));
+
+    HP_LAUNCH(c, ctl_init_kernel, 1, 1, 0, ctl, (const unsigned long long *)sc, patience, learned ? 1 : 0,
+              (const int32_t *)(B.goff + n), coarser, judged ? 1 : 0);
+    int64_t log_r0 = 0;
+    if (recording) {
+        unsigned long long lc = 0;
+        HP_TRY(hp_read_scalars(c, c->log_count, sizeof(lc), &lc));
+        log_r0 = (int64_t)std::min<unsigned long long>(lc, (unsigned long long)c->log_cap);
+    }
+    PassCfg P{k, finest, any_big, recording, ls.maxdeg > chunkd, judged, ls.maxdeg > mchunkd, ctl, best_pw};
+    const bool use_graph = graph_loop(c);
+    RefineCtl h{};
+    if (use_graph) {
         ll->graph = true;
         HP_TRY(run_passes_graph(c, g, B, P, learned, &ll->n_common, ll->n_mode, keep));
         HP_LAUNCH(c, restore_best_kernel, std::min<unsigned>(nblk(n), (unsigned)(c->sm_count * 4)), 256, 0, ctl, n,
