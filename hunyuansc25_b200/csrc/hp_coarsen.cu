@@ -565,7 +565,8 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
                     int4 *__restrict__ rinfo, int32_t *__restrict__ cvwgt, int32_t *__restrict__ ltlen,
                     int32_t *__restrict__ lists, int32_t *__restrict__ counts, int32_t cn,
                     int32_t *__restrict__ maxlen, unsigned long long *__restrict__ long_total,
-                    int32_t *__restrict__ small_max, int32_t thread_row, int32_t warp_row, int32_t cta_row)
+                    int32_t *__restrict__ small_max, int32_t thread_row, int32_t warp_row, int32_t cta_row,
+                    int32_t mid_row, int32_t *__restrict__ sub_counts)
 {
     hp::pdl_wait();
     // no early exit: the list appends and maxima are aggregated per warp
@@ -599,6 +600,14 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
     for (int q = 0; q < 3; q++) {
         const int32_t pos = hp::warp_append(&counts[q], cls == q);
         if (cls == q) lists[(int64_t)q * cn + pos] = c;
+    }
+    // list 1 once more, split at mid_row (lists 3 and 4): each CTA radix
+    // instance walks only the rows it sorts
+    const int sub = cls != 1 ? -1 : (len <= mid_row ? 0 : 1);
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int32_t pos = hp::warp_append(&sub_counts[q], sub == q);
+        if (sub == q) lists[(int64_t)(3 + q) * cn + pos] = c;
     }
     // the longest short row above 8 entries picks the assembly kernel's network
     const int32_t sm = hp::warp_max(lead && !is_long && len > 8 ? len : 0);
@@ -858,13 +867,35 @@ copy_long_rows_kernel(const int32_t *__restrict__ lists, const int32_t *__restri
     const int64_t total = CTA ? (int64_t)counts[1] + counts[2] : (int64_t)counts[0];
     const int64_t first = CTA ? blockIdx.x : (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t step = CTA ? gridDim.x : ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int32_t n1 = counts[1];
+    auto row_at = [&](int64_t i) -> int32_t {
+        return lists[CTA ? (i < n1 ? (int64_t)cn + i : 2 * (int64_t)cn + (i - n1)) : i];
+    };
+    // the next row's id is loaded while the current row is copied, and each
+    // thread keeps four entries' loads in flight
+    int32_t c_next = first < total ? row_at(first) : 0;
     for (int64_t i = first; i < total; i += step) {
-        const int64_t slot = CTA ? (i < counts[1] ? (int64_t)cn + i : 2 * (int64_t)cn + (i - counts[1])) : i;
-        const int32_t c = lists[slot];
+        const int32_t c = c_next;
+        if (i + step < total) c_next = row_at(i + step);
         const int32_t src = toff[c], dst = cxadj[c], cnt = ucnt[c];
-        for (int32_t j = lane; j < cnt; j += width) {
-            cadjncy[dst + j] = tk[src + j];
-            cadjwgt[dst + j] = tw[src + j];
+        for (int32_t j0 = lane; j0 < cnt; j0 += 4 * width) {
+            int32_t a[4], b[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int32_t j = j0 + q * width;
+                if (j < cnt) {
+                    a[q] = tk[src + j];
+                    b[q] = tw[src + j];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int32_t j = j0 + q * width;
+                if (j < cnt) {
+                    cadjncy[dst + j] = a[q];
+                    cadjwgt[dst + j] = b[q];
+                }
+            }
         }
     }
 }
@@ -1798,23 +1829,32 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     int4 *rinfo = ralloc_t<int4>(c, cn);
     int32_t *toff = ralloc_t<int32_t>(c, (int64_t)cn + 1);
     int32_t *ucnt = ralloc_t<int32_t>(c, (int64_t)cn + 1);
-    int32_t *lists = ralloc_t<int32_t>(c, 3 * (int64_t)cn);
+    int32_t *lists = ralloc_t<int32_t>(c, 5 * (int64_t)cn);
     const int64_t ntiles = ((int64_t)cn + ASM_TILE - 1) / ASM_TILE;
     if (ntiles > c->lb_cap) return HP_ERR_INTERNAL;   // reserved at the start of every call
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 5, c->stream));
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 6, c->stream));
     int32_t *counts = (int32_t *)sc;          // 3 long-row class counts + max length in slots 0-1
     int32_t *maxlen = counts + 3;
     unsigned long long *long_total = &sc[2];  // entries of the long rows
     int32_t *small_max = (int32_t *)&sc[3];   // longest short row above 8 entries (0: none)
+    int32_t *sub_counts = (int32_t *)&sc[5];  // list 1 split at MROW_MAX entries (lists 3 and 4)
 
     int tok = hp_prof_begin(c);
     HP_LAUNCH(c, coarse_setup_kernel, blocks_for(n), 256, 0, n, g.match, g.cmap, g.xadj, g.vwgt, rinfo, cg.vwgt,
               toff, lists, counts, cn, maxlen, long_total, small_max, c->tune.contract_thread_row,
-              c->tune.contract_warp_row, c->tune.contract_cta_row);
+              c->tune.contract_warp_row, c->tune.contract_cta_row, MROW_MAX, sub_counts);
     hp_prof_end(c, tok, HP_PROF_CONTRACT, 0);
-    struct { int32_t cnt[3]; int32_t maxlen; unsigned long long total; int32_t small_max, pad; } h;
+    struct {
+        int32_t cnt[3];
+        int32_t maxlen;
+        unsigned long long total;
+        int32_t small_max, pad;
+        unsigned long long spill;
+        int32_t sub[2];
+    } h;
+    static_assert(sizeof(h) == 6 * sizeof(unsigned long long), "the six scalar slots");
     HP_TRY(hp_read_scalars(c, sc, sizeof(h), &h));
     const bool any_long = h.cnt[0] + h.cnt[1] + h.cnt[2] > 0;
     ContractSrc src{rinfo, g.adjncy, g.adjwgt, g.cmap};
@@ -1868,17 +1908,16 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
                       (cta_radix_smem<XROW_THREADS, XROW_MAX>()), spill, d_nspill, src, toff, tk, tw, ucnt, kbits, 0,
                       wchk, c->d_status);
         }
-        if (!smem_dense && !hybrid && h.cnt[1] > 0) {
+        if (!smem_dense && !hybrid && h.sub[0] > 0)
             HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>),
-                      (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 8), CROW_THREADS,
-                      (cta_radix_smem<CROW_THREADS, MROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt, kbits,
-                      0, wchk, c->d_status);
-            if (c->tune.contract_cta_row > MROW_MAX)
-                HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
-                          (unsigned)std::min<int64_t>(h.cnt[1], c->sm_count * 3), CROW_THREADS,
-                          (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + cn, &counts[1], src, toff, tk, tw, ucnt,
-                          kbits, MROW_MAX, wchk, c->d_status);
-        }
+                      (unsigned)std::min<int64_t>(h.sub[0], c->sm_count * 8), CROW_THREADS,
+                      (cta_radix_smem<CROW_THREADS, MROW_MAX>()), lists + 3 * (int64_t)cn, &sub_counts[0], src, toff,
+                      tk, tw, ucnt, kbits, 0, wchk, c->d_status);
+        if (!smem_dense && !hybrid && h.sub[1] > 0)
+            HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
+                      (unsigned)std::min<int64_t>(h.sub[1], c->sm_count * 3), CROW_THREADS,
+                      (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + 4 * (int64_t)cn, &sub_counts[1], src, toff,
+                      tk, tw, ucnt, kbits, MROW_MAX, wchk, c->d_status);
         if (!smem_dense && !hybrid && h.cnt[2] > 0)
             HP_LAUNCH(c, (contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>),
                       (unsigned)std::min<int64_t>(h.cnt[2], c->sm_count), XROW_THREADS,

@@ -42,11 +42,12 @@ __global__ void project_kernel(int32_t n, const int32_t *__restrict__ cmap,
 
 // Row capacities min(deg, k); rows longer than bigd go on the big list, rows
 // longer than huged (the caller's chunk_deg) also on the long-row list (count
-// d_bigcnt[3]); d_bigcnt[1] records the longest short row above 8 entries,
+// d_bigcnt[3]), rows longer than hubd (gain_hub_deg) on the hub list (count
+// d_bigcnt[4]); d_bigcnt[1] records the longest short row above 8 entries,
 // d_bigcnt[2] the longest row above huged.
 __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int32_t k,
-                                int32_t *__restrict__ cap, int32_t *big, int32_t *huge, int32_t *d_bigcnt,
-                                int32_t bigd, int32_t huged)
+                                int32_t *__restrict__ cap, int32_t *big, int32_t *huge, int32_t *hub,
+                                int32_t *d_bigcnt, int32_t bigd, int32_t huged, int32_t hubd)
 {
     hp::pdl_wait();
     // no early exit: the list appends and maxima are aggregated per warp
@@ -56,11 +57,13 @@ __global__ void gain_cap_kernel(int32_t n, const int32_t *__restrict__ xadj, int
         d = xadj[v + 1] - xadj[v];
         cap[v] = d < k ? d : k;
     }
-    const bool is_big = v < n && d > bigd, is_huge = is_big && d > huged;
+    const bool is_big = v < n && d > bigd, is_huge = is_big && d > huged, is_hub = is_big && d > hubd;
     const int32_t pb = hp::warp_append(d_bigcnt, is_big);
     const int32_t ph = hp::warp_append(d_bigcnt + 3, is_huge);
+    const int32_t pu = hp::warp_append(d_bigcnt + 4, is_hub);
     if (is_big) big[pb] = v;
     if (is_huge) huge[ph] = v;
+    if (is_hub) hub[pu] = v;
     const int32_t hm = hp::warp_max(is_huge ? d : 0);
     const int32_t sm = hp::warp_max(v < n && !is_big && d > 8 ? d : 0);
     if ((threadIdx.x & 31) == 0) {
@@ -1879,6 +1882,7 @@ __global__ void rs_assign_kernel(int32_t k, const int32_t *__restrict__ P, const
 struct RefineBufs {
     int32_t *goff, *gpart, *gconn, *big, *dest, *pregain, *moves, *oldp, *dirty;
     int32_t *small_l, *big_l, *best_where, *huge_mv, *huge;
+    int32_t *hub;     // rows longer than gain_hub_deg (the dense gain build's rows when k <= warp_dense_k)
     int32_t *recof;   // move log: a vertex's record (record mode)
     int32_t *plan_v, *plan_item, *plan_off, *plan_cnt;   // chunk plan of the current step
     int64_t nhub_cap;   // capacity of the long-row list and the plan (rows longer than chunk_deg)
@@ -1901,15 +1905,19 @@ struct RefineBufs {
 // the judge of a learned pass -- plain candidates, listed vertices, twice the
 // plain and the learned exact cut decrease); S_BIGCNT (the
 // level's list of rows longer than 32) lives above it and persists.
-// S_BIGCNT (slots 16-17) holds the big-row count, the longest short row and the
-// longest row above huged.
+// S_BIGCNT (slots 16-18) holds the big-row count, the longest short row, the
+// longest row above huged, the long-row count and the hub-row count.
 enum { S_NMOVES = 0, S_C1 = 1, S_C2 = 2, S_EXCESS = 3, S_NCAND = 4, S_CUT2 = 5, S_DIRTY = 6,
        S_HUGEMV = 7, S_LISTCNT = 8, S_NU = 9, S_NP = 10, S_NCANDP = 11, S_JN = 12, S_JP = 13, S_JL = 14,
        S_PASS_END = 16, S_BIGCNT = 16, S_DONE = 20 };
 
+// hub_list (nullable): the rows longer than gain_hub_deg among big_list, which
+// the dense build walks instead of big_list when k <= warp_dense_k (its other
+// rows are gain_bigwarp_kernel's)
 int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_t *small_list,
                const int32_t *d_small_cnt, const int32_t *big_list, const int32_t *d_big_cnt,
-               bool any_big, int32_t *dirty)
+               bool any_big, int32_t *dirty, const int32_t *hub_list = nullptr,
+               const int32_t *d_hub_cnt = nullptr)
 {
     const hp_tuning &tn = c->tune;
     if (small_list) {
@@ -1947,10 +1955,11 @@ int build_rows(hp_context *c, HpLevel &g, RefineBufs &B, int32_t k, const int32_
         // hub rows: every such row in a full build; in a rebuild only sparse
         // ones (deg < k), which exist only when k > gain_hub_deg
         const bool dense_rows = dirty ? (B.huge_rows && k > tn.gain_hub_deg) : B.huge_rows;
+        const bool hubs = hub_list && k <= tn.warp_dense_k;
         if (k > tn.warp_dense_k || dense_rows)
-            HP_LAUNCH(c, gain_dense_kernel<256>, (unsigned)(c->sm_count * 2), 256, smem, big_list, d_big_cnt,
-                      g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k, dirty, tn.gain_thread_deg,
-                      tn.gain_hub_deg, tn.warp_dense_k);
+            HP_LAUNCH(c, gain_dense_kernel<256>, (unsigned)(c->sm_count * 2), 256, smem, hubs ? hub_list : big_list,
+                      hubs ? d_hub_cnt : d_big_cnt, g.xadj, g.adjncy, g.adjwgt, g.where, B.goff, B.gpart, B.gconn, k,
+                      dirty, tn.gain_thread_deg, tn.gain_hub_deg, tn.warp_dense_k);
     }
     return HP_OK;
 }
@@ -3198,6 +3207,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     B.nhub_cap = nhub_cap;
     B.ab_acc = ralloc_t<unsigned long long>(c, nhub_cap);
     B.ab_acc2 = ralloc_t<unsigned long long>(c, nhub_cap);
+    // at most m / (huged + 1) rows are longer than huged
+    B.hub = ralloc_t<int32_t>(c, std::min<int64_t>((int64_t)n, g.m / ((int64_t)huged + 1)) + 1);
     B.plan_v = ralloc_t<int32_t>(c, nhub_cap);
     B.plan_item = ralloc_t<int32_t>(c, nhub_cap);
     B.plan_off = ralloc_t<int32_t>(c, nhub_cap);
@@ -3281,8 +3292,8 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     unsigned long long *sc = c->d_scal;
     HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * (S_DONE + 1), c->stream));
     int32_t *d_bigcnt = (int32_t *)&sc[S_BIGCNT];
-    HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, d_bigcnt,
-              c->tune.gain_thread_deg, chunkd);
+    HP_LAUNCH(c, gain_cap_kernel, nblk(n), 256, 0, n, g.xadj, k, B.goff, B.big, B.huge, B.hub, d_bigcnt,
+              c->tune.gain_thread_deg, chunkd, huged);
     if (ls.maxdeg > chunkd) {
         HP_CUDA(cudaMemsetAsync(B.ab_acc, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
         HP_CUDA(cudaMemsetAsync(B.ab_acc2, 0, sizeof(unsigned long long) * (size_t)nhub_cap, c->stream));
@@ -3298,7 +3309,7 @@ int refine_level(hp_context *c, HpLevel &g, int32_t k, bool finest, const int64_
     HP_CHECK_OOM(c);
     const bool any_big = ls.nbig > 0;
     int tok = hp_prof_begin(c);
-    HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt, any_big, nullptr));
+    HP_TRY(build_rows(c, g, B, k, nullptr, nullptr, B.big, d_bigcnt, any_big, nullptr, B.hub, d_bigcnt + 4));
     // xadj, adjncy, adjwgt, where (own), goff in; gain rows (8 G) out
     hp_prof_end(c, tok, HP_PROF_GAIN, 4 * ((int64_t)n + 1) + 8 * g.m + 4 * (int64_t)n + 4 * ((int64_t)n + 1));
     ll->gain_tok = tok;
