@@ -659,6 +659,12 @@ row_weight_range_kernel(int32_t n, const int32_t *__restrict__ xadj, const int32
 // The fine rows merged into coarse row c: entry i is the i-th entry of the
 // leader's row, then of the mate's row, mapped through cmap (the coarse self key
 // is dropped).
+// Entries per thread whose row loads, then coarse-id gathers, are in flight
+// together in the long-row kernels.  The gathers are all issued before any of
+// their results is stored, so they overlap even where the compiler cannot prove
+// that the stores (or atomics) leave cmap alone.
+constexpr int GATHER_DEPTH = 8;
+
 struct ContractSrc {
     const int4 *rinfo;
     const int32_t *adjncy, *adjwgt, *cmap;
@@ -790,10 +796,13 @@ contract_assemble_kernel(int32_t cn, ContractSrc src, const int32_t *__restrict_
                 w[q] = src.adjwgt[j];
             }
         }
+        int32_t kq[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) kq[q] = rt[q] >= 0 ? src.cmap[a[q]] : 0;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             if (rt[q] < 0) continue;
-            const int32_t k = src.cmap[a[q]];
+            const int32_t k = kq[q];
             asm_stage[f0 + q * ASM_TILE] =
                 k == c0 + rt[q] ? hp::PACK_NONE : (((unsigned long long)(uint32_t)k << 32) | (uint32_t)w[q]);
         }
@@ -1091,21 +1100,26 @@ __device__ int group_gather_row(const ContractSrc &src, int32_t c, const RowInfo
     const int t = threadIdx.x % G;
     int self = 0;
     long long ws = 0;   // this thread's share of the row's kept weights
-    // four entries per thread at a time: the row loads, then the coarse-id
-    // gathers, are issued together
-    for (int i0 = t; i0 < len; i0 += 4 * G) {
-        int32_t j[4], a[4], w[4];
+    // D entries per thread at a time: the row loads, then the coarse-id
+    // gathers, are issued together (a warp's rows of at most 256 entries take
+    // two batches of four)
+    constexpr int D = G == 32 ? 4 : GATHER_DEPTH;
+    for (int i0 = t; i0 < len; i0 += D * G) {
+        int32_t j[D], a[D], w[D];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < D; q++) {
             const int i = i0 + q * G;
             j[q] = i < len ? (i < r.l0 ? r.s0 + i : r.s1 + (i - r.l0)) : -1;
             a[q] = j[q] >= 0 ? src.adjncy[j[q]] : 0;
             w[q] = j[q] >= 0 ? src.adjwgt[j[q]] : 0;
         }
+        int32_t kq[D];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < D; q++) kq[q] = j[q] >= 0 ? src.cmap[a[q]] : 0;
+#pragma unroll
+        for (int q = 0; q < D; q++) {
             if (j[q] < 0) continue;
-            int32_t k = src.cmap[a[q]];
+            int32_t k = kq[q];
             int32_t ww = w[q];
             if (k == c) { k = hp::KEY_NONE; ww = 0; }
             self += k == hp::KEY_NONE;
@@ -1279,22 +1293,25 @@ contract_hybrid_kernel(const int32_t *__restrict__ list, const int32_t *__restri
         src.row(c, r, len);
         if (len <= min_len) continue;   // (uniform over the CTA)
         long long ws = 0;
-        // four entries per thread in flight: the row loads, then the cmap gathers
-        for (int32_t i0 = tid; i0 < len; i0 += 4 * HY_THREADS) {
-            int32_t a[4], w[4];
-            bool in[4];
+        // GATHER_DEPTH entries per thread in flight: the row loads, then the cmap gathers
+        for (int32_t i0 = tid; i0 < len; i0 += GATHER_DEPTH * HY_THREADS) {
+            int32_t a[GATHER_DEPTH], w[GATHER_DEPTH];
+            bool in[GATHER_DEPTH];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < GATHER_DEPTH; q++) {
                 const int32_t i = i0 + q * HY_THREADS;
                 in[q] = i < len;
                 const int32_t j = in[q] ? (i < r.l0 ? r.s0 + i : r.s1 + (i - r.l0)) : 0;
                 a[q] = in[q] ? src.adjncy[j] : 0;
                 w[q] = in[q] ? src.adjwgt[j] : 0;
             }
+            int32_t kq[GATHER_DEPTH];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < GATHER_DEPTH; q++) kq[q] = in[q] ? src.cmap[a[q]] : 0;
+#pragma unroll
+            for (int q = 0; q < GATHER_DEPTH; q++) {
                 if (!in[q]) continue;
-                const int32_t k = src.cmap[a[q]];
+                const int32_t k = kq[q];
                 if (k == c) continue;   // the coarse self key
                 ws += w[q];
                 if (k < HY_HOT) {
@@ -1405,11 +1422,11 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
         if (len <= min_len) continue;   // another kernel's row
         const bool two_level = (int64_t)len * ratio < ((int64_t)cn + 31) / 32;
         long long ws = 0;   // this thread's share of the row's kept weights (weight range)
-        for (int32_t i0 = threadIdx.x; i0 < len; i0 += 4 * NT) {
-            int32_t a[4], wq[4];
-            bool in[4];
+        for (int32_t i0 = threadIdx.x; i0 < len; i0 += GATHER_DEPTH * NT) {
+            int32_t a[GATHER_DEPTH], wq[GATHER_DEPTH], kq[GATHER_DEPTH];
+            bool in[GATHER_DEPTH];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < GATHER_DEPTH; q++) {
                 const int32_t i = i0 + q * NT;
                 in[q] = i < len;
                 const int32_t j = in[q] ? (i < r.l0 ? r.s0 + i : r.s1 + (i - r.l0)) : 0;
@@ -1417,9 +1434,11 @@ contract_dense_kernel(const int32_t *__restrict__ list, const int32_t *__restric
                 wq[q] = in[q] ? src.adjwgt[j] : 0;
             }
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < GATHER_DEPTH; q++) kq[q] = in[q] ? src.cmap[a[q]] : 0;
+#pragma unroll
+            for (int q = 0; q < GATHER_DEPTH; q++) {
                 if (!in[q]) continue;
-                const int32_t k = src.cmap[a[q]];
+                const int32_t k = kq[q];
                 if (k == c) continue;   // the coarse self key
                 ws += wq[q];
                 if (two_level) {
