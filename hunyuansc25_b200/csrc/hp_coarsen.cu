@@ -1187,12 +1187,15 @@ contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__re
 }
 
 // CTA class: one CTA of NT threads per row of min_len+1 .. CAP entries.  Three
-// instances: <256, 1024> and <256, 4096> split list 1 (rows up to 1024 entries
-// take 24 KB of shared memory, so 8 CTAs share an SM instead of 3), and
-// <1024, 12288> takes the rows of list 2 up to 12288 entries, whose longer
-// rows stay with the dense kernel; 2 CAP packed entries plus NT/32 digit
-// histograms fit the 227 KB of shared memory of one CTA.
+// instances: <64, 1024> and <256, 4096> split list 1, and <1024, 12288> takes
+// the rows of list 2 up to 12288 entries, whose longer rows stay with the
+// dense kernel; 2 CAP packed entries plus NT/32 digit histograms fit the 227 KB
+// of shared memory of one CTA.  Rows of up to 1024 entries take two warps and
+// 18 KB, so eleven rows are in flight per SM: on rows of 257-1024 entries that
+// sorts 1.5x faster than a CTA of 256 threads (fewer threads per barrier, more
+// rows in flight), while rows of 1025-4096 entries sort fastest with 256.
 constexpr int CROW_THREADS = 256;
+constexpr int MROW_THREADS = 64;
 constexpr int XROW_THREADS = 1024, XROW_MAX = 12288;
 constexpr int MROW_MAX = 1024;   // the smaller CTA instance of list 1
 
@@ -1928,9 +1931,9 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
                       wchk, c->d_status);
         }
         if (!smem_dense && !hybrid && h.sub[0] > 0)
-            HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>),
-                      (unsigned)std::min<int64_t>(h.sub[0], c->sm_count * 8), CROW_THREADS,
-                      (cta_radix_smem<CROW_THREADS, MROW_MAX>()), lists + 3 * (int64_t)cn, &sub_counts[0], src, toff,
+            HP_LAUNCH(c, (contract_cta_radix_kernel<MROW_THREADS, MROW_MAX>),
+                      (unsigned)std::min<int64_t>(h.sub[0], c->sm_count * 12), MROW_THREADS,
+                      (cta_radix_smem<MROW_THREADS, MROW_MAX>()), lists + 3 * (int64_t)cn, &sub_counts[0], src, toff,
                       tk, tw, ucnt, kbits, 0, wchk, c->d_status);
         if (!smem_dense && !hybrid && h.sub[1] > 0)
             HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
@@ -2004,9 +2007,9 @@ int hp_coarsen_init()
                                                           (HP_TUNE_SMEM_CN_MAX + 1023) / 1024))));
     HP_CUDA(cudaFuncSetAttribute(contract_hybrid_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)hybrid_smem()));
-    HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<CROW_THREADS, MROW_MAX>,
+    HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<MROW_THREADS, MROW_MAX>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)cta_radix_smem<CROW_THREADS, MROW_MAX>()));
+                                 (int)cta_radix_smem<MROW_THREADS, MROW_MAX>()));
     HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_radix_smem<CROW_THREADS, CROW_MAX>()));
