@@ -566,7 +566,7 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
                     int32_t *__restrict__ lists, int32_t *__restrict__ counts, int32_t cn,
                     int32_t *__restrict__ maxlen, unsigned long long *__restrict__ long_total,
                     int32_t *__restrict__ small_max, int32_t thread_row, int32_t warp_row, int32_t cta_row,
-                    int32_t mid_row, int32_t *__restrict__ sub_counts)
+                    int32_t mid_row, int32_t mid2_row, int32_t *__restrict__ sub_counts)
 {
     hp::pdl_wait();
     // no early exit: the list appends and maxima are aggregated per warp
@@ -601,11 +601,11 @@ coarse_setup_kernel(int32_t n, const int32_t *__restrict__ match, int32_t *__res
         const int32_t pos = hp::warp_append(&counts[q], cls == q);
         if (cls == q) lists[(int64_t)q * cn + pos] = c;
     }
-    // list 1 once more, split at mid_row (lists 3 and 4): each CTA radix
-    // instance walks only the rows it sorts
-    const int sub = cls != 1 ? -1 : (len <= mid_row ? 0 : 1);
+    // list 1 once more, split at mid_row and mid2_row (lists 3, 4 and 5): each
+    // CTA radix instance walks only the rows it sorts
+    const int sub = cls != 1 ? -1 : (len <= mid_row ? 0 : (len <= mid2_row ? 1 : 2));
 #pragma unroll
-    for (int q = 0; q < 2; q++) {
+    for (int q = 0; q < 3; q++) {
         const int32_t pos = hp::warp_append(&sub_counts[q], sub == q);
         if (sub == q) lists[(int64_t)(3 + q) * cn + pos] = c;
     }
@@ -1186,16 +1186,19 @@ contract_warp_radix_kernel(const int32_t *__restrict__ list, const int32_t *__re
     }
 }
 
-// CTA class: one CTA of NT threads per row of min_len+1 .. CAP entries.  Three
-// instances: <64, 1024> and <256, 4096> split list 1, and <1024, 12288> takes
-// the rows of list 2 up to 12288 entries, whose longer rows stay with the
-// dense kernel; 2 CAP packed entries plus NT/32 digit histograms fit the 227 KB
-// of shared memory of one CTA.  Rows of up to 1024 entries take two warps and
-// 18 KB, so eleven rows are in flight per SM: on rows of 257-1024 entries that
-// sorts 1.5x faster than a CTA of 256 threads (fewer threads per barrier, more
-// rows in flight), while rows of 1025-4096 entries sort fastest with 256.
+// CTA class: one CTA of NT threads per row of min_len+1 .. CAP entries.  Four
+// instances: <64, 1024>, <128, 2048> and <256, 4096> split list 1, and
+// <1024, 12288> takes the rows of list 2 up to 12288 entries, whose longer rows
+// stay with the dense kernel; 2 CAP packed entries plus NT/32 digit histograms
+// fit the 227 KB of shared memory of one CTA.  Rows of up to 1024 entries take
+// two warps and 18 KB, so eleven rows are in flight per SM: on rows of 257-1024
+// entries that sorts 1.5x faster than a CTA of 256 threads (fewer threads per
+// barrier, more rows in flight); rows of 1025-2048 entries sort 1.24x faster
+// with four warps and 36 KB (six rows per SM), rows of 2049-4096 fastest with
+// 256 threads.
 constexpr int CROW_THREADS = 256;
 constexpr int MROW_THREADS = 64;
+constexpr int NROW_THREADS = 128, NROW_MAX = 2048;   // the middle CTA instance of list 1
 constexpr int XROW_THREADS = 1024, XROW_MAX = 12288;
 constexpr int MROW_MAX = 1024;   // the smaller CTA instance of list 1
 
@@ -1851,22 +1854,22 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
     int4 *rinfo = ralloc_t<int4>(c, cn);
     int32_t *toff = ralloc_t<int32_t>(c, (int64_t)cn + 1);
     int32_t *ucnt = ralloc_t<int32_t>(c, (int64_t)cn + 1);
-    int32_t *lists = ralloc_t<int32_t>(c, 5 * (int64_t)cn);
+    int32_t *lists = ralloc_t<int32_t>(c, 6 * (int64_t)cn);
     const int64_t ntiles = ((int64_t)cn + ASM_TILE - 1) / ASM_TILE;
     if (ntiles > c->lb_cap) return HP_ERR_INTERNAL;   // reserved at the start of every call
     HP_CHECK_OOM(c);
     unsigned long long *sc = c->d_scal;
-    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 6, c->stream));
+    HP_CUDA(cudaMemsetAsync(sc, 0, sizeof(unsigned long long) * 7, c->stream));
     int32_t *counts = (int32_t *)sc;          // 3 long-row class counts + max length in slots 0-1
     int32_t *maxlen = counts + 3;
     unsigned long long *long_total = &sc[2];  // entries of the long rows
     int32_t *small_max = (int32_t *)&sc[3];   // longest short row above 8 entries (0: none)
-    int32_t *sub_counts = (int32_t *)&sc[5];  // list 1 split at MROW_MAX entries (lists 3 and 4)
+    int32_t *sub_counts = (int32_t *)&sc[5];  // list 1 split at MROW_MAX and NROW_MAX entries (lists 3-5)
 
     int tok = hp_prof_begin(c);
     HP_LAUNCH(c, coarse_setup_kernel, blocks_for(n), 256, 0, n, g.match, g.cmap, g.xadj, g.vwgt, rinfo, cg.vwgt,
               toff, lists, counts, cn, maxlen, long_total, small_max, c->tune.contract_thread_row,
-              c->tune.contract_warp_row, c->tune.contract_cta_row, MROW_MAX, sub_counts);
+              c->tune.contract_warp_row, c->tune.contract_cta_row, MROW_MAX, NROW_MAX, sub_counts);
     hp_prof_end(c, tok, HP_PROF_CONTRACT, 0);
     struct {
         int32_t cnt[3];
@@ -1874,9 +1877,9 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
         unsigned long long total;
         int32_t small_max, pad;
         unsigned long long spill;
-        int32_t sub[2];
+        int32_t sub[3], pad2;
     } h;
-    static_assert(sizeof(h) == 6 * sizeof(unsigned long long), "the six scalar slots");
+    static_assert(sizeof(h) == 7 * sizeof(unsigned long long), "the seven scalar slots");
     HP_TRY(hp_read_scalars(c, sc, sizeof(h), &h));
     const bool any_long = h.cnt[0] + h.cnt[1] + h.cnt[2] > 0;
     ContractSrc src{rinfo, g.adjncy, g.adjwgt, g.cmap};
@@ -1936,10 +1939,15 @@ int contract_level(hp_context *c, HpLevel &g, int32_t cn, HpLevel &cg)
                       (cta_radix_smem<MROW_THREADS, MROW_MAX>()), lists + 3 * (int64_t)cn, &sub_counts[0], src, toff,
                       tk, tw, ucnt, kbits, 0, wchk, c->d_status);
         if (!smem_dense && !hybrid && h.sub[1] > 0)
-            HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
-                      (unsigned)std::min<int64_t>(h.sub[1], c->sm_count * 3), CROW_THREADS,
-                      (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + 4 * (int64_t)cn, &sub_counts[1], src, toff,
+            HP_LAUNCH(c, (contract_cta_radix_kernel<NROW_THREADS, NROW_MAX>),
+                      (unsigned)std::min<int64_t>(h.sub[1], c->sm_count * 6), NROW_THREADS,
+                      (cta_radix_smem<NROW_THREADS, NROW_MAX>()), lists + 4 * (int64_t)cn, &sub_counts[1], src, toff,
                       tk, tw, ucnt, kbits, MROW_MAX, wchk, c->d_status);
+        if (!smem_dense && !hybrid && h.sub[2] > 0)
+            HP_LAUNCH(c, (contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>),
+                      (unsigned)std::min<int64_t>(h.sub[2], c->sm_count * 3), CROW_THREADS,
+                      (cta_radix_smem<CROW_THREADS, CROW_MAX>()), lists + 5 * (int64_t)cn, &sub_counts[2], src, toff,
+                      tk, tw, ucnt, kbits, NROW_MAX, wchk, c->d_status);
         if (!smem_dense && !hybrid && h.cnt[2] > 0)
             HP_LAUNCH(c, (contract_cta_radix_kernel<XROW_THREADS, XROW_MAX>),
                       (unsigned)std::min<int64_t>(h.cnt[2], c->sm_count), XROW_THREADS,
@@ -2010,6 +2018,9 @@ int hp_coarsen_init()
     HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<MROW_THREADS, MROW_MAX>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_radix_smem<MROW_THREADS, MROW_MAX>()));
+    HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<NROW_THREADS, NROW_MAX>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)cta_radix_smem<NROW_THREADS, NROW_MAX>()));
     HP_CUDA(cudaFuncSetAttribute(contract_cta_radix_kernel<CROW_THREADS, CROW_MAX>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)cta_radix_smem<CROW_THREADS, CROW_MAX>()));
