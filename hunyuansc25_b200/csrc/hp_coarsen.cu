@@ -185,7 +185,9 @@ pref_big_kernel(const int32_t *__restrict__ list, const int32_t *__restrict__ d_
 // later round the first cached candidate that is still unmatched is exactly the
 // best eligible neighbour; if the cache held fewer than TOPK candidates its
 // exhaustion means none is left.  Only a vertex whose full cache was matched
-// away rescans its row.  Results equal a full rescan every round.
+// away rescans its row.  Results equal a full rescan every round.  (Eight
+// candidates made the R-MAT matching slower: the first round's scans nearly
+// doubled and the later rounds did not get cheaper.)
 constexpr int TOPK = 4;
 
 // The TOPK best candidates of a row, kept by a whole warp: every lane holds the
@@ -280,17 +282,25 @@ __device__ __forceinline__ void scan_row_top(WarpTop &t, int32_t v, int32_t j0, 
     }
 }
 
-// Later rounds: the proposal from the cache, or -2 when the row must be rescanned.
+// Later rounds: the proposal from the cache, or -2 when the row must be
+// rescanned.  All 32 lanes call with the same v: lane q < TOPK checks entry q,
+// so the cache costs two dependent loads whatever its length.  The first entry
+// (in cache order) that is empty (-1: the cache held every eligible candidate)
+// or still unmatched (the best now) decides.
+static_assert(TOPK <= 32, "one cache entry per lane");
 __device__ __forceinline__ int32_t cached_proposal(const int32_t *__restrict__ cand, int32_t v,
                                                   const int32_t *__restrict__ elig)
 {
-#pragma unroll
-    for (int q = 0; q < TOPK; q++) {
-        const int32_t cu = cand[(int64_t)v * TOPK + q];
-        if (cu < 0) return -1;                  // the cache held every eligible candidate
-        if (elig[cu] != INT_MAX) return cu;     // still unmatched: the best now
-    }
-    return -2;
+    const int lane = threadIdx.x & 31;
+    const int32_t cu = lane < TOPK ? cand[(int64_t)v * TOPK + lane] : INT_MAX;
+    const bool empty = lane < TOPK && cu < 0;
+    const bool live = lane < TOPK && cu >= 0 && elig[cu] != INT_MAX;
+    const unsigned em = __ballot_sync(HP_FULL_MASK, empty), lm = __ballot_sync(HP_FULL_MASK, live);
+    const unsigned ev = em | lm;
+    if (!ev) return -2;
+    const int f = __ffs(ev) - 1;
+    const int32_t pick = __shfl_sync(HP_FULL_MASK, cu, f);
+    return (em >> f) & 1u ? -1 : pick;
 }
 
 __global__ void __launch_bounds__(256)
